@@ -1,0 +1,229 @@
+/*
+ * xfd_engine.h -- C ABI of the B200 FDTD engine (libxfd_engine.so).
+ *
+ * The engine owns every device buffer of one 3-D FDTD simulation and runs its
+ * time loop on one GPU.  Host code (the C++20 xfdtd::Simulation library, or
+ * any FFI) computes the FP64 set-up data -- material classes, curl factors,
+ * CPML grading, TFSF incident tables, ADE and lumped coefficients, NF2FF
+ * phasors -- and hands it over through these calls.  Host pointers are only
+ * borrowed for the duration of a call.  No call throws; each returns an
+ * xfd_status and xfd_last_error() describes the most recent failure.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the EMinsight/XFDTD_CORE source tree).  The reference has no C ABI: its
+ * hot path is a set of virtual C++ interfaces driven by Domain::run
+ * (src/domain/domain.cpp:82-135).
+ *
+ * Lattice layout.  Every field component, the per-lattice material-class
+ * index and the CPML auxiliaries live on the (nx+1) x (ny+1) x (nz+1) node
+ * lattice, k fastest.  Component arrays keep the reference shapes
+ * (Ex(nx,ny+1,nz+1) ... Hz(nx,ny,nz+1), src/simulation/simulation.cpp:514-528)
+ * at the host boundary; the device pads rows to a 32-element pitch.
+ *
+ * Component order everywhere: 0=Ex 1=Ey 2=Ez 3=Hx 4=Hy 5=Hz; axes 0=x 1=y 2=z;
+ * the tangential axes of axis c are a=(c+1)%3 and b=(c+2)%3.
+ */
+#ifndef XFD_ENGINE_H_
+#define XFD_ENGINE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct xfd_engine xfd_engine;
+
+typedef enum {
+  XFD_OK = 0,
+  XFD_ERR_INVALID_ARGUMENT = 1,
+  XFD_ERR_CUDA = 2,
+  XFD_ERR_UNSUPPORTED = 3,
+  XFD_ERR_STATE = 4,
+  XFD_ERR_OUT_OF_MEMORY = 5,
+  XFD_ERR_NUMERIC = 6
+} xfd_status;
+
+typedef enum { XFD_FP64 = 0, XFD_FP32 = 1 } xfd_precision;
+
+typedef struct {
+  int32_t nx, ny, nz;   /* cells, CPML included */
+  int32_t precision;    /* xfd_precision of fields, coefficients, CPML and ADE state */
+  int64_t n_steps;      /* steps of the run: sizes the per-step source tables */
+  double dt;
+  int32_t device;       /* CUDA device ordinal */
+} xfd_grid_desc;
+
+/* Creates an engine with zeroed fields and no boundaries or sources.
+ * Replaces: Simulation::init's EMF/coefficient allocation
+ * (src/simulation/simulation.cpp:319-371, :514-528). */
+xfd_status xfd_create(const xfd_grid_desc* grid, xfd_engine** out);
+
+/* Frees every device and pinned buffer of the engine. */
+void xfd_destroy(xfd_engine* e);
+
+/* Message of the last failed call on `e` (or of the last failed xfd_create
+ * when e is NULL).  Valid until the next call on the same engine. */
+const char* xfd_last_error(const xfd_engine* e);
+
+/* Material classes.  `table` holds n_classes rows of 12 doubles: (ca, cb) for
+ * Ex, Ey, Ez, Hx, Hy, Hz, where the E update of component c is
+ *   E_c = ca*E_c + cb*( fe_a[x_a]*(H_b - H_b[x_a-1]) - fe_b[x_b]*(H_a - H_a[x_b-1]) )
+ * and the H update
+ *   H_c = ca*H_c + cb*( fh_b[x_b]*(E_a[x_b+1] - E_a) - fh_a[x_a]*(E_b[x_a+1] - E_b) )
+ * with the per-axis curl factors of xfd_set_curl_factors.  `lattice_class`
+ * gives the class of every lattice node ((nx+1)*(ny+1)*(nz+1), k fastest).
+ * Replaces: the 18 full-grid FDTDUpdateCoefficient arrays
+ * (include/xfdtd/calculation_param/fdtd_update_coefficient.h:102-121) filled by
+ * CalculationParam::calculateCoefficient (src/calculation_param/calculation_param.cpp:170-264). */
+xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t n_classes,
+                                    const uint16_t* lattice_class);
+
+/* Per-axis curl factors.  fe[a] has n_a+1 entries, 1/(h_size * kappa_e);
+ * fh[a] has n_a entries, 1/(e_size * kappa_h) (kappa = 1 outside CPML).
+ * Replaces: the grid sizes folded into the coefficients
+ * (calculation_param.cpp:235-263) and the kappa division of
+ * PML::correctCoefficientX/Y/Z (src/boundary/pml.cpp:286-524). */
+xfd_status xfd_set_curl_factors(xfd_engine* e, const double* const fe[3], const double* const fh[3]);
+
+/* One CPML slab (one PML boundary).  E corrections act on layers
+ * [e_start, e_start+thickness) of the slab axis, H corrections on
+ * [h_start, h_start+thickness); a_*, b_* have `thickness` entries indexed by
+ * layer.  Slabs are applied in the order they are added.
+ * Replaces: PML::generateDomainCorrector (src/boundary/pml.cpp:246-284) and
+ * PMLCorrector<xyz>::correctE/correctH (src/include/boundary/pml_corrector.h:178-382). */
+typedef struct {
+  int32_t axis;
+  int32_t negative;
+  int32_t thickness;
+  int32_t e_start, h_start;
+  const double *a_e, *b_e, *a_h, *b_h;
+} xfd_cpml_slab;
+xfd_status xfd_add_cpml(xfd_engine* e, const xfd_cpml_slab* slab);
+
+/* TFSF3D plane-wave source.  e_inc (n_steps x aux) and h_inc
+ * (n_steps x (aux-1)) are the FP64 1-D incident grid for every step; p_int[a]
+ * (box size + 1 entries) and p_half[a] (box size + 2) the projections.
+ * Replaces: TFSF3D::generateCorrector (src/waveform_source/tfsf_3d.cpp:21-45),
+ * TFSF3DCorrector::correctE/correctH (src/waveform_source/tfsf_corrector.cpp:177-232). */
+typedef struct {
+  int32_t box_s[3], box_e[3];
+  int32_t aux;
+  const double* e_inc;
+  const double* h_inc;
+  const double* p_int[3];
+  const double* p_half[3];
+  double ca[3], cb[3];
+  double te[3], th[3];
+} xfd_tfsf_desc;
+xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* tfsf);
+
+/* Lumped current source on a box of E_comp nodes [box_s, box_e): per step
+ * E += coff[node] * waveform[t].  coff is box-shaped (k fastest); waveform has
+ * n_steps entries.  Replaces: CurrentSource::generateCorrector
+ * (src/object/lumped_element/current_source.cpp:198-222) and
+ * CurrentSourceCorrector::correctE (src/object/lumped_element/lumped_element_corrrector.cpp:24-37). */
+xfd_status xfd_add_current_source(xfd_engine* e, int32_t comp, const int32_t box_s[3],
+                                  const int32_t box_e[3], const double* coff,
+                                  const double* waveform);
+
+/* Dispersive (ADE) E nodes on a compacted list.  kind 0 = modified Lorentz
+ * (J, J_prev, E_prev), 1 = Drude, 2 = Debye.  mat_coeff holds, per material,
+ * 2 + 7*n_poles doubles: c_e_j_sum, c_e_e_prev, then per pole
+ * (c_j_j, c_j_j_prev, c_j_e_next, c_j_e, c_j_e_prev, c_j_sum_j, c_j_sum_j_prev).
+ * Entry n updates component comp[n] at lattice node (i,j,k) = node[3n..3n+2]
+ * with material material[n].  The E coefficients of these nodes must already
+ * be the overwritten ADE ones in the class table.
+ * Replaces: Simulation::buildDispersiveSpace (src/simulation/simulation.cpp:745-829)
+ * and MLorentzUpdator / DrudeADEUpdator3D / DebyeADEUpdator3D::updateE
+ * (src/updator/m_lor_ade_updator.cpp:21-140,
+ *  src/include/updator/ade_updator/template_ade_update_scheme.h:14-88). */
+typedef struct {
+  int32_t kind;
+  int32_t n_poles;
+  int32_t n_materials;
+  const double* mat_coeff;
+  int64_t n_entries;
+  const uint8_t* comp;
+  const int32_t* node;
+  const uint8_t* material;
+} xfd_ade_desc;
+xfd_status xfd_set_ade(xfd_engine* e, const xfd_ade_desc* ade);
+
+/* Frequency-domain NF2FF on the six Huygens faces.  Face d (XN XP YN YP ZN ZP)
+ * covers nodes [task_s[d], task_e[d]) (empty when any extent is <= 0).
+ * te / th are the FP64 phasors dt*exp(-j 2 pi f (t+1) dt) and
+ * dt*exp(-j 2 pi f (t+1/2) dt), laid out (n_freq, n_steps, re/im).  Each step
+ * adds `scale` times the step's term (scale = n_freq reproduces the
+ * reference's per-step nF-fold accumulation).  Surface samples are batched
+ * `batch` steps before the FP64 DFT accumulation.
+ * Replaces: NFFFTFrequencyDomain::update (src/nffft/nffft_frequency_domain.cpp:45-53)
+ * -> FDPlaneData::update/calculateJ/calculateM (src/nffft/nffft_fd_data_update.cpp:6-122). */
+typedef struct {
+  int32_t n_freq;
+  int32_t batch;
+  int32_t task_s[6][3];
+  int32_t task_e[6][3];
+  const double* te;
+  const double* th;
+  double scale;
+} xfd_nf2ff_desc;
+xfd_status xfd_set_nf2ff(xfd_engine* e, const xfd_nf2ff_desc* nf);
+
+/* Accumulated J/M surface currents, complex interleaved, laid out
+ * [freq][face][quantity ja jb ma mb][face nodes, k fastest].  `count` gets the
+ * number of complex values.  Flushes a partial sample batch first.
+ * Replaces: FDPlaneData's _ja/_jb/_ma/_mb arrays (src/nffft/nffft_fd_data.cpp:21-63). */
+xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* count);
+
+/* Movie monitor: every `interval` steps (from step 0) the box [box_s, box_e)
+ * of `field` is recorded into a device frame store.
+ * Replaces: MovieMonitor::update -> FieldMonitor::output
+ * (src/monitor/movie_monitor.cpp:26-34, src/monitor/field_monitor.cpp:82-96). */
+xfd_status xfd_add_movie(xfd_engine* e, int32_t field, const int32_t box_s[3],
+                         const int32_t box_e[3], int32_t interval, int32_t* id);
+
+/* Copies the frames recorded so far (in the engine precision) into `out`.
+ * Replaces: Monitor::output (src/monitor/monitor.cpp:42-54). */
+xfd_status xfd_get_movie_frames(xfd_engine* e, int32_t id, void* out, int64_t capacity_bytes,
+                                int64_t* n_frames);
+
+/* Field exchange in the reference shapes, elements in the engine precision
+ * (double for XFD_FP64, float for XFD_FP32).  fields[0..5] = Ex..Hz.
+ * Replaces: direct access to EMF (include/xfdtd/electromagnetic_field/electromagnetic_field.h:18-126). */
+xfd_status xfd_upload_fields(xfd_engine* e, const void* const fields[6]);
+xfd_status xfd_download_fields(xfd_engine* e, void* const fields[6]);
+
+/* One field component, `field` 0..5, in its reference shape. */
+xfd_status xfd_download_field(xfd_engine* e, int32_t field, void* out);
+
+/* Advances n_steps time steps (captured as CUDA graphs where possible).
+ * Asynchronous with respect to the host; xfd_sync waits.
+ * Replaces: Simulation::run() -> Domain::run (src/simulation/simulation.cpp:291-317,
+ * src/domain/domain.cpp:45-138). */
+xfd_status xfd_run(xfd_engine* e, int64_t n_steps);
+xfd_status xfd_sync(xfd_engine* e);
+
+/* Steps completed (queued) so far. */
+int64_t xfd_current_step(const xfd_engine* e);
+
+/* Engine options: "graph" (0/1, default 1), "graph_chunk" (steps per graph,
+ * default 32), "kernel" (0 = split H/E sweeps, 1 = fused H-then-E sweep). */
+xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value);
+
+/* The CUDA stream the engine launches on (a cudaStream_t), for callers that
+ * time the engine with events on that stream. */
+void* xfd_stream(xfd_engine* e);
+
+/* Number of kernel launches per time step of the current configuration. */
+int32_t xfd_launches_per_step(const xfd_engine* e);
+
+/* Algorithmic DRAM bytes per time step of the stencil sweep (fields read and
+ * written once, class index, CPML auxiliaries) -- the roofline numerator. */
+int64_t xfd_stencil_bytes_per_step(const xfd_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XFD_ENGINE_H_ */

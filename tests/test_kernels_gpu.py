@@ -1,0 +1,108 @@
+"""Kernel-level parity: each CUDA kernel of the engine, driven through the C
+ABI, against the oracle's restatement of the reference loops on the same
+seeded inputs (tests/cases.py).  FP64 tolerance: relative L2 <= 1e-12 per
+field component (the reference's FP64 path; the two sides differ only in
+rounding order and FMA contraction).  FP32 form: <= 1e-5 after a few steps."""
+import numpy as np
+import pytest
+
+from tests.cases import KernelCase, rel_l2
+from xfdtd_core_b200 import scene as S
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+
+
+def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True):
+    orc = case.oracle()
+    orc.run(steps)
+    eng = case.engine(precision=precision, n_steps=max(steps, 8))
+    eng.set_option("graph", int(graph))
+    eng.run(steps)
+    eng.sync()
+    got = eng.download_fields()
+    want = orc.e + orc.h
+    errs = [rel_l2(got[c], want[c]) for c in range(6)]
+    assert max(errs) <= tol, errs
+    return eng, orc
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_yee_cpml_fp64(seed):
+    _compare(KernelCase(n=(9, 10, 11), seed=seed), steps=4)
+
+
+def test_yee_no_cpml_fp64():
+    _compare(KernelCase(n=(12, 7, 9), seed=3, slabs=()), steps=3)
+
+
+def test_yee_cpml_fp32():
+    _compare(KernelCase(n=(9, 10, 11), seed=4), steps=3, precision=1, tol=1e-5)
+
+
+def test_graph_matches_eager():
+    c = KernelCase(n=(10, 9, 8), seed=5)
+    a = c.engine(n_steps=64)
+    a.set_option("graph", 1)
+    a.set_option("graph_chunk", 8)
+    a.run(40)
+    b = c.engine(n_steps=64)
+    b.set_option("graph", 0)
+    b.run(40)
+    fa, fb = a.download_fields(), b.download_fields()
+    for x, y in zip(fa, fb):
+        assert np.array_equal(x, y)
+
+
+def test_tfsf_faces_fp64():
+    sc = S.dielectric_sphere(steps=24, dl=0.35 / 16, radius=0.06, pml=4, tfsf_start=6,
+                             movie_interval=0)
+    from oracle.reference_model import RefSimulation
+    r = RefSimulation(sc)
+    # Let the pulse reach the box: start from the incident grid of late steps.
+    case = KernelCase(n=(r.nx, r.ny, r.nz), seed=6, field_scale=1e-3)
+    t = dict(r.tfsf)
+    t["e_inc"] = np.ascontiguousarray(np.roll(t["e_inc"], -12, axis=0))
+    t["h_inc"] = np.ascontiguousarray(np.roll(t["h_inc"], -12, axis=0))
+    case.tfsf = t
+    orc = case.oracle()
+    orc.run(6)
+    eng = case.engine(n_steps=24)
+    eng.run(6)
+    eng.sync()
+    got = eng.download_fields()
+    want = orc.e + orc.h
+    errs = [rel_l2(got[c], want[c]) for c in range(6)]
+    assert max(errs) <= FP64_TOL, errs
+
+
+def test_lumped_current_source_fp64():
+    case = KernelCase(n=(9, 10, 11), seed=7)
+    case.add_lumped(comp=2, s=(3, 4, 4), e=(5, 6, 6), n_steps=8)
+    case.add_lumped(comp=0, s=(2, 2, 2), e=(3, 4, 3), n_steps=8)
+    _compare(case, steps=5)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_ade_fp64(kind):
+    case = KernelCase(n=(9, 10, 11), seed=8 + kind, slabs=())
+    case.add_ade(kind=kind, n_poles=2, n_mat=3)
+    _compare(case, steps=5)
+
+
+def test_ade_fp32():
+    case = KernelCase(n=(9, 10, 11), seed=12, slabs=())
+    case.add_ade(kind=0, n_poles=1, n_mat=2)
+    _compare(case, steps=3, precision=1, tol=1e-5)
+
+
+def test_nf2ff_fp64():
+    case = KernelCase(n=(10, 11, 12), seed=13)
+    case.add_nf2ff(nf=3, nt=8, dist=2, batch=3)
+    eng, orc = _compare(case, steps=7)
+    got = eng.nf2ff()
+    acc = orc.nf2ff["acc"]
+    want = acc[0::2] + 1j * acc[1::2]
+    assert got.shape == want.shape
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= FP64_TOL

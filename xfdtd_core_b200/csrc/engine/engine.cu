@@ -1,0 +1,973 @@
+// C-ABI implementation of the B200 FDTD engine (include/xfd_engine.h).
+//
+// One engine = one simulation on one GPU.  The host hands over FP64 set-up
+// data; the engine converts it to its precision (fields, class table, curl
+// factors, CPML and ADE state in FP32 or FP64; TFSF tables, lumped sources and
+// NF2FF phasors/accumulators always FP64), keeps everything resident in HBM
+// and runs the time loop on one stream, captured into CUDA graphs of whole
+// step chunks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "xfd_engine.h"
+
+using namespace xfd;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct MovieH {
+  MovieD d;
+  long long n_nodes;
+  long long recorded;  // frames written so far
+};
+
+struct LumpedH {
+  int comp;
+  std::vector<long long> node;
+  std::vector<double> coff;
+  std::vector<double> wave;
+};
+
+}  // namespace
+
+struct xfd_engine {
+  int device = 0;
+  int precision = XFD_FP64;
+  size_t wsize = 8;
+  Lat L{};
+  long long n_lat = 0;  // NX * NY * KP
+  int64_t n_steps = 0;
+  double dt = 0;
+  std::string err;
+  cudaStream_t stream = nullptr;
+
+  std::vector<void*> allocs;
+  void* f[6] = {};
+  void** d_fields = nullptr;  // device array of the 6 field pointers
+  uint16_t* cls = nullptr;
+  void* tab = nullptr;
+  int n_classes = 0;
+  void* fe[3] = {};
+  void* fh[3] = {};
+  bool have_classes = false, have_curl = false;
+
+  struct Slab {
+    int m, neg, n, e_lo, h_lo;
+    void *a_e, *b_e, *a_h, *b_h;
+    void* psi_e[2];
+    void* psi_h[2];
+  };
+  std::vector<Slab> slabs;
+
+  bool have_tfsf = false;
+  TfsfD tfsf{};
+  TfsfGroupD tfsf_groups[4]{};  // H group 1, H group 2, E group 1, E group 2
+
+  std::vector<LumpedH> lumped_h;
+  LumpedD lumped{};
+  bool lumped_dirty = false;
+
+  int ade_kind = -1;
+  AdeD<double> ade64{};
+  AdeD<float> ade32{};
+
+  bool have_nf2ff = false;
+  Nf2ffD nf2ff{};
+  long long nf_sampled_since_flush = 0;
+  long long nf_last_flush_step = 0;
+
+  std::vector<MovieH> movies;
+
+  long long* d_step = nullptr;
+  int* d_err = nullptr;
+  int64_t host_step = 0;
+
+  // graph
+  bool use_graph = true;
+  int graph_chunk = 32;
+  int kernel_mode = 0;
+  cudaGraphExec_t graph_exec = nullptr;
+  long long graph_len = 0;
+  bool graph_dirty = true;
+};
+
+namespace {
+
+xfd_status fail(xfd_engine* e, xfd_status s, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (e) e->err = buf;
+  else g_create_error = buf;
+  return s;
+}
+
+#define CUDA_TRY(e, call)                                                                   \
+  do {                                                                                      \
+    cudaError_t _c = (call);                                                                \
+    if (_c != cudaSuccess)                                                                  \
+      return fail((e), XFD_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_c));      \
+  } while (0)
+
+xfd_status dev_alloc(xfd_engine* e, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t c = cudaMalloc(p, bytes);
+  if (c != cudaSuccess) {
+    *p = nullptr;
+    return fail(e, c == cudaErrorMemoryAllocation ? XFD_ERR_OUT_OF_MEMORY : XFD_ERR_CUDA,
+                "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(c));
+  }
+  e->allocs.push_back(*p);
+  c = cudaMemsetAsync(*p, 0, bytes, e->stream);
+  if (c != cudaSuccess) return fail(e, XFD_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(c));
+  return XFD_OK;
+}
+
+// Uploads `n` doubles, converted to the engine precision.
+xfd_status upload_real(xfd_engine* e, void** dst, const double* src, size_t n) {
+  xfd_status s = dev_alloc(e, dst, n * e->wsize);
+  if (s != XFD_OK) return s;
+  if (n == 0) return XFD_OK;
+  if (e->precision == XFD_FP64) {
+    CUDA_TRY(e, cudaMemcpyAsync(*dst, src, n * 8, cudaMemcpyHostToDevice, e->stream));
+  } else {
+    std::vector<float> tmp(src, src + n);
+    CUDA_TRY(e, cudaMemcpyAsync(*dst, tmp.data(), n * 4, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  }
+  return XFD_OK;
+}
+
+template <typename U>
+xfd_status upload_raw(xfd_engine* e, U** dst, const U* src, size_t n) {
+  void* p = nullptr;
+  xfd_status s = dev_alloc(e, &p, n * sizeof(U));
+  if (s != XFD_OK) return s;
+  *dst = static_cast<U*>(p);
+  if (n) CUDA_TRY(e, cudaMemcpyAsync(p, src, n * sizeof(U), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
+// Extent of component c (0..5) in the reference shape.
+void comp_shape(const Lat& L, int c, int out[3]) {
+  const int n[3] = {L.nx, L.ny, L.nz};
+  const int ax = c % 3;
+  const bool is_e = c < 3;
+  for (int d = 0; d < 3; ++d) {
+    if (is_e) out[d] = (d == ax) ? n[d] : n[d] + 1;
+    else out[d] = (d == ax) ? n[d] + 1 : n[d];
+  }
+}
+
+cudaMemcpy3DParms copy_parms(const xfd_engine* e, int c, void* dev, void* host, bool to_dev,
+                             size_t elem) {
+  int shp[3];
+  comp_shape(e->L, c, shp);
+  cudaMemcpy3DParms p{};
+  cudaPitchedPtr hp = make_cudaPitchedPtr(host, (size_t)shp[2] * elem, (size_t)shp[2],
+                                          (size_t)shp[1]);
+  cudaPitchedPtr dp = make_cudaPitchedPtr(dev, (size_t)e->L.KP * elem, (size_t)e->L.KP,
+                                          (size_t)e->L.NY);
+  p.extent = make_cudaExtent((size_t)shp[2] * elem, (size_t)shp[1], (size_t)shp[0]);
+  if (to_dev) {
+    p.srcPtr = hp;
+    p.dstPtr = dp;
+    p.kind = cudaMemcpyHostToDevice;
+  } else {
+    p.srcPtr = dp;
+    p.dstPtr = hp;
+    p.kind = cudaMemcpyDeviceToHost;
+  }
+  return p;
+}
+
+template <typename T>
+YeeP<T> yee_params(xfd_engine* e) {
+  YeeP<T> p{};
+  p.L = e->L;
+  for (int c = 0; c < 6; ++c) p.f[c] = static_cast<T*>(e->f[c]);
+  p.cls = e->cls;
+  p.tab = static_cast<const T*>(e->tab);
+  for (int a = 0; a < 3; ++a) {
+    p.fe[a] = static_cast<const T*>(e->fe[a]);
+    p.fh[a] = static_cast<const T*>(e->fh[a]);
+  }
+  p.n_slab = (int)e->slabs.size();
+  for (size_t s = 0; s < e->slabs.size(); ++s) {
+    const auto& S = e->slabs[s];
+    auto& D = p.slab[s];
+    D.m = S.m;
+    D.n = S.n;
+    D.e_lo = S.e_lo;
+    D.h_lo = S.h_lo;
+    D.a_e = static_cast<const T*>(S.a_e);
+    D.b_e = static_cast<const T*>(S.b_e);
+    D.a_h = static_cast<const T*>(S.a_h);
+    D.b_h = static_cast<const T*>(S.b_h);
+    for (int w = 0; w < 2; ++w) {
+      D.psi_e[w] = static_cast<T*>(S.psi_e[w]);
+      D.psi_h[w] = static_cast<T*>(S.psi_h[w]);
+    }
+  }
+  return p;
+}
+
+unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b); }
+
+// Launches one time step (host step index t decides the periodic kernels).
+template <typename T>
+cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
+  cudaStream_t s = e->stream;
+  T* const* fields = reinterpret_cast<T* const*>(e->d_fields);
+  const YeeP<T> yp = yee_params<T>(e);
+  const dim3 blk(32, 8, 1);
+  const dim3 grd((unsigned)((e->L.nz + 1 + 31) / 32), (unsigned)((e->L.ny + 1 + 7) / 8),
+                 (unsigned)(e->L.nx + 1));
+  // H phase: updateH + CPML (fused) -> TFSF H faces.
+  k_update_h<T><<<grd, blk, 0, s>>>(yp);
+  if (e->have_tfsf) {
+    for (int g = 0; g < 2; ++g) {
+      const auto& G = e->tfsf_groups[g];
+      if (G.total > 0)
+        k_tfsf<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fields, e->d_step,
+                                                           e->d_err);
+    }
+  }
+  // E phase: ADE e_cur gather -> updateE + CPML -> ADE -> lumped -> TFSF E faces.
+  AdeD<T> ad{};
+  if (e->ade_kind >= 0) {
+    if constexpr (sizeof(T) == 8) ad = e->ade64; else ad = e->ade32;
+    k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+  }
+  k_update_e<T><<<grd, blk, 0, s>>>(yp);
+  if (e->ade_kind == 0) k_ade_update<T, 0><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+  if (e->ade_kind == 1) k_ade_update<T, 1><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+  if (e->ade_kind == 2) k_ade_update<T, 2><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+  if (e->lumped.n > 0)
+    k_lumped<T><<<blocks_for(e->lumped.n, 256), 256, 0, s>>>(e->lumped, fields, e->d_step);
+  if (e->have_tfsf) {
+    for (int g = 2; g < 4; ++g) {
+      const auto& G = e->tfsf_groups[g];
+      if (G.total > 0)
+        k_tfsf<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fields, e->d_step,
+                                                           e->d_err);
+    }
+  }
+  // record: monitors, then NF2FF (Domain::record, src/domain/domain.cpp:176-184).
+  for (auto& mv : e->movies) {
+    if (t % mv.d.interval == 0)
+      k_movie<T><<<blocks_for(mv.n_nodes, 256), 256, 0, s>>>(mv.d, e->L, fields, e->d_step);
+  }
+  if (e->have_nf2ff) {
+    k_nf2ff_sample<T><<<blocks_for(e->nf2ff.P, 256), 256, 0, s>>>(e->nf2ff, e->L, fields,
+                                                                  e->d_step);
+    if ((t + 1) % e->nf2ff.batch == 0) {
+      const size_t smem = (size_t)2 * e->nf2ff.nf * e->nf2ff.batch * sizeof(double2);
+      k_nf2ff_dft<8><<<blocks_for(4 * e->nf2ff.P, 256), 256, smem, s>>>(e->nf2ff, e->d_step, 0,
+                                                                        0);
+    }
+  }
+  k_advance<<<1, 1, 0, s>>>(e->d_step);
+  return cudaGetLastError();
+}
+
+cudaError_t enqueue_step(xfd_engine* e, long long t) {
+  return e->precision == XFD_FP64 ? enqueue_step_t<double>(e, t) : enqueue_step_t<float>(e, t);
+}
+
+// Steps between identical launch patterns: lcm of every periodic kernel's
+// period, replicated up to the configured chunk length.
+long long pattern_period(const xfd_engine* e) {
+  long long per = 1;
+  for (const auto& mv : e->movies) per = per / gcd_ll(per, mv.d.interval) * mv.d.interval;
+  if (e->have_nf2ff) per = per / gcd_ll(per, e->nf2ff.batch) * e->nf2ff.batch;
+  return per;
+}
+
+xfd_status ensure_ready(xfd_engine* e) {
+  if (!e->have_classes) return fail(e, XFD_ERR_STATE, "material classes not set");
+  if (!e->have_curl) return fail(e, XFD_ERR_STATE, "curl factors not set");
+  if (e->lumped_dirty) {
+    // Concatenate the current sources into one device list.
+    std::vector<long long> node;
+    std::vector<int> comp, src;
+    std::vector<double> coff, wave;
+    for (size_t q = 0; q < e->lumped_h.size(); ++q) {
+      const auto& l = e->lumped_h[q];
+      for (size_t n = 0; n < l.node.size(); ++n) {
+        node.push_back(l.node[n]);
+        comp.push_back(l.comp);
+        src.push_back((int)q);
+        coff.push_back(l.coff[n]);
+      }
+      wave.insert(wave.end(), l.wave.begin(), l.wave.end());
+    }
+    LumpedD d{};
+    d.n = (long long)node.size();
+    d.n_steps = (int)e->n_steps;
+    long long* dn = nullptr;
+    int *dc = nullptr, *ds = nullptr;
+    double *dco = nullptr, *dw = nullptr;
+    xfd_status st;
+    if ((st = upload_raw(e, &dn, node.data(), node.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dc, comp.data(), comp.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &ds, src.data(), src.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dco, coff.data(), coff.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dw, wave.data(), wave.size())) != XFD_OK) return st;
+    d.node = dn;
+    d.comp = dc;
+    d.source = ds;
+    d.coff = dco;
+    d.wave = dw;
+    e->lumped = d;
+    e->lumped_dirty = false;
+  }
+  return XFD_OK;
+}
+
+void drop_graph(xfd_engine* e) {
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  e->graph_exec = nullptr;
+  e->graph_len = 0;
+}
+
+xfd_status build_graph(xfd_engine* e, long long t0) {
+  drop_graph(e);
+  const long long per = pattern_period(e);
+  long long len = per;
+  while (len < e->graph_chunk) len += per;
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  for (long long s = 0; s < len; ++s) {
+    cudaError_t c = enqueue_step(e, t0 + s);
+    if (c != cudaSuccess) {
+      cudaGraph_t dummy;
+      cudaStreamEndCapture(e->stream, &dummy);
+      if (dummy) cudaGraphDestroy(dummy);
+      return fail(e, XFD_ERR_CUDA, "kernel launch during capture: %s", cudaGetErrorString(c));
+    }
+  }
+  CUDA_TRY(e, cudaStreamEndCapture(e->stream, &g));
+  cudaError_t c = cudaGraphInstantiate(&e->graph_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (c != cudaSuccess) return fail(e, XFD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(c));
+  e->graph_len = len;
+  e->graph_dirty = false;
+  return XFD_OK;
+}
+
+xfd_status flush_nf2ff(xfd_engine* e) {
+  if (!e->have_nf2ff) return XFD_OK;
+  const long long pending = e->host_step - e->nf_last_flush_step;
+  const long long done_batches = (e->host_step / e->nf2ff.batch) * e->nf2ff.batch;
+  // Steps after the last full batch boundary are not yet folded in.
+  const long long t0 = std::max(done_batches, e->nf_last_flush_step);
+  const long long nb = e->host_step - t0;
+  (void)pending;
+  if (nb > 0) {
+    const size_t smem = (size_t)2 * e->nf2ff.nf * e->nf2ff.batch * sizeof(double2);
+    k_nf2ff_dft<8><<<blocks_for(4 * e->nf2ff.P, 256), 256, smem, e->stream>>>(
+        e->nf2ff, e->d_step, (int)nb, t0);
+    CUDA_TRY(e, cudaGetLastError());
+    // Zero the folded slots so the batch-end DFT of this window adds nothing
+    // for them again.
+    const long long slot0 = t0 % e->nf2ff.batch;
+    CUDA_TRY(e, cudaMemsetAsync(e->nf2ff.sample + slot0 * 4 * e->nf2ff.P, 0,
+                                (size_t)nb * 4 * e->nf2ff.P * sizeof(double), e->stream));
+  }
+  e->nf_last_flush_step = e->host_step;
+  return XFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
+  if (!g || !out) return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+    return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "grid too small (%d, %d, %d)", g->nx, g->ny,
+                g->nz);
+  if (g->precision != XFD_FP64 && g->precision != XFD_FP32)
+    return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "unknown precision %d", g->precision);
+  if (g->n_steps < 0) return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "negative n_steps");
+  auto e = std::make_unique<xfd_engine>();
+  e->device = g->device;
+  cudaError_t c = cudaSetDevice(g->device);
+  if (c != cudaSuccess)
+    return fail(nullptr, XFD_ERR_CUDA, "cudaSetDevice(%d): %s", g->device, cudaGetErrorString(c));
+  c = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (c != cudaSuccess) return fail(nullptr, XFD_ERR_CUDA, "stream: %s", cudaGetErrorString(c));
+  e->precision = g->precision;
+  e->wsize = g->precision == XFD_FP64 ? 8 : 4;
+  e->n_steps = g->n_steps;
+  e->dt = g->dt;
+  e->L.nx = g->nx;
+  e->L.ny = g->ny;
+  e->L.nz = g->nz;
+  e->L.NY = g->ny + 1;
+  e->L.KP = ((g->nz + 1) + 31) / 32 * 32;
+  e->n_lat = (long long)(g->nx + 1) * e->L.NY * e->L.KP;
+  if (e->n_lat > (1LL << 40))
+    return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "grid too large");
+  xfd_engine* ep = e.get();
+  for (int k = 0; k < 6; ++k) {
+    if (dev_alloc(ep, &e->f[k], (size_t)e->n_lat * e->wsize) != XFD_OK) {
+      g_create_error = ep->err;
+      for (void* p : ep->allocs) cudaFree(p);
+      cudaStreamDestroy(ep->stream);
+      return g_create_error.find("cudaMalloc") != std::string::npos ? XFD_ERR_OUT_OF_MEMORY
+                                                                     : XFD_ERR_CUDA;
+    }
+  }
+  void* df = nullptr;
+  void* ds = nullptr;
+  void* de = nullptr;
+  if (dev_alloc(ep, &df, 6 * sizeof(void*)) != XFD_OK ||
+      dev_alloc(ep, &ds, sizeof(long long)) != XFD_OK || dev_alloc(ep, &de, sizeof(int)) != XFD_OK) {
+    g_create_error = ep->err;
+    for (void* p : ep->allocs) cudaFree(p);
+    cudaStreamDestroy(ep->stream);
+    return XFD_ERR_CUDA;
+  }
+  e->d_fields = static_cast<void**>(df);
+  e->d_step = static_cast<long long*>(ds);
+  e->d_err = static_cast<int*>(de);
+  c = cudaMemcpyAsync(e->d_fields, e->f, sizeof e->f, cudaMemcpyHostToDevice, e->stream);
+  if (c == cudaSuccess) c = cudaStreamSynchronize(e->stream);
+  if (c != cudaSuccess) {
+    g_create_error = cudaGetErrorString(c);
+    for (void* p : ep->allocs) cudaFree(p);
+    cudaStreamDestroy(ep->stream);
+    return XFD_ERR_CUDA;
+  }
+  *out = e.release();
+  return XFD_OK;
+}
+
+void xfd_destroy(xfd_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  drop_graph(e);
+  for (void* p : e->allocs) cudaFree(p);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+const char* xfd_last_error(const xfd_engine* e) {
+  return e ? e->err.c_str() : g_create_error.c_str();
+}
+
+xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t n_classes,
+                                    const uint16_t* lattice_class) {
+  if (!e || !table || !lattice_class || n_classes <= 0 || n_classes > 65536)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad material class arguments (n_classes=%d)",
+                n_classes);
+  const long long n_nodes = (long long)(e->L.nx + 1) * (e->L.ny + 1) * (e->L.nz + 1);
+  for (long long q = 0; q < n_nodes; ++q) {
+    if (lattice_class[q] >= n_classes)
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "class index %u at node %lld >= %d",
+                  lattice_class[q], q, n_classes);
+  }
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s = upload_real(e, &e->tab, table, (size_t)n_classes * 12);
+  if (s != XFD_OK) return s;
+  void* p = nullptr;
+  if ((s = dev_alloc(e, &p, (size_t)e->n_lat * sizeof(uint16_t))) != XFD_OK) return s;
+  e->cls = static_cast<uint16_t*>(p);
+  cudaMemcpy3DParms prm{};
+  const size_t rowb = (size_t)(e->L.nz + 1) * sizeof(uint16_t);
+  prm.srcPtr = make_cudaPitchedPtr(const_cast<uint16_t*>(lattice_class), rowb,
+                                   (size_t)(e->L.nz + 1), (size_t)(e->L.ny + 1));
+  prm.dstPtr = make_cudaPitchedPtr(p, (size_t)e->L.KP * sizeof(uint16_t), (size_t)e->L.KP,
+                                   (size_t)e->L.NY);
+  prm.extent = make_cudaExtent(rowb, (size_t)(e->L.ny + 1), (size_t)(e->L.nx + 1));
+  prm.kind = cudaMemcpyHostToDevice;
+  CUDA_TRY(e, cudaMemcpy3DAsync(&prm, e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  e->n_classes = n_classes;
+  e->have_classes = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_set_curl_factors(xfd_engine* e, const double* const fe[3],
+                                const double* const fh[3]) {
+  if (!e || !fe || !fh) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null curl factors");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+  for (int a = 0; a < 3; ++a) {
+    if (!fe[a] || !fh[a]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null curl factor axis %d", a);
+    std::vector<double> he(fe[a], fe[a] + n[a] + 1);
+    std::vector<double> hh(fh[a], fh[a] + n[a]);
+    hh.push_back(0.0);  // pad to n+1 so both tables share one length
+    xfd_status s = upload_real(e, &e->fe[a], he.data(), he.size());
+    if (s != XFD_OK) return s;
+    s = upload_real(e, &e->fh[a], hh.data(), hh.size());
+    if (s != XFD_OK) return s;
+  }
+  e->have_curl = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_add_cpml(xfd_engine* e, const xfd_cpml_slab* sl) {
+  if (!e || !sl) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null slab");
+  const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+  if (sl->axis < 0 || sl->axis > 2 || sl->thickness <= 0)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad CPML slab axis/thickness");
+  if (e->slabs.size() >= 6) return fail(e, XFD_ERR_UNSUPPORTED, "at most 6 CPML slabs");
+  const int m = sl->axis;
+  if (sl->e_start < 1 || sl->e_start + sl->thickness > n[m] + 1 || sl->h_start < 0 ||
+      sl->h_start + sl->thickness > n[m])
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "CPML layers out of the grid");
+  if (!sl->a_e || !sl->b_e || !sl->a_h || !sl->b_h)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "null CPML coefficient");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_engine::Slab S{};
+  S.m = m;
+  S.neg = sl->negative;
+  S.n = sl->thickness;
+  S.e_lo = sl->e_start;
+  S.h_lo = sl->h_start;
+  xfd_status s;
+  if ((s = upload_real(e, &S.a_e, sl->a_e, S.n)) != XFD_OK) return s;
+  if ((s = upload_real(e, &S.b_e, sl->b_e, S.n)) != XFD_OK) return s;
+  if ((s = upload_real(e, &S.a_h, sl->a_h, S.n)) != XFD_OK) return s;
+  if ((s = upload_real(e, &S.b_h, sl->b_h, S.n)) != XFD_OK) return s;
+  long long sz;
+  if (m == 0) sz = (long long)S.n * e->L.NY * e->L.KP;
+  else if (m == 1) sz = (long long)(e->L.nx + 1) * S.n * e->L.KP;
+  else sz = (long long)(e->L.nx + 1) * e->L.NY * S.n;
+  for (int w = 0; w < 2; ++w) {
+    if ((s = dev_alloc(e, &S.psi_e[w], (size_t)sz * e->wsize)) != XFD_OK) return s;
+    if ((s = dev_alloc(e, &S.psi_h[w], (size_t)sz * e->wsize)) != XFD_OK) return s;
+  }
+  e->slabs.push_back(S);
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* t) {
+  if (!e || !t) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null TFSF");
+  const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+  for (int a = 0; a < 3; ++a) {
+    if (t->box_s[a] < 1 || t->box_e[a] > n[a] - 1 || t->box_e[a] <= t->box_s[a])
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "TFSF box out of the grid on axis %d", a);
+    if (!t->p_int[a] || !t->p_half[a]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null projection");
+  }
+  if (t->aux < 3 || !t->e_inc || !t->h_inc) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad TFSF grid");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  TfsfD d{};
+  for (int a = 0; a < 3; ++a) {
+    d.bs[a] = t->box_s[a];
+    d.te[a] = t->te[a];
+    d.th[a] = t->th[a];
+  }
+  d.aux = t->aux;
+  xfd_status s;
+  double* p = nullptr;
+  if ((s = upload_raw(e, &p, t->e_inc, (size_t)e->n_steps * t->aux)) != XFD_OK) return s;
+  d.e_inc = p;
+  if ((s = upload_raw(e, &p, t->h_inc, (size_t)e->n_steps * (t->aux - 1))) != XFD_OK) return s;
+  d.h_inc = p;
+  for (int a = 0; a < 3; ++a) {
+    const int sz = t->box_e[a] - t->box_s[a];
+    if ((s = upload_raw(e, &p, t->p_int[a], (size_t)sz + 1)) != XFD_OK) return s;
+    d.p_int[a] = p;
+    if ((s = upload_raw(e, &p, t->p_half[a], (size_t)sz + 2)) != XFD_OK) return s;
+    d.p_half[a] = p;
+  }
+  e->tfsf = d;
+  // Pass table in the order of TFSF3DCorrector::correctE/correctH; group 1
+  // takes each component's first face axis, group 2 its second.
+  struct PassSpec { int axis, neg, field; };
+  static const PassSpec h1[6] = {{0, 1, 1}, {0, 0, 1}, {1, 1, 0}, {1, 0, 0}, {0, 1, 2}, {0, 0, 2}};
+  static const PassSpec h2[6] = {{2, 1, 0}, {2, 0, 0}, {1, 1, 2}, {1, 0, 2}, {2, 1, 1}, {2, 0, 1}};
+  static const PassSpec e1[6] = {{0, 1, 2}, {0, 0, 2}, {2, 1, 1}, {2, 0, 1}, {2, 1, 0}, {2, 0, 0}};
+  static const PassSpec e2[6] = {{1, 1, 2}, {1, 0, 2}, {0, 1, 1}, {0, 0, 1}, {1, 1, 0}, {1, 0, 0}};
+  const PassSpec* groups[4] = {h1, h2, e1, e2};
+  for (int g = 0; g < 4; ++g) {
+    TfsfGroupD G{};
+    G.n = 6;
+    const bool is_e = g >= 2;
+    long long begin = 0;
+    for (int q = 0; q < 6; ++q) {
+      const PassSpec& ps = groups[g][q];
+      TfsfPassD P{};
+      P.axis = ps.axis;
+      P.neg = ps.neg;
+      P.field = ps.field;
+      P.is_e = is_e;
+      const int m = ps.axis, A = (m + 1) % 3, B = (m + 2) % 3;
+      for (int a = 0; a < 3; ++a) {
+        P.s[a] = t->box_s[a];
+        P.e[a] = t->box_e[a];
+      }
+      // offset_a / offset_b (src/include/waveform_source/tfsf_corrector.h:122-140)
+      const bool off_a = (is_e && ps.field == B) || (!is_e && ps.field == A);
+      if (off_a) P.e[A] += 1; else P.e[B] += 1;
+      const int cs = ps.neg ? t->box_s[m] : t->box_e[m];
+      P.s[m] = cs;
+      P.e[m] = cs + 1;
+      const int equation_flag = is_e ? 1 : -1;
+      const int different_flag = (ps.field == A) ? -1 : 1;
+      const int direction_flag = ps.neg ? -1 : 1;
+      const double coef = is_e ? t->ca[m] : t->cb[m];
+      P.coeff = coef * (double)(equation_flag * different_flag * direction_flag);
+      P.begin = begin;
+      begin += (long long)(P.e[0] - P.s[0]) * (P.e[1] - P.s[1]) * (P.e[2] - P.s[2]);
+      G.pass[q] = P;
+    }
+    G.total = begin;
+    e->tfsf_groups[g] = G;
+  }
+  e->have_tfsf = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_add_current_source(xfd_engine* e, int32_t comp, const int32_t box_s[3],
+                                  const int32_t box_e[3], const double* coff,
+                                  const double* waveform) {
+  if (!e || !box_s || !box_e || !coff || !waveform || comp < 0 || comp > 2)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad current source arguments");
+  int shp[3];
+  comp_shape(e->L, comp, shp);
+  LumpedH l;
+  l.comp = comp;
+  for (int a = 0; a < 3; ++a) {
+    if (box_s[a] < 0 || box_e[a] > shp[a] || box_e[a] <= box_s[a])
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "current source box out of range on axis %d", a);
+  }
+  long long q = 0;
+  for (int i = box_s[0]; i < box_e[0]; ++i)
+    for (int j = box_s[1]; j < box_e[1]; ++j)
+      for (int k = box_s[2]; k < box_e[2]; ++k, ++q) {
+        l.node.push_back(lat_index(e->L, i, j, k));
+        l.coff.push_back(coff[q]);
+      }
+  l.wave.assign(waveform, waveform + e->n_steps);
+  e->lumped_h.push_back(std::move(l));
+  e->lumped_dirty = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_set_ade(xfd_engine* e, const xfd_ade_desc* a) {
+  if (!e || !a) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null ADE");
+  if (a->kind < 0 || a->kind > 2 || a->n_poles <= 0 || a->n_materials <= 0 ||
+      a->n_materials > 256 || a->n_entries < 0)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad ADE description");
+  if (e->ade_kind >= 0) return fail(e, XFD_ERR_STATE, "ADE already set");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  const long long n = a->n_entries;
+  std::vector<long long> node(n);
+  for (long long q = 0; q < n; ++q) {
+    const int c = a->comp[q];
+    const int i = a->node[3 * q], j = a->node[3 * q + 1], k = a->node[3 * q + 2];
+    int shp[3];
+    comp_shape(e->L, c, shp);
+    if (c > 2 || i < 0 || j < 0 || k < 0 || i >= shp[0] || j >= shp[1] || k >= shp[2] ||
+        a->material[q] >= a->n_materials)
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad ADE entry %lld", q);
+    node[q] = lat_index(e->L, i, j, k);
+  }
+  xfd_status s;
+  long long* dn = nullptr;
+  uint8_t *dc = nullptr, *dm = nullptr;
+  if ((s = upload_raw(e, &dn, node.data(), (size_t)n)) != XFD_OK) return s;
+  if ((s = upload_raw(e, &dc, a->comp, (size_t)n)) != XFD_OK) return s;
+  if ((s = upload_raw(e, &dm, a->material, (size_t)n)) != XFD_OK) return s;
+  void* coef = nullptr;
+  if ((s = upload_real(e, &coef, a->mat_coeff, (size_t)a->n_materials * (2 + 7 * a->n_poles))) !=
+      XFD_OK)
+    return s;
+  void *j = nullptr, *jp = nullptr, *ep = nullptr, *ec = nullptr;
+  if ((s = dev_alloc(e, &j, (size_t)n * a->n_poles * e->wsize)) != XFD_OK) return s;
+  if ((s = dev_alloc(e, &ec, (size_t)n * e->wsize)) != XFD_OK) return s;
+  if (a->kind == 0) {
+    if ((s = dev_alloc(e, &jp, (size_t)n * a->n_poles * e->wsize)) != XFD_OK) return s;
+    if ((s = dev_alloc(e, &ep, (size_t)n * e->wsize)) != XFD_OK) return s;
+  }
+  if (e->precision == XFD_FP64) {
+    AdeD<double> d{n, a->n_poles, dn, dc, dm, static_cast<double*>(coef), static_cast<double*>(j),
+                   static_cast<double*>(jp), static_cast<double*>(ep), static_cast<double*>(ec)};
+    e->ade64 = d;
+  } else {
+    AdeD<float> d{n, a->n_poles, dn, dc, dm, static_cast<float*>(coef), static_cast<float*>(j),
+                  static_cast<float*>(jp), static_cast<float*>(ep), static_cast<float*>(ec)};
+    e->ade32 = d;
+  }
+  e->ade_kind = a->kind;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_set_nf2ff(xfd_engine* e, const xfd_nf2ff_desc* d) {
+  if (!e || !d || d->n_freq <= 0 || !d->te || !d->th || d->batch <= 0 || d->batch > 1024)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad NF2FF description");
+  if (e->have_nf2ff) return fail(e, XFD_ERR_STATE, "NF2FF already set");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  Nf2ffD nf{};
+  nf.nf = d->n_freq;
+  nf.batch = d->batch;
+  nf.scale = d->scale;
+  nf.n_steps = (int)e->n_steps;
+  long long total = 0;
+  const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+  for (int f = 0; f < 6; ++f) {
+    nf.begin[f] = total;
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) {
+      nf.s[f][a] = d->task_s[f][a];
+      nf.e[f][a] = d->task_e[f][a];
+      if (nf.e[f][a] <= nf.s[f][a]) empty = true;
+    }
+    if (empty) {
+      for (int a = 0; a < 3; ++a) nf.s[f][a] = nf.e[f][a] = 0;
+      continue;
+    }
+    for (int a = 0; a < 3; ++a) {
+      // interpolation stencils read one node on either side
+      if (nf.s[f][a] < 1 || nf.e[f][a] > n[a])
+        return fail(e, XFD_ERR_INVALID_ARGUMENT, "NF2FF face %d out of range", f);
+    }
+    total += (long long)(nf.e[f][0] - nf.s[f][0]) * (nf.e[f][1] - nf.s[f][1]) *
+             (nf.e[f][2] - nf.s[f][2]);
+  }
+  nf.begin[6] = total;
+  nf.P = total;
+  xfd_status s;
+  void* p = nullptr;
+  if ((s = dev_alloc(e, &p, (size_t)nf.batch * 4 * total * sizeof(double))) != XFD_OK) return s;
+  nf.sample = static_cast<double*>(p);
+  if ((s = dev_alloc(e, &p, (size_t)nf.nf * 4 * total * sizeof(double2))) != XFD_OK) return s;
+  nf.acc = static_cast<double2*>(p);
+  double* q = nullptr;
+  if ((s = upload_raw(e, &q, d->te, (size_t)nf.nf * e->n_steps * 2)) != XFD_OK) return s;
+  nf.te = reinterpret_cast<const double2*>(q);
+  if ((s = upload_raw(e, &q, d->th, (size_t)nf.nf * e->n_steps * 2)) != XFD_OK) return s;
+  nf.th = reinterpret_cast<const double2*>(q);
+  const size_t smem = (size_t)2 * nf.nf * nf.batch * sizeof(double2);
+  if (smem > 200 * 1024) return fail(e, XFD_ERR_UNSUPPORTED, "n_freq * batch too large");
+  CUDA_TRY(e, cudaFuncSetAttribute(k_nf2ff_dft<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  e->nf2ff = nf;
+  e->have_nf2ff = true;
+  e->nf_last_flush_step = e->host_step;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* count) {
+  if (!e || !e->have_nf2ff) return fail(e, XFD_ERR_STATE, "no NF2FF");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s = flush_nf2ff(e);
+  if (s != XFD_OK) return s;
+  const Nf2ffD& nf = e->nf2ff;
+  const long long total = (long long)nf.nf * 4 * nf.P;
+  if (count) *count = total;
+  if (!out) return XFD_OK;
+  if (capacity < total) return fail(e, XFD_ERR_INVALID_ARGUMENT, "NF2FF buffer too small");
+  std::vector<double2> h((size_t)total);
+  CUDA_TRY(e, cudaMemcpyAsync(h.data(), nf.acc, total * sizeof(double2), cudaMemcpyDeviceToHost,
+                              e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  // device [f][q][p] (p over all faces) -> [f][face][q][face nodes]
+  long long o = 0;
+  for (int f = 0; f < nf.nf; ++f)
+    for (int d = 0; d < 6; ++d)
+      for (int q = 0; q < 4; ++q)
+        for (long long p = nf.begin[d]; p < nf.begin[d + 1]; ++p, ++o) {
+          const double2 z = h[((size_t)f * 4 + q) * nf.P + p];
+          out[2 * o] = z.x;
+          out[2 * o + 1] = z.y;
+        }
+  return XFD_OK;
+}
+
+xfd_status xfd_add_movie(xfd_engine* e, int32_t field, const int32_t box_s[3],
+                         const int32_t box_e[3], int32_t interval, int32_t* id) {
+  if (!e || !box_s || !box_e || field < 0 || field > 5 || interval <= 0)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad movie arguments");
+  int shp[3];
+  comp_shape(e->L, field, shp);
+  MovieH m{};
+  m.d.field = field;
+  m.d.interval = interval;
+  long long nn = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (box_s[a] < 0 || box_e[a] > shp[a] || box_e[a] <= box_s[a])
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "movie box out of range on axis %d", a);
+    m.d.s[a] = box_s[a];
+    m.d.e[a] = box_e[a];
+    nn *= box_e[a] - box_s[a];
+  }
+  m.n_nodes = nn;
+  m.d.max_frames = (e->n_steps + interval - 1) / interval;
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s = dev_alloc(e, &m.d.store, (size_t)m.d.max_frames * nn * e->wsize);
+  if (s != XFD_OK) return s;
+  e->movies.push_back(m);
+  if (id) *id = (int32_t)e->movies.size() - 1;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_get_movie_frames(xfd_engine* e, int32_t id, void* out, int64_t capacity_bytes,
+                                int64_t* n_frames) {
+  if (!e || id < 0 || id >= (int32_t)e->movies.size())
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad movie id");
+  const auto& m = e->movies[id];
+  long long frames = (e->host_step + m.d.interval - 1) / m.d.interval;
+  frames = std::min(frames, m.d.max_frames);
+  if (n_frames) *n_frames = frames;
+  if (!out) return XFD_OK;
+  const size_t bytes = (size_t)frames * m.n_nodes * e->wsize;
+  if ((size_t)capacity_bytes < bytes) return fail(e, XFD_ERR_INVALID_ARGUMENT, "movie buffer too small");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  CUDA_TRY(e, cudaMemcpyAsync(out, m.d.store, bytes, cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
+xfd_status xfd_upload_fields(xfd_engine* e, const void* const fields[6]) {
+  if (!e || !fields) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null fields");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  for (int c = 0; c < 6; ++c) {
+    if (!fields[c]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null field %d", c);
+    cudaMemcpy3DParms p = copy_parms(e, c, e->f[c], const_cast<void*>(fields[c]), true, e->wsize);
+    CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
+  }
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
+xfd_status xfd_download_field(xfd_engine* e, int32_t field, void* out) {
+  if (!e || !out || field < 0 || field > 5) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad field");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  cudaMemcpy3DParms p = copy_parms(e, field, e->f[field], out, false, e->wsize);
+  CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
+xfd_status xfd_download_fields(xfd_engine* e, void* const fields[6]) {
+  if (!e || !fields) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null fields");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  for (int c = 0; c < 6; ++c) {
+    if (!fields[c]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null field %d", c);
+    cudaMemcpy3DParms p = copy_parms(e, c, e->f[c], fields[c], false, e->wsize);
+    CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
+  }
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
+xfd_status xfd_run(xfd_engine* e, int64_t n) {
+  if (!e) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null engine");
+  if (n < 0) return fail(e, XFD_ERR_INVALID_ARGUMENT, "negative step count");
+  if (e->host_step + n > e->n_steps)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "run past n_steps (%lld + %lld > %lld)",
+                (long long)e->host_step, (long long)n, (long long)e->n_steps);
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s = ensure_ready(e);
+  if (s != XFD_OK) return s;
+  long long left = n;
+  const long long per = pattern_period(e);
+  while (left > 0) {
+    const bool aligned = (e->host_step % per) == 0;
+    if (e->use_graph && aligned) {
+      if (e->graph_dirty || !e->graph_exec) {
+        if ((s = build_graph(e, e->host_step)) != XFD_OK) return s;
+      }
+      if (left >= e->graph_len) {
+        CUDA_TRY(e, cudaGraphLaunch(e->graph_exec, e->stream));
+        e->host_step += e->graph_len;
+        left -= e->graph_len;
+        continue;
+      }
+    }
+    cudaError_t c = enqueue_step(e, e->host_step);
+    if (c != cudaSuccess) return fail(e, XFD_ERR_CUDA, "step launch: %s", cudaGetErrorString(c));
+    e->host_step += 1;
+    left -= 1;
+  }
+  return XFD_OK;
+}
+
+xfd_status xfd_sync(xfd_engine* e) {
+  if (!e) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null engine");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  int err = 0;
+  CUDA_TRY(e, cudaMemcpy(&err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return fail(e, XFD_ERR_NUMERIC, "TFSF projection left the incident grid");
+  return XFD_OK;
+}
+
+int64_t xfd_current_step(const xfd_engine* e) { return e ? e->host_step : -1; }
+
+xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
+  if (!e || !name) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null option");
+  if (!strcmp(name, "graph")) {
+    e->use_graph = value != 0;
+  } else if (!strcmp(name, "graph_chunk")) {
+    if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "graph_chunk range");
+    e->graph_chunk = (int)value;
+  } else if (!strcmp(name, "kernel")) {
+    if (value != 0) return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
+    e->kernel_mode = (int)value;
+  } else {
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
+  }
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+void* xfd_stream(xfd_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+int32_t xfd_launches_per_step(const xfd_engine* e) {
+  if (!e) return 0;
+  int n = 2 + 1;  // H sweep, E sweep, step counter
+  if (e->have_tfsf) n += 4;
+  if (e->ade_kind >= 0) n += 2;
+  if (!e->lumped_h.empty()) n += 1;
+  if (e->have_nf2ff) n += 1;
+  return n;
+}
+
+int64_t xfd_stencil_bytes_per_step(const xfd_engine* e) {
+  if (!e) return 0;
+  const long long cells = (long long)e->L.nx * e->L.ny * e->L.nz;
+  long long b = cells * (12LL * (long long)e->wsize + 2);
+  for (const auto& s : e->slabs) {
+    const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+    long long slab_cells = (long long)s.n;
+    for (int a = 0; a < 3; ++a)
+      if (a != s.m) slab_cells *= n[a];
+    b += slab_cells * 8LL * (long long)e->wsize;
+  }
+  return b;
+}
+
+}  // extern "C"

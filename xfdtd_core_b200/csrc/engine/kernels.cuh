@@ -1,0 +1,553 @@
+// Device kernels of the B200 FDTD engine.
+//
+// Data layout: every field component, the uint16 material-class index and the
+// per-slab CPML psi arrays are stored on the (nx+1) x (ny+1) x (nz+1) node
+// lattice, k fastest, with rows padded to a pitch KP (a multiple of 32
+// elements) so that a warp of 32 consecutive k reads whole 128 B (FP32) or
+// 256 B (FP64) lines.  A component that is shorter than the lattice along an
+// axis (Ex has nx entries along x, ...) leaves the last plane unused.
+//
+// The update of component c reads its (ca, cb) pair from the class table
+// row of its node and the per-axis curl factors fe/fh, which fold in the cell
+// size and the CPML kappa:
+//   E_c = ca E_c + cb (fe_a (H_b - H_b[x_a-1]) - fe_b (H_a - H_a[x_b-1]))
+//   H_c = ca H_c + cb (fh_b (E_a[x_b+1] - E_a) - fh_a (E_b[x_a+1] - E_b))
+// with a = (c+1)%3, b = (c+2)%3 -- the structure of eNext/hNext in the
+// reference (src/include/updator/update_scheme.h:26-62) with its coefficient
+// arrays factored into class x axis terms.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace xfd {
+
+struct Lat {
+  int nx, ny, nz;
+  int NY;  // ny + 1
+  int KP;  // k pitch
+};
+
+__host__ __device__ __forceinline__ long long lat_index(const Lat& L, int i, int j, int k) {
+  return ((long long)i * L.NY + j) * L.KP + k;
+}
+
+// One CPML slab.  psi[0] belongs to the slab's tangential component A =
+// (m+1)%3, psi[1] to B = (m+2)%3.  Layer l of the slab is coordinate
+// lo + l along m.  psi layout: m=0 -> [l][j][k] (pitch NY*KP, KP),
+// m=1 -> [i][l][k] (pitch n*KP, KP), m=2 -> [i][j][l] (pitch NY*n, n).
+template <typename T>
+struct SlabD {
+  int m, n, e_lo, h_lo;
+  const T* a_e;
+  const T* b_e;
+  const T* a_h;
+  const T* b_h;
+  T* psi_e[2];
+  T* psi_h[2];
+};
+
+template <typename T>
+__device__ __forceinline__ long long psi_index(const SlabD<T>& s, const Lat& L, int i, int j,
+                                               int k, int l) {
+  if (s.m == 0) return ((long long)l * L.NY + j) * L.KP + k;
+  if (s.m == 1) return ((long long)i * s.n + l) * L.KP + k;
+  return ((long long)i * L.NY + j) * s.n + l;
+}
+
+template <typename T>
+struct YeeP {
+  Lat L;
+  T* f[6];  // Ex Ey Ez Hx Hy Hz
+  const uint16_t* cls;
+  const T* tab;  // n_classes x 12: (ca, cb) of Ex Ey Ez Hx Hy Hz
+  const T* fe[3];
+  const T* fh[3];
+  int n_slab;
+  SlabD<T> slab[6];
+};
+
+// ---------------------------------------------------------------------------
+// H sweep.  One thread per lattice node (i, j, k); each handles Hx, Hy, Hz.
+// Main update over i<nx, j<ny, k<nz (BasicUpdator::updateH,
+// src/updator/basic_updator.cpp:23-36), then the CPML correction of every
+// slab whose H layers contain the node (PMLCorrector<xyz>::correctH,
+// src/include/boundary/pml_corrector.h:290-382) over the component's whole
+// transverse extent, in slab insertion order.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_h(YeeP<T> p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  const Lat L = p.L;
+  if (k > L.nz || j > L.ny || i > L.nx) return;
+  const long long id = lat_index(L, i, j, k);
+  const int x[3] = {i, j, k};
+  const int n[3] = {L.nx, L.ny, L.nz};
+  const long long st[3] = {(long long)L.NY * L.KP, (long long)L.KP, 1};
+  const bool main_rng = (i < L.nx) && (j < L.ny) && (k < L.nz);
+  const T* row = p.tab + (size_t)p.cls[id] * 12;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    bool valid = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) valid = valid && ((d == c) ? (x[d] <= n[d]) : (x[d] < n[d]));
+    if (!valid) continue;
+    const int ta = (c + 1) % 3, tb = (c + 2) % 3;
+    T* H = p.f[3 + c];
+    const T ca = row[6 + 2 * c];
+    const T cb = row[7 + 2 * c];
+    T h = H[id];
+    if (main_rng) {
+      const T* Ea = p.f[ta];
+      const T* Eb = p.f[tb];
+      const T d_a = Ea[id + st[tb]] - Ea[id];
+      const T d_b = Eb[id + st[ta]] - Eb[id];
+      h = ca * h + cb * (p.fh[tb][x[tb]] * d_a - p.fh[ta][x[ta]] * d_b);
+    }
+    for (int s = 0; s < p.n_slab; ++s) {
+      const SlabD<T>& sl = p.slab[s];
+      if (sl.m == c) continue;
+      const int l = x[sl.m] - sl.h_lo;
+      if (l < 0 || l >= sl.n) continue;
+      const int which = (c == (sl.m + 1) % 3) ? 0 : 1;
+      // H_A differences E_B, H_B differences E_A, forward along m.
+      const T* D = p.f[which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3];
+      const T diff = D[id + st[sl.m]] - D[id];
+      T* ps = sl.psi_h[which] + psi_index(sl, L, i, j, k, l);
+      const T psi = sl.b_h[l] * *ps + sl.a_h[l] * diff;
+      *ps = psi;
+      h += (which == 0 ? cb : -cb) * psi;
+    }
+    H[id] = h;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// E sweep.  Main update over x_c < n_c and 1 <= x < n across
+// (BasicUpdator3D::updateE, src/updator/basic_updator_3d.cpp:38-69), then
+// CPML (PMLCorrector<xyz>::correctE, pml_corrector.h:178-288): layers
+// [e_lo, e_lo + n) along m, whole transverse extent.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_e(YeeP<T> p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  const Lat L = p.L;
+  if (k > L.nz || j > L.ny || i > L.nx) return;
+  const long long id = lat_index(L, i, j, k);
+  const int x[3] = {i, j, k};
+  const int n[3] = {L.nx, L.ny, L.nz};
+  const long long st[3] = {(long long)L.NY * L.KP, (long long)L.KP, 1};
+  const T* row = p.tab + (size_t)p.cls[id] * 12;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    bool valid = true, main_rng = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d == c) {
+        valid = valid && (x[d] < n[d]);
+      } else {
+        valid = valid && (x[d] <= n[d]);
+        main_rng = main_rng && (x[d] >= 1) && (x[d] < n[d]);
+      }
+    }
+    if (!valid) continue;
+    main_rng = main_rng && valid;
+    const int ta = (c + 1) % 3, tb = (c + 2) % 3;
+    T* E = p.f[c];
+    const T ca = row[2 * c];
+    const T cb = row[2 * c + 1];
+    T e = E[id];
+    if (main_rng) {
+      const T* Ha = p.f[3 + ta];
+      const T* Hb = p.f[3 + tb];
+      const T d_a = Hb[id] - Hb[id - st[ta]];
+      const T d_b = Ha[id] - Ha[id - st[tb]];
+      e = ca * e + cb * (p.fe[ta][x[ta]] * d_a - p.fe[tb][x[tb]] * d_b);
+    }
+    for (int s = 0; s < p.n_slab; ++s) {
+      const SlabD<T>& sl = p.slab[s];
+      if (sl.m == c) continue;
+      const int l = x[sl.m] - sl.e_lo;
+      if (l < 0 || l >= sl.n) continue;
+      const int which = (c == (sl.m + 1) % 3) ? 0 : 1;
+      // E_A differences H_B, E_B differences H_A, backward along m.
+      const T* D = p.f[3 + (which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3)];
+      const T diff = D[id] - D[id - st[sl.m]];
+      T* ps = sl.psi_e[which] + psi_index(sl, L, i, j, k, l);
+      const T psi = sl.b_e[l] * *ps + sl.a_e[l] * diff;
+      *ps = psi;
+      e += (which == 0 ? -cb : cb) * psi;
+    }
+    E[id] = e;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TFSF3D face corrections (TFSF3DCorrector, src/waveform_source/tfsf_corrector.cpp:177-232,
+// correctTFSF, src/include/waveform_source/tfsf_corrector.h:89-229).  The 12
+// passes of one phase go in two launches so that the passes that meet on a
+// box edge (same component, different face axes) are applied in the
+// reference order; within a launch no two threads touch the same node.
+// The incident value is interpolated in FP64 from the 1-D grid row of the
+// current step (exInc..hzInc, tfsf_corrector.cpp:16-122).
+// ---------------------------------------------------------------------------
+struct TfsfD {
+  int bs[3];
+  int aux;
+  const double* e_inc;
+  const double* h_inc;
+  const double* p_int[3];
+  const double* p_half[3];
+  double te[3], th[3];
+};
+
+struct TfsfPassD {
+  int axis, neg, field, is_e;
+  int s[3], e[3];
+  long long begin;
+  double coeff;
+};
+
+struct TfsfGroupD {
+  int n;
+  long long total;
+  TfsfPassD pass[6];
+};
+
+__device__ __forceinline__ double tfsf_incident(const TfsfD& tf, bool inc_e, int comp,
+                                                long long t, const int x[3], int* err) {
+  int r[3] = {x[0] - tf.bs[0], x[1] - tf.bs[1], x[2] - tf.bs[2]};
+  double parts[3];
+  double proj;
+  if (inc_e) {
+    r[comp] += 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) parts[d] = (d == comp) ? tf.p_half[d][r[d]] : tf.p_int[d][r[d]];
+    proj = parts[0] + parts[1] + parts[2];
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (d != comp) r[d] += 1;
+      parts[d] = (d == comp) ? tf.p_int[d][r[d]] : tf.p_half[d][r[d]];
+    }
+    proj = parts[0] + parts[1] + parts[2] - 0.5;
+  }
+  long long idx = (long long)proj;
+  const double w = proj - (double)idx;
+  const int len = inc_e ? tf.aux : tf.aux - 1;
+  if (idx < 0 || idx + 1 >= len) {
+    *err = 1;
+    idx = idx < 0 ? 0 : (long long)len - 2;
+  }
+  const double* row = inc_e ? tf.e_inc + t * tf.aux : tf.h_inc + t * (tf.aux - 1);
+  const double tr = inc_e ? tf.te[comp] : tf.th[comp];
+  return tr * ((1 - w) * row[idx] + w * row[idx + 1]);
+}
+
+template <typename T>
+__global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const long long* step,
+                       int* err) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= g.total) return;
+  int q = 0;
+  while (q + 1 < g.n && tid >= g.pass[q + 1].begin) ++q;
+  const TfsfPassD& P = g.pass[q];
+  long long r = tid - P.begin;
+  const int e2 = P.e[2] - P.s[2], e1 = P.e[1] - P.s[1];
+  const int k = P.s[2] + (int)(r % e2);
+  r /= e2;
+  const int j = P.s[1] + (int)(r % e1);
+  r /= e1;
+  const int i = P.s[0] + (int)r;
+  const long long t = *step;
+  int xi[3] = {i, j, k};
+  int xf[3] = {i, j, k};
+  const int m = P.axis;
+  bool inc_e;
+  if (P.is_e) {
+    inc_e = false;  // E face reads the H incident half a cell outside
+    if (P.neg) xi[m] -= 1;
+  } else {
+    inc_e = true;   // H face corrects the node half a cell outside
+    if (P.neg) xf[m] -= 1;
+  }
+  const int dual = (P.field == (m + 1) % 3) ? (m + 2) % 3 : (m + 1) % 3;
+  int e_flag = 0;
+  const double v = tfsf_incident(tf, inc_e, dual, t, xi, &e_flag);
+  if (e_flag) atomicOr(err, 1);
+  T* F = fields[(P.is_e ? 0 : 3) + P.field];
+  const long long id = lat_index(L, xf[0], xf[1], xf[2]);
+  F[id] = (T)((double)F[id] + v * P.coeff);
+}
+
+// ---------------------------------------------------------------------------
+// Lumped current sources: E += coff * waveform[t]
+// (CurrentSourceCorrector::correctE, src/object/lumped_element/lumped_element_corrrector.cpp:24-37).
+// ---------------------------------------------------------------------------
+struct LumpedD {
+  long long n;
+  int n_steps;
+  const long long* node;
+  const int* comp;
+  const int* source;
+  const double* coff;
+  const double* wave;  // n_sources x n_steps
+};
+
+template <typename T>
+__global__ void k_lumped(LumpedD lp, T* const* fields, const long long* step) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= lp.n) return;
+  const long long t = *step;
+  T* E = fields[lp.comp[e]];
+  const long long id = lp.node[e];
+  const double w = lp.wave[(long long)lp.source[e] * lp.n_steps + t];
+  E[id] = (T)((double)E[id] + lp.coff[e] * w);
+}
+
+// ---------------------------------------------------------------------------
+// ADE on the compacted dispersive node list.  The E sweep has already
+// written the plain Yee value with the ADE-overwritten (ca, cb) of the node;
+// k_ade_update adds the polarisation terms and advances J
+// (MLorentzUpdator::updateE/updateJ/calculateJSum/recordEPrevious,
+//  src/updator/m_lor_ade_updator.cpp:21-140; Drude/Debye J updates,
+//  src/updator/ade_updator/drude_ade_updator.cpp:31-39,
+//  src/updator/ade_updator/debye_ade_updator.cpp:43-51).  k_ade_gather saves
+// the node's field value before the E sweep (the reference's e_cur).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct AdeD {
+  long long n;
+  int np;
+  const long long* node;
+  const uint8_t* comp;
+  const uint8_t* mat;
+  const T* coef;  // per material: cejsum, ceep, then per pole 7 values
+  T* j;           // np x n
+  T* jp;          // np x n (kind 0)
+  T* ep;          // n (kind 0)
+  T* ec;          // n
+};
+
+template <typename T>
+__global__ void k_ade_gather(AdeD<T> a, T* const* fields) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n) return;
+  a.ec[e] = fields[a.comp[e]][a.node[e]];
+}
+
+template <typename T, int KIND>
+__global__ void k_ade_update(AdeD<T> a, T* const* fields) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n) return;
+  const T* cf = a.coef + (size_t)a.mat[e] * (2 + 7 * a.np);
+  T* E = fields[a.comp[e]];
+  const long long id = a.node[e];
+  const T e_yee = E[id];
+  const T e_cur = a.ec[e];
+  const T e_prev = (KIND == 0) ? a.ep[e] : T(0);
+  T j_sum = 0;
+  for (int p = 0; p < a.np; ++p) {
+    const T* pc = cf + 2 + 7 * p;
+    const long long q = (long long)p * a.n + e;
+    if (KIND == 0) {
+      j_sum += pc[5] * a.j[q] + pc[6] * a.jp[q];
+    } else {
+      j_sum += pc[5] * a.j[q];
+    }
+  }
+  const T e_next = (cf[1] * e_prev + e_yee) + cf[0] * j_sum;
+  E[id] = e_next;
+  for (int p = 0; p < a.np; ++p) {
+    const T* pc = cf + 2 + 7 * p;
+    const long long q = (long long)p * a.n + e;
+    if (KIND == 0) {
+      const T jn = pc[2] * e_next + pc[3] * e_cur + pc[4] * e_prev + pc[0] * a.j[q] +
+                   pc[1] * a.jp[q];
+      a.jp[q] = a.j[q];
+      a.j[q] = jn;
+    } else if (KIND == 1) {
+      a.j[q] = pc[0] * a.j[q] + pc[3] * (e_next + e_cur);
+    } else {
+      a.j[q] = pc[0] * a.j[q] + pc[3] * (e_next - e_cur);
+    }
+  }
+  if (KIND == 0) a.ep[e] = e_cur;
+}
+
+// ---------------------------------------------------------------------------
+// NF2FF.  k_nf2ff_sample writes, per Huygens node, the four signed
+// surface-centre field values of the step into slot t % batch of an FP64
+// sample buffer (calculateJ/calculateM, src/nffft/nffft_fd_data_update.cpp:22-122,
+// with interpolateSurfaceCenter, src/include/nffft/interpolate_scheme.h:19-138);
+// k_nf2ff_dft folds a full batch into the complex FP64 accumulators with the
+// per-step phasors (FDPlaneData::initDFT, src/nffft/nffft_fd_data.cpp:65-76).
+// ---------------------------------------------------------------------------
+struct Nf2ffD {
+  int nf, batch;
+  int s[6][3], e[6][3];
+  long long begin[7];  // node offsets per face, begin[6] = total
+  long long P;
+  double* sample;      // batch x 4 x P
+  double2* acc;        // (nf*4) x P
+  const double2* te;   // nf x n_steps
+  const double2* th;
+  int n_steps;
+  double scale;
+};
+
+template <typename T>
+__device__ __forceinline__ T fld(const T* F, const Lat& L, int i, int j, int k) {
+  return F[lat_index(L, i, j, k)];
+}
+
+template <typename T>
+__device__ double surf_e(T* const* f, const Lat& L, int m, int comp, int i, int j, int k) {
+  int q[3] = {i, j, k};
+  q[3 - m - comp] += 1;
+  const T* E = f[comp];
+  return 0.5 * ((double)fld(E, L, q[0], q[1], q[2]) + (double)fld(E, L, i, j, k));
+}
+
+template <typename T>
+__device__ double surf_h(T* const* f, const Lat& L, int m, int comp, int i, int j, int k) {
+  const T* H = f[3 + comp];
+  if (m == 0) {
+    int p1[3] = {i, j, k};
+    p1[comp] += 1;
+    return 0.25 * ((double)fld(H, L, p1[0], p1[1], p1[2]) + (double)fld(H, L, i, j, k) +
+                   (double)fld(H, L, p1[0] - 1, p1[1], p1[2]) + (double)fld(H, L, i - 1, j, k));
+  }
+  if (m == 1) {
+    if (comp == 2)
+      return 0.25 * ((double)fld(H, L, i, j, k + 1) + (double)fld(H, L, i, j, k) +
+                     (double)fld(H, L, i, j - 1, k + 1) + (double)fld(H, L, i, j - 1, k));
+    return 0.25 * ((double)fld(H, L, i + 1, j, k) + (double)fld(H, L, i, j, k) +
+                   (double)fld(H, L, i + 1, j - 1, k) + (double)fld(H, L, i, j - 1, k));
+  }
+  if (comp == 0)
+    return 0.25 * ((double)fld(H, L, i + 1, j, k) + (double)fld(H, L, i, j, k) +
+                   (double)fld(H, L, i, j, k - 1) + (double)fld(H, L, i + 1, j, k - 1));
+  return 0.25 * ((double)fld(H, L, i, j, k) + (double)fld(H, L, i, j + 1, k) +
+                 (double)fld(H, L, i, j, k - 1) + (double)fld(H, L, i, j + 1, k - 1));
+}
+
+template <typename T>
+__global__ void k_nf2ff_sample(Nf2ffD nf, Lat L, T* const* fields, const long long* step) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nf.P) return;
+  int d = 0;
+  while (d < 5 && p >= nf.begin[d + 1]) ++d;
+  long long r = p - nf.begin[d];
+  const int* s = nf.s[d];
+  const int* e = nf.e[d];
+  const int e2 = e[2] - s[2], e1 = e[1] - s[1];
+  const int k = s[2] + (int)(r % e2);
+  r /= e2;
+  const int j = s[1] + (int)(r % e1);
+  r /= e1;
+  const int i = s[0] + (int)r;
+  const int m = d / 2;
+  const bool positive = (d % 2) == 1;
+  const int A = (m + 1) % 3, B = (m + 2) % 3;
+  const long long slot = *step % nf.batch;
+  double* out = nf.sample + slot * 4 * nf.P + p;
+  const double cj1 = positive ? -1.0 : 1.0, cj2 = positive ? 1.0 : -1.0;
+  out[0] = cj1 * surf_h(fields, L, m, B, i, j, k);
+  out[nf.P] = cj2 * surf_h(fields, L, m, A, i, j, k);
+  out[2 * nf.P] = -cj1 * surf_e(fields, L, m, B, i, j, k);
+  out[3 * nf.P] = -cj2 * surf_e(fields, L, m, A, i, j, k);
+}
+
+// Batch DFT: acc[f][q][p] += scale * sum_s sample[s][q][p] * phasor_q[f][t0+s].
+// One thread per (q, p); phasors of the batch staged in shared memory.
+template <int FCH>
+__global__ void __launch_bounds__(256) k_nf2ff_dft(Nf2ffD nf, const long long* step, int nb,
+                                                   long long t0_explicit) {
+  extern __shared__ double2 sh[];  // [2][nf][batch]
+  long long t0;
+  if (nb <= 0) {
+    nb = nf.batch;
+    t0 = *step + 1 - nf.batch;
+  } else {
+    t0 = t0_explicit;
+  }
+  // Steps t0 .. t0+nb-1 lie in one batch window: slots slot0 .. slot0+nb-1.
+  const long long slot0 = t0 % nf.batch;
+  for (int x = threadIdx.x; x < nf.nf * nb; x += blockDim.x) {
+    const int f = x / nb, s = x % nb;
+    sh[f * nf.batch + s] = nf.th[(long long)f * nf.n_steps + t0 + s];
+    sh[nf.nf * nf.batch + f * nf.batch + s] = nf.te[(long long)f * nf.n_steps + t0 + s];
+  }
+  __syncthreads();
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= 4 * nf.P) return;
+  const int q = (int)(tid / nf.P);
+  const long long p = tid % nf.P;
+  const double2* ph = sh + (q < 2 ? 0 : nf.nf * nf.batch);
+  const double* smp = nf.sample + (slot0 * 4 + q) * nf.P + p;
+  for (int f0 = 0; f0 < nf.nf; f0 += FCH) {
+    double re[FCH], im[FCH];
+#pragma unroll
+    for (int u = 0; u < FCH; ++u) re[u] = im[u] = 0.0;
+    for (int s = 0; s < nb; ++s) {
+      const double v = smp[(long long)s * 4 * nf.P];
+#pragma unroll
+      for (int u = 0; u < FCH; ++u) {
+        if (f0 + u < nf.nf) {
+          const double2 z = ph[(f0 + u) * nf.batch + s];
+          re[u] += v * z.x;
+          im[u] += v * z.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < FCH; ++u) {
+      if (f0 + u < nf.nf) {
+        double2* a = nf.acc + ((long long)(f0 + u) * 4 + q) * nf.P + p;
+        double2 z = *a;
+        z.x += nf.scale * re[u];
+        z.y += nf.scale * im[u];
+        *a = z;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Movie frame: copy the monitor box of one component into frame t/interval
+// (FieldMonitor::output, src/monitor/field_monitor.cpp:82-96).
+// ---------------------------------------------------------------------------
+struct MovieD {
+  int field;
+  int s[3], e[3];
+  int interval;
+  long long max_frames;
+  void* store;
+};
+
+template <typename T>
+__global__ void k_movie(MovieD mv, Lat L, T* const* fields, const long long* step) {
+  const int e2 = mv.e[2] - mv.s[2], e1 = mv.e[1] - mv.s[1], e0 = mv.e[0] - mv.s[0];
+  const long long n = (long long)e0 * e1 * e2;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= n) return;
+  const long long frame = *step / mv.interval;
+  if (frame >= mv.max_frames) return;
+  long long r = tid;
+  const int k = mv.s[2] + (int)(r % e2);
+  r /= e2;
+  const int j = mv.s[1] + (int)(r % e1);
+  r /= e1;
+  const int i = mv.s[0] + (int)r;
+  T* out = static_cast<T*>(mv.store) + frame * n + tid;
+  *out = fields[mv.field][lat_index(L, i, j, k)];
+}
+
+__global__ void k_advance(long long* step) { *step += 1; }
+
+}  // namespace xfd

@@ -1,0 +1,311 @@
+"""ctypes binding of the engine C ABI (include/xfd_engine.h).
+
+This is the Python side of the drop-in boundary: every call goes through
+``lib/libxfd_engine.so``; there is no Python or CPU implementation of the
+time step behind it.  If the library is missing, or no CUDA device is
+present, the calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+
+FP64, FP32 = 0, 1
+FIELD_NAMES = ("EX", "EY", "EZ", "HX", "HY", "HZ")
+_STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "UNSUPPORTED", 4: "STATE",
+           5: "OUT_OF_MEMORY", 6: "NUMERIC"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("precision", _i32),
+                ("n_steps", _i64), ("dt", ctypes.c_double), ("device", _i32)]
+
+
+class CpmlSlab(ctypes.Structure):
+    _fields_ = [("axis", _i32), ("negative", _i32), ("thickness", _i32), ("e_start", _i32),
+                ("h_start", _i32), ("a_e", _dp), ("b_e", _dp), ("a_h", _dp), ("b_h", _dp)]
+
+
+class TfsfDesc(ctypes.Structure):
+    _fields_ = [("box_s", _i32 * 3), ("box_e", _i32 * 3), ("aux", _i32), ("e_inc", _dp),
+                ("h_inc", _dp), ("p_int", _dp * 3), ("p_half", _dp * 3),
+                ("ca", ctypes.c_double * 3), ("cb", ctypes.c_double * 3),
+                ("te", ctypes.c_double * 3), ("th", ctypes.c_double * 3)]
+
+
+class AdeDesc(ctypes.Structure):
+    _fields_ = [("kind", _i32), ("n_poles", _i32), ("n_materials", _i32), ("mat_coeff", _dp),
+                ("n_entries", _i64), ("comp", ctypes.POINTER(ctypes.c_uint8)),
+                ("node", ctypes.POINTER(_i32)), ("material", ctypes.POINTER(ctypes.c_uint8))]
+
+
+class Nf2ffDesc(ctypes.Structure):
+    _fields_ = [("n_freq", _i32), ("batch", _i32), ("task_s", (_i32 * 3) * 6),
+                ("task_e", (_i32 * 3) * 6), ("te", _dp), ("th", _dp), ("scale", ctypes.c_double)]
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def library_path() -> str:
+    return _build.ENGINE_LIB
+
+
+def load(build_if_missing: bool = True):
+    """Loads libxfd_engine.so (building it first if absent and nvcc exists)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.ENGINE_LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise EngineError(f"engine library not built: {path}")
+        _build.build_engine()
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sig = {
+        "xfd_create": ([ctypes.POINTER(GridDesc), ctypes.POINTER(vp)], ctypes.c_int),
+        "xfd_destroy": ([vp], None),
+        "xfd_last_error": ([vp], ctypes.c_char_p),
+        "xfd_set_material_classes": ([vp, _dp, _i32, ctypes.POINTER(ctypes.c_uint16)],
+                                     ctypes.c_int),
+        "xfd_set_curl_factors": ([vp, _dp * 3, _dp * 3], ctypes.c_int),
+        "xfd_add_cpml": ([vp, ctypes.POINTER(CpmlSlab)], ctypes.c_int),
+        "xfd_set_tfsf": ([vp, ctypes.POINTER(TfsfDesc)], ctypes.c_int),
+        "xfd_add_current_source": ([vp, _i32, _i32 * 3, _i32 * 3, _dp, _dp], ctypes.c_int),
+        "xfd_set_ade": ([vp, ctypes.POINTER(AdeDesc)], ctypes.c_int),
+        "xfd_set_nf2ff": ([vp, ctypes.POINTER(Nf2ffDesc)], ctypes.c_int),
+        "xfd_get_nf2ff": ([vp, _dp, _i64, ctypes.POINTER(_i64)], ctypes.c_int),
+        "xfd_add_movie": ([vp, _i32, _i32 * 3, _i32 * 3, _i32, ctypes.POINTER(_i32)],
+                          ctypes.c_int),
+        "xfd_get_movie_frames": ([vp, _i32, vp, _i64, ctypes.POINTER(_i64)], ctypes.c_int),
+        "xfd_upload_fields": ([vp, vp * 6], ctypes.c_int),
+        "xfd_download_fields": ([vp, vp * 6], ctypes.c_int),
+        "xfd_download_field": ([vp, _i32, vp], ctypes.c_int),
+        "xfd_run": ([vp, _i64], ctypes.c_int),
+        "xfd_sync": ([vp], ctypes.c_int),
+        "xfd_current_step": ([vp], _i64),
+        "xfd_set_option": ([vp, ctypes.c_char_p, _i64], ctypes.c_int),
+        "xfd_stream": ([vp], vp),
+        "xfd_launches_per_step": ([vp], _i32),
+        "xfd_stencil_bytes_per_step": ([vp], _i64),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+def exported_symbols() -> List[str]:
+    """Names declared in include/xfd_engine.h that the library must export."""
+    return ["xfd_create", "xfd_destroy", "xfd_last_error", "xfd_set_material_classes",
+            "xfd_set_curl_factors", "xfd_add_cpml", "xfd_set_tfsf", "xfd_add_current_source",
+            "xfd_set_ade", "xfd_set_nf2ff", "xfd_get_nf2ff", "xfd_add_movie",
+            "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
+            "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
+            "xfd_stream", "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def comp_shape(n: Sequence[int], c: int):
+    """Reference shape of component c (0..5) on an (nx, ny, nz) grid."""
+    ax = c % 3
+    if c < 3:
+        return tuple(n[d] if d == ax else n[d] + 1 for d in range(3))
+    return tuple(n[d] + 1 if d == ax else n[d] for d in range(3))
+
+
+class Engine:
+    """Owning handle of one xfd_engine."""
+
+    def __init__(self, nx: int, ny: int, nz: int, precision: int = FP64, n_steps: int = 1,
+                 dt: float = 0.0, device: int = 0):
+        self.L = load()
+        self.n = (nx, ny, nz)
+        self.precision = precision
+        self.dtype = np.float64 if precision == FP64 else np.float32
+        self.n_steps = n_steps
+        g = GridDesc(nx, ny, nz, precision, n_steps, dt, device)
+        h = ctypes.c_void_p()
+        st = self.L.xfd_create(ctypes.byref(g), ctypes.byref(h))
+        if st != 0:
+            raise EngineError(f"xfd_create: {_STATUS.get(st, st)}: "
+                              f"{self.L.xfd_last_error(None).decode()}")
+        self.h = h
+        self._keep: list = []
+
+    # ------------------------------------------------------------ plumbing
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = self.L.xfd_last_error(self.h).decode()
+            raise EngineError(f"{what}: {_STATUS.get(st, st)}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.xfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --------------------------------------------------------------- set-up
+    def set_material_classes(self, table: np.ndarray, lattice_class: np.ndarray):
+        table = _f64(table).reshape(-1, 12)
+        lc = np.ascontiguousarray(lattice_class, dtype=np.uint16)
+        assert lc.shape == (self.n[0] + 1, self.n[1] + 1, self.n[2] + 1), lc.shape
+        self._check(self.L.xfd_set_material_classes(
+            self.h, _p(table), table.shape[0],
+            lc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))), "set_material_classes")
+
+    def set_curl_factors(self, fe: Sequence[np.ndarray], fh: Sequence[np.ndarray]):
+        fe = [_f64(a) for a in fe]
+        fh = [_f64(a) for a in fh]
+        ae = (_dp * 3)(*[_p(a) for a in fe])
+        ah = (_dp * 3)(*[_p(a) for a in fh])
+        self._check(self.L.xfd_set_curl_factors(self.h, ae, ah), "set_curl_factors")
+
+    def add_cpml(self, axis: int, negative: bool, thickness: int, e_start: int, h_start: int,
+                 a_e, b_e, a_h, b_h):
+        arrs = [_f64(a) for a in (a_e, b_e, a_h, b_h)]
+        s = CpmlSlab(axis, int(negative), thickness, e_start, h_start, *[_p(a) for a in arrs])
+        self._check(self.L.xfd_add_cpml(self.h, ctypes.byref(s)), "add_cpml")
+
+    def set_tfsf(self, box_s, box_e, e_inc, h_inc, p_int, p_half, ca, cb, te, th):
+        e_inc, h_inc = _f64(e_inc), _f64(h_inc)
+        p_int = [_f64(a) for a in p_int]
+        p_half = [_f64(a) for a in p_half]
+        d = TfsfDesc()
+        for a in range(3):
+            d.box_s[a], d.box_e[a] = int(box_s[a]), int(box_e[a])
+            d.p_int[a], d.p_half[a] = _p(p_int[a]), _p(p_half[a])
+            d.ca[a], d.cb[a], d.te[a], d.th[a] = ca[a], cb[a], te[a], th[a]
+        d.aux = e_inc.shape[1]
+        d.e_inc, d.h_inc = _p(e_inc), _p(h_inc)
+        self._check(self.L.xfd_set_tfsf(self.h, ctypes.byref(d)), "set_tfsf")
+
+    def add_current_source(self, comp: int, box_s, box_e, coff, waveform):
+        coff, waveform = _f64(coff), _f64(waveform)
+        self._check(self.L.xfd_add_current_source(
+            self.h, comp, (_i32 * 3)(*box_s), (_i32 * 3)(*box_e), _p(coff), _p(waveform)),
+            "add_current_source")
+
+    def set_ade(self, kind: int, n_poles: int, mat_coeff: np.ndarray, comp: np.ndarray,
+                node: np.ndarray, material: np.ndarray):
+        mc = _f64(mat_coeff).ravel()
+        comp = np.ascontiguousarray(comp, dtype=np.uint8)
+        node = np.ascontiguousarray(node, dtype=np.int32).reshape(-1, 3)
+        material = np.ascontiguousarray(material, dtype=np.uint8)
+        n_mat = mc.size // (2 + 7 * n_poles)
+        d = AdeDesc(kind, n_poles, n_mat, _p(mc), comp.size,
+                    comp.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                    node.ctypes.data_as(ctypes.POINTER(_i32)),
+                    material.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        self._check(self.L.xfd_set_ade(self.h, ctypes.byref(d)), "set_ade")
+
+    def set_nf2ff(self, tasks, te: np.ndarray, th: np.ndarray, scale: float, batch: int = 64):
+        te, th = _f64(te), _f64(th)
+        d = Nf2ffDesc()
+        d.n_freq = te.shape[0]
+        d.batch = batch
+        for f in range(6):
+            t = tasks[f]
+            for a in range(3):
+                d.task_s[f][a] = 0 if t is None else int(t[0][a])
+                d.task_e[f][a] = 0 if t is None else int(t[1][a])
+        d.te, d.th, d.scale = _p(te), _p(th), float(scale)
+        self._check(self.L.xfd_set_nf2ff(self.h, ctypes.byref(d)), "set_nf2ff")
+
+    def add_movie(self, field: int, box_s, box_e, interval: int) -> int:
+        out = _i32()
+        self._check(self.L.xfd_add_movie(self.h, field, (_i32 * 3)(*box_s), (_i32 * 3)(*box_e),
+                                         interval, ctypes.byref(out)), "add_movie")
+        return out.value
+
+    def set_option(self, name: str, value: int):
+        self._check(self.L.xfd_set_option(self.h, name.encode(), int(value)), "set_option")
+
+    # ---------------------------------------------------------------- fields
+    def upload_fields(self, fields: Sequence[np.ndarray]):
+        arrs = []
+        for c in range(6):
+            a = np.ascontiguousarray(fields[c], dtype=self.dtype)
+            assert a.shape == comp_shape(self.n, c), (c, a.shape)
+            arrs.append(a)
+        ptrs = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+        self._check(self.L.xfd_upload_fields(self.h, ptrs), "upload_fields")
+
+    def download_fields(self) -> List[np.ndarray]:
+        arrs = [np.empty(comp_shape(self.n, c), dtype=self.dtype) for c in range(6)]
+        ptrs = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+        self._check(self.L.xfd_download_fields(self.h, ptrs), "download_fields")
+        return arrs
+
+    def download_field(self, c: int) -> np.ndarray:
+        a = np.empty(comp_shape(self.n, c), dtype=self.dtype)
+        self._check(self.L.xfd_download_field(self.h, c, ctypes.c_void_p(a.ctypes.data)),
+                    "download_field")
+        return a
+
+    # ------------------------------------------------------------------- run
+    def run(self, n: int):
+        self._check(self.L.xfd_run(self.h, int(n)), "run")
+
+    def sync(self):
+        self._check(self.L.xfd_sync(self.h), "sync")
+
+    @property
+    def step(self) -> int:
+        return int(self.L.xfd_current_step(self.h))
+
+    def stream(self) -> int:
+        return int(self.L.xfd_stream(self.h) or 0)
+
+    def launches_per_step(self) -> int:
+        return int(self.L.xfd_launches_per_step(self.h))
+
+    def stencil_bytes_per_step(self) -> int:
+        return int(self.L.xfd_stencil_bytes_per_step(self.h))
+
+    # --------------------------------------------------------------- outputs
+    def movie_frames(self, mid: int, box_shape) -> np.ndarray:
+        n = _i64()
+        self._check(self.L.xfd_get_movie_frames(self.h, mid, None, 0, ctypes.byref(n)),
+                    "get_movie_frames")
+        out = np.empty((n.value, *box_shape), dtype=self.dtype)
+        self._check(self.L.xfd_get_movie_frames(self.h, mid, ctypes.c_void_p(out.ctypes.data),
+                                                out.nbytes, ctypes.byref(n)),
+                    "get_movie_frames")
+        return out
+
+    def nf2ff(self) -> np.ndarray:
+        cnt = _i64()
+        self._check(self.L.xfd_get_nf2ff(self.h, None, 0, ctypes.byref(cnt)), "get_nf2ff")
+        out = np.empty(2 * cnt.value, dtype=np.float64)
+        self._check(self.L.xfd_get_nf2ff(self.h, _p(out), cnt.value, ctypes.byref(cnt)),
+                    "get_nf2ff")
+        return out[0::2] + 1j * out[1::2]

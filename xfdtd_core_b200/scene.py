@@ -1,0 +1,380 @@
+"""Scene descriptions for the XFDTD 3-D hot path.
+
+A :class:`Scene` is the data a user program hands to ``xfdtd::Simulation``
+(objects, boundaries, sources, monitors, NF2FF, step count).  It mirrors the
+reference's user-facing API one to one:
+
+* ``Object(name, Cube|Sphere, Material)``            include/xfdtd/object/object.h:28-29
+* ``ElectroMagneticProperty(eps_r, mu_r, s_e, s_m)`` src/material/material.cpp:11-26
+* ``DrudeMedium / DebyeMedium / MLorentzMaterial``   include/xfdtd/material/dispersive_material.h:71-122
+* ``PML(thickness, dir, order, sigma_ratio, alpha_min, alpha_max, kappa_max)``
+                                                       include/xfdtd/boundary/pml.h:19-21
+* ``TFSF3D(x, y, z, theta, phi, psi, waveform)``      include/xfdtd/waveform_source/tfsf_3d.h:10-11
+* ``CurrentSource(name, cube, dir, R, waveform)``     include/xfdtd/object/lumped_element/current_source.h:11-14
+* ``MovieMonitor(FieldMonitor(cube, field), k)``      include/xfdtd/monitor/movie_monitor.h:13-15
+* ``NFFFTFrequencyDomain(dx, dy, dz, freqs)``         include/xfdtd/nffft/nffft_frequency_domain.h:19-45
+* ``Waveform::gaussian / cosineModulatedGaussian``    src/waveform/waveform.cpp:80-96
+
+``Scene.to_text()`` serialises the scene into the line format that the C++
+host library (``xfdtd_scene_open``) parses into exactly those API calls, with
+every float printed as a round-trip ``repr`` so both sides see identical
+doubles.  The workload builders at the bottom define the five benchmark
+scenes (dielectric sphere, dielectric boxes, dispersive spheres) with a size
+knob so that the same geometry rule gives small parity cases.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+Vec3 = Tuple[float, float, float]
+
+DIRECTIONS = ("XN", "XP", "YN", "YP", "ZN", "ZP")
+FIELDS = ("EX", "EY", "EZ", "HX", "HY", "HZ")
+
+
+def _f(x: float) -> str:
+    if math.isinf(x):
+        return "inf" if x > 0 else "-inf"
+    return repr(float(x))
+
+
+@dataclass
+class Waveform:
+    """``Waveform::gaussian(tau, t0)`` or ``cosineModulatedGaussian(tau, t0, f)``."""
+
+    kind: str  # "gaussian" | "cosgauss"
+    tau: float
+    t0: float
+    freq: float = 0.0
+    amplitude: float = 1.0
+
+    def text(self) -> str:
+        if self.kind == "gaussian":
+            return f"gaussian {_f(self.tau)} {_f(self.t0)} {_f(self.amplitude)}"
+        if self.kind == "cosgauss":
+            return (f"cosgauss {_f(self.tau)} {_f(self.t0)} {_f(self.freq)} "
+                    f"{_f(self.amplitude)}")
+        raise ValueError(self.kind)
+
+    def __call__(self, t):
+        """Samples the waveform like ``Waveform::init`` (waveform.cpp:28-34)."""
+        t = np.asarray(t, dtype=np.float64)
+        if self.kind == "gaussian":
+            v = np.exp(-np.power((t - self.t0) / self.tau, 2))
+        else:
+            v = (np.exp(-np.power((t - self.t0) / self.tau, 2)) *
+                 np.cos(2 * math.pi * self.freq * (t - self.t0)))
+        return self.amplitude * v
+
+
+@dataclass
+class Material:
+    """A simple (eps_r, mu_r, sigma_e, sigma_m) medium or a linear dispersive one.
+
+    ``kind`` is "simple", "drude", "debye" or "mlorentz".  Dispersive media
+    carry ``eps_inf`` and per-pole parameter lists; their em-property is air
+    (``ElectroMagneticProperty::air()``), as the reference factories build them.
+    """
+
+    kind: str = "simple"
+    eps_r: float = 1.0
+    mu_r: float = 1.0
+    sigma_e: float = 0.0
+    sigma_m: float = 0.0
+    eps_inf: float = 1.0
+    # drude: omega_p, gamma; debye: eps_static, tau; mlorentz: a0, a1, b0, b1, b2
+    poles: List[Tuple[float, ...]] = field(default_factory=list)
+
+    def text(self) -> str:
+        if self.kind == "simple":
+            return (f"simple {_f(self.eps_r)} {_f(self.mu_r)} {_f(self.sigma_e)} "
+                    f"{_f(self.sigma_m)}")
+        body = " ".join(" ".join(_f(v) for v in p) for p in self.poles)
+        return f"{self.kind} {_f(self.eps_inf)} {len(self.poles)} {body}"
+
+    @property
+    def dispersive(self) -> bool:
+        return self.kind != "simple"
+
+
+def air() -> Material:
+    return Material("simple", 1.0, 1.0, 0.0, 0.0)
+
+
+def drude(eps_inf: float, omega_p: Sequence[float], gamma: Sequence[float]) -> Material:
+    return Material("drude", eps_inf=eps_inf,
+                    poles=[(float(w), float(g)) for w, g in zip(omega_p, gamma)])
+
+
+def debye(eps_inf: float, eps_static: Sequence[float], tau: Sequence[float]) -> Material:
+    return Material("debye", eps_inf=eps_inf,
+                    poles=[(float(e), float(t)) for e, t in zip(eps_static, tau)])
+
+
+def mlorentz(eps_inf: float, a0, a1, b0, b1, b2) -> Material:
+    return Material("mlorentz", eps_inf=eps_inf,
+                    poles=[tuple(float(v) for v in p) for p in zip(a0, a1, b0, b1, b2)])
+
+
+@dataclass
+class Shape:
+    kind: str  # "cube" | "sphere"
+    origin: Vec3  # cube origin or sphere centre
+    size: Vec3 = (0.0, 0.0, 0.0)  # cube size
+    radius: float = 0.0
+
+    def text(self) -> str:
+        if self.kind == "cube":
+            return "cube " + " ".join(_f(v) for v in (*self.origin, *self.size))
+        return "sphere " + " ".join(_f(v) for v in (*self.origin, self.radius))
+
+
+def cube(origin: Vec3, size: Vec3) -> Shape:
+    return Shape("cube", tuple(map(float, origin)), tuple(map(float, size)))
+
+
+def sphere(center: Vec3, radius: float) -> Shape:
+    return Shape("sphere", tuple(map(float, center)), radius=float(radius))
+
+
+@dataclass
+class ObjectSpec:
+    name: str
+    shape: Shape
+    material: Material
+
+    def text(self) -> str:
+        return f"object {self.name} {self.shape.text()} {self.material.text()}"
+
+
+@dataclass
+class CurrentSourceSpec:
+    name: str
+    shape: Shape  # a Cube
+    direction: str
+    resistance: float
+    waveform: Waveform
+
+    def text(self) -> str:
+        o, s = self.shape.origin, self.shape.size
+        return (f"current_source {self.name} " +
+                " ".join(_f(v) for v in (*o, *s)) +
+                f" {self.direction} {_f(self.resistance)} {self.waveform.text()}")
+
+
+@dataclass
+class PMLSpec:
+    thickness: int
+    direction: str
+    order: int = 4
+    sigma_ratio: float = 1.0
+    alpha_min: float = 0.0
+    alpha_max: float = 0.05
+    kappa_max: float = 10.0
+
+    def text(self) -> str:
+        return (f"pml {self.thickness} {self.direction} {self.order} "
+                f"{_f(self.sigma_ratio)} {_f(self.alpha_min)} {_f(self.alpha_max)} "
+                f"{_f(self.kappa_max)}")
+
+
+@dataclass
+class TFSFSpec:
+    x: int
+    y: int
+    z: int
+    theta: float
+    phi: float
+    psi: float
+    waveform: Waveform
+
+    def text(self) -> str:
+        return (f"tfsf3d {self.x} {self.y} {self.z} {_f(self.theta)} {_f(self.phi)} "
+                f"{_f(self.psi)} {self.waveform.text()}")
+
+
+@dataclass
+class MovieSpec:
+    name: str
+    field: str
+    shape: Shape  # Cube
+    interval: int
+
+    def text(self) -> str:
+        o, s = self.shape.origin, self.shape.size
+        return (f"movie {self.name} {self.field} " +
+                " ".join(_f(v) for v in (*o, *s)) + f" {self.interval}")
+
+
+@dataclass
+class NF2FFSpec:
+    distance: Tuple[int, int, int]
+    freqs: Sequence[float]
+
+    def text(self) -> str:
+        d = self.distance
+        return (f"nf2ff_fd {d[0]} {d[1]} {d[2]} {len(self.freqs)} " +
+                " ".join(_f(f) for f in self.freqs))
+
+
+@dataclass
+class Scene:
+    """Everything a reference user program passes to ``xfdtd::Simulation``."""
+
+    dl: Vec3
+    cfl: float
+    steps: int
+    objects: List[ObjectSpec] = field(default_factory=list)
+    current_sources: List[CurrentSourceSpec] = field(default_factory=list)
+    pmls: List[PMLSpec] = field(default_factory=list)
+    tfsf: Optional[TFSFSpec] = None
+    movies: List[MovieSpec] = field(default_factory=list)
+    nf2ff: Optional[NF2FFSpec] = None
+    name: str = "scene"
+
+    def to_text(self) -> str:
+        lines = ["xfdtd-scene 1", f"name {self.name}",
+                 "grid " + " ".join(_f(v) for v in self.dl) + f" {_f(self.cfl)}",
+                 f"steps {self.steps}"]
+        lines += [o.text() for o in self.objects]
+        lines += [c.text() for c in self.current_sources]
+        lines += [p.text() for p in self.pmls]
+        if self.tfsf is not None:
+            lines.append(self.tfsf.text())
+        lines += [m.text() for m in self.movies]
+        if self.nf2ff is not None:
+            lines.append(self.nf2ff.text())
+        return "\n".join(lines) + "\n"
+
+    def write(self, path: str) -> str:
+        with open(path, "w") as fh:
+            fh.write(self.to_text())
+        return path
+
+
+def pml_all(thickness: int, **kw) -> List[PMLSpec]:
+    return [PMLSpec(thickness, d, **kw) for d in DIRECTIONS]
+
+
+# ---------------------------------------------------------------------------
+# Workloads.  Each keeps its geometry rule for every size so that the small
+# variants used by the parity tests exercise the same code paths.
+# ---------------------------------------------------------------------------
+
+def dielectric_sphere(steps: int = 2000, dl: float = 7.5e-3, half: float = 0.175,
+                      radius: float = 0.1, pml: int = 8, tfsf_start: int = 15,
+                      movie_interval: int = 10, nf2ff_freqs: Sequence[float] = (),
+                      nf2ff_distance: int = 11) -> Scene:
+    """Plain FP64 dielectric-sphere scatter (the reference's
+    test/src/examples/dielectric_sphere_scatter.cpp:26-129 at dl=7.5e-3):
+    0.35 m air cube, 8-cell PML, sphere r=0.1 eps_r=3 mu_r=2, TFSF3D at index
+    15 with a Gaussian (tau = 20*dl/6e8, t0 = 4.5 tau), CFL 0.9, an Ex XZ-plane
+    movie every 10 steps."""
+    tau = dl * 20 / 6e8
+    s = Scene(dl=(dl, dl, dl), cfl=0.9, steps=steps, name="dielectric_sphere")
+    s.objects.append(ObjectSpec("domain", cube((-half,) * 3, (2 * half,) * 3), air()))
+    s.objects.append(ObjectSpec("dielectric_sphere", sphere((0, 0, 0), radius),
+                                Material("simple", 3.0, 2.0, 0.0, 0.0)))
+    s.pmls = pml_all(pml)
+    s.tfsf = TFSFSpec(tfsf_start, tfsf_start, tfsf_start, 0.0, 0.0, 0.0,
+                      Waveform("gaussian", tau, 4.5 * tau))
+    if movie_interval:
+        s.movies.append(MovieSpec("movie_ex_xz", "EX",
+                                  cube((-half, 0.0, -half), (2 * half, dl, 2 * half)),
+                                  movie_interval))
+    if nf2ff_freqs:
+        s.nf2ff = NF2FFSpec((nf2ff_distance,) * 3, list(nf2ff_freqs))
+    return s
+
+
+def random_boxes(n_cells: int, n_boxes: int, seed: int, edge_lo: int, edge_hi: int):
+    """Box list for the dielectric-boxes scene, drawn with
+    numpy.random.default_rng(seed): integer edges U[edge_lo, edge_hi] per axis,
+    integer origin uniform so that the box lies inside the interior, eps_r
+    U[1.5, 12], sigma_e U[0, 0.05] S/m, in generation (= painting) order."""
+    rng = np.random.default_rng(seed)
+    boxes = []
+    for _ in range(n_boxes):
+        edges = rng.integers(edge_lo, edge_hi + 1, size=3)
+        edges = np.minimum(edges, n_cells)
+        origin = np.array([rng.integers(0, n_cells - e + 1) for e in edges])
+        eps_r = float(rng.uniform(1.5, 12.0))
+        sigma = float(rng.uniform(0.0, 0.05))
+        boxes.append((tuple(int(v) for v in origin), tuple(int(v) for v in edges),
+                      eps_r, sigma))
+    return boxes
+
+
+def dielectric_boxes(n: int = 256, pml: int = 12, dl: float = 1e-3, n_boxes: int = 64,
+                     steps: int = 4000, seed: int = 0, edge_lo: int = 8,
+                     edge_hi: int = 40, movie_interval: int = 0) -> Scene:
+    """Large vacuum/dielectric scene: n^3 cells including a `pml`-cell CPML
+    (order 3, sigma_ratio 1, alpha 0..0.05, kappa_max 5), `n_boxes` random
+    dielectric boxes, a z-directed one-cell CurrentSource (R = inf) at the
+    centre driven by cosineModulatedGaussian(tau, 4.5 tau, 30 GHz) with
+    tau = sqrt(2 ln 2)/(pi * 15 GHz), CFL 0.99."""
+    interior = n - 2 * pml
+    half = interior * dl / 2
+    s = Scene(dl=(dl, dl, dl), cfl=0.99, steps=steps, name="dielectric_boxes")
+    s.objects.append(ObjectSpec("domain", cube((-half,) * 3, (2 * half,) * 3), air()))
+    for b, (o, e, eps_r, sig) in enumerate(random_boxes(interior, n_boxes, seed,
+                                                        edge_lo, edge_hi)):
+        org = tuple(-half + o[a] * dl for a in range(3))
+        size = tuple(e[a] * dl for a in range(3))
+        s.objects.append(ObjectSpec(f"box{b}", cube(org, size),
+                                    Material("simple", eps_r, 1.0, sig, 0.0)))
+    tau = math.sqrt(2 * math.log(2)) / (math.pi * 15e9)
+    s.current_sources.append(CurrentSourceSpec(
+        "dipole", cube((0.0, 0.0, 0.0), (0.0, 0.0, dl)), "ZP", math.inf,
+        Waveform("cosgauss", tau, 4.5 * tau, 30e9)))
+    s.pmls = pml_all(pml, order=3, sigma_ratio=1.0, alpha_min=0.0, alpha_max=0.05,
+                     kappa_max=5.0)
+    if movie_interval:
+        s.movies.append(MovieSpec("movie_ez_xy", "EZ",
+                                  cube((-half, -half, 0.0), (2 * half, 2 * half, dl)),
+                                  movie_interval))
+    return s
+
+
+def dispersive_spheres(n: int = 384, pml: int = 10, dl: float = 5e-4, radius_cells: int = 40,
+                       offsets_cells=((-100, 0), (50, 87), (50, -87)), steps: int = 6000,
+                       tfsf_start: int = 20, nf2ff_distance: int = 15,
+                       n_freqs: int = 32, movie_interval: int = 0) -> Scene:
+    """Dispersive ADE + TFSF + NF2FF scene: n^3 cells including a `pml`-cell
+    CPML (default parameters), three spheres of radius `radius_cells` in the
+    z = 0 plane (Drude eps_inf=1, wp=2pi*60 GHz, gamma=2pi*5 GHz; Lorentz
+    eps_s=4, eps_inf=2, w0=2pi*40 GHz, delta=2pi*2 GHz as MLorentz(a0 =
+    (eps_s-eps_inf) w0^2, a1=0, b0=w0^2, b1=2 delta, b2=1); Debye eps_s=10,
+    eps_inf=3, tau=5 ps), TFSF3D(theta=45 deg, phi=30 deg, psi=0) with a
+    Gaussian reaching -20 dB at 80 GHz, NF2FF at `n_freqs` frequencies in
+    [10, 80] GHz, CFL 0.9."""
+    interior = n - 2 * pml
+    half = interior * dl / 2
+    s = Scene(dl=(dl, dl, dl), cfl=0.9, steps=steps, name="dispersive_spheres")
+    s.objects.append(ObjectSpec("domain", cube((-half,) * 3, (2 * half,) * 3), air()))
+    r = radius_cells * dl
+    two_pi = 2 * math.pi
+    w0 = two_pi * 40e9
+    mats = [
+        drude(1.0, [two_pi * 60e9], [two_pi * 5e9]),
+        mlorentz(2.0, [(4.0 - 2.0) * w0 * w0], [0.0], [w0 * w0], [2 * two_pi * 2e9], [1.0]),
+        debye(3.0, [10.0], [5e-12]),
+    ]
+    for m, ((ox, oy), mat) in enumerate(zip(offsets_cells, mats)):
+        s.objects.append(ObjectSpec(f"sphere{m}", sphere((ox * dl, oy * dl, 0.0), r), mat))
+    tau = math.sqrt(math.log(10)) / (math.pi * 80e9)
+    s.pmls = pml_all(pml)
+    s.tfsf = TFSFSpec(tfsf_start, tfsf_start, tfsf_start, math.pi / 4, math.pi / 6, 0.0,
+                      Waveform("gaussian", tau, 4.5 * tau))
+    if n_freqs:
+        s.nf2ff = NF2FFSpec((nf2ff_distance,) * 3,
+                            list(np.linspace(10e9, 80e9, n_freqs)))
+    if movie_interval:
+        s.movies.append(MovieSpec("movie_ex_xy", "EX",
+                                  cube((-half, -half, 0.0), (2 * half, 2 * half, dl)),
+                                  movie_interval))
+    return s
