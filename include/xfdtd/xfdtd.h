@@ -1,0 +1,554 @@
+// xfdtd.h -- C++20 public API of the B200 host library (libxfdtd_host.so).
+//
+// Source-compatible subset of EMinsight/XFDTD_CORE's user API for the 3-D
+// FDTD path: the same class names, constructor arguments and call sequence
+// (include/xfdtd/simulation/simulation.h:37-155 and friends), so that a
+// reference user program that builds a Simulation from Objects, PML
+// boundaries, a TFSF3D source, CurrentSources, MovieMonitors and an
+// NFFFTFrequencyDomain runs unchanged, with Simulation::run(n) executing the
+// time loop on a B200 through the engine C ABI (xfd_engine.h).
+//
+// Deliberate differences, each documented at the member:
+// * ThreadConfig is accepted and ignored (the time loop runs on the GPU).
+// * Array1D is a small owning vector, not xt::xtensor; xt_compat.h gives the
+//   xt::xarray / xt::linspace spellings reference programs use.
+// * Precision is chosen per Simulation (FP64 default, FP32 form optional)
+//   instead of at build time (CMake XFDTD_CORE_SINGLE_PRECISION).
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <functional>
+#include <initializer_list>
+#include <memory>
+#include <numbers>
+#include <stdexcept>
+#include <string>
+#include <string_view>
+#include <vector>
+
+struct xfd_engine;
+
+namespace xfdtd {
+
+using Real = double;
+using Index = std::size_t;
+
+// ---------------------------------------------------------------- Array1D
+template <typename T>
+class Array1D {
+ public:
+  Array1D() = default;
+  Array1D(std::initializer_list<T> v) : _v(v) {}
+  explicit Array1D(std::vector<T> v) : _v(std::move(v)) {}
+  explicit Array1D(std::size_t n, T fill = T{}) : _v(n, fill) {}
+  std::size_t size() const { return _v.size(); }
+  T& operator()(std::size_t i) { return _v[i]; }
+  const T& operator()(std::size_t i) const { return _v[i]; }
+  T& operator[](std::size_t i) { return _v[i]; }
+  const T& operator[](std::size_t i) const { return _v[i]; }
+  T* data() { return _v.data(); }
+  const T* data() const { return _v.data(); }
+  auto begin() { return _v.begin(); }
+  auto end() { return _v.end(); }
+  auto begin() const { return _v.begin(); }
+  auto end() const { return _v.end(); }
+  const T& front() const { return _v.front(); }
+  const T& back() const { return _v.back(); }
+  std::vector<T>& vec() { return _v; }
+  const std::vector<T>& vec() const { return _v; }
+
+ private:
+  std::vector<T> _v;
+};
+
+/// Row-major 3-D array (k fastest), the EMF field storage.
+template <typename T>
+class Array3D {
+ public:
+  Array3D() = default;
+  Array3D(std::size_t n0, std::size_t n1, std::size_t n2)
+      : _n{n0, n1, n2}, _v(n0 * n1 * n2, T{}) {}
+  T& operator()(std::size_t i, std::size_t j, std::size_t k) {
+    return _v[(i * _n[1] + j) * _n[2] + k];
+  }
+  const T& operator()(std::size_t i, std::size_t j, std::size_t k) const {
+    return _v[(i * _n[1] + j) * _n[2] + k];
+  }
+  const std::array<std::size_t, 3>& shape() const { return _n; }
+  std::size_t size() const { return _v.size(); }
+  T* data() { return _v.data(); }
+  const T* data() const { return _v.data(); }
+
+ private:
+  std::array<std::size_t, 3> _n{0, 0, 0};
+  std::vector<T> _v;
+};
+
+// ------------------------------------------------------------- constants
+// include/xfdtd/common/constant.h:11-18
+namespace constant {
+inline constexpr Real PI{std::numbers::pi_v<Real>};
+inline constexpr Real EPSILON_0{8.854187817e-12};
+inline constexpr Real MU_0{4 * PI * 1e-7};
+inline const Real C_0{1 / std::sqrt(EPSILON_0 * MU_0)};
+inline constexpr Real SIGMA_E_ZERO_APPROX{1e-20};
+inline constexpr Real SIGMA_M_ZERO_APPROX{1e-20};
+}  // namespace constant
+
+class XFDTDException : public std::runtime_error {
+ public:
+  explicit XFDTDException(const std::string& m) : std::runtime_error(m) {}
+};
+
+// --------------------------------------------------------------- geometry
+class Vector {
+ public:
+  Vector() = default;
+  Vector(Real x, Real y, Real z) : _d{x, y, z} {}
+  Real x() const { return _d[0]; }
+  Real y() const { return _d[1]; }
+  Real z() const { return _d[2]; }
+  Real operator()(int a) const { return _d[a]; }
+  Vector operator+(const Vector& o) const { return {x() + o.x(), y() + o.y(), z() + o.z()}; }
+  Vector operator-(const Vector& o) const { return {x() - o.x(), y() - o.y(), z() - o.z()}; }
+
+ private:
+  std::array<Real, 3> _d{0, 0, 0};
+};
+
+struct Axis {
+  enum class XYZ { X = 0, Y = 1, Z = 2 };
+  enum class Direction { XN, XP, YN, YP, ZN, ZP };
+  static int axisOf(Direction d) { return static_cast<int>(d) / 2; }
+  static bool negative(Direction d) { return static_cast<int>(d) % 2 == 0; }
+};
+
+class Cube;
+
+class Shape {
+ public:
+  virtual ~Shape() = default;
+  virtual bool isInside(Real x, Real y, Real z, Real eps) const = 0;
+  virtual std::unique_ptr<Cube> wrappedCube() const = 0;
+  virtual std::unique_ptr<Shape> clone() const = 0;
+};
+
+/// Cube(origin, size); end = origin + size (src/shape/cube.cpp).
+class Cube : public Shape {
+ public:
+  Cube(Vector origin, Vector size) : _origin{origin}, _size{size}, _end{origin + size} {}
+  bool isInside(Real x, Real y, Real z, Real eps) const override;
+  std::unique_ptr<Cube> wrappedCube() const override { return std::make_unique<Cube>(*this); }
+  std::unique_ptr<Shape> clone() const override { return std::make_unique<Cube>(*this); }
+  const Vector& origin() const { return _origin; }
+  const Vector& size() const { return _size; }
+  const Vector& end() const { return _end; }
+
+ private:
+  Vector _origin, _size, _end;
+};
+
+class Sphere : public Shape {
+ public:
+  Sphere(Vector center, Real radius) : _center{center}, _radius{radius} {}
+  bool isInside(Real x, Real y, Real z, Real eps) const override;
+  std::unique_ptr<Cube> wrappedCube() const override;
+  std::unique_ptr<Shape> clone() const override { return std::make_unique<Sphere>(*this); }
+  const Vector& center() const { return _center; }
+  Real radius() const { return _radius; }
+
+ private:
+  Vector _center;
+  Real _radius;
+};
+
+// -------------------------------------------------------------- materials
+/// ElectroMagneticProperty(eps_r, mu_r, sigma_e, sigma_m); zero conductivities
+/// become 1e-20 (src/material/material.cpp:11-26).
+class ElectroMagneticProperty {
+ public:
+  ElectroMagneticProperty(Real eps_r = 1, Real mu_r = 1, Real sigma_e = 0, Real sigma_m = 0);
+  static ElectroMagneticProperty air() { return {1, 1, 0, 0}; }
+  Real epsilonR() const { return _eps_r; }
+  Real muR() const { return _mu_r; }
+  Real sigmaE() const { return _sigma_e; }
+  Real sigmaM() const { return _sigma_m; }
+  Real epsilon() const { return _eps_r * constant::EPSILON_0; }
+  Real mu() const { return _mu_r * constant::MU_0; }
+
+ private:
+  Real _eps_r, _mu_r, _sigma_e, _sigma_m;
+};
+
+class Material {
+ public:
+  Material(std::string_view name, ElectroMagneticProperty emp, bool dispersion = false)
+      : _name{name}, _emp{emp}, _dispersion{dispersion} {}
+  virtual ~Material() = default;
+  static std::unique_ptr<Material> createAir() {
+    return std::make_unique<Material>("air", ElectroMagneticProperty::air());
+  }
+  const std::string& name() const { return _name; }
+  const ElectroMagneticProperty& emProperty() const { return _emp; }
+  bool dispersion() const { return _dispersion; }
+
+ private:
+  std::string _name;
+  ElectroMagneticProperty _emp;
+  bool _dispersion;
+};
+
+/// Linear dispersive medium in modified-Lorentz form with per-pole
+/// (a0, a1, b0, b1, b2) (src/material/dispersive_material_equation.cpp:15-54).
+class LinearDispersiveMaterial : public Material {
+ public:
+  enum class Kind { Drude, Debye, MLorentz };
+  LinearDispersiveMaterial(std::string_view name, Real eps_inf, Kind kind,
+                           std::vector<std::array<Real, 5>> poles,
+                           std::vector<std::array<Real, 2>> native)
+      : Material{name, ElectroMagneticProperty::air(), true},
+        _eps_inf{eps_inf},
+        _kind{kind},
+        _poles{std::move(poles)},
+        _native{std::move(native)} {}
+  Real epsilonInf() const { return _eps_inf; }
+  Kind kind() const { return _kind; }
+  Index numPoles() const { return _poles.size(); }
+  /// (a0, a1, b0, b1, b2) of pole p.
+  const std::array<Real, 5>& pole(Index p) const { return _poles[p]; }
+  /// Drude (omega_p, gamma) or Debye (eps_static, tau) of pole p.
+  const std::array<Real, 2>& native(Index p) const { return _native[p]; }
+
+ private:
+  Real _eps_inf;
+  Kind _kind;
+  std::vector<std::array<Real, 5>> _poles;
+  std::vector<std::array<Real, 2>> _native;
+};
+
+class DrudeMedium : public LinearDispersiveMaterial {
+ public:
+  using LinearDispersiveMaterial::LinearDispersiveMaterial;
+  static std::unique_ptr<DrudeMedium> makeDrudeMedium(std::string_view name, Real eps_inf,
+                                                      Array1D<Real> omega_p,
+                                                      Array1D<Real> gamma);
+};
+
+class DebyeMedium : public LinearDispersiveMaterial {
+ public:
+  using LinearDispersiveMaterial::LinearDispersiveMaterial;
+  static std::unique_ptr<DebyeMedium> makeDebyeMedium(std::string_view name, Real eps_inf,
+                                                      Array1D<Real> eps_static,
+                                                      Array1D<Real> tau);
+};
+
+class MLorentzMaterial : public LinearDispersiveMaterial {
+ public:
+  using LinearDispersiveMaterial::LinearDispersiveMaterial;
+  static std::unique_ptr<MLorentzMaterial> makeMLorentz(std::string_view name, Real eps_inf,
+                                                        Array1D<Real> a0, Array1D<Real> a1,
+                                                        Array1D<Real> b0, Array1D<Real> b1,
+                                                        Array1D<Real> b2);
+};
+using LorentzMedium = MLorentzMaterial;
+
+// --------------------------------------------------------------- waveform
+/// Waveform sampled once per run (src/waveform/waveform.cpp).
+class Waveform {
+ public:
+  Waveform(std::function<Real(Real)> f, Real amplitude = 1.0)
+      : _f{std::move(f)}, _amplitude{amplitude} {}
+  static std::unique_ptr<Waveform> gaussian(Real tau, Real t_0, Real amplitude = 1.0);
+  static std::unique_ptr<Waveform> cosineModulatedGaussian(Real tau, Real t_0, Real frequency,
+                                                           Real amplitude = 1.0);
+  static std::unique_ptr<Waveform> sine(Real frequency, Real amplitude = 1.0);
+  Real amplitude() const { return _amplitude; }
+  Real operator()(Real t) const { return _f(t); }
+  void init(const std::vector<Real>& time);
+  const Array1D<Real>& value() const { return _value; }
+  const Array1D<Real>& time() const { return _time; }
+
+ private:
+  std::function<Real(Real)> _f;
+  Real _amplitude;
+  Array1D<Real> _value, _time;
+};
+
+// ---------------------------------------------------------------- objects
+class Object {
+ public:
+  Object(std::string name, std::unique_ptr<Shape> shape, std::unique_ptr<Material> material)
+      : _name{std::move(name)}, _shape{std::move(shape)}, _material{std::move(material)} {}
+  Object(std::string name, std::unique_ptr<Shape> shape, std::shared_ptr<Material> material)
+      : _name{std::move(name)}, _shape{std::move(shape)}, _material{std::move(material)} {}
+  virtual ~Object() = default;
+  const std::string& name() const { return _name; }
+  const std::unique_ptr<Shape>& shape() const { return _shape; }
+  const std::shared_ptr<Material>& material() const { return _material; }
+
+ private:
+  std::string _name;
+  std::unique_ptr<Shape> _shape;
+  std::shared_ptr<Material> _material;
+};
+
+/// Lumped current source on a Cube of E nodes along its direction
+/// (src/object/lumped_element/current_source.cpp).  Resistance 0 becomes 1e-20;
+/// an infinite resistance leaves the E coefficients unchanged (beta = 0).
+class CurrentSource : public Object {
+ public:
+  CurrentSource(std::string name, std::unique_ptr<Cube> cube, Axis::Direction direction,
+                Real resistance, std::unique_ptr<Waveform> waveform,
+                std::unique_ptr<Material> material = Material::createAir())
+      : Object{std::move(name), std::move(cube), std::move(material)},
+        _direction{direction},
+        _resistance{resistance == 0 ? 1e-20 : resistance},
+        _waveform{std::move(waveform)} {}
+  Axis::Direction direction() const { return _direction; }
+  Real resistance() const { return _resistance; }
+  const std::unique_ptr<Waveform>& waveform() const { return _waveform; }
+
+ private:
+  Axis::Direction _direction;
+  Real _resistance;
+  std::unique_ptr<Waveform> _waveform;
+};
+
+// --------------------------------------------------------------- boundary
+class Boundary {
+ public:
+  virtual ~Boundary() = default;
+};
+
+/// CPML boundary (include/xfdtd/boundary/pml.h:19-21).
+class PML : public Boundary {
+ public:
+  PML(int thickness, Axis::Direction direction, int order = 4, Real sigma_ratio = 1,
+      Real alpha_min = 0, Real alpha_max = 0.05, Real kappa_max = 10)
+      : _thickness{thickness},
+        _direction{direction},
+        _order{order},
+        _sigma_ratio{sigma_ratio},
+        _alpha_min{alpha_min},
+        _alpha_max{alpha_max},
+        _kappa_max{kappa_max} {}
+  int thickness() const { return _thickness; }
+  Axis::Direction direction() const { return _direction; }
+  int order() const { return _order; }
+  Real sigmaRatio() const { return _sigma_ratio; }
+  Real alphaMin() const { return _alpha_min; }
+  Real alphaMax() const { return _alpha_max; }
+  Real kappaMax() const { return _kappa_max; }
+
+ private:
+  int _thickness;
+  Axis::Direction _direction;
+  int _order;
+  Real _sigma_ratio, _alpha_min, _alpha_max, _kappa_max;
+};
+
+// --------------------------------------------------------- waveform source
+class WaveformSource {
+ public:
+  explicit WaveformSource(std::unique_ptr<Waveform> w) : _waveform{std::move(w)} {}
+  virtual ~WaveformSource() = default;
+  const std::unique_ptr<Waveform>& waveform() const { return _waveform; }
+
+ private:
+  std::unique_ptr<Waveform> _waveform;
+};
+
+/// TFSF3D(x, y, z, theta, phi, psi, waveform): the total-field box starts x, y,
+/// z cells from the grid faces (src/waveform_source/tfsf.cpp:118-175).
+class TFSF3D : public WaveformSource {
+ public:
+  TFSF3D(std::size_t x, std::size_t y, std::size_t z, Real theta, Real phi, Real psi,
+         std::unique_ptr<Waveform> waveform)
+      : WaveformSource{std::move(waveform)}, _x{x}, _y{y}, _z{z}, _theta{theta}, _phi{phi},
+        _psi{psi} {}
+  std::size_t x() const { return _x; }
+  std::size_t y() const { return _y; }
+  std::size_t z() const { return _z; }
+  Real theta() const { return _theta; }
+  Real phi() const { return _phi; }
+  Real psi() const { return _psi; }
+
+ private:
+  std::size_t _x, _y, _z;
+  Real _theta, _phi, _psi;
+};
+
+// --------------------------------------------------------------- monitors
+struct EMF {
+  enum class Field { EX, EY, EZ, HX, HY, HZ };
+  Array3D<Real>& field(Field f) { return _f[static_cast<int>(f)]; }
+  const Array3D<Real>& field(Field f) const { return _f[static_cast<int>(f)]; }
+  Array3D<Real>& ex() { return _f[0]; }
+  Array3D<Real>& ey() { return _f[1]; }
+  Array3D<Real>& ez() { return _f[2]; }
+  Array3D<Real>& hx() { return _f[3]; }
+  Array3D<Real>& hy() { return _f[4]; }
+  Array3D<Real>& hz() { return _f[5]; }
+  std::array<Array3D<Real>, 6> _f;
+};
+
+class Monitor {
+ public:
+  Monitor(std::string name, std::string output_dir)
+      : _name{std::move(name)}, _output_dir{std::move(output_dir)} {}
+  virtual ~Monitor() = default;
+  const std::string& name() const { return _name; }
+  const std::string& outputDir() const { return _output_dir; }
+  void setOutputDir(std::string d) { _output_dir = std::move(d); }
+
+ private:
+  std::string _name, _output_dir;
+};
+
+class FieldMonitor : public Monitor {
+ public:
+  FieldMonitor(std::unique_ptr<Shape> shape, EMF::Field field, std::string name = "",
+               std::string output_dir = "")
+      : Monitor{std::move(name), std::move(output_dir)}, _shape{std::move(shape)},
+        _field{field} {}
+  const std::unique_ptr<Shape>& shape() const { return _shape; }
+  EMF::Field field() const { return _field; }
+
+ private:
+  std::unique_ptr<Shape> _shape;
+  EMF::Field _field;
+};
+
+/// MovieMonitor(frame, interval, name, dir): frame every `interval` steps from
+/// step 0, written as <dir>/<frame index, 5 digits>.npy
+/// (src/monitor/movie_monitor.cpp:26-34).
+class MovieMonitor : public Monitor {
+ public:
+  MovieMonitor(std::unique_ptr<FieldMonitor> frame, std::size_t interval, std::string name,
+               std::string output_dir)
+      : Monitor{std::move(name), std::move(output_dir)}, _frame{std::move(frame)},
+        _interval{interval} {}
+  const std::unique_ptr<FieldMonitor>& frame() const { return _frame; }
+  std::size_t frameInterval() const { return _interval; }
+  /// Frames recorded by the last run, each the monitor box in (i, j, k) order.
+  const std::vector<std::vector<Real>>& frames() const { return _frames; }
+  std::array<std::size_t, 3> frameShape() const { return _shape; }
+  std::vector<std::vector<Real>>& framesMutable() { return _frames; }
+  void setFrameShape(std::array<std::size_t, 3> s) { _shape = s; }
+
+ private:
+  std::unique_ptr<FieldMonitor> _frame;
+  std::size_t _interval;
+  std::vector<std::vector<Real>> _frames;
+  std::array<std::size_t, 3> _shape{0, 0, 0};
+};
+
+// ------------------------------------------------------------------ NF2FF
+/// Frequency-domain NF2FF on a Huygens box `distance` cells inside the grid
+/// faces (src/nffft/nffft_frequency_domain.cpp).  After run() the surface
+/// currents are available per frequency and face.
+class NFFFTFrequencyDomain {
+ public:
+  NFFFTFrequencyDomain(Index dx, Index dy, Index dz, Array1D<Real> freqs,
+                       std::string output_dir = "")
+      : _d{dx, dy, dz}, _freqs{std::move(freqs)}, _output_dir{std::move(output_dir)} {}
+  std::array<Index, 3> distance() const { return _d; }
+  const Array1D<Real>& frequencies() const { return _freqs; }
+  const std::string& outputDir() const { return _output_dir; }
+  void setOutputDir(std::string d) { _output_dir = std::move(d); }
+  /// J/M accumulators laid out [freq][face XN..ZP][ja jb ma mb][face nodes].
+  const std::vector<std::complex<Real>>& surfaceCurrents() const { return _acc; }
+  std::vector<std::complex<Real>>& surfaceCurrentsMutable() { return _acc; }
+  /// Face node boxes [s, e) in global indices (empty when invalid).
+  std::array<std::array<int, 6>, 6> faces{};
+
+ private:
+  std::array<Index, 3> _d;
+  Array1D<Real> _freqs;
+  std::string _output_dir;
+  std::vector<std::complex<Real>> _acc;
+};
+
+class ThreadConfig {
+ public:
+  ThreadConfig(std::size_t x = 1, std::size_t y = 1, std::size_t z = 1) : _n{x, y, z} {}
+
+ private:
+  std::array<std::size_t, 3> _n;
+};
+
+enum class Precision { FP64 = 0, FP32 = 1 };
+
+// ------------------------------------------------------------- Simulation
+class Simulation {
+ public:
+  /// Simulation(dx, dy, dz, cfl, thread_config) -- thread_config is accepted
+  /// and ignored: the time loop runs on the GPU.
+  Simulation(Real dx, Real dy, Real dz, Real cfl, ThreadConfig thread_config = {1, 1, 1});
+  ~Simulation();
+  Simulation(const Simulation&) = delete;
+  Simulation& operator=(const Simulation&) = delete;
+
+  void addObject(std::shared_ptr<Object> object);
+  void addBoundary(std::shared_ptr<Boundary> boundary);
+  void addWaveformSource(std::shared_ptr<WaveformSource> source);
+  void addMonitor(std::shared_ptr<Monitor> monitor);
+  void addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> nffft);
+
+  /// Builds the grid and coefficients, runs `time_step` steps on the GPU and
+  /// copies fields, movie frames and NF2FF currents back to the host.
+  void run(Index time_step);
+
+  /// Set-up only (grid, coefficients, engine upload) for `time_step` steps;
+  /// run() calls it.  Exposed so that a caller can time the steps alone.
+  void init(Index time_step);
+  /// Advances `n` steps of an initialised simulation (asynchronous).
+  void advance(Index n);
+  /// Waits for the GPU and copies the outputs back (what run() does last).
+  void finish();
+
+  void setPrecision(Precision p) { _precision = p; }
+  /// With false, init() stops after the host set-up (grid, classes, curl
+  /// factors, CPML, ADE) and creates no engine: for checking the set-up
+  /// arithmetic on a machine without a GPU.
+  void setEngineEnabled(bool on) { _use_engine = on; }
+  Precision precision() const { return _precision; }
+
+  const EMF& emf() const { return _emf; }
+  Real dt() const { return _dt; }
+  std::array<Index, 3> gridSize() const { return {_n[0], _n[1], _n[2]}; }
+  xfd_engine* engine() const { return _engine; }
+
+  /// The 18 Yee coefficient arrays as the engine applies them (class table x
+  /// curl factors), in the reference shapes; order cexe cexhy cexhz ceye
+  /// ceyhz ceyhx ceze cezhx cezhy chxh chxey chxez chyh chyez chyex chzh
+  /// chzex chzey.  For checking the set-up against the reference's formulas.
+  std::vector<std::vector<Real>> coefficientArrays() const;
+
+  struct Impl;
+
+ private:
+  void setupTfsf(xfd_engine* e);
+  void setupNf2ff(xfd_engine* e);
+
+  Real _dl[3];
+  Real _cfl;
+  Precision _precision = Precision::FP64;
+  bool _use_engine = true;
+  std::vector<std::shared_ptr<Object>> _objects;
+  std::vector<std::shared_ptr<Boundary>> _boundaries;
+  std::vector<std::shared_ptr<WaveformSource>> _sources;
+  std::vector<std::shared_ptr<Monitor>> _monitors;
+  std::vector<std::shared_ptr<NFFFTFrequencyDomain>> _nffts;
+  EMF _emf;
+  Real _dt = 0;
+  Index _n[3] = {0, 0, 0};
+  Index _steps = 0;
+  xfd_engine* _engine = nullptr;
+  std::unique_ptr<Impl> _impl;
+};
+
+}  // namespace xfdtd

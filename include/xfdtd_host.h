@@ -1,0 +1,62 @@
+/*
+ * xfdtd_host.h -- C entry points of the C++20 host library (libxfdtd_host.so)
+ * for callers that cannot use the C++ API (Python ctypes, test harnesses).
+ *
+ * A scene file is the line format written by xfdtd_core_b200.scene.Scene:
+ * each line becomes the xfdtd:: API call a reference user program would make
+ * (Simulation ctor, addObject, addBoundary(PML), addWaveformSource(TFSF3D),
+ * CurrentSource, MovieMonitor, NFFFTFrequencyDomain).  These calls have no
+ * counterpart in the reference, whose only user interface is C++.
+ */
+#ifndef XFDTD_HOST_H_
+#define XFDTD_HOST_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct xfd_engine;
+typedef struct xfdtd_scene xfdtd_scene;
+
+/* Parses `path`, builds the Simulation and runs its set-up (grid, classes,
+ * CPML, TFSF, ADE, NF2FF, engine upload) for the scene's step count.
+ * precision: 0 = FP64, 1 = FP32, optionally or-ed with XFDTD_SCENE_NO_ENGINE
+ * (host set-up only, no GPU needed; only xfdtd_scene_info and
+ * xfdtd_scene_coefficients are then usable).  Returns 0 on success. */
+#define XFDTD_SCENE_NO_ENGINE 0x100
+int xfdtd_scene_open(const char* path, int32_t precision, xfdtd_scene** out);
+void xfdtd_scene_close(xfdtd_scene* s);
+/* Message of the last failure on this thread. */
+const char* xfdtd_host_last_error(void);
+
+/* The engine the scene drives (owned by the scene). */
+struct xfd_engine* xfdtd_scene_engine(xfdtd_scene* s);
+/* Grid size (cells), time step and scene step count. */
+int xfdtd_scene_info(xfdtd_scene* s, int32_t n[3], double* dt, int64_t* steps);
+/* Queues n time steps (Simulation::advance). */
+int xfdtd_scene_advance(xfdtd_scene* s, int64_t n);
+/* Waits and copies fields, movie frames and NF2FF currents to the host
+ * (Simulation::finish). */
+int xfdtd_scene_finish(xfdtd_scene* s);
+/* The 18 coefficient arrays in reference shapes (see
+ * Simulation::coefficientArrays); each out[q] must hold the array. */
+int xfdtd_scene_coefficients(xfdtd_scene* s, double* const out[18]);
+/* Host copy of field `comp` (0..5) after finish, reference shape. */
+int xfdtd_scene_field(xfdtd_scene* s, int32_t comp, double* out);
+/* Frames of movie `index` (scene order): n_frames and the box shape; with
+ * out != NULL copies n_frames*prod(shape) doubles. */
+int xfdtd_scene_movie(xfdtd_scene* s, int32_t index, double* out, int64_t capacity,
+                      int64_t* n_frames, int32_t shape[3]);
+/* NF2FF surface currents (complex interleaved, [f][face][ja jb ma mb][nodes]). */
+int xfdtd_scene_nf2ff(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count);
+/* Writes <dir>/fields/{EX..HZ}.npy, <dir>/<movie>/<step:05d>.npy and
+ * <dir>/nf2ff.npy like the reference's Monitor::output (src/monitor/monitor.cpp:42-54). */
+int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XFDTD_HOST_H_ */

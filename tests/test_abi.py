@@ -26,3 +26,13 @@ def test_engine_exports_header_symbols():
 
 def test_engine_built_for_sm100a_only():
     assert "compute_100a" in " ".join(build.NVCC_FLAGS)
+
+
+def test_host_exports_header_symbols():
+    from xfdtd_core_b200 import host
+    build.build_host()
+    lib = ctypes.CDLL(build.HOST_LIB)
+    names = [n for n in _declared("xfdtd_host.h")]
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(host.exported_symbols()) == names

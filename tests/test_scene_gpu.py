@@ -1,0 +1,83 @@
+"""End-to-end parity through the drop-in host: the C++ xfdtd::Simulation built
+from a scene runs on the GPU; fields, movie frames and NF2FF surface currents
+are compared with the oracle on the same scene.  FP64 tolerance: relative L2
+<= 1e-12 (north_star's bar for the plain form).  FP32 form: the error budget
+against the FP64 oracle is stated per test."""
+import numpy as np
+import pytest
+
+from oracle.reference_model import RefSimulation
+from tests.cases import rel_l2
+from tests.scenes import ALL, sphere_small, dispersive_small
+from xfdtd_core_b200 import scene as S
+from xfdtd_core_b200.host import SceneRun
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-12
+
+
+def _fields_rel(run, orc):
+    got = run.fields()
+    want = orc.e + orc.h
+    ref = max(np.linalg.norm(w) for w in want)
+    return [float(np.linalg.norm(g - w) / ref) for g, w in zip(got, want)]
+
+
+@pytest.mark.parametrize("name", sorted(ALL))
+def test_scene_fp64_matches_oracle(name):
+    sc = ALL[name](steps=150)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc)
+    run.run()
+    errs = _fields_rel(run, orc)
+    assert max(errs) <= TOL64, errs
+    if sc.movies:
+        got = run.movie(0)
+        want = np.array(orc.movie_frames[sc.movies[0].name])
+        assert got.shape == want.shape
+        assert rel_l2(got, want) <= TOL64
+    if sc.nf2ff is not None:
+        got = run.nf2ff()
+        acc = orc.nf2ff["acc"]
+        want = acc[0::2] + 1j * acc[1::2]
+        assert got.shape == want.shape
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
+
+
+def test_dielectric_sphere_full_size_fp64():
+    """The reference example at 63^3 with 8-cell PML, 2000 steps, Ex XZ movie
+    every 10 steps: all 200 frames within 1e-12 of the oracle."""
+    sc = S.dielectric_sphere(steps=2000)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc)
+    run.run()
+    got = run.movie(0)
+    want = np.array(orc.movie_frames["movie_ex_xz"])
+    assert got.shape == want.shape == (200, 47, 1, 47)
+    assert rel_l2(got, want) <= TOL64
+    assert max(_fields_rel(run, orc)) <= TOL64
+
+
+@pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
+                                         ("dispersive", 1e-4)])
+def test_scene_fp32_error_budget(name, budget):
+    sc = ALL[name](steps=150)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc, precision=1)
+    run.run()
+    errs = _fields_rel(run, orc)
+    assert max(errs) <= budget, errs
+
+
+def test_outputs_written(tmp_path):
+    sc = sphere_small(steps=30)
+    run = SceneRun(sc)
+    run.run()
+    run.write_outputs(str(tmp_path))
+    ex = np.load(tmp_path / "fields" / "EX.npy")
+    assert ex.shape == run.field(0).shape
+    frames = sorted((tmp_path / "movie_ex_xz").glob("*.npy"))
+    assert [f.name for f in frames] == ["00000.npy", "00010.npy", "00020.npy"]

@@ -77,7 +77,7 @@ def build_host(force: bool = False) -> str:
         return ""
     if not force and not _newer(HOST_LIB, srcs + [ENGINE_LIB]):
         return HOST_LIB
-    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra",
+    cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-fopenmp", "-Wall", "-Wextra",
            "-ffp-contract=off", "-I" + INCLUDE, "-I" + HOST_SRC, "-o", HOST_LIB + ".tmp", *cpp,
            "-L" + LIBDIR, "-lxfd_engine", "-Wl,-rpath,$ORIGIN"]
     subprocess.check_call(cmd)

@@ -1,0 +1,362 @@
+// Scene-file front end of the host library: parses the line format of
+// xfdtd_core_b200.scene.Scene into the xfdtd:: API calls a reference user
+// program makes, and exposes the Simulation through the C entry points of
+// xfdtd_host.h.
+#include <cmath>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "xfd_engine.h"
+#include "xfdtd/xfdtd.h"
+#include "xfdtd_host.h"
+
+using namespace xfdtd;
+
+namespace {
+
+thread_local std::string g_err;
+
+Axis::Direction parseDir(const std::string& s) {
+  static const char* names[6] = {"XN", "XP", "YN", "YP", "ZN", "ZP"};
+  for (int i = 0; i < 6; ++i)
+    if (s == names[i]) return static_cast<Axis::Direction>(i);
+  throw XFDTDException("bad direction '" + s + "'");
+}
+
+EMF::Field parseField(const std::string& s) {
+  static const char* names[6] = {"EX", "EY", "EZ", "HX", "HY", "HZ"};
+  for (int i = 0; i < 6; ++i)
+    if (s == names[i]) return static_cast<EMF::Field>(i);
+  throw XFDTDException("bad field '" + s + "'");
+}
+
+double num(std::istringstream& in) {
+  std::string tok;
+  if (!(in >> tok)) throw XFDTDException("unexpected end of line");
+  char* end = nullptr;
+  const double v = std::strtod(tok.c_str(), &end);
+  if (end == tok.c_str() || *end != '\0') throw XFDTDException("bad number '" + tok + "'");
+  return v;
+}
+
+std::unique_ptr<Waveform> parseWaveform(std::istringstream& in) {
+  std::string kind;
+  in >> kind;
+  if (kind == "gaussian") {
+    const double tau = num(in), t0 = num(in), amp = num(in);
+    return Waveform::gaussian(tau, t0, amp);
+  }
+  if (kind == "cosgauss") {
+    const double tau = num(in), t0 = num(in), f = num(in), amp = num(in);
+    return Waveform::cosineModulatedGaussian(tau, t0, f, amp);
+  }
+  throw XFDTDException("bad waveform '" + kind + "'");
+}
+
+std::shared_ptr<Material> parseMaterial(std::istringstream& in, const std::string& name) {
+  std::string kind;
+  in >> kind;
+  if (kind == "simple") {
+    const double er = num(in), mr = num(in), se = num(in), sm = num(in);
+    return std::make_shared<Material>(name, ElectroMagneticProperty{er, mr, se, sm});
+  }
+  const double eps_inf = num(in);
+  const int P = static_cast<int>(num(in));
+  if (kind == "drude" || kind == "debye") {
+    std::vector<Real> x, y;
+    for (int p = 0; p < P; ++p) {
+      x.push_back(num(in));
+      y.push_back(num(in));
+    }
+    if (kind == "drude")
+      return DrudeMedium::makeDrudeMedium(name, eps_inf, Array1D<Real>(x), Array1D<Real>(y));
+    return DebyeMedium::makeDebyeMedium(name, eps_inf, Array1D<Real>(x), Array1D<Real>(y));
+  }
+  if (kind == "mlorentz") {
+    std::vector<Real> v[5];
+    for (int p = 0; p < P; ++p)
+      for (int q = 0; q < 5; ++q) v[q].push_back(num(in));
+    return MLorentzMaterial::makeMLorentz(name, eps_inf, Array1D<Real>(v[0]), Array1D<Real>(v[1]),
+                                          Array1D<Real>(v[2]), Array1D<Real>(v[3]),
+                                          Array1D<Real>(v[4]));
+  }
+  throw XFDTDException("bad material '" + kind + "'");
+}
+
+void writeNpy(const std::string& path, const std::vector<double>& data,
+              const std::vector<std::size_t>& shape) {
+  std::ostringstream hdr;
+  hdr << "{'descr': '<f8', 'fortran_order': False, 'shape': (";
+  for (std::size_t i = 0; i < shape.size(); ++i) hdr << shape[i] << (shape.size() == 1 ? "," : (i + 1 < shape.size() ? ", " : ""));
+  hdr << "), }";
+  std::string h = hdr.str();
+  const std::size_t total = 10 + h.size() + 1;
+  h.append((64 - total % 64) % 64, ' ');
+  h.push_back('\n');
+  std::ofstream f(path, std::ios::binary);
+  if (!f) throw XFDTDException("cannot write " + path);
+  const char magic[] = "\x93NUMPY\x01\x00";
+  f.write(magic, 8);
+  const uint16_t len = static_cast<uint16_t>(h.size());
+  f.write(reinterpret_cast<const char*>(&len), 2);
+  f.write(h.data(), (std::streamsize)h.size());
+  f.write(reinterpret_cast<const char*>(data.data()), (std::streamsize)(data.size() * 8));
+}
+
+}  // namespace
+
+struct xfdtd_scene {
+  std::unique_ptr<Simulation> sim;
+  std::vector<std::shared_ptr<MovieMonitor>> movies;
+  std::shared_ptr<NFFFTFrequencyDomain> nf2ff;
+  int64_t steps = 0;
+  bool finished = false;
+};
+
+static xfdtd_scene* buildScene(const char* path, int32_t precision) {
+  std::ifstream f(path);
+  if (!f) throw XFDTDException(std::string("cannot open scene file ") + path);
+  auto sc = std::make_unique<xfdtd_scene>();
+  std::string line;
+  double dl[3] = {0, 0, 0}, cfl = 0;
+  bool have_grid = false;
+  std::vector<std::string> body;
+  while (std::getline(f, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream in(line);
+    std::string kw;
+    in >> kw;
+    if (kw == "grid") {
+      dl[0] = num(in);
+      dl[1] = num(in);
+      dl[2] = num(in);
+      cfl = num(in);
+      have_grid = true;
+    } else if (kw == "steps") {
+      sc->steps = static_cast<int64_t>(num(in));
+    } else if (kw == "xfdtd-scene" || kw == "name") {
+      continue;
+    } else {
+      body.push_back(line);
+    }
+  }
+  if (!have_grid) throw XFDTDException("scene has no grid line");
+  sc->sim = std::make_unique<Simulation>(dl[0], dl[1], dl[2], cfl, ThreadConfig{1, 1, 1});
+  sc->sim->setPrecision((precision & 0xFF) == 1 ? Precision::FP32 : Precision::FP64);
+  sc->sim->setEngineEnabled((precision & XFDTD_SCENE_NO_ENGINE) == 0);
+  for (const auto& l : body) {
+    std::istringstream in(l);
+    std::string kw, name;
+    in >> kw;
+    if (kw == "object") {
+      std::string shape;
+      in >> name >> shape;
+      std::unique_ptr<Shape> sh;
+      if (shape == "cube") {
+        const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                     sz = num(in);
+        sh = std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz});
+      } else if (shape == "sphere") {
+        const double cx = num(in), cy = num(in), cz = num(in), r = num(in);
+        sh = std::make_unique<Sphere>(Vector{cx, cy, cz}, r);
+      } else {
+        throw XFDTDException("bad shape '" + shape + "'");
+      }
+      auto mat = parseMaterial(in, name);
+      sc->sim->addObject(std::make_shared<Object>(name, std::move(sh), mat));
+    } else if (kw == "current_source") {
+      in >> name;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      std::string dir;
+      in >> dir;
+      const double r = num(in);
+      auto w = parseWaveform(in);
+      sc->sim->addObject(std::make_shared<CurrentSource>(
+          name, std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), parseDir(dir), r,
+          std::move(w)));
+    } else if (kw == "pml") {
+      const int t = static_cast<int>(num(in));
+      std::string dir;
+      in >> dir;
+      const int order = static_cast<int>(num(in));
+      const double sr = num(in), amin = num(in), amax = num(in), kmax = num(in);
+      sc->sim->addBoundary(std::make_shared<PML>(t, parseDir(dir), order, sr, amin, amax, kmax));
+    } else if (kw == "tfsf3d") {
+      const auto x = static_cast<std::size_t>(num(in)), y = static_cast<std::size_t>(num(in)),
+                 z = static_cast<std::size_t>(num(in));
+      const double th = num(in), ph = num(in), ps = num(in);
+      sc->sim->addWaveformSource(std::make_shared<TFSF3D>(x, y, z, th, ph, ps, parseWaveform(in)));
+    } else if (kw == "movie") {
+      std::string field;
+      in >> name >> field;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      const auto interval = static_cast<std::size_t>(num(in));
+      auto fm = std::make_unique<FieldMonitor>(
+          std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), parseField(field));
+      auto mv = std::make_shared<MovieMonitor>(std::move(fm), interval, name, name);
+      sc->movies.push_back(mv);
+      sc->sim->addMonitor(mv);
+    } else if (kw == "nf2ff_fd") {
+      const auto dx = static_cast<Index>(num(in)), dy = static_cast<Index>(num(in)),
+                 dz = static_cast<Index>(num(in));
+      const int nf = static_cast<int>(num(in));
+      std::vector<Real> fr;
+      for (int q = 0; q < nf; ++q) fr.push_back(num(in));
+      sc->nf2ff = std::make_shared<NFFFTFrequencyDomain>(dx, dy, dz, Array1D<Real>(fr));
+      sc->sim->addNF2FF(sc->nf2ff);
+    } else {
+      throw XFDTDException("unknown scene line: " + l);
+    }
+  }
+  sc->sim->init(static_cast<Index>(sc->steps));
+  return sc.release();
+}
+
+#define HOST_TRY(...)                   \
+  try {                                 \
+    __VA_ARGS__;                        \
+    return 0;                           \
+  } catch (const std::exception& ex) {  \
+    g_err = ex.what();                  \
+    return 1;                           \
+  }
+
+extern "C" {
+
+int xfdtd_scene_open(const char* path, int32_t precision, xfdtd_scene** out) {
+  HOST_TRY({
+    if (!path || !out) throw XFDTDException("null argument");
+    *out = buildScene(path, precision);
+  })
+}
+
+void xfdtd_scene_close(xfdtd_scene* s) { delete s; }
+
+const char* xfdtd_host_last_error(void) { return g_err.c_str(); }
+
+struct xfd_engine* xfdtd_scene_engine(xfdtd_scene* s) { return s ? s->sim->engine() : nullptr; }
+
+int xfdtd_scene_info(xfdtd_scene* s, int32_t n[3], double* dt, int64_t* steps) {
+  HOST_TRY({
+    if (!s) throw XFDTDException("null scene");
+    auto g = s->sim->gridSize();
+    if (n)
+      for (int a = 0; a < 3; ++a) n[a] = (int32_t)g[a];
+    if (dt) *dt = s->sim->dt();
+    if (steps) *steps = s->steps;
+  })
+}
+
+int xfdtd_scene_advance(xfdtd_scene* s, int64_t n) {
+  HOST_TRY({
+    if (!s) throw XFDTDException("null scene");
+    s->sim->advance(static_cast<Index>(n));
+    s->finished = false;
+  })
+}
+
+int xfdtd_scene_finish(xfdtd_scene* s) {
+  HOST_TRY({
+    if (!s) throw XFDTDException("null scene");
+    s->sim->finish();
+    s->finished = true;
+  })
+}
+
+int xfdtd_scene_coefficients(xfdtd_scene* s, double* const out[18]) {
+  HOST_TRY({
+    if (!s || !out) throw XFDTDException("null argument");
+    auto arrs = s->sim->coefficientArrays();
+    for (int q = 0; q < 18; ++q) std::memcpy(out[q], arrs[q].data(), arrs[q].size() * 8);
+  })
+}
+
+int xfdtd_scene_field(xfdtd_scene* s, int32_t comp, double* out) {
+  HOST_TRY({
+    if (!s || !out || comp < 0 || comp > 5) throw XFDTDException("bad argument");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    const auto& a = s->sim->emf().field(static_cast<EMF::Field>(comp));
+    std::memcpy(out, a.data(), a.size() * 8);
+  })
+}
+
+int xfdtd_scene_movie(xfdtd_scene* s, int32_t index, double* out, int64_t capacity,
+                      int64_t* n_frames, int32_t shape[3]) {
+  HOST_TRY({
+    if (!s || index < 0 || index >= (int32_t)s->movies.size())
+      throw XFDTDException("bad movie index");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    const auto& mv = s->movies[index];
+    const auto& fr = mv->frames();
+    const auto shp = mv->frameShape();
+    if (n_frames) *n_frames = (int64_t)fr.size();
+    if (shape)
+      for (int a = 0; a < 3; ++a) shape[a] = (int32_t)shp[a];
+    if (out) {
+      const std::size_t per = shp[0] * shp[1] * shp[2];
+      if ((std::size_t)capacity < per * fr.size()) throw XFDTDException("buffer too small");
+      for (std::size_t q = 0; q < fr.size(); ++q) std::memcpy(out + q * per, fr[q].data(), per * 8);
+    }
+  })
+}
+
+int xfdtd_scene_nf2ff(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count) {
+  HOST_TRY({
+    if (!s || !s->nf2ff) throw XFDTDException("scene has no NF2FF");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    const auto& acc = s->nf2ff->surfaceCurrents();
+    if (count) *count = (int64_t)acc.size();
+    if (out) {
+      if ((std::size_t)capacity < acc.size()) throw XFDTDException("buffer too small");
+      for (std::size_t q = 0; q < acc.size(); ++q) {
+        out[2 * q] = acc[q].real();
+        out[2 * q + 1] = acc[q].imag();
+      }
+    }
+  })
+}
+
+int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir) {
+  HOST_TRY({
+    if (!s || !dir) throw XFDTDException("null argument");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    namespace fs = std::filesystem;
+    const fs::path root(dir);
+    fs::create_directories(root / "fields");
+    static const char* names[6] = {"EX", "EY", "EZ", "HX", "HY", "HZ"};
+    for (int c = 0; c < 6; ++c) {
+      const auto& a = s->sim->emf().field(static_cast<EMF::Field>(c));
+      std::vector<double> v(a.data(), a.data() + a.size());
+      writeNpy((root / "fields" / (std::string(names[c]) + ".npy")).string(), v,
+               {a.shape()[0], a.shape()[1], a.shape()[2]});
+    }
+    for (const auto& mv : s->movies) {
+      const fs::path d = root / mv->name();
+      fs::create_directories(d);
+      const auto shp = mv->frameShape();
+      for (std::size_t q = 0; q < mv->frames().size(); ++q) {
+        std::ostringstream nm;  // MovieMonitor::formatFrameCount: the step, 5 digits
+        nm << std::setw(5) << std::setfill('0') << q * mv->frameInterval();
+        writeNpy((d / (nm.str() + ".npy")).string(), mv->frames()[q], {shp[0], shp[1], shp[2]});
+      }
+    }
+    if (s->nf2ff) {
+      const auto& acc = s->nf2ff->surfaceCurrents();
+      std::vector<double> v;
+      for (const auto& z : acc) {
+        v.push_back(z.real());
+        v.push_back(z.imag());
+      }
+      writeNpy((root / "nf2ff.npy").string(), v, {acc.size(), 2});
+    }
+  })
+}
+
+}  // extern "C"

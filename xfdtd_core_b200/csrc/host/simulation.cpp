@@ -1,0 +1,1084 @@
+// xfdtd::Simulation on the B200 engine.
+//
+// Simulation::init restates, in FP64 on the host, the reference's set-up of
+// the 3-D FDTD path and hands the result to the engine C ABI:
+//   grid generation        src/grid_space/grid_space_generator.cpp:16-217,
+//                          src/grid_space/grid_space.cpp:517-544
+//   time step              src/calculation_param/time_param.cpp:10-13
+//   painting               src/object/object.cpp:114-198 (cell centre inside,
+//                          last object wins)
+//   edge/face averaging    src/calculation_param/calculation_param.cpp:43-168
+//   Yee coefficients       calculation_param.cpp:170-264
+//   lumped current source  src/object/lumped_element/current_source.cpp:43-165
+//   CPML grading / kappa   src/boundary/pml.cpp:98-244, 286-633
+//   TFSF incident grid     src/waveform_source/tfsf.cpp:36-302
+//   ADE coefficients       src/material/ade_method/{m_lor,drude,debye}_ade_method.cpp
+//   NF2FF surfaces/phasors src/nffft/nffft.cpp:88-245, nffft_fd_data.cpp:65-76
+// Instead of 18 full-grid coefficient arrays the engine receives a table of
+// material classes (the (ca, cb) pair of each component, keyed by the
+// materials of the 2x2x2 cells around a lattice node) plus a uint16 class per
+// node, and per-axis curl factors 1/(d*kappa).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <numeric>
+#include <sstream>
+#include <unordered_map>
+
+#include "xfd_engine.h"
+#include "xfdtd/xfdtd.h"
+
+namespace xfdtd {
+
+using constant::C_0;
+using constant::EPSILON_0;
+using constant::MU_0;
+using constant::PI;
+
+// ------------------------------------------------------------ shapes
+static bool floatLE(Real lhs, Real rhs, Real eps) {
+  // floatCompare(lhs, rhs, LessEqual, eps) (src/include/util/float_compare.h:20-42)
+  return std::abs(lhs - rhs) <= eps ? true : lhs < rhs;
+}
+
+bool Cube::isInside(Real x, Real y, Real z, Real eps) const {
+  // Cube::isInside (src/shape/cube.cpp:58-73)
+  return floatLE(_origin.x(), x, eps) && floatLE(x, _end.x(), eps) &&
+         floatLE(_origin.y(), y, eps) && floatLE(y, _end.y(), eps) &&
+         floatLE(_origin.z(), z, eps) && floatLE(z, _end.z(), eps);
+}
+
+bool Sphere::isInside(Real x, Real y, Real z, Real eps) const {
+  // Sphere::isInside (src/shape/sphere.cpp:29-32)
+  const Real dx = x - _center.x(), dy = y - _center.y(), dz = z - _center.z();
+  return floatLE(std::sqrt(dx * dx + dy * dy + dz * dz), _radius, eps);
+}
+
+std::unique_ptr<Cube> Sphere::wrappedCube() const {
+  // Sphere::wrappedCube (src/shape/sphere.cpp:34-37)
+  return std::make_unique<Cube>(_center - Vector{_radius, _radius, _radius},
+                                Vector{_radius * 2, _radius * 2, _radius * 2});
+}
+
+ElectroMagneticProperty::ElectroMagneticProperty(Real eps_r, Real mu_r, Real sigma_e,
+                                                 Real sigma_m)
+    : _eps_r{eps_r},
+      _mu_r{mu_r},
+      _sigma_e{sigma_e == 0 ? constant::SIGMA_E_ZERO_APPROX : sigma_e},
+      _sigma_m{sigma_m == 0 ? constant::SIGMA_M_ZERO_APPROX : sigma_m} {}
+
+// --------------------------------------------------------- materials
+std::unique_ptr<DrudeMedium> DrudeMedium::makeDrudeMedium(std::string_view name, Real eps_inf,
+                                                          Array1D<Real> omega_p,
+                                                          Array1D<Real> gamma) {
+  // DrudeEqDecision: a0 = wp^2, a1 = 0, b0 = 0, b1 = gamma, b2 = 1
+  // (src/material/dispersive_material_equation.cpp:49-54)
+  std::vector<std::array<Real, 5>> poles;
+  std::vector<std::array<Real, 2>> native;
+  for (Index p = 0; p < omega_p.size(); ++p) {
+    poles.push_back({omega_p[p] * omega_p[p], 0.0, 0.0, gamma[p], 1.0});
+    native.push_back({omega_p[p], gamma[p]});
+  }
+  return std::make_unique<DrudeMedium>(name, eps_inf, Kind::Drude, poles, native);
+}
+
+std::unique_ptr<DebyeMedium> DebyeMedium::makeDebyeMedium(std::string_view name, Real eps_inf,
+                                                          Array1D<Real> eps_static,
+                                                          Array1D<Real> tau) {
+  // DebyeEqDecision: a0 = eps_s - eps_inf, a1 = 0, b0 = 1, b1 = tau, b2 = 0
+  // (dispersive_material_equation.cpp:43-47)
+  std::vector<std::array<Real, 5>> poles;
+  std::vector<std::array<Real, 2>> native;
+  for (Index p = 0; p < eps_static.size(); ++p) {
+    poles.push_back({eps_static[p] - eps_inf, 0.0, 1.0, tau[p], 0.0});
+    native.push_back({eps_static[p], tau[p]});
+  }
+  return std::make_unique<DebyeMedium>(name, eps_inf, Kind::Debye, poles, native);
+}
+
+std::unique_ptr<MLorentzMaterial> MLorentzMaterial::makeMLorentz(
+    std::string_view name, Real eps_inf, Array1D<Real> a0, Array1D<Real> a1, Array1D<Real> b0,
+    Array1D<Real> b1, Array1D<Real> b2) {
+  if (a1.size() != a0.size() || b0.size() != a0.size() || b1.size() != a0.size() ||
+      b2.size() != a0.size())
+    throw XFDTDException("Modified Lorentz Model paramater doesn't have same size.");
+  std::vector<std::array<Real, 5>> poles;
+  std::vector<std::array<Real, 2>> native;
+  for (Index p = 0; p < a0.size(); ++p) {
+    poles.push_back({a0[p], a1[p], b0[p], b1[p], b2[p]});
+    native.push_back({0.0, 0.0});
+  }
+  return std::make_unique<MLorentzMaterial>(name, eps_inf, Kind::MLorentz, poles, native);
+}
+
+// ---------------------------------------------------------- waveform
+std::unique_ptr<Waveform> Waveform::gaussian(Real tau, Real t_0, Real amplitude) {
+  return std::make_unique<Waveform>(
+      [tau, t_0](Real t) { return std::exp(-std::pow((t - t_0) / tau, 2)); }, amplitude);
+}
+
+std::unique_ptr<Waveform> Waveform::cosineModulatedGaussian(Real tau, Real t_0, Real frequency,
+                                                            Real amplitude) {
+  return std::make_unique<Waveform>(
+      [tau, t_0, frequency](Real t) {
+        return std::exp(-std::pow((t - t_0) / tau, 2)) *
+               std::cos(2 * constant::PI * frequency * (t - t_0));
+      },
+      amplitude);
+}
+
+std::unique_ptr<Waveform> Waveform::sine(Real frequency, Real amplitude) {
+  return std::make_unique<Waveform>(
+      [frequency](Real t) { return std::sin(2 * constant::PI * frequency * t); }, amplitude);
+}
+
+void Waveform::init(const std::vector<Real>& time) {
+  // Waveform::init (src/waveform/waveform.cpp:28-34)
+  std::vector<Real> v(time.size());
+  for (std::size_t i = 0; i < time.size(); ++i) v[i] = amplitude() * _f(time[i]);
+  _value = Array1D<Real>(std::move(v));
+  _time = Array1D<Real>(time);
+}
+
+// --------------------------------------------------------- helpers
+namespace {
+
+std::vector<Real> linspace(Real a, Real b, std::size_t n) {
+  // xt::linspace with endpoint: a + i*step, the last sample exactly b.
+  std::vector<Real> v(n);
+  if (n == 1) {
+    v[0] = a;
+    return v;
+  }
+  const Real step = (b - a) / static_cast<Real>(n - 1);
+  for (std::size_t i = 0; i < n; ++i) v[i] = a + step * static_cast<Real>(i);
+  v[n - 1] = b;
+  return v;
+}
+
+std::size_t nearestNode(const std::vector<Real>& nodes, Real x) {
+  // argmin |e_node - x| (src/grid_space/grid_space.cpp:505-515); first on ties.
+  std::size_t best = 0;
+  Real bd = std::abs(nodes[0] - x);
+  for (std::size_t i = 1; i < nodes.size(); ++i) {
+    const Real d = std::abs(nodes[i] - x);
+    if (d < bd) {
+      bd = d;
+      best = i;
+    }
+  }
+  return best;
+}
+
+constexpr uint16_t kNoCell = 0xFFFF;
+
+struct ClassKey {
+  uint16_t m[8];
+  uint8_t flags;
+  bool operator==(const ClassKey& o) const {
+    return flags == o.flags && std::memcmp(m, o.m, sizeof m) == 0;
+  }
+};
+
+struct ClassKeyHash {
+  std::size_t operator()(const ClassKey& k) const {
+    uint64_t a, b;
+    std::memcpy(&a, k.m, 8);
+    std::memcpy(&b, k.m + 4, 8);
+    uint64_t h = a * 0x9E3779B97F4A7C15ULL ^ (b + 0x632BE59BD9B4E019ULL + (a << 6) + (a >> 2));
+    return static_cast<std::size_t>(h ^ (uint64_t)k.flags * 0xC2B2AE3D27D4EB4FULL);
+  }
+};
+
+struct MatP {
+  Real eps, mu, se, sm;
+};
+
+void checkStatus(xfd_engine* e, int st, const char* what) {
+  if (st != 0) {
+    std::ostringstream os;
+    os << what << " failed (" << st << "): " << xfd_last_error(e);
+    throw XFDTDException(os.str());
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- impl
+struct Simulation::Impl {
+  std::vector<Real> e_node[3], h_node[3], e_size[3], h_size[3];
+  Real min_d[3]{};
+  std::vector<uint16_t> cell;  // painter index per cell (nx*ny*nz)
+  std::vector<const Material*> painters;
+  std::vector<MatP> mat;
+  std::vector<double> table;    // classes x 12
+  std::vector<uint16_t> lattice_class;
+  std::vector<Real> fe[3], fh[3];
+  struct SlabH {
+    int axis, neg, n, e_start, h_start;
+    std::vector<Real> a_e, b_e, a_h, b_h, kappa_e, kappa_h;
+  };
+  std::vector<SlabH> slabs;
+  struct MovieH {
+    MovieMonitor* mon;
+    int id;
+    int s[3], e[3];
+  };
+  std::vector<MovieH> movies;
+  NFFFTFrequencyDomain* nf2ff = nullptr;
+  bool initialised = false;
+};
+
+Simulation::Simulation(Real dx, Real dy, Real dz, Real cfl, ThreadConfig)
+    : _dl{dx, dy, dz}, _cfl{cfl}, _impl{std::make_unique<Impl>()} {}
+
+Simulation::~Simulation() {
+  if (_engine) xfd_destroy(_engine);
+}
+
+void Simulation::addObject(std::shared_ptr<Object> o) { _objects.push_back(std::move(o)); }
+void Simulation::addBoundary(std::shared_ptr<Boundary> b) { _boundaries.push_back(std::move(b)); }
+void Simulation::addWaveformSource(std::shared_ptr<WaveformSource> s) {
+  _sources.push_back(std::move(s));
+}
+void Simulation::addMonitor(std::shared_ptr<Monitor> m) { _monitors.push_back(std::move(m)); }
+void Simulation::addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> n) {
+  _nffts.push_back(std::move(n));
+}
+
+void Simulation::run(Index time_step) {
+  init(time_step);
+  advance(time_step);
+  finish();
+}
+
+void Simulation::init(Index time_step) {
+  if (_objects.empty()) throw XFDTDException("No object is added");
+  Impl& I = *_impl;
+  I = Impl{};
+  if (_engine) {
+    xfd_destroy(_engine);
+    _engine = nullptr;
+  }
+  _steps = time_step;
+
+  // ---------------------------------------------------------------- grid
+  Real lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = std::numeric_limits<Real>::max();
+    hi[a] = std::numeric_limits<Real>::lowest();
+  }
+  for (const auto& o : _objects) {  // Shape::makeWrappedCube (src/shape/shape.cpp:8-38)
+    auto c = o->shape()->wrappedCube();
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], c->origin()(a));
+      hi[a] = std::max(hi[a], c->end()(a));
+    }
+  }
+  {
+    Cube dom{Vector{lo[0], lo[1], lo[2]}, Vector{hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]}};
+    Real mn[3] = {dom.origin().x(), dom.origin().y(), dom.origin().z()};
+    Real mx[3] = {dom.end().x(), dom.end().y(), dom.end().z()};
+    for (const auto& b : _boundaries) {  // extendDomain (grid_space_generator.cpp:36-99)
+      auto p = std::dynamic_pointer_cast<PML>(b);
+      if (!p || p->thickness() < 0) continue;
+      const int a = Axis::axisOf(p->direction());
+      if (Axis::negative(p->direction())) mn[a] -= p->thickness() * _dl[a];
+      else mx[a] += p->thickness() * _dl[a];
+    }
+    Cube ext{Vector{mn[0], mn[1], mn[2]}, Vector{mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]}};
+    for (int a = 0; a < 3; ++a) {  // generateGridSpace3D (:183-217)
+      const Real l0 = ext.origin()(a), l1 = ext.end()(a);
+      const auto na = static_cast<Index>(std::round((l1 - l0) / _dl[a]));
+      if (na <= 1) throw XFDTDException("GridSpace is too small");
+      const Real top = l0 + _dl[a] * na;
+      I.e_node[a] = linspace(l0, l0 + (top - l0), na + 1);
+      _n[a] = na;
+      auto& e = I.e_node[a];
+      I.h_node[a].resize(na);
+      I.e_size[a].resize(na);
+      for (Index i = 0; i < na; ++i) {
+        I.h_node[a][i] = (e[i] + e[i + 1]) / 2;
+        I.e_size[a][i] = e[i + 1] - e[i];
+      }
+      std::vector<Real> tmp;
+      tmp.push_back(e.front() - _dl[a] / 2);
+      tmp.insert(tmp.end(), I.h_node[a].begin(), I.h_node[a].end());
+      tmp.push_back(e.back() + _dl[a] / 2);
+      I.h_size[a].resize(na + 1);
+      for (Index i = 0; i <= na; ++i) I.h_size[a][i] = tmp[i + 1] - tmp[i];
+      I.min_d[a] = *std::min_element(I.e_size[a].begin(), I.e_size[a].end());
+    }
+  }
+  const Index nx = _n[0], ny = _n[1], nz = _n[2];
+  _dt = _cfl / (C_0 * std::sqrt(1.0 / (I.min_d[0] * I.min_d[0]) +
+                                1.0 / (I.min_d[1] * I.min_d[1]) +
+                                1.0 / (I.min_d[2] * I.min_d[2])));
+  const Real dt = _dt;
+  const Real eps_tol = std::min({I.min_d[0], I.min_d[1], I.min_d[2]}) / 1000;
+  if (_objects.size() >= kNoCell) throw XFDTDException("too many objects");
+
+  // ------------------------------------------------------------ painting
+  I.cell.assign(nx * ny * nz, 0);
+  for (std::size_t idx = 0; idx < _objects.size(); ++idx) {
+    const auto& o = _objects[idx];
+    I.painters.push_back(o->material().get());
+    const auto& mp = o->material()->emProperty();
+    if (o->material()->dispersion()) {
+      auto air = ElectroMagneticProperty::air();
+      I.mat.push_back({air.epsilon(), air.mu(), air.sigmaE(), air.sigmaM()});
+    } else {
+      I.mat.push_back({mp.epsilon(), mp.mu(), mp.sigmaE(), mp.sigmaM()});
+    }
+    // Only cells whose centre lies within the wrapped cube (+ tolerance) can
+    // test inside; the reference tests every cell with the same predicate.
+    auto wc = o->shape()->wrappedCube();
+    Index r0[3], r1[3];
+    for (int a = 0; a < 3; ++a) {
+      const auto& hn = I.h_node[a];
+      const Real a0 = wc->origin()(a) - 2 * eps_tol, a1 = wc->end()(a) + 2 * eps_tol;
+      r0[a] = std::lower_bound(hn.begin(), hn.end(), a0) - hn.begin();
+      r1[a] = std::upper_bound(hn.begin(), hn.end(), a1) - hn.begin();
+    }
+    const Shape* sh = o->shape().get();
+#pragma omp parallel for schedule(static)
+    for (Index i = r0[0]; i < r1[0]; ++i)
+      for (Index j = r0[1]; j < r1[1]; ++j)
+        for (Index k = r0[2]; k < r1[2]; ++k)
+          if (sh->isInside(I.h_node[0][i], I.h_node[1][j], I.h_node[2][k], eps_tol))
+            I.cell[(i * ny + j) * nz + k] = static_cast<uint16_t>(idx);
+  }
+
+  // ------------------------------------------------------ material classes
+  const MatP def{EPSILON_0, MU_0, constant::SIGMA_E_ZERO_APPROX, constant::SIGMA_M_ZERO_APPROX};
+  auto classRow = [&](const ClassKey& key, double* row) {
+    auto P = [&](int a, int b, int c) -> const MatP& {
+      const uint16_t m = key.m[a * 4 + b * 2 + c];
+      return m == kNoCell ? def : I.mat[m];
+    };
+    const bool ig = key.flags & 1, il = key.flags & 2, jg = key.flags & 4, jl = key.flags & 8,
+               kg = key.flags & 16, kl = key.flags & 32;
+    auto eCoef = [&](Real eps, Real sig, double* out) {
+      out[0] = (2 * eps - dt * sig) / (2 * eps + dt * sig);
+      out[1] = (2 * dt) / (2 * eps + sig * dt);
+    };
+    auto hCoef = [&](Real mu, Real sig, double* out) {
+      out[0] = (2 * mu - dt * sig) / (2 * mu + dt * sig);
+      out[1] = (2 * dt) / (2 * mu + sig * dt);
+    };
+    auto avg4 = [](Real a, Real b, Real c, Real d) { return 0.25 * (((a + b) + c) + d); };
+    auto harm = [](Real a, Real b) { return 2 * a * b / (a + b); };
+    std::fill(row, row + 12, 0.0);
+    // Ex(i, j, k): cells (i, j-1..j, k-1..k)
+    if (il) {
+      if (jg && jl && kg && kl) {
+        eCoef(avg4(P(1, 1, 1).eps, P(1, 0, 1).eps, P(1, 1, 0).eps, P(1, 0, 0).eps),
+              avg4(P(1, 1, 1).se, P(1, 0, 1).se, P(1, 1, 0).se, P(1, 0, 0).se), row + 0);
+      } else if (jl && kl) {
+        eCoef(P(1, 1, 1).eps, P(1, 1, 1).se, row + 0);
+      } else {
+        eCoef(def.eps, def.se, row + 0);
+      }
+    }
+    // Ey(i, j, k): cells (i-1..i, j, k-1..k)
+    if (jl) {
+      if (ig && il && kg && kl) {
+        eCoef(avg4(P(1, 1, 1).eps, P(0, 1, 1).eps, P(1, 1, 0).eps, P(0, 1, 0).eps),
+              avg4(P(1, 1, 1).se, P(0, 1, 1).se, P(1, 1, 0).se, P(0, 1, 0).se), row + 2);
+      } else if (il && kl) {
+        eCoef(P(1, 1, 1).eps, P(1, 1, 1).se, row + 2);
+      } else {
+        eCoef(def.eps, def.se, row + 2);
+      }
+    }
+    // Ez(i, j, k): cells (i-1..i, j-1..j, k)
+    if (kl) {
+      if (ig && il && jg && jl) {
+        eCoef(avg4(P(1, 1, 1).eps, P(0, 1, 1).eps, P(1, 0, 1).eps, P(0, 0, 1).eps),
+              avg4(P(1, 1, 1).se, P(0, 1, 1).se, P(1, 0, 1).se, P(0, 0, 1).se), row + 4);
+      } else if (il && jl) {
+        eCoef(P(1, 1, 1).eps, P(1, 1, 1).se, row + 4);
+      } else {
+        eCoef(def.eps, def.se, row + 4);
+      }
+    }
+    // Hx(i, j, k): cells (i-1..i, j, k), harmonic mean
+    if (jl && kl) {
+      if (ig && il) {
+        hCoef(harm(P(1, 1, 1).mu, P(0, 1, 1).mu), harm(P(1, 1, 1).sm, P(0, 1, 1).sm), row + 6);
+      } else if (il) {
+        hCoef(P(1, 1, 1).mu, P(1, 1, 1).sm, row + 6);
+      } else {
+        hCoef(def.mu, def.sm, row + 6);
+      }
+    }
+    // Hy(i, j, k): cells (i, j-1..j, k)
+    if (il && kl) {
+      if (jg && jl) {
+        hCoef(harm(P(1, 1, 1).mu, P(1, 0, 1).mu), harm(P(1, 1, 1).sm, P(1, 0, 1).sm), row + 8);
+      } else if (jl) {
+        hCoef(P(1, 1, 1).mu, P(1, 1, 1).sm, row + 8);
+      } else {
+        hCoef(def.mu, def.sm, row + 8);
+      }
+    }
+    // Hz(i, j, k): cells (i, j, k-1..k)
+    if (il && jl) {
+      if (kg && kl) {
+        hCoef(harm(P(1, 1, 1).mu, P(1, 1, 0).mu), harm(P(1, 1, 1).sm, P(1, 1, 0).sm), row + 10);
+      } else if (kl) {
+        hCoef(P(1, 1, 1).mu, P(1, 1, 1).sm, row + 10);
+      } else {
+        hCoef(def.mu, def.sm, row + 10);
+      }
+    }
+  };
+  const Index NX = nx + 1, NY = ny + 1, NZ = nz + 1;
+  I.lattice_class.assign(NX * NY * NZ, 0);
+  {
+    std::unordered_map<ClassKey, uint16_t, ClassKeyHash> ids;
+    ClassKey last{};
+    uint16_t last_id = 0;
+    bool have_last = false;
+    for (Index i = 0; i < NX; ++i)
+      for (Index j = 0; j < NY; ++j)
+        for (Index k = 0; k < NZ; ++k) {
+          ClassKey key{};
+          key.flags = (i >= 1) | ((i < nx) << 1) | ((j >= 1) << 2) | ((j < ny) << 3) |
+                      ((k >= 1) << 4) | ((k < nz) << 5);
+          for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+              for (int c = 0; c < 2; ++c) {
+                const long ci = (long)i - 1 + a, cj = (long)j - 1 + b, ck = (long)k - 1 + c;
+                uint16_t m = kNoCell;
+                if (ci >= 0 && ci < (long)nx && cj >= 0 && cj < (long)ny && ck >= 0 &&
+                    ck < (long)nz)
+                  m = I.cell[((Index)ci * ny + cj) * nz + ck];
+                key.m[a * 4 + b * 2 + c] = m;
+              }
+          uint16_t id;
+          if (have_last && key == last) {
+            id = last_id;
+          } else {
+            auto it = ids.find(key);
+            if (it == ids.end()) {
+              if (ids.size() >= 65535) throw XFDTDException("more than 65535 material classes");
+              id = static_cast<uint16_t>(ids.size());
+              ids.emplace(key, id);
+              I.table.resize(I.table.size() + 12);
+              classRow(key, I.table.data() + 12 * id);
+            } else {
+              id = it->second;
+            }
+            last = key;
+            last_id = id;
+            have_last = true;
+          }
+          I.lattice_class[(i * NY + j) * NZ + k] = id;
+        }
+  }
+  // Overrides create new classes: (base class, override tag) -> class.
+  std::map<std::pair<uint16_t, int>, uint16_t> override_ids;
+  auto overrideClass = [&](Index node, int tag, const std::function<void(double*)>& edit) {
+    const uint16_t base = I.lattice_class[node];
+    auto key = std::make_pair(base, tag);
+    auto it = override_ids.find(key);
+    if (it != override_ids.end()) {
+      I.lattice_class[node] = it->second;
+      return;
+    }
+    const std::size_t n_cls = I.table.size() / 12;
+    if (n_cls >= 65535) throw XFDTDException("more than 65535 material classes");
+    std::vector<double> row(I.table.begin() + 12 * base, I.table.begin() + 12 * base + 12);
+    edit(row.data());
+    I.table.insert(I.table.end(), row.begin(), row.end());
+    override_ids.emplace(key, static_cast<uint16_t>(n_cls));
+    I.lattice_class[node] = static_cast<uint16_t>(n_cls);
+  };
+  auto lat = [&](Index i, Index j, Index k) { return (i * NY + j) * NZ + k; };
+
+  // --------------------------------------------------- lumped current sources
+  struct CsH {
+    int comp;
+    int s[3], e[3];
+    std::vector<double> coff, wave;
+  };
+  std::vector<CsH> current_sources;
+  int override_tag = 0;
+  for (const auto& o : _objects) {
+    auto cs = std::dynamic_pointer_cast<CurrentSource>(o);
+    if (!cs) continue;
+    const Cube* cube = dynamic_cast<const Cube*>(cs->shape().get());
+    if (!cube) throw XFDTDException("CurrentSource needs a Cube");
+    const int ax = Axis::axisOf(cs->direction());
+    const int A = (ax + 1) % 3, B = (ax + 2) % 3;
+    Index gs[3], ge[3];
+    for (int a = 0; a < 3; ++a) {
+      gs[a] = nearestNode(I.e_node[a], cube->origin()(a));
+      ge[a] = nearestNode(I.e_node[a], cube->end()(a));
+    }
+    CsH h;
+    h.comp = ax;
+    for (int a = 0; a < 3; ++a) {  // LumpedElement::rangeX/Y/Z
+      h.s[a] = (int)gs[a];
+      h.e[a] = (int)(a == ax ? ge[a] : ge[a] + 1);
+    }
+    const Real r = cs->resistance();
+    const Index na = ge[A] - gs[A] + 1, nb = ge[B] - gs[B] + 1, nc = ge[ax] - gs[ax];
+    const Real res_factor = r * na * nb / nc;
+    Real amp = cs->waveform()->amplitude() / (na * nb);
+    if (Axis::negative(cs->direction())) amp *= -1;
+    for (int i = h.s[0]; i < h.e[0]; ++i)
+      for (int j = h.s[1]; j < h.e[1]; ++j)
+        for (int k = h.s[2]; k < h.e[2]; ++k) {
+          const int x[3] = {i, j, k};
+          auto dsize = [&](int a) { return a == ax ? I.e_size[a][x[a]] : I.h_size[a][x[a]]; };
+          const Real da = dsize(A), db = dsize(B), dc = dsize(ax);
+          const Real beta = (dt * dc) / (res_factor * da * db);
+          // Averaged eps / sigma of this E node: the class row's source values.
+          const Index node = lat(i, j, k);
+          const double* row = &I.table[12 * I.lattice_class[node]];
+          // Recover (2 eps + dt sigma) and (2 eps - dt sigma) from (ca, cb):
+          // cb = 2 dt / (2 eps + sigma dt), ca = (2 eps - dt sigma) / (2 eps + dt sigma).
+          const Real denom = 2 * dt / row[2 * ax + 1];
+          const Real numer = row[2 * ax] * denom;
+          const Real den_b = denom + beta;
+          const Real ca = (numer - beta) / den_b;
+          const Real cb = 2 * dt / den_b;
+          h.coff.push_back(-2 * dt / (den_b * (db * da)) * amp);
+          overrideClass(node, override_tag++, [&](double* rw) {
+            rw[2 * ax] = ca;
+            rw[2 * ax + 1] = cb;
+          });
+        }
+    std::vector<Real> h_time = linspace((0 + 0.5) * dt, (0 + _steps + 0.5) * dt, _steps);
+    cs->waveform()->init(h_time);
+    h.wave.assign(cs->waveform()->value().begin(), cs->waveform()->value().end());
+    current_sources.push_back(std::move(h));
+  }
+
+  // --------------------------------------------------------------- CPML
+  std::vector<Real> ke[3], kh[3];
+  for (int a = 0; a < 3; ++a) {
+    ke[a].assign(_n[a] + 1, 1.0);
+    kh[a].assign(_n[a], 1.0);
+  }
+  for (const auto& b : _boundaries) {
+    auto p = std::dynamic_pointer_cast<PML>(b);
+    if (!p) continue;
+    Impl::SlabH S;
+    S.axis = Axis::axisOf(p->direction());
+    S.neg = Axis::negative(p->direction());
+    S.n = std::abs(p->thickness());
+    const int m = S.axis;
+    if (S.n == 0) continue;
+    S.e_start = S.neg ? 1 : (int)_n[m] - S.n;
+    S.h_start = S.neg ? 0 : (int)_n[m] - S.n;
+    const int n = S.n;
+    std::vector<Real> gh(I.h_size[m].begin() + S.e_start, I.h_size[m].begin() + S.e_start + n);
+    std::vector<Real> ge(I.e_size[m].begin() + S.h_start, I.e_size[m].begin() + S.h_start + n);
+    auto rho = [&](const std::vector<Real>& size, Real frac) {
+      // PML::calculateRhoE / calculateRhoM (src/boundary/pml.cpp:564-606)
+      std::vector<Real> d(n);
+      d[0] = size[0] - frac * size[0];
+      Real sum = 0;
+      for (int i = 1; i < n; ++i) {
+        sum += size[i - 1];
+        d[i] = sum + (size[i] - frac * size[i]);
+      }
+      sum += size[n - 1];
+      if (S.neg) std::reverse(d.begin(), d.end());
+      for (auto& v : d) v /= sum;
+      return d;
+    };
+    const int order = p->order();
+    const Real e2m = MU_0 / EPSILON_0;
+    const Real smax_e =
+        p->sigmaRatio() * (order + 1) / (150 * PI * *std::min_element(gh.begin(), gh.end()));
+    const Real smax_m = p->sigmaRatio() * (order + 1) /
+                        (150 * PI * *std::min_element(ge.begin(), ge.end())) * e2m;
+    auto re = rho(gh, 0.75), rm = rho(ge, 0.25);
+    S.a_e.resize(n);
+    S.b_e.resize(n);
+    S.a_h.resize(n);
+    S.b_h.resize(n);
+    S.kappa_e.resize(n);
+    S.kappa_h.resize(n);
+    for (int l = 0; l < n; ++l) {
+      const Real sig_e = smax_e * std::pow(re[l], order);
+      const Real alp_e = p->alphaMin() + (p->alphaMax() - p->alphaMin()) * (1 - re[l]);
+      const Real kap_e = 1 + (p->kappaMax() - 1) * std::pow(re[l], order);
+      S.b_e[l] = std::exp((-dt / EPSILON_0) * (sig_e / kap_e + alp_e));
+      S.a_e[l] = (S.b_e[l] - 1) * sig_e / ((sig_e + kap_e * alp_e) * kap_e * gh[l]);
+      S.kappa_e[l] = kap_e;
+      const Real sig_m = smax_m * std::pow(rm[l], order);
+      const Real alp_m = (p->alphaMin() + (p->alphaMax() - p->alphaMin()) * (1 - rm[l])) * e2m;
+      const Real kap_h = 1 + (p->kappaMax() - 1) * std::pow(rm[l], order);
+      S.b_h[l] = std::exp((-dt / MU_0) * (sig_m / kap_h + alp_m));
+      S.a_h[l] = (S.b_h[l] - 1) * sig_m / ((sig_m + kap_h * alp_m) * kap_h * ge[l]);
+      S.kappa_h[l] = kap_h;
+      ke[m][S.e_start + l] = kap_e;
+      kh[m][S.h_start + l] = kap_h;
+    }
+    I.slabs.push_back(std::move(S));
+  }
+  for (int a = 0; a < 3; ++a) {
+    I.fe[a].resize(_n[a] + 1);
+    I.fh[a].resize(_n[a]);
+    for (Index x = 0; x <= _n[a]; ++x) I.fe[a][x] = 1.0 / (I.h_size[a][x] * ke[a][x]);
+    for (Index x = 0; x < _n[a]; ++x) I.fh[a][x] = 1.0 / (I.e_size[a][x] * kh[a][x]);
+  }
+
+  // ---------------------------------------------------------------- ADE
+  std::vector<const LinearDispersiveMaterial*> disp;
+  for (auto* m : I.painters)
+    if (m->dispersion()) disp.push_back(dynamic_cast<const LinearDispersiveMaterial*>(m));
+  int ade_kind = -1;
+  int num_pole = 0;
+  std::vector<double> ade_coef;
+  std::vector<uint8_t> ade_comp, ade_mat;
+  std::vector<int32_t> ade_node;
+  if (!disp.empty()) {
+    bool d_drude = false, d_debye = false, d_lor = false;
+    for (auto* m : disp) {
+      if (!m) throw XFDTDException("dispersive material is not a LinearDispersiveMaterial");
+      num_pole = std::max<int>(num_pole, (int)m->numPoles());
+      d_drude |= m->kind() == LinearDispersiveMaterial::Kind::Drude;
+      d_debye |= m->kind() == LinearDispersiveMaterial::Kind::Debye;
+      d_lor |= m->kind() == LinearDispersiveMaterial::Kind::MLorentz;
+    }
+    // Simulation::buildDispersiveSpace storage choice (simulation.cpp:800-818)
+    ade_kind = (d_drude && !d_debye && !d_lor) ? 1 : (!d_drude && d_debye && !d_lor) ? 2 : 0;
+    // Per painter: ADE material slot, coefficients, overwritten (ca, cb).
+    std::vector<int> slot(I.painters.size(), -1);
+    std::vector<std::array<double, 2>> e_coef;
+    const int stride = 2 + 7 * num_pole;
+    for (std::size_t pi = 0; pi < I.painters.size(); ++pi) {
+      auto* m = dynamic_cast<const LinearDispersiveMaterial*>(I.painters[pi]);
+      if (!m || !m->dispersion()) continue;
+      if (slot.size() > 0 && (int)e_coef.size() >= 256)
+        throw XFDTDException("more than 256 dispersive objects");
+      slot[pi] = (int)e_coef.size();
+      std::vector<double> c(stride, 0.0);
+      const Real eps_inf = m->epsilonInf();
+      const Real sigma = m->emProperty().sigmaE();
+      const int P = (int)m->numPoles();
+      if (ade_kind == 0) {
+        // MLorentzADEMethodStorage::correctCoeff (m_lor_ade_method.cpp:66-159)
+        std::vector<Real> a(P), bb(P), cc(P), d(P), e(P), f(P);
+        for (int p = 0; p < P; ++p) {
+          const auto& q = m->pole(p);
+          const Real a0 = q[0], a1 = q[1], b0 = q[2], b1 = q[3], b2 = q[4];
+          a[p] = (a1 * EPSILON_0 / (dt * dt)) + (0.5 * a0 * EPSILON_0 / dt);
+          bb[p] = (-2 * a1 * EPSILON_0) / (dt * dt);
+          cc[p] = (a1 * EPSILON_0 / (dt * dt)) - (0.5 * a0 * EPSILON_0 / dt);
+          d[p] = (2 * b2 / (dt * dt)) - b0;
+          e[p] = (-b2 / (dt * dt)) + (b1 / (2 * dt));
+          f[p] = (b2 / (dt * dt)) + (b1 / (2 * dt));
+        }
+        Real sum_a = 0, sum_b = 0, sum_c = 0;
+        for (int p = 0; p < P; ++p) sum_a += a[p] / f[p];
+        for (int p = 0; p < P; ++p) sum_b += bb[p] / f[p];
+        for (int p = 0; p < P; ++p) sum_c += cc[p] / f[p];
+        const Real temp = (eps_inf * EPSILON_0) / dt + 0.5 * sum_a + 0.5 * sigma;
+        c[0] = -1 / temp;
+        c[1] = -0.5 * sum_c / temp;
+        for (int p = 0; p < P; ++p) {
+          double* pc = &c[2 + 7 * p];
+          pc[0] = d[p] / f[p];
+          pc[1] = e[p] / f[p];
+          pc[2] = a[p] / f[p];
+          pc[3] = bb[p] / f[p];
+          pc[4] = cc[p] / f[p];
+          pc[5] = 0.5 * (1 + d[p] / f[p]);
+          pc[6] = 0.5 * (e[p] / f[p]);
+        }
+        e_coef.push_back({((eps_inf * EPSILON_0) / dt - 0.5 * sum_b - 0.5 * sigma) / temp,
+                          1 / temp});
+      } else if (ade_kind == 1) {
+        // DrudeADEMethodStorage::correctCoeff (drude_ade_method.cpp:61-133)
+        Real sum_beta = 0;
+        std::vector<Real> kk(P), beta(P);
+        for (int p = 0; p < P; ++p) {
+          const Real wp = m->native(p)[0], g = m->native(p)[1];
+          kk[p] = (1 - g * dt / 2) / (1 + g * dt / 2);
+          beta[p] = (EPSILON_0 * wp * wp * dt / 2) / (1 + g * dt / 2);
+        }
+        for (int p = 0; p < P; ++p) sum_beta += beta[p];
+        const Real a = (2 * EPSILON_0 * eps_inf - dt * sum_beta - dt * sigma) /
+                       (2 * EPSILON_0 * eps_inf - dt * sum_beta + dt * sigma);
+        const Real b = (2 * dt) / (2 * EPSILON_0 * eps_inf - dt * sum_beta + dt * sigma);
+        c[0] = -b;
+        for (int p = 0; p < P; ++p) {
+          c[2 + 7 * p + 0] = kk[p];
+          c[2 + 7 * p + 3] = beta[p];
+          c[2 + 7 * p + 5] = 0.5 * (1 + kk[p]);
+        }
+        e_coef.push_back({a, b});
+      } else {
+        // DebyeADEMethodStorage::correctCoeff (debye_ade_method.cpp:47-122)
+        Real sum_beta = 0;
+        std::vector<Real> kk(P), beta(P);
+        for (int p = 0; p < P; ++p) {
+          const Real es = m->native(p)[0], tau = m->native(p)[1];
+          kk[p] = (2 * tau - dt) / (2 * tau + dt);
+          beta[p] = (2 * EPSILON_0 * (es - eps_inf) * dt) / (2 * tau + dt);
+        }
+        for (int p = 0; p < P; ++p) sum_beta += beta[p];
+        const Real a = (2 * EPSILON_0 * eps_inf + sum_beta - dt * sigma) /
+                       (2 * EPSILON_0 * eps_inf + sum_beta + dt * sigma);
+        const Real b = (2 * dt) / (2 * EPSILON_0 * eps_inf + sum_beta + dt * sigma);
+        c[0] = -b;
+        for (int p = 0; p < P; ++p) {
+          c[2 + 7 * p + 0] = kk[p];
+          c[2 + 7 * p + 3] = beta[p] / dt;
+          c[2 + 7 * p + 5] = 0.5 * (1 + kk[p]);
+        }
+        e_coef.push_back({a, b});
+      }
+      ade_coef.insert(ade_coef.end(), c.begin(), c.end());
+    }
+    // CPML E layers per axis: dispersive cells there are not supported.
+    std::vector<char> in_pml[3];
+    for (int a = 0; a < 3; ++a) in_pml[a].assign(_n[a] + 1, 0);
+    for (const auto& S : I.slabs)
+      for (int l = 0; l < S.n; ++l) in_pml[S.axis][S.e_start + l] = 1;
+    for (Index i = 0; i < nx; ++i)
+      for (Index j = 0; j < ny; ++j)
+        for (Index k = 0; k < nz; ++k) {
+          const uint16_t pm = I.cell[(i * ny + j) * nz + k];
+          if (slot[pm] < 0) continue;
+          if (in_pml[0][i] || in_pml[1][j] || in_pml[2][k])
+            throw XFDTDException(
+                "a dispersive object reaches into the CPML; this engine keeps ADE media out of "
+                "the absorbing layers");
+          const auto& ec = e_coef[slot[pm]];
+          // Object::handleDispersion -> correctCoeff overwrites Ex, Ey, Ez at (i,j,k).
+          overrideClass(lat(i, j, k), 1000000 + slot[pm], [&](double* rw) {
+            for (int c = 0; c < 3; ++c) {
+              rw[2 * c] = ec[0];
+              rw[2 * c + 1] = ec[1];
+            }
+          });
+          const Index x[3] = {i, j, k};
+          for (int c = 0; c < 3; ++c) {
+            if (x[(c + 1) % 3] < 1 || x[(c + 2) % 3] < 1) continue;  // E update ranges
+            ade_comp.push_back((uint8_t)c);
+            ade_node.push_back((int32_t)i);
+            ade_node.push_back((int32_t)j);
+            ade_node.push_back((int32_t)k);
+            ade_mat.push_back((uint8_t)slot[pm]);
+          }
+        }
+  }
+
+  if (!_use_engine) {
+    I.initialised = true;
+    return;
+  }
+  // ------------------------------------------------------------- engine
+  xfd_grid_desc g{};
+  g.nx = (int32_t)nx;
+  g.ny = (int32_t)ny;
+  g.nz = (int32_t)nz;
+  g.precision = _precision == Precision::FP64 ? XFD_FP64 : XFD_FP32;
+  g.n_steps = (int64_t)_steps;
+  g.dt = dt;
+  g.device = 0;
+  if (xfd_create(&g, &_engine) != XFD_OK)
+    throw XFDTDException(std::string("xfd_create failed: ") + xfd_last_error(nullptr));
+  xfd_engine* E = _engine;
+  checkStatus(E, xfd_set_material_classes(E, I.table.data(), (int32_t)(I.table.size() / 12),
+                                          I.lattice_class.data()),
+              "xfd_set_material_classes");
+  const double* fe[3] = {I.fe[0].data(), I.fe[1].data(), I.fe[2].data()};
+  const double* fh[3] = {I.fh[0].data(), I.fh[1].data(), I.fh[2].data()};
+  checkStatus(E, xfd_set_curl_factors(E, fe, fh), "xfd_set_curl_factors");
+  for (const auto& S : I.slabs) {
+    xfd_cpml_slab s{S.axis, S.neg, S.n, S.e_start, S.h_start,
+                    S.a_e.data(), S.b_e.data(), S.a_h.data(), S.b_h.data()};
+    checkStatus(E, xfd_add_cpml(E, &s), "xfd_add_cpml");
+  }
+  for (const auto& h : current_sources)
+    checkStatus(E, xfd_add_current_source(E, h.comp, h.s, h.e, h.coff.data(), h.wave.data()),
+                "xfd_add_current_source");
+  if (ade_kind >= 0) {
+    xfd_ade_desc a{ade_kind, num_pole, (int32_t)(ade_coef.size() / (2 + 7 * num_pole)),
+                   ade_coef.data(), (int64_t)ade_comp.size(), ade_comp.data(), ade_node.data(),
+                   ade_mat.data()};
+    checkStatus(E, xfd_set_ade(E, &a), "xfd_set_ade");
+  }
+  setupTfsf(E);
+  setupNf2ff(E);
+  // Movie monitors (FieldMonitor box with the +1 origin shift at index 0,
+  // src/monitor/field_monitor.cpp:17-67).
+  for (const auto& mon : _monitors) {
+    auto mv = std::dynamic_pointer_cast<MovieMonitor>(mon);
+    if (!mv) continue;
+    const Shape* sh = mv->frame()->shape().get();
+    auto wc = sh->wrappedCube();
+    Impl::MovieH h{mv.get(), -1, {}, {}};
+    for (int a = 0; a < 3; ++a) {
+      int s = (int)nearestNode(I.e_node[a], wc->origin()(a));
+      int e = (int)nearestNode(I.e_node[a], wc->end()(a));
+      int size = e - s;
+      if (s == 0) {
+        s += 1;
+        size -= 1;
+      }
+      h.s[a] = s;
+      h.e[a] = s + size;
+    }
+    checkStatus(E, xfd_add_movie(E, static_cast<int32_t>(mv->frame()->field()), h.s, h.e,
+                                 (int32_t)mv->frameInterval(), &h.id),
+                "xfd_add_movie");
+    mv->setFrameShape({(std::size_t)(h.e[0] - h.s[0]), (std::size_t)(h.e[1] - h.s[1]),
+                       (std::size_t)(h.e[2] - h.s[2])});
+    I.movies.push_back(h);
+  }
+  I.initialised = true;
+}
+
+void Simulation::advance(Index n) {
+  if (!_impl->initialised || !_engine) throw XFDTDException("Simulation not initialised");
+  checkStatus(_engine, xfd_run(_engine, (int64_t)n), "xfd_run");
+}
+
+void Simulation::finish() {
+  if (!_engine) throw XFDTDException("Simulation not initialised");
+  Impl& I = *_impl;
+  checkStatus(_engine, xfd_sync(_engine), "xfd_sync");
+  // Fields back into the host EMF.
+  const Index n[3] = {_n[0], _n[1], _n[2]};
+  for (int c = 0; c < 6; ++c) {
+    Index s[3];
+    for (int d = 0; d < 3; ++d) {
+      const bool along = (d == c % 3);
+      s[d] = (c < 3) ? (along ? n[d] : n[d] + 1) : (along ? n[d] + 1 : n[d]);
+    }
+    _emf._f[c] = Array3D<Real>(s[0], s[1], s[2]);
+    if (_precision == Precision::FP64) {
+      checkStatus(_engine, xfd_download_field(_engine, c, _emf._f[c].data()), "download");
+    } else {
+      std::vector<float> tmp(_emf._f[c].size());
+      checkStatus(_engine, xfd_download_field(_engine, c, tmp.data()), "download");
+      std::copy(tmp.begin(), tmp.end(), _emf._f[c].data());
+    }
+  }
+  for (auto& h : I.movies) {
+    int64_t frames = 0;
+    checkStatus(_engine, xfd_get_movie_frames(_engine, h.id, nullptr, 0, &frames), "movie");
+    const std::size_t per = (std::size_t)(h.e[0] - h.s[0]) * (h.e[1] - h.s[1]) * (h.e[2] - h.s[2]);
+    const std::size_t w = _precision == Precision::FP64 ? 8 : 4;
+    std::vector<char> buf((std::size_t)frames * per * w);
+    checkStatus(_engine, xfd_get_movie_frames(_engine, h.id, buf.data(), (int64_t)buf.size(),
+                                              &frames),
+                "movie");
+    auto& out = h.mon->framesMutable();
+    out.assign((std::size_t)frames, std::vector<Real>(per));
+    for (int64_t f = 0; f < frames; ++f)
+      for (std::size_t q = 0; q < per; ++q)
+        out[f][q] = (w == 8) ? reinterpret_cast<double*>(buf.data())[f * per + q]
+                             : reinterpret_cast<float*>(buf.data())[f * per + q];
+  }
+  if (I.nf2ff) {
+    int64_t cnt = 0;
+    checkStatus(_engine, xfd_get_nf2ff(_engine, nullptr, 0, &cnt), "nf2ff");
+    std::vector<double> raw(2 * (std::size_t)cnt);
+    checkStatus(_engine, xfd_get_nf2ff(_engine, raw.data(), cnt, &cnt), "nf2ff");
+    auto& acc = I.nf2ff->surfaceCurrentsMutable();
+    acc.resize((std::size_t)cnt);
+    for (int64_t q = 0; q < cnt; ++q) acc[q] = {raw[2 * q], raw[2 * q + 1]};
+  }
+}
+
+std::vector<std::vector<Real>> Simulation::coefficientArrays() const {
+  const Impl& I = *_impl;
+  if (!I.initialised) throw XFDTDException("Simulation not initialised");
+  const Index n[3] = {_n[0], _n[1], _n[2]};
+  const Index NY = n[1] + 1, NZ = n[2] + 1;
+  std::vector<std::vector<Real>> out;
+  for (int h = 0; h < 2; ++h)
+    for (int c = 0; c < 3; ++c) {
+      Index s[3];
+      for (int d = 0; d < 3; ++d) {
+        const bool along = (d == c);
+        s[d] = (h == 0) ? (along ? n[d] : n[d] + 1) : (along ? n[d] + 1 : n[d]);
+      }
+      const int ta = (c + 1) % 3, tb = (c + 2) % 3;
+      std::vector<Real> c0(s[0] * s[1] * s[2]), ca(c0.size()), cb(c0.size());
+      for (Index i = 0; i < s[0]; ++i)
+        for (Index j = 0; j < s[1]; ++j)
+          for (Index k = 0; k < s[2]; ++k) {
+            const Index x[3] = {i, j, k};
+            const double* row = &I.table[12 * I.lattice_class[(i * NY + j) * NZ + k]];
+            const Real a = row[6 * h + 2 * c], b = row[6 * h + 2 * c + 1];
+            const Index q = (i * s[1] + j) * s[2] + k;
+            c0[q] = a;
+            if (h == 0) {  // ceh_a = -cb fe_b, ceh_b = cb fe_a
+              ca[q] = -b * I.fe[tb][x[tb]];
+              cb[q] = b * I.fe[ta][x[ta]];
+            } else {       // che_a = cb fh_b, che_b = -cb fh_a
+              ca[q] = b * I.fh[tb][x[tb]];
+              cb[q] = -b * I.fh[ta][x[ta]];
+            }
+          }
+      out.push_back(std::move(c0));
+      out.push_back(std::move(ca));
+      out.push_back(std::move(cb));
+    }
+  return out;
+}
+
+void Simulation::setupTfsf(xfd_engine* E) {
+  std::shared_ptr<TFSF3D> t;
+  for (const auto& s : _sources) {
+    if (auto p = std::dynamic_pointer_cast<TFSF3D>(s)) {
+      if (t) throw XFDTDException("only one TFSF3D source is supported");
+      t = p;
+    } else {
+      throw XFDTDException("unsupported waveform source (TFSF3D only)");
+    }
+  }
+  if (!t) return;
+  const Real dt = _dt;
+  const Index org[3] = {t->x(), t->y(), t->z()};
+  Index size[3];
+  for (int a = 0; a < 3; ++a) {
+    if (2 * org[a] >= _n[a]) throw XFDTDException("TFSF box is empty");
+    size[a] = _n[a] - 2 * org[a];
+  }
+  // TFSF ctor / initTransform (src/waveform_source/tfsf.cpp:14-30, 231-254)
+  const Real st = std::sin(t->theta()), ct = std::cos(t->theta());
+  const Real sp = std::sin(t->phi()), cp = std::cos(t->phi());
+  const Real ss = std::sin(t->psi()), cs = std::cos(t->psi());
+  const Real k[3] = {st * cp, st * sp, ct};
+  const Real va[3] = {-sp, ct * cp, st * cp}, vb[3] = {cp, ct * sp, st * sp},
+             vc[3] = {0, -st, ct}, ke[3] = {ss, cs, 0};
+  auto dot = [](const Real* x, const Real* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+  const Real te[3] = {dot(va, ke), dot(vb, ke), dot(vc, ke)};
+  const Real th[3] = {k[1] * te[2] - k[2] * te[1], k[2] * te[0] - k[0] * te[2],
+                      k[0] * te[1] - k[1] * te[0]};
+  // TFSF::defaultInit (tfsf.cpp:118-175)
+  const Real ratio = 1 / std::sqrt(std::pow(st, 4) * (std::pow(cp, 4) + std::pow(sp, 4)) +
+                                   std::pow(ct, 4));
+  const auto aux = static_cast<Index>(
+      std::ceil(ratio * (std::sqrt(std::pow(size[0], 2) + std::pow(size[1], 2) +
+                                   std::pow(size[2], 2)))) + 4 + 1);
+  // calculateProjection / calculateInjectPostion (tfsf.cpp:256-340)
+  std::vector<Real> p_int[3], p_half[3];
+  for (int a = 0; a < 3; ++a) {
+    const Real inj = k[a] >= 0 ? (Real)org[a] : (Real)(org[a] + size[a]);
+    const Real inc = inj - (2 * k[a] / ratio);
+    for (Index i = 0; i < size[a] + 1; ++i)
+      p_int[a].push_back(((Real)i + (Real)org[a] - inc) * k[a] * ratio);
+    for (Index i = 0; i < size[a] + 2; ++i)
+      p_half[a].push_back(((Real)i + (Real)org[a] - inc - 0.5) * k[a] * ratio);
+  }
+  const Real scaled_dl = _dl[2] / ratio;
+  const Real ceie = 1, chih = 1;
+  const Real ceih = -(dt / (EPSILON_0 * scaled_dl));
+  const Real chie = -(dt / (MU_0 * scaled_dl));
+  const Real abc0 = (C_0 * dt - scaled_dl) / (C_0 * dt + scaled_dl);
+  const Real abc1 = 2 * scaled_dl / (C_0 * dt + scaled_dl);
+  // initTimeDependentVariable (tfsf.cpp:36-78): source sampled at eTime - dt.
+  const Index nt = _steps;
+  std::vector<Real> e_time = linspace((0 + 1) * dt, (0 + nt) * dt, nt);
+  for (auto& v : e_time) v -= dt;
+  t->waveform()->init(e_time);
+  const auto& src = t->waveform()->value();
+  const Index nl = aux - 1;
+  std::vector<Real> e_inc(nt * aux, 0.0), h_inc(nt * nl, 0.0);
+  auto E_ = [&](Index tt, Index l) -> Real& { return e_inc[tt * aux + l]; };
+  auto H_ = [&](Index tt, Index l) -> Real& { return h_inc[tt * nl + l]; };
+  if (nt > 0) {
+    E_(0, 0) = src[0];
+    for (Index l = 1; l < nl; ++l) H_(0, l) = chih * H_(0, l) + chie * (E_(0, l + 1) - E_(0, l));
+  }
+  for (Index tt = 1; tt < nt; ++tt) {
+    for (Index l = 1; l < nl; ++l) {
+      E_(tt, 0) = src[tt];
+      E_(tt, l) = ceie * E_(tt - 1, l) + ceih * (H_(tt - 1, l) - H_(tt - 1, l - 1));
+    }
+    const Real ep2 = (tt < 2) ? 0.0 : E_(tt - 2, nl - 1);
+    const Real el2 = (tt < 2) ? 0.0 : E_(tt - 2, nl);
+    E_(tt, nl) = -ep2 + abc0 * (E_(tt, nl - 1) + el2) + abc1 * (E_(tt - 1, nl) + E_(tt - 1, nl - 1));
+    for (Index l = 0; l < nl; ++l) H_(tt, l) = chih * H_(tt - 1, l) + chie * (E_(tt, l + 1) - E_(tt, l));
+  }
+  xfd_tfsf_desc d{};
+  for (int a = 0; a < 3; ++a) {
+    d.box_s[a] = (int32_t)org[a];
+    d.box_e[a] = (int32_t)(org[a] + size[a]);
+    d.p_int[a] = p_int[a].data();
+    d.p_half[a] = p_half[a].data();
+    d.ca[a] = dt / (EPSILON_0 * _dl[a]);  // TFSF::cax..caz (tfsf.cpp:177-205)
+    d.cb[a] = dt / (MU_0 * _dl[a]);
+    d.te[a] = te[a];
+    d.th[a] = th[a];
+  }
+  d.aux = (int32_t)aux;
+  d.e_inc = e_inc.data();
+  d.h_inc = h_inc.data();
+  checkStatus(E, xfd_set_tfsf(E, &d), "xfd_set_tfsf");
+}
+
+void Simulation::setupNf2ff(xfd_engine* E) {
+  if (_nffts.empty()) return;
+  if (_nffts.size() > 1) throw XFDTDException("one NFFFTFrequencyDomain per simulation");
+  auto& nf = *_nffts[0];
+  _impl->nf2ff = &nf;
+  const auto d = nf.distance();
+  // NFFFT::initGlobal / makeNodeAxisTask (src/nffft/nffft.cpp:88-245), one domain.
+  xfd_nf2ff_desc desc{};
+  for (int face = 0; face < 6; ++face) {
+    const int m = face / 2;
+    const bool positive = face % 2;
+    int s[3], e[3];
+    for (int a = 0; a < 3; ++a) {
+      s[a] = (int)d[a];
+      e[a] = (int)(_n[a] - d[a]);
+    }
+    const int c = positive ? e[m] : s[m];
+    bool valid = positive ? (c < (int)_n[m]) : (c > 1);
+    s[m] = c;
+    e[m] = c + 1;
+    for (int a = 0; a < 3; ++a) {
+      if (a == m) continue;
+      if (s[a] <= 0) s[a] = 1;
+      if (e[a] >= (int)_n[a]) e[a] = (int)_n[a] - 1;
+      if (e[a] <= s[a]) valid = false;
+    }
+    for (int a = 0; a < 3; ++a) {
+      desc.task_s[face][a] = valid ? s[a] : 0;
+      desc.task_e[face][a] = valid ? e[a] : 0;
+      nf.faces[face][a] = desc.task_s[face][a];
+      nf.faces[face][3 + a] = desc.task_e[face][a];
+    }
+  }
+  const auto& freqs = nf.frequencies();
+  const Index nt = _steps;
+  const Real dt = _dt;
+  std::vector<double> te(freqs.size() * nt * 2), th(freqs.size() * nt * 2);
+  for (Index f = 0; f < freqs.size(); ++f)
+    for (Index t = 0; t < nt; ++t) {
+      // dt * exp(-j 2 pi f (t+1) dt), dt * exp(-j 2 pi f (t+1/2) dt)
+      const Real ae = (-2.0 * PI) * ((freqs[f] * (Real)(t + 1)) * dt);
+      const Real ah = (-2.0 * PI) * ((freqs[f] * ((Real)t + 0.5)) * dt);
+      te[(f * nt + t) * 2] = dt * std::cos(ae);
+      te[(f * nt + t) * 2 + 1] = dt * std::sin(ae);
+      th[(f * nt + t) * 2] = dt * std::cos(ah);
+      th[(f * nt + t) * 2 + 1] = dt * std::sin(ah);
+    }
+  desc.n_freq = (int32_t)freqs.size();
+  desc.batch = 64;
+  desc.te = te.data();
+  desc.th = th.data();
+  // The reference adds each step's term once per frequency plane
+  // (nffft_frequency_domain.cpp:45-53).
+  desc.scale = (double)freqs.size();
+  checkStatus(E, xfd_set_nf2ff(E, &desc), "xfd_set_nf2ff");
+}
+
+}  // namespace xfdtd

@@ -1,0 +1,158 @@
+"""ctypes binding of the host library's C entry points (include/xfdtd_host.h).
+
+A :class:`SceneRun` is one ``xfdtd::Simulation`` built from a
+:class:`xfdtd_core_b200.scene.Scene` by the C++20 host library, which does the
+FP64 set-up and drives the CUDA engine.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from . import build as _build
+from . import engine as _engine
+
+NO_ENGINE = 0x100
+_dp = ctypes.POINTER(ctypes.c_double)
+_LIB = None
+
+
+class HostError(RuntimeError):
+    pass
+
+
+def load():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(_build.HOST_LIB):
+        _build.build_engine()
+        _build.build_host()
+    L = ctypes.CDLL(_build.HOST_LIB)
+    vp = ctypes.c_void_p
+    i32, i64 = ctypes.c_int32, ctypes.c_int64
+    sig = {
+        "xfdtd_scene_open": ([ctypes.c_char_p, i32, ctypes.POINTER(vp)], ctypes.c_int),
+        "xfdtd_scene_close": ([vp], None),
+        "xfdtd_host_last_error": ([], ctypes.c_char_p),
+        "xfdtd_scene_engine": ([vp], vp),
+        "xfdtd_scene_info": ([vp, i32 * 3, ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(i64)], ctypes.c_int),
+        "xfdtd_scene_advance": ([vp, i64], ctypes.c_int),
+        "xfdtd_scene_finish": ([vp], ctypes.c_int),
+        "xfdtd_scene_coefficients": ([vp, _dp * 18], ctypes.c_int),
+        "xfdtd_scene_field": ([vp, i32, _dp], ctypes.c_int),
+        "xfdtd_scene_movie": ([vp, i32, _dp, i64, ctypes.POINTER(i64), i32 * 3], ctypes.c_int),
+        "xfdtd_scene_nf2ff": ([vp, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "xfdtd_scene_write_outputs": ([vp, ctypes.c_char_p], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _LIB = L
+    return L
+
+
+def exported_symbols() -> List[str]:
+    return ["xfdtd_scene_open", "xfdtd_scene_close", "xfdtd_host_last_error",
+            "xfdtd_scene_engine", "xfdtd_scene_info", "xfdtd_scene_advance",
+            "xfdtd_scene_finish", "xfdtd_scene_coefficients", "xfdtd_scene_field",
+            "xfdtd_scene_movie", "xfdtd_scene_nf2ff", "xfdtd_scene_write_outputs"]
+
+
+class SceneRun:
+    """A Simulation built from a scene by the C++ host library."""
+
+    def __init__(self, scene, precision: int = 0, engine: bool = True):
+        self.L = load()
+        self.scene = scene
+        fd, self.path = tempfile.mkstemp(suffix=".scene")
+        with os.fdopen(fd, "w") as fh:
+            fh.write(scene.to_text())
+        h = ctypes.c_void_p()
+        flags = precision | (0 if engine else NO_ENGINE)
+        st = self.L.xfdtd_scene_open(self.path.encode(), flags, ctypes.byref(h))
+        os.unlink(self.path)
+        if st != 0:
+            raise HostError(self.L.xfdtd_host_last_error().decode())
+        self.h = h
+        n = (ctypes.c_int32 * 3)()
+        dt = ctypes.c_double()
+        steps = ctypes.c_int64()
+        self._check(self.L.xfdtd_scene_info(self.h, n, ctypes.byref(dt), ctypes.byref(steps)))
+        self.n = tuple(n)
+        self.dt = dt.value
+        self.steps = steps.value
+
+    def _check(self, st):
+        if st != 0:
+            raise HostError(self.L.xfdtd_host_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.xfdtd_scene_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def engine_handle(self) -> int:
+        return int(self.L.xfdtd_scene_engine(self.h) or 0)
+
+    def advance(self, n: int):
+        self._check(self.L.xfdtd_scene_advance(self.h, int(n)))
+
+    def finish(self):
+        self._check(self.L.xfdtd_scene_finish(self.h))
+
+    def run(self, n: Optional[int] = None):
+        self.advance(self.steps if n is None else n)
+        self.finish()
+
+    def coefficients(self) -> List[np.ndarray]:
+        """cexe cexhy cexhz ceye ceyhz ceyhx ceze cezhx cezhy chxh chxey chxez
+        chyh chyez chyex chzh chzex chzey, reference shapes."""
+        shapes = []
+        for c in range(6):
+            s = _engine.comp_shape(self.n, c)
+            shapes += [s, s, s]
+        arrs = [np.empty(s) for s in shapes]
+        ptrs = (_dp * 18)(*[a.ctypes.data_as(_dp) for a in arrs])
+        self._check(self.L.xfdtd_scene_coefficients(self.h, ptrs))
+        return arrs
+
+    def field(self, c: int) -> np.ndarray:
+        a = np.empty(_engine.comp_shape(self.n, c))
+        self._check(self.L.xfdtd_scene_field(self.h, c, a.ctypes.data_as(_dp)))
+        return a
+
+    def fields(self) -> List[np.ndarray]:
+        return [self.field(c) for c in range(6)]
+
+    def movie(self, index: int = 0) -> np.ndarray:
+        nfr = ctypes.c_int64()
+        shp = (ctypes.c_int32 * 3)()
+        self._check(self.L.xfdtd_scene_movie(self.h, index, None, 0, ctypes.byref(nfr), shp))
+        out = np.empty((nfr.value, *tuple(shp)))
+        self._check(self.L.xfdtd_scene_movie(self.h, index, out.ctypes.data_as(_dp), out.size,
+                                             ctypes.byref(nfr), shp))
+        return out
+
+    def nf2ff(self) -> np.ndarray:
+        cnt = ctypes.c_int64()
+        self._check(self.L.xfdtd_scene_nf2ff(self.h, None, 0, ctypes.byref(cnt)))
+        out = np.empty(2 * cnt.value)
+        self._check(self.L.xfdtd_scene_nf2ff(self.h, out.ctypes.data_as(_dp), cnt.value,
+                                             ctypes.byref(cnt)))
+        return out[0::2] + 1j * out[1::2]
+
+    def write_outputs(self, directory: str):
+        self._check(self.L.xfdtd_scene_write_outputs(self.h, directory.encode()))
