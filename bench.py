@@ -1,0 +1,390 @@
+"""Benchmark: Gcell-updates/s of the XFDTD 3-D time step on B200.
+
+Workload (one "step" = one FDTD time step of this scene): the dielectric-boxes
+scene -- 256^3 cells including a 12-cell CPML (order 3, kappa_max 5,
+alpha_max 0.05), 64 random dielectric boxes (numpy default_rng(0)), a
+z-directed one-cell current source with a 30 GHz cosine-modulated Gaussian,
+CFL 0.99.  The headline `value` is the FP32 form; the FP64 plain form is
+timed in the same run and reported under "forms".  Inputs (fields: 6 x 257^3
+values) are larger than the 126 MB L2, so no flush is needed between steps.
+
+Lines (one JSON line on rank 0):
+  ours:       python bench.py [--gpus N --steps K --warmup W]
+  reference:  python bench.py --impl reference ...  (the CPU restatement of
+              the reference's std::thread FP64 path, all host threads)
+
+Under torchrun each rank runs its own replica of the scene (the path's
+multi-GPU form in this round is replicas: no data-path collective), the
+timed region is bracketed by barriers, and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-updates/s"
+UNIT = "Gcell/s"
+WORKLOAD = "dielectric_boxes_256^3_cpml12_64boxes_dipole"
+
+
+def workload_scene(steps: int, n: int = 256):
+    from xfdtd_core_b200 import scene as S
+    return S.dielectric_boxes(n=n, pml=12, dl=1e-3, n_boxes=64, steps=steps, seed=0)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import torch
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ GPU timing
+def time_engine_steps(eng_handle: int, steps: int, warmup: int, pg, device: int, sampler=None):
+    """Runs `warmup` untimed then `steps` timed steps; CUDA events on the
+    engine's stream; returns milliseconds (max over ranks)."""
+    import torch
+    from xfdtd_core_b200 import engine as E
+    L = E.load()
+    h = ctypes_handle(eng_handle)
+    _ck(L, h, L.xfd_run(h, warmup))
+    _ck(L, h, L.xfd_sync(h))
+    stream = torch.cuda.ExternalStream(int(L.xfd_stream(h)), device=device)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    start.record(stream)
+    _ck(L, h, L.xfd_run(h, steps))
+    end.record(stream)
+    _ck(L, h, L.xfd_sync(h))
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    barrier(pg)
+    ms = start.elapsed_time(end)
+    return max_over_ranks(pg, ms), clocks
+
+
+def ctypes_handle(h: int):
+    import ctypes
+    return ctypes.c_void_p(h)
+
+
+def _ck(L, h, st):
+    if st != 0:
+        raise RuntimeError(L.xfd_last_error(h).decode())
+
+
+def run_e2e(scene, steps: int, warmup: int, pg, device: int):
+    """End to end through the C ABI with host buffers: initial fields uploaded
+    from pinned host memory, `steps` steps with a movie monitor whose frame (the
+    Ez z-plane through the source) is copied to pinned host memory every step on
+    the engine's side stream, final fields read back -- all inside the timed
+    region (CUDA events on the engine stream; max over ranks)."""
+    import ctypes
+    import torch
+    from xfdtd_core_b200 import engine as E
+    from xfdtd_core_b200.host import SceneRun
+    run = SceneRun(scene, precision=1)
+    L = E.load()
+    h = ctypes.c_void_p(run.engine_handle())
+    nx, ny, nz = run.n
+    mid = ctypes.c_int32()
+    _ck(L, h, L.xfd_add_movie(h, 2, (ctypes.c_int32 * 3)(0, 0, nz // 2),
+                              (ctypes.c_int32 * 3)(nx + 1, ny + 1, nz // 2 + 1), 1,
+                              ctypes.byref(mid)))
+    _ck(L, h, L.xfd_run(h, warmup))
+    _ck(L, h, L.xfd_sync(h))
+    shapes = [E.comp_shape(run.n, c) for c in range(6)]
+    host_in = [torch.zeros(s, dtype=torch.float32).pin_memory() for s in shapes]
+    host_out = [torch.empty(s, dtype=torch.float32).pin_memory() for s in shapes]
+    ptr_in = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in host_in])
+    ptr_out = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in host_out])
+    stream = torch.cuda.ExternalStream(int(L.xfd_stream(h)), device=device)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    nfr = ctypes.c_int64()
+    barrier(pg)
+    torch.cuda.synchronize()
+    start.record(stream)
+    _ck(L, h, L.xfd_upload_fields(h, ptr_in))
+    _ck(L, h, L.xfd_run(h, steps))
+    _ck(L, h, L.xfd_sync(h))
+    _ck(L, h, L.xfd_get_movie_frames(h, mid.value, None, 0, ctypes.byref(nfr)))
+    _ck(L, h, L.xfd_download_fields(h, ptr_out))
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    elapsed = start.elapsed_time(end) / 1e3
+    frame_bytes = (nx + 1) * (ny + 1) * 4
+    field_bytes = sum(int(np.prod(s)) * 4 for s in shapes)
+    run.close()
+    return max_over_ranks(pg, elapsed), field_bytes, field_bytes + steps * frame_bytes
+
+
+def scene_n(scene) -> int:
+    half = scene.objects[0].shape.size[0] / 2
+    return int(round(2 * half / scene.dl[0])) + 2 * scene.pmls[0].thickness
+
+
+# ------------------------------------------------------------- CPU oracle
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def time_oracle(scene, budget_s: float, max_steps: int):
+    """The oracle (CPU restatement of the reference's FP64 std::thread path,
+    OpenMP over all host threads) on the same scene: one warm-up step, then
+    as many steps as fit in `budget_s` (at most max_steps)."""
+    from oracle.reference_model import RefSimulation, lib
+    threads = cpu_threads()
+    r = RefSimulation(scene, threads=threads)
+    lib().orc_set_num_threads(threads)
+    r.run(1)
+    t0 = time.perf_counter()
+    r.run(1)
+    one = time.perf_counter() - t0
+    k = int(max(1, min(max_steps, budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    r.run(k)
+    el = time.perf_counter() - t0
+    cells = r.nx * r.ny * r.nz
+    return cells * k / el / 1e9, k, threads, el
+
+
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="grid size (cells incl. CPML)")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+    steps = args.steps
+
+    world, rank, local, pg = dist_setup(args.gpus)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        scene = workload_scene(steps=warmup + steps + 2, n=args.n)
+        value, k, threads, el = time_oracle(scene, budget_s=60.0, max_steps=steps)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": k, "warmup": 1, "ms_per_step": el / k * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "cells": args.n ** 3,
+                           "l2": "inputs larger than L2"},
+                "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"{k} FDTD steps of the full {args.n}^3 scene "
+                                           f"(requested {steps}; bounded to ~60 s), "
+                                           f"{cpu_model()}"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from xfdtd_core_b200.host import SceneRun
+    from xfdtd_core_b200 import engine as E
+    hbm, peak_kind = peaks()
+
+    # FP32 form (headline)
+    sc = workload_scene(steps=warmup + steps, n=args.n)
+    run32 = SceneRun(sc, precision=1)
+    nx, ny, nz = run32.n
+    cells = nx * ny * nz
+    h32 = run32.engine_handle()
+    L = E.load()
+    launches = int(L.xfd_launches_per_step(ctypes_handle(h32)))
+    bytes32 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h32)))
+    sampler = ClockSampler(local)
+    ms32, clocks = time_engine_steps(h32, steps, warmup, pg, local, sampler)
+    run32.close()
+    value = cells * steps * world / (ms32 / 1e3) / 1e9
+    step_s = ms32 / 1e3 / steps
+    achieved = bytes32 / step_s / 1e9
+
+    # FP64 plain form
+    run64 = SceneRun(workload_scene(steps=warmup + steps, n=args.n), precision=0)
+    h64 = run64.engine_handle()
+    bytes64 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h64)))
+    ms64, _ = time_engine_steps(h64, steps, warmup, pg, local, None)
+    run64.close()
+    value64 = cells * steps * world / (ms64 / 1e3) / 1e9
+    achieved64 = bytes64 / (ms64 / 1e3 / steps) / 1e9
+
+    # end to end through the C ABI with host buffers (FP32)
+    e2e_s, h2d, d2h = run_e2e(workload_scene(steps=warmup + steps, n=args.n), steps, warmup, pg,
+                              local)
+    e2e_value = cells * steps * world / e2e_s / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cv, k, threads, el = time_oracle(workload_scene(steps=400, n=args.n),
+                                             budget_s=args.cpu_budget, max_steps=300)
+            cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{k} FDTD steps of the full {args.n}^3 scene in {el:.1f} s, "
+                             f"FP64, OpenMP on {threads} threads, {cpu_model()}"}
+        except Exception as ex:  # reported, not hidden
+            cpu = {"value": None, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                   "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms32 / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": cells, "grid": [nx, ny, nz],
+                       "cpml": 12, "boxes": 64, "precision": "fp32",
+                       "l2": "inputs larger than L2 (fields 6x257^3 fp32 = 407 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "peak_source": peak_kind,
+                         "note": "achieved = algorithmic stencil bytes per step "
+                                 f"({bytes32} B: 12 field values + uint16 class per cell, "
+                                 "8 CPML psi per slab cell) / whole-step time"},
+            "forms": {"fp64_plain": {"value": value64, "unit": UNIT,
+                                     "ms_per_step": ms64 / steps,
+                                     "roofline_achieved_gbs": achieved64,
+                                     "roofline_frac": achieved64 / hbm},
+                      "fp32_over_fp64": value / value64},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+                    "note": "C ABI with pinned host buffers: field upload, steps with an Ez "
+                            "plane copied out every step on a side stream, field download"},
+            "gpu_launches": launches * steps,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

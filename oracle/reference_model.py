@@ -310,7 +310,6 @@ class RefSimulation:
         sig_e = [np.full(s, SIGMA_E_ZERO) for s in shp_e]
         mu = [np.full(s, MU_0) for s in shp_h]
         sig_m = [np.full(s, SIGMA_M_ZERO) for s in shp_h]
-        X, Y, Z = np.meshgrid(self.h_node[0], self.h_node[1], self.h_node[2], indexing="ij")
         self.cell_material = np.zeros((nx, ny, nz), dtype=np.int32)
         mats = []
         painters = [(o.shape, o.material) for o in self.scene.objects]
@@ -327,7 +326,22 @@ class RefSimulation:
             e_val, m_val = er * EPSILON_0, mr * MU_0
             se = SIGMA_E_ZERO if se == 0 else se
             sm = SIGMA_M_ZERO if sm == 0 else sm
-            mask = inside(shape, X, Y, Z, self.eps)
+            # Only cells whose centre lies within the shape's wrapped cube
+            # (+ tolerance) can test inside; the reference evaluates the same
+            # predicate on every cell.
+            cb = wrapped_cube(shape)
+            lo = [int(np.searchsorted(self.h_node[a], cb.origin[a] - 2 * self.eps, "left"))
+                  for a in range(3)]
+            hi = [int(np.searchsorted(self.h_node[a], cb.end[a] + 2 * self.eps, "right"))
+                  for a in range(3)]
+            if any(hi[a] <= lo[a] for a in range(3)):
+                mats.append(mat)
+                continue
+            X, Y, Z = np.meshgrid(self.h_node[0][lo[0]:hi[0]], self.h_node[1][lo[1]:hi[1]],
+                                  self.h_node[2][lo[2]:hi[2]], indexing="ij")
+            sub = inside(shape, X, Y, Z, self.eps)
+            mask = np.zeros((nx, ny, nz), dtype=bool)
+            mask[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = sub
             for c in range(3):
                 eps[c][:nx, :ny, :nz][mask] = e_val
                 sig_e[c][:nx, :ny, :nz][mask] = se

@@ -29,7 +29,8 @@ thread_local std::string g_create_error;
 struct MovieH {
   MovieD d;
   long long n_nodes;
-  long long recorded;  // frames written so far
+  long long copied;  // frames already queued for copy-out to `host`
+  void* host;        // pinned host frame store (max_frames x n_nodes)
 };
 
 struct LumpedH {
@@ -92,6 +93,11 @@ struct xfd_engine {
   long long* d_step = nullptr;
   int* d_err = nullptr;
   int64_t host_step = 0;
+
+  // monitor copy-out: D2H of finished frames on a side stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ev = nullptr;
+  std::vector<void*> host_allocs;
 
   // graph
   bool use_graph = true;
@@ -372,6 +378,33 @@ xfd_status build_graph(xfd_engine* e, long long t0) {
   return XFD_OK;
 }
 
+// Queues the D2H copy of every movie frame finished so far on the copy
+// stream, ordered after the compute stream's work to date, so that it
+// overlaps the following steps.
+xfd_status queue_frame_copies(xfd_engine* e) {
+  bool any = false;
+  for (auto& m : e->movies) {
+    const long long done = std::min<long long>((e->host_step + m.d.interval - 1) / m.d.interval,
+                                               m.d.max_frames);
+    if (done > m.copied) any = true;
+  }
+  if (!any) return XFD_OK;
+  CUDA_TRY(e, cudaEventRecord(e->copy_ev, e->stream));
+  CUDA_TRY(e, cudaStreamWaitEvent(e->copy_stream, e->copy_ev, 0));
+  for (auto& m : e->movies) {
+    const long long done = std::min<long long>((e->host_step + m.d.interval - 1) / m.d.interval,
+                                               m.d.max_frames);
+    if (done <= m.copied) continue;
+    const size_t per = (size_t)m.n_nodes * e->wsize;
+    CUDA_TRY(e, cudaMemcpyAsync(static_cast<char*>(m.host) + m.copied * per,
+                                static_cast<char*>(m.d.store) + m.copied * per,
+                                (size_t)(done - m.copied) * per, cudaMemcpyDeviceToHost,
+                                e->copy_stream));
+    m.copied = done;
+  }
+  return XFD_OK;
+}
+
 xfd_status flush_nf2ff(xfd_engine* e) {
   if (!e->have_nf2ff) return XFD_OK;
   const long long pending = e->host_step - e->nf_last_flush_step;
@@ -415,6 +448,12 @@ xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
     return fail(nullptr, XFD_ERR_CUDA, "cudaSetDevice(%d): %s", g->device, cudaGetErrorString(c));
   c = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
   if (c != cudaSuccess) return fail(nullptr, XFD_ERR_CUDA, "stream: %s", cudaGetErrorString(c));
+  c = cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking);
+  if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->copy_ev, cudaEventDisableTiming);
+  if (c != cudaSuccess) {
+    cudaStreamDestroy(e->stream);
+    return fail(nullptr, XFD_ERR_CUDA, "copy stream: %s", cudaGetErrorString(c));
+  }
   e->precision = g->precision;
   e->wsize = g->precision == XFD_FP64 ? 8 : 4;
   e->n_steps = g->n_steps;
@@ -466,8 +505,12 @@ void xfd_destroy(xfd_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
   drop_graph(e);
   for (void* p : e->allocs) cudaFree(p);
+  for (void* p : e->host_allocs) cudaFreeHost(p);
+  if (e->copy_ev) cudaEventDestroy(e->copy_ev);
+  if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -827,6 +870,15 @@ xfd_status xfd_add_movie(xfd_engine* e, int32_t field, const int32_t box_s[3],
   CUDA_TRY(e, cudaSetDevice(e->device));
   xfd_status s = dev_alloc(e, &m.d.store, (size_t)m.d.max_frames * nn * e->wsize);
   if (s != XFD_OK) return s;
+  void* h = nullptr;
+  const size_t hb = std::max<size_t>((size_t)m.d.max_frames * nn * e->wsize, 16);
+  cudaError_t c = cudaHostAlloc(&h, hb, cudaHostAllocDefault);
+  if (c != cudaSuccess)
+    return fail(e, XFD_ERR_OUT_OF_MEMORY, "pinned frame store (%zu B): %s", hb,
+                cudaGetErrorString(c));
+  e->host_allocs.push_back(h);
+  m.host = h;
+  m.copied = 0;
   e->movies.push_back(m);
   if (id) *id = (int32_t)e->movies.size() - 1;
   e->graph_dirty = true;
@@ -845,8 +897,10 @@ xfd_status xfd_get_movie_frames(xfd_engine* e, int32_t id, void* out, int64_t ca
   const size_t bytes = (size_t)frames * m.n_nodes * e->wsize;
   if ((size_t)capacity_bytes < bytes) return fail(e, XFD_ERR_INVALID_ARGUMENT, "movie buffer too small");
   CUDA_TRY(e, cudaSetDevice(e->device));
-  CUDA_TRY(e, cudaMemcpyAsync(out, m.d.store, bytes, cudaMemcpyDeviceToHost, e->stream));
-  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  xfd_status s = queue_frame_copies(e);
+  if (s != XFD_OK) return s;
+  CUDA_TRY(e, cudaStreamSynchronize(e->copy_stream));
+  std::memcpy(out, m.host, bytes);
   return XFD_OK;
 }
 
@@ -904,6 +958,7 @@ xfd_status xfd_run(xfd_engine* e, int64_t n) {
         CUDA_TRY(e, cudaGraphLaunch(e->graph_exec, e->stream));
         e->host_step += e->graph_len;
         left -= e->graph_len;
+        if ((s = queue_frame_copies(e)) != XFD_OK) return s;
         continue;
       }
     }
@@ -912,13 +967,14 @@ xfd_status xfd_run(xfd_engine* e, int64_t n) {
     e->host_step += 1;
     left -= 1;
   }
-  return XFD_OK;
+  return queue_frame_copies(e);
 }
 
 xfd_status xfd_sync(xfd_engine* e) {
   if (!e) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null engine");
   CUDA_TRY(e, cudaSetDevice(e->device));
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->copy_stream));
   int err = 0;
   CUDA_TRY(e, cudaMemcpy(&err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) return fail(e, XFD_ERR_NUMERIC, "TFSF projection left the incident grid");
