@@ -275,7 +275,7 @@ def main():
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="grid size (cells incl. CPML)")
+    ap.add_argument("--grid", type=int, default=256, help="cells per axis incl. CPML")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -287,17 +287,17 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        scene = workload_scene(steps=warmup + steps + 2, n=args.n)
+        scene = workload_scene(steps=warmup + steps + 2, n=args.grid)
         value, k, threads, el = time_oracle(scene, budget_s=60.0, max_steps=steps)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": k, "warmup": 1, "ms_per_step": el / k * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "cells": args.n ** 3,
+                "config": {"workload": WORKLOAD, "cells": args.grid ** 3,
                            "l2": "inputs larger than L2"},
                 "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{k} FDTD steps of the full {args.n}^3 scene "
+                                 "sample": f"{k} FDTD steps of the full {args.grid}^3 scene "
                                            f"(requested {steps}; bounded to ~60 s), "
                                            f"{cpu_model()}"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -312,7 +312,7 @@ def main():
     hbm, peak_kind = peaks()
 
     # FP32 form (headline)
-    sc = workload_scene(steps=warmup + steps, n=args.n)
+    sc = workload_scene(steps=warmup + steps, n=args.grid)
     run32 = SceneRun(sc, precision=1)
     nx, ny, nz = run32.n
     cells = nx * ny * nz
@@ -328,7 +328,7 @@ def main():
     achieved = bytes32 / step_s / 1e9
 
     # FP64 plain form
-    run64 = SceneRun(workload_scene(steps=warmup + steps, n=args.n), precision=0)
+    run64 = SceneRun(workload_scene(steps=warmup + steps, n=args.grid), precision=0)
     h64 = run64.engine_handle()
     bytes64 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h64)))
     ms64, _ = time_engine_steps(h64, steps, warmup, pg, local, None)
@@ -337,17 +337,17 @@ def main():
     achieved64 = bytes64 / (ms64 / 1e3 / steps) / 1e9
 
     # end to end through the C ABI with host buffers (FP32)
-    e2e_s, h2d, d2h = run_e2e(workload_scene(steps=warmup + steps, n=args.n), steps, warmup, pg,
+    e2e_s, h2d, d2h = run_e2e(workload_scene(steps=warmup + steps, n=args.grid), steps, warmup, pg,
                               local)
     e2e_value = cells * steps * world / e2e_s / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cv, k, threads, el = time_oracle(workload_scene(steps=400, n=args.n),
+            cv, k, threads, el = time_oracle(workload_scene(steps=400, n=args.grid),
                                              budget_s=args.cpu_budget, max_steps=300)
             cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{k} FDTD steps of the full {args.n}^3 scene in {el:.1f} s, "
+                   "sample": f"{k} FDTD steps of the full {args.grid}^3 scene in {el:.1f} s, "
                              f"FP64, OpenMP on {threads} threads, {cpu_model()}"}
         except Exception as ex:  # reported, not hidden
             cpu = {"value": None, "unit": UNIT, "cores": cpu_threads(), "kind": "port",

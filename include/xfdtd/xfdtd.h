@@ -446,6 +446,28 @@ class MovieMonitor : public Monitor {
   std::array<std::size_t, 3> _shape{0, 0, 0};
 };
 
+/// FieldTimeMonitor(name, cube, dir, field): every step, the field at the last
+/// node of the cube's node box (the reference's update loop overwrites the
+/// sample node by node, src/monitor/field_time_monitor.cpp:81-95).  After run,
+/// time() holds the E or H time axis and data() the samples.
+class FieldTimeMonitor : public Monitor {
+ public:
+  FieldTimeMonitor(std::string name, std::unique_ptr<Cube> cube, std::string output_dir,
+                   EMF::Field field)
+      : Monitor{std::move(name), std::move(output_dir)}, _cube{std::move(cube)}, _field{field} {}
+  const std::unique_ptr<Cube>& cube() const { return _cube; }
+  EMF::Field field() const { return _field; }
+  const std::vector<Real>& time() const { return _time; }
+  const std::vector<Real>& data() const { return _data; }
+  std::vector<Real>& timeMutable() { return _time; }
+  std::vector<Real>& dataMutable() { return _data; }
+
+ private:
+  std::unique_ptr<Cube> _cube;
+  EMF::Field _field;
+  std::vector<Real> _time, _data;
+};
+
 // ------------------------------------------------------------------ NF2FF
 /// Frequency-domain NF2FF on a Huygens box `distance` cells inside the grid
 /// faces (src/nffft/nffft_frequency_domain.cpp).  After run() the surface
@@ -527,6 +549,14 @@ class Simulation {
   /// ceyhz ceyhx ceze cezhx cezhy chxh chxey chxez chyh chyez chyex chzh
   /// chzex chzey.  For checking the set-up against the reference's formulas.
   std::vector<std::vector<Real>> coefficientArrays() const;
+
+  /// The TFSF3D set-up handed to the engine: the 1-D incident grid for every
+  /// step (e_inc: steps x aux, h_inc: steps x (aux-1)) and the projections.
+  struct TfsfTables {
+    int aux = 0;
+    std::vector<Real> e_inc, h_inc, p_int[3], p_half[3];
+  };
+  TfsfTables tfsfTables() const;
 
   struct Impl;
 

@@ -43,12 +43,23 @@ int xfdtd_scene_finish(xfdtd_scene* s);
 /* The 18 coefficient arrays in reference shapes (see
  * Simulation::coefficientArrays); each out[q] must hold the array. */
 int xfdtd_scene_coefficients(xfdtd_scene* s, double* const out[18]);
+/* The TFSF3D set-up (1-D incident grid for every step and the projections);
+ * aux = 0 when the scene has no TFSF.  Any output pointer may be NULL;
+ * e_inc holds steps*aux, h_inc steps*(aux-1), p_int[a] box_size[a]+1 and
+ * p_half[a] box_size[a]+2 doubles. */
+int xfdtd_scene_tfsf(xfdtd_scene* s, double* e_inc, double* h_inc, double* const p_int[3],
+                     double* const p_half[3], int32_t* aux);
 /* Host copy of field `comp` (0..5) after finish, reference shape. */
 int xfdtd_scene_field(xfdtd_scene* s, int32_t comp, double* out);
 /* Frames of movie `index` (scene order): n_frames and the box shape; with
  * out != NULL copies n_frames*prod(shape) doubles. */
 int xfdtd_scene_movie(xfdtd_scene* s, int32_t index, double* out, int64_t capacity,
                       int64_t* n_frames, int32_t shape[3]);
+/* Field time monitor `index` (scene order): count = number of steps; with
+ * out != NULL writes the time axis then the samples (2*count doubles), like
+ * TimeMonitor::output's [time; data] (src/monitor/time_monitor.cpp:11-21). */
+int xfdtd_scene_field_time(xfdtd_scene* s, int32_t index, double* out, int64_t capacity,
+                           int64_t* count);
 /* NF2FF surface currents (complex interleaved, [f][face][ja jb ma mb][nodes]). */
 int xfdtd_scene_nf2ff(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count);
 /* Writes <dir>/fields/{EX..HZ}.npy, <dir>/<movie>/<step:05d>.npy and

@@ -219,6 +219,7 @@ class RefSimulation:
         self.threads = threads
         self.movie_frames = {}
         self.movies = []
+        self.field_times = []
         self._keep = []
         self.nx, self.ny, self.nz = n
         f = lambda arrs: [np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
@@ -487,20 +488,23 @@ class RefSimulation:
                     d = d[::-1].copy()
                 return d / total
 
+            # C library pow/exp element by element, as xt::pow/xt::exp call them.
+            cpow = lambda v: np.array([math.pow(x, order) for x in v.tolist()])
+            cexp = lambda v: np.array([math.exp(x) for x in v.tolist()])
             sigma_max_e = p.sigma_ratio * (order + 1) / (150 * PI * float(np.min(g_h)))
             rho_e = rho(g_h, 0.75)
-            sigma_e = sigma_max_e * np.power(rho_e, order)
+            sigma_e = sigma_max_e * cpow(rho_e)
             alpha_e = p.alpha_min + (p.alpha_max - p.alpha_min) * (1 - rho_e)
-            kappa_e = 1 + (p.kappa_max - 1) * np.power(rho_e, order)
-            b_e = np.exp((-dt / EPSILON_0) * (sigma_e / kappa_e + alpha_e))
+            kappa_e = 1 + (p.kappa_max - 1) * cpow(rho_e)
+            b_e = cexp((-dt / EPSILON_0) * (sigma_e / kappa_e + alpha_e))
             a_e = (b_e - 1) * sigma_e / ((sigma_e + kappa_e * alpha_e) * kappa_e * g_h)
             e2m = MU_0 / EPSILON_0
             sigma_max_m = p.sigma_ratio * (order + 1) / (150 * PI * float(np.min(g_e))) * e2m
             rho_m = rho(g_e, 0.25)
-            sigma_m = sigma_max_m * np.power(rho_m, order)
+            sigma_m = sigma_max_m * cpow(rho_m)
             alpha_m = (p.alpha_min + (p.alpha_max - p.alpha_min) * (1 - rho_m)) * e2m
-            kappa_h = 1 + (p.kappa_max - 1) * np.power(rho_m, order)
-            b_h = np.exp((-dt / MU_0) * (sigma_m / kappa_h + alpha_m))
+            kappa_h = 1 + (p.kappa_max - 1) * cpow(rho_m)
+            b_h = cexp((-dt / MU_0) * (sigma_m / kappa_h + alpha_m))
             a_h = (b_h - 1) * sigma_m / ((sigma_m + kappa_h * alpha_m) * kappa_h * g_e)
             # correctCoefficientX/Y/Z: the slab-normal curl coefficients
             # E_A<-H_B, E_B<-H_A, H_A<-E_B, H_B<-E_A.
@@ -798,13 +802,14 @@ class RefSimulation:
         te = np.zeros((nf, nt, 2))
         th = np.zeros((nf, nt, 2))
         for fi, f in enumerate(spec.freqs):
-            t = np.arange(nt, dtype=np.float64)
-            ang_e = (-2.0 * PI) * ((f * (t + 1)) * dt)
-            ang_h = (-2.0 * PI) * ((f * (t + 0.5)) * dt)
-            te[fi, :, 0] = dt * np.cos(ang_e)
-            te[fi, :, 1] = dt * np.sin(ang_e)
-            th[fi, :, 0] = dt * np.cos(ang_h)
-            th[fi, :, 1] = dt * np.sin(ang_h)
+            for t in range(nt):
+                # dt * std::exp(-j 2 pi f (t+1) dt): the C library cos/sin of the angle
+                ae = (-2.0 * PI) * ((f * (t + 1)) * dt)
+                ah = (-2.0 * PI) * ((f * (t + 0.5)) * dt)
+                te[fi, t, 0] = dt * math.cos(ae)
+                te[fi, t, 1] = dt * math.sin(ae)
+                th[fi, t, 0] = dt * math.cos(ah)
+                th[fi, t, 1] = dt * math.sin(ah)
         offs = []
         total = 0
         for fi in range(nf):
@@ -851,6 +856,27 @@ class RefSimulation:
             self.movies.append({"name": mv.name, "field": mv.field, "interval": mv.interval,
                                 "s": o, "e": [o[a] + size[a] for a in range(3)], "count": 0})
             self.movie_frames[mv.name] = []
+        # FieldTimeMonitor::init/update (src/monitor/field_time_monitor.cpp:17-95):
+        # the same box shift; update() overwrites data(t) for every node of the
+        # box, leaving the value of its last node.
+        self.field_times = []
+        self.field_time_data: Dict[str, np.ndarray] = {}
+        nt = self.scene.steps
+        for ft in self.scene.field_times:
+            o, e = self.grid_box(ft.shape)
+            o = list(o)
+            size = [e[a] - o[a] for a in range(3)]
+            for a in range(3):
+                if o[a] == 0:
+                    o[a] += 1
+                    size[a] -= 1
+            last = None
+            if all(size[a] > 0 for a in range(3)):
+                last = [o[a] + size[a] - 1 for a in range(3)]
+            self.field_times.append({"name": ft.name, "field": ft.field, "node": last})
+            t_arr = (linspace((0 + 1) * self.dt, (0 + nt) * self.dt, nt) if ft.field[0] == "E"
+                     else linspace((0 + 0.5) * self.dt, (0 + nt + 0.5) * self.dt, nt))
+            self.field_time_data[ft.name] = np.stack([t_arr, np.zeros(nt)])
 
     # ----------------------------------------------------------------- init
     def _init(self):
@@ -967,6 +993,11 @@ class RefSimulation:
 
     # ------------------------------------------------------------------ run
     def _record_monitors(self):
+        for ft in self.field_times:
+            if ft["node"] is not None:
+                f = ft["field"]
+                arr = (self.e if f[0] == "E" else self.h)["XYZ".index(f[1])]
+                self.field_time_data[ft["name"]][1, self.t] = arr[tuple(ft["node"])]
         for mv in self.movies:
             if mv["count"] % mv["interval"] == 0:
                 f = mv["field"]
@@ -981,7 +1012,7 @@ class RefSimulation:
         if self.threads:
             L.orc_set_num_threads(self.threads)
         n = self.scene.steps - self.t if nsteps is None else nsteps
-        if not self.movies:
+        if not self.movies and not getattr(self, "field_times", None):
             L.orc_run(ctypes.byref(self._sim), self.t, n)
             self.t += n
             return

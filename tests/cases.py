@@ -116,9 +116,12 @@ class KernelCase:
             lumped=self.lumped, ade=self.oracle_ade(), nf2ff=self.oracle_nf2ff())
 
     # -------------------------------------------------------------- engine
-    def engine(self, precision=0, n_steps=8):
+    def engine(self, precision=0, n_steps=8, kernel=1, ichunk=None):
         from xfdtd_core_b200.engine import Engine
         eng = Engine(*self.n, precision=precision, n_steps=n_steps, dt=1.0)
+        eng.set_option("kernel", kernel)
+        if ichunk is not None:
+            eng.set_option("ichunk", ichunk)
         eng.set_material_classes(self.table, self.lattice_class)
         eng.set_curl_factors(self.fe, self.fh)
         for s in self.slabs:

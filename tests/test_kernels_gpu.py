@@ -14,10 +14,15 @@ pytestmark = pytest.mark.gpu
 FP64_TOL = 1e-12
 
 
-def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True):
+KERNELS = [pytest.param((0, None), id="split"), pytest.param((1, None), id="fused"),
+           pytest.param((1, 3), id="fused-ichunk3")]
+
+
+def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True, kernel=(1, None)):
     orc = case.oracle()
     orc.run(steps)
-    eng = case.engine(precision=precision, n_steps=max(steps, 8))
+    eng = case.engine(precision=precision, n_steps=max(steps, 8), kernel=kernel[0],
+                      ichunk=kernel[1])
     eng.set_option("graph", int(graph))
     eng.run(steps)
     eng.sync()
@@ -28,26 +33,36 @@ def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True):
     return eng, orc
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("seed", [0, 1])
-def test_yee_cpml_fp64(seed):
-    _compare(KernelCase(n=(9, 10, 11), seed=seed), steps=4)
+def test_yee_cpml_fp64(seed, kernel):
+    _compare(KernelCase(n=(9, 10, 11), seed=seed), steps=4, kernel=kernel)
 
 
-def test_yee_no_cpml_fp64():
-    _compare(KernelCase(n=(12, 7, 9), seed=3, slabs=()), steps=3)
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_yee_no_cpml_fp64(kernel):
+    _compare(KernelCase(n=(12, 7, 9), seed=3, slabs=()), steps=3, kernel=kernel)
 
 
-def test_yee_cpml_fp32():
-    _compare(KernelCase(n=(9, 10, 11), seed=4), steps=3, precision=1, tol=1e-5)
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_yee_large_tile_crossing_fp64(kernel):
+    # Several (j, k) tiles and i-chunks: 40 x 20 x 70 nodes.
+    _compare(KernelCase(n=(39, 19, 69), seed=14), steps=3, kernel=kernel)
 
 
-def test_graph_matches_eager():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_yee_cpml_fp32(kernel):
+    _compare(KernelCase(n=(9, 10, 11), seed=4), steps=3, precision=1, tol=1e-5, kernel=kernel)
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_graph_matches_eager(kernel):
     c = KernelCase(n=(10, 9, 8), seed=5)
-    a = c.engine(n_steps=64)
+    a = c.engine(n_steps=64, kernel=kernel)
     a.set_option("graph", 1)
     a.set_option("graph_chunk", 8)
     a.run(40)
-    b = c.engine(n_steps=64)
+    b = c.engine(n_steps=64, kernel=kernel)
     b.set_option("graph", 0)
     b.run(40)
     fa, fb = a.download_fields(), b.download_fields()
@@ -55,7 +70,8 @@ def test_graph_matches_eager():
         assert np.array_equal(x, y)
 
 
-def test_tfsf_faces_fp64():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_tfsf_faces_fp64(kernel):
     sc = S.dielectric_sphere(steps=24, dl=0.35 / 16, radius=0.06, pml=4, tfsf_start=6,
                              movie_interval=0)
     from oracle.reference_model import RefSimulation
@@ -68,7 +84,7 @@ def test_tfsf_faces_fp64():
     case.tfsf = t
     orc = case.oracle()
     orc.run(6)
-    eng = case.engine(n_steps=24)
+    eng = case.engine(n_steps=24, kernel=kernel[0], ichunk=kernel[1])
     eng.run(6)
     eng.sync()
     got = eng.download_fields()
@@ -77,18 +93,20 @@ def test_tfsf_faces_fp64():
     assert max(errs) <= FP64_TOL, errs
 
 
-def test_lumped_current_source_fp64():
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_lumped_current_source_fp64(kernel):
     case = KernelCase(n=(9, 10, 11), seed=7)
     case.add_lumped(comp=2, s=(3, 4, 4), e=(5, 6, 6), n_steps=8)
     case.add_lumped(comp=0, s=(2, 2, 2), e=(3, 4, 3), n_steps=8)
-    _compare(case, steps=5)
+    _compare(case, steps=5, kernel=kernel)
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("kind", [0, 1, 2])
-def test_ade_fp64(kind):
+def test_ade_fp64(kind, kernel):
     case = KernelCase(n=(9, 10, 11), seed=8 + kind, slabs=())
     case.add_ade(kind=kind, n_poles=2, n_mat=3)
-    _compare(case, steps=5)
+    _compare(case, steps=5, kernel=kernel)
 
 
 def test_ade_fp32():

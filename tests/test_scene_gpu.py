@@ -37,6 +37,12 @@ def test_scene_fp64_matches_oracle(name):
         want = np.array(orc.movie_frames[sc.movies[0].name])
         assert got.shape == want.shape
         assert rel_l2(got, want) <= TOL64
+    for q, ft in enumerate(sc.field_times):
+        got = run.field_time(q)
+        want = orc.field_time_data[ft.name]
+        assert got.shape == want.shape
+        assert np.array_equal(got[0], want[0])
+        assert rel_l2(got[1], want[1]) <= TOL64
     if sc.nf2ff is not None:
         got = run.nf2ff()
         acc = orc.nf2ff["acc"]

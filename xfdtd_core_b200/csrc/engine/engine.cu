@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "fused.cuh"
 #include "kernels.cuh"
 #include "xfd_engine.h"
 
@@ -54,8 +55,9 @@ struct xfd_engine {
   cudaStream_t stream = nullptr;
 
   std::vector<void*> allocs;
-  void* f[6] = {};
-  void** d_fields = nullptr;  // device array of the 6 field pointers
+  void* fbuf[2][6] = {};          // ping-pong field buffers
+  void** d_fields[2] = {};        // device arrays of the 6 field pointers per buffer
+  int cur = 0;                    // buffer holding the current fields
   uint16_t* cls = nullptr;
   void* tab = nullptr;
   int n_classes = 0;
@@ -66,14 +68,15 @@ struct xfd_engine {
   struct Slab {
     int m, neg, n, e_lo, h_lo;
     void *a_e, *b_e, *a_h, *b_h;
-    void* psi_e[2];
-    void* psi_h[2];
+    void* psi_e[2];     // [component A / B]
+    void* psi_h[2][2];  // [buffer][component A / B]; follows the field buffer
   };
   std::vector<Slab> slabs;
 
   bool have_tfsf = false;
   TfsfD tfsf{};
   TfsfGroupD tfsf_groups[4]{};  // H group 1, H group 2, E group 1, E group 2
+  TfsfHD tfsf_h{};              // H passes per component for the fused sweep
 
   std::vector<LumpedH> lumped_h;
   LumpedD lumped{};
@@ -103,7 +106,9 @@ struct xfd_engine {
   bool use_graph = true;
   int graph_chunk = 32;
   int kernel_mode = 0;
+  int ichunk = 32;
   cudaGraphExec_t graph_exec = nullptr;
+  int graph_cur = -1;
   long long graph_len = 0;
   bool graph_dirty = true;
 };
@@ -205,7 +210,7 @@ template <typename T>
 YeeP<T> yee_params(xfd_engine* e) {
   YeeP<T> p{};
   p.L = e->L;
-  for (int c = 0; c < 6; ++c) p.f[c] = static_cast<T*>(e->f[c]);
+  for (int c = 0; c < 6; ++c) p.f[c] = static_cast<T*>(e->fbuf[e->cur][c]);
   p.cls = e->cls;
   p.tab = static_cast<const T*>(e->tab);
   for (int a = 0; a < 3; ++a) {
@@ -226,7 +231,7 @@ YeeP<T> yee_params(xfd_engine* e) {
     D.b_h = static_cast<const T*>(S.b_h);
     for (int w = 0; w < 2; ++w) {
       D.psi_e[w] = static_cast<T*>(S.psi_e[w]);
-      D.psi_h[w] = static_cast<T*>(S.psi_h[w]);
+      D.psi_h[w] = static_cast<T*>(S.psi_h[e->cur][w]);
     }
   }
   return p;
@@ -234,37 +239,93 @@ YeeP<T> yee_params(xfd_engine* e) {
 
 unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+constexpr int kTJ = 8, kTK = 32;
+
+template <typename T>
+FusedP<T> fused_params(xfd_engine* e, int in, int out) {
+  FusedP<T> p{};
+  p.L = e->L;
+  for (int c = 0; c < 6; ++c) {
+    p.in[c] = static_cast<const T*>(e->fbuf[in][c]);
+    p.out[c] = static_cast<T*>(e->fbuf[out][c]);
+  }
+  p.cls = e->cls;
+  p.tab = static_cast<const T*>(e->tab);
+  for (int a = 0; a < 3; ++a) {
+    p.fe[a] = static_cast<const T*>(e->fe[a]);
+    p.fh[a] = static_cast<const T*>(e->fh[a]);
+  }
+  for (const auto& S : e->slabs) {
+    auto& A = p.slab[S.m];
+    const int q = A.count++;
+    A.n[q] = S.n;
+    A.e_lo[q] = S.e_lo;
+    A.h_lo[q] = S.h_lo;
+    A.a_e[q] = static_cast<const T*>(S.a_e);
+    A.b_e[q] = static_cast<const T*>(S.b_e);
+    A.a_h[q] = static_cast<const T*>(S.a_h);
+    A.b_h[q] = static_cast<const T*>(S.b_h);
+    for (int w = 0; w < 2; ++w) {
+      A.psi_e[q][w] = static_cast<T*>(S.psi_e[w]);
+      A.psi_h_in[q][w] = static_cast<const T*>(S.psi_h[in][w]);
+      A.psi_h_out[q][w] = static_cast<T*>(S.psi_h[out][w]);
+    }
+  }
+  p.tf = e->tfsf;
+  p.tfh = e->tfsf_h;
+  p.tfh.enabled = e->have_tfsf ? 1 : 0;
+  p.ichunk = e->ichunk;
+  p.step = e->d_step;
+  p.err = e->d_err;
+  return p;
+}
+
 long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b); }
 
 // Launches one time step (host step index t decides the periodic kernels).
 template <typename T>
 cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   cudaStream_t s = e->stream;
-  T* const* fields = reinterpret_cast<T* const*>(e->d_fields);
-  const YeeP<T> yp = yee_params<T>(e);
-  const dim3 blk(32, 8, 1);
-  const dim3 grd((unsigned)((e->L.nz + 1 + 31) / 32), (unsigned)((e->L.ny + 1 + 7) / 8),
-                 (unsigned)(e->L.nx + 1));
-  // H phase: updateH + CPML (fused) -> TFSF H faces.
-  k_update_h<T><<<grd, blk, 0, s>>>(yp);
-  if (e->have_tfsf) {
-    for (int g = 0; g < 2; ++g) {
-      const auto& G = e->tfsf_groups[g];
-      if (G.total > 0)
-        k_tfsf<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fields, e->d_step,
-                                                           e->d_err);
-    }
-  }
-  // E phase: ADE e_cur gather -> updateE + CPML -> ADE -> lumped -> TFSF E faces.
+  const bool fused = e->kernel_mode == 1;
+  const int in = e->cur, out = fused ? 1 - e->cur : e->cur;
+  T* const* fields = reinterpret_cast<T* const*>(e->d_fields[out]);
+  T* const* fields_in = reinterpret_cast<T* const*>(e->d_fields[in]);
   AdeD<T> ad{};
   if (e->ade_kind >= 0) {
     if constexpr (sizeof(T) == 8) ad = e->ade64; else ad = e->ade32;
-    k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
   }
-  k_update_e<T><<<grd, blk, 0, s>>>(yp);
-  if (e->ade_kind == 0) k_ade_update<T, 0><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
-  if (e->ade_kind == 1) k_ade_update<T, 1><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
-  if (e->ade_kind == 2) k_ade_update<T, 2><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+  if (fused) {
+    // H + TFSF-H + CPML-H, then E + CPML-E, in one sweep: in -> out.
+    const FusedP<T> fp = fused_params<T>(e, in, out);
+    const dim3 blk(kTK, kTJ, 1);
+    const dim3 grd((unsigned)((e->L.nz + 1 + kTK - 1) / kTK),
+                   (unsigned)((e->L.ny + 1 + kTJ - 1) / kTJ),
+                   (unsigned)((e->L.nx + 1 + e->ichunk - 1) / e->ichunk));
+    k_fused<T, kTJ, kTK><<<grd, blk, 0, s>>>(fp);
+  } else {
+    const YeeP<T> yp = yee_params<T>(e);
+    const dim3 blk(32, 8, 1);
+    const dim3 grd((unsigned)((e->L.nz + 1 + 31) / 32), (unsigned)((e->L.ny + 1 + 7) / 8),
+                   (unsigned)(e->L.nx + 1));
+    // H phase: updateH + CPML (fused) -> TFSF H faces.
+    k_update_h<T><<<grd, blk, 0, s>>>(yp);
+    if (e->have_tfsf) {
+      for (int g = 0; g < 2; ++g) {
+        const auto& G = e->tfsf_groups[g];
+        if (G.total > 0)
+          k_tfsf<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fields,
+                                                             e->d_step, e->d_err);
+      }
+    }
+    // E phase: ADE e_cur gather -> updateE + CPML.
+    if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+    k_update_e<T><<<grd, blk, 0, s>>>(yp);
+  }
+  // ADE -> lumped -> TFSF E faces (the reference's updateE then correctE order).
+  T* const* ecur = fused ? fields_in : nullptr;
+  if (e->ade_kind == 0) k_ade_update<T, 0><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
+  if (e->ade_kind == 1) k_ade_update<T, 1><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
+  if (e->ade_kind == 2) k_ade_update<T, 2><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
   if (e->lumped.n > 0)
     k_lumped<T><<<blocks_for(e->lumped.n, 256), 256, 0, s>>>(e->lumped, fields, e->d_step);
   if (e->have_tfsf) {
@@ -290,6 +351,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
   }
   k_advance<<<1, 1, 0, s>>>(e->d_step);
+  e->cur = out;
   return cudaGetLastError();
 }
 
@@ -303,6 +365,7 @@ long long pattern_period(const xfd_engine* e) {
   long long per = 1;
   for (const auto& mv : e->movies) per = per / gcd_ll(per, mv.d.interval) * mv.d.interval;
   if (e->have_nf2ff) per = per / gcd_ll(per, e->nf2ff.batch) * e->nf2ff.batch;
+  if (e->kernel_mode == 1 && per % 2) per *= 2;  // buffers alternate every step
   return per;
 }
 
@@ -359,21 +422,25 @@ xfd_status build_graph(xfd_engine* e, long long t0) {
   long long len = per;
   while (len < e->graph_chunk) len += per;
   cudaGraph_t g = nullptr;
+  const int cur0 = e->cur;
   CUDA_TRY(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   for (long long s = 0; s < len; ++s) {
     cudaError_t c = enqueue_step(e, t0 + s);
     if (c != cudaSuccess) {
+      e->cur = cur0;
       cudaGraph_t dummy;
       cudaStreamEndCapture(e->stream, &dummy);
       if (dummy) cudaGraphDestroy(dummy);
       return fail(e, XFD_ERR_CUDA, "kernel launch during capture: %s", cudaGetErrorString(c));
     }
   }
+  e->cur = cur0;  // capture only recorded the launches
   CUDA_TRY(e, cudaStreamEndCapture(e->stream, &g));
   cudaError_t c = cudaGraphInstantiate(&e->graph_exec, g, 0);
   cudaGraphDestroy(g);
   if (c != cudaSuccess) return fail(e, XFD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(c));
   e->graph_len = len;
+  e->graph_cur = cur0;
   e->graph_dirty = false;
   return XFD_OK;
 }
@@ -467,8 +534,8 @@ xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
   if (e->n_lat > (1LL << 40))
     return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "grid too large");
   xfd_engine* ep = e.get();
-  for (int k = 0; k < 6; ++k) {
-    if (dev_alloc(ep, &e->f[k], (size_t)e->n_lat * e->wsize) != XFD_OK) {
+  for (int k = 0; k < 12; ++k) {
+    if (dev_alloc(ep, &e->fbuf[k / 6][k % 6], (size_t)e->n_lat * e->wsize) != XFD_OK) {
       g_create_error = ep->err;
       for (void* p : ep->allocs) cudaFree(p);
       cudaStreamDestroy(ep->stream);
@@ -477,19 +544,26 @@ xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
     }
   }
   void* df = nullptr;
+  void* df2 = nullptr;
   void* ds = nullptr;
   void* de = nullptr;
   if (dev_alloc(ep, &df, 6 * sizeof(void*)) != XFD_OK ||
+      dev_alloc(ep, &df2, 6 * sizeof(void*)) != XFD_OK ||
       dev_alloc(ep, &ds, sizeof(long long)) != XFD_OK || dev_alloc(ep, &de, sizeof(int)) != XFD_OK) {
     g_create_error = ep->err;
     for (void* p : ep->allocs) cudaFree(p);
     cudaStreamDestroy(ep->stream);
     return XFD_ERR_CUDA;
   }
-  e->d_fields = static_cast<void**>(df);
+  e->d_fields[0] = static_cast<void**>(df);
+  e->d_fields[1] = static_cast<void**>(df2);
   e->d_step = static_cast<long long*>(ds);
   e->d_err = static_cast<int*>(de);
-  c = cudaMemcpyAsync(e->d_fields, e->f, sizeof e->f, cudaMemcpyHostToDevice, e->stream);
+  c = cudaMemcpyAsync(e->d_fields[0], e->fbuf[0], sizeof e->fbuf[0], cudaMemcpyHostToDevice,
+                      e->stream);
+  if (c == cudaSuccess)
+    c = cudaMemcpyAsync(e->d_fields[1], e->fbuf[1], sizeof e->fbuf[1], cudaMemcpyHostToDevice,
+                        e->stream);
   if (c == cudaSuccess) c = cudaStreamSynchronize(e->stream);
   if (c != cudaSuccess) {
     g_create_error = cudaGetErrorString(c);
@@ -602,7 +676,8 @@ xfd_status xfd_add_cpml(xfd_engine* e, const xfd_cpml_slab* sl) {
   else sz = (long long)(e->L.nx + 1) * e->L.NY * S.n;
   for (int w = 0; w < 2; ++w) {
     if ((s = dev_alloc(e, &S.psi_e[w], (size_t)sz * e->wsize)) != XFD_OK) return s;
-    if ((s = dev_alloc(e, &S.psi_h[w], (size_t)sz * e->wsize)) != XFD_OK) return s;
+    for (int b = 0; b < 2; ++b)
+      if ((s = dev_alloc(e, &S.psi_h[b][w], (size_t)sz * e->wsize)) != XFD_OK) return s;
   }
   e->slabs.push_back(S);
   e->graph_dirty = true;
@@ -683,6 +758,29 @@ xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* t) {
     G.total = begin;
     e->tfsf_groups[g] = G;
   }
+  // Per-component H passes for the fused sweep, in pass order: the node the
+  // pass corrects sits half a cell outside the box on a negative face.
+  TfsfHD th{};
+  for (int g = 0; g < 2; ++g)
+    for (int q = 0; q < 6; ++q) {
+      const TfsfPassD& P = e->tfsf_groups[g].pass[q];
+      const int c = P.field, m = P.axis;
+      TfsfHPass hp{};
+      hp.m = m;
+      hp.neg = P.neg;
+      hp.dual = (c == (m + 1) % 3) ? (m + 2) % 3 : (m + 1) % 3;
+      for (int a = 0; a < 3; ++a) {
+        hp.lo[a] = P.s[a];
+        hp.hi[a] = P.e[a];
+      }
+      if (P.neg) {
+        hp.lo[m] -= 1;
+        hp.hi[m] -= 1;
+      }
+      hp.coeff = P.coeff;
+      th.pass[c][th.n[c]++] = hp;
+    }
+  e->tfsf_h = th;
   e->have_tfsf = true;
   e->graph_dirty = true;
   return XFD_OK;
@@ -909,7 +1007,8 @@ xfd_status xfd_upload_fields(xfd_engine* e, const void* const fields[6]) {
   CUDA_TRY(e, cudaSetDevice(e->device));
   for (int c = 0; c < 6; ++c) {
     if (!fields[c]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null field %d", c);
-    cudaMemcpy3DParms p = copy_parms(e, c, e->f[c], const_cast<void*>(fields[c]), true, e->wsize);
+    cudaMemcpy3DParms p =
+        copy_parms(e, c, e->fbuf[e->cur][c], const_cast<void*>(fields[c]), true, e->wsize);
     CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
   }
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
@@ -919,7 +1018,7 @@ xfd_status xfd_upload_fields(xfd_engine* e, const void* const fields[6]) {
 xfd_status xfd_download_field(xfd_engine* e, int32_t field, void* out) {
   if (!e || !out || field < 0 || field > 5) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad field");
   CUDA_TRY(e, cudaSetDevice(e->device));
-  cudaMemcpy3DParms p = copy_parms(e, field, e->f[field], out, false, e->wsize);
+  cudaMemcpy3DParms p = copy_parms(e, field, e->fbuf[e->cur][field], out, false, e->wsize);
   CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
   return XFD_OK;
@@ -930,7 +1029,7 @@ xfd_status xfd_download_fields(xfd_engine* e, void* const fields[6]) {
   CUDA_TRY(e, cudaSetDevice(e->device));
   for (int c = 0; c < 6; ++c) {
     if (!fields[c]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null field %d", c);
-    cudaMemcpy3DParms p = copy_parms(e, c, e->f[c], fields[c], false, e->wsize);
+    cudaMemcpy3DParms p = copy_parms(e, c, e->fbuf[e->cur][c], fields[c], false, e->wsize);
     CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
   }
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
@@ -951,12 +1050,13 @@ xfd_status xfd_run(xfd_engine* e, int64_t n) {
   while (left > 0) {
     const bool aligned = (e->host_step % per) == 0;
     if (e->use_graph && aligned) {
-      if (e->graph_dirty || !e->graph_exec) {
+      if (e->graph_dirty || !e->graph_exec || e->graph_cur != e->cur) {
         if ((s = build_graph(e, e->host_step)) != XFD_OK) return s;
       }
       if (left >= e->graph_len) {
         CUDA_TRY(e, cudaGraphLaunch(e->graph_exec, e->stream));
         e->host_step += e->graph_len;
+        if (e->graph_len % 2 && e->kernel_mode == 1) e->cur = 1 - e->cur;
         left -= e->graph_len;
         if ((s = queue_frame_copies(e)) != XFD_OK) return s;
         continue;
@@ -991,8 +1091,12 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "graph_chunk range");
     e->graph_chunk = (int)value;
   } else if (!strcmp(name, "kernel")) {
-    if (value != 0) return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
+    if (value != 0 && value != 1)
+      return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
     e->kernel_mode = (int)value;
+  } else if (!strcmp(name, "ichunk")) {
+    if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "ichunk range");
+    e->ichunk = (int)value;
   } else {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
@@ -1004,9 +1108,9 @@ void* xfd_stream(xfd_engine* e) { return e ? (void*)e->stream : nullptr; }
 
 int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (!e) return 0;
-  int n = 2 + 1;  // H sweep, E sweep, step counter
-  if (e->have_tfsf) n += 4;
-  if (e->ade_kind >= 0) n += 2;
+  int n = e->kernel_mode == 1 ? 2 : 3;  // sweep(s) + step counter
+  if (e->have_tfsf) n += e->kernel_mode == 1 ? 2 : 4;
+  if (e->ade_kind >= 0) n += e->kernel_mode == 1 ? 1 : 2;
   if (!e->lumped_h.empty()) n += 1;
   if (e->have_nf2ff) n += 1;
   return n;

@@ -75,8 +75,15 @@ struct YeeP {
 // src/include/boundary/pml_corrector.h:290-382) over the component's whole
 // transverse extent, in slab insertion order.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int sel3(int m, int a, int b, int c) {
+  return m == 0 ? a : (m == 1 ? b : c);
+}
+__device__ __forceinline__ long long sel3(int m, long long a, long long b, long long c) {
+  return m == 0 ? a : (m == 1 ? b : c);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_h(YeeP<T> p) {
+__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeP<T> p) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -109,12 +116,12 @@ __global__ void __launch_bounds__(256) k_update_h(YeeP<T> p) {
     for (int s = 0; s < p.n_slab; ++s) {
       const SlabD<T>& sl = p.slab[s];
       if (sl.m == c) continue;
-      const int l = x[sl.m] - sl.h_lo;
+      const int l = sel3(sl.m, i, j, k) - sl.h_lo;
       if (l < 0 || l >= sl.n) continue;
       const int which = (c == (sl.m + 1) % 3) ? 0 : 1;
       // H_A differences E_B, H_B differences E_A, forward along m.
       const T* D = p.f[which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3];
-      const T diff = D[id + st[sl.m]] - D[id];
+      const T diff = D[id + sel3(sl.m, st[0], st[1], st[2])] - D[id];
       T* ps = sl.psi_h[which] + psi_index(sl, L, i, j, k, l);
       const T psi = sl.b_h[l] * *ps + sl.a_h[l] * diff;
       *ps = psi;
@@ -131,7 +138,7 @@ __global__ void __launch_bounds__(256) k_update_h(YeeP<T> p) {
 // [e_lo, e_lo + n) along m, whole transverse extent.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_e(YeeP<T> p) {
+__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeP<T> p) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -171,12 +178,12 @@ __global__ void __launch_bounds__(256) k_update_e(YeeP<T> p) {
     for (int s = 0; s < p.n_slab; ++s) {
       const SlabD<T>& sl = p.slab[s];
       if (sl.m == c) continue;
-      const int l = x[sl.m] - sl.e_lo;
+      const int l = sel3(sl.m, i, j, k) - sl.e_lo;
       if (l < 0 || l >= sl.n) continue;
       const int which = (c == (sl.m + 1) % 3) ? 0 : 1;
       // E_A differences H_B, E_B differences H_A, backward along m.
       const T* D = p.f[3 + (which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3)];
-      const T diff = D[id] - D[id - st[sl.m]];
+      const T diff = D[id] - D[id - sel3(sl.m, st[0], st[1], st[2])];
       T* ps = sl.psi_e[which] + psi_index(sl, L, i, j, k, l);
       const T psi = sl.b_e[l] * *ps + sl.a_e[l] * diff;
       *ps = psi;
@@ -340,15 +347,17 @@ __global__ void k_ade_gather(AdeD<T> a, T* const* fields) {
   a.ec[e] = fields[a.comp[e]][a.node[e]];
 }
 
+// fields_in (ping-pong sweeps): the buffer still holding E^n, read directly
+// as e_cur; null when k_ade_gather saved it.
 template <typename T, int KIND>
-__global__ void k_ade_update(AdeD<T> a, T* const* fields) {
+__global__ void k_ade_update(AdeD<T> a, T* const* fields, T* const* fields_in) {
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.n) return;
   const T* cf = a.coef + (size_t)a.mat[e] * (2 + 7 * a.np);
   T* E = fields[a.comp[e]];
   const long long id = a.node[e];
   const T e_yee = E[id];
-  const T e_cur = a.ec[e];
+  const T e_cur = fields_in ? fields_in[a.comp[e]][id] : a.ec[e];
   const T e_prev = (KIND == 0) ? a.ep[e] : T(0);
   T j_sum = 0;
   for (int p = 0; p < a.np; ++p) {

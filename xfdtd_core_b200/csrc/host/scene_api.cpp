@@ -113,6 +113,7 @@ void writeNpy(const std::string& path, const std::vector<double>& data,
 struct xfdtd_scene {
   std::unique_ptr<Simulation> sim;
   std::vector<std::shared_ptr<MovieMonitor>> movies;
+  std::vector<std::shared_ptr<FieldTimeMonitor>> probes;
   std::shared_ptr<NFFFTFrequencyDomain> nf2ff;
   int64_t steps = 0;
   bool finished = false;
@@ -203,6 +204,16 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       auto mv = std::make_shared<MovieMonitor>(std::move(fm), interval, name, name);
       sc->movies.push_back(mv);
       sc->sim->addMonitor(mv);
+    } else if (kw == "field_time") {
+      std::string field;
+      in >> name >> field;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      auto ft = std::make_shared<FieldTimeMonitor>(
+          name, std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), name,
+          parseField(field));
+      sc->probes.push_back(ft);
+      sc->sim->addMonitor(ft);
     } else if (kw == "nf2ff_fd") {
       const auto dx = static_cast<Index>(num(in)), dy = static_cast<Index>(num(in)),
                  dz = static_cast<Index>(num(in));
@@ -278,6 +289,21 @@ int xfdtd_scene_coefficients(xfdtd_scene* s, double* const out[18]) {
   })
 }
 
+int xfdtd_scene_tfsf(xfdtd_scene* s, double* e_inc, double* h_inc, double* const p_int[3],
+                     double* const p_half[3], int32_t* aux) {
+  HOST_TRY({
+    if (!s) throw XFDTDException("null scene");
+    const auto t = s->sim->tfsfTables();
+    if (aux) *aux = t.aux;
+    if (e_inc) std::memcpy(e_inc, t.e_inc.data(), t.e_inc.size() * 8);
+    if (h_inc) std::memcpy(h_inc, t.h_inc.data(), t.h_inc.size() * 8);
+    for (int a = 0; a < 3; ++a) {
+      if (p_int && p_int[a]) std::memcpy(p_int[a], t.p_int[a].data(), t.p_int[a].size() * 8);
+      if (p_half && p_half[a]) std::memcpy(p_half[a], t.p_half[a].data(), t.p_half[a].size() * 8);
+    }
+  })
+}
+
 int xfdtd_scene_field(xfdtd_scene* s, int32_t comp, double* out) {
   HOST_TRY({
     if (!s || !out || comp < 0 || comp > 5) throw XFDTDException("bad argument");
@@ -303,6 +329,23 @@ int xfdtd_scene_movie(xfdtd_scene* s, int32_t index, double* out, int64_t capaci
       const std::size_t per = shp[0] * shp[1] * shp[2];
       if ((std::size_t)capacity < per * fr.size()) throw XFDTDException("buffer too small");
       for (std::size_t q = 0; q < fr.size(); ++q) std::memcpy(out + q * per, fr[q].data(), per * 8);
+    }
+  })
+}
+
+int xfdtd_scene_field_time(xfdtd_scene* s, int32_t index, double* out, int64_t capacity,
+                           int64_t* count) {
+  HOST_TRY({
+    if (!s || index < 0 || index >= (int32_t)s->probes.size())
+      throw XFDTDException("bad field time monitor index");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    const auto& p = s->probes[index];
+    const std::size_t n = p->data().size();
+    if (count) *count = (int64_t)n;
+    if (out) {
+      if ((std::size_t)capacity < 2 * n) throw XFDTDException("buffer too small");
+      std::memcpy(out, p->time().data(), n * 8);
+      std::memcpy(out + n, p->data().data(), n * 8);
     }
   })
 }
@@ -346,6 +389,13 @@ int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir) {
         nm << std::setw(5) << std::setfill('0') << q * mv->frameInterval();
         writeNpy((d / (nm.str() + ".npy")).string(), mv->frames()[q], {shp[0], shp[1], shp[2]});
       }
+    }
+    for (const auto& p : s->probes) {  // TimeMonitor::output: [time; data]
+      const fs::path d = root / p->name();
+      fs::create_directories(d);
+      std::vector<double> v(p->time().begin(), p->time().end());
+      v.insert(v.end(), p->data().begin(), p->data().end());
+      writeNpy((d / (p->name() + ".npy")).string(), v, {2, p->data().size()});
     }
     if (s->nf2ff) {
       const auto& acc = s->nf2ff->surfaceCurrents();

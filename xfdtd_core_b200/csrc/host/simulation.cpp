@@ -227,7 +227,15 @@ struct Simulation::Impl {
     int s[3], e[3];
   };
   std::vector<MovieH> movies;
+  struct ProbeH {
+    FieldTimeMonitor* mon;
+    int id;  // engine movie id, -1 when the box is empty
+  };
+  std::vector<ProbeH> probes;
   NFFFTFrequencyDomain* nf2ff = nullptr;
+  // TFSF set-up kept for inspection (Simulation::tfsfTables)
+  std::vector<double> tf_e_inc, tf_h_inc, tf_p_int[3], tf_p_half[3];
+  int tf_aux = 0;
   bool initialised = false;
 };
 
@@ -775,6 +783,7 @@ void Simulation::init(Index time_step) {
   }
 
   if (!_use_engine) {
+    setupTfsf(nullptr);
     I.initialised = true;
     return;
   }
@@ -838,6 +847,34 @@ void Simulation::init(Index time_step) {
                        (std::size_t)(h.e[2] - h.s[2])});
     I.movies.push_back(h);
   }
+  // Field time monitors: the last node of the shifted box, every step.
+  for (const auto& mon : _monitors) {
+    auto ft = std::dynamic_pointer_cast<FieldTimeMonitor>(mon);
+    if (!ft) continue;
+    Impl::ProbeH p{ft.get(), -1};
+    int s[3], e[3];
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) {
+      int o = (int)nearestNode(I.e_node[a], ft->cube()->origin()(a));
+      int en = (int)nearestNode(I.e_node[a], ft->cube()->end()(a));
+      int size = en - o;
+      if (o == 0) {
+        o += 1;
+        size -= 1;
+      }
+      if (size <= 0) empty = true;
+      s[a] = o + size - 1;
+      e[a] = o + size;
+    }
+    if (!empty)
+      checkStatus(E, xfd_add_movie(E, static_cast<int32_t>(ft->field()), s, e, 1, &p.id),
+                  "xfd_add_movie");
+    const bool is_e = static_cast<int>(ft->field()) < 3;
+    ft->timeMutable() = is_e ? linspace((0 + 1) * dt, (0 + _steps) * dt, _steps)
+                             : linspace((0 + 0.5) * dt, (0 + _steps + 0.5) * dt, _steps);
+    ft->dataMutable().assign(_steps, 0.0);
+    I.probes.push_back(p);
+  }
   I.initialised = true;
 }
 
@@ -882,6 +919,20 @@ void Simulation::finish() {
       for (std::size_t q = 0; q < per; ++q)
         out[f][q] = (w == 8) ? reinterpret_cast<double*>(buf.data())[f * per + q]
                              : reinterpret_cast<float*>(buf.data())[f * per + q];
+  }
+  for (auto& p : I.probes) {
+    if (p.id < 0) continue;
+    int64_t frames = 0;
+    checkStatus(_engine, xfd_get_movie_frames(_engine, p.id, nullptr, 0, &frames), "probe");
+    const std::size_t w = _precision == Precision::FP64 ? 8 : 4;
+    std::vector<char> buf((std::size_t)frames * w);
+    checkStatus(_engine, xfd_get_movie_frames(_engine, p.id, buf.data(), (int64_t)buf.size(),
+                                              &frames),
+                "probe");
+    auto& d = p.mon->dataMutable();
+    for (int64_t f = 0; f < frames && f < (int64_t)d.size(); ++f)
+      d[f] = (w == 8) ? reinterpret_cast<double*>(buf.data())[f]
+                      : reinterpret_cast<float*>(buf.data())[f];
   }
   if (I.nf2ff) {
     int64_t cnt = 0;
@@ -1021,7 +1072,28 @@ void Simulation::setupTfsf(xfd_engine* E) {
   d.aux = (int32_t)aux;
   d.e_inc = e_inc.data();
   d.h_inc = h_inc.data();
-  checkStatus(E, xfd_set_tfsf(E, &d), "xfd_set_tfsf");
+  if (E) checkStatus(E, xfd_set_tfsf(E, &d), "xfd_set_tfsf");
+  auto& I = *_impl;
+  I.tf_aux = (int)aux;
+  for (int a = 0; a < 3; ++a) {
+    I.tf_p_int[a] = p_int[a];
+    I.tf_p_half[a] = p_half[a];
+  }
+  I.tf_e_inc = std::move(e_inc);
+  I.tf_h_inc = std::move(h_inc);
+}
+
+Simulation::TfsfTables Simulation::tfsfTables() const {
+  const Impl& I = *_impl;
+  TfsfTables t;
+  t.aux = I.tf_aux;
+  t.e_inc = I.tf_e_inc;
+  t.h_inc = I.tf_h_inc;
+  for (int a = 0; a < 3; ++a) {
+    t.p_int[a] = I.tf_p_int[a];
+    t.p_half[a] = I.tf_p_half[a];
+  }
+  return t;
 }
 
 void Simulation::setupNf2ff(xfd_engine* E) {

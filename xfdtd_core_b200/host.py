@@ -46,8 +46,11 @@ def load():
         "xfdtd_scene_finish": ([vp], ctypes.c_int),
         "xfdtd_scene_coefficients": ([vp, _dp * 18], ctypes.c_int),
         "xfdtd_scene_field": ([vp, i32, _dp], ctypes.c_int),
+        "xfdtd_scene_tfsf": ([vp, _dp, _dp, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.POINTER(i32)], ctypes.c_int),
         "xfdtd_scene_movie": ([vp, i32, _dp, i64, ctypes.POINTER(i64), i32 * 3], ctypes.c_int),
         "xfdtd_scene_nf2ff": ([vp, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "xfdtd_scene_field_time": ([vp, i32, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
         "xfdtd_scene_write_outputs": ([vp, ctypes.c_char_p], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
@@ -60,9 +63,10 @@ def load():
 
 def exported_symbols() -> List[str]:
     return ["xfdtd_scene_open", "xfdtd_scene_close", "xfdtd_host_last_error",
-            "xfdtd_scene_engine", "xfdtd_scene_info", "xfdtd_scene_advance",
+            "xfdtd_scene_engine", "xfdtd_scene_info", "xfdtd_scene_advance", "xfdtd_scene_tfsf",
             "xfdtd_scene_finish", "xfdtd_scene_coefficients", "xfdtd_scene_field",
-            "xfdtd_scene_movie", "xfdtd_scene_nf2ff", "xfdtd_scene_write_outputs"]
+            "xfdtd_scene_movie", "xfdtd_scene_nf2ff", "xfdtd_scene_field_time",
+            "xfdtd_scene_write_outputs"]
 
 
 class SceneRun:
@@ -129,6 +133,23 @@ class SceneRun:
         self._check(self.L.xfdtd_scene_coefficients(self.h, ptrs))
         return arrs
 
+    def tfsf_tables(self, box_size):
+        """(e_inc, h_inc, p_int[3], p_half[3]) the host computed, or None."""
+        aux = ctypes.c_int32()
+        self._check(self.L.xfdtd_scene_tfsf(self.h, None, None, None, None, ctypes.byref(aux)))
+        if aux.value == 0:
+            return None
+        e_inc = np.empty((self.steps, aux.value))
+        h_inc = np.empty((self.steps, aux.value - 1))
+        p_int = [np.empty(box_size[a] + 1) for a in range(3)]
+        p_half = [np.empty(box_size[a] + 2) for a in range(3)]
+        pi = (_dp * 3)(*[x.ctypes.data_as(_dp) for x in p_int])
+        ph = (_dp * 3)(*[x.ctypes.data_as(_dp) for x in p_half])
+        self._check(self.L.xfdtd_scene_tfsf(self.h, e_inc.ctypes.data_as(_dp),
+                                            h_inc.ctypes.data_as(_dp), ctypes.cast(pi, ctypes.c_void_p),
+                                            ctypes.cast(ph, ctypes.c_void_p), ctypes.byref(aux)))
+        return e_inc, h_inc, p_int, p_half
+
     def field(self, c: int) -> np.ndarray:
         a = np.empty(_engine.comp_shape(self.n, c))
         self._check(self.L.xfdtd_scene_field(self.h, c, a.ctypes.data_as(_dp)))
@@ -145,6 +166,15 @@ class SceneRun:
         self._check(self.L.xfdtd_scene_movie(self.h, index, out.ctypes.data_as(_dp), out.size,
                                              ctypes.byref(nfr), shp))
         return out
+
+    def field_time(self, index: int = 0) -> np.ndarray:
+        """[time; samples] of field time monitor `index`, shape (2, steps)."""
+        cnt = ctypes.c_int64()
+        self._check(self.L.xfdtd_scene_field_time(self.h, index, None, 0, ctypes.byref(cnt)))
+        out = np.empty(2 * cnt.value)
+        self._check(self.L.xfdtd_scene_field_time(self.h, index, out.ctypes.data_as(_dp),
+                                                  out.size, ctypes.byref(cnt)))
+        return out.reshape(2, cnt.value)
 
     def nf2ff(self) -> np.ndarray:
         cnt = ctypes.c_int64()

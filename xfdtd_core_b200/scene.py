@@ -61,14 +61,21 @@ class Waveform:
         raise ValueError(self.kind)
 
     def __call__(self, t):
-        """Samples the waveform like ``Waveform::init`` (waveform.cpp:28-34)."""
+        """Samples the waveform like ``Waveform::init`` (waveform.cpp:28-34),
+        element by element with the C library's exp/pow/cos (the functions
+        std::exp/std::pow/std::cos call), not numpy's vectorised ones, whose
+        last-ulp results differ."""
         t = np.asarray(t, dtype=np.float64)
-        if self.kind == "gaussian":
-            v = np.exp(-np.power((t - self.t0) / self.tau, 2))
-        else:
-            v = (np.exp(-np.power((t - self.t0) / self.tau, 2)) *
-                 np.cos(2 * math.pi * self.freq * (t - self.t0)))
-        return self.amplitude * v
+        out = np.empty(t.shape)
+        flat, res = t.ravel(), out.ravel()
+        for q, tv in enumerate(flat.tolist()):
+            g = math.exp(-math.pow((tv - self.t0) / self.tau, 2))
+            if self.kind == "gaussian":
+                v = g
+            else:
+                v = g * math.cos(2 * math.pi * self.freq * (tv - self.t0))
+            res[q] = self.amplitude * v
+        return out
 
 
 @dataclass
@@ -211,6 +218,20 @@ class MovieSpec:
 
 
 @dataclass
+class FieldTimeSpec:
+    """FieldTimeMonitor(name, cube, dir, field): the field at the last node of
+    the cube's node box, every step (src/monitor/field_time_monitor.cpp:81-95)."""
+    name: str
+    field: str
+    shape: Shape  # Cube
+
+    def text(self) -> str:
+        o, s = self.shape.origin, self.shape.size
+        return (f"field_time {self.name} {self.field} " +
+                " ".join(_f(v) for v in (*o, *s)))
+
+
+@dataclass
 class NF2FFSpec:
     distance: Tuple[int, int, int]
     freqs: Sequence[float]
@@ -233,6 +254,7 @@ class Scene:
     pmls: List[PMLSpec] = field(default_factory=list)
     tfsf: Optional[TFSFSpec] = None
     movies: List[MovieSpec] = field(default_factory=list)
+    field_times: List[FieldTimeSpec] = field(default_factory=list)
     nf2ff: Optional[NF2FFSpec] = None
     name: str = "scene"
 
@@ -246,6 +268,7 @@ class Scene:
         if self.tfsf is not None:
             lines.append(self.tfsf.text())
         lines += [m.text() for m in self.movies]
+        lines += [m.text() for m in self.field_times]
         if self.nf2ff is not None:
             lines.append(self.nf2ff.text())
         return "\n".join(lines) + "\n"
@@ -286,6 +309,9 @@ def dielectric_sphere(steps: int = 2000, dl: float = 7.5e-3, half: float = 0.175
         s.movies.append(MovieSpec("movie_ex_xz", "EX",
                                   cube((-half, 0.0, -half), (2 * half, dl, 2 * half)),
                                   movie_interval))
+        # the example's scattered-field probe (dielectric_sphere_scatter.cpp:85-90)
+        s.field_times.append(FieldTimeSpec("ex_point", "EX",
+                                           cube((0.0, -half + 3 * dl, 0.0), (dl, dl, dl))))
     if nf2ff_freqs:
         s.nf2ff = NF2FFSpec((nf2ff_distance,) * 3, list(nf2ff_freqs))
     return s
