@@ -178,7 +178,7 @@ def _ck(L, h, st):
         raise RuntimeError(L.xfd_last_error(h).decode())
 
 
-def run_e2e(scene, steps: int, warmup: int, pg, device: int):
+def run_e2e(scene, steps: int, warmup: int, pg, device: int, options=None):
     """End to end through the C ABI with host buffers: initial fields uploaded
     from pinned host memory, `steps` steps with a movie monitor whose frame (the
     Ez z-plane through the source) is copied to pinned host memory every step on
@@ -188,7 +188,7 @@ def run_e2e(scene, steps: int, warmup: int, pg, device: int):
     import torch
     from xfdtd_core_b200 import engine as E
     from xfdtd_core_b200.host import SceneRun
-    run = SceneRun(scene, precision=1)
+    run = SceneRun(scene, precision=1, options=options)
     L = E.load()
     h = ctypes.c_void_p(run.engine_handle())
     nx, ny, nz = run.n
@@ -278,6 +278,8 @@ def main():
     ap.add_argument("--grid", type=int, default=256, help="cells per axis incl. CPML")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", type=int, default=None,
+                    help="engine sweep: 0 split, 1 fused, 2 fused with TMA pipeline")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
     steps = args.steps
@@ -313,12 +315,17 @@ def main():
 
     # FP32 form (headline)
     sc = workload_scene(steps=warmup + steps, n=args.grid)
-    run32 = SceneRun(sc, precision=1)
+    opts = {} if args.kernel is None else {"kernel": args.kernel}
+    run32 = SceneRun(sc, precision=1, options=opts)
     nx, ny, nz = run32.n
     cells = nx * ny * nz
     h32 = run32.engine_handle()
     L = E.load()
     launches = int(L.xfd_launches_per_step(ctypes_handle(h32)))
+    kmode = ctypes.c_int64()
+    _ck(L, ctypes_handle(h32), L.xfd_get_option(ctypes_handle(h32), b"kernel", ctypes.byref(kmode)))
+    sweep = {0: "split H and E sweeps", 1: "fused H-then-E sweep",
+             2: "fused H-then-E sweep, TMA-staged planes"}[kmode.value]
     bytes32 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h32)))
     sampler = ClockSampler(local)
     ms32, clocks = time_engine_steps(h32, steps, warmup, pg, local, sampler)
@@ -328,7 +335,7 @@ def main():
     achieved = bytes32 / step_s / 1e9
 
     # FP64 plain form
-    run64 = SceneRun(workload_scene(steps=warmup + steps, n=args.grid), precision=0)
+    run64 = SceneRun(workload_scene(steps=warmup + steps, n=args.grid), precision=0, options=opts)
     h64 = run64.engine_handle()
     bytes64 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h64)))
     ms64, _ = time_engine_steps(h64, steps, warmup, pg, local, None)
@@ -338,7 +345,7 @@ def main():
 
     # end to end through the C ABI with host buffers (FP32)
     e2e_s, h2d, d2h = run_e2e(workload_scene(steps=warmup + steps, n=args.grid), steps, warmup, pg,
-                              local)
+                              local, opts)
     e2e_value = cells * steps * world / e2e_s / 1e9
 
     cpu = None
@@ -361,7 +368,7 @@ def main():
             "config": {"workload": WORKLOAD, "cells": cells, "grid": [nx, ny, nz],
                        "cpml": 12, "boxes": 64, "precision": "fp32",
                        "l2": "inputs larger than L2 (fields 6x257^3 fp32 = 407 MB)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "sweep": sweep},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": None,
                          "peak_source": peak_kind,

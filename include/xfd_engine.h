@@ -208,8 +208,12 @@ xfd_status xfd_sync(xfd_engine* e);
 int64_t xfd_current_step(const xfd_engine* e);
 
 /* Engine options: "graph" (0/1, default 1), "graph_chunk" (steps per graph,
- * default 32), "kernel" (0 = split H/E sweeps, 1 = fused H-then-E sweep). */
+ * default 32), "kernel" (0 = split H/E sweeps, 1 = fused H-then-E sweep,
+ * 2 = fused sweep with its per-plane inputs staged by TMA), "ichunk" (planes
+ * per CTA of a fused sweep, default 32). */
 xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value);
+/* Current value of an option of xfd_set_option. */
+xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value);
 
 /* The CUDA stream the engine launches on (a cudaStream_t), for callers that
  * time the engine with events on that stream. */

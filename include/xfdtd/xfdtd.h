@@ -537,6 +537,9 @@ class Simulation {
   /// factors, CPML, ADE) and creates no engine: for checking the set-up
   /// arithmetic on a machine without a GPU.
   void setEngineEnabled(bool on) { _use_engine = on; }
+  /// Engine option (xfd_set_option: "graph", "graph_chunk", "kernel",
+  /// "ichunk"), applied when the engine is created, or at once if it exists.
+  void setEngineOption(const std::string& name, long long value);
   Precision precision() const { return _precision; }
 
   const EMF& emf() const { return _emf; }
@@ -568,6 +571,7 @@ class Simulation {
   Real _cfl;
   Precision _precision = Precision::FP64;
   bool _use_engine = true;
+  std::vector<std::pair<std::string, long long>> _engine_options;
   std::vector<std::shared_ptr<Object>> _objects;
   std::vector<std::shared_ptr<Boundary>> _boundaries;
   std::vector<std::shared_ptr<WaveformSource>> _sources;

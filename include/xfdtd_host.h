@@ -33,6 +33,9 @@ const char* xfdtd_host_last_error(void);
 
 /* The engine the scene drives (owned by the scene). */
 struct xfd_engine* xfdtd_scene_engine(xfdtd_scene* s);
+/* Engine option (xfd_set_option names), applied when the engine is created
+ * by the first advance, or at once afterwards (Simulation::setEngineOption). */
+int xfdtd_scene_set_engine_option(xfdtd_scene* s, const char* name, int64_t value);
 /* Grid size (cells), time step and scene step count. */
 int xfdtd_scene_info(xfdtd_scene* s, int32_t n[3], double* dt, int64_t* steps);
 /* Queues n time steps (Simulation::advance). */

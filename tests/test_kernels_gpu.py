@@ -15,7 +15,8 @@ FP64_TOL = 1e-12
 
 
 KERNELS = [pytest.param((0, None), id="split"), pytest.param((1, None), id="fused"),
-           pytest.param((1, 3), id="fused-ichunk3")]
+           pytest.param((1, 3), id="fused-ichunk3"), pytest.param((2, None), id="fused-tma"),
+           pytest.param((2, 3), id="fused-tma-ichunk3")]
 
 
 def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True, kernel=(1, None)):
@@ -55,7 +56,7 @@ def test_yee_cpml_fp32(kernel):
     _compare(KernelCase(n=(9, 10, 11), seed=4), steps=3, precision=1, tol=1e-5, kernel=kernel)
 
 
-@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("kernel", [0, 1, 2])
 def test_graph_matches_eager(kernel):
     c = KernelCase(n=(10, 9, 8), seed=5)
     a = c.engine(n_steps=64, kernel=kernel)

@@ -23,12 +23,13 @@ def _fields_rel(run, orc):
     return [float(np.linalg.norm(g - w) / ref) for g, w in zip(got, want)]
 
 
+@pytest.mark.parametrize("kernel", [0, 1, 2], ids=["split", "fused", "fused-tma"])
 @pytest.mark.parametrize("name", sorted(ALL))
-def test_scene_fp64_matches_oracle(name):
+def test_scene_fp64_matches_oracle(name, kernel):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)
     orc.run()
-    run = SceneRun(sc)
+    run = SceneRun(sc, options={"kernel": kernel})
     run.run()
     errs = _fields_rel(run, orc)
     assert max(errs) <= TOL64, errs
@@ -76,13 +77,14 @@ def test_dielectric_sphere_full_size_fp64():
     assert max(late) <= TOL64, late
 
 
+@pytest.mark.parametrize("kernel", [0, 2], ids=["split", "fused-tma"])
 @pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
                                          ("dispersive", 1e-4)])
-def test_scene_fp32_error_budget(name, budget):
+def test_scene_fp32_error_budget(name, budget, kernel):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)
     orc.run()
-    run = SceneRun(sc, precision=1)
+    run = SceneRun(sc, precision=1, options={"kernel": kernel})
     run.run()
     errs = _fields_rel(run, orc)
     assert max(errs) <= budget, errs

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "fused.cuh"
+#include "fused_tma.cuh"
 #include "kernels.cuh"
 #include "xfd_engine.h"
 
@@ -107,6 +108,8 @@ struct xfd_engine {
   int graph_chunk = 32;
   int kernel_mode = 0;
   int ichunk = 32;
+  bool tma_ready = false;
+  TmaMaps tma[2]{};  // tensor maps over buffer 0 / 1 (and the class index)
   cudaGraphExec_t graph_exec = nullptr;
   int graph_cur = -1;
   long long graph_len = 0;
@@ -241,6 +244,58 @@ unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs);
 
 constexpr int kTJ = 8, kTK = 32;
 
+constexpr int kStagesF32 = 4, kStagesF64 = 3;
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// Tensor maps for the pipelined sweep: one per field component and buffer
+// (3-D: k, j, i over the logical lattice extent so out-of-range boxes read
+// zeros) and one for the class index.
+template <typename T>
+xfd_status build_tma_maps(xfd_engine* e) {
+  using G = TmaGeom<T, kTJ, kTK>;
+  static EncodeTiledFn encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CUDA_TRY(e, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess)
+      return fail(e, XFD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    encode = reinterpret_cast<EncodeTiledFn>(fn);
+  }
+  const Lat& L = e->L;
+  const cuuint64_t dims[3] = {(cuuint64_t)L.nz + 1, (cuuint64_t)L.ny + 1, (cuuint64_t)L.nx + 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType dt =
+      sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  for (int b = 0; b < 2; ++b) {
+    const cuuint64_t strides[2] = {(cuuint64_t)L.KP * sizeof(T),
+                                   (cuuint64_t)L.KP * L.NY * sizeof(T)};
+    for (int c = 0; c < 6; ++c) {
+      const cuuint32_t box[3] = {(cuuint32_t)G::WE, (cuuint32_t)(c < 3 ? G::RE : G::RH), 1};
+      CUtensorMap* m = c < 3 ? &e->tma[b].e[c] : &e->tma[b].h[c - 3];
+      CUresult r = encode(m, dt, 3, e->fbuf[b][c], dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (field %d): %d", c, (int)r);
+    }
+    const cuuint64_t cstrides[2] = {(cuuint64_t)L.KP * 2, (cuuint64_t)L.KP * L.NY * 2};
+    const cuuint32_t cbox[3] = {(cuuint32_t)G::WC, (cuuint32_t)G::RH, 1};
+    CUresult r = encode(&e->tma[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, e->cls, dims, cstrides,
+                        cbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (class): %d", (int)r);
+  }
+  constexpr int S = sizeof(T) == 8 ? kStagesF64 : kStagesF32;
+  CUDA_TRY(e, cudaFuncSetAttribute(k_fused_tma<T, kTJ, kTK, S>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem(S)));
+  e->tma_ready = true;
+  return XFD_OK;
+}
+
 template <typename T>
 FusedP<T> fused_params(xfd_engine* e, int in, int out) {
   FusedP<T> p{};
@@ -286,7 +341,7 @@ long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b
 template <typename T>
 cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   cudaStream_t s = e->stream;
-  const bool fused = e->kernel_mode == 1;
+  const bool fused = e->kernel_mode >= 1;
   const int in = e->cur, out = fused ? 1 - e->cur : e->cur;
   T* const* fields = reinterpret_cast<T* const*>(e->d_fields[out]);
   T* const* fields_in = reinterpret_cast<T* const*>(e->d_fields[in]);
@@ -296,12 +351,21 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   }
   if (fused) {
     // H + TFSF-H + CPML-H, then E + CPML-E, in one sweep: in -> out.
-    const FusedP<T> fp = fused_params<T>(e, in, out);
     const dim3 blk(kTK, kTJ, 1);
     const dim3 grd((unsigned)((e->L.nz + 1 + kTK - 1) / kTK),
                    (unsigned)((e->L.ny + 1 + kTJ - 1) / kTJ),
                    (unsigned)((e->L.nx + 1 + e->ichunk - 1) / e->ichunk));
-    k_fused<T, kTJ, kTK><<<grd, blk, 0, s>>>(fp);
+    if (e->kernel_mode == 2) {
+      FusedTmaP<T> tp{};
+      tp.p = fused_params<T>(e, in, out);
+      tp.m = e->tma[in];
+      constexpr int S = sizeof(T) == 8 ? kStagesF64 : kStagesF32;
+      k_fused_tma<T, kTJ, kTK, S>
+          <<<grd, blk, TmaGeom<T, kTJ, kTK>::smem(S), s>>>(tp);
+    } else {
+      const FusedP<T> fp = fused_params<T>(e, in, out);
+      k_fused<T, kTJ, kTK><<<grd, blk, 0, s>>>(fp);
+    }
   } else {
     const YeeP<T> yp = yee_params<T>(e);
     const dim3 blk(32, 8, 1);
@@ -365,13 +429,17 @@ long long pattern_period(const xfd_engine* e) {
   long long per = 1;
   for (const auto& mv : e->movies) per = per / gcd_ll(per, mv.d.interval) * mv.d.interval;
   if (e->have_nf2ff) per = per / gcd_ll(per, e->nf2ff.batch) * e->nf2ff.batch;
-  if (e->kernel_mode == 1 && per % 2) per *= 2;  // buffers alternate every step
+  if (e->kernel_mode >= 1 && per % 2) per *= 2;  // buffers alternate every step
   return per;
 }
 
 xfd_status ensure_ready(xfd_engine* e) {
   if (!e->have_classes) return fail(e, XFD_ERR_STATE, "material classes not set");
   if (!e->have_curl) return fail(e, XFD_ERR_STATE, "curl factors not set");
+  if (e->kernel_mode == 2 && !e->tma_ready) {
+    xfd_status st = e->precision == XFD_FP64 ? build_tma_maps<double>(e) : build_tma_maps<float>(e);
+    if (st != XFD_OK) return st;
+  }
   if (e->lumped_dirty) {
     // Concatenate the current sources into one device list.
     std::vector<long long> node;
@@ -622,6 +690,7 @@ xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t 
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
   e->n_classes = n_classes;
   e->have_classes = true;
+  e->tma_ready = false;
   e->graph_dirty = true;
   return XFD_OK;
 }
@@ -1056,7 +1125,7 @@ xfd_status xfd_run(xfd_engine* e, int64_t n) {
       if (left >= e->graph_len) {
         CUDA_TRY(e, cudaGraphLaunch(e->graph_exec, e->stream));
         e->host_step += e->graph_len;
-        if (e->graph_len % 2 && e->kernel_mode == 1) e->cur = 1 - e->cur;
+        if (e->graph_len % 2 && e->kernel_mode >= 1) e->cur = 1 - e->cur;
         left -= e->graph_len;
         if ((s = queue_frame_copies(e)) != XFD_OK) return s;
         continue;
@@ -1083,6 +1152,17 @@ xfd_status xfd_sync(xfd_engine* e) {
 
 int64_t xfd_current_step(const xfd_engine* e) { return e ? e->host_step : -1; }
 
+xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value) {
+  xfd_engine* m = const_cast<xfd_engine*>(e);
+  if (!e || !name || !value) return fail(m, XFD_ERR_INVALID_ARGUMENT, "null option");
+  if (!strcmp(name, "graph")) *value = e->use_graph ? 1 : 0;
+  else if (!strcmp(name, "graph_chunk")) *value = e->graph_chunk;
+  else if (!strcmp(name, "kernel")) *value = e->kernel_mode;
+  else if (!strcmp(name, "ichunk")) *value = e->ichunk;
+  else return fail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
+  return XFD_OK;
+}
+
 xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
   if (!e || !name) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null option");
   if (!strcmp(name, "graph")) {
@@ -1091,7 +1171,7 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "graph_chunk range");
     e->graph_chunk = (int)value;
   } else if (!strcmp(name, "kernel")) {
-    if (value != 0 && value != 1)
+    if (value < 0 || value > 2)
       return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
     e->kernel_mode = (int)value;
   } else if (!strcmp(name, "ichunk")) {
@@ -1108,9 +1188,10 @@ void* xfd_stream(xfd_engine* e) { return e ? (void*)e->stream : nullptr; }
 
 int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (!e) return 0;
-  int n = e->kernel_mode == 1 ? 2 : 3;  // sweep(s) + step counter
-  if (e->have_tfsf) n += e->kernel_mode == 1 ? 2 : 4;
-  if (e->ade_kind >= 0) n += e->kernel_mode == 1 ? 1 : 2;
+  const bool fused = e->kernel_mode >= 1;
+  int n = fused ? 2 : 3;  // sweep(s) + step counter
+  if (e->have_tfsf) n += fused ? 2 : 4;
+  if (e->ade_kind >= 0) n += fused ? 1 : 2;
   if (!e->lumped_h.empty()) n += 1;
   if (e->have_nf2ff) n += 1;
   return n;

@@ -254,6 +254,13 @@ const char* xfdtd_host_last_error(void) { return g_err.c_str(); }
 
 struct xfd_engine* xfdtd_scene_engine(xfdtd_scene* s) { return s ? s->sim->engine() : nullptr; }
 
+int xfdtd_scene_set_engine_option(xfdtd_scene* s, const char* name, int64_t value) {
+  HOST_TRY({
+    if (!s || !name) throw XFDTDException("null argument");
+    s->sim->setEngineOption(name, (long long)value);
+  });
+}
+
 int xfdtd_scene_info(xfdtd_scene* s, int32_t n[3], double* dt, int64_t* steps) {
   HOST_TRY({
     if (!s) throw XFDTDException("null scene");

@@ -799,6 +799,8 @@ void Simulation::init(Index time_step) {
   if (xfd_create(&g, &_engine) != XFD_OK)
     throw XFDTDException(std::string("xfd_create failed: ") + xfd_last_error(nullptr));
   xfd_engine* E = _engine;
+  for (const auto& [name, value] : _engine_options)
+    checkStatus(E, xfd_set_option(E, name.c_str(), value), "xfd_set_option");
   checkStatus(E, xfd_set_material_classes(E, I.table.data(), (int32_t)(I.table.size() / 12),
                                           I.lattice_class.data()),
               "xfd_set_material_classes");
@@ -876,6 +878,11 @@ void Simulation::init(Index time_step) {
     I.probes.push_back(p);
   }
   I.initialised = true;
+}
+
+void Simulation::setEngineOption(const std::string& name, long long value) {
+  if (_engine) checkStatus(_engine, xfd_set_option(_engine, name.c_str(), value), "xfd_set_option");
+  _engine_options.emplace_back(name, value);
 }
 
 void Simulation::advance(Index n) {

@@ -99,6 +99,7 @@ def load(build_if_missing: bool = True):
         "xfd_sync": ([vp], ctypes.c_int),
         "xfd_current_step": ([vp], _i64),
         "xfd_set_option": ([vp, ctypes.c_char_p, _i64], ctypes.c_int),
+        "xfd_get_option": ([vp, ctypes.c_char_p, ctypes.POINTER(_i64)], ctypes.c_int),
         "xfd_stream": ([vp], vp),
         "xfd_launches_per_step": ([vp], _i32),
         "xfd_stencil_bytes_per_step": ([vp], _i64),
@@ -118,7 +119,7 @@ def exported_symbols() -> List[str]:
             "xfd_set_ade", "xfd_set_nf2ff", "xfd_get_nf2ff", "xfd_add_movie",
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
-            "xfd_stream", "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
+            "xfd_get_option", "xfd_stream", "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
 
 
 def _f64(a) -> np.ndarray:
@@ -248,6 +249,11 @@ class Engine:
 
     def set_option(self, name: str, value: int):
         self._check(self.L.xfd_set_option(self.h, name.encode(), int(value)), "set_option")
+
+    def get_option(self, name: str) -> int:
+        v = _i64()
+        self._check(self.L.xfd_get_option(self.h, name.encode(), ctypes.byref(v)), "get_option")
+        return int(v.value)
 
     # ---------------------------------------------------------------- fields
     def upload_fields(self, fields: Sequence[np.ndarray]):

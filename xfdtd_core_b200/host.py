@@ -40,6 +40,7 @@ def load():
         "xfdtd_scene_close": ([vp], None),
         "xfdtd_host_last_error": ([], ctypes.c_char_p),
         "xfdtd_scene_engine": ([vp], vp),
+        "xfdtd_scene_set_engine_option": ([vp, ctypes.c_char_p, i64], ctypes.c_int),
         "xfdtd_scene_info": ([vp, i32 * 3, ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(i64)], ctypes.c_int),
         "xfdtd_scene_advance": ([vp, i64], ctypes.c_int),
@@ -63,7 +64,7 @@ def load():
 
 def exported_symbols() -> List[str]:
     return ["xfdtd_scene_open", "xfdtd_scene_close", "xfdtd_host_last_error",
-            "xfdtd_scene_engine", "xfdtd_scene_info", "xfdtd_scene_advance", "xfdtd_scene_tfsf",
+            "xfdtd_scene_engine", "xfdtd_scene_set_engine_option", "xfdtd_scene_info", "xfdtd_scene_advance", "xfdtd_scene_tfsf",
             "xfdtd_scene_finish", "xfdtd_scene_coefficients", "xfdtd_scene_field",
             "xfdtd_scene_movie", "xfdtd_scene_nf2ff", "xfdtd_scene_field_time",
             "xfdtd_scene_write_outputs"]
@@ -72,7 +73,8 @@ def exported_symbols() -> List[str]:
 class SceneRun:
     """A Simulation built from a scene by the C++ host library."""
 
-    def __init__(self, scene, precision: int = 0, engine: bool = True):
+    def __init__(self, scene, precision: int = 0, engine: bool = True,
+                 options: Optional[dict] = None):
         self.L = load()
         self.scene = scene
         fd, self.path = tempfile.mkstemp(suffix=".scene")
@@ -92,6 +94,12 @@ class SceneRun:
         self.n = tuple(n)
         self.dt = dt.value
         self.steps = steps.value
+        for name, value in (options or {}).items():
+            self.set_engine_option(name, value)
+
+    def set_engine_option(self, name: str, value: int):
+        """Engine option (graph, graph_chunk, kernel, ichunk)."""
+        self._check(self.L.xfdtd_scene_set_engine_option(self.h, name.encode(), int(value)))
 
     def _check(self, st):
         if st != 0:
