@@ -20,6 +20,7 @@ timed region is bracketed by barriers, and the time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -279,7 +280,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", type=int, default=None,
-                    help="engine sweep: 0 split, 1 fused, 2 fused with TMA pipeline")
+                    help="engine sweep: 0 split, 1 fused, 2 fused with TMA pipeline, "
+                         "3 split marching, 4 split marching with TMA pipeline, "
+                         "5 fused marching with TMA pipeline")
+    ap.add_argument("--ichunk", type=int, default=None, help="planes per CTA, fused sweeps")
+    ap.add_argument("--march-ichunk", type=int, default=None,
+                    help="planes per CTA, split marching sweeps")
+    ap.add_argument("--fm-tj", type=int, default=None, help="warps per CTA, fused marching")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
     steps = args.steps
@@ -316,6 +323,10 @@ def main():
     # FP32 form (headline)
     sc = workload_scene(steps=warmup + steps, n=args.grid)
     opts = {} if args.kernel is None else {"kernel": args.kernel}
+    for key, val in (("ichunk", args.ichunk), ("march_ichunk", args.march_ichunk),
+                     ("fm_tj", args.fm_tj)):
+        if val is not None:
+            opts[key] = val
     run32 = SceneRun(sc, precision=1, options=opts)
     nx, ny, nz = run32.n
     cells = nx * ny * nz
@@ -325,7 +336,11 @@ def main():
     kmode = ctypes.c_int64()
     _ck(L, ctypes_handle(h32), L.xfd_get_option(ctypes_handle(h32), b"kernel", ctypes.byref(kmode)))
     sweep = {0: "split H and E sweeps", 1: "fused H-then-E sweep",
-             2: "fused H-then-E sweep, TMA-staged planes"}[kmode.value]
+             2: "fused H-then-E sweep, TMA-staged planes",
+             3: "split H and E sweeps marching along x",
+             4: "split H and E sweeps marching along x, TMA-staged planes",
+             5: "fused H-then-E sweep marching along x, overlapped tiles, TMA-staged planes"
+             }[kmode.value]
     bytes32 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h32)))
     sampler = ClockSampler(local)
     ms32, clocks = time_engine_steps(h32, steps, warmup, pg, local, sampler)

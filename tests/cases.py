@@ -122,6 +122,7 @@ class KernelCase:
         eng.set_option("kernel", kernel)
         if ichunk is not None:
             eng.set_option("ichunk", ichunk)
+            eng.set_option("march_ichunk", ichunk)
         eng.set_material_classes(self.table, self.lattice_class)
         eng.set_curl_factors(self.fe, self.fh)
         for s in self.slabs:

@@ -16,7 +16,11 @@ FP64_TOL = 1e-12
 
 KERNELS = [pytest.param((0, None), id="split"), pytest.param((1, None), id="fused"),
            pytest.param((1, 3), id="fused-ichunk3"), pytest.param((2, None), id="fused-tma"),
-           pytest.param((2, 3), id="fused-tma-ichunk3")]
+           pytest.param((2, 3), id="fused-tma-ichunk3"), pytest.param((3, None), id="march"),
+           pytest.param((3, 3), id="march-ichunk3"), pytest.param((4, None), id="march-tma"),
+           pytest.param((4, 3), id="march-tma-ichunk3"), pytest.param((4, 1), id="march-tma-ichunk1"),
+           pytest.param((5, None), id="fmarch"), pytest.param((5, 3), id="fmarch-ichunk3"),
+           pytest.param((5, 1), id="fmarch-ichunk1")]
 
 
 def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True, kernel=(1, None)):
@@ -46,6 +50,23 @@ def test_yee_no_cpml_fp64(kernel):
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("fm_tj", [8, 16])
+def test_yee_large_tile_crossing_fp32(kernel, fm_tj):
+    """Several tiles along j and k in the FP32 form (both CTA heights of the
+    fused marching sweep)."""
+    case = KernelCase(n=(21, 40, 70), seed=15)
+    orc = case.oracle()
+    orc.run(3)
+    eng = case.engine(precision=1, n_steps=8, kernel=kernel[0], ichunk=kernel[1])
+    eng.set_option("fm_tj", fm_tj)
+    eng.run(3)
+    eng.sync()
+    got = eng.download_fields()
+    errs = [rel_l2(got[c], (orc.e + orc.h)[c]) for c in range(6)]
+    assert max(errs) <= 1e-5, errs
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
 def test_yee_large_tile_crossing_fp64(kernel):
     # Several (j, k) tiles and i-chunks: 40 x 20 x 70 nodes.
     _compare(KernelCase(n=(39, 19, 69), seed=14), steps=3, kernel=kernel)
@@ -56,7 +77,7 @@ def test_yee_cpml_fp32(kernel):
     _compare(KernelCase(n=(9, 10, 11), seed=4), steps=3, precision=1, tol=1e-5, kernel=kernel)
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5])
 def test_graph_matches_eager(kernel):
     c = KernelCase(n=(10, 9, 8), seed=5)
     a = c.engine(n_steps=64, kernel=kernel)

@@ -19,6 +19,9 @@
 
 #include "fused.cuh"
 #include "fused_tma.cuh"
+#include "march.cuh"
+#include "march_tma.cuh"
+#include "fmarch.cuh"
 #include "kernels.cuh"
 #include "xfd_engine.h"
 
@@ -106,10 +109,16 @@ struct xfd_engine {
   // graph
   bool use_graph = true;
   int graph_chunk = 32;
+  // 0 split, 1 fused, 2 fused + TMA, 3 split marching, 4 split marching + TMA,
+  // 5 fused marching (overlapped tiles) + TMA
   int kernel_mode = 0;
   int ichunk = 32;
+  int march_ichunk = 16;  // planes per CTA of the marching split sweeps
+  int fm_tj = 8;          // warps per CTA of the fused marching sweep (FP32)
   bool tma_ready = false;
-  TmaMaps tma[2]{};  // tensor maps over buffer 0 / 1 (and the class index)
+  TmaMaps tma[2]{};       // tensor maps over buffer 0 / 1 (and the class index)
+  MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
+  FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
   cudaGraphExec_t graph_exec = nullptr;
   int graph_cur = -1;
   long long graph_len = 0;
@@ -245,6 +254,28 @@ unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs);
 constexpr int kTJ = 8, kTK = 32;
 
 constexpr int kStagesF32 = 4, kStagesF64 = 3;
+constexpr int kMarchStagesF32 = 6, kMarchStagesF64 = 4;
+template <typename T>
+constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32; }
+constexpr int kFmStages = 4;
+constexpr int kFmTJ64 = 8;
+
+inline bool is_fused(const xfd_engine* e) {
+  return e->kernel_mode == 1 || e->kernel_mode == 2 || e->kernel_mode == 5;
+}
+
+// Encodes one 3-D tiled map over the (nz+1, ny+1, nx+1) lattice of `base`.
+template <typename EncFn>
+CUresult encode_lattice(EncFn encode, CUtensorMap* m, CUtensorMapDataType dt, size_t elem,
+                        void* base, const Lat& L, int box_k, int box_j) {
+  const cuuint64_t dims[3] = {(cuuint64_t)L.nz + 1, (cuuint64_t)L.ny + 1, (cuuint64_t)L.nx + 1};
+  const cuuint64_t strides[2] = {(cuuint64_t)L.KP * elem, (cuuint64_t)L.KP * L.NY * elem};
+  const cuuint32_t box[3] = {(cuuint32_t)box_k, (cuuint32_t)box_j, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return encode(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -289,9 +320,57 @@ xfd_status build_tma_maps(xfd_engine* e) {
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (class): %d", (int)r);
   }
+  // Marching sweeps: halo and tile boxes of every component, class tiles.
+  using MG = MarchGeom<T, 8, 32>;
+  for (int b = 0; b < 2; ++b) {
+    for (int c = 0; c < 6; ++c) {
+      CUresult r = encode_lattice(encode, &e->mtma[b].halo[c], dt, sizeof(T), e->fbuf[b][c], L,
+                                  MG::W, MG::R);
+      if (r == CUDA_SUCCESS)
+        r = encode_lattice(encode, &e->mtma[b].tile[c], dt, sizeof(T), e->fbuf[b][c], L, 32, 8);
+      if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march %d): %d", c, (int)r);
+    }
+    CUresult r = encode_lattice(encode, &e->mtma[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, e->cls,
+                                L, 32, 8);
+    if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march class): %d", (int)r);
+  }
+  // Fused marching sweep: E (TJ+1 rows) and H (TJ rows) boxes of width
+  // 32 elements + 16 bytes, class boxes of 40.
+  const int fm_tj = sizeof(T) == 8 ? kFmTJ64 : e->fm_tj;
+  for (int b = 0; b < 2; ++b) {
+    const int W = 32 + 16 / (int)sizeof(T);
+    for (int c = 0; c < 3; ++c) {
+      CUresult r = encode_lattice(encode, &e->fmaps[b].e[c], dt, sizeof(T), e->fbuf[b][c], L, W,
+                                  fm_tj + 1);
+      if (r == CUDA_SUCCESS)
+        r = encode_lattice(encode, &e->fmaps[b].h[c], dt, sizeof(T), e->fbuf[b][3 + c], L, W,
+                           fm_tj);
+      if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (fmarch %d): %d", c, (int)r);
+    }
+    CUresult r = encode_lattice(encode, &e->fmaps[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                                e->cls, L, 40, fm_tj);
+    if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (fmarch class): %d", (int)r);
+  }
+  if constexpr (sizeof(T) == 8) {
+    CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, kFmTJ64, kFmStages>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     FmarchGeom<T, kFmTJ64>::smem(kFmStages)));
+  } else {
+    CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, 8, kFmStages>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     FmarchGeom<T, 8>::smem(kFmStages)));
+    CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, 16, kFmStages>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     FmarchGeom<T, 16>::smem(kFmStages)));
+  }
   constexpr int S = sizeof(T) == 8 ? kStagesF64 : kStagesF32;
   CUDA_TRY(e, cudaFuncSetAttribute(k_fused_tma<T, kTJ, kTK, S>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem(S)));
+  constexpr int MS = march_stages<T>();
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
   e->tma_ready = true;
   return XFD_OK;
 }
@@ -335,13 +414,31 @@ FusedP<T> fused_params(xfd_engine* e, int in, int out) {
   return p;
 }
 
+template <typename T>
+MarchP<T> march_params(xfd_engine* e) {
+  const FusedP<T> f = fused_params<T>(e, e->cur, e->cur);
+  MarchP<T> p{};
+  p.L = f.L;
+  for (int c = 0; c < 6; ++c) p.f[c] = f.out[c];
+  p.cls = f.cls;
+  p.tab = f.tab;
+  p.n_classes = e->n_classes;
+  for (int a = 0; a < 3; ++a) {
+    p.fe[a] = f.fe[a];
+    p.fh[a] = f.fh[a];
+    p.slab[a] = f.slab[a];
+  }
+  p.ichunk = e->march_ichunk;
+  return p;
+}
+
 long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b); }
 
 // Launches one time step (host step index t decides the periodic kernels).
 template <typename T>
 cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   cudaStream_t s = e->stream;
-  const bool fused = e->kernel_mode >= 1;
+  const bool fused = is_fused(e);
   const int in = e->cur, out = fused ? 1 - e->cur : e->cur;
   T* const* fields = reinterpret_cast<T* const*>(e->d_fields[out]);
   T* const* fields_in = reinterpret_cast<T* const*>(e->d_fields[in]);
@@ -355,7 +452,25 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     const dim3 grd((unsigned)((e->L.nz + 1 + kTK - 1) / kTK),
                    (unsigned)((e->L.ny + 1 + kTJ - 1) / kTJ),
                    (unsigned)((e->L.nx + 1 + e->ichunk - 1) / e->ichunk));
-    if (e->kernel_mode == 2) {
+    if (e->kernel_mode == 5) {
+      FmarchP<T> fm{};
+      fm.p = fused_params<T>(e, in, out);
+      fm.m = e->fmaps[in];
+      const int tj = sizeof(T) == 8 ? kFmTJ64 : e->fm_tj;
+      const dim3 fgrd((unsigned)FmarchGeom<T, 8>::tiles_k(e->L.nz),
+                      (unsigned)((e->L.ny + 1 + tj - 2) / (tj - 1)),
+                      (unsigned)((e->L.nx + 1 + e->ichunk - 1) / e->ichunk));
+      if constexpr (sizeof(T) == 8) {
+        k_fmarch<T, kFmTJ64, kFmStages><<<fgrd, dim3(32, kFmTJ64, 1),
+                                          FmarchGeom<T, kFmTJ64>::smem(kFmStages), s>>>(fm);
+      } else if (tj == 16) {
+        k_fmarch<T, 16, kFmStages><<<fgrd, dim3(32, 16, 1), FmarchGeom<T, 16>::smem(kFmStages),
+                                     s>>>(fm);
+      } else {
+        k_fmarch<T, 8, kFmStages><<<fgrd, dim3(32, 8, 1), FmarchGeom<T, 8>::smem(kFmStages),
+                                    s>>>(fm);
+      }
+    } else if (e->kernel_mode == 2) {
       FusedTmaP<T> tp{};
       tp.p = fused_params<T>(e, in, out);
       tp.m = e->tma[in];
@@ -368,11 +483,29 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
   } else {
     const YeeP<T> yp = yee_params<T>(e);
+    const bool march = e->kernel_mode == 3 || e->kernel_mode == 4;
+    const bool march_tma = e->kernel_mode == 4;
+    constexpr int MS = march_stages<T>();
+    MarchP<T> mp{};
+    MarchTmaP<T> mtp{};
+    if (march) mp = march_params<T>(e);
+    if (march_tma) {
+      mtp.p = mp;
+      mtp.m = e->mtma[e->cur];
+      mtp.err = e->d_err;
+    }
     const dim3 blk(32, 8, 1);
     const dim3 grd((unsigned)((e->L.nz + 1 + 31) / 32), (unsigned)((e->L.ny + 1 + 7) / 8),
                    (unsigned)(e->L.nx + 1));
+    const dim3 grd_m(grd.x, grd.y,
+                     (unsigned)((e->L.nx + 1 + mp.ichunk - 1) / std::max(1, mp.ichunk)));
     // H phase: updateH + CPML (fused) -> TFSF H faces.
-    k_update_h<T><<<grd, blk, 0, s>>>(yp);
+    if (march_tma)
+      k_march_h_tma<T, 8, 32, MS><<<grd_m, blk, MarchGeom<T, 8, 32>::smem(MS), s>>>(mtp);
+    else if (march)
+      k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
+    else
+      k_update_h<T><<<grd, blk, 0, s>>>(yp);
     if (e->have_tfsf) {
       for (int g = 0; g < 2; ++g) {
         const auto& G = e->tfsf_groups[g];
@@ -383,7 +516,12 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
-    k_update_e<T><<<grd, blk, 0, s>>>(yp);
+    if (march_tma)
+      k_march_e_tma<T, 8, 32, MS><<<grd_m, blk, MarchGeom<T, 8, 32>::smem(MS), s>>>(mtp);
+    else if (march)
+      k_march_e<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
+    else
+      k_update_e<T><<<grd, blk, 0, s>>>(yp);
   }
   // ADE -> lumped -> TFSF E faces (the reference's updateE then correctE order).
   T* const* ecur = fused ? fields_in : nullptr;
@@ -429,14 +567,14 @@ long long pattern_period(const xfd_engine* e) {
   long long per = 1;
   for (const auto& mv : e->movies) per = per / gcd_ll(per, mv.d.interval) * mv.d.interval;
   if (e->have_nf2ff) per = per / gcd_ll(per, e->nf2ff.batch) * e->nf2ff.batch;
-  if (e->kernel_mode >= 1 && per % 2) per *= 2;  // buffers alternate every step
+  if (is_fused(e) && per % 2) per *= 2;  // buffers alternate every step
   return per;
 }
 
 xfd_status ensure_ready(xfd_engine* e) {
   if (!e->have_classes) return fail(e, XFD_ERR_STATE, "material classes not set");
   if (!e->have_curl) return fail(e, XFD_ERR_STATE, "curl factors not set");
-  if (e->kernel_mode == 2 && !e->tma_ready) {
+  if ((e->kernel_mode == 2 || e->kernel_mode == 4 || e->kernel_mode == 5) && !e->tma_ready) {
     xfd_status st = e->precision == XFD_FP64 ? build_tma_maps<double>(e) : build_tma_maps<float>(e);
     if (st != XFD_OK) return st;
   }
@@ -673,7 +811,24 @@ xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t 
                   lattice_class[q], q, n_classes);
   }
   CUDA_TRY(e, cudaSetDevice(e->device));
-  xfd_status s = upload_real(e, &e->tab, table, (size_t)n_classes * 12);
+  // Relabel the classes by descending node count, so that the classes
+  // covering most nodes have the smallest indices and stay hot in cache.
+  std::vector<long long> freq(n_classes, 0);
+  for (long long q = 0; q < n_nodes; ++q) ++freq[lattice_class[q]];
+  std::vector<int> order(n_classes);
+  for (int c = 0; c < n_classes; ++c) order[c] = c;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return freq[a] > freq[b]; });
+  std::vector<uint16_t> remap(n_classes);
+  std::vector<double> table2((size_t)n_classes * 12);
+  for (int r = 0; r < n_classes; ++r) {
+    remap[order[r]] = (uint16_t)r;
+    for (int x = 0; x < 12; ++x) table2[(size_t)r * 12 + x] = table[(size_t)order[r] * 12 + x];
+  }
+  std::vector<uint16_t> lattice2((size_t)n_nodes);
+  for (long long q = 0; q < n_nodes; ++q) lattice2[q] = remap[lattice_class[q]];
+  lattice_class = lattice2.data();
+  xfd_status s = upload_real(e, &e->tab, table2.data(), (size_t)n_classes * 12);
   if (s != XFD_OK) return s;
   void* p = nullptr;
   if ((s = dev_alloc(e, &p, (size_t)e->n_lat * sizeof(uint16_t))) != XFD_OK) return s;
@@ -727,6 +882,17 @@ xfd_status xfd_add_cpml(xfd_engine* e, const xfd_cpml_slab* sl) {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "CPML layers out of the grid");
   if (!sl->a_e || !sl->b_e || !sl->a_h || !sl->b_h)
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "null CPML coefficient");
+  // One slab per side of an axis, layers disjoint from the other side's (the
+  // reference's PML objects, one per direction).
+  for (const auto& O : e->slabs) {
+    if (O.m != m) continue;
+    if ((O.neg != 0) == (sl->negative != 0))
+      return fail(e, XFD_ERR_UNSUPPORTED, "two CPML slabs on one side of axis %d", m);
+    const bool e_overlap = sl->e_start < O.e_lo + O.n && O.e_lo < sl->e_start + sl->thickness;
+    const bool h_overlap = sl->h_start < O.h_lo + O.n && O.h_lo < sl->h_start + sl->thickness;
+    if (e_overlap || h_overlap)
+      return fail(e, XFD_ERR_UNSUPPORTED, "CPML slabs on axis %d overlap", m);
+  }
   CUDA_TRY(e, cudaSetDevice(e->device));
   xfd_engine::Slab S{};
   S.m = m;
@@ -1125,7 +1291,7 @@ xfd_status xfd_run(xfd_engine* e, int64_t n) {
       if (left >= e->graph_len) {
         CUDA_TRY(e, cudaGraphLaunch(e->graph_exec, e->stream));
         e->host_step += e->graph_len;
-        if (e->graph_len % 2 && e->kernel_mode >= 1) e->cur = 1 - e->cur;
+        if (e->graph_len % 2 && is_fused(e)) e->cur = 1 - e->cur;
         left -= e->graph_len;
         if ((s = queue_frame_copies(e)) != XFD_OK) return s;
         continue;
@@ -1159,6 +1325,8 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "graph_chunk")) *value = e->graph_chunk;
   else if (!strcmp(name, "kernel")) *value = e->kernel_mode;
   else if (!strcmp(name, "ichunk")) *value = e->ichunk;
+  else if (!strcmp(name, "march_ichunk")) *value = e->march_ichunk;
+  else if (!strcmp(name, "fm_tj")) *value = e->fm_tj;
   else return fail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -1171,12 +1339,20 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "graph_chunk range");
     e->graph_chunk = (int)value;
   } else if (!strcmp(name, "kernel")) {
-    if (value < 0 || value > 2)
+    if (value < 0 || value > 5)
       return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
     e->kernel_mode = (int)value;
   } else if (!strcmp(name, "ichunk")) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "ichunk range");
     e->ichunk = (int)value;
+  } else if (!strcmp(name, "march_ichunk")) {
+    if (value < 1 || value > 4096)
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "march_ichunk range");
+    e->march_ichunk = (int)value;
+  } else if (!strcmp(name, "fm_tj")) {
+    if (value != 8 && value != 16) return fail(e, XFD_ERR_INVALID_ARGUMENT, "fm_tj is 8 or 16");
+    e->fm_tj = (int)value;
+    e->tma_ready = false;
   } else {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
@@ -1188,7 +1364,7 @@ void* xfd_stream(xfd_engine* e) { return e ? (void*)e->stream : nullptr; }
 
 int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (!e) return 0;
-  const bool fused = e->kernel_mode >= 1;
+  const bool fused = is_fused(e);
   int n = fused ? 2 : 3;  // sweep(s) + step counter
   if (e->have_tfsf) n += fused ? 2 : 4;
   if (e->ade_kind >= 0) n += fused ? 1 : 2;

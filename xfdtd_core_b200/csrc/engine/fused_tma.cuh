@@ -68,8 +68,9 @@ __global__ void __launch_bounds__(TJ* TK) k_fused_tma(const __grid_constant__ Fu
   const int n_planes = i_hi - i_first;
   const long long t = *p.step;
   // A sweep whose stage wait timed out poisons the step sequence: later
-  // launches return at once instead of waiting out their own budgets.
-  if (*(volatile int*)p.err & 2) return;
+  // launches return at once instead of waiting out their own budgets.  One
+  // thread reads the error word, so that the whole CTA returns or none.
+  if (__syncthreads_or(tid == 0 && (*(volatile int*)p.err & 2))) return;
 
   auto stage_e = [&](int s, int c) {
     return reinterpret_cast<T*>(smem + s * G::STAGE + G::E_OFF + c * G::pad(G::EB));

@@ -1,0 +1,437 @@
+// Marching split sweeps with TMA-staged planes.  Same arithmetic, ranges and
+// correction order as k_march_h / k_march_e (march.cuh); the difference is
+// how the per-plane inputs arrive: one thread of the CTA issues TMA tile
+// loads (cp.async.bulk.tensor, no multicast) of the planes S-1 ahead into a
+// ring of S shared-memory stages, each completing on its own mbarrier, so
+// that a CTA keeps several planes of DRAM reads in flight while it computes.
+// Results are stored straight from registers (coalesced rows along k).
+//
+// Stage contents (box origins along k are multiples of 32 elements, or that
+// minus 16 bytes, so every TMA x coordinate is 16-byte aligned):
+//   H sweep, plane i: E_x,E_y,E_z "halo" boxes over j0..j0+TJ, k0..k0+TK+XA-1
+//                     (the +1 neighbours along j and k), H_x,H_y,H_z and the
+//                     class index over the tile.  The E of plane i+1 comes
+//                     from the next stage.
+//   E sweep, plane i: H_x,H_y,H_z halo boxes over j0-1..j0+TJ-1,
+//                     k0-XA..k0+TK-1 (the -1 neighbours), E_x,E_y,E_z and the
+//                     class index over the tile.  The H of plane i-1 is the
+//                     previous stage, kept until plane i is done.
+// Out-of-range rows, columns and planes read as zeros and are never used.
+// Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
+// the engine's error word, drains its loads in flight and returns, and later
+// launches that find the bit set return at once.
+#pragma once
+
+#include "march.cuh"
+#include "tma.cuh"
+
+namespace xfd {
+
+struct MarchMaps {
+  CUtensorMap halo[6];  // box (TK+XA) x (TJ+1) of each field component
+  CUtensorMap tile[6];  // box TK x TJ
+  CUtensorMap cls;      // box TK x TJ (uint16)
+};
+
+template <typename T>
+struct MarchTmaP {
+  MarchP<T> p;
+  MarchMaps m;
+  int* err;
+};
+
+template <typename T, int TJ, int TK>
+struct MarchGeom {
+  static constexpr int XA = 16 / (int)sizeof(T);
+  static constexpr int W = TK + XA;  // halo box width
+  static constexpr int R = TJ + 1;   // halo box rows
+  __host__ __device__ static constexpr int pad(int b) { return (b + 127) / 128 * 128; }
+  static constexpr int HALO_B = R * W * (int)sizeof(T);
+  static constexpr int TILE_B = TJ * TK * (int)sizeof(T);
+  static constexpr int CLS_B = TJ * TK * 2;
+  static constexpr int HALO_OFF = 0;
+  static constexpr int TILE_OFF = 3 * pad(HALO_B);
+  static constexpr int CLS_OFF = TILE_OFF + 3 * pad(TILE_B);
+  static constexpr int STAGE = CLS_OFF + pad(CLS_B);
+  static constexpr int TX_FULL = 3 * HALO_B + 3 * TILE_B + CLS_B;
+  static constexpr int TX_HALO = 3 * HALO_B;
+  __host__ __device__ static constexpr int smem(int S) { return S * STAGE + 8 * S; }
+};
+
+// Ring bookkeeping shared by the TMA sweeps: bounded stage waits and the
+// drain on failure.  All threads keep identical copies of parity/pending.
+struct StageRing {
+  uint64_t* bars;
+  uint32_t parity = 0;   // bit s: phase to wait for on stage s
+  uint32_t pending = 0;  // bit s: a load into stage s is in flight
+
+  __device__ __forceinline__ bool try_once(uint32_t a, uint32_t ph) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(ph)
+        : "memory");
+    return done != 0;
+  }
+  __device__ bool wait(int s) {
+    const uint32_t a = smem_u32(&bars[s]);
+    const uint32_t ph = (parity >> s) & 1u;
+    if (!try_once(a, ph)) {
+      const long long t0 = clock64();
+      while (!try_once(a, ph))
+        if (clock64() - t0 > 4000000000LL) return false;  // about 2 s
+    }
+    parity ^= 1u << s;
+    pending &= ~(1u << s);
+    return true;
+  }
+  __device__ void drain(int S) {
+    for (int s = 0; s < S; ++s)
+      if ((pending >> s) & 1u) wait(s);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// H sweep.  Planes q = 0 .. n_planes of the chunk are staged (plane n_planes
+// is i_hi, E only, when i_hi <= nx); plane q lives in stage q % S.
+// ---------------------------------------------------------------------------
+template <typename T, int TJ, int TK, int S>
+__global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ MarchTmaP<T> P) {
+  using G = MarchGeom<T, TJ, TK>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const MarchP<T>& p = P.p;
+  const Lat L = p.L;
+  const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
+  // One thread reads the error word, so that the whole CTA returns or none.
+  if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
+  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+  const int k = k0 + tk, j = j0 + tj;
+  const int i_lo = blockIdx.z * p.ichunk;
+  const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
+  const int n_planes = i_hi - i_lo;
+  const int n_staged = n_planes + (i_hi <= L.nx ? 1 : 0);
+
+  StageRing ring;
+  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE);
+  auto halo = [&](int s, int c) {
+    return reinterpret_cast<const T*>(smem + s * G::STAGE + G::HALO_OFF + c * G::pad(G::HALO_B));
+  };
+  auto tile = [&](int s, int c) {
+    return reinterpret_cast<const T*>(smem + s * G::STAGE + G::TILE_OFF + c * G::pad(G::TILE_B));
+  };
+  auto ctile = [&](int s) {
+    return reinterpret_cast<const uint16_t*>(smem + s * G::STAGE + G::CLS_OFF);
+  };
+  auto issue = [&](int q) {
+    const int s = q % S, i = i_lo + q;
+    uint64_t* bar = &ring.bars[s];
+    unsigned char* base = smem + s * G::STAGE;
+    const bool e_only = q == n_planes;
+    mbar_expect_tx(bar, e_only ? G::TX_HALO : G::TX_FULL);
+    for (int c = 0; c < 3; ++c)
+      tma_load_3d(base + G::HALO_OFF + c * G::pad(G::HALO_B), &P.m.halo[c], k0, j0, i, bar);
+    if (!e_only) {
+      for (int c = 0; c < 3; ++c)
+        tma_load_3d(base + G::TILE_OFF + c * G::pad(G::TILE_B), &P.m.tile[3 + c], k0, j0, i, bar);
+      tma_load_3d(base + G::CLS_OFF, &P.m.cls, k0, j0, i, bar);
+    }
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&ring.bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int q = 0; q < S && q < n_staged; ++q) issue(q);
+  for (int q = 0; q < S && q < n_staged; ++q) ring.pending |= 1u << (q % S);
+
+  // Per-thread constants (as k_march_h).
+  const bool act = k <= L.nz && j <= L.ny;
+  const long long PS = (long long)L.NY * L.KP;
+  const int KP = L.KP;
+  const long long row = (long long)j * KP + k;
+  const bool jv = j < L.ny, kv = k < L.nz;
+  const T fhj = (act && jv) ? p.fh[1][j] : T(0);
+  const T fhk = (act && kv) ? p.fh[2][k] : T(0);
+  int qy = 0, qz = 0;
+  const int ly = act ? layer_of(p.slab[1], j, false, qy) : -1;
+  const int lz = act ? layer_of(p.slab[2], k, false, qz) : -1;
+  T ay = 0, by = 0, az = 0, bz = 0;
+  T* psy[2] = {nullptr, nullptr};
+  T* psz[2] = {nullptr, nullptr};
+  long long psy_st = 0, psz_st = 0;
+  if (ly >= 0) {
+    const SlabAxisD<T>& A = p.slab[1];
+    ay = A.a_h[qy][ly];
+    by = A.b_h[qy][ly];
+    psy_st = (long long)A.n[qy] * KP;
+    for (int w = 0; w < 2; ++w) psy[w] = A.psi_h_out[qy][w] + (long long)ly * KP + k;
+  }
+  if (lz >= 0) {
+    const SlabAxisD<T>& A = p.slab[2];
+    az = A.a_h[qz][lz];
+    bz = A.b_h[qz][lz];
+    psz_st = (long long)L.NY * A.n[qz];
+    for (int w = 0; w < 2; ++w) psz[w] = A.psi_h_out[qz][w] + (long long)j * A.n[qz] + lz;
+  }
+  T* Hx = p.f[3] + row;
+  T* Hy = p.f[4] + row;
+  T* Hz = p.f[5] + row;
+  const int hq = tj * G::W + tk;  // (j, k) in a halo box
+  const int tq = tj * TK + tk;    // (j, k) in a tile box
+
+  bool ok = true;
+  if (n_staged > 0) ok = ring.wait(0);
+  for (int q = 0; q < n_planes; ++q) {
+    const int i = i_lo + q;
+    const bool iv = i < L.nx;
+    const int sc = q % S, sn = (q + 1) % S;
+    if (ok && iv) ok = ring.wait(sn);  // plane i+1 (exists when i < nx)
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    if (act) {
+      const bool main_rng = iv && jv && kv;
+      const T fhi = iv ? p.fh[0][i] : T(0);
+      const T* r = p.tab + (size_t)ctile(sc)[tq] * 12 + 6;
+      const T* Exs = halo(sc, 0);
+      const T* Eys = halo(sc, 1);
+      const T* Ezs = halo(sc, 2);
+      const T ex = Exs[hq], ex_k = Exs[hq + 1], ex_j = Exs[hq + G::W];
+      const T ey = Eys[hq], ey_k = Eys[hq + 1];
+      const T ez = Ezs[hq], ez_j = Ezs[hq + G::W];
+      const T ey_n = iv ? halo(sn, 1)[hq] : T(0);
+      const T ez_n = iv ? halo(sn, 2)[hq] : T(0);
+      const T dEy_k = ey_k - ey, dEz_j = ez_j - ez;  // Hx
+      const T dEz_i = ez_n - ez, dEx_k = ex_k - ex;  // Hy
+      const T dEx_j = ex_j - ex, dEy_i = ey_n - ey;  // Hz
+      const long long o = i * PS;
+      int qx;
+      const int lx = layer_of(p.slab[0], i, false, qx);
+      if (jv && kv) {
+        const T ca = r[0], cb = r[1];
+        T h = tile(sc, 0)[tq];
+        if (main_rng) h = ca * h + cb * (fhk * dEy_k - fhj * dEz_j);
+        if (ly >= 0) h -= cb * psi_step(psy[1] + i * psy_st, by, ay, dEz_j);
+        if (lz >= 0) h += cb * psi_step(psz[0] + i * psz_st, bz, az, dEy_k);
+        Hx[o] = h;
+      }
+      if (iv && kv) {
+        const T ca = r[2], cb = r[3];
+        T h = tile(sc, 1)[tq];
+        if (main_rng) h = ca * h + cb * (fhi * dEz_i - fhk * dEx_k);
+        if (lx >= 0) {
+          const SlabAxisD<T>& A = p.slab[0];
+          h += cb * psi_step(A.psi_h_out[qx][0] + (long long)lx * PS + row, A.b_h[qx][lx],
+                             A.a_h[qx][lx], dEz_i);
+        }
+        if (lz >= 0) h -= cb * psi_step(psz[1] + i * psz_st, bz, az, dEx_k);
+        Hy[o] = h;
+      }
+      if (iv && jv) {
+        const T ca = r[4], cb = r[5];
+        T h = tile(sc, 2)[tq];
+        if (main_rng) h = ca * h + cb * (fhj * dEx_j - fhi * dEy_i);
+        if (lx >= 0) {
+          const SlabAxisD<T>& A = p.slab[0];
+          h -= cb * psi_step(A.psi_h_out[qx][1] + (long long)lx * PS + row, A.b_h[qx][lx],
+                             A.a_h[qx][lx], dEy_i);
+        }
+        if (ly >= 0) h += cb * psi_step(psy[0] + i * psy_st, by, ay, dEx_j);
+        Hz[o] = h;
+      }
+    }
+    __syncthreads();
+    // Stage sc (plane i) is free: refill it with plane q+S.
+    if (q + S < n_staged) {
+      if (tid == 0) {
+        fence_proxy_async();
+        issue(q + S);
+      }
+      ring.pending |= 1u << sc;
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(P.err, 2);
+    ring.drain(S);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// E sweep.  Staged planes q = -1 .. n_planes-1 (plane -1 = i_lo-1, H only,
+// when i_lo >= 1); plane q lives in stage (q+1) % S.
+// ---------------------------------------------------------------------------
+template <typename T, int TJ, int TK, int S>
+__global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ MarchTmaP<T> P) {
+  using G = MarchGeom<T, TJ, TK>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const MarchP<T>& p = P.p;
+  const Lat L = p.L;
+  const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
+  // One thread reads the error word, so that the whole CTA returns or none.
+  if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
+  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+  const int k = k0 + tk, j = j0 + tj;
+  const int i_lo = blockIdx.z * p.ichunk;
+  const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
+  const int n_planes = i_hi - i_lo;
+  const int q_first = i_lo >= 1 ? -1 : 0;  // first staged plane
+
+  StageRing ring;
+  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE);
+  auto slot = [](int q) { return (q + 1) % S; };
+  auto halo = [&](int s, int c) {
+    return reinterpret_cast<const T*>(smem + s * G::STAGE + G::HALO_OFF + c * G::pad(G::HALO_B));
+  };
+  auto tile = [&](int s, int c) {
+    return reinterpret_cast<const T*>(smem + s * G::STAGE + G::TILE_OFF + c * G::pad(G::TILE_B));
+  };
+  auto ctile = [&](int s) {
+    return reinterpret_cast<const uint16_t*>(smem + s * G::STAGE + G::CLS_OFF);
+  };
+  auto issue = [&](int q) {
+    const int s = slot(q), i = i_lo + q;
+    uint64_t* bar = &ring.bars[s];
+    unsigned char* base = smem + s * G::STAGE;
+    const bool h_only = q < 0;
+    mbar_expect_tx(bar, h_only ? G::TX_HALO : G::TX_FULL);
+    for (int c = 0; c < 3; ++c)
+      tma_load_3d(base + G::HALO_OFF + c * G::pad(G::HALO_B), &P.m.halo[3 + c], k0 - G::XA,
+                  j0 - 1, i, bar);
+    if (!h_only) {
+      for (int c = 0; c < 3; ++c)
+        tma_load_3d(base + G::TILE_OFF + c * G::pad(G::TILE_B), &P.m.tile[c], k0, j0, i, bar);
+      tma_load_3d(base + G::CLS_OFF, &P.m.cls, k0, j0, i, bar);
+    }
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&ring.bars[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const int q_end = n_planes;  // one past the last staged plane
+  if (tid == 0)
+    for (int q = q_first; q < q_first + S && q < q_end; ++q) issue(q);
+  for (int q = q_first; q < q_first + S && q < q_end; ++q) ring.pending |= 1u << slot(q);
+
+  const bool act = k <= L.nz && j <= L.ny;
+  const long long PS = (long long)L.NY * L.KP;
+  const int KP = L.KP;
+  const long long row = (long long)j * KP + k;
+  const bool jv = j < L.ny, kv = k < L.nz;
+  const bool jm = j >= 1 && jv, km = k >= 1 && kv;
+  const T fej = act ? p.fe[1][j] : T(0);
+  const T fek = act ? p.fe[2][k] : T(0);
+  int qy = 0, qz = 0;
+  const int ly = act ? layer_of(p.slab[1], j, true, qy) : -1;
+  const int lz = act ? layer_of(p.slab[2], k, true, qz) : -1;
+  T ay = 0, by = 0, az = 0, bz = 0;
+  T* psy[2] = {nullptr, nullptr};
+  T* psz[2] = {nullptr, nullptr};
+  long long psy_st = 0, psz_st = 0;
+  if (ly >= 0) {
+    const SlabAxisD<T>& A = p.slab[1];
+    ay = A.a_e[qy][ly];
+    by = A.b_e[qy][ly];
+    psy_st = (long long)A.n[qy] * KP;
+    for (int w = 0; w < 2; ++w) psy[w] = A.psi_e[qy][w] + (long long)ly * KP + k;
+  }
+  if (lz >= 0) {
+    const SlabAxisD<T>& A = p.slab[2];
+    az = A.a_e[qz][lz];
+    bz = A.b_e[qz][lz];
+    psz_st = (long long)L.NY * A.n[qz];
+    for (int w = 0; w < 2; ++w) psz[w] = A.psi_e[qz][w] + (long long)j * A.n[qz] + lz;
+  }
+  T* Ex = p.f[0] + row;
+  T* Ey = p.f[1] + row;
+  T* Ez = p.f[2] + row;
+  const int hq = (tj + 1) * G::W + tk + G::XA;  // (j, k) in a halo box
+  const int tq = tj * TK + tk;
+
+  bool ok = true;
+  if (q_first < 0) ok = ring.wait(slot(-1));
+  for (int q = 0; q < n_planes; ++q) {
+    const int i = i_lo + q;
+    const int sc = slot(q), sp = slot(q - 1);
+    if (ok) ok = ring.wait(sc);
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    if (act) {
+      const bool iv = i < L.nx, i1 = i >= 1;
+      const bool im = i1 && iv;
+      const T fei = p.fe[0][i];
+      const T* r = p.tab + (size_t)ctile(sc)[tq] * 12;
+      const T* Hxs = halo(sc, 0);
+      const T* Hys = halo(sc, 1);
+      const T* Hzs = halo(sc, 2);
+      const T hx = Hxs[hq], hy = Hys[hq], hz = Hzs[hq];
+      const T hx_k = Hxs[hq - 1], hx_j = Hxs[hq - G::W];
+      const T hy_k = Hys[hq - 1];
+      const T hz_j = Hzs[hq - G::W];
+      const T hy_p = i1 ? halo(sp, 1)[hq] : T(0);
+      const T hz_p = i1 ? halo(sp, 2)[hq] : T(0);
+      const T dHz_j = hz - hz_j, dHy_k = hy - hy_k;  // Ex
+      const T dHx_k = hx - hx_k, dHz_i = hz - hz_p;  // Ey
+      const T dHy_i = hy - hy_p, dHx_j = hx - hx_j;  // Ez
+      const long long o = i * PS;
+      int qx;
+      const int lx = layer_of(p.slab[0], i, true, qx);
+      if (iv) {
+        const T ca = r[0], cb = r[1];
+        T e = tile(sc, 0)[tq];
+        if (jm && km) e = ca * e + cb * (fej * dHz_j - fek * dHy_k);
+        if (ly >= 0) e += cb * psi_step(psy[1] + i * psy_st, by, ay, dHz_j);
+        if (lz >= 0) e -= cb * psi_step(psz[0] + i * psz_st, bz, az, dHy_k);
+        Ex[o] = e;
+      }
+      if (jv) {
+        const T ca = r[2], cb = r[3];
+        T e = tile(sc, 1)[tq];
+        if (im && km) e = ca * e + cb * (fek * dHx_k - fei * dHz_i);
+        if (lx >= 0) {
+          const SlabAxisD<T>& A = p.slab[0];
+          e -= cb * psi_step(A.psi_e[qx][0] + (long long)lx * PS + row, A.b_e[qx][lx],
+                             A.a_e[qx][lx], dHz_i);
+        }
+        if (lz >= 0) e += cb * psi_step(psz[1] + i * psz_st, bz, az, dHx_k);
+        Ey[o] = e;
+      }
+      if (kv) {
+        const T ca = r[4], cb = r[5];
+        T e = tile(sc, 2)[tq];
+        if (im && jm) e = ca * e + cb * (fei * dHy_i - fej * dHx_j);
+        if (lx >= 0) {
+          const SlabAxisD<T>& A = p.slab[0];
+          e += cb * psi_step(A.psi_e[qx][1] + (long long)lx * PS + row, A.b_e[qx][lx],
+                             A.a_e[qx][lx], dHy_i);
+        }
+        if (ly >= 0) e -= cb * psi_step(psy[0] + i * psy_st, by, ay, dHx_j);
+        Ez[o] = e;
+      }
+    }
+    __syncthreads();
+    // Stage sp (plane i-1) is free: refill it with plane q-1+S.
+    const int qn = q - 1 + S;
+    if (q - 1 >= q_first && qn < q_end) {
+      if (tid == 0) {
+        fence_proxy_async();
+        issue(qn);
+      }
+      ring.pending |= 1u << sp;
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicOr(P.err, 2);
+    ring.drain(S);
+  }
+}
+
+}  // namespace xfd
