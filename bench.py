@@ -286,7 +286,6 @@ def main():
     ap.add_argument("--ichunk", type=int, default=None, help="planes per CTA, fused sweeps")
     ap.add_argument("--march-ichunk", type=int, default=None,
                     help="planes per CTA, split marching sweeps")
-    ap.add_argument("--fm-tj", type=int, default=None, help="warps per CTA, fused marching")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
     steps = args.steps
@@ -323,8 +322,7 @@ def main():
     # FP32 form (headline)
     sc = workload_scene(steps=warmup + steps, n=args.grid)
     opts = {} if args.kernel is None else {"kernel": args.kernel}
-    for key, val in (("ichunk", args.ichunk), ("march_ichunk", args.march_ichunk),
-                     ("fm_tj", args.fm_tj)):
+    for key, val in (("ichunk", args.ichunk), ("march_ichunk", args.march_ichunk)):
         if val is not None:
             opts[key] = val
     run32 = SceneRun(sc, precision=1, options=opts)

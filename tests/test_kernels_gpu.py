@@ -50,15 +50,12 @@ def test_yee_no_cpml_fp64(kernel):
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
-@pytest.mark.parametrize("fm_tj", [8, 16])
-def test_yee_large_tile_crossing_fp32(kernel, fm_tj):
-    """Several tiles along j and k in the FP32 form (both CTA heights of the
-    fused marching sweep)."""
+def test_yee_large_tile_crossing_fp32(kernel):
+    """Several tiles along j and k in the FP32 form."""
     case = KernelCase(n=(21, 40, 70), seed=15)
     orc = case.oracle()
     orc.run(3)
     eng = case.engine(precision=1, n_steps=8, kernel=kernel[0], ichunk=kernel[1])
-    eng.set_option("fm_tj", fm_tj)
     eng.run(3)
     eng.sync()
     got = eng.download_fields()

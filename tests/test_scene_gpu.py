@@ -23,14 +23,19 @@ def _fields_rel(run, orc):
     return [float(np.linalg.norm(g - w) / ref) for g, w in zip(got, want)]
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5],
-                         ids=["split", "fused", "fused-tma", "march", "march-tma", "fmarch"])
+SWEEPS = [pytest.param({"kernel": 0}, id="split"), pytest.param({"kernel": 1}, id="fused"),
+          pytest.param({"kernel": 2}, id="fused-tma"), pytest.param({"kernel": 3}, id="march"),
+          pytest.param({"kernel": 4}, id="march-tma"), pytest.param({"kernel": 5}, id="fmarch"),
+          pytest.param({"kernel": 5, "ichunk": 4}, id="fmarch-ichunk4")]
+
+
+@pytest.mark.parametrize("opts", SWEEPS)
 @pytest.mark.parametrize("name", sorted(ALL))
-def test_scene_fp64_matches_oracle(name, kernel):
+def test_scene_fp64_matches_oracle(name, opts):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)
     orc.run()
-    run = SceneRun(sc, options={"kernel": kernel})
+    run = SceneRun(sc, options=opts)
     run.run()
     errs = _fields_rel(run, orc)
     assert max(errs) <= TOL64, errs
@@ -78,18 +83,17 @@ def test_dielectric_sphere_full_size_fp64():
     assert max(late) <= TOL64, late
 
 
-@pytest.mark.parametrize("kernel", [0, 2, 3, 4, 5],
-                         ids=["split", "fused-tma", "march", "march-tma", "fmarch"])
+@pytest.mark.parametrize("opts", [s for s in SWEEPS if s.id != "fused"])
 # FP32 budgets: relative L2 against the FP64 oracle after 150 steps, about
 # twice the largest error any sweep showed (dispersive: ~1.0e-4, from the
 # ADE recursions accumulating FP32 rounding).
 @pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
                                          ("dispersive", 2e-4)])
-def test_scene_fp32_error_budget(name, budget, kernel):
+def test_scene_fp32_error_budget(name, budget, opts):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)
     orc.run()
-    run = SceneRun(sc, precision=1, options={"kernel": kernel})
+    run = SceneRun(sc, precision=1, options=opts)
     run.run()
     errs = _fields_rel(run, orc)
     assert max(errs) <= budget, errs

@@ -114,7 +114,6 @@ struct xfd_engine {
   int kernel_mode = 0;
   int ichunk = 32;
   int march_ichunk = 16;  // planes per CTA of the marching split sweeps
-  int fm_tj = 8;          // warps per CTA of the fused marching sweep (FP32)
   bool tma_ready = false;
   TmaMaps tma[2]{};       // tensor maps over buffer 0 / 1 (and the class index)
   MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
@@ -258,7 +257,7 @@ constexpr int kMarchStagesF32 = 6, kMarchStagesF64 = 4;
 template <typename T>
 constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32; }
 constexpr int kFmStages = 4;
-constexpr int kFmTJ64 = 8;
+constexpr int kFmTJ = 8;
 
 inline bool is_fused(const xfd_engine* e) {
   return e->kernel_mode == 1 || e->kernel_mode == 2 || e->kernel_mode == 5;
@@ -336,7 +335,7 @@ xfd_status build_tma_maps(xfd_engine* e) {
   }
   // Fused marching sweep: E (TJ+1 rows) and H (TJ rows) boxes of width
   // 32 elements + 16 bytes, class boxes of 40.
-  const int fm_tj = sizeof(T) == 8 ? kFmTJ64 : e->fm_tj;
+  const int fm_tj = kFmTJ;
   for (int b = 0; b < 2; ++b) {
     const int W = 32 + 16 / (int)sizeof(T);
     for (int c = 0; c < 3; ++c) {
@@ -351,18 +350,12 @@ xfd_status build_tma_maps(xfd_engine* e) {
                                 e->cls, L, 40, fm_tj);
     if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (fmarch class): %d", (int)r);
   }
-  if constexpr (sizeof(T) == 8) {
-    CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, kFmTJ64, kFmStages>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     FmarchGeom<T, kFmTJ64>::smem(kFmStages)));
-  } else {
-    CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, 8, kFmStages>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     FmarchGeom<T, 8>::smem(kFmStages)));
-    CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, 16, kFmStages>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     FmarchGeom<T, 16>::smem(kFmStages)));
-  }
+  CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, kFmTJ, kFmStages, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   FmarchGeom<T, kFmTJ>::smem(kFmStages)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, kFmTJ, kFmStages, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   FmarchGeom<T, kFmTJ>::smem(kFmStages)));
   constexpr int S = sizeof(T) == 8 ? kStagesF64 : kStagesF32;
   CUDA_TRY(e, cudaFuncSetAttribute(k_fused_tma<T, kTJ, kTK, S>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem(S)));
@@ -385,6 +378,7 @@ FusedP<T> fused_params(xfd_engine* e, int in, int out) {
   }
   p.cls = e->cls;
   p.tab = static_cast<const T*>(e->tab);
+  p.n_classes = e->n_classes;
   for (int a = 0; a < 3; ++a) {
     p.fe[a] = static_cast<const T*>(e->fe[a]);
     p.fh[a] = static_cast<const T*>(e->fh[a]);
@@ -412,6 +406,49 @@ FusedP<T> fused_params(xfd_engine* e, int in, int out) {
   p.step = e->d_step;
   p.err = e->d_err;
   return p;
+}
+
+// Tile counts of the fused marching sweep along (k, j, chunks of i) and the
+// box of tile/chunk indices whose nodes meet no CPML layer of either phase.
+// A k tile bx holds nodes 31 bx - 1 .. 31 bx + 30, a j tile by holds
+// (TJ-1) by - 1 .. (TJ-1) by + TJ - 2, a chunk bz computes planes
+// max(bz ichunk - 1, 0) .. min((bz+1) ichunk, nx+1) - 1.
+void fmarch_split(const xfd_engine* e, int nt[3], int lo[3], int hi[3]) {
+  const Lat& L = e->L;
+  const int tj = kFmTJ;
+  nt[0] = (L.nz + 1 + 29) / 31;
+  nt[1] = (L.ny + 1 + tj - 2) / (tj - 1);
+  nt[2] = (L.nx + 1 + e->ichunk - 1) / e->ichunk;
+  const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
+  for (int g = 0; g < 3; ++g) {
+    const int m = axis_of[g];
+    auto range = [&](int b, int& a0, int& a1) {
+      if (g == 0) { a0 = 31 * b - 1; a1 = 31 * b + 30; }
+      else if (g == 1) { a0 = (tj - 1) * b - 1; a1 = (tj - 1) * b + tj - 2; }
+      else { a0 = std::max(b * e->ichunk - 1, 0); a1 = std::min((b + 1) * e->ichunk, L.nx + 1) - 1; }
+    };
+    auto is_free = [&](int b) {
+      int a0, a1;
+      range(b, a0, a1);
+      for (const auto& S : e->slabs) {
+        if (S.m != m) continue;
+        if (a0 < S.e_lo + S.n && S.e_lo <= a1) return false;
+        if (a0 < S.h_lo + S.n && S.h_lo <= a1) return false;
+      }
+      return true;
+    };
+    // Longest run of free indices.
+    int best_lo = 0, best_len = 0;
+    for (int b = 0; b < nt[g];) {
+      if (!is_free(b)) { ++b; continue; }
+      int c = b;
+      while (c < nt[g] && is_free(c)) ++c;
+      if (c - b > best_len) { best_lo = b; best_len = c - b; }
+      b = c;
+    }
+    lo[g] = best_lo;
+    hi[g] = best_lo + best_len;
+  }
 }
 
 template <typename T>
@@ -456,20 +493,20 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       FmarchP<T> fm{};
       fm.p = fused_params<T>(e, in, out);
       fm.m = e->fmaps[in];
-      const int tj = sizeof(T) == 8 ? kFmTJ64 : e->fm_tj;
-      const dim3 fgrd((unsigned)FmarchGeom<T, 8>::tiles_k(e->L.nz),
-                      (unsigned)((e->L.ny + 1 + tj - 2) / (tj - 1)),
-                      (unsigned)((e->L.nx + 1 + e->ichunk - 1) / e->ichunk));
-      if constexpr (sizeof(T) == 8) {
-        k_fmarch<T, kFmTJ64, kFmStages><<<fgrd, dim3(32, kFmTJ64, 1),
-                                          FmarchGeom<T, kFmTJ64>::smem(kFmStages), s>>>(fm);
-      } else if (tj == 16) {
-        k_fmarch<T, 16, kFmStages><<<fgrd, dim3(32, 16, 1), FmarchGeom<T, 16>::smem(kFmStages),
-                                     s>>>(fm);
-      } else {
-        k_fmarch<T, 8, kFmStages><<<fgrd, dim3(32, 8, 1), FmarchGeom<T, 8>::smem(kFmStages),
-                                    s>>>(fm);
+      int nt[3], lo[3], hi[3];
+      fmarch_split(e, nt, lo, hi);
+      for (int a = 0; a < 3; ++a) {
+        fm.box_lo[a] = lo[a];
+        fm.box_hi[a] = hi[a];
+        fm.org[a] = lo[a];
       }
+      const size_t sm = FmarchGeom<T, kFmTJ>::smem(kFmStages);
+      const dim3 blk(32, kFmTJ, 1);
+      if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2])
+        k_fmarch<T, kFmTJ, kFmStages, false>
+            <<<dim3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]), blk, sm, s>>>(fm);
+      fm.org[0] = fm.org[1] = fm.org[2] = 0;
+      k_fmarch<T, kFmTJ, kFmStages, true><<<dim3(nt[0], nt[1], nt[2]), blk, sm, s>>>(fm);
     } else if (e->kernel_mode == 2) {
       FusedTmaP<T> tp{};
       tp.p = fused_params<T>(e, in, out);
@@ -1326,7 +1363,6 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "kernel")) *value = e->kernel_mode;
   else if (!strcmp(name, "ichunk")) *value = e->ichunk;
   else if (!strcmp(name, "march_ichunk")) *value = e->march_ichunk;
-  else if (!strcmp(name, "fm_tj")) *value = e->fm_tj;
   else return fail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -1349,10 +1385,7 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096)
       return fail(e, XFD_ERR_INVALID_ARGUMENT, "march_ichunk range");
     e->march_ichunk = (int)value;
-  } else if (!strcmp(name, "fm_tj")) {
-    if (value != 8 && value != 16) return fail(e, XFD_ERR_INVALID_ARGUMENT, "fm_tj is 8 or 16");
-    e->fm_tj = (int)value;
-    e->tma_ready = false;
+
   } else {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
@@ -1366,6 +1399,11 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (!e) return 0;
   const bool fused = is_fused(e);
   int n = fused ? 2 : 3;  // sweep(s) + step counter
+  if (e->kernel_mode == 5) {
+    int nt[3], lo[3], hi[3];
+    fmarch_split(e, nt, lo, hi);
+    if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 1;  // CPML-free part
+  }
   if (e->have_tfsf) n += fused ? 2 : 4;
   if (e->ade_kind >= 0) n += fused ? 1 : 2;
   if (!e->lumped_h.empty()) n += 1;

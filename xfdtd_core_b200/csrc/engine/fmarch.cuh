@@ -24,7 +24,15 @@
 //    stage of plane q-1 is refilled), one between the H and E phases.
 //  * The CPML terms are compiled into a second form of the plane body that
 //    the CTA takes only on planes or tiles meeting a slab (a CTA-uniform
-//    test), so the interior runs without them.
+//    test), so the interior runs without them; the old psi values a node
+//    reads are loaded one phase ahead (H psi of plane i+1 after the H phase
+//    of plane i, E psi after the E phase), so their DRAM latency overlaps
+//    the compute of the other phase.  The TFSF H-face corrections are compiled
+//    in only for launches of a scene that has them.
+//  * The table rows of the NC most frequent material classes (the engine
+//    numbers classes by descending node count) are copied to shared memory
+//    once per CTA; rarer classes are read from global memory.  The shared
+//    copy keeps the lookups off L1, which the stage ring mostly occupies.
 //  * Box origins along k are rounded down to 16 bytes; the thread's column
 //    inside a box is offset by the remainder.  Out-of-range rows, columns
 //    and planes read as zeros and feed no update.
@@ -58,10 +66,17 @@ struct FmarchMaps {
   CUtensorMap cls;   // class index, box (TK+8) x TJ
 };
 
+// Work split: the tiles and plane chunks that meet no CPML layer form a box
+// in (tile k, tile j, chunk) index space, swept by the ANYCP = false form
+// of the kernel (no CPML code at all, fewer registers) with its grid offset
+// by `org`; the ANYCP = true form takes the full grid and its CTAs inside
+// the box [box_lo, box_hi) return at once.
 template <typename T>
 struct FmarchP {
   FusedP<T> p;
   FmarchMaps m;
+  int org[3];
+  int box_lo[3], box_hi[3];
 };
 
 template <typename T, int TJ>
@@ -81,7 +96,11 @@ struct FmarchGeom {
   static constexpr int TX_FULL = 3 * EB + 3 * HB + CB;
   static constexpr int TX_E = 3 * EB;
   static constexpr int XB = 2 * 2 * TJ * TK * (int)sizeof(T);  // H exchange [2][Hx,Hz][TJ][TK]
-  __host__ __device__ static constexpr int smem(int S) { return S * STAGE + pad(XB) + 8 * S; }
+  static constexpr int NC = 128;                             // classes cached in shared memory
+  static constexpr int TB = NC * 12 * (int)sizeof(T);
+  __host__ __device__ static constexpr int smem(int S) {
+    return S * STAGE + pad(XB) + TB + 8 * S;
+  }
   // Tiles: k0 = (TK-1) bx, j0 = (TJ-1) by.
   __host__ __device__ static constexpr int tiles_k(int nz) { return (nz + 1 + TK - 2) / (TK - 1); }
   __host__ __device__ static constexpr int tiles_j(int ny) { return (ny + 1 + TJ - 2) / (TJ - 1); }
@@ -106,19 +125,30 @@ __device__ __forceinline__ T tfsf_h_apply(const FusedP<T>& p, int c, int i, int 
   return h;
 }
 
-template <typename T, int TJ, int S>
-__global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ FmarchP<T> P) {
+// Resident CTAs per SM each form is compiled for (its register budget).
+template <typename T, bool ANYCP>
+constexpr int fmarch_min_blocks() {
+  return ANYCP ? (sizeof(T) == 8 ? 2 : 3) : (sizeof(T) == 8 ? 3 : 5);
+}
+
+template <typename T, int TJ, int S, bool ANYCP>
+__global__ void __launch_bounds__(TJ * 32, (fmarch_min_blocks<T, ANYCP>()))
+    k_fmarch(const __grid_constant__ FmarchP<T> P) {
   using G = FmarchGeom<T, TJ>;
   constexpr int TK = G::TK;
   extern __shared__ __align__(128) unsigned char smem[];
   const FusedP<T>& p = P.p;
   const Lat L = p.L;
   const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
+  const int bx = blockIdx.x + P.org[0], by = blockIdx.y + P.org[1], bz = blockIdx.z + P.org[2];
+  if (ANYCP && bx >= P.box_lo[0] && bx < P.box_hi[0] && by >= P.box_lo[1] &&
+      by < P.box_hi[1] && bz >= P.box_lo[2] && bz < P.box_hi[2])
+    return;  // swept by the CPML-free form
   // One thread reads the error word, so that the whole CTA returns or none.
   if (__syncthreads_or(tid == 0 && (*(volatile int*)p.err & 2))) return;
-  const int k0 = blockIdx.x * (TK - 1), j0 = blockIdx.y * (TJ - 1);
+  const int k0 = bx * (TK - 1), j0 = by * (TJ - 1);
   const int k = k0 - 1 + tk, j = j0 - 1 + tj;
-  const int i_lo = blockIdx.z * p.ichunk;
+  const int i_lo = bz * p.ichunk;
   const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
   const int i_first = i_lo > 0 ? i_lo - 1 : 0;
   const int n_planes = i_hi - i_first;                     // computed planes
@@ -131,7 +161,8 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
 
   StageRing ring;
   T* sX = reinterpret_cast<T*>(smem + S * G::STAGE);  // [2][2][TJ][TK]
-  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::pad(G::XB));
+  T* sT = reinterpret_cast<T*>(smem + S * G::STAGE + G::pad(G::XB));  // [NC][12]
+  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::pad(G::XB) + G::TB);
   auto ebox = [&](int s, int c) {
     return reinterpret_cast<const T*>(smem + s * G::STAGE + G::E_OFF + c * G::pad(G::EB));
   };
@@ -164,6 +195,10 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
   if (tid == 0)
     for (int q = 0; q < S && q < n_staged; ++q) issue(q);
   for (int q = 0; q < S && q < n_staged; ++q) ring.pending |= 1u << (q % S);
+  {
+    const int nt = min(p.n_classes, G::NC) * 12;
+    for (int x = tid; x < nt; x += TJ * TK) sT[x] = p.tab[x];
+  }
 
   // ---------------------------------------------------------- per thread
   const bool act = j >= 0 && j <= L.ny && k >= 0 && k <= L.nz;
@@ -189,19 +224,77 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
   const int xq = tj * TK + tk;          // node (j, k) in the exchange array
   T hy_p = T(0), hz_p = T(0);           // H_y, H_z of plane i-1
 
+  // CPML grading of the node's y and z layers, fixed for the march.
+  T ahy = 0, bhy = 0, ahz = 0, bhz = 0, aey = 0, bey = 0, aez = 0, bez = 0;
+  if (lyh >= 0) ahy = p.slab[1].a_h[qyh][lyh], bhy = p.slab[1].b_h[qyh][lyh];
+  if (lzh >= 0) ahz = p.slab[2].a_h[qzh][lzh], bhz = p.slab[2].b_h[qzh][lzh];
+  if (lye >= 0) aey = p.slab[1].a_e[qye][lye], bey = p.slab[1].b_e[qye][lye];
+  if (lze >= 0) aez = p.slab[2].a_e[qze][lze], bez = p.slab[2].b_e[qze][lze];
+  // psi cell offsets within a slab array on plane i: y slab [i][l][k],
+  // z slab [i][j][l], x slab [l][j][k].
+  auto off_y = [&](int i, int q, int l) { return ((long long)i * p.slab[1].n[q] + l) * KP + k; };
+  auto off_z = [&](int i, int q, int l) {
+    return ((long long)i * L.NY + j) * p.slab[2].n[q] + l;
+  };
+  auto off_x = [&](int l) { return (long long)l * PS + (long long)j * KP + k; };
+  // The psi values the node reads on plane i, in slot order
+  //   H: 0 Hx-y 1 Hx-z 2 Hy-x 3 Hy-z 4 Hz-x 5 Hz-y   (old psi_h)
+  //   E: 6 Ex-y 7 Ex-z 8 Ey-x 9 Ey-z 10 Ez-x 11 Ez-y (psi_e)
+  // Slabs store component A=(m+1)%3 at index 0 and B=(m+2)%3 at index 1.
+  auto load_psi_h = [&](int i, T (&v)[12]) {
+    const SlabAxisD<T>& X = p.slab[0];
+    const SlabAxisD<T>& Y = p.slab[1];
+    const SlabAxisD<T>& Z = p.slab[2];
+    int qxh = 0;
+    const int lxh = act ? layer_of(X, i, false, qxh) : -1;
+    v[0] = lyh >= 0 ? Y.psi_h_in[qyh][1][off_y(i, qyh, lyh)] : T(0);
+    v[5] = lyh >= 0 ? Y.psi_h_in[qyh][0][off_y(i, qyh, lyh)] : T(0);
+    v[1] = lzh >= 0 ? Z.psi_h_in[qzh][0][off_z(i, qzh, lzh)] : T(0);
+    v[3] = lzh >= 0 ? Z.psi_h_in[qzh][1][off_z(i, qzh, lzh)] : T(0);
+    v[2] = lxh >= 0 ? X.psi_h_in[qxh][0][off_x(lxh)] : T(0);
+    v[4] = lxh >= 0 ? X.psi_h_in[qxh][1][off_x(lxh)] : T(0);
+  };
+  auto load_psi_e = [&](int i, T (&v)[12]) {
+    const SlabAxisD<T>& X = p.slab[0];
+    const SlabAxisD<T>& Y = p.slab[1];
+    const SlabAxisD<T>& Z = p.slab[2];
+    int qxe = 0;
+    const int lxe = (own && i >= i_lo) ? layer_of(X, i, true, qxe) : -1;
+    const bool e_rd = i >= i_lo;  // E psi is read only on updated planes
+    v[6] = (e_rd && lye >= 0) ? Y.psi_e[qye][1][off_y(i, qye, lye)] : T(0);
+    v[11] = (e_rd && lye >= 0) ? Y.psi_e[qye][0][off_y(i, qye, lye)] : T(0);
+    v[7] = (e_rd && lze >= 0) ? Z.psi_e[qze][0][off_z(i, qze, lze)] : T(0);
+    v[9] = (e_rd && lze >= 0) ? Z.psi_e[qze][1][off_z(i, qze, lze)] : T(0);
+    v[8] = lxe >= 0 ? X.psi_e[qxe][0][off_x(lxe)] : T(0);
+    v[10] = lxe >= 0 ? X.psi_e[qxe][1][off_x(lxe)] : T(0);
+  };
+
   // One plane: H(i) (all threads), the row/column exchange, E(i) (owners).
-  auto plane = [&](int i, int q, int sc, int sn, bool iv, auto cp_tag) {
+  // CP: the CPML terms, with the old psi values of plane i in ps; each
+  // phase, once done, reloads its slots of ps for plane i+1 when `nxt`.
+  // TF: the TFSF H faces.
+  auto plane = [&](int i, int q, int sc, int sn, bool iv, T fhi, T fei, T (&ps)[12], bool nxt,
+                   auto cp_tag, auto tf_tag) {
     constexpr bool CP = decltype(cp_tag)::value;
+    constexpr bool TF = decltype(tf_tag)::value;
     const bool upd = i >= i_lo;  // E update and writes (plane i_lo-1 is H only)
-    const T fhi = iv ? p.fh[0][i] : T(0);
-    const T fei = p.fe[0][i];
     const long long o = i * PS + row;
     T* xb = sX + (q & 1) * (2 * TJ * TK);
     T hx = T(0), hy = T(0), hz = T(0);
     const T* r = nullptr;
+    const SlabAxisD<T>& X = p.slab[0];
+    const SlabAxisD<T>& Y = p.slab[1];
+    const SlabAxisD<T>& Z = p.slab[2];
+    int qxh = 0, qxe = 0;
+    const int lxh = CP ? layer_of(X, i, false, qxh) : -1;
+    const int lxe = CP ? layer_of(X, i, true, qxe) : -1;
+    T axh = 0, bxh = 0, axe = 0, bxe = 0;
+    if (CP && lxh >= 0) axh = X.a_h[qxh][lxh], bxh = X.b_h[qxh][lxh];
+    if (CP && lxe >= 0) axe = X.a_e[qxe][lxe], bxe = X.b_e[qxe][lxe];
     // ---------------------------------------------------------- H(i)
     if (act) {
-      r = p.tab + (size_t)cbox(sc)[cq] * 12;
+      const int cl = cbox(sc)[cq];
+      r = cl < G::NC ? sT + cl * 12 : p.tab + (size_t)cl * 12;
       const T* Ex = ebox(sc, 0);
       const T* Ey = ebox(sc, 1);
       const T* Ez = ebox(sc, 2);
@@ -215,26 +308,20 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
       const T dEx_j = ex_j - ex, dEy_i = ey_n - ey;  // Hz
       const bool main_rng = iv && jv && kv;
       const bool wr = own && upd;
-      int qx = 0;
-      const int lx = CP ? layer_of(p.slab[0], i, false, qx) : -1;
       if (jv && kv) {  // Hx: i <= nx, j < ny, k < nz
         const T ca = r[6], cb = r[7];
         T h = hbox(sc, 0)[eq];
         if (main_rng) h = ca * h + cb * (fhk * dEy_k - fhj * dEz_j);
-        if (p.tfh.enabled) h = tfsf_h_apply(p, 0, i, j, k, t, h);
+        if constexpr (TF) h = tfsf_h_apply(p, 0, i, j, k, t, h);
         if constexpr (CP) {
           if (lyh >= 0) {
-            const SlabAxisD<T>& A = p.slab[1];
-            const long long pi = ((long long)i * A.n[qyh] + lyh) * KP + k;
-            const T v = A.b_h[qyh][lyh] * A.psi_h_in[qyh][1][pi] + A.a_h[qyh][lyh] * dEz_j;
-            if (wr) A.psi_h_out[qyh][1][pi] = v;
+            const T v = bhy * ps[0] + ahy * dEz_j;
+            if (wr) Y.psi_h_out[qyh][1][off_y(i, qyh, lyh)] = v;
             h -= cb * v;
           }
           if (lzh >= 0) {
-            const SlabAxisD<T>& A = p.slab[2];
-            const long long pi = ((long long)i * L.NY + j) * A.n[qzh] + lzh;
-            const T v = A.b_h[qzh][lzh] * A.psi_h_in[qzh][0][pi] + A.a_h[qzh][lzh] * dEy_k;
-            if (wr) A.psi_h_out[qzh][0][pi] = v;
+            const T v = bhz * ps[1] + ahz * dEy_k;
+            if (wr) Z.psi_h_out[qzh][0][off_z(i, qzh, lzh)] = v;
             h += cb * v;
           }
         }
@@ -245,20 +332,16 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
         const T ca = r[8], cb = r[9];
         T h = hbox(sc, 1)[eq];
         if (main_rng) h = ca * h + cb * (fhi * dEz_i - fhk * dEx_k);
-        if (p.tfh.enabled) h = tfsf_h_apply(p, 1, i, j, k, t, h);
+        if constexpr (TF) h = tfsf_h_apply(p, 1, i, j, k, t, h);
         if constexpr (CP) {
-          if (lx >= 0) {
-            const SlabAxisD<T>& A = p.slab[0];
-            const long long pi = (long long)lx * PS + (long long)j * KP + k;
-            const T v = A.b_h[qx][lx] * A.psi_h_in[qx][0][pi] + A.a_h[qx][lx] * dEz_i;
-            if (wr) A.psi_h_out[qx][0][pi] = v;
+          if (lxh >= 0) {
+            const T v = bxh * ps[2] + axh * dEz_i;
+            if (wr) X.psi_h_out[qxh][0][off_x(lxh)] = v;
             h += cb * v;
           }
           if (lzh >= 0) {
-            const SlabAxisD<T>& A = p.slab[2];
-            const long long pi = ((long long)i * L.NY + j) * A.n[qzh] + lzh;
-            const T v = A.b_h[qzh][lzh] * A.psi_h_in[qzh][1][pi] + A.a_h[qzh][lzh] * dEx_k;
-            if (wr) A.psi_h_out[qzh][1][pi] = v;
+            const T v = bhz * ps[3] + ahz * dEx_k;
+            if (wr) Z.psi_h_out[qzh][1][off_z(i, qzh, lzh)] = v;
             h -= cb * v;
           }
         }
@@ -269,26 +352,25 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
         const T ca = r[10], cb = r[11];
         T h = hbox(sc, 2)[eq];
         if (main_rng) h = ca * h + cb * (fhj * dEx_j - fhi * dEy_i);
-        if (p.tfh.enabled) h = tfsf_h_apply(p, 2, i, j, k, t, h);
+        if constexpr (TF) h = tfsf_h_apply(p, 2, i, j, k, t, h);
         if constexpr (CP) {
-          if (lx >= 0) {
-            const SlabAxisD<T>& A = p.slab[0];
-            const long long pi = (long long)lx * PS + (long long)j * KP + k;
-            const T v = A.b_h[qx][lx] * A.psi_h_in[qx][1][pi] + A.a_h[qx][lx] * dEy_i;
-            if (wr) A.psi_h_out[qx][1][pi] = v;
+          if (lxh >= 0) {
+            const T v = bxh * ps[4] + axh * dEy_i;
+            if (wr) X.psi_h_out[qxh][1][off_x(lxh)] = v;
             h -= cb * v;
           }
           if (lyh >= 0) {
-            const SlabAxisD<T>& A = p.slab[1];
-            const long long pi = ((long long)i * A.n[qyh] + lyh) * KP + k;
-            const T v = A.b_h[qyh][lyh] * A.psi_h_in[qyh][0][pi] + A.a_h[qyh][lyh] * dEx_j;
-            if (wr) A.psi_h_out[qyh][0][pi] = v;
+            const T v = bhy * ps[5] + ahy * dEx_j;
+            if (wr) Y.psi_h_out[qyh][0][off_y(i, qyh, lyh)] = v;
             h += cb * v;
           }
         }
         hz = h;
         if (wr) p.out[5][o] = h;
       }
+    }
+    if constexpr (CP) {
+      if (nxt) load_psi_h(i + 1, ps);  // in flight through the E phase
     }
     // H_x, H_z for the row above; H_y, H_x from lane k-1 by shuffle.
     xb[xq] = hx;
@@ -304,22 +386,20 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
       const T dHz_j = hz - hz_j, dHy_k = hy - hy_k;  // Ex
       const T dHx_k = hx - hx_k, dHz_i = hz - hz_p;  // Ey
       const T dHy_i = hy - hy_p, dHx_j = hx - hx_j;  // Ez
-      int qx = 0;
-      const int lx = CP ? layer_of(p.slab[0], i, true, qx) : -1;
       if (iv) {  // Ex: i < nx; main 1 <= j < ny, 1 <= k < nz
         const T ca = r[0], cb = r[1];
         T e = ebox(sc, 0)[eq];
         if (jm && km) e = ca * e + cb * (fej * dHz_j - fek * dHy_k);
         if constexpr (CP) {
           if (lye >= 0) {
-            const SlabAxisD<T>& A = p.slab[1];
-            e += cb * psi_step(A.psi_e[qye][1] + ((long long)i * A.n[qye] + lye) * KP + k,
-                               A.b_e[qye][lye], A.a_e[qye][lye], dHz_j);
+            const T v = bey * ps[6] + aey * dHz_j;
+            Y.psi_e[qye][1][off_y(i, qye, lye)] = v;
+            e += cb * v;
           }
           if (lze >= 0) {
-            const SlabAxisD<T>& A = p.slab[2];
-            e -= cb * psi_step(A.psi_e[qze][0] + ((long long)i * L.NY + j) * A.n[qze] + lze,
-                               A.b_e[qze][lze], A.a_e[qze][lze], dHy_k);
+            const T v = bez * ps[7] + aez * dHy_k;
+            Z.psi_e[qze][0][off_z(i, qze, lze)] = v;
+            e -= cb * v;
           }
         }
         p.out[0][o] = e;
@@ -329,15 +409,15 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
         T e = ebox(sc, 1)[eq];
         if (im && km) e = ca * e + cb * (fek * dHx_k - fei * dHz_i);
         if constexpr (CP) {
-          if (lx >= 0) {
-            const SlabAxisD<T>& A = p.slab[0];
-            e -= cb * psi_step(A.psi_e[qx][0] + (long long)lx * PS + (long long)j * KP + k,
-                               A.b_e[qx][lx], A.a_e[qx][lx], dHz_i);
+          if (lxe >= 0) {
+            const T v = bxe * ps[8] + axe * dHz_i;
+            X.psi_e[qxe][0][off_x(lxe)] = v;
+            e -= cb * v;
           }
           if (lze >= 0) {
-            const SlabAxisD<T>& A = p.slab[2];
-            e += cb * psi_step(A.psi_e[qze][1] + ((long long)i * L.NY + j) * A.n[qze] + lze,
-                               A.b_e[qze][lze], A.a_e[qze][lze], dHx_k);
+            const T v = bez * ps[9] + aez * dHx_k;
+            Z.psi_e[qze][1][off_z(i, qze, lze)] = v;
+            e += cb * v;
           }
         }
         p.out[1][o] = e;
@@ -347,22 +427,32 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
         T e = ebox(sc, 2)[eq];
         if (im && jm) e = ca * e + cb * (fei * dHy_i - fej * dHx_j);
         if constexpr (CP) {
-          if (lx >= 0) {
-            const SlabAxisD<T>& A = p.slab[0];
-            e += cb * psi_step(A.psi_e[qx][1] + (long long)lx * PS + (long long)j * KP + k,
-                               A.b_e[qx][lx], A.a_e[qx][lx], dHy_i);
+          if (lxe >= 0) {
+            const T v = bxe * ps[10] + axe * dHy_i;
+            X.psi_e[qxe][1][off_x(lxe)] = v;
+            e += cb * v;
           }
           if (lye >= 0) {
-            const SlabAxisD<T>& A = p.slab[1];
-            e -= cb * psi_step(A.psi_e[qye][0] + ((long long)i * A.n[qye] + lye) * KP + k,
-                               A.b_e[qye][lye], A.a_e[qye][lye], dHx_j);
+            const T v = bey * ps[11] + aey * dHx_j;
+            Y.psi_e[qye][0][off_y(i, qye, lye)] = v;
+            e -= cb * v;
           }
         }
         p.out[2][o] = e;
       }
     }
+    if constexpr (CP) {
+      if (nxt) load_psi_e(i + 1, ps);  // in flight through the next H phase
+    }
     hy_p = hy;
     hz_p = hz;
+  };
+  auto run_plane = [&](int i, int q, int sc, int sn, bool iv, T fhi, T fei, T (&ps)[12],
+                       bool nxt, auto cp_tag) {
+    if (p.tfh.enabled)
+      plane(i, q, sc, sn, iv, fhi, fei, ps, nxt, cp_tag, std::true_type{});
+    else
+      plane(i, q, sc, sn, iv, fhi, fei, ps, nxt, cp_tag, std::false_type{});
   };
   // CPML layers of plane i along x (either phase), uniform over the CTA.
   auto x_cpml = [&](int i) {
@@ -373,10 +463,20 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
 
   bool ok = true;
   if (n_staged > 0) ok = ring.wait(0);
+  // x curl factors and the psi values of the next plane, loaded one plane ahead
+  T fhi_n = i_first < L.nx ? p.fh[0][i_first] : T(0);
+  T fei_n = p.fe[0][i_first];
+  T pf[12] = {};
+  int pf_i = -1;
   for (int q = 0; q < n_planes; ++q) {
     const int i = i_first + q;
     const bool iv = i < L.nx;
     const int sc = q % S, sn = (q + 1) % S;
+    const T fhi = fhi_n, fei = fei_n;
+    if (q + 1 < n_planes) {
+      fhi_n = i + 1 < L.nx ? p.fh[0][i + 1] : T(0);
+      fei_n = p.fe[0][i + 1];
+    }
     if (ok && iv) ok = ring.wait(sn);  // E of plane i+1
     if (__syncthreads_or(!ok)) {
       ok = false;
@@ -390,16 +490,19 @@ __global__ void __launch_bounds__(TJ * 32) k_fmarch(const __grid_constant__ Fmar
       }
       ring.pending |= 1u << ((q - 1) % S);
     }
-    if (act && q + 1 < n_planes) {
-      // Warm L1 with the class-table row of the next plane (its stage is in).
-      const T* nr = p.tab + (size_t)cbox(sn)[cq] * 12;
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(nr));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(nr + 11));
+    if constexpr (ANYCP) {
+      if (tile_cpml || x_cpml(i)) {  // CTA-uniform
+        if (pf_i != i) {
+          load_psi_h(i, pf);
+          load_psi_e(i, pf);
+        }
+        const bool nxt = q + 1 < n_planes && (tile_cpml || x_cpml(i + 1));
+        run_plane(i, q, sc, sn, iv, fhi, fei, pf, nxt, std::true_type{});
+        pf_i = nxt ? i + 1 : -1;
+        continue;
+      }
     }
-    if (tile_cpml || x_cpml(i))  // CTA-uniform
-      plane(i, q, sc, sn, iv, std::true_type{});
-    else
-      plane(i, q, sc, sn, iv, std::false_type{});
+    run_plane(i, q, sc, sn, iv, fhi, fei, pf, false, std::false_type{});
   }
   if (!ok) {
     if (tid == 0) atomicOr(p.err, 2);

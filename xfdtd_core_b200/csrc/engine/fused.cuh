@@ -59,6 +59,7 @@ struct FusedP {
   T* out[6];
   const uint16_t* cls;
   const T* tab;
+  int n_classes;
   const T* fe[3];
   const T* fh[3];
   SlabAxisD<T> slab[3];
