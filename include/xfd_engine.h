@@ -208,9 +208,13 @@ xfd_status xfd_sync(xfd_engine* e);
 int64_t xfd_current_step(const xfd_engine* e);
 
 /* Engine options: "graph" (0/1, default 1), "graph_chunk" (steps per graph,
- * default 32), "kernel" (0 = split H/E sweeps, 1 = fused H-then-E sweep,
- * 2 = fused sweep with its per-plane inputs staged by TMA), "ichunk" (planes
- * per CTA of a fused sweep, default 32). */
+ * default 32), "kernel" (the Yee sweep: 0 = split H/E sweeps, 1 = fused
+ * H-then-E sweep, 2 = fused sweep with its per-plane inputs staged by TMA,
+ * 3 = split sweeps marching along x, 4 = the same with TMA-staged planes,
+ * 5 = fused marching sweep with overlapped tiles and TMA-staged planes),
+ * "ichunk" (planes per CTA of the fused sweeps, default 32), "march_ichunk"
+ * (planes per CTA of the split marching sweeps, default 16).  Every sweep
+ * computes the same update; they differ in speed only. */
 xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value);
 /* Current value of an option of xfd_set_option. */
 xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value);
