@@ -230,6 +230,55 @@ int32_t xfd_launches_per_step(const xfd_engine* e);
  * written once, class index, CPML auxiliaries) -- the roofline numerator. */
 int64_t xfd_stencil_bytes_per_step(const xfd_engine* e);
 
+/* ---- Allocation-free NF2FF step -------------------------------------------
+ * No counterpart in the reference: an addition of this library for callers
+ * that cannot allocate device memory -- an FDTD loop embedded in a larger GPU
+ * application whose device memory is all owned by its own pool or a fixed
+ * arena, where a cudaMalloc would fail or would synchronise the device in the
+ * middle of the caller's time loop.  It folds ONE time step of the Huygens-
+ * surface fields into the NF2FF frequency-domain surface currents, exactly
+ * what the engine's NF2FF does per step (xfd_set_nf2ff), but on the caller's
+ * arrays and without allocating: it calls no cudaMalloc or cudaFree and no
+ * allocating library routine.  The per-step samples go to a fixed scratch
+ * array of 4 x XFD_NF2FF_STATIC_MAX_POINTS doubles (4 MiB) compiled into the
+ * library, which every GPU that loads the library holds until exit.
+ *   - The first call on a device looks up that array's device address
+ *     (cudaGetSymbolAddress) with the device current; make that first call
+ *     before any stream capture.
+ *   - All calls on a device share the one scratch array: calls whose kernels
+ *     overlap on the GPU (different streams or host threads) race and corrupt
+ *     each other's samples -- serialise them.
+ *   - Nothing in the scratch has to start at zero (each call writes every
+ *     entry it reads).  `acc` is accumulated into: zero it before the first
+ *     step, as the engine zeroes its own accumulator.
+ *   - Surfaces of more than XFD_NF2FF_STATIC_MAX_POINTS points, or more than
+ *     XFD_NF2FF_STATIC_MAX_FREQ frequencies, are rejected with
+ *     XFD_ERR_UNSUPPORTED / XFD_ERR_INVALID_ARGUMENT and a message in
+ *     xfd_last_error(NULL); nothing is launched then. */
+#define XFD_NF2FF_STATIC_MAX_POINTS 131072
+#define XFD_NF2FF_STATIC_MAX_FREQ 1024
+
+typedef struct {
+  int32_t nx, ny, nz;     /* grid cells */
+  int32_t precision;      /* element type of the fields: XFD_FP64 or XFD_FP32 */
+  const void* fields[6];  /* device arrays Ex Ey Ez Hx Hy Hz in the reference
+                             component shapes, C order (Ex: nx x (ny+1) x (nz+1),
+                             Hx: (nx+1) x ny x nz, ...) */
+  int32_t n_freq;
+  int32_t task_s[6][3];   /* Huygens faces, as in xfd_nf2ff_desc */
+  int32_t task_e[6][3];
+  const double* te;       /* device, n_freq x n_steps complex (re, im): E-time phasors */
+  const double* th;       /* device, n_freq x n_steps complex: H-time phasors */
+  int64_t n_steps;
+  int64_t step;           /* time index t of this step, 0 <= step < n_steps */
+  double scale;
+  double* acc;            /* device, n_freq x 4 x P complex, accumulated in place
+                             (P = points of the six faces, face by face) */
+} xfd_nf2ff_step_desc;
+
+/* Queues the step on `stream` (a cudaStream_t; NULL = legacy default). */
+xfd_status xfd_nf2ff_step_static(const xfd_nf2ff_step_desc* d, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

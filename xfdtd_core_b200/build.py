@@ -61,7 +61,8 @@ def build_engine(force: bool = False, verbose: bool = False) -> str:
         return ENGINE_LIB
     nvcc = os.path.join(_cuda_home(), "bin", "nvcc")
     cmd = [nvcc, *NVCC_FLAGS, "-I" + INCLUDE, "-o", ENGINE_LIB + ".tmp",
-           os.path.join(ENGINE_SRC, "engine.cu"), "-lcudart"]
+           os.path.join(ENGINE_SRC, "engine.cu"), os.path.join(ENGINE_SRC, "nf2ff_static.cu"),
+           "-lcudart"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.check_call(cmd)

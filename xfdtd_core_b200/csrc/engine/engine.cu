@@ -836,6 +836,9 @@ const char* xfd_last_error(const xfd_engine* e) {
   return e ? e->err.c_str() : g_create_error.c_str();
 }
 
+// Message for xfd_last_error(NULL) from entry points without an engine.
+void xfd_internal_set_error(const char* msg) { g_create_error = msg; }
+
 xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t n_classes,
                                     const uint16_t* lattice_class) {
   if (!e || !table || !lattice_class || n_classes <= 0 || n_classes > 65536)

@@ -53,6 +53,15 @@ class Nf2ffDesc(ctypes.Structure):
                 ("task_e", (_i32 * 3) * 6), ("te", _dp), ("th", _dp), ("scale", ctypes.c_double)]
 
 
+class Nf2ffStepDesc(ctypes.Structure):
+    """xfd_nf2ff_step_desc: one allocation-free NF2FF step on caller arrays."""
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("precision", _i32),
+                ("fields", ctypes.c_void_p * 6), ("n_freq", _i32),
+                ("task_s", (_i32 * 3) * 6), ("task_e", (_i32 * 3) * 6),
+                ("te", ctypes.c_void_p), ("th", ctypes.c_void_p), ("n_steps", _i64),
+                ("step", _i64), ("scale", ctypes.c_double), ("acc", ctypes.c_void_p)]
+
+
 class EngineError(RuntimeError):
     pass
 
@@ -100,6 +109,7 @@ def load(build_if_missing: bool = True):
         "xfd_current_step": ([vp], _i64),
         "xfd_set_option": ([vp, ctypes.c_char_p, _i64], ctypes.c_int),
         "xfd_get_option": ([vp, ctypes.c_char_p, ctypes.POINTER(_i64)], ctypes.c_int),
+        "xfd_nf2ff_step_static": ([ctypes.POINTER(Nf2ffStepDesc), vp], ctypes.c_int),
         "xfd_stream": ([vp], vp),
         "xfd_launches_per_step": ([vp], _i32),
         "xfd_stencil_bytes_per_step": ([vp], _i64),
@@ -119,7 +129,7 @@ def exported_symbols() -> List[str]:
             "xfd_set_ade", "xfd_set_nf2ff", "xfd_get_nf2ff", "xfd_add_movie",
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
-            "xfd_get_option", "xfd_stream", "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
+            "xfd_get_option", "xfd_nf2ff_step_static", "xfd_stream", "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
 
 
 def _f64(a) -> np.ndarray:
@@ -315,3 +325,29 @@ class Engine:
         self._check(self.L.xfd_get_nf2ff(self.h, _p(out), cnt.value, ctypes.byref(cnt)),
                     "get_nf2ff")
         return out[0::2] + 1j * out[1::2]
+
+
+def nf2ff_step_static(n, precision: int, fields, tasks, te_dev: int, th_dev: int, n_freq: int,
+                      n_steps: int, step: int, scale: float, acc_dev: int, stream: int = 0):
+    """Folds one time step of the Huygens-surface fields into `acc_dev` through
+    xfd_nf2ff_step_static, the entry point that allocates no device memory
+    (for callers whose device memory belongs to another allocator).  `fields`
+    are six device addresses of the component arrays in the reference shapes;
+    te_dev/th_dev/acc_dev are device addresses of complex128 arrays."""
+    L = load()
+    d = Nf2ffStepDesc()
+    d.nx, d.ny, d.nz = (int(x) for x in n)
+    d.precision = int(precision)
+    for c in range(6):
+        d.fields[c] = int(fields[c])
+    d.n_freq = int(n_freq)
+    for f in range(6):
+        t = tasks[f]
+        for a in range(3):
+            d.task_s[f][a] = 0 if t is None else int(t[0][a])
+            d.task_e[f][a] = 0 if t is None else int(t[1][a])
+    d.te, d.th, d.acc = int(te_dev), int(th_dev), int(acc_dev)
+    d.n_steps, d.step, d.scale = int(n_steps), int(step), float(scale)
+    st = L.xfd_nf2ff_step_static(ctypes.byref(d), ctypes.c_void_p(int(stream)))
+    if st != 0:
+        raise EngineError(f"xfd_nf2ff_step_static: {L.xfd_last_error(None).decode()} (status {st})")
