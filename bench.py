@@ -282,7 +282,8 @@ def main():
     ap.add_argument("--kernel", type=int, default=None,
                     help="engine sweep: 0 split, 1 fused, 2 fused with TMA pipeline, "
                          "3 split marching, 4 split marching with TMA pipeline, "
-                         "5 fused marching with TMA pipeline")
+                         "5 fused marching with TMA pipeline, 6 = 5 with a two-nodes-per-thread "
+                         "interior")
     ap.add_argument("--ichunk", type=int, default=None, help="planes per CTA, fused sweeps")
     ap.add_argument("--march-ichunk", type=int, default=None,
                     help="planes per CTA, split marching sweeps")
@@ -337,7 +338,8 @@ def main():
              2: "fused H-then-E sweep, TMA-staged planes",
              3: "split H and E sweeps marching along x",
              4: "split H and E sweeps marching along x, TMA-staged planes",
-             5: "fused H-then-E sweep marching along x, overlapped tiles, TMA-staged planes"
+             5: "fused H-then-E sweep marching along x, overlapped tiles, TMA-staged planes",
+             6: "fused marching sweep, two nodes per thread in the CPML-free interior"
              }[kmode.value]
     bytes32 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h32)))
     sampler = ClockSampler(local)

@@ -26,7 +26,8 @@ def _fields_rel(run, orc):
 SWEEPS = [pytest.param({"kernel": 0}, id="split"), pytest.param({"kernel": 1}, id="fused"),
           pytest.param({"kernel": 2}, id="fused-tma"), pytest.param({"kernel": 3}, id="march"),
           pytest.param({"kernel": 4}, id="march-tma"), pytest.param({"kernel": 5}, id="fmarch"),
-          pytest.param({"kernel": 5, "ichunk": 4}, id="fmarch-ichunk4")]
+          pytest.param({"kernel": 5, "ichunk": 4}, id="fmarch-ichunk4"),
+          pytest.param({"kernel": 6, "ichunk": 4}, id="fvec-ichunk4")]
 
 
 @pytest.mark.parametrize("opts", SWEEPS)

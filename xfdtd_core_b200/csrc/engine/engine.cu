@@ -22,6 +22,7 @@
 #include "march.cuh"
 #include "march_tma.cuh"
 #include "fmarch.cuh"
+#include "fvec.cuh"
 #include "kernels.cuh"
 #include "xfd_engine.h"
 
@@ -110,7 +111,8 @@ struct xfd_engine {
   bool use_graph = true;
   int graph_chunk = 32;
   // 0 split, 1 fused, 2 fused + TMA, 3 split marching, 4 split marching + TMA,
-  // 5 fused marching (overlapped tiles) + TMA
+  // 5 fused marching (overlapped tiles) + TMA, 6 = 5 with a two-nodes-per-
+  // thread form on the CPML-free interior
   int kernel_mode = 0;
   int ichunk = 32;
   int march_ichunk = 16;  // planes per CTA of the marching split sweeps
@@ -118,6 +120,7 @@ struct xfd_engine {
   TmaMaps tma[2]{};       // tensor maps over buffer 0 / 1 (and the class index)
   MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
+  FvecMaps fvmaps[2]{};   // tensor maps of its two-nodes-per-thread interior form
   cudaGraphExec_t graph_exec = nullptr;
   int graph_cur = -1;
   long long graph_len = 0;
@@ -258,9 +261,16 @@ template <typename T>
 constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32; }
 constexpr int kFmStages = 4;
 constexpr int kFmTJ = 8;
+template <typename T>
+constexpr int kFvStages() { return sizeof(T) == 8 ? 3 : 4; }
 
 inline bool is_fused(const xfd_engine* e) {
-  return e->kernel_mode == 1 || e->kernel_mode == 2 || e->kernel_mode == 5;
+  return e->kernel_mode == 1 || e->kernel_mode == 2 || e->kernel_mode == 5 ||
+         e->kernel_mode == 6;
+}
+inline bool uses_tma(const xfd_engine* e) {
+  return e->kernel_mode == 2 || e->kernel_mode == 4 || e->kernel_mode == 5 ||
+         e->kernel_mode == 6;
 }
 
 // Encodes one 3-D tiled map over the (nz+1, ny+1, nx+1) lattice of `base`.
@@ -350,6 +360,24 @@ xfd_status build_tma_maps(xfd_engine* e) {
                                 e->cls, L, 40, fm_tj);
     if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (fmarch class): %d", (int)r);
   }
+  // Two-nodes-per-thread interior form: boxes (64 elements + 16 bytes) wide.
+  for (int b = 0; b < 2; ++b) {
+    const int W = 64 + 16 / (int)sizeof(T);
+    for (int c = 0; c < 3; ++c) {
+      CUresult r = encode_lattice(encode, &e->fvmaps[b].e[c], dt, sizeof(T), e->fbuf[b][c], L, W,
+                                  kFmTJ + 1);
+      if (r == CUDA_SUCCESS)
+        r = encode_lattice(encode, &e->fvmaps[b].h[c], dt, sizeof(T), e->fbuf[b][3 + c], L, W,
+                           kFmTJ);
+      if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (fvec %d): %d", c, (int)r);
+    }
+    CUresult r = encode_lattice(encode, &e->fvmaps[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                                e->cls, L, 72, kFmTJ);
+    if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (fvec class): %d", (int)r);
+  }
+  CUDA_TRY(e, cudaFuncSetAttribute(k_fvec<T, kFmTJ, kFvStages<T>()>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   FvecGeom<T, kFmTJ>::smem(kFvStages<T>())));
   CUDA_TRY(e, cudaFuncSetAttribute(k_fmarch<T, kFmTJ, kFmStages, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    FmarchGeom<T, kFmTJ>::smem(kFmStages)));
@@ -489,24 +517,53 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     const dim3 grd((unsigned)((e->L.nz + 1 + kTK - 1) / kTK),
                    (unsigned)((e->L.ny + 1 + kTJ - 1) / kTJ),
                    (unsigned)((e->L.nx + 1 + e->ichunk - 1) / e->ichunk));
-    if (e->kernel_mode == 5) {
+    if (e->kernel_mode == 5 || e->kernel_mode == 6) {
       FmarchP<T> fm{};
       fm.p = fused_params<T>(e, in, out);
       fm.m = e->fmaps[in];
       int nt[3], lo[3], hi[3];
       fmarch_split(e, nt, lo, hi);
-      for (int a = 0; a < 3; ++a) {
-        fm.box_lo[a] = lo[a];
-        fm.box_hi[a] = hi[a];
-        fm.org[a] = lo[a];
+      if (e->kernel_mode == 6) {
+        // The interior in pairs of k tiles for the two-nodes-per-thread form;
+        // the CPML form sweeps everything outside those pairs.
+        const int v0 = (lo[0] + 1) / 2, v1 = hi[0] / 2;
+        if (v1 > v0 && hi[1] > lo[1] && hi[2] > lo[2]) {
+          FvecP<T> fv{};
+          fv.p = fm.p;
+          fv.m = e->fvmaps[in];
+          fv.org[0] = v0;
+          fv.org[1] = lo[1];
+          fv.org[2] = lo[2];
+          constexpr int FS = kFvStages<T>();
+          k_fvec<T, kFmTJ, FS><<<dim3(v1 - v0, hi[1] - lo[1], hi[2] - lo[2]), dim3(32, kFmTJ, 1),
+                                 FvecGeom<T, kFmTJ>::smem(FS), s>>>(fv);
+          lo[0] = 2 * v0;
+          hi[0] = 2 * v1;
+        } else {
+          hi[0] = lo[0];  // no interior form: the CPML form sweeps all
+        }
+        for (int a = 0; a < 3; ++a) {
+          fm.box_lo[a] = lo[a];
+          fm.box_hi[a] = hi[a];
+          fm.org[a] = 0;
+        }
+        k_fmarch<T, kFmTJ, kFmStages, true>
+            <<<dim3(nt[0], nt[1], nt[2]), dim3(32, kFmTJ, 1), FmarchGeom<T, kFmTJ>::smem(kFmStages),
+               s>>>(fm);
+      } else {
+        for (int a = 0; a < 3; ++a) {
+          fm.box_lo[a] = lo[a];
+          fm.box_hi[a] = hi[a];
+          fm.org[a] = lo[a];
+        }
+        const size_t sm = FmarchGeom<T, kFmTJ>::smem(kFmStages);
+        const dim3 blk(32, kFmTJ, 1);
+        if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2])
+          k_fmarch<T, kFmTJ, kFmStages, false>
+              <<<dim3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]), blk, sm, s>>>(fm);
+        fm.org[0] = fm.org[1] = fm.org[2] = 0;
+        k_fmarch<T, kFmTJ, kFmStages, true><<<dim3(nt[0], nt[1], nt[2]), blk, sm, s>>>(fm);
       }
-      const size_t sm = FmarchGeom<T, kFmTJ>::smem(kFmStages);
-      const dim3 blk(32, kFmTJ, 1);
-      if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2])
-        k_fmarch<T, kFmTJ, kFmStages, false>
-            <<<dim3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]), blk, sm, s>>>(fm);
-      fm.org[0] = fm.org[1] = fm.org[2] = 0;
-      k_fmarch<T, kFmTJ, kFmStages, true><<<dim3(nt[0], nt[1], nt[2]), blk, sm, s>>>(fm);
     } else if (e->kernel_mode == 2) {
       FusedTmaP<T> tp{};
       tp.p = fused_params<T>(e, in, out);
@@ -611,7 +668,7 @@ long long pattern_period(const xfd_engine* e) {
 xfd_status ensure_ready(xfd_engine* e) {
   if (!e->have_classes) return fail(e, XFD_ERR_STATE, "material classes not set");
   if (!e->have_curl) return fail(e, XFD_ERR_STATE, "curl factors not set");
-  if ((e->kernel_mode == 2 || e->kernel_mode == 4 || e->kernel_mode == 5) && !e->tma_ready) {
+  if (uses_tma(e) && !e->tma_ready) {
     xfd_status st = e->precision == XFD_FP64 ? build_tma_maps<double>(e) : build_tma_maps<float>(e);
     if (st != XFD_OK) return st;
   }
@@ -1378,7 +1435,7 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "graph_chunk range");
     e->graph_chunk = (int)value;
   } else if (!strcmp(name, "kernel")) {
-    if (value < 0 || value > 5)
+    if (value < 0 || value > 6)
       return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
     e->kernel_mode = (int)value;
   } else if (!strcmp(name, "ichunk")) {
