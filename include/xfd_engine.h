@@ -210,8 +210,9 @@ int64_t xfd_current_step(const xfd_engine* e);
 /* Engine options: "graph" (0/1, default 1), "graph_chunk" (steps per graph,
  * default 32), "kernel" (the Yee sweep: 0 = split H/E sweeps, 1 = fused
  * H-then-E sweep, 2 = fused sweep with its per-plane inputs staged by TMA,
- * 3 = split sweeps marching along x, 4 = the same with TMA-staged planes,
- * 5 = fused marching sweep with overlapped tiles and TMA-staged planes),
+ * 3 = split sweeps marching along x, 4 = the same with TMA-staged planes
+ * (default), 5 = fused marching sweep with overlapped tiles and TMA-staged
+ * planes, 6 = 5 with a two-nodes-per-thread form in the CPML-free interior),
  * "ichunk" (planes per CTA of the fused sweeps, default 32), "march_ichunk"
  * (planes per CTA of the split marching sweeps, default 16).  Every sweep
  * computes the same update; they differ in speed only. */

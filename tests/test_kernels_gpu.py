@@ -64,14 +64,15 @@ def test_yee_large_tile_crossing_fp32(kernel):
     assert max(errs) <= 1e-5, errs
 
 
+@pytest.mark.parametrize("kernel", [4, 5, 6])
 @pytest.mark.parametrize("ichunk", [3, 4])
 @pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, 1e-5)], ids=["fp64", "fp32"])
-def test_interior_pair_form(ichunk, precision, tol):
+def test_interior_forms(kernel, ichunk, precision, tol):
     """A grid long enough along z that the CPML-free interior holds whole
-    pairs of k tiles, so the two-nodes-per-thread form (kernel 6) sweeps part
-    of it next to the CPML form."""
+    tiles (pairs of tiles for kernel 6), so the CPML-free forms of the
+    marching sweeps run next to their CPML forms."""
     _compare(KernelCase(n=(24, 20, 140), seed=16), steps=3, precision=precision, tol=tol,
-             kernel=(6, ichunk))
+             kernel=(kernel, ichunk))
 
 
 @pytest.mark.parametrize("kernel", KERNELS)

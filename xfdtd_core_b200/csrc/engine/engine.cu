@@ -113,7 +113,7 @@ struct xfd_engine {
   // 0 split, 1 fused, 2 fused + TMA, 3 split marching, 4 split marching + TMA,
   // 5 fused marching (overlapped tiles) + TMA, 6 = 5 with a two-nodes-per-
   // thread form on the CPML-free interior
-  int kernel_mode = 0;
+  int kernel_mode = 4;
   int ichunk = 32;
   int march_ichunk = 16;  // planes per CTA of the marching split sweeps
   bool tma_ready = false;
@@ -388,9 +388,13 @@ xfd_status build_tma_maps(xfd_engine* e) {
   CUDA_TRY(e, cudaFuncSetAttribute(k_fused_tma<T, kTJ, kTK, S>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem(S)));
   constexpr int MS = march_stages<T>();
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
   e->tma_ready = true;
   return XFD_OK;
@@ -466,6 +470,39 @@ void fmarch_split(const xfd_engine* e, int nt[3], int lo[3], int hi[3]) {
       return true;
     };
     // Longest run of free indices.
+    int best_lo = 0, best_len = 0;
+    for (int b = 0; b < nt[g];) {
+      if (!is_free(b)) { ++b; continue; }
+      int c = b;
+      while (c < nt[g] && is_free(c)) ++c;
+      if (c - b > best_len) { best_lo = b; best_len = c - b; }
+      b = c;
+    }
+    lo[g] = best_lo;
+    hi[g] = best_lo + best_len;
+  }
+}
+
+// The box of (k tile of 32, j tile of 8, chunk of march_ichunk planes) of
+// the split marching sweeps whose nodes lie in no CPML layer of either phase.
+void march_split(const xfd_engine* e, int lo[3], int hi[3]) {
+  const Lat& L = e->L;
+  const int nt[3] = {(L.nz + 1 + 31) / 32, (L.ny + 1 + 7) / 8,
+                     (L.nx + 1 + e->march_ichunk - 1) / e->march_ichunk};
+  const int size[3] = {32, 8, e->march_ichunk};
+  const int n_nodes[3] = {L.nz + 1, L.ny + 1, L.nx + 1};
+  const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
+  for (int g = 0; g < 3; ++g) {
+    const int m = axis_of[g];
+    auto is_free = [&](int b) {
+      const int a0 = b * size[g], a1 = std::min((b + 1) * size[g], n_nodes[g]) - 1;
+      for (const auto& S : e->slabs) {
+        if (S.m != m) continue;
+        if (a0 < S.e_lo + S.n && S.e_lo <= a1) return false;
+        if (a0 < S.h_lo + S.n && S.h_lo <= a1) return false;
+      }
+      return true;
+    };
     int best_lo = 0, best_len = 0;
     for (int b = 0; b < nt[g];) {
       if (!is_free(b)) { ++b; continue; }
@@ -593,9 +630,29 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
                    (unsigned)(e->L.nx + 1));
     const dim3 grd_m(grd.x, grd.y,
                      (unsigned)((e->L.nx + 1 + mp.ichunk - 1) / std::max(1, mp.ichunk)));
+    // The CPML-free box of (k tile, j tile, chunk) for the TMA marching sweeps.
+    int mlo[3] = {0, 0, 0}, mhi[3] = {0, 0, 0};
+    bool mbox = false;
+    if (march_tma) {
+      march_split(e, mlo, mhi);
+      mbox = mhi[0] > mlo[0] && mhi[1] > mlo[1] && mhi[2] > mlo[2];
+      for (int a = 0; a < 3; ++a) {
+        mtp.box_lo[a] = mbox ? mlo[a] : 0;
+        mtp.box_hi[a] = mbox ? mhi[a] : 0;
+      }
+    }
+    const size_t msm = MarchGeom<T, 8, 32>::smem(MS);
+    auto launch_march = [&](auto kfree, auto kcp) {
+      if (mbox) {
+        MarchTmaP<T> q = mtp;
+        for (int a = 0; a < 3; ++a) q.org[a] = mlo[a];
+        kfree<<<dim3(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]), blk, msm, s>>>(q);
+      }
+      kcp<<<grd_m, blk, msm, s>>>(mtp);
+    };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma)
-      k_march_h_tma<T, 8, 32, MS><<<grd_m, blk, MarchGeom<T, 8, 32>::smem(MS), s>>>(mtp);
+      launch_march(k_march_h_tma<T, 8, 32, MS, false>, k_march_h_tma<T, 8, 32, MS, true>);
     else if (march)
       k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
@@ -611,7 +668,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
     if (march_tma)
-      k_march_e_tma<T, 8, 32, MS><<<grd_m, blk, MarchGeom<T, 8, 32>::smem(MS), s>>>(mtp);
+      launch_march(k_march_e_tma<T, 8, 32, MS, false>, k_march_e_tma<T, 8, 32, MS, true>);
     else if (march)
       k_march_e<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
@@ -1459,10 +1516,16 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (!e) return 0;
   const bool fused = is_fused(e);
   int n = fused ? 2 : 3;  // sweep(s) + step counter
-  if (e->kernel_mode == 5) {
+  if (e->kernel_mode == 5 || e->kernel_mode == 6) {
     int nt[3], lo[3], hi[3];
     fmarch_split(e, nt, lo, hi);
+    if (e->kernel_mode == 6) lo[0] = 2 * ((lo[0] + 1) / 2), hi[0] = 2 * (hi[0] / 2);
     if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 1;  // CPML-free part
+  }
+  if (e->kernel_mode == 4) {
+    int lo[3], hi[3];
+    march_split(e, lo, hi);
+    if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 2;  // CPML-free H and E
   }
   if (e->have_tfsf) n += fused ? 2 : 4;
   if (e->ade_kind >= 0) n += fused ? 1 : 2;

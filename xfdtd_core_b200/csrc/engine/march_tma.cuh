@@ -1,6 +1,7 @@
 // Marching split sweeps with TMA-staged planes.  Same arithmetic, ranges and
 // correction order as k_march_h / k_march_e (march.cuh); the difference is
-// how the per-plane inputs arrive: one thread of the CTA issues TMA tile
+// how the per-plane inputs arrive (and that the CPML forms load the old psi
+// values of a node one plane ahead): one thread of the CTA issues TMA tile
 // loads (cp.async.bulk.tensor, no multicast) of the planes S-1 ahead into a
 // ring of S shared-memory stages, each completing on its own mbarrier, so
 // that a CTA keeps several planes of DRAM reads in flight while it computes.
@@ -33,11 +34,16 @@ struct MarchMaps {
   CUtensorMap cls;      // box TK x TJ (uint16)
 };
 
+// Work split as for the fused marching sweep: CP = false forms sweep the
+// box of tiles and chunks whose nodes lie in no CPML layer, with their grid
+// offset by `org`; CP = true forms take the full grid and skip that box.
 template <typename T>
 struct MarchTmaP {
   MarchP<T> p;
   MarchMaps m;
   int* err;
+  int org[3];
+  int box_lo[3], box_hi[3];
 };
 
 template <typename T, int TJ, int TK>
@@ -57,6 +63,15 @@ struct MarchGeom {
   static constexpr int TX_HALO = 3 * HALO_B;
   __host__ __device__ static constexpr int smem(int S) { return S * STAGE + 8 * S; }
 };
+
+// CPML psi update from an already loaded old value: psi = b psi + a diff,
+// stored in place.
+template <typename T>
+__device__ __forceinline__ T psi_upd(T* ps, T old, T b, T a, T diff) {
+  const T v = b * old + a * diff;
+  *ps = v;
+  return v;
+}
 
 // Ring bookkeeping shared by the TMA sweeps: bounded stage waits and the
 // drain on failure.  All threads keep identical copies of parity/pending.
@@ -97,18 +112,22 @@ struct StageRing {
 // H sweep.  Planes q = 0 .. n_planes of the chunk are staged (plane n_planes
 // is i_hi, E only, when i_hi <= nx); plane q lives in stage q % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S>
+template <typename T, int TJ, int TK, int S, bool CP>
 __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ MarchTmaP<T> P) {
   using G = MarchGeom<T, TJ, TK>;
   extern __shared__ __align__(128) unsigned char smem[];
   const MarchP<T>& p = P.p;
   const Lat L = p.L;
   const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
+  const int gx = blockIdx.x + P.org[0], gy = blockIdx.y + P.org[1], gz = blockIdx.z + P.org[2];
+  if (CP && gx >= P.box_lo[0] && gx < P.box_hi[0] && gy >= P.box_lo[1] && gy < P.box_hi[1] &&
+      gz >= P.box_lo[2] && gz < P.box_hi[2])
+    return;  // swept by the CPML-free form
   // One thread reads the error word, so that the whole CTA returns or none.
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
-  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+  const int k0 = gx * TK, j0 = gy * TJ;
   const int k = k0 + tk, j = j0 + tj;
-  const int i_lo = blockIdx.z * p.ichunk;
+  const int i_lo = gz * p.ichunk;
   const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
   const int n_planes = i_hi - i_lo;
   const int n_staged = n_planes + (i_hi <= L.nx ? 1 : 0);
@@ -157,8 +176,8 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   const T fhj = (act && jv) ? p.fh[1][j] : T(0);
   const T fhk = (act && kv) ? p.fh[2][k] : T(0);
   int qy = 0, qz = 0;
-  const int ly = act ? layer_of(p.slab[1], j, false, qy) : -1;
-  const int lz = act ? layer_of(p.slab[2], k, false, qz) : -1;
+  const int ly = (CP && act) ? layer_of(p.slab[1], j, false, qy) : -1;
+  const int lz = (CP && act) ? layer_of(p.slab[2], k, false, qz) : -1;
   T ay = 0, by = 0, az = 0, bz = 0;
   T* psy[2] = {nullptr, nullptr};
   T* psz[2] = {nullptr, nullptr};
@@ -183,12 +202,41 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   const int hq = tj * G::W + tk;  // (j, k) in a halo box
   const int tq = tj * TK + tk;    // (j, k) in a tile box
 
+  // psi cells of the node on plane i, by slot: 0 Hx-y, 1 Hx-z, 2 Hy-x,
+  // 3 Hy-z, 4 Hz-x, 5 Hz-y (CPML form only).  Old values are loaded one plane
+  // ahead, so their DRAM latency overlaps the compute of the plane before.
+  auto psi_cell = [&](int i, int slot) -> T* {
+    if (slot == 0) return ly >= 0 ? psy[1] + i * psy_st : nullptr;
+    if (slot == 5) return ly >= 0 ? psy[0] + i * psy_st : nullptr;
+    if (slot == 1) return lz >= 0 ? psz[0] + i * psz_st : nullptr;
+    if (slot == 3) return lz >= 0 ? psz[1] + i * psz_st : nullptr;
+    int qx = 0;
+    const int lx = act ? layer_of(p.slab[0], i, false, qx) : -1;
+    if (lx < 0) return nullptr;
+    return p.slab[0].psi_h_out[qx][slot == 2 ? 0 : 1] + (long long)lx * PS + row;
+  };
+  T pv[6] = {};
+  auto load_psi = [&](int i) {
+#pragma unroll
+    for (int x = 0; x < 6; ++x) {
+      const T* c = psi_cell(i, x);
+      pv[x] = c ? *c : T(0);
+    }
+  };
+  if constexpr (CP) load_psi(i_lo);
+
   bool ok = true;
   if (n_staged > 0) ok = ring.wait(0);
   for (int q = 0; q < n_planes; ++q) {
     const int i = i_lo + q;
     const bool iv = i < L.nx;
     const int sc = q % S, sn = (q + 1) % S;
+    T po[6];
+#pragma unroll
+    for (int x = 0; x < 6; ++x) po[x] = pv[x];
+    if constexpr (CP) {
+      if (q + 1 < n_planes) load_psi(i + 1);
+    }
     if (ok && iv) ok = ring.wait(sn);  // plane i+1 (exists when i < nx)
     if (__syncthreads_or(!ok)) {
       ok = false;
@@ -210,14 +258,14 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
       const T dEz_i = ez_n - ez, dEx_k = ex_k - ex;  // Hy
       const T dEx_j = ex_j - ex, dEy_i = ey_n - ey;  // Hz
       const long long o = i * PS;
-      int qx;
-      const int lx = layer_of(p.slab[0], i, false, qx);
+      int qx = 0;
+      const int lx = CP ? layer_of(p.slab[0], i, false, qx) : -1;
       if (jv && kv) {
         const T ca = r[0], cb = r[1];
         T h = tile(sc, 0)[tq];
         if (main_rng) h = ca * h + cb * (fhk * dEy_k - fhj * dEz_j);
-        if (ly >= 0) h -= cb * psi_step(psy[1] + i * psy_st, by, ay, dEz_j);
-        if (lz >= 0) h += cb * psi_step(psz[0] + i * psz_st, bz, az, dEy_k);
+        if (ly >= 0) h -= cb * psi_upd(psy[1] + i * psy_st, po[0], by, ay, dEz_j);
+        if (lz >= 0) h += cb * psi_upd(psz[0] + i * psz_st, po[1], bz, az, dEy_k);
         Hx[o] = h;
       }
       if (iv && kv) {
@@ -226,10 +274,10 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
         if (main_rng) h = ca * h + cb * (fhi * dEz_i - fhk * dEx_k);
         if (lx >= 0) {
           const SlabAxisD<T>& A = p.slab[0];
-          h += cb * psi_step(A.psi_h_out[qx][0] + (long long)lx * PS + row, A.b_h[qx][lx],
-                             A.a_h[qx][lx], dEz_i);
+          h += cb * psi_upd(A.psi_h_out[qx][0] + (long long)lx * PS + row, po[2], A.b_h[qx][lx],
+                            A.a_h[qx][lx], dEz_i);
         }
-        if (lz >= 0) h -= cb * psi_step(psz[1] + i * psz_st, bz, az, dEx_k);
+        if (lz >= 0) h -= cb * psi_upd(psz[1] + i * psz_st, po[3], bz, az, dEx_k);
         Hy[o] = h;
       }
       if (iv && jv) {
@@ -238,10 +286,10 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
         if (main_rng) h = ca * h + cb * (fhj * dEx_j - fhi * dEy_i);
         if (lx >= 0) {
           const SlabAxisD<T>& A = p.slab[0];
-          h -= cb * psi_step(A.psi_h_out[qx][1] + (long long)lx * PS + row, A.b_h[qx][lx],
-                             A.a_h[qx][lx], dEy_i);
+          h -= cb * psi_upd(A.psi_h_out[qx][1] + (long long)lx * PS + row, po[4], A.b_h[qx][lx],
+                            A.a_h[qx][lx], dEy_i);
         }
-        if (ly >= 0) h += cb * psi_step(psy[0] + i * psy_st, by, ay, dEx_j);
+        if (ly >= 0) h += cb * psi_upd(psy[0] + i * psy_st, po[5], by, ay, dEx_j);
         Hz[o] = h;
       }
     }
@@ -265,18 +313,22 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
 // E sweep.  Staged planes q = -1 .. n_planes-1 (plane -1 = i_lo-1, H only,
 // when i_lo >= 1); plane q lives in stage (q+1) % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S>
+template <typename T, int TJ, int TK, int S, bool CP>
 __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ MarchTmaP<T> P) {
   using G = MarchGeom<T, TJ, TK>;
   extern __shared__ __align__(128) unsigned char smem[];
   const MarchP<T>& p = P.p;
   const Lat L = p.L;
   const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
+  const int gx = blockIdx.x + P.org[0], gy = blockIdx.y + P.org[1], gz = blockIdx.z + P.org[2];
+  if (CP && gx >= P.box_lo[0] && gx < P.box_hi[0] && gy >= P.box_lo[1] && gy < P.box_hi[1] &&
+      gz >= P.box_lo[2] && gz < P.box_hi[2])
+    return;  // swept by the CPML-free form
   // One thread reads the error word, so that the whole CTA returns or none.
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
-  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+  const int k0 = gx * TK, j0 = gy * TJ;
   const int k = k0 + tk, j = j0 + tj;
-  const int i_lo = blockIdx.z * p.ichunk;
+  const int i_lo = gz * p.ichunk;
   const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
   const int n_planes = i_hi - i_lo;
   const int q_first = i_lo >= 1 ? -1 : 0;  // first staged plane
@@ -328,8 +380,8 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
   const T fej = act ? p.fe[1][j] : T(0);
   const T fek = act ? p.fe[2][k] : T(0);
   int qy = 0, qz = 0;
-  const int ly = act ? layer_of(p.slab[1], j, true, qy) : -1;
-  const int lz = act ? layer_of(p.slab[2], k, true, qz) : -1;
+  const int ly = (CP && act) ? layer_of(p.slab[1], j, true, qy) : -1;
+  const int lz = (CP && act) ? layer_of(p.slab[2], k, true, qz) : -1;
   T ay = 0, by = 0, az = 0, bz = 0;
   T* psy[2] = {nullptr, nullptr};
   T* psz[2] = {nullptr, nullptr};
@@ -354,11 +406,41 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
   const int hq = (tj + 1) * G::W + tk + G::XA;  // (j, k) in a halo box
   const int tq = tj * TK + tk;
 
+  // psi cells of the node on plane i, by slot: 0 Ex-y, 1 Ex-z, 2 Ey-x,
+  // 3 Ey-z, 4 Ez-x, 5 Ez-y (CPML form only), old values loaded a plane ahead.
+  auto psi_cell = [&](int i, int slot) -> T* {
+    if (slot == 0) return ly >= 0 ? psy[1] + i * psy_st : nullptr;
+    if (slot == 5) return ly >= 0 ? psy[0] + i * psy_st : nullptr;
+    if (slot == 1) return lz >= 0 ? psz[0] + i * psz_st : nullptr;
+    if (slot == 3) return lz >= 0 ? psz[1] + i * psz_st : nullptr;
+    int qx = 0;
+    const int lx = act ? layer_of(p.slab[0], i, true, qx) : -1;
+    if (lx < 0) return nullptr;
+    return p.slab[0].psi_e[qx][slot == 2 ? 0 : 1] + (long long)lx * PS + row;
+  };
+  T pv[6] = {};
+  auto load_psi = [&](int i) {
+#pragma unroll
+    for (int x = 0; x < 6; ++x) {
+      const T* c = psi_cell(i, x);
+      pv[x] = c ? *c : T(0);
+    }
+  };
+  if constexpr (CP) {
+    if (n_planes > 0) load_psi(i_lo);
+  }
+
   bool ok = true;
   if (q_first < 0) ok = ring.wait(slot(-1));
   for (int q = 0; q < n_planes; ++q) {
     const int i = i_lo + q;
     const int sc = slot(q), sp = slot(q - 1);
+    T po[6];
+#pragma unroll
+    for (int x = 0; x < 6; ++x) po[x] = pv[x];
+    if constexpr (CP) {
+      if (q + 1 < n_planes) load_psi(i + 1);
+    }
     if (ok) ok = ring.wait(sc);
     if (__syncthreads_or(!ok)) {
       ok = false;
@@ -382,14 +464,14 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
       const T dHx_k = hx - hx_k, dHz_i = hz - hz_p;  // Ey
       const T dHy_i = hy - hy_p, dHx_j = hx - hx_j;  // Ez
       const long long o = i * PS;
-      int qx;
-      const int lx = layer_of(p.slab[0], i, true, qx);
+      int qx = 0;
+      const int lx = CP ? layer_of(p.slab[0], i, true, qx) : -1;
       if (iv) {
         const T ca = r[0], cb = r[1];
         T e = tile(sc, 0)[tq];
         if (jm && km) e = ca * e + cb * (fej * dHz_j - fek * dHy_k);
-        if (ly >= 0) e += cb * psi_step(psy[1] + i * psy_st, by, ay, dHz_j);
-        if (lz >= 0) e -= cb * psi_step(psz[0] + i * psz_st, bz, az, dHy_k);
+        if (ly >= 0) e += cb * psi_upd(psy[1] + i * psy_st, po[0], by, ay, dHz_j);
+        if (lz >= 0) e -= cb * psi_upd(psz[0] + i * psz_st, po[1], bz, az, dHy_k);
         Ex[o] = e;
       }
       if (jv) {
@@ -398,10 +480,10 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
         if (im && km) e = ca * e + cb * (fek * dHx_k - fei * dHz_i);
         if (lx >= 0) {
           const SlabAxisD<T>& A = p.slab[0];
-          e -= cb * psi_step(A.psi_e[qx][0] + (long long)lx * PS + row, A.b_e[qx][lx],
-                             A.a_e[qx][lx], dHz_i);
+          e -= cb * psi_upd(A.psi_e[qx][0] + (long long)lx * PS + row, po[2], A.b_e[qx][lx],
+                            A.a_e[qx][lx], dHz_i);
         }
-        if (lz >= 0) e += cb * psi_step(psz[1] + i * psz_st, bz, az, dHx_k);
+        if (lz >= 0) e += cb * psi_upd(psz[1] + i * psz_st, po[3], bz, az, dHx_k);
         Ey[o] = e;
       }
       if (kv) {
@@ -410,10 +492,10 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
         if (im && jm) e = ca * e + cb * (fei * dHy_i - fej * dHx_j);
         if (lx >= 0) {
           const SlabAxisD<T>& A = p.slab[0];
-          e += cb * psi_step(A.psi_e[qx][1] + (long long)lx * PS + row, A.b_e[qx][lx],
-                             A.a_e[qx][lx], dHy_i);
+          e += cb * psi_upd(A.psi_e[qx][1] + (long long)lx * PS + row, po[4], A.b_e[qx][lx],
+                            A.a_e[qx][lx], dHy_i);
         }
-        if (ly >= 0) e -= cb * psi_step(psy[0] + i * psy_st, by, ay, dHx_j);
+        if (ly >= 0) e -= cb * psi_upd(psy[0] + i * psy_st, po[5], by, ay, dHx_j);
         Ez[o] = e;
       }
     }
