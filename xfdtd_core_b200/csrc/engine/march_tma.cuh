@@ -17,6 +17,10 @@
 //                     k0-XA..k0+TK-1 (the -1 neighbours), E_x,E_y,E_z and the
 //                     class index over the tile.  The H of plane i-1 is the
 //                     previous stage, kept until plane i is done.
+// One CTA barrier per plane: a stage is refilled right after the barrier
+// that follows its last use.  The (ca, cb) half-rows of the NC most frequent
+// material classes (the engine numbers classes by descending node count) are
+// read from a shared-memory copy.
 // Out-of-range rows, columns and planes read as zeros and are never used.
 // Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
 // the engine's error word, drains its loads in flight and returns, and later
@@ -61,8 +65,22 @@ struct MarchGeom {
   static constexpr int STAGE = CLS_OFF + pad(CLS_B);
   static constexpr int TX_FULL = 3 * HALO_B + 3 * TILE_B + CLS_B;
   static constexpr int TX_HALO = 3 * HALO_B;
-  __host__ __device__ static constexpr int smem(int S) { return S * STAGE + 8 * S; }
+  static constexpr int NC = 64;  // classes whose (ca, cb) half-rows are cached
+  static constexpr int TB = NC * 6 * (int)sizeof(T);
+  __host__ __device__ static constexpr int smem(int S) { return S * STAGE + TB + 8 * S; }
 };
+
+// Copies the (ca, cb) pairs of one half of the class table (0: E, 1: H) of
+// the first NC classes to shared memory.
+template <typename T, int NC, int NT>
+__device__ __forceinline__ void stage_half_table(T* sT, const T* tab, int n_classes, int half,
+                                                 int tid) {
+  const int n = min(n_classes, NC) * 6;
+  for (int x = tid; x < n; x += NT) {
+    const int c = x / 6;
+    sT[x] = tab[(size_t)c * 12 + half * 6 + (x - c * 6)];
+  }
+}
 
 // CPML psi update from an already loaded old value: psi = b psi + a diff,
 // stored in place.
@@ -133,7 +151,8 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   const int n_staged = n_planes + (i_hi <= L.nx ? 1 : 0);
 
   StageRing ring;
-  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE);
+  T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);  // [NC][6] (ca, cb) half-rows
+  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::TB);
   auto halo = [&](int s, int c) {
     return reinterpret_cast<const T*>(smem + s * G::STAGE + G::HALO_OFF + c * G::pad(G::HALO_B));
   };
@@ -166,6 +185,7 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   if (tid == 0)
     for (int q = 0; q < S && q < n_staged; ++q) issue(q);
   for (int q = 0; q < S && q < n_staged; ++q) ring.pending |= 1u << (q % S);
+  stage_half_table<T, G::NC, TJ * TK>(sT, p.tab, p.n_classes, 1, tid);
 
   // Per-thread constants (as k_march_h).
   const bool act = k <= L.nz && j <= L.ny;
@@ -205,23 +225,17 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   // psi cells of the node on plane i, by slot: 0 Hx-y, 1 Hx-z, 2 Hy-x,
   // 3 Hy-z, 4 Hz-x, 5 Hz-y (CPML form only).  Old values are loaded one plane
   // ahead, so their DRAM latency overlaps the compute of the plane before.
-  auto psi_cell = [&](int i, int slot) -> T* {
-    if (slot == 0) return ly >= 0 ? psy[1] + i * psy_st : nullptr;
-    if (slot == 5) return ly >= 0 ? psy[0] + i * psy_st : nullptr;
-    if (slot == 1) return lz >= 0 ? psz[0] + i * psz_st : nullptr;
-    if (slot == 3) return lz >= 0 ? psz[1] + i * psz_st : nullptr;
-    int qx = 0;
-    const int lx = act ? layer_of(p.slab[0], i, false, qx) : -1;
-    if (lx < 0) return nullptr;
-    return p.slab[0].psi_h_out[qx][slot == 2 ? 0 : 1] + (long long)lx * PS + row;
-  };
   T pv[6] = {};
   auto load_psi = [&](int i) {
-#pragma unroll
-    for (int x = 0; x < 6; ++x) {
-      const T* c = psi_cell(i, x);
-      pv[x] = c ? *c : T(0);
-    }
+    pv[0] = ly >= 0 ? psy[1][i * psy_st] : T(0);
+    pv[5] = ly >= 0 ? psy[0][i * psy_st] : T(0);
+    pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
+    pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
+    int qx = 0;
+    const int lx = act ? layer_of(p.slab[0], i, false, qx) : -1;
+    const long long ox = (long long)lx * PS + row;
+    pv[2] = lx >= 0 ? p.slab[0].psi_h_out[qx][0][ox] : T(0);
+    pv[4] = lx >= 0 ? p.slab[0].psi_h_out[qx][1][ox] : T(0);
   };
   if constexpr (CP) load_psi(i_lo);
 
@@ -242,10 +256,19 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
       ok = false;
       break;
     }
+    // Every thread is past plane q-1: refill its stage with plane q-1+S.
+    if (q >= 1 && q - 1 + S < n_staged) {
+      if (tid == 0) {
+        fence_proxy_async();
+        issue(q - 1 + S);
+      }
+      ring.pending |= 1u << ((q - 1) % S);
+    }
     if (act) {
       const bool main_rng = iv && jv && kv;
       const T fhi = iv ? p.fh[0][i] : T(0);
-      const T* r = p.tab + (size_t)ctile(sc)[tq] * 12 + 6;
+      const int cl = ctile(sc)[tq];
+      const T* r = cl < G::NC ? sT + cl * 6 : p.tab + (size_t)cl * 12 + 6;
       const T* Exs = halo(sc, 0);
       const T* Eys = halo(sc, 1);
       const T* Ezs = halo(sc, 2);
@@ -293,15 +316,6 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
         Hz[o] = h;
       }
     }
-    __syncthreads();
-    // Stage sc (plane i) is free: refill it with plane q+S.
-    if (q + S < n_staged) {
-      if (tid == 0) {
-        fence_proxy_async();
-        issue(q + S);
-      }
-      ring.pending |= 1u << sc;
-    }
   }
   if (!ok) {
     if (tid == 0) atomicOr(P.err, 2);
@@ -334,7 +348,8 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
   const int q_first = i_lo >= 1 ? -1 : 0;  // first staged plane
 
   StageRing ring;
-  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE);
+  T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);  // [NC][6] (ca, cb) half-rows
+  ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::TB);
   auto slot = [](int q) { return (q + 1) % S; };
   auto halo = [&](int s, int c) {
     return reinterpret_cast<const T*>(smem + s * G::STAGE + G::HALO_OFF + c * G::pad(G::HALO_B));
@@ -370,6 +385,7 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
   if (tid == 0)
     for (int q = q_first; q < q_first + S && q < q_end; ++q) issue(q);
   for (int q = q_first; q < q_first + S && q < q_end; ++q) ring.pending |= 1u << slot(q);
+  stage_half_table<T, G::NC, TJ * TK>(sT, p.tab, p.n_classes, 0, tid);
 
   const bool act = k <= L.nz && j <= L.ny;
   const long long PS = (long long)L.NY * L.KP;
@@ -408,23 +424,17 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
 
   // psi cells of the node on plane i, by slot: 0 Ex-y, 1 Ex-z, 2 Ey-x,
   // 3 Ey-z, 4 Ez-x, 5 Ez-y (CPML form only), old values loaded a plane ahead.
-  auto psi_cell = [&](int i, int slot) -> T* {
-    if (slot == 0) return ly >= 0 ? psy[1] + i * psy_st : nullptr;
-    if (slot == 5) return ly >= 0 ? psy[0] + i * psy_st : nullptr;
-    if (slot == 1) return lz >= 0 ? psz[0] + i * psz_st : nullptr;
-    if (slot == 3) return lz >= 0 ? psz[1] + i * psz_st : nullptr;
-    int qx = 0;
-    const int lx = act ? layer_of(p.slab[0], i, true, qx) : -1;
-    if (lx < 0) return nullptr;
-    return p.slab[0].psi_e[qx][slot == 2 ? 0 : 1] + (long long)lx * PS + row;
-  };
   T pv[6] = {};
   auto load_psi = [&](int i) {
-#pragma unroll
-    for (int x = 0; x < 6; ++x) {
-      const T* c = psi_cell(i, x);
-      pv[x] = c ? *c : T(0);
-    }
+    pv[0] = ly >= 0 ? psy[1][i * psy_st] : T(0);
+    pv[5] = ly >= 0 ? psy[0][i * psy_st] : T(0);
+    pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
+    pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
+    int qx = 0;
+    const int lx = act ? layer_of(p.slab[0], i, true, qx) : -1;
+    const long long ox = (long long)lx * PS + row;
+    pv[2] = lx >= 0 ? p.slab[0].psi_e[qx][0][ox] : T(0);
+    pv[4] = lx >= 0 ? p.slab[0].psi_e[qx][1][ox] : T(0);
   };
   if constexpr (CP) {
     if (n_planes > 0) load_psi(i_lo);
@@ -446,11 +456,20 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
       ok = false;
       break;
     }
+    // Every thread is past plane q-1, so plane q-2 is free: refill its stage.
+    if (q - 2 >= q_first && q - 2 + S < q_end) {
+      if (tid == 0) {
+        fence_proxy_async();
+        issue(q - 2 + S);
+      }
+      ring.pending |= 1u << slot(q - 2);
+    }
     if (act) {
       const bool iv = i < L.nx, i1 = i >= 1;
       const bool im = i1 && iv;
       const T fei = p.fe[0][i];
-      const T* r = p.tab + (size_t)ctile(sc)[tq] * 12;
+      const int cl = ctile(sc)[tq];
+      const T* r = cl < G::NC ? sT + cl * 6 : p.tab + (size_t)cl * 12;
       const T* Hxs = halo(sc, 0);
       const T* Hys = halo(sc, 1);
       const T* Hzs = halo(sc, 2);
@@ -498,16 +517,6 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
         if (ly >= 0) e -= cb * psi_upd(psy[0] + i * psy_st, po[5], by, ay, dHx_j);
         Ez[o] = e;
       }
-    }
-    __syncthreads();
-    // Stage sp (plane i-1) is free: refill it with plane q-1+S.
-    const int qn = q - 1 + S;
-    if (q - 1 >= q_first && qn < q_end) {
-      if (tid == 0) {
-        fence_proxy_async();
-        issue(qn);
-      }
-      ring.pending |= 1u << sp;
     }
   }
   if (!ok) {
