@@ -53,6 +53,21 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def profiled_traffic(grid: int, kmode: int):
+    """DRAM bytes per FP32 step of the default sweep from the committed ncu
+    summary (profiles/traffic_march_tma_boxes.md), for the 256^3 workload."""
+    if grid != 256 or kmode != 4:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_march_tma_boxes.md")) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_step_fp32_256"):
+                    return int(line.split("=")[1])
+    except OSError:
+        pass
+    return None
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples during the timed region."""
@@ -385,11 +400,16 @@ def main():
                        "l2": "inputs larger than L2 (fields 6x257^3 fp32 = 407 MB)",
                        "parallelism": f"replicas x{world}", "sweep": sweep},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
+                         "frac": achieved / hbm,
+                         "traffic": profiled_traffic(args.grid, kmode.value),
                          "peak_source": peak_kind,
+                         "kernel": "the step's sweep launches (k_march_h_tma + k_march_e_tma, "
+                                   "CPML-free and CPML forms; 99% of a step's device time)",
                          "note": "achieved = algorithmic stencil bytes per step "
                                  f"({bytes32} B: 12 field values + uint16 class per cell, "
-                                 "8 CPML psi per slab cell) / whole-step time"},
+                                 "8 CPML psi per slab cell) / step time by CUDA events on "
+                                 "the engine stream; traffic = DRAM bytes per step from "
+                                 "profiles/traffic_march_tma_boxes.md"},
             "forms": {"fp64_plain": {"value": value64, "unit": UNIT,
                                      "ms_per_step": ms64 / steps,
                                      "roofline_achieved_gbs": achieved64,
