@@ -259,6 +259,10 @@ constexpr int kStagesF32 = 4, kStagesF64 = 3;
 constexpr int kMarchStagesF32 = 6, kMarchStagesF64 = 4;
 template <typename T>
 constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32; }
+// The CPML-free forms need fewer registers, so they run more CTAs per SM;
+// fewer stages keep their shared memory from capping that.
+template <typename T>
+constexpr int march_free_stages() { return sizeof(T) == 8 ? 3 : 4; }
 constexpr int kFmStages = 4;
 constexpr int kFmTJ = 8;
 template <typename T>
@@ -392,10 +396,11 @@ xfd_status build_tma_maps(xfd_engine* e) {
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
   CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS, false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
+  constexpr int MF = march_free_stages<T>();
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MF, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MF, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
   e->tma_ready = true;
   return XFD_OK;
 }
@@ -642,17 +647,19 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       }
     }
     const size_t msm = MarchGeom<T, 8, 32>::smem(MS);
+    constexpr int MF = march_free_stages<T>();
+    const size_t msm_free = MarchGeom<T, 8, 32>::smem(MF);
     auto launch_march = [&](auto kfree, auto kcp) {
       if (mbox) {
         MarchTmaP<T> q = mtp;
         for (int a = 0; a < 3; ++a) q.org[a] = mlo[a];
-        kfree<<<dim3(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]), blk, msm, s>>>(q);
+        kfree<<<dim3(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]), blk, msm_free, s>>>(q);
       }
       kcp<<<grd_m, blk, msm, s>>>(mtp);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma)
-      launch_march(k_march_h_tma<T, 8, 32, MS, false>, k_march_h_tma<T, 8, 32, MS, true>);
+      launch_march(k_march_h_tma<T, 8, 32, MF, false>, k_march_h_tma<T, 8, 32, MS, true>);
     else if (march)
       k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
@@ -668,7 +675,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
     if (march_tma)
-      launch_march(k_march_e_tma<T, 8, 32, MS, false>, k_march_e_tma<T, 8, 32, MS, true>);
+      launch_march(k_march_e_tma<T, 8, 32, MF, false>, k_march_e_tma<T, 8, 32, MS, true>);
     else if (march)
       k_march_e<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
