@@ -492,10 +492,10 @@ void fmarch_split(const xfd_engine* e, int nt[3], int lo[3], int hi[3]) {
 // the split marching sweeps whose nodes lie in no CPML layer of either phase.
 void march_split(const xfd_engine* e, int lo[3], int hi[3]) {
   const Lat& L = e->L;
-  const int nt[3] = {(L.nz + 1 + 31) / 32, (L.ny + 1 + 7) / 8,
+  const int nt[3] = {(L.nz + 31) / 32, (L.ny + 7) / 8,
                      (L.nx + 1 + e->march_ichunk - 1) / e->march_ichunk};
   const int size[3] = {32, 8, e->march_ichunk};
-  const int n_nodes[3] = {L.nz + 1, L.ny + 1, L.nx + 1};
+  const int n_nodes[3] = {L.nz, L.ny, L.nx + 1};
   const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
   for (int g = 0; g < 3; ++g) {
     const int m = axis_of[g];
@@ -633,8 +633,12 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     const dim3 blk(32, 8, 1);
     const dim3 grd((unsigned)((e->L.nz + 1 + 31) / 32), (unsigned)((e->L.ny + 1 + 7) / 8),
                    (unsigned)(e->L.nx + 1));
-    const dim3 grd_m(grd.x, grd.y,
+    // The TMA marching sweeps tile k < nz, j < ny (the faces k = nz, j = ny
+    // go to k_edge_h / k_edge_e); the plain marching sweeps tile all nodes.
+    const dim3 grd_m(march_tma ? (unsigned)((e->L.nz + 31) / 32) : grd.x,
+                     march_tma ? (unsigned)((e->L.ny + 7) / 8) : grd.y,
                      (unsigned)((e->L.nx + 1 + mp.ichunk - 1) / std::max(1, mp.ichunk)));
+    const unsigned edge_blocks = (unsigned)((edge_nodes(e->L) + 255) / 256);
     // The CPML-free box of (k tile, j tile, chunk) for the TMA marching sweeps.
     int mlo[3] = {0, 0, 0}, mhi[3] = {0, 0, 0};
     bool mbox = false;
@@ -658,8 +662,10 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       kcp<<<grd_m, blk, msm, s>>>(mtp);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
-    if (march_tma)
+    if (march_tma) {
       launch_march(k_march_h_tma<T, 8, 32, MF, false>, k_march_h_tma<T, 8, 32, MS, true>);
+      k_edge_h<T><<<edge_blocks, 256, 0, s>>>(yp);
+    }
     else if (march)
       k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
@@ -674,8 +680,10 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
-    if (march_tma)
+    if (march_tma) {
       launch_march(k_march_e_tma<T, 8, 32, MF, false>, k_march_e_tma<T, 8, 32, MS, true>);
+      k_edge_e<T><<<edge_blocks, 256, 0, s>>>(yp);
+    }
     else if (march)
       k_march_e<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
@@ -1530,6 +1538,7 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
     if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 1;  // CPML-free part
   }
   if (e->kernel_mode == 4) {
+    n += 2;  // lattice-face sweeps k_edge_h / k_edge_e
     int lo[3], hi[3];
     march_split(e, lo, hi);
     if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 2;  // CPML-free H and E

@@ -83,12 +83,8 @@ __device__ __forceinline__ long long sel3(int m, long long a, long long b, long 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeP<T> p) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
+__device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, int k) {
   const Lat L = p.L;
-  if (k > L.nz || j > L.ny || i > L.nx) return;
   const long long id = lat_index(L, i, j, k);
   const int x[3] = {i, j, k};
   const int n[3] = {L.nx, L.ny, L.nz};
@@ -138,12 +134,8 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeP<T
 // [e_lo, e_lo + n) along m, whole transverse extent.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeP<T> p) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
+__device__ __forceinline__ void update_e_node(const YeeP<T>& p, int i, int j, int k) {
   const Lat L = p.L;
-  if (k > L.nz || j > L.ny || i > L.nx) return;
   const long long id = lat_index(L, i, j, k);
   const int x[3] = {i, j, k};
   const int n[3] = {L.nx, L.ny, L.nz};
@@ -191,6 +183,65 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeP<T
     }
     E[id] = e;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeP<T> p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k > p.L.nz || j > p.L.ny || i > p.L.nx) return;
+  update_h_node(p, i, j, k);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeP<T> p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k > p.L.nz || j > p.L.ny || i > p.L.nx) return;
+  update_e_node(p, i, j, k);
+}
+
+// The lattice faces k = nz (all i, j) and j = ny (all i, k < nz), which hold
+// only boundary nodes (their components are either fixed or receive CPML
+// terms only).  Sweeps that tile k < nz, j < ny leave these faces to the
+// two kernels below, one thread per node, with the arithmetic of
+// k_update_h / k_update_e.
+__host__ __device__ __forceinline__ long long edge_nodes(const Lat& L) {
+  return (long long)(L.nx + 1) * (L.ny + 1) + (long long)(L.nx + 1) * L.nz;
+}
+
+__device__ __forceinline__ void edge_node(const Lat& L, long long t, int& i, int& j, int& k) {
+  const long long fa = (long long)(L.nx + 1) * (L.ny + 1);
+  if (t < fa) {
+    i = (int)(t / (L.ny + 1));
+    j = (int)(t - (long long)i * (L.ny + 1));
+    k = L.nz;
+  } else {
+    t -= fa;
+    i = (int)(t / L.nz);
+    k = (int)(t - (long long)i * L.nz);
+    j = L.ny;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_edge_h(const __grid_constant__ YeeP<T> p) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= edge_nodes(p.L)) return;
+  int i, j, k;
+  edge_node(p.L, t, i, j, k);
+  update_h_node(p, i, j, k);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_edge_e(const __grid_constant__ YeeP<T> p) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= edge_nodes(p.L)) return;
+  int i, j, k;
+  edge_node(p.L, t, i, j, k);
+  update_e_node(p, i, j, k);
 }
 
 // ---------------------------------------------------------------------------

@@ -22,6 +22,9 @@
 // material classes (the engine numbers classes by descending node count) are
 // read from a shared-memory copy.
 // Out-of-range rows, columns and planes read as zeros and are never used.
+// The tiles cover k < nz and j < ny; the lattice faces k = nz and j = ny hold
+// only boundary nodes and are swept by k_edge_h / k_edge_e (kernels.cuh), so
+// no CTA marches through a one-column or one-row remainder tile.
 // Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
 // the engine's error word, drains its loads in flight and returns, and later
 // launches that find the bit set return at once.
@@ -187,8 +190,9 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   for (int q = 0; q < S && q < n_staged; ++q) ring.pending |= 1u << (q % S);
   stage_half_table<T, G::NC, TJ * TK>(sT, p.tab, p.n_classes, 1, tid);
 
-  // Per-thread constants (as k_march_h).
-  const bool act = k <= L.nz && j <= L.ny;
+  // Per-thread constants (as k_march_h).  The faces k = nz and j = ny are
+  // left to k_edge_h (kernels.cuh).
+  const bool act = k < L.nz && j < L.ny;
   const long long PS = (long long)L.NY * L.KP;
   const int KP = L.KP;
   const long long row = (long long)j * KP + k;
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
   for (int q = q_first; q < q_first + S && q < q_end; ++q) ring.pending |= 1u << slot(q);
   stage_half_table<T, G::NC, TJ * TK>(sT, p.tab, p.n_classes, 0, tid);
 
-  const bool act = k <= L.nz && j <= L.ny;
+  const bool act = k < L.nz && j < L.ny;  // faces k = nz, j = ny: k_edge_e
   const long long PS = (long long)L.NY * L.KP;
   const int KP = L.KP;
   const long long row = (long long)j * KP + k;
