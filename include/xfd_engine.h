@@ -176,6 +176,29 @@ xfd_status xfd_set_nf2ff(xfd_engine* e, const xfd_nf2ff_desc* nf);
  * Replaces: FDPlaneData's _ja/_jb/_ma/_mb arrays (src/nffft/nffft_fd_data.cpp:21-63). */
 xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* count);
 
+/* Far-field potentials of the accumulated surface currents, computed on the
+ * GPU for n_angles (theta[a], phi[a]) pairs and every NF2FF frequency:
+ * out = complex interleaved [freq][a_theta, f_phi, a_phi, f_theta][angle]
+ * (n_freq * 4 * n_angles complex values).  freqs: the NF2FF frequencies (Hz),
+ * n_freq of them; node_e / node_h / size_e: per axis the grid's node
+ * coordinates (n+1), cell-centre coordinates (n) and cell sizes (n).
+ * Replaces: FDPlaneData::getPotential / calculatePotential
+ * (src/nffft/nffft_fd_data_process.cpp:15-144) as called by
+ * NFFFTFrequencyDomain::processFarField (src/nffft/nffft_frequency_domain.cpp:103-129). */
+typedef struct {
+  int32_t n_angles;
+  const double* theta;   /* host, n_angles */
+  const double* phi;     /* host, n_angles */
+  int32_t n_freq;
+  const double* freqs;   /* host, n_freq */
+  double origin[3];
+  const double* node_e[3];
+  const double* node_h[3];
+  const double* size_e[3];
+} xfd_far_field_desc;
+xfd_status xfd_nf2ff_far_field(xfd_engine* e, const xfd_far_field_desc* d, double* out,
+                               int64_t capacity);
+
 /* Movie monitor: every `interval` steps (from step 0) the box [box_s, box_e)
  * of `field` is recorded into a device frame store.
  * Replaces: MovieMonitor::update -> FieldMonitor::output

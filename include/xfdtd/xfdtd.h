@@ -487,11 +487,31 @@ class NFFFTFrequencyDomain {
   /// Face node boxes [s, e) in global indices (empty when invalid).
   std::array<std::array<int, 6>, 6> faces{};
 
+  /// Far-field potentials of the surface currents, computed on the GPU:
+  /// laid out [frequency][a_theta, f_phi, a_phi, f_theta][angle] over the
+  /// angles theta x phi, one of which must hold a single value
+  /// (FDPlaneData::getPotential, src/nffft/nffft_fd_data_process.cpp:15-144).
+  /// Needs the simulation that ran this NF2FF to be alive.
+  std::vector<std::complex<Real>> farField(const Array1D<Real>& theta, const Array1D<Real>& phi,
+                                           const Vector& origin = Vector{0, 0, 0}) const;
+  /// processFarField (nffft_frequency_domain.h:35-62): writes, per
+  /// frequency, <outputDir>/<sub_dir>/<f in GHz, 2 decimals>GHz_{a_theta,
+  /// f_phi,a_phi,f_theta}.npy (complex128, one value per angle).
+  void processFarField(const Array1D<Real>& theta, Real phi, const std::string& sub_dir,
+                       const Vector& origin = Vector{0, 0, 0}) const;
+  void processFarField(Real theta, const Array1D<Real>& phi, const std::string& sub_dir,
+                       const Vector& origin = Vector{0, 0, 0}) const;
+  void processFarField(const Array1D<Real>& theta, const Array1D<Real>& phi,
+                       const std::string& sub_dir, const Vector& origin) const;
+
  private:
+  friend class Simulation;
   std::array<Index, 3> _d;
   Array1D<Real> _freqs;
   std::string _output_dir;
   std::vector<std::complex<Real>> _acc;
+  xfd_engine* _engine = nullptr;  // set while the owning Simulation lives
+  std::array<std::vector<Real>, 3> _node_e, _node_h, _size_e;  // grid, per axis
 };
 
 class ThreadConfig {

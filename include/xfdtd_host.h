@@ -65,6 +65,14 @@ int xfdtd_scene_field_time(xfdtd_scene* s, int32_t index, double* out, int64_t c
                            int64_t* count);
 /* NF2FF surface currents (complex interleaved, [f][face][ja jb ma mb][nodes]). */
 int xfdtd_scene_nf2ff(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count);
+/* NF2FF far-field potentials on the GPU (NFFFTFrequencyDomain::farField):
+ * complex interleaved [freq][a_theta f_phi a_phi f_theta][angle] for the
+ * angles theta x phi (n_theta or n_phi must be 1).  With `sub_dir` non-NULL
+ * it also writes them like processFarField, under <dir>/<sub_dir>. */
+int xfdtd_scene_far_field(xfdtd_scene* s, int32_t n_theta, const double* theta, int32_t n_phi,
+                          const double* phi, const double origin[3], double* out,
+                          int64_t capacity, int64_t* count, const char* dir,
+                          const char* sub_dir);
 /* Writes <dir>/fields/{EX..HZ}.npy, <dir>/<movie>/<step:05d>.npy and
  * <dir>/nf2ff.npy like the reference's Monitor::output (src/monitor/monitor.cpp:42-54). */
 int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir);

@@ -825,6 +825,60 @@ class RefSimulation:
                       "acc": np.zeros(2 * total), "off": np.array(offs, dtype=np.int64),
                       "freqs": np.array(spec.freqs, dtype=np.float64)}
 
+    def far_field(self, theta, phi, origin=(0.0, 0.0, 0.0)) -> np.ndarray:
+        """Far-field potentials from the accumulated surface currents:
+        FDPlaneData::getPotential / calculatePotential
+        (src/nffft/nffft_fd_data_process.cpp:15-144) summed over the faces
+        XN, XP, YN, YP, ZN, ZP, for every frequency in the order of
+        NFFFTFrequencyDomain::processFarField
+        (src/nffft/nffft_frequency_domain.cpp:103-129): returns complex
+        [n_freq, 4, n_angles] with rows a_theta, f_phi, a_phi, f_theta.
+        Face-centre positions rVector and areas ds follow
+        nffft_fd_data_process.cpp:185-215; the Cartesian-to-spherical unit
+        vector components follow cCSToSCSTransformMatrix
+        (include/xfdtd/util/transform.h:25-59)."""
+        theta = np.atleast_1d(np.asarray(theta, dtype=np.float64))
+        phi = np.atleast_1d(np.asarray(phi, dtype=np.float64))
+        if theta.size != 1 and phi.size != 1:
+            raise ValueError("There must be only one theta or phi")
+        n_ang = theta.size * phi.size
+        th = np.broadcast_to(theta, (n_ang,)) if theta.size == n_ang else np.full(n_ang, theta[0])
+        ph = np.broadcast_to(phi, (n_ang,)) if phi.size == n_ang else np.full(n_ang, phi[0])
+        cos_t, sin_t = np.cos(th), np.sin(th)
+        cos_p, sin_p = np.cos(ph), np.sin(ph)
+        st_sp, st_cp = sin_t * sin_p, sin_t * cos_p
+        # unit vectors of the Cartesian axes projected on theta-hat / phi-hat
+        tr = {"theta": [cos_t * cos_p, cos_t * sin_p, -1 * sin_t],
+              "phi": [-1 * sin_p, cos_p, np.zeros_like(th)]}
+        nf = self.nf2ff
+        out = np.zeros((nf["nf"], 4, n_ang), dtype=np.complex128)
+        plan = [(0, "theta"), (2, "phi"), (0, "phi"), (2, "theta")]  # (q of a, scs)
+        for fi, freq in enumerate(nf["freqs"]):
+            k0 = 2.0 * PI * freq / C_0
+            for row, (q0, scs) in enumerate(plan):
+                acc = np.zeros(n_ang, dtype=np.complex128)
+                for face in range(6):
+                    if nf["tasks"][face] is None:
+                        continue
+                    s, e = nf["tasks"][face]
+                    m = face // 2
+                    A, B = (m + 1) % 3, (m + 2) % 3
+                    a = self.nf2ff_surface(fi, face, q0).ravel()
+                    b = self.nf2ff_surface(fi, face, q0 + 1).ravel()
+                    ii, jj, kk = np.meshgrid(np.arange(s[0], e[0]), np.arange(s[1], e[1]),
+                                             np.arange(s[2], e[2]), indexing="ij")
+                    idx = [ii.ravel(), jj.ravel(), kk.ravel()]
+                    pos = [(self.e_node[x] if x == m else self.h_node[x])[idx[x]] - origin[x]
+                           for x in range(3)]
+                    ds = self.e_size[A][idx[A]] * self.e_size[B][idx[B]]
+                    arg = (pos[0][:, None] * st_cp[None, :] + pos[1][:, None] * st_sp[None, :]
+                           + pos[2][:, None] * cos_t[None, :])
+                    phase = np.exp(1j * k0 * arg)
+                    term = (a[:, None] * tr[scs][A][None, :] + b[:, None] * tr[scs][B][None, :])
+                    acc += np.sum(term * phase * ds[:, None], axis=0)
+                out[fi, row] = acc
+        return out
+
     def nf2ff_surface(self, f: int, face: int, q: int) -> Optional[np.ndarray]:
         """Complex accumulator (ja, jb, ma, mb) of frequency f on face d, shaped
         like the face task."""

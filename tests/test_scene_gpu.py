@@ -109,3 +109,30 @@ def test_outputs_written(tmp_path):
     assert ex.shape == run.field(0).shape
     frames = sorted((tmp_path / "movie_ex_xz").glob("*.npy"))
     assert [f.name for f in frames] == ["00000.npy", "00010.npy", "00020.npy"]
+
+
+def test_far_field_matches_oracle(tmp_path):
+    """NF2FF far-field potentials computed on the GPU from the engine's
+    surface currents against the oracle's restatement of
+    FDPlaneData::calculatePotential, for a theta sweep at one phi and a phi
+    sweep at one theta; the processFarField files hold the same values."""
+    sc = dispersive_small(steps=150)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc)
+    run.run()
+    theta = np.linspace(0.0, np.pi, 19)
+    phi = np.linspace(0.0, 2 * np.pi, 13)
+    origin = (0.001, -0.002, 0.0005)
+    got = run.far_field(theta, np.pi / 6, origin, directory=str(tmp_path), sub_dir="ff")
+    want = orc.far_field(theta, np.pi / 6, origin)
+    assert got.shape == want.shape
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
+    got2 = run.far_field(np.pi / 3, phi)
+    want2 = orc.far_field(np.pi / 3, phi)
+    assert np.linalg.norm(got2 - want2) / np.linalg.norm(want2) <= TOL64
+    f0 = sc.nf2ff.freqs[0]
+    a_theta = np.load(tmp_path / "ff" / f"{f0 / 1e9:.2f}GHz_a_theta.npy")
+    np.testing.assert_array_equal(a_theta, got[0, 0])
+    f_theta = np.load(tmp_path / "ff" / f"{f0 / 1e9:.2f}GHz_f_theta.npy")
+    np.testing.assert_array_equal(f_theta, got[0, 3])

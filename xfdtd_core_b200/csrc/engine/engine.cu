@@ -23,6 +23,7 @@
 #include "march_tma.cuh"
 #include "fmarch.cuh"
 #include "fvec.cuh"
+#include "farfield.cuh"
 #include "kernels.cuh"
 #include "xfd_engine.h"
 
@@ -1321,6 +1322,105 @@ xfd_status xfd_set_nf2ff(xfd_engine* e, const xfd_nf2ff_desc* d) {
   e->nf_last_flush_step = e->host_step;
   e->graph_dirty = true;
   return XFD_OK;
+}
+
+xfd_status xfd_nf2ff_far_field(xfd_engine* e, const xfd_far_field_desc* d, double* out,
+                               int64_t capacity) {
+  if (!e || !e->have_nf2ff) return fail(e, XFD_ERR_STATE, "no NF2FF");
+  if (!d || !out || !d->theta || !d->phi || !d->freqs || d->n_angles < 1)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad far-field arguments");
+  const Nf2ffD& nf = e->nf2ff;
+  if (d->n_freq != nf.nf)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "far field: %d frequencies, NF2FF has %d",
+                d->n_freq, nf.nf);
+  const long long total = (long long)nf.nf * 4 * d->n_angles;
+  if (capacity < total) return fail(e, XFD_ERR_INVALID_ARGUMENT, "far-field buffer too small");
+  const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+  for (int a = 0; a < 3; ++a)
+    if (!d->node_e[a] || !d->node_h[a] || !d->size_e[a])
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "null grid axis %d", a);
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status st = flush_nf2ff(e);
+  if (st != XFD_OK) return st;
+  // Host tables: per angle the theta-hat / phi-hat components of x, y, z and
+  // sin(theta) cos/sin(phi) (cCSToSCSTransformMatrix), per frequency 2 pi f / c.
+  const int na = d->n_angles;
+  std::vector<double> ang((size_t)na * 8), cos_t(na), k0(nf.nf);
+  for (int q = 0; q < na; ++q) {
+    const double ct = std::cos(d->theta[q]), stt = std::sin(d->theta[q]);
+    const double cp = std::cos(d->phi[q]), sp = std::sin(d->phi[q]);
+    double* T = &ang[(size_t)q * 8];
+    T[0] = ct * cp;
+    T[1] = ct * sp;
+    T[2] = -1 * stt;
+    T[3] = -1 * sp;
+    T[4] = cp;
+    T[5] = 0.0;
+    T[6] = stt * cp;
+    T[7] = stt * sp;
+    cos_t[q] = ct;
+  }
+  const double pi = 3.14159265358979323846;
+  const double eps0 = 8.854187817e-12, mu0 = 4 * pi * 1e-7;
+  const double c0 = 1 / std::sqrt(eps0 * mu0);
+  for (int f = 0; f < nf.nf; ++f) k0[f] = 2.0 * pi * d->freqs[f] / c0;
+  // Temporary device copies (freed before returning).
+  std::vector<void*> tmp;
+  auto up = [&](const double* src, size_t count, const double** dst) -> xfd_status {
+    void* p = nullptr;
+    cudaError_t c = cudaMalloc(&p, count * sizeof(double));
+    if (c != cudaSuccess) return fail(e, XFD_ERR_OUT_OF_MEMORY, "far field: %s", cudaGetErrorString(c));
+    tmp.push_back(p);
+    c = cudaMemcpyAsync(p, src, count * sizeof(double), cudaMemcpyHostToDevice, e->stream);
+    if (c != cudaSuccess) return fail(e, XFD_ERR_CUDA, "far field: %s", cudaGetErrorString(c));
+    *dst = static_cast<const double*>(p);
+    return XFD_OK;
+  };
+  FarFieldD fd{};
+  fd.nf = nf.nf;
+  fd.n_ang = na;
+  fd.P = nf.P;
+  for (int f = 0; f < 7; ++f) fd.begin[f] = nf.begin[f];
+  for (int f = 0; f < 6; ++f)
+    for (int a = 0; a < 3; ++a) {
+      fd.s[f][a] = nf.s[f][a];
+      fd.e[f][a] = nf.e[f][a];
+    }
+  fd.acc = nf.acc;
+  for (int a = 0; a < 3; ++a) fd.origin[a] = d->origin[a];
+  xfd_status s2 = XFD_OK;
+  double2* dout = nullptr;
+  do {
+    if ((s2 = up(ang.data(), ang.size(), &fd.ang)) != XFD_OK) break;
+    if ((s2 = up(cos_t.data(), cos_t.size(), &fd.cos_t)) != XFD_OK) break;
+    if ((s2 = up(k0.data(), k0.size(), &fd.k0)) != XFD_OK) break;
+    for (int a = 0; a < 3 && s2 == XFD_OK; ++a) {
+      if ((s2 = up(d->node_e[a], (size_t)n[a] + 1, &fd.node_e[a])) != XFD_OK) break;
+      if ((s2 = up(d->node_h[a], (size_t)n[a], &fd.node_h[a])) != XFD_OK) break;
+      s2 = up(d->size_e[a], (size_t)n[a], &fd.size_e[a]);
+    }
+    if (s2 != XFD_OK) break;
+    cudaError_t c = cudaMalloc(reinterpret_cast<void**>(&dout), total * sizeof(double2));
+    if (c != cudaSuccess) {
+      s2 = fail(e, XFD_ERR_OUT_OF_MEMORY, "far field: %s", cudaGetErrorString(c));
+      break;
+    }
+    tmp.push_back(dout);
+    fd.out = dout;
+    if (nf.P > 0) {
+      k_far_field<<<dim3((unsigned)na, (unsigned)nf.nf), 256, 0, e->stream>>>(fd);
+    } else {
+      cudaMemsetAsync(dout, 0, total * sizeof(double2), e->stream);
+    }
+    c = cudaGetLastError();
+    if (c == cudaSuccess)
+      c = cudaMemcpyAsync(out, dout, total * sizeof(double2), cudaMemcpyDeviceToHost, e->stream);
+    if (c == cudaSuccess) c = cudaStreamSynchronize(e->stream);
+    if (c != cudaSuccess) s2 = fail(e, XFD_ERR_CUDA, "far field: %s", cudaGetErrorString(c));
+  } while (false);
+  cudaStreamSynchronize(e->stream);
+  for (void* p : tmp) cudaFree(p);
+  return s2;
 }
 
 xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* count) {

@@ -373,6 +373,33 @@ int xfdtd_scene_nf2ff(xfdtd_scene* s, double* out, int64_t capacity, int64_t* co
   })
 }
 
+int xfdtd_scene_far_field(xfdtd_scene* s, int32_t n_theta, const double* theta, int32_t n_phi,
+                          const double* phi, const double origin[3], double* out,
+                          int64_t capacity, int64_t* count, const char* dir,
+                          const char* sub_dir) {
+  HOST_TRY({
+    if (!s || !s->nf2ff) throw XFDTDException("scene has no NF2FF");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    if (!theta || !phi || n_theta < 1 || n_phi < 1) throw XFDTDException("bad angles");
+    Array1D<Real> th(std::vector<Real>(theta, theta + n_theta));
+    Array1D<Real> ph(std::vector<Real>(phi, phi + n_phi));
+    const Vector o = origin ? Vector{origin[0], origin[1], origin[2]} : Vector{0, 0, 0};
+    const auto data = s->nf2ff->farField(th, ph, o);
+    if (count) *count = (int64_t)data.size();
+    if (out) {
+      if ((std::size_t)capacity < data.size()) throw XFDTDException("buffer too small");
+      for (std::size_t q = 0; q < data.size(); ++q) {
+        out[2 * q] = data[q].real();
+        out[2 * q + 1] = data[q].imag();
+      }
+    }
+    if (sub_dir) {
+      if (dir) s->nf2ff->setOutputDir(dir);
+      s->nf2ff->processFarField(th, ph, sub_dir, o);
+    }
+  })
+}
+
 int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir) {
   HOST_TRY({
     if (!s || !dir) throw XFDTDException("null argument");

@@ -14,6 +14,7 @@
 //   TFSF incident grid     src/waveform_source/tfsf.cpp:36-302
 //   ADE coefficients       src/material/ade_method/{m_lor,drude,debye}_ade_method.cpp
 //   NF2FF surfaces/phasors src/nffft/nffft.cpp:88-245, nffft_fd_data.cpp:65-76
+//   NF2FF far field        src/nffft/nffft_fd_data_process.cpp:15-144 (on the GPU)
 // Instead of 18 full-grid coefficient arrays the engine receives a table of
 // material classes (the (ca, cb) pair of each component, keyed by the
 // materials of the 2x2x2 cells around a lattice node) plus a uint16 class per
@@ -21,6 +22,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
 #include <limits>
 #include <map>
 #include <numeric>
@@ -243,6 +247,8 @@ Simulation::Simulation(Real dx, Real dy, Real dz, Real cfl, ThreadConfig)
     : _dl{dx, dy, dz}, _cfl{cfl}, _impl{std::make_unique<Impl>()} {}
 
 Simulation::~Simulation() {
+  for (auto& nf : _nffts)
+    if (nf) nf->_engine = nullptr;
   if (_engine) xfd_destroy(_engine);
 }
 
@@ -1158,6 +1164,100 @@ void Simulation::setupNf2ff(xfd_engine* E) {
   // (nffft_frequency_domain.cpp:45-53).
   desc.scale = (double)freqs.size();
   checkStatus(E, xfd_set_nf2ff(E, &desc), "xfd_set_nf2ff");
+  // Grid geometry for the far-field transform (GridSpace e/h nodes, e sizes).
+  nf._engine = E;
+  for (int a = 0; a < 3; ++a) {
+    nf._node_e[a] = _impl->e_node[a];
+    nf._node_h[a] = _impl->h_node[a];
+    nf._size_e[a] = _impl->e_size[a];
+  }
+}
+
+}  // namespace xfdtd
+
+// ---------------------------------------------------------------- far field
+namespace xfdtd {
+
+std::vector<std::complex<Real>> NFFFTFrequencyDomain::farField(const Array1D<Real>& theta,
+                                                               const Array1D<Real>& phi,
+                                                               const Vector& origin) const {
+  if (theta.size() == 0 || phi.size() == 0) throw XFDTDException("Invalid theta or phi size");
+  if (theta.size() != 1 && phi.size() != 1)
+    throw XFDTDException("There must be only one theta or phi");
+  if (!_engine) throw XFDTDException("far field: the simulation of this NF2FF is not running");
+  // The angle list of the reference's broadcast of theta against phi.
+  const std::size_t n = theta.size() * phi.size();
+  std::vector<double> th(n), ph(n);
+  for (std::size_t q = 0; q < n; ++q) {
+    th[q] = theta.size() == 1 ? theta[0] : theta[q];
+    ph[q] = phi.size() == 1 ? phi[0] : phi[q];
+  }
+  xfd_far_field_desc d{};
+  d.n_angles = (int32_t)n;
+  d.theta = th.data();
+  d.phi = ph.data();
+  d.n_freq = (int32_t)_freqs.size();
+  d.freqs = _freqs.data();
+  d.origin[0] = origin.x();
+  d.origin[1] = origin.y();
+  d.origin[2] = origin.z();
+  for (int a = 0; a < 3; ++a) {
+    d.node_e[a] = _node_e[a].data();
+    d.node_h[a] = _node_h[a].data();
+    d.size_e[a] = _size_e[a].data();
+  }
+  std::vector<std::complex<Real>> out(_freqs.size() * 4 * n);
+  const int st = xfd_nf2ff_far_field(_engine, &d, reinterpret_cast<double*>(out.data()),
+                                     (int64_t)out.size());
+  if (st != XFD_OK)
+    throw XFDTDException(std::string("xfd_nf2ff_far_field: ") + xfd_last_error(_engine));
+  return out;
+}
+
+namespace {
+void writeComplexNpy(const std::string& path, const std::complex<Real>* data, std::size_t n) {
+  std::ostringstream hdr;
+  hdr << "{'descr': '<c16', 'fortran_order': False, 'shape': (" << n << ",), }";
+  std::string h = hdr.str();
+  const std::size_t total = 10 + h.size() + 1;
+  h.append((64 - total % 64) % 64, ' ');
+  h.push_back('\n');
+  std::ofstream f(path, std::ios::binary);
+  if (!f) throw XFDTDException("cannot write " + path);
+  f.write("\x93NUMPY\x01\x00", 8);
+  const uint16_t len = static_cast<uint16_t>(h.size());
+  f.write(reinterpret_cast<const char*>(&len), 2);
+  f.write(h.data(), (std::streamsize)h.size());
+  f.write(reinterpret_cast<const char*>(data), (std::streamsize)(n * sizeof(std::complex<Real>)));
+}
+}  // namespace
+
+void NFFFTFrequencyDomain::processFarField(const Array1D<Real>& theta, const Array1D<Real>& phi,
+                                           const std::string& sub_dir,
+                                           const Vector& origin) const {
+  const auto data = farField(theta, phi, origin);
+  const std::size_t n = theta.size() * phi.size();
+  const std::filesystem::path dir = std::filesystem::path(_output_dir) / sub_dir;
+  std::filesystem::create_directories(dir);
+  static const char* names[4] = {"_a_theta.npy", "_f_phi.npy", "_a_phi.npy", "_f_theta.npy"};
+  for (std::size_t f = 0; f < _freqs.size(); ++f) {
+    std::ostringstream ss;
+    ss << std::fixed << std::setprecision(2) << _freqs[f] / 1e9 << "GHz";
+    for (int r = 0; r < 4; ++r)
+      writeComplexNpy((dir / (ss.str() + names[r])).string(), data.data() + (f * 4 + r) * n, n);
+  }
+}
+
+void NFFFTFrequencyDomain::processFarField(const Array1D<Real>& theta, Real phi,
+                                           const std::string& sub_dir,
+                                           const Vector& origin) const {
+  processFarField(theta, Array1D<Real>{phi}, sub_dir, origin);
+}
+
+void NFFFTFrequencyDomain::processFarField(Real theta, const Array1D<Real>& phi,
+                                           const std::string& sub_dir,
+                                           const Vector& origin) const {
+  processFarField(Array1D<Real>{theta}, phi, sub_dir, origin);
 }
 
 }  // namespace xfdtd

@@ -62,6 +62,13 @@ class Nf2ffStepDesc(ctypes.Structure):
                 ("step", _i64), ("scale", ctypes.c_double), ("acc", ctypes.c_void_p)]
 
 
+class FarFieldDesc(ctypes.Structure):
+    """xfd_far_field_desc."""
+    _fields_ = [("n_angles", _i32), ("theta", _dp), ("phi", _dp), ("n_freq", _i32),
+                ("freqs", _dp), ("origin", ctypes.c_double * 3), ("node_e", _dp * 3),
+                ("node_h", _dp * 3), ("size_e", _dp * 3)]
+
+
 class EngineError(RuntimeError):
     pass
 
@@ -110,6 +117,7 @@ def load(build_if_missing: bool = True):
         "xfd_set_option": ([vp, ctypes.c_char_p, _i64], ctypes.c_int),
         "xfd_get_option": ([vp, ctypes.c_char_p, ctypes.POINTER(_i64)], ctypes.c_int),
         "xfd_nf2ff_step_static": ([ctypes.POINTER(Nf2ffStepDesc), vp], ctypes.c_int),
+        "xfd_nf2ff_far_field": ([vp, ctypes.POINTER(FarFieldDesc), _dp, _i64], ctypes.c_int),
         "xfd_stream": ([vp], vp),
         "xfd_launches_per_step": ([vp], _i32),
         "xfd_stencil_bytes_per_step": ([vp], _i64),
@@ -129,7 +137,8 @@ def exported_symbols() -> List[str]:
             "xfd_set_ade", "xfd_set_nf2ff", "xfd_get_nf2ff", "xfd_add_movie",
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
-            "xfd_get_option", "xfd_nf2ff_step_static", "xfd_stream", "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
+            "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
+            "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
 
 
 def _f64(a) -> np.ndarray:

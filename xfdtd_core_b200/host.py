@@ -51,6 +51,8 @@ def load():
                               ctypes.POINTER(i32)], ctypes.c_int),
         "xfdtd_scene_movie": ([vp, i32, _dp, i64, ctypes.POINTER(i64), i32 * 3], ctypes.c_int),
         "xfdtd_scene_nf2ff": ([vp, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "xfdtd_scene_far_field": ([vp, i32, _dp, i32, _dp, _dp, _dp, i64, ctypes.POINTER(i64),
+                                   ctypes.c_char_p, ctypes.c_char_p], ctypes.c_int),
         "xfdtd_scene_field_time": ([vp, i32, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
         "xfdtd_scene_write_outputs": ([vp, ctypes.c_char_p], ctypes.c_int),
     }
@@ -64,9 +66,10 @@ def load():
 
 def exported_symbols() -> List[str]:
     return ["xfdtd_scene_open", "xfdtd_scene_close", "xfdtd_host_last_error",
-            "xfdtd_scene_engine", "xfdtd_scene_set_engine_option", "xfdtd_scene_info", "xfdtd_scene_advance", "xfdtd_scene_tfsf",
-            "xfdtd_scene_finish", "xfdtd_scene_coefficients", "xfdtd_scene_field",
-            "xfdtd_scene_movie", "xfdtd_scene_nf2ff", "xfdtd_scene_field_time",
+            "xfdtd_scene_engine", "xfdtd_scene_set_engine_option", "xfdtd_scene_info",
+            "xfdtd_scene_advance", "xfdtd_scene_tfsf", "xfdtd_scene_finish",
+            "xfdtd_scene_coefficients", "xfdtd_scene_field", "xfdtd_scene_movie",
+            "xfdtd_scene_nf2ff", "xfdtd_scene_far_field", "xfdtd_scene_field_time",
             "xfdtd_scene_write_outputs"]
 
 
@@ -191,6 +194,25 @@ class SceneRun:
         self._check(self.L.xfdtd_scene_nf2ff(self.h, out.ctypes.data_as(_dp), cnt.value,
                                              ctypes.byref(cnt)))
         return out[0::2] + 1j * out[1::2]
+
+    def far_field(self, theta, phi, origin=(0.0, 0.0, 0.0), directory: Optional[str] = None,
+                  sub_dir: Optional[str] = None) -> np.ndarray:
+        """Far-field potentials computed on the GPU: complex
+        [n_freq, 4 (a_theta, f_phi, a_phi, f_theta), n_angles]; with `sub_dir`
+        the per-frequency .npy files of processFarField are written too."""
+        th = np.ascontiguousarray(np.atleast_1d(theta), dtype=np.float64)
+        ph = np.ascontiguousarray(np.atleast_1d(phi), dtype=np.float64)
+        org = np.ascontiguousarray(origin, dtype=np.float64)
+        cnt = ctypes.c_int64()
+        args = (self.h, th.size, th.ctypes.data_as(_dp), ph.size, ph.ctypes.data_as(_dp),
+                org.ctypes.data_as(_dp))
+        self._check(self.L.xfdtd_scene_far_field(*args, None, 0, ctypes.byref(cnt), None, None))
+        out = np.empty(2 * cnt.value)
+        self._check(self.L.xfdtd_scene_far_field(
+            *args, out.ctypes.data_as(_dp), cnt.value, ctypes.byref(cnt),
+            directory.encode() if directory else None, sub_dir.encode() if sub_dir else None))
+        n_ang = th.size * ph.size
+        return (out[0::2] + 1j * out[1::2]).reshape(-1, 4, n_ang)
 
     def write_outputs(self, directory: str):
         self._check(self.L.xfdtd_scene_write_outputs(self.h, directory.encode()))
