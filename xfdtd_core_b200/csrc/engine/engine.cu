@@ -120,6 +120,8 @@ struct xfd_engine {
   bool tma_ready = false;
   TmaMaps tma[2]{};       // tensor maps over buffer 0 / 1 (and the class index)
   MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
+  int2* d_xlayer = nullptr;  // per x plane: CPML layer code of the H / E layers
+  size_t xlayer_slabs = (size_t)-1;  // slab count the table was built for
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
   FvecMaps fvmaps[2]{};   // tensor maps of its two-nodes-per-thread interior form
   cudaGraphExec_t graph_exec = nullptr;
@@ -537,6 +539,7 @@ MarchP<T> march_params(xfd_engine* e) {
     p.slab[a] = f.slab[a];
   }
   p.ichunk = e->march_ichunk;
+  p.xl = e->d_xlayer;
   return p;
 }
 
@@ -744,6 +747,30 @@ xfd_status ensure_ready(xfd_engine* e) {
   if (uses_tma(e) && !e->tma_ready) {
     xfd_status st = e->precision == XFD_FP64 ? build_tma_maps<double>(e) : build_tma_maps<float>(e);
     if (st != XFD_OK) return st;
+  }
+  if (e->xlayer_slabs != e->slabs.size()) {
+    // Per x plane the layer of the x-normal CPML slabs, for the H and the E
+    // layers: (layer << 1) | slab, or -1 outside every slab.
+    std::vector<int2> xl((size_t)e->L.nx + 1, make_int2(-1, -1));
+    int q[2] = {0, 0};
+    for (const auto& S : e->slabs) {
+      if (S.m != 0) continue;
+      const int slot = q[0]++;
+      for (int l = 0; l < S.n; ++l) {
+        xl[(size_t)S.h_lo + l].x = (l << 1) | slot;
+        xl[(size_t)S.e_lo + l].y = (l << 1) | slot;
+      }
+    }
+    if (!e->d_xlayer) {
+      void* p = nullptr;
+      xfd_status st = dev_alloc(e, &p, xl.size() * sizeof(int2));
+      if (st != XFD_OK) return st;
+      e->d_xlayer = static_cast<int2*>(p);
+    }
+    CUDA_TRY(e, cudaMemcpy(e->d_xlayer, xl.data(), xl.size() * sizeof(int2),
+                           cudaMemcpyHostToDevice));
+    e->xlayer_slabs = e->slabs.size();
+    e->graph_dirty = true;
   }
   if (e->lumped_dirty) {
     // Concatenate the current sources into one device list.

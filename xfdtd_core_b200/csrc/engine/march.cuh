@@ -34,6 +34,7 @@ struct MarchP {
   const T* fh[3];
   SlabAxisD<T> slab[3];  // psi_h_in == psi_h_out
   int ichunk;
+  const int2* xl;  // per x plane: (layer << 1 | slab) of the H (.x) / E (.y) layers, or -1
 };
 
 // CPML layer of coordinate x along a slab axis: the layer index, or -1, and

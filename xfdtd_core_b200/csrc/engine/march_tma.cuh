@@ -236,7 +236,9 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
     pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
     pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
     int qx = 0;
-    const int lx = act ? layer_of(p.slab[0], i, false, qx) : -1;
+    const int cx = p.xl[i].x;
+    const int lx = (act && cx >= 0) ? (cx >> 1) : -1;
+    qx = cx & 1;
     const long long ox = (long long)lx * PS + row;
     pv[2] = lx >= 0 ? p.slab[0].psi_h_out[qx][0][ox] : T(0);
     pv[4] = lx >= 0 ? p.slab[0].psi_h_out[qx][1][ox] : T(0);
@@ -286,7 +288,9 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
       const T dEx_j = ex_j - ex, dEy_i = ey_n - ey;  // Hz
       const long long o = i * PS;
       int qx = 0;
-      const int lx = CP ? layer_of(p.slab[0], i, false, qx) : -1;
+      const int cx = CP ? p.xl[i].x : -1;
+      const int lx = cx >= 0 ? (cx >> 1) : -1;
+      qx = cx & 1;
       if (jv && kv) {
         const T ca = r[0], cb = r[1];
         T h = tile(sc, 0)[tq];
@@ -435,7 +439,9 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
     pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
     pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
     int qx = 0;
-    const int lx = act ? layer_of(p.slab[0], i, true, qx) : -1;
+    const int cx = p.xl[i].y;
+    const int lx = (act && cx >= 0) ? (cx >> 1) : -1;
+    qx = cx & 1;
     const long long ox = (long long)lx * PS + row;
     pv[2] = lx >= 0 ? p.slab[0].psi_e[qx][0][ox] : T(0);
     pv[4] = lx >= 0 ? p.slab[0].psi_e[qx][1][ox] : T(0);
@@ -488,7 +494,9 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
       const T dHy_i = hy - hy_p, dHx_j = hx - hx_j;  // Ez
       const long long o = i * PS;
       int qx = 0;
-      const int lx = CP ? layer_of(p.slab[0], i, true, qx) : -1;
+      const int cx = CP ? p.xl[i].y : -1;
+      const int lx = cx >= 0 ? (cx >> 1) : -1;
+      qx = cx & 1;
       if (iv) {
         const T ca = r[0], cb = r[1];
         T e = tile(sc, 0)[tq];
