@@ -395,14 +395,18 @@ xfd_status build_tma_maps(xfd_engine* e) {
   CUDA_TRY(e, cudaFuncSetAttribute(k_fused_tma<T, kTJ, kTK, S>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem(S)));
   constexpr int MS = march_stages<T>();
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS, true>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS, true, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, true>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, true, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
   constexpr int MF = march_free_stages<T>();
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MF, false>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MF, false, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MF, false>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MF, false, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MF, false, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MF, false, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
   e->tma_ready = true;
   return XFD_OK;
@@ -657,17 +661,28 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     const size_t msm = MarchGeom<T, 8, 32>::smem(MS);
     constexpr int MF = march_free_stages<T>();
     const size_t msm_free = MarchGeom<T, 8, 32>::smem(MF);
-    auto launch_march = [&](auto kfree, auto kcp) {
+    // The box is away from every lattice boundary when no tile holds k = 0,
+    // j = 0 or a node past nz-1 / ny-1 and no chunk holds plane 0 or nx.
+    const bool m_in = mbox && mlo[0] >= 1 && 32 * mhi[0] <= e->L.nz && mlo[1] >= 1 &&
+                      8 * mhi[1] <= e->L.ny && mlo[2] >= 1 &&
+                      mhi[2] * e->march_ichunk <= e->L.nx;
+    auto launch_march = [&](auto kfree, auto kfree_in, auto kcp) {
       if (mbox) {
         MarchTmaP<T> q = mtp;
         for (int a = 0; a < 3; ++a) q.org[a] = mlo[a];
-        kfree<<<dim3(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]), blk, msm_free, s>>>(q);
+        const dim3 g(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]);
+        if (m_in)
+          kfree_in<<<g, blk, msm_free, s>>>(q);
+        else
+          kfree<<<g, blk, msm_free, s>>>(q);
       }
       kcp<<<grd_m, blk, msm, s>>>(mtp);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma) {
-      launch_march(k_march_h_tma<T, 8, 32, MF, false>, k_march_h_tma<T, 8, 32, MS, true>);
+      launch_march(k_march_h_tma<T, 8, 32, MF, false, false>,
+                   k_march_h_tma<T, 8, 32, MF, false, true>,
+                   k_march_h_tma<T, 8, 32, MS, true, false>);
       k_edge_h<T><<<edge_blocks, 256, 0, s>>>(yp);
     }
     else if (march)
@@ -685,7 +700,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
     if (march_tma) {
-      launch_march(k_march_e_tma<T, 8, 32, MF, false>, k_march_e_tma<T, 8, 32, MS, true>);
+      launch_march(k_march_e_tma<T, 8, 32, MF, false, false>,
+                   k_march_e_tma<T, 8, 32, MF, false, true>,
+                   k_march_e_tma<T, 8, 32, MS, true, false>);
       k_edge_e<T><<<edge_blocks, 256, 0, s>>>(yp);
     }
     else if (march)

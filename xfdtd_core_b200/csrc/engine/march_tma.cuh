@@ -44,6 +44,9 @@ struct MarchMaps {
 // Work split as for the fused marching sweep: CP = false forms sweep the
 // box of tiles and chunks whose nodes lie in no CPML layer, with their grid
 // offset by `org`; CP = true forms take the full grid and skip that box.
+// IN = true (CP = false only) is for a box away from every lattice boundary:
+// all nodes of its tiles have every component in range and the full main
+// update, so the form carries no range tests.
 template <typename T>
 struct MarchTmaP {
   MarchP<T> p;
@@ -133,7 +136,7 @@ struct StageRing {
 // H sweep.  Planes q = 0 .. n_planes of the chunk are staged (plane n_planes
 // is i_hi, E only, when i_hi <= nx); plane q lives in stage q % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S, bool CP>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN>
 __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ MarchTmaP<T> P) {
   using G = MarchGeom<T, TJ, TK>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -192,11 +195,11 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
 
   // Per-thread constants (as k_march_h).  The faces k = nz and j = ny are
   // left to k_edge_h (kernels.cuh).
-  const bool act = k < L.nz && j < L.ny;
+  const bool act = IN || (k < L.nz && j < L.ny);
   const long long PS = (long long)L.NY * L.KP;
   const int KP = L.KP;
   const long long row = (long long)j * KP + k;
-  const bool jv = j < L.ny, kv = k < L.nz;
+  const bool jv = IN || j < L.ny, kv = IN || k < L.nz;
   const T fhj = (act && jv) ? p.fh[1][j] : T(0);
   const T fhk = (act && kv) ? p.fh[2][k] : T(0);
   int qy = 0, qz = 0;
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
   if (n_staged > 0) ok = ring.wait(0);
   for (int q = 0; q < n_planes; ++q) {
     const int i = i_lo + q;
-    const bool iv = i < L.nx;
+    const bool iv = IN || i < L.nx;
     const int sc = q % S, sn = (q + 1) % S;
     T po[6];
 #pragma unroll
@@ -335,7 +338,7 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
 // E sweep.  Staged planes q = -1 .. n_planes-1 (plane -1 = i_lo-1, H only,
 // when i_lo >= 1); plane q lives in stage (q+1) % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S, bool CP>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN>
 __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ MarchTmaP<T> P) {
   using G = MarchGeom<T, TJ, TK>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -395,12 +398,12 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
   for (int q = q_first; q < q_first + S && q < q_end; ++q) ring.pending |= 1u << slot(q);
   stage_half_table<T, G::NC, TJ * TK>(sT, p.tab, p.n_classes, 0, tid);
 
-  const bool act = k < L.nz && j < L.ny;  // faces k = nz, j = ny: k_edge_e
+  const bool act = IN || (k < L.nz && j < L.ny);  // faces k = nz, j = ny: k_edge_e
   const long long PS = (long long)L.NY * L.KP;
   const int KP = L.KP;
   const long long row = (long long)j * KP + k;
-  const bool jv = j < L.ny, kv = k < L.nz;
-  const bool jm = j >= 1 && jv, km = k >= 1 && kv;
+  const bool jv = IN || j < L.ny, kv = IN || k < L.nz;
+  const bool jm = IN || (j >= 1 && jv), km = IN || (k >= 1 && kv);
   const T fej = act ? p.fe[1][j] : T(0);
   const T fek = act ? p.fe[2][k] : T(0);
   int qy = 0, qz = 0;
@@ -475,7 +478,7 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
       ring.pending |= 1u << slot(q - 2);
     }
     if (act) {
-      const bool iv = i < L.nx, i1 = i >= 1;
+      const bool iv = IN || i < L.nx, i1 = IN || i >= 1;
       const bool im = i1 && iv;
       const T fei = p.fe[0][i];
       const int cl = ctile(sc)[tq];
