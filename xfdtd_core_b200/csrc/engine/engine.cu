@@ -260,6 +260,7 @@ constexpr int kTJ = 8, kTK = 32;
 
 constexpr int kStagesF32 = 4, kStagesF64 = 3;
 constexpr int kMarchStagesF32 = 6, kMarchStagesF64 = 4;
+constexpr int kMTJ = 8;  // rows (warps) per CTA of the TMA marching sweeps
 template <typename T>
 constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32; }
 // The CPML-free forms need fewer registers, so they run more CTAs per SM;
@@ -337,17 +338,17 @@ xfd_status build_tma_maps(xfd_engine* e) {
     if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (class): %d", (int)r);
   }
   // Marching sweeps: halo and tile boxes of every component, class tiles.
-  using MG = MarchGeom<T, 8, 32>;
+  using MG = MarchGeom<T, kMTJ, 32>;
   for (int b = 0; b < 2; ++b) {
     for (int c = 0; c < 6; ++c) {
       CUresult r = encode_lattice(encode, &e->mtma[b].halo[c], dt, sizeof(T), e->fbuf[b][c], L,
                                   MG::W, MG::R);
       if (r == CUDA_SUCCESS)
-        r = encode_lattice(encode, &e->mtma[b].tile[c], dt, sizeof(T), e->fbuf[b][c], L, 32, 8);
+        r = encode_lattice(encode, &e->mtma[b].tile[c], dt, sizeof(T), e->fbuf[b][c], L, 32, kMTJ);
       if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march %d): %d", c, (int)r);
     }
     CUresult r = encode_lattice(encode, &e->mtma[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, e->cls,
-                                L, 32, 8);
+                                L, 32, kMTJ);
     if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march class): %d", (int)r);
   }
   // Fused marching sweep: E (TJ+1 rows) and H (TJ rows) boxes of width
@@ -395,18 +396,18 @@ xfd_status build_tma_maps(xfd_engine* e) {
   CUDA_TRY(e, cudaFuncSetAttribute(k_fused_tma<T, kTJ, kTK, S>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem(S)));
   constexpr int MS = march_stages<T>();
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MS, true, false>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, kMTJ, 32, MS, true, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MS, true, false>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, kMTJ, 32, MS, true, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS)));
   constexpr int MF = march_free_stages<T>();
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MF, false, false>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, kMTJ, 32, MF, false, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MF, false, false>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, kMTJ, 32, MF, false, false>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, 8, 32, MF, false, true>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_tma<T, kMTJ, 32, MF, false, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
-  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, 8, 32, MF, false, true>,
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, kMTJ, 32, MF, false, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
   e->tma_ready = true;
   return XFD_OK;
@@ -499,9 +500,9 @@ void fmarch_split(const xfd_engine* e, int nt[3], int lo[3], int hi[3]) {
 // the split marching sweeps whose nodes lie in no CPML layer of either phase.
 void march_split(const xfd_engine* e, int lo[3], int hi[3]) {
   const Lat& L = e->L;
-  const int nt[3] = {(L.nz + 31) / 32, (L.ny + 7) / 8,
+  const int nt[3] = {(L.nz + 31) / 32, (L.ny + kMTJ - 1) / kMTJ,
                      (L.nx + 1 + e->march_ichunk - 1) / e->march_ichunk};
-  const int size[3] = {32, 8, e->march_ichunk};
+  const int size[3] = {32, kMTJ, e->march_ichunk};
   const int n_nodes[3] = {L.nz, L.ny, L.nx + 1};
   const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
   for (int g = 0; g < 3; ++g) {
@@ -644,7 +645,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     // The TMA marching sweeps tile k < nz, j < ny (the faces k = nz, j = ny
     // go to k_edge_h / k_edge_e); the plain marching sweeps tile all nodes.
     const dim3 grd_m(march_tma ? (unsigned)((e->L.nz + 31) / 32) : grd.x,
-                     march_tma ? (unsigned)((e->L.ny + 7) / 8) : grd.y,
+                     march_tma ? (unsigned)((e->L.ny + kMTJ - 1) / kMTJ) : grd.y,
                      (unsigned)((e->L.nx + 1 + mp.ichunk - 1) / std::max(1, mp.ichunk)));
     const unsigned edge_blocks = (unsigned)((edge_nodes(e->L) + 255) / 256);
     // The CPML-free box of (k tile, j tile, chunk) for the TMA marching sweeps.
@@ -658,13 +659,14 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
         mtp.box_hi[a] = mbox ? mhi[a] : 0;
       }
     }
-    const size_t msm = MarchGeom<T, 8, 32>::smem(MS);
+    const dim3 blk_m(32, kMTJ, 1);
+    const size_t msm = MarchGeom<T, kMTJ, 32>::smem(MS);
     constexpr int MF = march_free_stages<T>();
-    const size_t msm_free = MarchGeom<T, 8, 32>::smem(MF);
+    const size_t msm_free = MarchGeom<T, kMTJ, 32>::smem(MF);
     // The box is away from every lattice boundary when no tile holds k = 0,
     // j = 0 or a node past nz-1 / ny-1 and no chunk holds plane 0 or nx.
     const bool m_in = mbox && mlo[0] >= 1 && 32 * mhi[0] <= e->L.nz && mlo[1] >= 1 &&
-                      8 * mhi[1] <= e->L.ny && mlo[2] >= 1 &&
+                      kMTJ * mhi[1] <= e->L.ny && mlo[2] >= 1 &&
                       mhi[2] * e->march_ichunk <= e->L.nx;
     auto launch_march = [&](auto kfree, auto kfree_in, auto kcp) {
       if (mbox) {
@@ -672,17 +674,17 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
         for (int a = 0; a < 3; ++a) q.org[a] = mlo[a];
         const dim3 g(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]);
         if (m_in)
-          kfree_in<<<g, blk, msm_free, s>>>(q);
+          kfree_in<<<g, blk_m, msm_free, s>>>(q);
         else
-          kfree<<<g, blk, msm_free, s>>>(q);
+          kfree<<<g, blk_m, msm_free, s>>>(q);
       }
-      kcp<<<grd_m, blk, msm, s>>>(mtp);
+      kcp<<<grd_m, blk_m, msm, s>>>(mtp);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma) {
-      launch_march(k_march_h_tma<T, 8, 32, MF, false, false>,
-                   k_march_h_tma<T, 8, 32, MF, false, true>,
-                   k_march_h_tma<T, 8, 32, MS, true, false>);
+      launch_march(k_march_h_tma<T, kMTJ, 32, MF, false, false>,
+                   k_march_h_tma<T, kMTJ, 32, MF, false, true>,
+                   k_march_h_tma<T, kMTJ, 32, MS, true, false>);
       k_edge_h<T><<<edge_blocks, 256, 0, s>>>(yp);
     }
     else if (march)
@@ -700,9 +702,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
     if (march_tma) {
-      launch_march(k_march_e_tma<T, 8, 32, MF, false, false>,
-                   k_march_e_tma<T, 8, 32, MF, false, true>,
-                   k_march_e_tma<T, 8, 32, MS, true, false>);
+      launch_march(k_march_e_tma<T, kMTJ, 32, MF, false, false>,
+                   k_march_e_tma<T, kMTJ, 32, MF, false, true>,
+                   k_march_e_tma<T, kMTJ, 32, MS, true, false>);
       k_edge_e<T><<<edge_blocks, 256, 0, s>>>(yp);
     }
     else if (march)
