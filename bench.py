@@ -37,10 +37,23 @@ if ROOT not in sys.path:
 METRIC = "Gcell-updates/s"
 UNIT = "Gcell/s"
 WORKLOAD = "dielectric_boxes_256^3_cpml12_64boxes_dipole"
+KIND = "boxes"  # --workload: boxes (the default) or dispersive
+
+
+def workload_name(n: int) -> str:
+    if KIND == "dispersive":
+        return f"dispersive_spheres_{n}^3_cpml10_ade3_tfsf_nf2ff32"
+    return WORKLOAD if n == 256 else f"dielectric_boxes_{n}^3_cpml12_64boxes_dipole"
 
 
 def workload_scene(steps: int, n: int = 256):
+    """The bench scenes, synthetic and seeded: `boxes` = 64 random dielectric
+    boxes with a dipole in a 12-cell CPML; `dispersive` = three ADE spheres
+    (Drude, Lorentz, Debye) lit by a TFSF plane wave with a 32-frequency NF2FF
+    box inside a 10-cell CPML."""
     from xfdtd_core_b200 import scene as S
+    if KIND == "dispersive":
+        return S.dispersive_spheres(n=n, steps=steps)
     return S.dielectric_boxes(n=n, pml=12, dl=1e-3, n_boxes=64, steps=steps, seed=0)
 
 
@@ -292,6 +305,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=256, help="cells per axis incl. CPML")
+    ap.add_argument("--workload", default="boxes", choices=["boxes", "dispersive"],
+                    help="boxes: the headline dielectric-boxes scene; dispersive: ADE + TFSF + "
+                         "NF2FF spheres (use --grid 384 for its full size)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", type=int, default=None,
@@ -303,6 +319,8 @@ def main():
     ap.add_argument("--march-ichunk", type=int, default=None,
                     help="planes per CTA, split marching sweeps")
     args = ap.parse_args()
+    global KIND
+    KIND = args.workload
     warmup = max(3, args.warmup)
     steps = args.steps
 
@@ -317,7 +335,7 @@ def main():
                 "steps": k, "warmup": 1, "ms_per_step": el / k * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "cells": args.grid ** 3,
+                "config": {"workload": workload_name(args.grid), "cells": args.grid ** 3,
                            "l2": "inputs larger than L2"},
                 "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
@@ -395,13 +413,16 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": ms32 / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": cells, "grid": [nx, ny, nz],
-                       "cpml": 12, "boxes": 64, "precision": "fp32",
-                       "l2": "inputs larger than L2 (fields 6x257^3 fp32 = 407 MB)",
+            "config": {"workload": workload_name(args.grid), "cells": cells, "grid": [nx, ny, nz],
+                       "cpml": 10 if KIND == "dispersive" else 12,
+                       "boxes": 0 if KIND == "dispersive" else 64, "precision": "fp32",
+                       "l2": "inputs larger than L2 (fields 6 x (n+1)^3 x 4 B = "
+                             f"{6 * (nx + 1) ** 3 * 4 / 1e6:.0f} MB)",
                        "parallelism": f"replicas x{world}", "sweep": sweep},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm,
-                         "traffic": profiled_traffic(args.grid, kmode.value),
+                         "traffic": (profiled_traffic(args.grid, kmode.value)
+                                     if KIND == "boxes" else None),
                          "peak_source": peak_kind,
                          "kernel": "the step's sweep launches (k_march_h_tma + k_march_e_tma, "
                                    "CPML-free and CPML forms; 99% of a step's device time)",
