@@ -16,6 +16,15 @@ Lines (one JSON line on rank 0):
 Under torchrun each rank runs its own replica of the scene (the path's
 multi-GPU form in this round is replicas: no data-path collective), the
 timed region is bracketed by barriers, and the time is the max over ranks.
+
+--workload batched: 96 independent sphere scenes of uneven sizes (64^3 to
+224^3 cells, numpy default_rng(1)), each with its own TFSF plane wave at a
+random angle, FP32, advanced together through the batch entry points
+(xfd_batch_*: every phase of a step one launch over all scenes' tiles, the
+tile depth chosen by the autotuner during warm-up).  A step advances every
+scene by one time step; `value` counts the cells of all scenes.  The same
+scenes run one at a time (FP32, and the FP64 plain form) are reported under
+"forms".  Under torchrun the scenes are dealt round-robin to the ranks.
 """
 from __future__ import annotations
 
@@ -41,6 +50,8 @@ KIND = "boxes"  # --workload: boxes (the default) or dispersive
 
 
 def workload_name(n: int) -> str:
+    if KIND == "batched":
+        return "batched_spheres_96_scenes_64^3-224^3_cpml8_tfsf"
     if KIND == "dispersive":
         return f"dispersive_spheres_{n}^3_cpml10_ade3_tfsf_nf2ff32"
     return WORKLOAD if n == 256 else f"dielectric_boxes_{n}^3_cpml12_64boxes_dipole"
@@ -54,6 +65,9 @@ def workload_scene(steps: int, n: int = 256):
     from xfdtd_core_b200 import scene as S
     if KIND == "dispersive":
         return S.dispersive_spheres(n=n, steps=steps)
+    if KIND == "batched":  # the median-size scene of the batch (the CPU sample)
+        params = S.batched_sphere_params()
+        return S.batched_sphere(steps=steps, **sorted(params, key=lambda p: p["n"])[len(params) // 2])
     return S.dielectric_boxes(n=n, pml=12, dl=1e-3, n_boxes=64, steps=steps, seed=0)
 
 
@@ -254,6 +268,11 @@ def run_e2e(scene, steps: int, warmup: int, pg, device: int, options=None):
     return max_over_ranks(pg, elapsed), field_bytes, field_bytes + steps * frame_bytes
 
 
+def scene_cells(scene) -> int:
+    n = scene_n(scene)
+    return n ** 3
+
+
 def scene_n(scene) -> int:
     half = scene.objects[0].shape.size[0] / 2
     return int(round(2 * half / scene.dl[0])) + 2 * scene.pmls[0].thickness
@@ -297,17 +316,181 @@ def cpu_model() -> str:
     return "unknown"
 
 
+# ---------------------------------------------------------------- batched
+def time_alone(run, steps: int, warmup: int, device: int) -> float:
+    """One engine alone (xfd_run, its own graphs): ms for `steps` steps."""
+    import torch
+    from xfdtd_core_b200 import engine as E
+    L = E.load()
+    h = ctypes_handle(run.engine_handle())
+    _ck(L, h, L.xfd_run(h, warmup))
+    _ck(L, h, L.xfd_sync(h))
+    stream = torch.cuda.ExternalStream(int(L.xfd_stream(h)), device=device)
+    a = torch.cuda.Event(enable_timing=True)
+    z = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    _ck(L, h, L.xfd_run(h, steps))
+    z.record(stream)
+    _ck(L, h, L.xfd_sync(h))
+    return a.elapsed_time(z)
+
+
+def run_batched(args, world, rank, local, pg, warmup, steps):
+    import torch
+    torch.cuda.set_device(local)
+    from xfdtd_core_b200 import engine as E
+    from xfdtd_core_b200 import scene as S
+    from xfdtd_core_b200.host import SceneRun
+    hbm, peak_kind = peaks()
+    params = S.batched_sphere_params(args.scenes)
+    mine = params[rank::world]
+    all_cells = sum(p["n"] ** 3 for p in params)
+    seq = max(1, args.seq_steps)
+    # Warm-up holds the autotuning: 4 depths x (1 warm + K timed) steps.
+    tune = max(1, warmup // 4 - 1)
+    warm = max(warmup, 4 * (1 + tune))
+    n_total = warm + 2 * steps + seq + 36
+    t0 = time.perf_counter()
+    runs = [SceneRun(S.batched_sphere(steps=n_total, **p), precision=1) for p in mine]
+    setup_s = time.perf_counter() - t0
+    L = E.load()
+    handles = [r.engine_handle() for r in runs]
+    bytes_step = sum(int(L.xfd_stencil_bytes_per_step(ctypes_handle(h))) for h in handles)
+    batch = E.Batch(handles, {"autotune": tune})
+    batch.run(warm)
+    batch.sync()
+    tuning = batch.tuning()
+    depth = batch.get_option("march_ichunk")
+    launches = batch.launches_per_step()
+    stream = torch.cuda.ExternalStream(batch.stream(), device=local)
+
+    # device-resident: `steps` batch steps
+    sampler = ClockSampler(local)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    torch.cuda.synchronize()
+    sampler.start()
+    start.record(stream)
+    batch.run(steps)
+    end.record(stream)
+    batch.sync()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(pg)
+    ms = max_over_ranks(pg, start.elapsed_time(end))
+    value = all_cells * steps / (ms / 1e3) / 1e9
+    achieved = bytes_step / (start.elapsed_time(end) / 1e3 / steps) / 1e9
+
+    # end to end: every scene's fields uploaded from pinned host memory,
+    # `steps` batch steps, every scene's fields downloaded
+    shapes = [[E.comp_shape((p["n"],) * 3, c) for c in range(6)] for p in mine]
+    big = max(int(np.prod(s)) for sh in shapes for s in sh)
+    host_in = [torch.zeros(big, dtype=torch.float32).pin_memory() for _ in range(6)]
+    host_out = [torch.empty(big, dtype=torch.float32).pin_memory() for _ in range(6)]
+    ptr_in = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in host_in])
+    ptr_out = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in host_out])
+    field_bytes = sum(int(np.prod(s)) * 4 for sh in shapes for s in sh)
+    barrier(pg)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter()
+    start.record(stream)
+    for h in handles:
+        _ck(L, ctypes_handle(h), L.xfd_upload_fields(ctypes_handle(h), ptr_in))
+    batch.run(steps)
+    batch.sync()
+    for h in handles:
+        _ck(L, ctypes_handle(h), L.xfd_download_fields(ctypes_handle(h), ptr_out))
+    end.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_e2e
+    barrier(pg)
+    e2e_s = max_over_ranks(pg, max(start.elapsed_time(end) / 1e3, wall))
+    e2e_value = all_cells * steps / e2e_s / 1e9
+    batch.close()
+
+    # the same scenes one at a time: FP32 at the tuned depth, then FP64 plain
+    # (warm-up of one 32-step graph chunk: the timed steps run as graphs)
+    ms_alone32 = sum(time_alone(r, seq, 32, local) for r in runs)
+    for r in runs:
+        r.close()
+    ms_alone64 = 0.0
+    for p in mine:
+        r = SceneRun(S.batched_sphere(steps=seq + 36, **p), precision=0)
+        ms_alone64 += time_alone(r, seq, 32, local)
+        r.close()
+    ms_alone32 = max_over_ranks(pg, ms_alone32)
+    ms_alone64 = max_over_ranks(pg, ms_alone64)
+    v32 = all_cells * seq / (ms_alone32 / 1e3) / 1e9
+    v64 = all_cells * seq / (ms_alone64 / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        mid = sorted(params, key=lambda p: p["n"])[len(params) // 2]
+        try:
+            cv, k, threads, el = time_oracle(S.batched_sphere(steps=400, **mid),
+                                             budget_s=args.cpu_budget, max_steps=300)
+            cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{k} FDTD steps of the median scene ({mid['n']}^3) in {el:.1f} s, "
+                             f"FP64, OpenMP on {threads} threads, {cpu_model()}"}
+        except Exception as ex:  # reported, not hidden
+            cpu = {"value": None, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                   "sample": f"failed: {ex}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(0), "scenes": len(params),
+                       "cells": all_cells, "sizes": [p["n"] for p in params],
+                       "cpml": 8, "precision": "fp32",
+                       "l2": f"inputs larger than L2 (fields {12 * all_cells * 4 / 1e9:.1f} GB)",
+                       "parallelism": f"scenes round-robin over {world} GPU(s)",
+                       "sweep": "batched split H and E sweeps marching along x, TMA-staged "
+                                "planes, one launch per form over every scene's tiles",
+                       "tile_depth": depth, "autotune_ms_per_step": tuning,
+                       "host_setup_s": setup_s},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                         "kernel": "the batch step's sweep launches (k_march_h_tma_batch + "
+                                   "k_march_e_tma_batch over all scenes)",
+                         "note": "achieved = algorithmic stencil bytes per batch step "
+                                 f"({bytes_step} B summed over this rank's scenes) / batch step "
+                                 "time by CUDA events on the batch stream"},
+            "forms": {"one_at_a_time_fp32": {"value": v32, "unit": UNIT,
+                                             "steps_per_scene": seq},
+                      "one_at_a_time_fp64_plain": {"value": v64, "unit": UNIT,
+                                                   "steps_per_scene": seq},
+                      "batched_over_one_at_a_time_fp32": value / v32,
+                      "batched_over_one_at_a_time_fp64": value / v64},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": field_bytes / steps,
+                    "d2h_bytes_per_step": field_bytes / steps,
+                    "note": "C ABI with pinned host buffers: every scene's fields uploaded, "
+                            "the batch run, every scene's fields downloaded"},
+            "gpu_launches": launches * steps,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 4000; 3000 for --workload batched)")
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=256, help="cells per axis incl. CPML")
-    ap.add_argument("--workload", default="boxes", choices=["boxes", "dispersive"],
+    ap.add_argument("--workload", default="boxes", choices=["boxes", "dispersive", "batched"],
                     help="boxes: the headline dielectric-boxes scene; dispersive: ADE + TFSF + "
-                         "NF2FF spheres (use --grid 384 for its full size)")
+                         "NF2FF spheres (use --grid 384 for its full size); batched: 96 sphere "
+                         "scenes of uneven sizes advanced together")
+    ap.add_argument("--scenes", type=int, default=96, help="scenes of --workload batched")
+    ap.add_argument("--seq-steps", type=int, default=64,
+                    help="steps per scene of the one-at-a-time comparison (batched)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", type=int, default=None,
@@ -322,7 +505,7 @@ def main():
     global KIND
     KIND = args.workload
     warmup = max(3, args.warmup)
-    steps = args.steps
+    steps = args.steps if args.steps is not None else (3000 if KIND == "batched" else 4000)
 
     world, rank, local, pg = dist_setup(args.gpus)
 
@@ -333,18 +516,30 @@ def main():
         value, k, threads, el = time_oracle(scene, budget_s=60.0, max_steps=steps)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": k, "warmup": 1, "ms_per_step": el / k * 1e3,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "higher_is_better": True,
+                "scaling": "strong" if KIND == "batched" else "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_name(args.grid), "cells": args.grid ** 3,
-                           "l2": "inputs larger than L2"},
+                "config": ({"workload": workload_name(args.grid), "cells": args.grid ** 3,
+                            "l2": "inputs larger than L2"} if KIND != "batched" else
+                           {"workload": workload_name(0), "cells": scene_cells(scene),
+                            "sample": "the median-size scene of the batch"}),
                 "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{k} FDTD steps of the full {args.grid}^3 scene "
-                                           f"(requested {steps}; bounded to ~60 s), "
+                                 "sample": f"{k} FDTD steps of the "
+                                           + (f"full {args.grid}^3 scene" if KIND != "batched"
+                                              else f"median batched scene ({scene_cells(scene)} "
+                                                   "cells)")
+                                           + f" (requested {steps}; bounded to ~60 s), "
                                            f"{cpu_model()}"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+
+    if KIND == "batched":
+        run_batched(args, world, rank, local, pg, warmup, steps)
+        if pg is not None:
+            pg.destroy_process_group()
         return
 
     import torch

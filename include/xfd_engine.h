@@ -41,7 +41,8 @@ typedef enum {
   XFD_ERR_UNSUPPORTED = 3,
   XFD_ERR_STATE = 4,
   XFD_ERR_OUT_OF_MEMORY = 5,
-  XFD_ERR_NUMERIC = 6
+  XFD_ERR_NUMERIC = 6,
+  XFD_ERR_TIMEOUT = 7  /* a bounded device-side wait ran out of time */
 } xfd_status;
 
 typedef enum { XFD_FP64 = 0, XFD_FP32 = 1 } xfd_precision;
@@ -302,6 +303,50 @@ typedef struct {
 
 /* Queues the step on `stream` (a cudaStream_t; NULL = legacy default). */
 xfd_status xfd_nf2ff_step_static(const xfd_nf2ff_step_desc* d, void* stream);
+
+/* ---- Batched simulations ---------------------------------------------------
+ * No counterpart in the reference (which runs one Simulation per process):
+ * many independent simulations of uneven grid sizes -- design variants,
+ * incidence angles -- advanced together on one GPU.  Each is an engine set
+ * up as usual (xfd_create, classes, curl factors, CPML, TFSF, fields); the
+ * batch advances them with every phase of a time step one kernel launch over
+ * all their tiles (a tile work list per sweep form), captured as CUDA graphs.
+ * Per engine the arithmetic and order are those of xfd_run with the default
+ * sweep.  Engines with ADE media, lumped sources, movies or an NF2FF surface
+ * are rejected (XFD_ERR_UNSUPPORTED); all engines share one device and one
+ * precision.  The batch borrows the engines: destroy it before them, and do
+ * not call xfd_run on them while the batch runs.  After xfd_batch_run each
+ * engine's step count has advanced and its own stream is ordered after the
+ * batch, so xfd_download_fields / xfd_sync on an engine see the results. */
+typedef struct xfd_batch xfd_batch;
+
+xfd_status xfd_batch_create(xfd_engine* const* engines, int32_t n, xfd_batch** out);
+void xfd_batch_destroy(xfd_batch* b);
+/* Message of the last failure on `b` (NULL: of a failed xfd_batch_create). */
+const char* xfd_batch_last_error(const xfd_batch* b);
+
+/* Advances every engine of the batch n_steps (asynchronous; xfd_batch_sync
+ * waits and reports device-side errors of any engine). */
+xfd_status xfd_batch_run(xfd_batch* b, int64_t n_steps);
+xfd_status xfd_batch_sync(xfd_batch* b);
+
+/* Options: "graph" (0/1, default 1), "graph_chunk" (steps per graph, default
+ * 32), "march_ichunk" (x planes per CTA, the tile depth, default 16) and
+ * "autotune" (K > 0: the next xfd_batch_run of at least 4 (1 + K) steps times
+ * K steps of each candidate tile depth 8, 16, 32, 64 inside the run and keeps
+ * the fastest; tiling does not change the results). */
+xfd_status xfd_batch_set_option(xfd_batch* b, const char* name, int64_t value);
+xfd_status xfd_batch_get_option(const xfd_batch* b, const char* name, int64_t* value);
+
+/* The last autotuning: candidate tile depths and their ms per batch step. */
+xfd_status xfd_batch_tuning(const xfd_batch* b, int32_t* depth, double* ms_per_step,
+                            int32_t capacity, int32_t* count);
+
+int32_t xfd_batch_size(const xfd_batch* b);
+/* Kernel launches per batch step (after the first xfd_batch_run). */
+int32_t xfd_batch_launches_per_step(const xfd_batch* b);
+/* The CUDA stream the batch launches on (a cudaStream_t). */
+void* xfd_batch_stream(xfd_batch* b);
 
 #ifdef __cplusplus
 }

@@ -51,3 +51,36 @@ def test_tfsf_tables_match_oracle(name):
     for a in range(3):
         assert np.array_equal(p_int[a], t["p_int"][a])
         assert np.array_equal(p_half[a], t["p_half"][a])
+
+
+def test_batched_workload_parameters():
+    """The batched workload's 96 scenes: sizes log-uniform in [64, 224]
+    (mean N^3 about 2.9 M cells), reproducible from the seed."""
+    from xfdtd_core_b200 import scene as S
+    p = S.batched_sphere_params()
+    assert len(p) == 96 and p == S.batched_sphere_params()
+    n = np.array([q["n"] for q in p])
+    assert n.min() >= 64 and n.max() <= 224
+    assert 2.5e6 < float((n.astype(float) ** 3).mean()) < 3.3e6
+    for q in p:
+        assert 0.1 * q["n"] <= q["radius_cells"] <= 0.3 * q["n"]
+        assert 2 <= q["eps_r"] <= 10 and 0 <= q["theta"] <= np.pi
+
+
+def test_random_angle_tfsf_tables_match_oracle():
+    """A batched-workload scene (random theta, phi, psi): the host's TFSF
+    tables equal the oracle's, as for the fixed-angle scenes."""
+    from xfdtd_core_b200 import scene as S
+    sc = S.batched_sphere(n=40, radius_cells=8.0, eps_r=5.0, theta=2.2, phi=4.1, psi=0.7,
+                          pml=6, tfsf_start=9, steps=200)
+    host = SceneRun(sc, engine=False)
+    orc = RefSimulation(sc)
+    t = orc.tfsf
+    size = [t["box_e"][a] - t["box_s"][a] for a in range(3)]
+    e_inc, h_inc, p_int, p_half = host.tfsf_tables(size)
+    scale = np.abs(t["e_inc"]).max()
+    assert np.abs(e_inc - t["e_inc"]).max() <= 1e-30 * scale
+    assert np.abs(h_inc - t["h_inc"]).max() <= 1e-30 * scale
+    for a in range(3):
+        assert np.array_equal(p_int[a], t["p_int"][a])
+        assert np.array_equal(p_half[a], t["p_half"][a])

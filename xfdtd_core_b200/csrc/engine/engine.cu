@@ -1627,6 +1627,7 @@ xfd_status xfd_sync(xfd_engine* e) {
   CUDA_TRY(e, cudaStreamSynchronize(e->copy_stream));
   int err = 0;
   CUDA_TRY(e, cudaMemcpy(&err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err & 2) return fail(e, XFD_ERR_TIMEOUT, "a sweep stage wait ran out of time");
   if (err) return fail(e, XFD_ERR_NUMERIC, "TFSF projection left the incident grid");
   return XFD_OK;
 }
@@ -1711,3 +1712,5 @@ int64_t xfd_stencil_bytes_per_step(const xfd_engine* e) {
 }
 
 }  // extern "C"
+
+#include "batch.cuh"

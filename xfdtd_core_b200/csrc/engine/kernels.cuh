@@ -204,10 +204,11 @@ __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeP<T
 }
 
 // The lattice faces k = nz (all i, j) and j = ny (all i, k < nz), which hold
-// only boundary nodes (their components are either fixed or receive CPML
-// terms only).  Sweeps that tile k < nz, j < ny leave these faces to the
-// two kernels below, one thread per node, with the arithmetic of
-// k_update_h / k_update_e.
+// only boundary nodes: every component there is either out of range or
+// outside its main update range, so it changes only by CPML terms.  Sweeps
+// that tile k < nz, j < ny leave these faces to the two kernels below, one
+// thread per node, with the arithmetic of k_update_h / k_update_e; a node in
+// no CPML layer returns at once.
 __host__ __device__ __forceinline__ long long edge_nodes(const Lat& L) {
   return (long long)(L.nx + 1) * (L.ny + 1) + (long long)(L.nx + 1) * L.nz;
 }
@@ -227,21 +228,44 @@ __device__ __forceinline__ void edge_node(const Lat& L, long long t, int& i, int
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_edge_h(const __grid_constant__ YeeP<T> p) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ bool in_some_layer(const YeeP<T>& p, int i, int j, int k, bool e) {
+  for (int s = 0; s < p.n_slab; ++s) {
+    const SlabD<T>& sl = p.slab[s];
+    const int l = sel3(sl.m, i, j, k) - (e ? sl.e_lo : sl.h_lo);
+    if (l >= 0 && l < sl.n) return true;
+  }
+  return false;
+}
+
+template <typename T, bool E>
+__device__ __forceinline__ void edge_update(const YeeP<T>& p, long long t) {
   if (t >= edge_nodes(p.L)) return;
   int i, j, k;
   edge_node(p.L, t, i, j, k);
-  update_h_node(p, i, j, k);
+  if (!in_some_layer(p, i, j, k, E)) return;
+  if (E)
+    update_e_node(p, i, j, k);
+  else
+    update_h_node(p, i, j, k);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_edge_h(const __grid_constant__ YeeP<T> p) {
+  edge_update<T, false>(p, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_edge_e(const __grid_constant__ YeeP<T> p) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= edge_nodes(p.L)) return;
-  int i, j, k;
-  edge_node(p.L, t, i, j, k);
-  update_e_node(p, i, j, k);
+  edge_update<T, true>(p, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Many lattices in one launch: block b covers the 256 face nodes starting at
+// blocks[b].y * 256 of lattice blocks[b].x.
+template <typename T, bool E>
+__global__ void __launch_bounds__(256)
+    k_edge_batch(const YeeP<T>* __restrict__ scenes, const int2* __restrict__ blocks) {
+  const int2 b = blocks[blockIdx.x];
+  edge_update<T, E>(scenes[b.x], (long long)b.y * 256 + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -307,9 +331,9 @@ __device__ __forceinline__ double tfsf_incident(const TfsfD& tf, bool inc_e, int
 }
 
 template <typename T>
-__global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const long long* step,
-                       int* err) {
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, const Lat& L,
+                                          T* const* fields, const long long* step, int* err,
+                                          long long tid) {
   if (tid >= g.total) return;
   int q = 0;
   while (q + 1 < g.n && tid >= g.pass[q + 1].begin) ++q;
@@ -340,6 +364,37 @@ __global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const lo
   T* F = fields[(P.is_e ? 0 : 3) + P.field];
   const long long id = lat_index(L, xf[0], xf[1], xf[2]);
   F[id] = (T)((double)F[id] + v * P.coeff);
+}
+
+template <typename T>
+__global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const long long* step,
+                       int* err) {
+  tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Per-lattice TFSF state for the batched launch: the incident tables, the
+// four pass groups (H 1, H 2, E 1, E 2) and where the lattice's fields, step
+// counter and error word live.
+template <typename T>
+struct TfsfSceneD {
+  TfsfD tf;
+  TfsfGroupD g[4];
+  Lat L;
+  T* const* fields;
+  const long long* step;
+  int* err;
+};
+
+// Pass group `group` of many lattices in one launch: block b covers the 256
+// face nodes starting at blocks[b].y * 256 of lattice blocks[b].x.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_tfsf_batch(const TfsfSceneD<T>* __restrict__ scenes, const int2* __restrict__ blocks,
+                 int group) {
+  const int2 b = blocks[blockIdx.x];
+  const TfsfSceneD<T>& S = scenes[b.x];
+  tfsf_node<T>(S.tf, S.g[group], S.L, S.fields, S.step, S.err,
+               (long long)b.y * 256 + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -609,5 +664,11 @@ __global__ void k_movie(MovieD mv, Lat L, T* const* fields, const long long* ste
 }
 
 __global__ void k_advance(long long* step) { *step += 1; }
+
+// Step counters of many lattices.
+__global__ void k_advance_batch(long long* const* steps, int n) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) *steps[s] += 1;
+}
 
 }  // namespace xfd

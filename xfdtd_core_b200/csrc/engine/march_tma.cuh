@@ -28,6 +28,9 @@
 // Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
 // the engine's error word, drains its loads in flight and returns, and later
 // launches that find the bit set return at once.
+// The batched kernels (k_march_*_tma_batch) run the same CTA body over a tile
+// list that spans many lattices, each with its parameters and tensor maps in
+// device memory.
 #pragma once
 
 #include "march.cuh"
@@ -137,13 +140,13 @@ struct StageRing {
 // is i_hi, E only, when i_hi <= nx); plane q lives in stage q % S.
 // ---------------------------------------------------------------------------
 template <typename T, int TJ, int TK, int S, bool CP, bool IN>
-__global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ MarchTmaP<T> P) {
+__device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx, const int gy,
+                                            const int gz) {
   using G = MarchGeom<T, TJ, TK>;
   extern __shared__ __align__(128) unsigned char smem[];
   const MarchP<T>& p = P.p;
   const Lat L = p.L;
   const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
-  const int gx = blockIdx.x + P.org[0], gy = blockIdx.y + P.org[1], gz = blockIdx.z + P.org[2];
   if (CP && gx >= P.box_lo[0] && gx < P.box_hi[0] && gy >= P.box_lo[1] && gy < P.box_hi[1] &&
       gz >= P.box_lo[2] && gz < P.box_hi[2])
     return;  // swept by the CPML-free form
@@ -339,13 +342,13 @@ __global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ 
 // when i_lo >= 1); plane q lives in stage (q+1) % S.
 // ---------------------------------------------------------------------------
 template <typename T, int TJ, int TK, int S, bool CP, bool IN>
-__global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ MarchTmaP<T> P) {
+__device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx, const int gy,
+                                            const int gz) {
   using G = MarchGeom<T, TJ, TK>;
   extern __shared__ __align__(128) unsigned char smem[];
   const MarchP<T>& p = P.p;
   const Lat L = p.L;
   const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
-  const int gx = blockIdx.x + P.org[0], gy = blockIdx.y + P.org[1], gz = blockIdx.z + P.org[2];
   if (CP && gx >= P.box_lo[0] && gx < P.box_hi[0] && gy >= P.box_lo[1] && gy < P.box_hi[1] &&
       gz >= P.box_lo[2] && gz < P.box_hi[2])
     return;  // swept by the CPML-free form
@@ -538,6 +541,52 @@ __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ 
     if (tid == 0) atomicOr(P.err, 2);
     ring.drain(S);
   }
+}
+
+// One lattice: CTA (x, y, z) sweeps tile (x, y) and chunk z, offset by org.
+template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+__global__ void __launch_bounds__(TJ* TK) k_march_h_tma(const __grid_constant__ MarchTmaP<T> P) {
+  march_h_cta<T, TJ, TK, S, CP, IN>(P, blockIdx.x + P.org[0], blockIdx.y + P.org[1],
+                                    blockIdx.z + P.org[2]);
+}
+
+template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+__global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ MarchTmaP<T> P) {
+  march_e_cta<T, TJ, TK, S, CP, IN>(P, blockIdx.x + P.org[0], blockIdx.y + P.org[1],
+                                    blockIdx.z + P.org[2]);
+}
+
+// Many lattices in one launch: CTA b sweeps the tile list entry
+// tiles[b] = (lattice, k tile, j tile, chunk) with the parameters
+// scenes[lattice] (device memory, tensor maps included).  The host builds
+// the list so that every entry is a tile of the form launched (CPML-free
+// interior, CPML-free, or CPML), largest lattices first.
+// The thread that issues the TMA loads first acquires the lattice's tensor
+// maps, which the host copied into device memory.
+__device__ __forceinline__ void acquire_march_maps(const MarchMaps& m) {
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    for (int c = 0; c < 6; ++c) {
+      tensormap_acquire(&m.halo[c]);
+      tensormap_acquire(&m.tile[c]);
+    }
+    tensormap_acquire(&m.cls);
+  }
+}
+
+template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+__global__ void __launch_bounds__(TJ* TK)
+    k_march_h_tma_batch(const MarchTmaP<T>* __restrict__ scenes, const int4* __restrict__ tiles) {
+  const int4 w = tiles[blockIdx.x];
+  acquire_march_maps(scenes[w.x].m);
+  march_h_cta<T, TJ, TK, S, CP, IN>(scenes[w.x], w.y, w.z, w.w);
+}
+
+template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+__global__ void __launch_bounds__(TJ* TK)
+    k_march_e_tma_batch(const MarchTmaP<T>* __restrict__ scenes, const int4* __restrict__ tiles) {
+  const int4 w = tiles[blockIdx.x];
+  acquire_march_maps(scenes[w.x].m);
+  march_e_cta<T, TJ, TK, S, CP, IN>(scenes[w.x], w.y, w.z, w.w);
 }
 
 }  // namespace xfd

@@ -48,6 +48,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
 }
 
 // 3-D tiled TMA load (x fastest) into shared memory, completing on `bar`.
+// Makes a tensor map that the host wrote into device memory (cudaMemcpy)
+// visible to the TMA unit of this thread; maps passed as __grid_constant__
+// kernel parameters need no fence.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(
+                   reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
                                             uint64_t* bar) {
   asm volatile(

@@ -18,7 +18,7 @@ from . import build as _build
 FP64, FP32 = 0, 1
 FIELD_NAMES = ("EX", "EY", "EZ", "HX", "HY", "HZ")
 _STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "UNSUPPORTED", 4: "STATE",
-           5: "OUT_OF_MEMORY", 6: "NUMERIC"}
+           5: "OUT_OF_MEMORY", 6: "NUMERIC", 7: "TIMEOUT"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _i32 = ctypes.c_int32
@@ -121,6 +121,18 @@ def load(build_if_missing: bool = True):
         "xfd_stream": ([vp], vp),
         "xfd_launches_per_step": ([vp], _i32),
         "xfd_stencil_bytes_per_step": ([vp], _i64),
+        "xfd_batch_create": ([ctypes.POINTER(vp), _i32, ctypes.POINTER(vp)], ctypes.c_int),
+        "xfd_batch_destroy": ([vp], None),
+        "xfd_batch_last_error": ([vp], ctypes.c_char_p),
+        "xfd_batch_run": ([vp, _i64], ctypes.c_int),
+        "xfd_batch_sync": ([vp], ctypes.c_int),
+        "xfd_batch_set_option": ([vp, ctypes.c_char_p, _i64], ctypes.c_int),
+        "xfd_batch_get_option": ([vp, ctypes.c_char_p, ctypes.POINTER(_i64)], ctypes.c_int),
+        "xfd_batch_tuning": ([vp, ctypes.POINTER(_i32), _dp, _i32, ctypes.POINTER(_i32)],
+                             ctypes.c_int),
+        "xfd_batch_size": ([vp], _i32),
+        "xfd_batch_launches_per_step": ([vp], _i32),
+        "xfd_batch_stream": ([vp], vp),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -138,7 +150,10 @@ def exported_symbols() -> List[str]:
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
-            "xfd_launches_per_step", "xfd_stencil_bytes_per_step"]
+            "xfd_launches_per_step", "xfd_stencil_bytes_per_step", "xfd_batch_create",
+            "xfd_batch_destroy", "xfd_batch_last_error", "xfd_batch_run", "xfd_batch_sync",
+            "xfd_batch_set_option", "xfd_batch_get_option", "xfd_batch_tuning",
+            "xfd_batch_size", "xfd_batch_launches_per_step", "xfd_batch_stream"]
 
 
 def _f64(a) -> np.ndarray:
@@ -360,3 +375,75 @@ def nf2ff_step_static(n, precision: int, fields, tasks, te_dev: int, th_dev: int
     st = L.xfd_nf2ff_step_static(ctypes.byref(d), ctypes.c_void_p(int(stream)))
     if st != 0:
         raise EngineError(f"xfd_nf2ff_step_static: {L.xfd_last_error(None).decode()} (status {st})")
+
+
+class Batch:
+    """Owning handle of one xfd_batch over borrowed engine handles.
+
+    ``engines`` are raw xfd_engine pointers (``Engine.h`` or
+    ``SceneRun.engine_handle()``); their owners must outlive the batch.
+    """
+
+    def __init__(self, engines: Sequence[int], options: Optional[Dict[str, int]] = None):
+        self.L = load()
+        arr = (ctypes.c_void_p * len(engines))(*[int(e) for e in engines])
+        h = ctypes.c_void_p()
+        st = self.L.xfd_batch_create(arr, len(engines), ctypes.byref(h))
+        if st != 0:
+            raise EngineError(f"xfd_batch_create: {_STATUS.get(st, st)}: "
+                              f"{self.L.xfd_batch_last_error(None).decode()}")
+        self.h = h
+        for name, value in (options or {}).items():
+            self.set_option(name, value)
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = self.L.xfd_batch_last_error(self.h).decode()
+            raise EngineError(f"{what}: {_STATUS.get(st, st)}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.xfd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, n: int):
+        self._check(self.L.xfd_batch_run(self.h, int(n)), "batch_run")
+
+    def sync(self):
+        self._check(self.L.xfd_batch_sync(self.h), "batch_sync")
+
+    def set_option(self, name: str, value: int):
+        self._check(self.L.xfd_batch_set_option(self.h, name.encode(), int(value)),
+                    "batch_set_option")
+
+    def get_option(self, name: str) -> int:
+        v = _i64()
+        self._check(self.L.xfd_batch_get_option(self.h, name.encode(), ctypes.byref(v)),
+                    "batch_get_option")
+        return int(v.value)
+
+    def tuning(self) -> List[tuple]:
+        """(tile depth, ms per batch step) of the last autotuning."""
+        cnt = _i32()
+        self._check(self.L.xfd_batch_tuning(self.h, None, None, 0, ctypes.byref(cnt)),
+                    "batch_tuning")
+        d = (_i32 * max(cnt.value, 1))()
+        ms = np.zeros(max(cnt.value, 1))
+        self._check(self.L.xfd_batch_tuning(self.h, d, _p(ms), cnt.value, ctypes.byref(cnt)),
+                    "batch_tuning")
+        return [(int(d[q]), float(ms[q])) for q in range(cnt.value)]
+
+    def size(self) -> int:
+        return int(self.L.xfd_batch_size(self.h))
+
+    def launches_per_step(self) -> int:
+        return int(self.L.xfd_batch_launches_per_step(self.h))
+
+    def stream(self) -> int:
+        return int(self.L.xfd_batch_stream(self.h) or 0)

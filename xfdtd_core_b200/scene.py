@@ -404,3 +404,50 @@ def dispersive_spheres(n: int = 384, pml: int = 10, dl: float = 5e-4, radius_cel
                                   cube((-half, -half, 0.0), (2 * half, 2 * half, dl)),
                                   movie_interval))
     return s
+
+
+def batched_sphere_params(count: int = 96, seed: int = 1, n_lo: int = 64, n_hi: int = 224):
+    """Per-scene parameters of the batched workload, drawn in this order per
+    scene with numpy.random.default_rng(seed): N = round(exp(U[ln n_lo,
+    ln n_hi])) cells per axis (CPML included), sphere radius U[0.1, 0.3] N
+    cells, eps_r U[2, 10], TFSF theta U[0, pi], phi U[0, 2 pi), psi U[0, 2 pi)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        radius = float(rng.uniform(0.1, 0.3)) * n
+        eps_r = float(rng.uniform(2.0, 10.0))
+        theta = float(rng.uniform(0.0, math.pi))
+        phi = float(rng.uniform(0.0, 2 * math.pi))
+        psi = float(rng.uniform(0.0, 2 * math.pi))
+        out.append(dict(n=n, radius_cells=radius, eps_r=eps_r, theta=theta, phi=phi, psi=psi))
+    return out
+
+
+def batched_sphere(n: int, radius_cells: float, eps_r: float, theta: float, phi: float,
+                   psi: float, pml: int = 8, dl: float = 1e-3, tfsf_start: int = 11,
+                   steps: int = 3000) -> Scene:
+    """One scene of the batched workload: n^3 cells including an 8-cell CPML
+    (default parameters), a centred dielectric sphere, a TFSF plane wave from
+    index `tfsf_start` at (theta, phi, psi) with a Gaussian of 20 cells per
+    wavelength (tau = 20 dl / 6e8, t0 = 4.5 tau, the reference examples'
+    convention), CFL 0.9."""
+    interior = n - 2 * pml
+    half = interior * dl / 2
+    s = Scene(dl=(dl, dl, dl), cfl=0.9, steps=steps, name=f"batched_sphere_{n}")
+    s.objects.append(ObjectSpec("domain", cube((-half,) * 3, (2 * half,) * 3), air()))
+    s.objects.append(ObjectSpec("sphere", sphere((0.0, 0.0, 0.0), radius_cells * dl),
+                                Material("simple", eps_r, 1.0, 0.0, 0.0)))
+    s.pmls = pml_all(pml)
+    tau = 20 * dl / 6e8
+    s.tfsf = TFSFSpec(tfsf_start, tfsf_start, tfsf_start, theta, phi, psi,
+                      Waveform("gaussian", tau, 4.5 * tau))
+    return s
+
+
+def batched_spheres(count: int = 96, seed: int = 1, steps: int = 3000, n_lo: int = 64,
+                    n_hi: int = 224, **kw) -> List[Scene]:
+    """The batched workload: `count` independent sphere scenes of uneven
+    sizes (batched_sphere_params), each lit by its own plane wave."""
+    return [batched_sphere(steps=steps, **p, **kw)
+            for p in batched_sphere_params(count, seed, n_lo, n_hi)]
