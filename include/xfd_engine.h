@@ -80,6 +80,20 @@ const char* xfd_last_error(const xfd_engine* e);
 xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t n_classes,
                                     const uint16_t* lattice_class);
 
+/* Per-node E coefficient overrides: the E update of component comp[q] at
+ * node (node[3q], node[3q+1], node[3q+2]) uses (ca[q], cb[q]) instead of its
+ * class's pair -- for nodes whose coefficients are all distinct (a block of
+ * per-voxel permittivities would otherwise need one class per node).  Only
+ * for nodes in the main update range outside CPML layers; call after
+ * xfd_set_material_classes, once.  The sweep applies the class pair (ca0,
+ * cb0) and a fix-up completes the node: E' = (cb/cb0) E_sweep +
+ * (ca - (cb/cb0) ca0) E_old.
+ * Replaces: the per-cell coefficients that an Object overriding
+ * correctMaterialSpace (include/xfdtd/object/object.h:47) writes into the
+ * full-grid coefficient arrays. */
+xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, const int32_t* comp,
+                               const double* ca, const double* cb);
+
 /* Per-axis curl factors.  fe[a] has n_a+1 entries, 1/(h_size * kappa_e);
  * fh[a] has n_a entries, 1/(e_size * kappa_h) (kappa = 1 outside CPML).
  * Replaces: the grid sizes folded into the coefficients
@@ -303,6 +317,64 @@ typedef struct {
 
 /* Queues the step on `stream` (a cudaStream_t; NULL = legacy default). */
 xfd_status xfd_nf2ff_step_static(const xfd_nf2ff_step_desc* d, void* stream);
+
+/* ---- Saved states ----------------------------------------------------------
+ * No counterpart in the reference (whose TimeParam has a start step but no
+ * saved field state).  A slot holds a device copy of what the next step
+ * reads: the six fields, the CPML auxiliaries, the ADE currents and the step
+ * counter.  Movie frames and NF2FF sums are outputs and are not rewound.
+ * Slots are engine-owned device memory (0 <= slot < 4096); saving over a
+ * slot reuses it.  Loading a slot saved under another configuration (CPML
+ * slabs, ADE) is rejected (XFD_ERR_STATE). */
+xfd_status xfd_checkpoint_save(xfd_engine* e, int32_t slot);
+xfd_status xfd_checkpoint_load(xfd_engine* e, int32_t slot);
+xfd_status xfd_checkpoint_drop(xfd_engine* e, int32_t slot);
+/* Step at which `slot` was saved, -1 if empty. */
+int64_t xfd_checkpoint_step(const xfd_engine* e, int32_t slot);
+
+/* ---- Adjoint gradient ------------------------------------------------------
+ * No counterpart in the reference (no gradient path): the discrete adjoint
+ * of the time step -- the exact transpose of the E/H updates with their CPML
+ * auxiliaries, run backward in time (TFSF faces and lumped sources are
+ * state-independent terms and have none).  Engines with ADE media, an NF2FF
+ * surface or movies are rejected (XFD_ERR_UNSUPPORTED).
+ *
+ * xfd_adjoint_run advances n_steps from the current state (N = n_steps),
+ * saving the state every checkpoint_interval (K) steps and recording E
+ * component obj_field over the node box [obj_s, obj_e) after every step.
+ * It then calls `objective` once with that record (row n = after n+1 steps,
+ * points in box order, k fastest), which returns J in *value and dJ/drecord
+ * in d_record (same shape); return nonzero to abort (XFD_ERR_NUMERIC).  The
+ * reverse pass recomputes each K-step segment from its saved state (memory
+ * holds ceil(N/K) + 1 states and K + 1 design-box rows) and returns in
+ * `sens` (2 x 3 x n_design doubles, n_design = nodes of [design_s,
+ * design_e), k fastest):
+ *   sens[0][c][p] = sum_{m=1..N} lam_c^m(p) E_c^{m-1}(p)
+ *   sens[1][c][p] = sum_{m=1..N} lam_c^m(p) E_c^m(p)
+ * with lam^m = dJ/dE^m, the total derivative of J with respect to the E field
+ * after m steps (through every later step).  At a node where the step is
+ * E^m = ca E^{m-1} + cb C^m (main range, outside CPML layers, TFSF faces and
+ * sources), C^m = (E^m - ca E^{m-1}) / cb, so for a parameter p of the
+ * node's (ca, cb):
+ *   dJ/dp = (ca' - ca cb'/cb) sens[0] + (cb'/cb) sens[1]     (' = d/dp).
+ * On return the engine holds the state after the N forward steps. */
+typedef int32_t (*xfd_objective_fn)(void* user, int64_t n_steps, int64_t n_points,
+                                    const double* record, double* d_record, double* value);
+
+typedef struct {
+  int64_t n_steps;
+  int32_t checkpoint_interval;
+  int32_t forward_only;               /* 1: record and evaluate J only (no states saved,
+                                         no reverse pass, sens unused) */
+  int32_t obj_field;                  /* 0..2: Ex, Ey, Ez */
+  int32_t obj_s[3], obj_e[3];         /* objective node box [s, e) */
+  int32_t design_s[3], design_e[3];   /* design node box [s, e) */
+  xfd_objective_fn objective;
+  void* user;
+} xfd_adjoint_desc;
+
+xfd_status xfd_adjoint_run(xfd_engine* e, const xfd_adjoint_desc* d, double* value,
+                           double* sens);
 
 /* ---- Batched simulations ---------------------------------------------------
  * No counterpart in the reference (which runs one Simulation per process):

@@ -295,6 +295,32 @@ class Object {
   std::shared_ptr<Material> _material;
 };
 
+/// A block of per-voxel relative permittivities: the Cube divided into
+/// dims[0] x dims[1] x dims[2] voxels (eps_r in C order, the last index
+/// fastest); a cell whose centre lies in the Cube is painted, as for any
+/// object, and takes the eps_r of the voxel holding its centre, with the
+/// common mu_r and sigma_e.  This is the reference's extension point for
+/// per-cell materials -- an Object subclass overriding correctMaterialSpace
+/// (include/xfdtd/object/object.h:47) -- as a class of this library: the E
+/// nodes whose averaging cells include a voxel get their own coefficients
+/// (xfd_set_e_overrides), so any number of distinct voxel values costs no
+/// material classes.  The voxels must stay clear of CPML layers, TFSF faces
+/// and lumped sources.
+class VoxelObject : public Object {
+ public:
+  VoxelObject(std::string name, std::unique_ptr<Cube> cube, std::array<Index, 3> dims,
+              std::vector<Real> eps_r, Real mu_r = 1, Real sigma_e = 0);
+  const std::array<Index, 3>& dims() const { return _dims; }
+  const std::vector<Real>& epsR() const { return _eps_r; }
+  Real muR() const { return _mu_r; }
+  Real sigmaE() const { return _sigma_e; }
+
+ private:
+  std::array<Index, 3> _dims;
+  std::vector<Real> _eps_r;
+  Real _mu_r, _sigma_e;
+};
+
 /// Lumped current source on a Cube of E nodes along its direction
 /// (src/object/lumped_element/current_source.cpp).  Resistance 0 becomes 1e-20;
 /// an infinite resistance leaves the E coefficients unchanged (beta = 0).
@@ -580,6 +606,20 @@ class Simulation {
     std::vector<Real> e_inc, h_inc, p_int[3], p_half[3];
   };
   TfsfTables tfsfTables() const;
+
+  /// Objective J = sum_p |F_p|^2 over the E_field nodes p of the node box
+  /// [box_s, box_e), F_p = dt sum_n E^n(p) exp(-i 2 pi freq t_n) over the
+  /// next n_steps steps (t_n = n dt, E^n the field after step n).  With
+  /// `grad`, also dJ/deps_r of every voxel of the VoxelObject `voxel_object`
+  /// (its index among the simulation's VoxelObjects), by the discrete
+  /// adjoint (xfd_adjoint_run) with the forward state saved every
+  /// `checkpoint_interval` steps; grad is resized to the voxel count (C
+  /// order).  Advances the simulation n_steps either way.
+  /// No counterpart in the reference (no gradient path).
+  Real dftPowerObjective(Index n_steps, int field, const std::array<int, 3>& box_s,
+                         const std::array<int, 3>& box_e, Real freq,
+                         std::vector<Real>* grad = nullptr, int voxel_object = 0,
+                         Index checkpoint_interval = 250);
 
   struct Impl;
 

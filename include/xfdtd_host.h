@@ -75,6 +75,17 @@ int xfdtd_scene_far_field(xfdtd_scene* s, int32_t n_theta, const double* theta, 
                           const char* sub_dir);
 /* Writes <dir>/fields/{EX..HZ}.npy, <dir>/<movie>/<step:05d>.npy and
  * <dir>/nf2ff.npy like the reference's Monitor::output (src/monitor/monitor.cpp:42-54). */
+/* J = sum_p |F_p|^2 over the E component `field` at the nodes of [box_s,
+ * box_e), F_p = dt sum_n E^n(p) exp(-i 2 pi freq n dt), over the next n_steps
+ * steps (the scene advances).  With `grad` (capacity >= voxel count), also
+ * dJ/deps_r of every voxel of the scene's VoxelObject number `voxel_object`
+ * (C order) by the discrete adjoint, saving the state every
+ * checkpoint_interval steps.  Returns 0 on success. */
+int xfdtd_scene_dft_objective(xfdtd_scene* s, int64_t n_steps, int32_t field,
+                              const int32_t box_s[3], const int32_t box_e[3], double freq,
+                              int32_t voxel_object, int32_t checkpoint_interval, double* value,
+                              double* grad, int64_t capacity);
+
 int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir);
 
 #ifdef __cplusplus

@@ -314,8 +314,10 @@ class RefSimulation:
         self.cell_material = np.zeros((nx, ny, nz), dtype=np.int32)
         mats = []
         painters = [(o.shape, o.material) for o in self.scene.objects]
+        voxels = [o if hasattr(o, "voxel_index") else None for o in self.scene.objects]
         from_air = __import__("xfdtd_core_b200.scene", fromlist=["air"]).air
         painters += [(c.shape, from_air()) for c in self.scene.current_sources]
+        voxels += [None] * len(self.scene.current_sources)
         # Simulation::correctMaterialSpace (src/simulation/simulation.cpp:608-636)
         # -> Object::defaultCorrectMaterialSpace (src/object/object.cpp:114-198)
         for index, (shape, mat) in enumerate(painters):
@@ -343,6 +345,18 @@ class RefSimulation:
             sub = inside(shape, X, Y, Z, self.eps)
             mask = np.zeros((nx, ny, nz), dtype=bool)
             mask[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = sub
+            if voxels[index] is not None:
+                # A per-voxel permittivity block (an Object overriding
+                # correctMaterialSpace, include/xfdtd/object/object.h:47):
+                # each painted cell takes the eps_r of the voxel holding its
+                # centre.
+                v = voxels[index]
+                qi = [v.voxel_index(a, self.h_node[a][lo[a]:hi[a]]) for a in range(3)]
+                QI, QJ, QK = np.meshgrid(*qi, indexing="ij")
+                e_val = np.zeros((nx, ny, nz))
+                e_val[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = (
+                    np.asarray(v.eps_r, dtype=np.float64)[QI, QJ, QK] * EPSILON_0)
+                e_val = e_val[mask]
             for c in range(3):
                 eps[c][:nx, :ny, :nz][mask] = e_val
                 sig_e[c][:nx, :ny, :nz][mask] = se

@@ -22,4 +22,21 @@ def dispersive_small(steps=120, **kw):
     return S.dispersive_spheres(**base)
 
 
-ALL = {"sphere": sphere_small, "boxes": boxes_small, "dispersive": dispersive_small}
+def voxels_small(steps=120, **kw):
+    """The adjoint scene's geometry at 40 x 40 x 32: slab, 8 x 8 x 3 design
+    voxels, normal-incidence TFSF, Ez patch objective."""
+    base = dict(nxy=40, nz=32, pml=6, dl=2e-4, slab_z=(12, 18), design=(8, 8, 3),
+                tfsf_start=8, patch=4, patch_z=22, steps=steps, freq=3e11)
+    base.update(kw)
+    return S.adjoint_slab(**base)[0]
+
+
+def voxels_objective(**kw):
+    base = dict(nxy=40, nz=32, pml=6, dl=2e-4, slab_z=(12, 18), design=(8, 8, 3),
+                tfsf_start=8, patch=4, patch_z=22, freq=3e11)
+    base.update(kw)
+    return S.adjoint_slab(**base)[1]
+
+
+ALL = {"sphere": sphere_small, "boxes": boxes_small, "dispersive": dispersive_small,
+       "voxels": voxels_small}

@@ -89,7 +89,7 @@ def test_dielectric_sphere_full_size_fp64():
 # twice the largest error any sweep showed (dispersive: ~1.0e-4, from the
 # ADE recursions accumulating FP32 rounding).
 @pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
-                                         ("dispersive", 2e-4)])
+                                         ("dispersive", 2e-4), ("voxels", 2e-4)])
 def test_scene_fp32_error_budget(name, budget, opts):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)

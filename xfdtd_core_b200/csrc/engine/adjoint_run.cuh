@@ -1,0 +1,389 @@
+// Saved states and the adjoint driver.  Part of engine.cu's translation
+// unit (it uses the engine internals defined there).
+//
+// A saved state (xfd_checkpoint_save / _load) is a device copy of what the
+// next step reads: the six field arrays of the current buffer, the CPML psi
+// arrays, the ADE currents and the step counter.  Movie frames and NF2FF
+// sums are outputs and are not rewound.
+//
+// xfd_adjoint_run: forward n steps from the current state, saving the state
+// every K steps and recording the objective component over its node box
+// each step; the caller's objective turns the record into J and dJ/drecord;
+// the reverse pass then walks the segments from the last to the first:
+// restore the segment's saved state, recompute its K steps while recording
+// E over the design box (K + 1 rows: memory stays bounded by the segment),
+// and run K reverse steps (k_adj_h, the sensitivity sums, k_adj_e, the
+// objective's adjoint source).  The forward state at the end of the run is
+// restored last, so the engine is left as a plain forward run would leave
+// it.  Cost: one forward run, one recomputation, one reverse run.
+
+namespace {
+
+struct StateRegion {
+  void* p;
+  size_t bytes;
+};
+
+size_t slab_cells(const xfd_engine* e, const xfd_engine::Slab& S) {
+  if (S.m == 0) return (size_t)S.n * e->L.NY * e->L.KP;
+  if (S.m == 1) return (size_t)(e->L.nx + 1) * S.n * e->L.KP;
+  return (size_t)(e->L.nx + 1) * e->L.NY * S.n;
+}
+
+std::vector<StateRegion> state_regions(xfd_engine* e) {
+  std::vector<StateRegion> r;
+  for (int c = 0; c < 6; ++c) r.push_back({e->fbuf[e->cur][c], (size_t)e->n_lat * e->wsize});
+  for (const auto& S : e->slabs) {
+    const size_t b = slab_cells(e, S) * e->wsize;
+    for (int w = 0; w < 2; ++w) {
+      r.push_back({S.psi_e[w], b});
+      r.push_back({S.psi_h[e->cur][w], b});
+    }
+  }
+  if (e->ade_kind >= 0) {
+    const bool d = e->precision == XFD_FP64;
+    const long long n = d ? e->ade64.n : e->ade32.n;
+    const int np = d ? e->ade64.np : e->ade32.np;
+    void* j = d ? (void*)e->ade64.j : (void*)e->ade32.j;
+    void* jp = d ? (void*)e->ade64.jp : (void*)e->ade32.jp;
+    void* ep = d ? (void*)e->ade64.ep : (void*)e->ade32.ep;
+    r.push_back({j, (size_t)n * np * e->wsize});
+    if (jp) r.push_back({jp, (size_t)n * np * e->wsize});
+    if (ep) r.push_back({ep, (size_t)n * e->wsize});
+  }
+  r.push_back({e->d_step, sizeof(long long)});
+  return r;
+}
+
+size_t state_bytes(xfd_engine* e) {
+  size_t b = 0;
+  for (const auto& r : state_regions(e)) b += (r.bytes + 255) / 256 * 256;
+  return b;
+}
+
+xfd_status state_copy(xfd_engine* e, xfd_engine::Ckpt& c, bool save) {
+  size_t off = 0;
+  for (const auto& r : state_regions(e)) {
+    char* slot = static_cast<char*>(c.buf) + off;
+    CUDA_TRY(e, cudaMemcpyAsync(save ? (void*)slot : r.p, save ? r.p : (const void*)slot, r.bytes,
+                                cudaMemcpyDeviceToDevice, e->stream));
+    off += (r.bytes + 255) / 256 * 256;
+  }
+  if (save) c.step = e->host_step;
+  else e->host_step = c.step;
+  return XFD_OK;
+}
+
+xfd_status ckpt_save(xfd_engine* e, xfd_engine::Ckpt& c) {
+  const size_t need = state_bytes(e);
+  if (c.buf && c.bytes != need) {
+    CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    cudaFree(c.buf);
+    c.buf = nullptr;
+  }
+  if (!c.buf) {
+    cudaError_t r = cudaMalloc(&c.buf, need);
+    if (r != cudaSuccess) {
+      c.buf = nullptr;
+      return fail(e, r == cudaErrorMemoryAllocation ? XFD_ERR_OUT_OF_MEMORY : XFD_ERR_CUDA,
+                  "checkpoint cudaMalloc(%zu): %s", need, cudaGetErrorString(r));
+    }
+    c.bytes = need;
+  }
+  return state_copy(e, c, true);
+}
+
+void ckpt_free(xfd_engine::Ckpt& c) {
+  if (c.buf) cudaFree(c.buf);
+  c = xfd_engine::Ckpt{};
+}
+
+// Device buffers of one adjoint run, freed on every exit path.
+struct AdjBuffers {
+  std::vector<void*> p;
+  std::vector<xfd_engine::Ckpt> ck;
+  ~AdjBuffers() {
+    for (void* q : p) cudaFree(q);
+    for (auto& c : ck) ckpt_free(c);
+  }
+};
+
+xfd_status adj_alloc(xfd_engine* e, AdjBuffers& B, void** out, size_t bytes) {
+  cudaError_t r = cudaMalloc(out, std::max<size_t>(bytes, 16));
+  if (r != cudaSuccess) {
+    *out = nullptr;
+    return fail(e, r == cudaErrorMemoryAllocation ? XFD_ERR_OUT_OF_MEMORY : XFD_ERR_CUDA,
+                "adjoint cudaMalloc(%zu): %s", bytes, cudaGetErrorString(r));
+  }
+  B.p.push_back(*out);
+  CUDA_TRY(e, cudaMemsetAsync(*out, 0, std::max<size_t>(bytes, 16), e->stream));
+  return XFD_OK;
+}
+
+bool box_ok(const Lat& L, const int32_t s[3], const int32_t t[3]) {
+  const int n[3] = {L.nx, L.ny, L.nz};
+  for (int a = 0; a < 3; ++a)
+    if (s[a] < 0 || t[a] <= s[a] || t[a] > n[a] + 1) return false;
+  return true;
+}
+
+long long box_nodes(const int32_t s[3], const int32_t t[3]) {
+  return (long long)(t[0] - s[0]) * (t[1] - s[1]) * (t[2] - s[2]);
+}
+
+template <typename T>
+void set_rec(xfd_engine* e, int r, const BoxRecD<T>& d) {
+  if constexpr (sizeof(T) == 8) e->rec64[r] = d; else e->rec32[r] = d;
+}
+
+template <typename T>
+xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value, double* sens) {
+  const Lat L = e->L;
+  const long long N = d->n_steps, K = d->forward_only ? N : d->checkpoint_interval;
+  const long long S = (N + K - 1) / K;
+  const long long t0 = e->host_step;
+  const long long n_obj = box_nodes(d->obj_s, d->obj_e);
+  const long long n_des = box_nodes(d->design_s, d->design_e);
+  cudaStream_t st = e->stream;
+  AdjBuffers B;
+  xfd_status s;
+  void *rec = nullptr, *hist = nullptr, *src = nullptr, *g = nullptr, *lamp = nullptr;
+  if ((s = adj_alloc(e, B, &rec, (size_t)N * n_obj * sizeof(T))) != XFD_OK) return s;
+  if (d->forward_only) {
+    BoxRecD<T> ro{};
+    for (int q = 0; q < 3; ++q) {
+      ro.s[q] = d->obj_s[q];
+      ro.e[q] = d->obj_e[q];
+    }
+    ro.c0 = d->obj_field;
+    ro.nc = 1;
+    ro.n = n_obj;
+    ro.base = t0;
+    ro.rows = N;
+    ro.dst = static_cast<T*>(rec);
+    set_rec<T>(e, 0, ro);
+    e->n_rec = 1;
+    e->graph_dirty = true;
+    s = xfd_run(e, N);
+    e->n_rec = 0;
+    e->graph_dirty = true;
+    if (s != XFD_OK) return s;
+    std::vector<T> rec_h((size_t)(N * n_obj));
+    CUDA_TRY(e, cudaMemcpyAsync(rec_h.data(), rec, rec_h.size() * sizeof(T),
+                                cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(e, cudaStreamSynchronize(st));
+    std::vector<double> rec_d(rec_h.begin(), rec_h.end()), drec(rec_h.size(), 0.0);
+    double J = 0.0;
+    if (d->objective(d->user, N, n_obj, rec_d.data(), drec.data(), &J) != 0)
+      return fail(e, XFD_ERR_NUMERIC, "objective callback failed");
+    if (value) *value = J;
+    return XFD_OK;
+  }
+  if ((s = adj_alloc(e, B, &hist, (size_t)(K + 1) * 3 * n_des * sizeof(T))) != XFD_OK) return s;
+  if ((s = adj_alloc(e, B, &src, (size_t)N * n_obj * sizeof(double))) != XFD_OK) return s;
+  if ((s = adj_alloc(e, B, &g, (size_t)6 * n_des * sizeof(double))) != XFD_OK) return s;
+  if ((s = adj_alloc(e, B, &lamp, 6 * sizeof(void*))) != XFD_OK) return s;
+  void* lam[6];
+  for (int c = 0; c < 6; ++c)
+    if ((s = adj_alloc(e, B, &lam[c], (size_t)e->n_lat * e->wsize)) != XFD_OK) return s;
+  CUDA_TRY(e, cudaMemcpyAsync(lamp, lam, sizeof lam, cudaMemcpyHostToDevice, st));
+  YeeP<T> a = yee_params<T>(e);
+  for (int c = 0; c < 6; ++c) a.f[c] = static_cast<T*>(lam[c]);
+  for (size_t q = 0; q < e->slabs.size(); ++q) {
+    const size_t b = slab_cells(e, e->slabs[q]) * e->wsize;
+    for (int w = 0; w < 2; ++w) {
+      void *pe = nullptr, *ph = nullptr;
+      if ((s = adj_alloc(e, B, &pe, b)) != XFD_OK) return s;
+      if ((s = adj_alloc(e, B, &ph, b)) != XFD_OK) return s;
+      a.slab[q].psi_e[w] = static_cast<T*>(pe);
+      a.slab[q].psi_h[w] = static_cast<T*>(ph);
+    }
+  }
+  T* const* lam_dev = static_cast<T* const*>(lamp);
+  B.ck.resize((size_t)S + 1);
+  // Coefficient overrides as dense arrays over their bounding node box.
+  OvBoxD<T> ov{};
+  if (e->n_ovr) {
+    for (int q = 0; q < 3; ++q) {
+      ov.s[q] = INT32_MAX;
+      ov.e[q] = INT32_MIN;
+    }
+    for (long long q = 0; q < e->n_ovr; ++q)
+      for (int a2 = 0; a2 < 3; ++a2) {
+        ov.s[a2] = std::min(ov.s[a2], e->ovr_node[(size_t)(3 * q + a2)]);
+        ov.e[a2] = std::max(ov.e[a2], e->ovr_node[(size_t)(3 * q + a2)] + 1);
+      }
+    ov.n = (long long)(ov.e[0] - ov.s[0]) * (ov.e[1] - ov.s[1]) * (ov.e[2] - ov.s[2]);
+    std::vector<T> hca((size_t)(3 * ov.n), T(0)), hcb((size_t)(3 * ov.n), T(0));
+    for (long long q = 0; q < e->n_ovr; ++q) {
+      const int32_t* x = &e->ovr_node[(size_t)(3 * q)];
+      const long long p = ((long long)(x[0] - ov.s[0]) * (ov.e[1] - ov.s[1]) + (x[1] - ov.s[1])) *
+                              (ov.e[2] - ov.s[2]) +
+                          (x[2] - ov.s[2]);
+      hca[(size_t)(e->ovr_comp[(size_t)q] * ov.n + p)] = (T)e->ovr_ca[(size_t)q];
+      hcb[(size_t)(e->ovr_comp[(size_t)q] * ov.n + p)] = (T)e->ovr_cb[(size_t)q];
+    }
+    void *dca = nullptr, *dcb = nullptr;
+    if ((s = adj_alloc(e, B, &dca, hca.size() * sizeof(T))) != XFD_OK) return s;
+    if ((s = adj_alloc(e, B, &dcb, hcb.size() * sizeof(T))) != XFD_OK) return s;
+    CUDA_TRY(e, cudaMemcpyAsync(dca, hca.data(), hca.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                st));
+    CUDA_TRY(e, cudaMemcpyAsync(dcb, hcb.data(), hcb.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                st));
+    CUDA_TRY(e, cudaStreamSynchronize(st));
+    ov.ca = static_cast<const T*>(dca);
+    ov.cb = static_cast<const T*>(dcb);
+  }
+
+  // Forward: state saved at the start of every segment, objective recorded.
+  BoxRecD<T> ro{};
+  for (int q = 0; q < 3; ++q) {
+    ro.s[q] = d->obj_s[q];
+    ro.e[q] = d->obj_e[q];
+  }
+  ro.c0 = d->obj_field;
+  ro.nc = 1;
+  ro.n = n_obj;
+  ro.base = t0;
+  ro.shift = 0;
+  ro.rows = N;
+  ro.dst = static_cast<T*>(rec);
+  set_rec<T>(e, 0, ro);
+  e->n_rec = 1;
+  e->graph_dirty = true;
+  for (long long q = 0; q < S; ++q) {
+    if ((s = ckpt_save(e, B.ck[(size_t)q])) != XFD_OK) break;
+    if ((s = xfd_run(e, std::min(K, N - q * K))) != XFD_OK) break;
+  }
+  e->n_rec = 0;
+  e->graph_dirty = true;
+  if (s != XFD_OK) return s;
+  if ((s = ckpt_save(e, B.ck[(size_t)S])) != XFD_OK) return s;
+
+  // Objective on the host.
+  std::vector<T> rec_h((size_t)(N * n_obj));
+  CUDA_TRY(e, cudaMemcpyAsync(rec_h.data(), rec, rec_h.size() * sizeof(T),
+                              cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(e, cudaStreamSynchronize(st));
+  std::vector<double> rec_d(rec_h.begin(), rec_h.end()), drec(rec_h.size(), 0.0);
+  double J = 0.0;
+  if (d->objective(d->user, N, n_obj, rec_d.data(), drec.data(), &J) != 0)
+    return fail(e, XFD_ERR_NUMERIC, "objective callback failed");
+  if (value) *value = J;
+  CUDA_TRY(e, cudaMemcpyAsync(src, drec.data(), drec.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, st));
+
+  // Reverse.
+  BoxRecD<T> rd{};
+  for (int q = 0; q < 3; ++q) {
+    rd.s[q] = d->design_s[q];
+    rd.e[q] = d->design_e[q];
+  }
+  rd.c0 = 0;
+  rd.nc = 3;
+  rd.n = n_des;
+  rd.rows = K + 1;
+  rd.dst = static_cast<T*>(hist);
+  BoxRecD<T> rs = ro;
+  const double* srcd = static_cast<const double*>(src);
+  double* g0 = static_cast<double*>(g);
+  double* g1 = g0 + 3 * n_des;
+  const dim3 blk(32, 8, 1);
+  const dim3 grd((unsigned)((L.nz + 1 + 31) / 32), (unsigned)((L.ny + 1 + 7) / 8),
+                 (unsigned)(L.nx + 1));
+  const unsigned sb = blocks_for(n_obj, 256), db = blocks_for(3 * n_des, 256);
+  T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
+  k_adj_source<T><<<sb, 256, 0, st>>>(rs, L, lam_dev, srcd + (N - 1) * n_obj);  // dJ/dE^N
+  for (long long q = S - 1; q >= 0; --q) {
+    const long long base = t0 + q * K, len = std::min(K, N - q * K);
+    if ((s = state_copy(e, B.ck[(size_t)q], false)) != XFD_OK) return s;
+    rd.base = base;
+    rd.shift = 0;
+    k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
+    rd.shift = 1;
+    set_rec<T>(e, 0, rd);
+    e->n_rec = 1;
+    e->graph_dirty = true;
+    s = xfd_run(e, len);
+    e->n_rec = 0;
+    e->graph_dirty = true;
+    if (s != XFD_OK) return s;
+    for (long long m = len; m >= 1; --m) {
+      const long long gstep = q * K + m;  // lam holds dJ/dE^gstep
+      k_adj_h<T><<<grd, blk, 0, st>>>(a, ov);
+      k_adj_sens<T><<<db, 256, 0, st>>>(rd, L, lam_dev, static_cast<const T*>(hist), (int)m, g0,
+                                        g1);
+      k_adj_e<T><<<grd, blk, 0, st>>>(a, ov);
+      if (gstep - 1 >= 1)
+        k_adj_source<T><<<sb, 256, 0, st>>>(rs, L, lam_dev, srcd + (gstep - 2) * n_obj);
+    }
+    CUDA_TRY(e, cudaGetLastError());
+  }
+  if ((s = state_copy(e, B.ck[(size_t)S], false)) != XFD_OK) return s;
+  CUDA_TRY(e, cudaMemcpyAsync(sens, g, (size_t)6 * n_des * sizeof(double), cudaMemcpyDeviceToHost,
+                              st));
+  CUDA_TRY(e, cudaStreamSynchronize(st));
+  int err = 0;
+  CUDA_TRY(e, cudaMemcpy(&err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err & 2) return fail(e, XFD_ERR_TIMEOUT, "a sweep stage wait ran out of time");
+  if (err) return fail(e, XFD_ERR_NUMERIC, "TFSF projection left the incident grid");
+  return XFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+xfd_status xfd_checkpoint_save(xfd_engine* e, int32_t slot) {
+  if (!e || slot < 0 || slot > 4095) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad slot");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  if (e->ckpts.size() <= (size_t)slot) e->ckpts.resize((size_t)slot + 1);
+  return ckpt_save(e, e->ckpts[(size_t)slot]);
+}
+
+xfd_status xfd_checkpoint_load(xfd_engine* e, int32_t slot) {
+  if (!e || slot < 0 || (size_t)slot >= e->ckpts.size() || !e->ckpts[(size_t)slot].buf)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "no saved state in slot %d", slot);
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  if (e->ckpts[(size_t)slot].bytes != state_bytes(e))
+    return fail(e, XFD_ERR_STATE, "slot %d was saved with another configuration", slot);
+  return state_copy(e, e->ckpts[(size_t)slot], false);
+}
+
+xfd_status xfd_checkpoint_drop(xfd_engine* e, int32_t slot) {
+  if (!e || slot < 0) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad slot");
+  if ((size_t)slot >= e->ckpts.size()) return XFD_OK;
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  ckpt_free(e->ckpts[(size_t)slot]);
+  return XFD_OK;
+}
+
+int64_t xfd_checkpoint_step(const xfd_engine* e, int32_t slot) {
+  if (!e || slot < 0 || (size_t)slot >= e->ckpts.size()) return -1;
+  return e->ckpts[(size_t)slot].step;
+}
+
+xfd_status xfd_adjoint_run(xfd_engine* e, const xfd_adjoint_desc* d, double* value,
+                           double* sens) {
+  if (!e || !d || (!sens && !d->forward_only) || !d->objective)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "null adjoint argument");
+  if (d->n_steps < 1 || (d->checkpoint_interval < 1 && !d->forward_only))
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "adjoint needs n_steps >= 1 and an interval >= 1");
+  if (e->host_step + d->n_steps > e->n_steps)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "run past n_steps (%lld + %lld > %lld)",
+                (long long)e->host_step, (long long)d->n_steps, (long long)e->n_steps);
+  if (d->obj_field < 0 || d->obj_field > 2 || !box_ok(e->L, d->obj_s, d->obj_e) ||
+      (!d->forward_only && !box_ok(e->L, d->design_s, d->design_e)))
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad objective field or node box");
+  if (e->ade_kind >= 0 || e->have_nf2ff || !e->movies.empty())
+    return fail(e, XFD_ERR_UNSUPPORTED,
+                "the adjoint covers CPML, TFSF and lumped sources; not ADE media, NF2FF or movies");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s = ensure_ready(e);
+  if (s != XFD_OK) return s;
+  return e->precision == XFD_FP64 ? adjoint_run_t<double>(e, d, value, sens)
+                                  : adjoint_run_t<float>(e, d, value, sens);
+}
+
+}  // extern "C"

@@ -21,8 +21,8 @@
 // batched lattice follows the same step sequence as the same engine run
 // alone: H sweep, H lattice faces, TFSF H groups 1 and 2, E sweep, E lattice
 // faces, TFSF E groups 1 and 2, step counter.  Engines with ADE media,
-// lumped sources, movies or an NF2FF surface are not batched (their
-// per-step extras stay with xfd_run).
+// lumped sources, movies, an NF2FF surface or coefficient overrides are not
+// batched (their per-step extras stay with xfd_run).
 //
 // The x chunk length (planes per CTA) is the tile depth the autotuner
 // chooses: with the `autotune` option set to K, the next xfd_batch_run
@@ -381,9 +381,11 @@ xfd_status xfd_batch_create(xfd_engine* const* engines, int32_t n, xfd_batch** o
     if (e->device != engines[0]->device || e->precision != engines[0]->precision)
       return bfail(nullptr, XFD_ERR_INVALID_ARGUMENT,
                    "engine %d: all batched engines need one device and one precision", s);
-    if (e->ade_kind >= 0 || !e->lumped_h.empty() || !e->movies.empty() || e->have_nf2ff)
+    if (e->ade_kind >= 0 || !e->lumped_h.empty() || !e->movies.empty() || e->have_nf2ff ||
+        e->n_ovr)
       return bfail(nullptr, XFD_ERR_UNSUPPORTED,
-                   "engine %d: ADE media, lumped sources, movies and NF2FF are not batched", s);
+                   "engine %d: ADE media, lumped sources, movies, NF2FF and coefficient "
+                   "overrides are not batched", s);
     if (is_fused(e) && e->cur != 0)
       return bfail(nullptr, XFD_ERR_STATE,
                    "engine %d: fields are in the second buffer of a fused sweep", s);

@@ -25,6 +25,7 @@
 #include "fvec.cuh"
 #include "farfield.cuh"
 #include "kernels.cuh"
+#include "adjoint.cuh"
 #include "xfd_engine.h"
 
 using namespace xfd;
@@ -88,6 +89,14 @@ struct xfd_engine {
   LumpedD lumped{};
   bool lumped_dirty = false;
 
+  // per-node E coefficient overrides (device list + host copy for the adjoint)
+  long long n_ovr = 0;
+  OverrideD<double> ovr64{};
+  OverrideD<float> ovr32{};
+  std::vector<int32_t> ovr_node;  // 3 per entry
+  std::vector<uint8_t> ovr_comp;
+  std::vector<double> ovr_ca, ovr_cb;
+
   int ade_kind = -1;
   AdeD<double> ade64{};
   AdeD<float> ade32{};
@@ -128,6 +137,19 @@ struct xfd_engine {
   int graph_cur = -1;
   long long graph_len = 0;
   bool graph_dirty = true;
+
+  // Saved states (xfd_checkpoint_*): one device buffer per slot.
+  struct Ckpt {
+    void* buf = nullptr;
+    size_t bytes = 0;
+    int64_t step = -1;
+  };
+  std::vector<Ckpt> ckpts;
+  // Per-step node-box records of the adjoint (objective field, design
+  // history), launched after the record phase of each step.
+  BoxRecD<double> rec64[2]{};
+  BoxRecD<float> rec32[2]{};
+  int n_rec = 0;
 };
 
 namespace {
@@ -550,6 +572,11 @@ MarchP<T> march_params(xfd_engine* e) {
 
 long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b); }
 
+template <typename T>
+OverrideD<T> ovr_of(const xfd_engine* e) {
+  if constexpr (sizeof(T) == 8) return e->ovr64; else return e->ovr32;
+}
+
 // Launches one time step (host step index t decides the periodic kernels).
 template <typename T>
 cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
@@ -701,6 +728,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
     // E phase: ADE e_cur gather -> updateE + CPML.
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
+    if (e->n_ovr) k_ovr_gather<T><<<blocks_for(e->n_ovr, 256), 256, 0, s>>>(ovr_of<T>(e), fields);
     if (march_tma) {
       launch_march(k_march_e_tma<T, kMTJ, 32, MF, false, false>,
                    k_march_e_tma<T, kMTJ, 32, MF, false, true>,
@@ -712,6 +740,10 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     else
       k_update_e<T><<<grd, blk, 0, s>>>(yp);
   }
+  // Coefficient overrides complete the E update of their nodes.
+  if (e->n_ovr)
+    k_ovr_apply<T><<<blocks_for(e->n_ovr, 256), 256, 0, s>>>(ovr_of<T>(e), fields,
+                                                             fused ? fields_in : nullptr);
   // ADE -> lumped -> TFSF E faces (the reference's updateE then correctE order).
   T* const* ecur = fused ? fields_in : nullptr;
   if (e->ade_kind == 0) k_ade_update<T, 0><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
@@ -731,6 +763,11 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   for (auto& mv : e->movies) {
     if (t % mv.d.interval == 0)
       k_movie<T><<<blocks_for(mv.n_nodes, 256), 256, 0, s>>>(mv.d, e->L, fields, e->d_step);
+  }
+  for (int r = 0; r < e->n_rec; ++r) {
+    BoxRecD<T> rd;
+    if constexpr (sizeof(T) == 8) rd = e->rec64[r]; else rd = e->rec32[r];
+    k_box_record<T><<<blocks_for(rd.n * rd.nc, 256), 256, 0, s>>>(rd, e->L, fields, e->d_step);
   }
   if (e->have_nf2ff) {
     k_nf2ff_sample<T><<<blocks_for(e->nf2ff.P, 256), 256, 0, s>>>(e->nf2ff, e->L, fields,
@@ -1000,6 +1037,8 @@ void xfd_destroy(xfd_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
   drop_graph(e);
+  for (auto& c : e->ckpts)
+    if (c.buf) cudaFree(c.buf);
   for (void* p : e->allocs) cudaFree(p);
   for (void* p : e->host_allocs) cudaFreeHost(p);
   if (e->copy_ev) cudaEventDestroy(e->copy_ev);
@@ -1062,6 +1101,63 @@ xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t 
   e->n_classes = n_classes;
   e->have_classes = true;
   e->tma_ready = false;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, const int32_t* comp,
+                               const double* ca, const double* cb) {
+  if (!e || n < 0 || (n > 0 && (!node || !comp || !ca || !cb)))
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad override arguments");
+  if (!e->have_classes) return fail(e, XFD_ERR_STATE, "set the material classes first");
+  if (e->n_ovr) return fail(e, XFD_ERR_STATE, "overrides already set");
+  if (n == 0) return XFD_OK;
+  const int nn[3] = {e->L.nx, e->L.ny, e->L.nz};
+  std::vector<long long> id((size_t)n);
+  std::vector<uint8_t> cm((size_t)n);
+  for (int64_t q = 0; q < n; ++q) {
+    const int c = comp[q];
+    const int* x = node + 3 * q;
+    bool ok = c >= 0 && c <= 2 && cb[q] > 0;
+    for (int d = 0; d < 3 && ok; ++d)
+      ok = x[d] >= 0 && (d == c ? x[d] < nn[d] : x[d] <= nn[d]);
+    if (!ok) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad override entry %lld", (long long)q);
+    id[(size_t)q] = lat_index(e->L, x[0], x[1], x[2]);
+    cm[(size_t)q] = (uint8_t)c;
+  }
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s;
+  long long* dn = nullptr;
+  uint8_t* dc = nullptr;
+  double *dca = nullptr, *dcb = nullptr;
+  if ((s = upload_raw(e, &dn, id.data(), id.size())) != XFD_OK) return s;
+  if ((s = upload_raw(e, &dc, cm.data(), cm.size())) != XFD_OK) return s;
+  if ((s = upload_raw(e, &dca, ca, (size_t)n)) != XFD_OK) return s;
+  if ((s = upload_raw(e, &dcb, cb, (size_t)n)) != XFD_OK) return s;
+  void *r = nullptr, *d = nullptr, *old = nullptr;
+  if ((s = dev_alloc(e, &r, (size_t)n * e->wsize)) != XFD_OK) return s;
+  if ((s = dev_alloc(e, &d, (size_t)n * e->wsize)) != XFD_OK) return s;
+  if ((s = dev_alloc(e, &old, (size_t)n * e->wsize)) != XFD_OK) return s;
+  if (e->precision == XFD_FP64) {
+    OverrideD<double> o{n, dn, dc, static_cast<double*>(r), static_cast<double*>(d),
+                        static_cast<double*>(old)};
+    k_ovr_prepare<double><<<blocks_for(n, 256), 256, 0, e->stream>>>(
+        o, e->cls, static_cast<const double*>(e->tab), dca, dcb);
+    e->ovr64 = o;
+  } else {
+    OverrideD<float> o{n, dn, dc, static_cast<float*>(r), static_cast<float*>(d),
+                       static_cast<float*>(old)};
+    k_ovr_prepare<float><<<blocks_for(n, 256), 256, 0, e->stream>>>(
+        o, e->cls, static_cast<const float*>(e->tab), dca, dcb);
+    e->ovr32 = o;
+  }
+  CUDA_TRY(e, cudaGetLastError());
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  e->ovr_node.assign(node, node + 3 * n);
+  e->ovr_comp = cm;
+  e->ovr_ca.assign(ca, ca + n);
+  e->ovr_cb.assign(cb, cb + n);
+  e->n_ovr = n;
   e->graph_dirty = true;
   return XFD_OK;
 }
@@ -1694,7 +1790,8 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (e->ade_kind >= 0) n += fused ? 1 : 2;
   if (!e->lumped_h.empty()) n += 1;
   if (e->have_nf2ff) n += 1;
-  return n;
+  if (e->n_ovr) n += fused ? 1 : 2;
+  return n + e->n_rec;
 }
 
 int64_t xfd_stencil_bytes_per_step(const xfd_engine* e) {
@@ -1714,3 +1811,4 @@ int64_t xfd_stencil_bytes_per_step(const xfd_engine* e) {
 }  // extern "C"
 
 #include "batch.cuh"
+#include "adjoint_run.cuh"

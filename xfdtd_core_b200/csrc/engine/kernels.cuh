@@ -663,6 +663,55 @@ __global__ void k_movie(MovieD mv, Lat L, T* const* fields, const long long* ste
   *out = fields[mv.field][lat_index(L, i, j, k)];
 }
 
+// ---------------------------------------------------------------------------
+// Per-node E coefficient overrides: nodes whose E update uses its own
+// (ca, cb) instead of its material class's pair (ca0, cb0) -- for example
+// the nodes around a block of per-voxel permittivities, each of which would
+// otherwise need a class of its own.  The sweep applies the class pair; the
+// override then rescales: E' = r E_sweep + d E_old with r = cb / cb0 and
+// d = ca - r ca0, which is ca E_old + cb (curl H) for a node in the main
+// range outside CPML layers (the only nodes the host overrides).  E_old is
+// saved before a split sweep (k_ovr_gather) or read from the input buffer of
+// a ping-pong sweep.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct OverrideD {
+  long long n;
+  const long long* node;  // lattice index
+  const uint8_t* comp;    // 0..2
+  T* r;
+  T* d;
+  T* eold;
+};
+
+template <typename T>
+__global__ void k_ovr_prepare(OverrideD<T> o, const uint16_t* cls, const T* tab, const double* ca,
+                              const double* cb) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= o.n) return;
+  const T* row = tab + (size_t)cls[o.node[q]] * 12 + 2 * o.comp[q];
+  const double r = cb[q] / (double)row[1];
+  o.r[q] = (T)r;
+  o.d[q] = (T)(ca[q] - r * (double)row[0]);
+}
+
+template <typename T>
+__global__ void k_ovr_gather(OverrideD<T> o, T* const* fields) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= o.n) return;
+  o.eold[q] = fields[o.comp[q]][o.node[q]];
+}
+
+template <typename T>
+__global__ void k_ovr_apply(OverrideD<T> o, T* const* fields, T* const* fields_in) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= o.n) return;
+  T* E = fields[o.comp[q]];
+  const long long id = o.node[q];
+  const T old = fields_in ? fields_in[o.comp[q]][id] : o.eold[q];
+  E[id] = o.r[q] * E[id] + o.d[q] * old;
+}
+
 __global__ void k_advance(long long* step) { *step += 1; }
 
 // Step counters of many lattices.

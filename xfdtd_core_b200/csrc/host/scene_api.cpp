@@ -170,6 +170,22 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       }
       auto mat = parseMaterial(in, name);
       sc->sim->addObject(std::make_shared<Object>(name, std::move(sh), mat));
+    } else if (kw == "voxels") {
+      in >> name;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      std::array<Index, 3> dims;
+      for (int a = 0; a < 3; ++a) {
+        const double v = num(in);
+        if (v < 1) throw XFDTDException("bad voxel count");
+        dims[a] = (Index)v;
+      }
+      const double mu_r = num(in), sigma_e = num(in);
+      std::vector<Real> eps(dims[0] * dims[1] * dims[2]);
+      for (auto& v : eps) v = num(in);
+      sc->sim->addObject(std::make_shared<VoxelObject>(
+          name, std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), dims,
+          std::move(eps), mu_r, sigma_e));
     } else if (kw == "current_source") {
       in >> name;
       const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
@@ -397,6 +413,26 @@ int xfdtd_scene_far_field(xfdtd_scene* s, int32_t n_theta, const double* theta, 
       if (dir) s->nf2ff->setOutputDir(dir);
       s->nf2ff->processFarField(th, ph, sub_dir, o);
     }
+  })
+}
+
+int xfdtd_scene_dft_objective(xfdtd_scene* s, int64_t n_steps, int32_t field,
+                              const int32_t box_s[3], const int32_t box_e[3], double freq,
+                              int32_t voxel_object, int32_t checkpoint_interval, double* value,
+                              double* grad, int64_t capacity) {
+  HOST_TRY({
+    if (!s || !value || !box_s || !box_e) throw XFDTDException("null argument");
+    const std::array<int, 3> bs{box_s[0], box_s[1], box_s[2]}, be{box_e[0], box_e[1], box_e[2]};
+    if (!grad) {
+      *value = s->sim->dftPowerObjective((Index)n_steps, field, bs, be, freq);
+    } else {
+      std::vector<Real> g;
+      *value = s->sim->dftPowerObjective((Index)n_steps, field, bs, be, freq, &g, voxel_object,
+                                         (Index)checkpoint_interval);
+      if ((std::size_t)capacity < g.size()) throw XFDTDException("gradient buffer too small");
+      std::copy(g.begin(), g.end(), grad);
+    }
+    s->finished = false;
   })
 }
 

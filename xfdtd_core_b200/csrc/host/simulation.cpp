@@ -21,6 +21,7 @@
 // node, and per-axis curl factors 1/(d*kappa).
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
@@ -72,6 +73,29 @@ ElectroMagneticProperty::ElectroMagneticProperty(Real eps_r, Real mu_r, Real sig
       _mu_r{mu_r},
       _sigma_e{sigma_e == 0 ? constant::SIGMA_E_ZERO_APPROX : sigma_e},
       _sigma_m{sigma_m == 0 ? constant::SIGMA_M_ZERO_APPROX : sigma_m} {}
+
+// --------------------------------------------------------- voxel object
+namespace {
+Real meanOf(const std::vector<Real>& v) {
+  Real s = 0;
+  for (Real x : v) s += x;
+  return v.empty() ? 1 : s / (Real)v.size();
+}
+}  // namespace
+
+VoxelObject::VoxelObject(std::string name, std::unique_ptr<Cube> cube, std::array<Index, 3> dims,
+                         std::vector<Real> eps_r, Real mu_r, Real sigma_e)
+    : Object{name, std::move(cube),
+             std::make_shared<Material>(name, ElectroMagneticProperty{meanOf(eps_r), mu_r,
+                                                                      sigma_e, 0})},
+      _dims{dims},
+      _eps_r{std::move(eps_r)},
+      _mu_r{mu_r},
+      _sigma_e{sigma_e == 0 ? constant::SIGMA_E_ZERO_APPROX : sigma_e} {
+  if (dims[0] == 0 || dims[1] == 0 || dims[2] == 0 ||
+      _eps_r.size() != dims[0] * dims[1] * dims[2])
+    throw XFDTDException("VoxelObject: eps_r does not match dims");
+}
 
 // --------------------------------------------------------- materials
 std::unique_ptr<DrudeMedium> DrudeMedium::makeDrudeMedium(std::string_view name, Real eps_inf,
@@ -237,6 +261,19 @@ struct Simulation::Impl {
   };
   std::vector<ProbeH> probes;
   NFFFTFrequencyDomain* nf2ff = nullptr;
+  // E coefficient overrides of the nodes around VoxelObjects: the node, the
+  // averaged eps (absolute) and sigma of its edge, its (ca, cb), and the
+  // voxel (object index, flat voxel index; -1: not a voxel) of each cell of
+  // the average with the cell's weight in it.
+  struct OvrE {
+    int32_t node[3];
+    int32_t comp;
+    double eps, sig, ca, cb;
+    int vobj[4];
+    int64_t voxel[4];
+    double w;
+  };
+  std::vector<OvrE> ovr;
   // TFSF set-up kept for inspection (Simulation::tfsfTables)
   std::vector<double> tf_e_inc, tf_h_inc, tf_p_int[3], tf_p_half[3];
   int tf_aux = 0;
@@ -788,6 +825,144 @@ void Simulation::init(Index time_step) {
         }
   }
 
+  // ------------------------------------------- voxel objects: E overrides
+  {
+    std::vector<const VoxelObject*> vox;
+    std::vector<int> painter_vobj(_objects.size(), -1);
+    for (std::size_t idx = 0; idx < _objects.size(); ++idx)
+      if (auto v = dynamic_cast<const VoxelObject*>(_objects[idx].get())) {
+        painter_vobj[idx] = (int)vox.size();
+        vox.push_back(v);
+      }
+    I.ovr.clear();
+    if (!vox.empty()) {
+      // Voxel of a painted cell: the voxel holding the cell centre.
+      auto voxelOf = [&](Index ci, Index cj, Index ck, int& vo) -> int64_t {
+        vo = -1;
+        const uint16_t pm = I.cell[(ci * ny + cj) * nz + ck];
+        if (pm >= painter_vobj.size() || painter_vobj[pm] < 0) return -1;
+        vo = painter_vobj[pm];
+        const VoxelObject* v = vox[(std::size_t)vo];
+        const Cube* cube = static_cast<const Cube*>(v->shape().get());
+        const Index x[3] = {ci, cj, ck};
+        int64_t flat = 0;
+        for (int a = 0; a < 3; ++a) {
+          const Real w = cube->size()(a) / (Real)v->dims()[a];
+          auto q = (int64_t)std::floor((I.h_node[a][x[a]] - cube->origin()(a)) / w);
+          q = std::max<int64_t>(0, std::min<int64_t>(q, (int64_t)v->dims()[a] - 1));
+          flat = flat * (int64_t)v->dims()[a] + q;
+        }
+        return flat;
+      };
+      // Bounding box of the voxel cells.
+      Index lo[3] = {nx, ny, nz}, hi[3] = {0, 0, 0};
+      bool any = false;
+      for (Index i = 0; i < nx; ++i)
+        for (Index j = 0; j < ny; ++j)
+          for (Index k = 0; k < nz; ++k) {
+            const uint16_t pm = I.cell[(i * ny + j) * nz + k];
+            if (pm >= painter_vobj.size() || painter_vobj[pm] < 0) continue;
+            any = true;
+            const Index x[3] = {i, j, k};
+            for (int a = 0; a < 3; ++a) {
+              lo[a] = std::min(lo[a], x[a]);
+              hi[a] = std::max(hi[a], x[a] + 1);
+            }
+          }
+      if (any) {
+        std::vector<char> e_pml[3];
+        for (int a = 0; a < 3; ++a) e_pml[a].assign(_n[a] + 1, 0);
+        for (const auto& S : I.slabs)
+          for (int l = 0; l < S.n; ++l) e_pml[S.axis][S.e_start + l] = 1;
+        int tf_lo[3] = {-1, -1, -1}, tf_hi[3] = {-1, -1, -1};
+        for (const auto& src : _sources)
+          if (auto t = std::dynamic_pointer_cast<TFSF3D>(src)) {
+            const Index org[3] = {t->x(), t->y(), t->z()};
+            for (int a = 0; a < 3; ++a) {
+              tf_lo[a] = (int)org[a];
+              tf_hi[a] = (int)(_n[a] - org[a]);
+            }
+          }
+        auto cellMat = [&](Index ci, Index cj, Index ck, int& vo, int64_t& vx) -> MatP {
+          vx = voxelOf(ci, cj, ck, vo);
+          if (vx >= 0) {
+            const VoxelObject* v = vox[(std::size_t)vo];
+            return MatP{v->epsR()[(std::size_t)vx] * EPSILON_0, 0, v->sigmaE(), 0};
+          }
+          return I.mat[I.cell[(ci * ny + cj) * nz + ck]];
+        };
+        for (Index i = lo[0]; i <= std::min(hi[0], nx); ++i)
+          for (Index j = lo[1]; j <= std::min(hi[1], ny); ++j)
+            for (Index k = lo[2]; k <= std::min(hi[2], nz); ++k)
+              for (int c = 0; c < 3; ++c) {
+                const Index x[3] = {i, j, k};
+                const Index n3[3] = {nx, ny, nz};
+                if (x[c] >= n3[c]) continue;  // component out of range
+                const int A = (c + 1) % 3, B = (c + 2) % 3;
+                // The four cells of the edge average, in the order of the
+                // class rows: (x), (x - e_A), (x - e_B), (x - e_A - e_B) for Ex
+                // (A = y, B = z); Ey, Ez by the same rule on their axes.
+                const bool full = x[A] >= 1 && x[A] < n3[A] && x[B] >= 1 && x[B] < n3[B];
+                if (!full) continue;
+                Index cells[4][3];
+                for (int q = 0; q < 4; ++q)
+                  for (int a = 0; a < 3; ++a) cells[q][a] = x[a];
+                // Ex: P(1,1,1) P(1,0,1) P(1,1,0) P(1,0,0); Ey: P(1,1,1) P(0,1,1)
+                // P(1,1,0) P(0,1,0); Ez: P(1,1,1) P(0,1,1) P(1,0,1) P(0,0,1).
+                const int first = c == 0 ? 1 : 0;   // axis stepped by cells 1 and 3
+                const int second = c == 2 ? 1 : 2;  // axis stepped by cells 2 and 3
+                cells[1][first] -= 1;
+                cells[2][second] -= 1;
+                cells[3][first] -= 1;
+                cells[3][second] -= 1;
+                Impl::OvrE o{};
+                bool touches = false;
+                MatP m[4];
+                for (int q = 0; q < 4; ++q) {
+                  m[q] = cellMat(cells[q][0], cells[q][1], cells[q][2], o.vobj[q], o.voxel[q]);
+                  if (o.voxel[q] >= 0) touches = true;
+                }
+                if (!touches) continue;
+                for (int a = 0; a < 3; ++a)
+                  if (e_pml[a][x[a]] && a != c)
+                    throw XFDTDException("a VoxelObject reaches into the CPML");
+                for (int m2 = 0; m2 < 3 && tf_lo[0] >= 0; ++m2) {
+                  const long long xm = (long long)x[m2];
+                  if (xm != tf_lo[m2] && xm != tf_hi[m2]) continue;
+                  bool within = true;
+                  for (int a = 0; a < 3; ++a)
+                    if (a != m2)
+                      within = within && (long long)x[a] >= tf_lo[a] && (long long)x[a] <= tf_hi[a];
+                  if (within) throw XFDTDException("a VoxelObject touches a TFSF face");
+                }
+                for (const auto& h : current_sources)
+                  if (h.comp == c && i >= (Index)h.s[0] && i < (Index)h.e[0] &&
+                      j >= (Index)h.s[1] && j < (Index)h.e[1] && k >= (Index)h.s[2] &&
+                      k < (Index)h.e[2])
+                    throw XFDTDException("a VoxelObject touches a current source");
+                for (int q = 0; q < 4; ++q) {
+                  const uint16_t pm = I.cell[(cells[q][0] * ny + cells[q][1]) * nz + cells[q][2]];
+                  if (I.painters[pm]->dispersion())
+                    throw XFDTDException("a VoxelObject borders a dispersive object");
+                }
+                auto avg4 = [](Real a, Real b, Real cc, Real d) {
+                  return 0.25 * (((a + b) + cc) + d);
+                };
+                o.eps = avg4(m[0].eps, m[1].eps, m[2].eps, m[3].eps);
+                o.sig = avg4(m[0].se, m[1].se, m[2].se, m[3].se);
+                o.ca = (2 * o.eps - dt * o.sig) / (2 * o.eps + dt * o.sig);
+                o.cb = (2 * dt) / (2 * o.eps + o.sig * dt);
+                o.w = 0.25;
+                o.node[0] = (int32_t)i;
+                o.node[1] = (int32_t)j;
+                o.node[2] = (int32_t)k;
+                o.comp = c;
+                I.ovr.push_back(o);
+              }
+      }
+    }
+  }
+
   if (!_use_engine) {
     setupTfsf(nullptr);
     I.initialised = true;
@@ -810,6 +985,19 @@ void Simulation::init(Index time_step) {
   checkStatus(E, xfd_set_material_classes(E, I.table.data(), (int32_t)(I.table.size() / 12),
                                           I.lattice_class.data()),
               "xfd_set_material_classes");
+  if (!I.ovr.empty()) {
+    std::vector<int32_t> on, oc;
+    std::vector<double> oa, ob;
+    for (const auto& o : I.ovr) {
+      on.insert(on.end(), o.node, o.node + 3);
+      oc.push_back(o.comp);
+      oa.push_back(o.ca);
+      ob.push_back(o.cb);
+    }
+    checkStatus(E, xfd_set_e_overrides(E, (int64_t)oc.size(), on.data(), oc.data(), oa.data(),
+                                       ob.data()),
+                "xfd_set_e_overrides");
+  }
   const double* fe[3] = {I.fe[0].data(), I.fe[1].data(), I.fe[2].data()};
   const double* fh[3] = {I.fh[0].data(), I.fh[1].data(), I.fh[2].data()};
   checkStatus(E, xfd_set_curl_factors(E, fe, fh), "xfd_set_curl_factors");
@@ -989,11 +1177,119 @@ std::vector<std::vector<Real>> Simulation::coefficientArrays() const {
               cb[q] = -b * I.fh[ta][x[ta]];
             }
           }
+      if (h == 0)
+        for (const auto& o : I.ovr) {
+          if (o.comp != c) continue;
+          const Index x[3] = {(Index)o.node[0], (Index)o.node[1], (Index)o.node[2]};
+          const Index q = (x[0] * s[1] + x[1]) * s[2] + x[2];
+          c0[q] = o.ca;
+          ca[q] = -o.cb * I.fe[tb][x[tb]];
+          cb[q] = o.cb * I.fe[ta][x[ta]];
+        }
       out.push_back(std::move(c0));
       out.push_back(std::move(ca));
       out.push_back(std::move(cb));
     }
   return out;
+}
+
+// ------------------------------------------------------------ adjoint
+namespace {
+struct DftCtx {
+  double dt, omega;
+  int64_t t0;
+};
+
+// J = sum_p |F_p|^2, F_p = dt sum_n E^n(p) exp(-i omega t_n), t_n = (t0 + n + 1) dt;
+// dJ/dE^n(p) = 2 dt Re(conj(F_p) exp(-i omega t_n)).
+int32_t dftPower(void* user, int64_t N, int64_t P, const double* rec, double* drec,
+                 double* value) {
+  const auto* c = static_cast<const DftCtx*>(user);
+  std::vector<double> fr((std::size_t)P, 0.0), fi((std::size_t)P, 0.0);
+  std::vector<double> pr((std::size_t)N), pi((std::size_t)N);
+  for (int64_t n = 0; n < N; ++n) {
+    const double ph = c->omega * (double)(c->t0 + n + 1) * c->dt;
+    pr[(std::size_t)n] = c->dt * std::cos(ph);
+    pi[(std::size_t)n] = -c->dt * std::sin(ph);
+  }
+  for (int64_t n = 0; n < N; ++n)
+    for (int64_t p = 0; p < P; ++p) {
+      fr[(std::size_t)p] += rec[n * P + p] * pr[(std::size_t)n];
+      fi[(std::size_t)p] += rec[n * P + p] * pi[(std::size_t)n];
+    }
+  double J = 0;
+  for (int64_t p = 0; p < P; ++p) J += fr[(std::size_t)p] * fr[(std::size_t)p] + fi[(std::size_t)p] * fi[(std::size_t)p];
+  for (int64_t n = 0; n < N; ++n)
+    for (int64_t p = 0; p < P; ++p)
+      drec[n * P + p] = 2 * (fr[(std::size_t)p] * pr[(std::size_t)n] + fi[(std::size_t)p] * pi[(std::size_t)n]);
+  *value = J;
+  return 0;
+}
+}  // namespace
+
+Real Simulation::dftPowerObjective(Index n_steps, int field, const std::array<int, 3>& box_s,
+                                   const std::array<int, 3>& box_e, Real freq,
+                                   std::vector<Real>* grad, int voxel_object,
+                                   Index checkpoint_interval) {
+  Impl& I = *_impl;
+  if (!I.initialised || !_engine) throw XFDTDException("Simulation not initialised");
+  DftCtx ctx{_dt, 2 * PI * freq, (int64_t)xfd_current_step(_engine)};
+  xfd_adjoint_desc d{};
+  d.n_steps = (int64_t)n_steps;
+  d.checkpoint_interval = (int32_t)std::max<Index>(1, checkpoint_interval);
+  d.forward_only = grad ? 0 : 1;
+  d.obj_field = field;
+  for (int a = 0; a < 3; ++a) {
+    d.obj_s[a] = box_s[a];
+    d.obj_e[a] = box_e[a];
+  }
+  d.objective = &dftPower;
+  d.user = &ctx;
+  double J = 0;
+  if (!grad) {
+    checkStatus(_engine, xfd_adjoint_run(_engine, &d, &J, nullptr), "xfd_adjoint_run");
+    return J;
+  }
+  // The design box: every overridden node (of any voxel object).
+  const VoxelObject* vo = nullptr;
+  int count = 0;
+  for (const auto& o : _objects)
+    if (auto v = dynamic_cast<const VoxelObject*>(o.get())) {
+      if (count == voxel_object) vo = v;
+      ++count;
+    }
+  if (!vo || I.ovr.empty()) throw XFDTDException("no such VoxelObject on the grid");
+  int lo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, hi[3] = {INT32_MIN, INT32_MIN, INT32_MIN};
+  for (const auto& o : I.ovr)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], o.node[a]);
+      hi[a] = std::max(hi[a], o.node[a] + 1);
+    }
+  for (int a = 0; a < 3; ++a) {
+    d.design_s[a] = lo[a];
+    d.design_e[a] = hi[a];
+  }
+  const int64_t nd = (int64_t)(hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]);
+  std::vector<double> sens((std::size_t)(6 * nd), 0.0);
+  checkStatus(_engine, xfd_adjoint_run(_engine, &d, &J, sens.data()), "xfd_adjoint_run");
+  grad->assign(vo->epsR().size(), 0.0);
+  const Real dt = _dt;
+  for (const auto& o : I.ovr) {
+    const int64_t p = ((int64_t)(o.node[0] - lo[0]) * (hi[1] - lo[1]) + (o.node[1] - lo[1])) *
+                          (hi[2] - lo[2]) +
+                      (o.node[2] - lo[2]);
+    const double s0 = sens[(std::size_t)(o.comp * nd + p)];
+    const double s1 = sens[(std::size_t)((3 + o.comp) * nd + p)];
+    // ca = (2 eps - sig dt) / (2 eps + sig dt), cb = 2 dt / (2 eps + sig dt)
+    const double den = 2 * o.eps + o.sig * dt;
+    const double dca = 4 * o.sig * dt / (den * den);
+    const double dcb_cb = -2 / den;
+    const double dj = (dca - o.ca * dcb_cb) * s0 + dcb_cb * s1;  // dJ/d(edge eps)
+    for (int q = 0; q < 4; ++q)
+      if (o.voxel[q] >= 0 && o.vobj[q] == voxel_object)
+        (*grad)[(std::size_t)o.voxel[q]] += o.w * EPSILON_0 * dj;
+  }
+  return J;
 }
 
 void Simulation::setupTfsf(xfd_engine* E) {

@@ -121,6 +121,13 @@ def load(build_if_missing: bool = True):
         "xfd_stream": ([vp], vp),
         "xfd_launches_per_step": ([vp], _i32),
         "xfd_stencil_bytes_per_step": ([vp], _i64),
+        "xfd_set_e_overrides": ([vp, _i64, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _dp, _dp],
+                                ctypes.c_int),
+        "xfd_checkpoint_save": ([vp, _i32], ctypes.c_int),
+        "xfd_checkpoint_load": ([vp, _i32], ctypes.c_int),
+        "xfd_checkpoint_drop": ([vp, _i32], ctypes.c_int),
+        "xfd_checkpoint_step": ([vp, _i32], _i64),
+        "xfd_adjoint_run": ([vp, vp, _dp, _dp], ctypes.c_int),
         "xfd_batch_create": ([ctypes.POINTER(vp), _i32, ctypes.POINTER(vp)], ctypes.c_int),
         "xfd_batch_destroy": ([vp], None),
         "xfd_batch_last_error": ([vp], ctypes.c_char_p),
@@ -150,7 +157,9 @@ def exported_symbols() -> List[str]:
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
-            "xfd_launches_per_step", "xfd_stencil_bytes_per_step", "xfd_batch_create",
+            "xfd_launches_per_step", "xfd_stencil_bytes_per_step", "xfd_set_e_overrides",
+            "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
+            "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_batch_create",
             "xfd_batch_destroy", "xfd_batch_last_error", "xfd_batch_run", "xfd_batch_sync",
             "xfd_batch_set_option", "xfd_batch_get_option", "xfd_batch_tuning",
             "xfd_batch_size", "xfd_batch_launches_per_step", "xfd_batch_stream"]
@@ -330,6 +339,19 @@ class Engine:
 
     def stencil_bytes_per_step(self) -> int:
         return int(self.L.xfd_stencil_bytes_per_step(self.h))
+
+    # ------------------------------------------------------- saved states
+    def checkpoint_save(self, slot: int):
+        self._check(self.L.xfd_checkpoint_save(self.h, int(slot)), "checkpoint_save")
+
+    def checkpoint_load(self, slot: int):
+        self._check(self.L.xfd_checkpoint_load(self.h, int(slot)), "checkpoint_load")
+
+    def checkpoint_drop(self, slot: int):
+        self._check(self.L.xfd_checkpoint_drop(self.h, int(slot)), "checkpoint_drop")
+
+    def checkpoint_step(self, slot: int) -> int:
+        return int(self.L.xfd_checkpoint_step(self.h, int(slot)))
 
     # --------------------------------------------------------------- outputs
     def movie_frames(self, mid: int, box_shape) -> np.ndarray:

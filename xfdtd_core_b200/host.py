@@ -55,6 +55,8 @@ def load():
                                    ctypes.c_char_p, ctypes.c_char_p], ctypes.c_int),
         "xfdtd_scene_field_time": ([vp, i32, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
         "xfdtd_scene_write_outputs": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "xfdtd_scene_dft_objective": ([vp, i64, i32, i32 * 3, i32 * 3, ctypes.c_double, i32, i32,
+                                       _dp, _dp, i64], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -70,7 +72,7 @@ def exported_symbols() -> List[str]:
             "xfdtd_scene_advance", "xfdtd_scene_tfsf", "xfdtd_scene_finish",
             "xfdtd_scene_coefficients", "xfdtd_scene_field", "xfdtd_scene_movie",
             "xfdtd_scene_nf2ff", "xfdtd_scene_far_field", "xfdtd_scene_field_time",
-            "xfdtd_scene_write_outputs"]
+            "xfdtd_scene_write_outputs", "xfdtd_scene_dft_objective"]
 
 
 class SceneRun:
@@ -213,6 +215,29 @@ class SceneRun:
             directory.encode() if directory else None, sub_dir.encode() if sub_dir else None))
         n_ang = th.size * ph.size
         return (out[0::2] + 1j * out[1::2]).reshape(-1, 4, n_ang)
+
+    def dft_objective(self, n_steps: int, field: int, box_s, box_e, freq: float,
+                      grad: bool = False, voxel_object: int = 0,
+                      checkpoint_interval: int = 250):
+        """J = sum_p |F_p|^2, F_p = dt sum_n E^n(p) exp(-i 2 pi freq n dt) over the
+        next n_steps steps at the nodes of [box_s, box_e) of E component
+        `field`; with grad=True also dJ/deps_r per voxel of the VoxelObject
+        (discrete adjoint).  Returns J, or (J, grad array in the voxel shape)."""
+        J = ctypes.c_double()
+        bs = (ctypes.c_int32 * 3)(*box_s)
+        be = (ctypes.c_int32 * 3)(*box_e)
+        if not grad:
+            self._check(self.L.xfdtd_scene_dft_objective(self.h, int(n_steps), field, bs, be,
+                                                         float(freq), voxel_object,
+                                                         checkpoint_interval, ctypes.byref(J),
+                                                         None, 0))
+            return J.value
+        vox = [o for o in self.scene.objects if hasattr(o, "voxel_index")][voxel_object]
+        g = np.zeros(np.asarray(vox.eps_r).shape)
+        self._check(self.L.xfdtd_scene_dft_objective(
+            self.h, int(n_steps), field, bs, be, float(freq), voxel_object, checkpoint_interval,
+            ctypes.byref(J), g.ctypes.data_as(_dp), g.size))
+        return J.value, g
 
     def write_outputs(self, directory: str):
         self._check(self.L.xfdtd_scene_write_outputs(self.h, directory.encode()))

@@ -159,6 +159,41 @@ class ObjectSpec:
 
 
 @dataclass
+class VoxelSpec:
+    """A block of per-voxel relative permittivities (xfdtd::VoxelObject): the
+    cube (origin, size) divided into eps_r.shape voxels; a cell whose centre
+    lies in the cube is painted (in object order, like any object) with the
+    eps_r of the voxel holding its centre and the common mu_r, sigma_e."""
+    name: str
+    origin: Vec3
+    size: Vec3
+    eps_r: np.ndarray
+    mu_r: float = 1.0
+    sigma_e: float = 0.0
+
+    @property
+    def shape(self) -> Shape:
+        return cube(self.origin, self.size)
+
+    @property
+    def material(self) -> Material:
+        return Material("simple", float(np.mean(self.eps_r)), self.mu_r, self.sigma_e, 0.0)
+
+    def voxel_index(self, a: int, centre: np.ndarray) -> np.ndarray:
+        """Voxel index along axis a of cell centres (VoxelObject's rule)."""
+        n = self.eps_r.shape[a]
+        w = self.size[a] / n
+        q = np.floor((centre - self.origin[a]) / w).astype(np.int64)
+        return np.clip(q, 0, n - 1)
+
+    def text(self) -> str:
+        e = np.asarray(self.eps_r, dtype=np.float64)
+        return (f"voxels {self.name} " + " ".join(_f(v) for v in (*self.origin, *self.size)) +
+                f" {e.shape[0]} {e.shape[1]} {e.shape[2]} {_f(self.mu_r)} {_f(self.sigma_e)} " +
+                " ".join(repr(float(v)) for v in e.ravel()))
+
+
+@dataclass
 class CurrentSourceSpec:
     name: str
     shape: Shape  # a Cube
@@ -404,6 +439,47 @@ def dispersive_spheres(n: int = 384, pml: int = 10, dl: float = 5e-4, radius_cel
                                   cube((-half, -half, 0.0), (2 * half, 2 * half, dl)),
                                   movie_interval))
     return s
+
+
+def adjoint_slab(nxy: int = 256, nz: int = 128, pml: int = 12, dl: float = 2e-4,
+                 slab_z=(48, 64), slab_eps: float = 2.1, design=(96, 96, 16), seed: int = 2,
+                 eps_range=(1.0, 12.0), freq: float = 1e12, steps: int = 5000,
+                 tfsf_start: int = 16, patch: int = 16, patch_z: int = 72):
+    """Adjoint inverse-design scene: nxy x nxy x nz cells including a `pml`-cell
+    CPML (default parameters), dl = 0.2 mm, an eps_r = 2.1 slab over the whole
+    interior in x, y at cell layers z in [slab_z), a design block of
+    design[0] x design[1] x design[2] voxels (one per cell) centred in x, y
+    on the same layers with eps_r U[eps_range] from numpy default_rng(seed),
+    an x-polarised normal-incidence TFSF plane wave (theta = phi = psi = 0)
+    carrying a cosine-modulated Gaussian at `freq` (tau = 2 / (pi freq)),
+    CFL 0.99.  Returns (scene, objective) with objective = dict(field=2 (Ez),
+    box_s, box_e: the patch x patch node block centred in x, y at node layer
+    patch_z, freq)."""
+    s = Scene(dl=(dl, dl, dl), cfl=0.99, steps=steps, name="adjoint_slab")
+    n = (nxy, nxy, nz)
+    half = [(n[a] - 2 * pml) * dl / 2 for a in range(3)]
+    s.objects.append(ObjectSpec("domain", cube(tuple(-h for h in half),
+                                               tuple(2 * h for h in half)), air()))
+    # cell index c (CPML included) has its lower face at -half + (c - pml) dl
+    def x0(a, c):
+        return -half[a] + (c - pml) * dl
+    z0, z1 = slab_z
+    s.objects.append(ObjectSpec("slab", cube((-half[0], -half[1], x0(2, z0)),
+                                             (2 * half[0], 2 * half[1], (z1 - z0) * dl)),
+                                Material("simple", slab_eps, 1.0, 0.0, 0.0)))
+    rng = np.random.default_rng(seed)
+    eps = rng.uniform(eps_range[0], eps_range[1], size=design)
+    c0 = [(n[a] - design[a]) // 2 for a in range(2)] + [z0 + (z1 - z0 - design[2]) // 2]
+    s.objects.append(VoxelSpec("design", tuple(x0(a, c0[a]) for a in range(3)),
+                               tuple(design[a] * dl for a in range(3)), eps))
+    s.pmls = pml_all(pml)
+    tau = 2.0 / (math.pi * freq)
+    s.tfsf = TFSFSpec(tfsf_start, tfsf_start, tfsf_start, 0.0, 0.0, 0.0,
+                      Waveform("cosgauss", tau, 4.5 * tau, freq))
+    p0 = [(n[a] - patch) // 2 for a in range(2)]
+    objective = dict(field=2, box_s=(p0[0], p0[1], patch_z),
+                     box_e=(p0[0] + patch, p0[1] + patch, patch_z + 1), freq=freq)
+    return s, objective
 
 
 def batched_sphere_params(count: int = 96, seed: int = 1, n_lo: int = 64, n_hi: int = 224):
