@@ -50,6 +50,8 @@ KIND = "boxes"  # --workload: boxes (the default) or dispersive
 
 
 def workload_name(n: int) -> str:
+    if KIND == "adjoint":
+        return "adjoint_slab_256x256x128_cpml12_design96x96x16_dft1THz"
     if KIND == "batched":
         return "batched_spheres_96_scenes_64^3-224^3_cpml8_tfsf"
     if KIND == "dispersive":
@@ -65,6 +67,8 @@ def workload_scene(steps: int, n: int = 256):
     from xfdtd_core_b200 import scene as S
     if KIND == "dispersive":
         return S.dispersive_spheres(n=n, steps=steps)
+    if KIND == "adjoint":
+        return S.adjoint_slab(steps=steps)[0]
     if KIND == "batched":  # the median-size scene of the batch (the CPU sample)
         params = S.batched_sphere_params()
         return S.batched_sphere(steps=steps, **sorted(params, key=lambda p: p["n"])[len(params) // 2])
@@ -475,6 +479,126 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- adjoint
+def run_adjoint(args, world, rank, local, pg, warmup, steps):
+    """The adjoint workload: forward FP32 steps timed alone, then the gradient
+    dJ/deps_r of every design voxel (forward with saved states every K steps,
+    segment recompute, reverse sweeps) timed as one call, then the FP64
+    central-difference check on --fd-voxels random voxels."""
+    import torch
+    torch.cuda.set_device(local)
+    from xfdtd_core_b200 import engine as E
+    from xfdtd_core_b200 import scene as S
+    from xfdtd_core_b200.host import SceneRun
+    hbm, peak_kind = peaks()
+    sc, ob = S.adjoint_slab(steps=warmup + steps + 2)
+    args_ob = (ob["field"], ob["box_s"], ob["box_e"], ob["freq"])
+    # forward alone (FP32)
+    run = SceneRun(sc, precision=1)
+    nx, ny, nz = run.n
+    cells = nx * ny * nz
+    L = E.load()
+    h = ctypes_handle(run.engine_handle())
+    bytes_step = int(L.xfd_stencil_bytes_per_step(h))
+    launches_fwd = int(L.xfd_launches_per_step(h))
+    sampler = ClockSampler(local)
+    ms_fwd, clocks = time_engine_steps(run.engine_handle(), steps, warmup, pg, local, sampler)
+    run.close()
+    # gradient (FP32): one call, host objective included
+    sc32, _ = S.adjoint_slab(steps=steps)
+    run = SceneRun(sc32, precision=1)
+    torch.cuda.synchronize()
+    barrier(pg)
+    t0 = time.perf_counter()
+    J32, g32 = run.dft_objective(steps, *args_ob, grad=True,
+                                 checkpoint_interval=args.checkpoint_interval)
+    torch.cuda.synchronize()
+    adj_s = max_over_ranks(pg, time.perf_counter() - t0)
+    run.close()
+    fwd_s = ms_fwd / 1e3
+    value = cells * steps / adj_s / 1e9
+    vox = [o for o in sc32.objects if hasattr(o, "voxel_index")][0]
+    eps0 = np.array(vox.eps_r)
+    # FP64: the adjoint gradient and central differences on random voxels
+    fd = {}
+    if rank == 0 and args.fd_voxels > 0:
+        sc64, _ = S.adjoint_slab(steps=steps)
+        r64 = SceneRun(sc64, precision=0)
+        t1 = time.perf_counter()
+        J64, g64 = r64.dft_objective(steps, *args_ob, grad=True,
+                                     checkpoint_interval=args.checkpoint_interval)
+        adj64_s = time.perf_counter() - t1
+        r64.close()
+        rng = np.random.default_rng(7)
+        picks = rng.choice(eps0.size, size=args.fd_voxels, replace=False)
+        fdv, a32, a64 = [], [], []
+        hstep = 1e-4
+
+        def J_of(eps):
+            s2, _ = S.adjoint_slab(steps=steps)
+            v2 = [o for o in s2.objects if hasattr(o, "voxel_index")][0]
+            v2.eps_r = eps
+            r = SceneRun(s2, precision=0)
+            val = r.dft_objective(steps, *args_ob)
+            r.close()
+            return val
+        t2 = time.perf_counter()
+        for q in picks:
+            idx = np.unravel_index(int(q), eps0.shape)
+            ep, em = eps0.copy(), eps0.copy()
+            ep[idx] += hstep
+            em[idx] -= hstep
+            fdv.append((J_of(ep) - J_of(em)) / (2 * hstep))
+            a32.append(g32[idx])
+            a64.append(g64[idx])
+        fdv, a32, a64 = np.array(fdv), np.array(a32), np.array(a64)
+        fd = {"voxels": int(args.fd_voxels), "h": hstep,
+              "fp32_adjoint_vs_fp64_fd_rel_l2": float(np.linalg.norm(a32 - fdv) /
+                                                      np.linalg.norm(fdv)),
+              "fp64_adjoint_vs_fp64_fd_rel_l2": float(np.linalg.norm(a64 - fdv) /
+                                                      np.linalg.norm(fdv)),
+              "fp32_vs_fp64_adjoint_rel_l2_all_voxels": float(np.linalg.norm(g32 - g64) /
+                                                              np.linalg.norm(g64)),
+              "fp64_adjoint_s": adj64_s, "fd_runs_s": time.perf_counter() - t2,
+              "J_fp32": J32, "J_fp64": J64}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": adj_s * 1e3 / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(0), "cells": cells, "grid": [nx, ny, nz],
+                       "cpml": 12, "design_voxels": int(eps0.size),
+                       "checkpoint_interval": args.checkpoint_interval,
+                       "precision": "fp32",
+                       "l2": "inputs larger than L2 (fields 6 x 257 x 257 x 160 x 4 B = 254 MB)",
+                       "parallelism": f"replicas x{world}",
+                       "value_is": "cell-updates of the forward run per second of the whole "
+                                   "gradient computation (forward with saved states, segment "
+                                   "recompute, reverse sweeps, objective)"},
+            "roofline": {"bound": "hbm", "achieved": bytes_step / (fwd_s / steps) / 1e9,
+                         "peak": hbm, "unit": "GB/s",
+                         "frac": bytes_step / (fwd_s / steps) / 1e9 / hbm, "traffic": None,
+                         "peak_source": peak_kind,
+                         "kernel": "the forward step's sweep launches",
+                         "note": "forward FP32 step of the adjoint scene: algorithmic stencil "
+                                 f"bytes per step ({bytes_step} B) / step time"},
+            "forms": {"forward_fp32": {"value": cells * steps / fwd_s / 1e9, "unit": UNIT,
+                                       "ms_per_step": ms_fwd / steps},
+                      "adjoint_over_forward": adj_s / fwd_s,
+                      "gradient_s": adj_s, "forward_s": fwd_s},
+            "fd_check": fd,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(np.prod(np.array(ob["box_e"]) -
+                                                      np.array(ob["box_s"]))) * 4,
+                    "note": "the gradient call through the C ABI: objective record copied "
+                            "to the host, the objective evaluated there, gradient copied back"},
+            "gpu_launches": launches_fwd * steps,
+            "clocks": clocks,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -484,11 +608,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=256, help="cells per axis incl. CPML")
-    ap.add_argument("--workload", default="boxes", choices=["boxes", "dispersive", "batched"],
+    ap.add_argument("--workload", default="boxes",
+                    choices=["boxes", "dispersive", "batched", "adjoint"],
                     help="boxes: the headline dielectric-boxes scene; dispersive: ADE + TFSF + "
                          "NF2FF spheres (use --grid 384 for its full size); batched: 96 sphere "
                          "scenes of uneven sizes advanced together")
     ap.add_argument("--scenes", type=int, default=96, help="scenes of --workload batched")
+    ap.add_argument("--fd-voxels", type=int, default=32,
+                    help="voxels of the FP64 central-difference check (--workload adjoint)")
+    ap.add_argument("--checkpoint-interval", type=int, default=250,
+                    help="steps between saved states of the adjoint (--workload adjoint)")
     ap.add_argument("--seq-steps", type=int, default=64,
                     help="steps per scene of the one-at-a-time comparison (batched)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
@@ -505,7 +634,8 @@ def main():
     global KIND
     KIND = args.workload
     warmup = max(3, args.warmup)
-    steps = args.steps if args.steps is not None else (3000 if KIND == "batched" else 4000)
+    steps = args.steps if args.steps is not None else {"batched": 3000,
+                                                       "adjoint": 5000}.get(KIND, 4000)
 
     world, rank, local, pg = dist_setup(args.gpus)
 
@@ -538,6 +668,11 @@ def main():
 
     if KIND == "batched":
         run_batched(args, world, rank, local, pg, warmup, steps)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if KIND == "adjoint":
+        run_adjoint(args, world, rank, local, pg, warmup, steps)
         if pg is not None:
             pg.destroy_process_group()
         return

@@ -160,3 +160,44 @@ def test_checkpoint_save_load_roundtrip(precision):
     assert L.xfd_checkpoint_drop(h, 3) == 0
     assert L.xfd_checkpoint_step(h, 3) == -1
     r.close()
+
+
+class DftPower:
+    """torch.autograd.Function over the adjoint (test harness only): J(eps_r)
+    forward, dJ/deps_r from the discrete adjoint on backward."""
+
+    @staticmethod
+    def make():
+        import torch
+
+        class _F(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, eps):
+                sc, _ = _scene(eps.detach().cpu().numpy())
+                ob = voxels_objective()
+                r = SceneRun(sc)
+                J, g = r.dft_objective(STEPS, ob["field"], ob["box_s"], ob["box_e"], ob["freq"],
+                                       grad=True, checkpoint_interval=64)
+                r.close()
+                ctx.save_for_backward(torch.from_numpy(g))
+                return torch.tensor(J, dtype=torch.float64)
+
+            @staticmethod
+            def backward(ctx, gJ):
+                (g,) = ctx.saved_tensors
+                return gJ * g
+
+        return _F
+
+
+def test_torch_autograd_shim():
+    import torch
+    _, vox = _scene()
+    eps = torch.tensor(np.array(vox.eps_r), dtype=torch.float64, requires_grad=True)
+    J = DftPower.make().apply(eps)
+    (3.0 * J).backward()
+    idx = _sample(tuple(eps.shape), 2, seed=21)
+    e0 = np.array(vox.eps_r)
+    for q in idx:
+        fd = _fd(e0, q, _J_gpu)
+        assert abs(eps.grad[q].item() - 3.0 * fd) <= 1e-6 * abs(3.0 * fd)

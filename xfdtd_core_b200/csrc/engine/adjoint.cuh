@@ -17,8 +17,8 @@
 //                               slab along ta: d = d_a, "which" 1, sign +)
 //     E' = [M ? ca : 1] E + cb (M fe[ta] d_a - M fe[tb] d_b) + cb (-psi'_0 + psi'_1)
 // (M: the node is in the main update range.)  The adjoint variables lam
-// (fields) and lam_psi (CPML) live in arrays of the forward layout.  One
-// reverse step m -> m-1 is two lattice sweeps:
+// (fields, scaled as described below) and lam_psi (CPML) live in arrays of
+// the forward layout.  One reverse step m -> m-1 is two lattice sweeps:
 //   k_adj_h: per H node, lam_psi_h <- b_h (lam_psi_h + s cb lam_H);
 //            lam_H <- [M ? ca : 1] lam_H + (transposed E-update differences of lam_E)
 //   k_adj_e: per E node, lam_psi_e <- b_e (lam_psi_e + s cb lam_E);
@@ -30,7 +30,9 @@
 // transpose requires.
 #pragma once
 
+#include "fused.cuh"
 #include "kernels.cuh"
+#include "march.cuh"
 
 namespace xfd {
 
@@ -67,169 +69,185 @@ __device__ __forceinline__ void e_coeff(const OvBoxD<T>& ov, const T* row, int c
   }
 }
 
-// Adjoint of one curl difference of the E update of component c at node
-// (i, j, k): want_a selects d_a (else d_b).  lam fields in a.f, lam_psi_e
-// in the slabs' psi_e; zero where the node is outside the lattice or the
-// component outside its range.
-template <typename T>
-__device__ __forceinline__ T e_diff_adj(const YeeP<T>& a, const OvBoxD<T>& ov, int i, int j, int k,
-                                        int c, bool want_a) {
-  const Lat& L = a.L;
-  if (!in_lattice(L, i, j, k)) return T(0);
-  const int x[3] = {i, j, k};
-  const int n[3] = {L.nx, L.ny, L.nz};
-  bool valid = true, main_rng = true;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    if (d == c) {
-      valid = valid && (x[d] < n[d]);
-    } else {
-      valid = valid && (x[d] <= n[d]);
-      main_rng = main_rng && (x[d] >= 1) && (x[d] < n[d]);
-    }
-  }
-  if (!valid) return T(0);
-  const long long id = lat_index(L, i, j, k);
-  const T lam = a.f[c][id];
-  T ca, cb;
-  e_coeff(ov, a.tab + (size_t)a.cls[id] * 12, c, i, j, k, ca, cb);
-  const int ta = (c + 1) % 3, tb = (c + 2) % 3;
-  T v = T(0);
-  if (main_rng) v = want_a ? cb * a.fe[ta][x[ta]] * lam : -cb * a.fe[tb][x[tb]] * lam;
-  for (int s = 0; s < a.n_slab; ++s) {
-    const SlabD<T>& sl = a.slab[s];
-    if (sl.m == c) continue;
-    const int which = (c == (sl.m + 1) % 3) ? 0 : 1;  // 0: d_b (slab along tb), 1: d_a
-    if ((which == 1) != want_a) continue;
-    const int l = x[sl.m] - sl.e_lo;
-    if (l < 0 || l >= sl.n) continue;
-    const T pe = sl.psi_e[which][psi_index(sl, L, i, j, k, l)] + (which == 0 ? -cb : cb) * lam;
-    v += sl.a_e[l] * pe;
+// The reverse pass runs on scaled adjoint fields u_c = cb_c lam_E,c (E
+// nodes) and w_c = -cb_c lam_H,c (H nodes), with (ca, cb) the node's class
+// pair.  Written in u and w the reverse step is, node for node, the forward
+// step with the same (ca, cb): on a CPML-free box with uniform curl factors
+// (the transposed differences weigh the source node, the forward ones the
+// destination) the forward marching sweeps run it unchanged, and the gather
+// kernels below do the exact transpose on the rest of the lattice.  The CPML
+// adjoints lam_psi stay unscaled.
+//
+// Index of a psi cell of the slab in slot q along axis AX (layer l).
+template <typename T, int AX>
+__device__ __forceinline__ long long psi_at(const MarchP<T>& p, int q, int i, int j, int k, int l) {
+  const Lat& L = p.L;
+  if (AX == 0) return ((long long)l * L.NY + j) * L.KP + k;
+  if (AX == 1) return ((long long)i * p.slab[1].n[q] + l) * L.KP + k;
+  return ((long long)i * L.NY + j) * p.slab[2].n[q] + l;
+}
+
+// X terms (adjoint of one difference of the E update of component C at node
+// (i, j, k); zero outside the lattice or the component's range):
+//   X_a = M fe[ta][x_ta] u + a_e (lam_psi + u)    (d_a: slab along ta)
+//   X_b = -M fe[tb][x_tb] u + a_e (lam_psi - u)   (d_b: slab along tb)
+template <typename T, int C, bool WANT_A>
+__device__ __forceinline__ T x_term(const MarchP<T>& p, int i, int j, int k) {
+  constexpr int TA = (C + 1) % 3, TB = (C + 2) % 3, AX = WANT_A ? TA : TB;
+  constexpr int W = (C == (AX + 1) % 3) ? 0 : 1;  // psi component slot of C in that slab
+  const Lat& L = p.L;
+  if (i < 0 || j < 0 || k < 0 || i > L.nx || j > L.ny || k > L.nz) return T(0);
+  if (pick<C>(i, j, k) >= pick<C>(L.nx, L.ny, L.nz)) return T(0);
+  const int xa = pick<TA>(i, j, k), xb = pick<TB>(i, j, k);
+  const bool main_rng = xa >= 1 && xa < pick<TA>(L.nx, L.ny, L.nz) && xb >= 1 &&
+                        xb < pick<TB>(L.nx, L.ny, L.nz);
+  const T u = p.f[C][lat_index(L, i, j, k)];
+  T v = main_rng ? (WANT_A ? p.fe[TA][xa] * u : -p.fe[TB][xb] * u) : T(0);
+  int q;
+  const int l = layer_of(p.slab[AX], pick<AX>(i, j, k), true, q);
+  if (l >= 0) {
+    const SlabAxisD<T>& A = p.slab[AX];
+    v += A.a_e[q][l] * (A.psi_e[q][W][psi_at<T, AX>(p, q, i, j, k, l)] + (WANT_A ? u : -u));
   }
   return v;
 }
 
-// Adjoint of one curl difference of the H update of component c at node
-// (i, j, k): want_a selects d_a (else d_b).
+// Y terms (adjoint of one difference of the H update of component C at y):
+//   Y_a = -M fh[tb][y_tb] w + a_h (lam_psi - w)   (d_a: slab along tb)
+//   Y_b = M fh[ta][y_ta] w + a_h (lam_psi + w)    (d_b: slab along ta)
+template <typename T, int C, bool WANT_A>
+__device__ __forceinline__ T y_term(const MarchP<T>& p, int i, int j, int k) {
+  constexpr int TA = (C + 1) % 3, TB = (C + 2) % 3, AX = WANT_A ? TB : TA;
+  constexpr int W = (C == (AX + 1) % 3) ? 0 : 1;
+  const Lat& L = p.L;
+  if (i < 0 || j < 0 || k < 0 || i > L.nx || j > L.ny || k > L.nz) return T(0);
+  const int xa = pick<TA>(i, j, k), xb = pick<TB>(i, j, k);
+  if (xa >= pick<TA>(L.nx, L.ny, L.nz) || xb >= pick<TB>(L.nx, L.ny, L.nz)) return T(0);
+  const bool main_rng = pick<C>(i, j, k) < pick<C>(L.nx, L.ny, L.nz);
+  const T w = p.f[3 + C][lat_index(L, i, j, k)];
+  T v = main_rng ? (WANT_A ? -p.fh[TB][xb] * w : p.fh[TA][xa] * w) : T(0);
+  int q;
+  const int l = layer_of(p.slab[AX], pick<AX>(i, j, k), false, q);
+  if (l >= 0) {
+    const SlabAxisD<T>& A = p.slab[AX];
+    v += A.a_h[q][l] * (A.psi_h_out[q][W][psi_at<T, AX>(p, q, i, j, k, l)] + (WANT_A ? -w : w));
+  }
+  return v;
+}
+
+// Node box swept by the forward marching kernels on the scaled fields (k,
+// j, i ranges [lo, hi)); the gather kernels skip it.  The gather grid starts
+// at node (org_k, org_j) (<= 0) so that its 32 x 8 CTAs line up with the
+// box's tiles: a CTA lies wholly inside the box or wholly outside.
+struct AdjBox {
+  int lo[3], hi[3];
+  int org_k, org_j;
+};
+
+__device__ __forceinline__ bool in_adj_box(const AdjBox& b, int i, int j, int k) {
+  return k >= b.lo[0] && k < b.hi[0] && j >= b.lo[1] && j < b.hi[1] && i >= b.lo[2] &&
+         i < b.hi[2];
+}
+
+// The whole CTA of a gather kernel (32 x 8 nodes of plane i) in the box.
+__device__ __forceinline__ bool cta_in_adj_box(const AdjBox& b) {
+  const int k0 = b.org_k + blockIdx.x * blockDim.x, j0 = b.org_j + blockIdx.y * blockDim.y;
+  return in_adj_box(b, blockIdx.z, j0, k0) &&
+         in_adj_box(b, blockIdx.z, j0 + blockDim.y - 1, k0 + blockDim.x - 1);
+}
+
+// Psi adjoint of component Q in the slab along axis M at node (i, j, k):
+// lam_psi <- b (lam_psi + s v), s = -1 for the slab's first component.
+template <typename T, int Q, int M, bool E>
+__device__ __forceinline__ void psi_adj(const MarchP<T>& p, int i, int j, int k, T v) {
+  constexpr int W = (Q == (M + 1) % 3) ? 0 : 1;
+  int q;
+  const int l = layer_of(p.slab[M], pick<M>(i, j, k), E, q);
+  if (l < 0) return;
+  const SlabAxisD<T>& A = p.slab[M];
+  T* ps = (E ? A.psi_e[q][W] : A.psi_h_out[q][W]) + psi_at<T, M>(p, q, i, j, k, l);
+  *ps = (E ? A.b_e[q][l] : A.b_h[q][l]) * (*ps + (W == 0 ? -v : v));
+}
+
+// H_Q at y (R1 = Q+1, R2 = Q+2) is the d_a operand of E_R1 (differenced
+// along R2) and the d_b operand of E_R2 (differenced along R1) in the forward
+// E update.  Completes the previous reverse step's H adjoint first.
+template <typename T, int Q>
+__device__ __forceinline__ void adj_h_comp(const MarchP<T>& p, const T* row, int i, int j, int k,
+                                           long long id, bool main_rng) {
+  constexpr int R1 = (Q + 1) % 3, R2 = (Q + 2) % 3;
+  const Lat& L = p.L;
+  if (pick<R1>(i, j, k) >= pick<R1>(L.nx, L.ny, L.nz) ||
+      pick<R2>(i, j, k) >= pick<R2>(L.nx, L.ny, L.nz))
+    return;  // H_Q out of range
+  T* Wq = p.f[3 + Q];
+  const T w = Wq[id];
+  psi_adj<T, Q, R1, false>(p, i, j, k, w);
+  psi_adj<T, Q, R2, false>(p, i, j, k, w);
+  const T sum = x_term<T, R1, true>(p, i, j, k) -
+                x_term<T, R1, true>(p, i + (R2 == 0), j + (R2 == 1), k + (R2 == 2)) +
+                x_term<T, R2, false>(p, i, j, k) -
+                x_term<T, R2, false>(p, i + (R1 == 0), j + (R1 == 1), k + (R1 == 2));
+  Wq[id] = (main_rng ? row[6 + 2 * Q] * w : w) - row[7 + 2 * Q] * sum;
+}
+
+// E_Q at x (R1 = Q+1, R2 = Q+2) is the d_a operand of H_R2 (differenced
+// along R1) and the d_b operand of H_R1 (differenced along R2) in the forward
+// H update.  Nodes with a coefficient override take the class pair here and
+// the override fix-up afterwards, as in the forward step.
+template <typename T, int Q>
+__device__ __forceinline__ void adj_e_comp(const MarchP<T>& p, const T* row, int i, int j, int k,
+                                           long long id) {
+  constexpr int R1 = (Q + 1) % 3, R2 = (Q + 2) % 3;
+  const Lat& L = p.L;
+  if (pick<Q>(i, j, k) >= pick<Q>(L.nx, L.ny, L.nz)) return;  // E_Q out of range
+  T* Uq = p.f[Q];
+  const T u = Uq[id];
+  psi_adj<T, Q, R1, true>(p, i, j, k, u);
+  psi_adj<T, Q, R2, true>(p, i, j, k, u);
+  const int x1 = pick<R1>(i, j, k), x2 = pick<R2>(i, j, k);
+  const bool main_rng = x1 >= 1 && x1 < pick<R1>(L.nx, L.ny, L.nz) && x2 >= 1 &&
+                        x2 < pick<R2>(L.nx, L.ny, L.nz);
+  const T sum = y_term<T, R2, true>(p, i - (R1 == 0), j - (R1 == 1), k - (R1 == 2)) -
+                y_term<T, R2, true>(p, i, j, k) +
+                y_term<T, R1, false>(p, i - (R2 == 0), j - (R2 == 1), k - (R2 == 2)) -
+                y_term<T, R1, false>(p, i, j, k);
+  Uq[id] = (main_rng ? row[2 * Q] * u : u) + row[2 * Q + 1] * sum;
+}
+
+// Reverse H sweep outside the box (one thread per node).
 template <typename T>
-__device__ __forceinline__ T h_diff_adj(const YeeP<T>& a, int i, int j, int k, int c, bool want_a) {
-  const Lat& L = a.L;
-  if (!in_lattice(L, i, j, k)) return T(0);
-  const int x[3] = {i, j, k};
-  const int n[3] = {L.nx, L.ny, L.nz};
-  bool valid = true;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) valid = valid && ((d == c) ? (x[d] <= n[d]) : (x[d] < n[d]));
-  if (!valid) return T(0);
+__global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ MarchP<T> p,
+                                               const __grid_constant__ AdjBox box) {
+  if (cta_in_adj_box(box)) return;
+  const int k = box.org_k + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = box.org_j + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+  const int i = blockIdx.z;
+  const Lat& L = p.L;
+  if (k < 0 || j < 0 || k > L.nz || j > L.ny || i > L.nx || in_adj_box(box, i, j, k)) return;
+  const long long id = lat_index(L, i, j, k);
+  const T* row = p.tab + (size_t)p.cls[id] * 12;
   const bool main_rng = (i < L.nx) && (j < L.ny) && (k < L.nz);
-  const long long id = lat_index(L, i, j, k);
-  const T lam = a.f[3 + c][id];
-  const T cb = a.tab[(size_t)a.cls[id] * 12 + 7 + 2 * c];
-  const int ta = (c + 1) % 3, tb = (c + 2) % 3;
-  T v = T(0);
-  if (main_rng) v = want_a ? cb * a.fh[tb][x[tb]] * lam : -cb * a.fh[ta][x[ta]] * lam;
-  for (int s = 0; s < a.n_slab; ++s) {
-    const SlabD<T>& sl = a.slab[s];
-    if (sl.m == c) continue;
-    const int which = (c == (sl.m + 1) % 3) ? 0 : 1;  // 0: d_a (slab along tb), 1: d_b
-    if ((which == 0) != want_a) continue;
-    const int l = x[sl.m] - sl.h_lo;
-    if (l < 0 || l >= sl.n) continue;
-    const T ph = sl.psi_h[which][psi_index(sl, L, i, j, k, l)] + (which == 0 ? cb : -cb) * lam;
-    v += sl.a_h[l] * ph;
-  }
-  return v;
+  adj_h_comp<T, 0>(p, row, i, j, k, id, main_rng);
+  adj_h_comp<T, 1>(p, row, i, j, k, id, main_rng);
+  adj_h_comp<T, 2>(p, row, i, j, k, id, main_rng);
 }
 
-// Reverse H sweep.  For H_q at y (r1 = q+1, r2 = q+2): H_q is the d_a
-// operand of E_r1 (differenced along r2) and the d_b operand of E_r2
-// (differenced along r1) in the forward E update.
+// Reverse E sweep outside the box (one thread per node).
 template <typename T>
-__global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ YeeP<T> a,
-                                               const __grid_constant__ OvBoxD<T> ov) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ MarchP<T> p,
+                                               const __grid_constant__ AdjBox box) {
+  if (cta_in_adj_box(box)) return;
+  const int k = box.org_k + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = box.org_j + (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int i = blockIdx.z;
-  const Lat& L = a.L;
-  if (k > L.nz || j > L.ny || i > L.nx) return;
-  const int x[3] = {i, j, k};
-  const int n[3] = {L.nx, L.ny, L.nz};
+  const Lat& L = p.L;
+  if (k < 0 || j < 0 || k > L.nz || j > L.ny || i > L.nx || in_adj_box(box, i, j, k)) return;
   const long long id = lat_index(L, i, j, k);
-  const T* row = a.tab + (size_t)a.cls[id] * 12;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    bool valid = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) valid = valid && ((d == q) ? (x[d] <= n[d]) : (x[d] < n[d]));
-    if (!valid) continue;
-    T* Lq = a.f[3 + q];
-    const T lam = Lq[id];
-    const T ca = row[6 + 2 * q], cb = row[7 + 2 * q];
-    for (int s = 0; s < a.n_slab; ++s) {
-      const SlabD<T>& sl = a.slab[s];
-      if (sl.m == q) continue;
-      const int l = x[sl.m] - sl.h_lo;
-      if (l < 0 || l >= sl.n) continue;
-      const int which = (q == (sl.m + 1) % 3) ? 0 : 1;
-      T* ps = sl.psi_h[which] + psi_index(sl, L, i, j, k, l);
-      *ps = sl.b_h[l] * (*ps + (which == 0 ? cb : -cb) * lam);
-    }
-    const int r1 = (q + 1) % 3, r2 = (q + 2) % 3;
-    int y1[3] = {i, j, k}, y2[3] = {i, j, k};
-    y1[r2] += 1;  // the E_r1 node that reads H_q[y] as H_q[x - e_r2]
-    y2[r1] += 1;  // the E_r2 node that reads H_q[y] as H_q[x - e_r1]
-    const bool main_rng = (i < L.nx) && (j < L.ny) && (k < L.nz);
-    T v = main_rng ? ca * lam : lam;
-    v += e_diff_adj(a, ov, i, j, k, r1, true) - e_diff_adj(a, ov, y1[0], y1[1], y1[2], r1, true);
-    v += e_diff_adj(a, ov, i, j, k, r2, false) - e_diff_adj(a, ov, y2[0], y2[1], y2[2], r2, false);
-    Lq[id] = v;
-  }
-}
-
-// Reverse E sweep.  For E_q at x (r1 = q+1, r2 = q+2): E_q is the d_a
-// operand of H_r2 (differenced along r1) and the d_b operand of H_r1
-// (differenced along r2) in the forward H update.
-template <typename T>
-__global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ YeeP<T> a,
-                                               const __grid_constant__ OvBoxD<T> ov) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  const Lat& L = a.L;
-  if (k > L.nz || j > L.ny || i > L.nx) return;
-  const int x[3] = {i, j, k};
-  const int n[3] = {L.nx, L.ny, L.nz};
-  const long long id = lat_index(L, i, j, k);
-  const T* row = a.tab + (size_t)a.cls[id] * 12;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    bool valid = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) valid = valid && ((d == q) ? (x[d] < n[d]) : (x[d] <= n[d]));
-    if (!valid) continue;
-    T* Lq = a.f[q];
-    const T lam = Lq[id];
-    T ca, cb;
-    e_coeff(ov, row, q, i, j, k, ca, cb);
-    for (int s = 0; s < a.n_slab; ++s) {
-      const SlabD<T>& sl = a.slab[s];
-      if (sl.m == q) continue;
-      const int l = x[sl.m] - sl.e_lo;
-      if (l < 0 || l >= sl.n) continue;
-      const int which = (q == (sl.m + 1) % 3) ? 0 : 1;
-      T* ps = sl.psi_e[which] + psi_index(sl, L, i, j, k, l);
-      *ps = sl.b_e[l] * (*ps + (which == 0 ? -cb : cb) * lam);
-    }
-    const int r1 = (q + 1) % 3, r2 = (q + 2) % 3;
-    int y1[3] = {i, j, k}, y2[3] = {i, j, k};
-    y1[r1] -= 1;  // the H_r2 node that reads E_q[x] as E_q[y + e_r1]
-    y2[r2] -= 1;  // the H_r1 node that reads E_q[x] as E_q[y + e_r2]
-    const bool main_rng = x[r1] >= 1 && x[r1] < n[r1] && x[r2] >= 1 && x[r2] < n[r2];
-    T v = main_rng ? ca * lam : lam;
-    v += h_diff_adj(a, y1[0], y1[1], y1[2], r2, true) - h_diff_adj(a, i, j, k, r2, true);
-    v += h_diff_adj(a, y2[0], y2[1], y2[2], r1, false) - h_diff_adj(a, i, j, k, r1, false);
-    Lq[id] = v;
-  }
+  const T* row = p.tab + (size_t)p.cls[id] * 12;
+  adj_e_comp<T, 0>(p, row, i, j, k, id);
+  adj_e_comp<T, 1>(p, row, i, j, k, id);
+  adj_e_comp<T, 2>(p, row, i, j, k, id);
 }
 
 // A node box of the lattice and some of its field components, copied into
@@ -269,10 +287,11 @@ __global__ void k_box_record(BoxRecD<T> r, Lat L, T* const* fields, const long l
 }
 
 // Sensitivity sums over the design box: for E component c at node x,
-// G0 += lam_c(x) E_c^{m-1}(x) and G1 += lam_c(x) E_c^m(x), with E^{m-1},
-// E^m rows slot-1, slot of the recorded history (3 x n per row), in FP64.
+// G0 += lam_c(x) E_c^{m-1}(x) and G1 += lam_c(x) E_c^m(x), lam = u / cb with
+// the node's own cb (override or class), E^{m-1}, E^m rows slot-1, slot of
+// the recorded history (3 x n per row), in FP64.
 template <typename T>
-__global__ void k_adj_sens(BoxRecD<T> r, Lat L, T* const* lam, const T* hist, int slot,
+__global__ void k_adj_sens(BoxRecD<T> r, YeeP<T> a, OvBoxD<T> ov, const T* hist, int slot,
                            double* g0, double* g1) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= r.n * 3) return;
@@ -280,21 +299,30 @@ __global__ void k_adj_sens(BoxRecD<T> r, Lat L, T* const* lam, const T* hist, in
   const long long p = q - (long long)c * r.n;
   int i, j, k;
   box_node(r.s, r.e, p, i, j, k);
-  const double l = (double)lam[c][lat_index(L, i, j, k)];
+  const int x[3] = {i, j, k};
+  const int nn[3] = {a.L.nx, a.L.ny, a.L.nz};
+  if (x[c] >= nn[c]) return;  // component out of range
+  const long long id = lat_index(a.L, i, j, k);
+  T ca, cb;
+  e_coeff(ov, a.tab + (size_t)a.cls[id] * 12, c, i, j, k, ca, cb);
+  const double l = (double)a.f[c][id] / (double)cb;
   g0[q] += l * (double)hist[((long long)(slot - 1) * 3 + c) * r.n + p];
   g1[q] += l * (double)hist[((long long)slot * 3 + c) * r.n + p];
 }
 
-// Adjoint source: lam_c(x) += d[p] over the objective box (one component).
+// Adjoint source: u_c(x) += cb(x) d[p] over the objective box (one
+// component), cb the node's own (override or class).
 template <typename T>
-__global__ void k_adj_source(BoxRecD<T> r, Lat L, T* const* lam, const double* d) {
+__global__ void k_adj_source(BoxRecD<T> r, YeeP<T> a, OvBoxD<T> ov, const double* d) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= r.n) return;
   int i, j, k;
   box_node(r.s, r.e, p, i, j, k);
-  T* f = lam[r.c0];
-  const long long id = lat_index(L, i, j, k);
-  f[id] = (T)((double)f[id] + d[p]);
+  const long long id = lat_index(a.L, i, j, k);
+  T ca, cb;
+  e_coeff(ov, a.tab + (size_t)a.cls[id] * 12, r.c0, i, j, k, ca, cb);
+  T* f = a.f[r.c0];
+  f[id] = (T)((double)f[id] + (double)cb * d[p]);
 }
 
 }  // namespace xfd

@@ -120,6 +120,69 @@ xfd_status adj_alloc(xfd_engine* e, AdjBuffers& B, void** out, size_t bytes) {
   return XFD_OK;
 }
 
+// Tiles of the split marching sweeps (k tiles of 32, j tiles of kMTJ, x
+// chunks of `ich` planes, the grid moved by shift[g] nodes) on which the
+// scaled reverse step is the forward step: every node of the tile and its
+// neighbours one node away lie in no CPML layer and strictly inside the
+// lattice (main update range of every component), and the curl factors fe,
+// fh are one value per axis there.  Per axis the shift (a multiple of 8
+// nodes along k) and the run of tiles that cover the most nodes; an empty
+// box when some axis has none.
+void adjoint_split(const xfd_engine* e, int ich, int lo[3], int hi[3], int shift[3]) {
+  const Lat& L = e->L;
+  const int size[3] = {32, kMTJ, ich};
+  const int n_nodes[3] = {L.nz + 1, L.ny + 1, L.nx + 1};
+  const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
+  // k shifts in steps of 8 nodes: every TMA x coordinate stays a multiple of
+  // 16 bytes for the field maps (4 or 8 bytes per value) and for the uint16
+  // class map alike.
+  const int step[3] = {8, 1, 1};
+  for (int g = 0; g < 3; ++g) {
+    const int m = axis_of[g];
+    const int n_cells = n_nodes[g] - 1;
+    lo[g] = hi[g] = shift[g] = 0;
+    int best_len = 0;
+    for (int sh = 0; sh < size[g]; sh += step[g]) {
+      const int nt = (n_nodes[g] - sh + size[g] - 1) / size[g];
+      auto ok = [&](int b) {
+        const int a0 = sh + b * size[g] - 1;
+        const int a1 = std::min(sh + (b + 1) * size[g], n_nodes[g]) - 1 + 1;
+        if (a0 < 1 || a1 > n_cells - 1) return false;
+        for (const auto& S : e->slabs) {
+          if (S.m != m) continue;
+          if (a0 < S.e_lo + S.n && S.e_lo <= a1) return false;
+          if (a0 < S.h_lo + S.n && S.h_lo <= a1) return false;
+        }
+        // One curl factor per axis: spacings computed as differences of
+        // node coordinates may differ in their last bits, so equal within
+        // 1e-12 relative (the forward sweep's destination weights then stand
+        // for the transpose's source weights, far below a step's rounding).
+        const double f = e->fe_h[m][(size_t)a0];
+        for (int x = a0; x <= a1; ++x)
+          if (std::fabs(e->fe_h[m][(size_t)x] - f) > 1e-12 * std::fabs(f) ||
+              std::fabs(e->fh_h[m][(size_t)x] - f) > 1e-12 * std::fabs(f))
+            return false;
+        return true;
+      };
+      for (int b = 0; b < nt;) {
+        if (!ok(b)) {
+          ++b;
+          continue;
+        }
+        int c = b;
+        while (c < nt && ok(c)) ++c;
+        if (c - b > best_len) {
+          best_len = c - b;
+          lo[g] = b;
+          hi[g] = c;
+          shift[g] = sh;
+        }
+        b = c;
+      }
+    }
+  }
+}
+
 bool box_ok(const Lat& L, const int32_t s[3], const int32_t t[3]) {
   const int n[3] = {L.nx, L.ny, L.nz};
   for (int a = 0; a < 3; ++a)
@@ -189,14 +252,23 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   CUDA_TRY(e, cudaMemcpyAsync(lamp, lam, sizeof lam, cudaMemcpyHostToDevice, st));
   YeeP<T> a = yee_params<T>(e);
   for (int c = 0; c < 6; ++c) a.f[c] = static_cast<T*>(lam[c]);
+  // The same scaled fields and CPML adjoints in the marching-sweep layout.
+  MarchP<T> ap = march_params<T>(e);
+  for (int c = 0; c < 6; ++c) ap.f[c] = static_cast<T*>(lam[c]);
+  int slot_of[3] = {0, 0, 0};
   for (size_t q = 0; q < e->slabs.size(); ++q) {
     const size_t b = slab_cells(e, e->slabs[q]) * e->wsize;
+    SlabAxisD<T>& A = ap.slab[e->slabs[q].m];
+    const int slot = slot_of[e->slabs[q].m]++;
     for (int w = 0; w < 2; ++w) {
       void *pe = nullptr, *ph = nullptr;
       if ((s = adj_alloc(e, B, &pe, b)) != XFD_OK) return s;
       if ((s = adj_alloc(e, B, &ph, b)) != XFD_OK) return s;
       a.slab[q].psi_e[w] = static_cast<T*>(pe);
       a.slab[q].psi_h[w] = static_cast<T*>(ph);
+      A.psi_e[slot][w] = static_cast<T*>(pe);
+      A.psi_h_in[slot][w] = static_cast<const T*>(ph);
+      A.psi_h_out[slot][w] = static_cast<T*>(ph);
     }
   }
   T* const* lam_dev = static_cast<T* const*>(lamp);
@@ -251,8 +323,31 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   set_rec<T>(e, 0, ro);
   e->n_rec = 1;
   e->graph_dirty = true;
+  // The design history of the last segment is recorded on the way, so that
+  // segment needs no recomputation.
+  BoxRecD<T> rd{};
+  for (int q = 0; q < 3; ++q) {
+    rd.s[q] = d->design_s[q];
+    rd.e[q] = d->design_e[q];
+  }
+  rd.c0 = 0;
+  rd.nc = 3;
+  rd.n = n_des;
+  rd.rows = K + 1;
+  rd.dst = static_cast<T*>(hist);
+  const unsigned db = blocks_for(3 * n_des, 256);
+  T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
   for (long long q = 0; q < S; ++q) {
     if ((s = ckpt_save(e, B.ck[(size_t)q])) != XFD_OK) break;
+    if (q == S - 1) {
+      rd.base = t0 + q * K;
+      rd.shift = 0;
+      k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
+      rd.shift = 1;
+      set_rec<T>(e, 1, rd);
+      e->n_rec = 2;
+      e->graph_dirty = true;
+    }
     if ((s = xfd_run(e, std::min(K, N - q * K))) != XFD_OK) break;
   }
   e->n_rec = 0;
@@ -273,49 +368,75 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   CUDA_TRY(e, cudaMemcpyAsync(src, drec.data(), drec.size() * sizeof(double),
                               cudaMemcpyHostToDevice, st));
 
-  // Reverse.
-  BoxRecD<T> rd{};
-  for (int q = 0; q < 3; ++q) {
-    rd.s[q] = d->design_s[q];
-    rd.e[q] = d->design_e[q];
-  }
-  rd.c0 = 0;
-  rd.nc = 3;
-  rd.n = n_des;
-  rd.rows = K + 1;
-  rd.dst = static_cast<T*>(hist);
+  // Reverse, on the scaled fields (adjoint.cuh): the CPML-free box with
+  // uniform curl factors by the forward marching sweeps over tensor maps of
+  // the adjoint arrays, the rest by the transpose-gather kernels.
   BoxRecD<T> rs = ro;
   const double* srcd = static_cast<const double*>(src);
   double* g0 = static_cast<double*>(g);
   double* g1 = g0 + 3 * n_des;
+  const unsigned sb = blocks_for(n_obj, 256);
+  AdjBox abox{};
+  const int ich = e->march_ichunk;
+  int alo[3], ahi[3], ash[3];
+  adjoint_split(e, ich, alo, ahi, ash);
+  const bool has_box = ahi[0] > alo[0] && ahi[1] > alo[1] && ahi[2] > alo[2];
+  MarchTmaP<T> am{};
+  if (has_box) {
+    const int size[3] = {32, kMTJ, ich};
+    for (int q = 0; q < 3; ++q) {
+      abox.lo[q] = ash[q] + alo[q] * size[q];
+      abox.hi[q] = ash[q] + ahi[q] * size[q];
+      am.org[q] = alo[q];
+      am.box_lo[q] = alo[q];
+      am.box_hi[q] = ahi[q];
+      am.shift[q] = ash[q];
+    }
+    abox.org_k = ash[0] % 32 ? ash[0] % 32 - 32 : 0;
+    abox.org_j = ash[1] % kMTJ ? ash[1] % kMTJ - kMTJ : 0;
+    am.p = ap;
+    if ((s = build_march_maps<T>(e, lam, &am.m)) != XFD_OK) return s;
+    am.err = e->d_err;
+  }
+  static_assert(kMTJ == 8, "the gather CTAs are 32 x 8 nodes, the box tiles 32 x kMTJ");
   const dim3 blk(32, 8, 1);
-  const dim3 grd((unsigned)((L.nz + 1 + 31) / 32), (unsigned)((L.ny + 1 + 7) / 8),
-                 (unsigned)(L.nx + 1));
-  const unsigned sb = blocks_for(n_obj, 256), db = blocks_for(3 * n_des, 256);
-  T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
-  k_adj_source<T><<<sb, 256, 0, st>>>(rs, L, lam_dev, srcd + (N - 1) * n_obj);  // dJ/dE^N
+  const dim3 grd((unsigned)((L.nz + 1 - abox.org_k + 31) / 32),
+                 (unsigned)((L.ny + 1 - abox.org_j + 7) / 8), (unsigned)(L.nx + 1));
+  constexpr int MF = march_free_stages<T>();
+  const size_t msm_free = MarchGeom<T, kMTJ, 32>::smem(MF);
+  const dim3 gbox((unsigned)(ahi[0] - alo[0]), (unsigned)(ahi[1] - alo[1]),
+                  (unsigned)(ahi[2] - alo[2]));
+  const dim3 blk_m(32, kMTJ, 1);
+  const OverrideD<T> ovd = ovr_of<T>(e);
+  k_adj_source<T><<<sb, 256, 0, st>>>(rs, a, ov, srcd + (N - 1) * n_obj);  // dJ/dE^N
   for (long long q = S - 1; q >= 0; --q) {
     const long long base = t0 + q * K, len = std::min(K, N - q * K);
-    if ((s = state_copy(e, B.ck[(size_t)q], false)) != XFD_OK) return s;
-    rd.base = base;
-    rd.shift = 0;
-    k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
-    rd.shift = 1;
-    set_rec<T>(e, 0, rd);
-    e->n_rec = 1;
-    e->graph_dirty = true;
-    s = xfd_run(e, len);
-    e->n_rec = 0;
-    e->graph_dirty = true;
-    if (s != XFD_OK) return s;
+    if (q < S - 1) {  // recompute the segment, recording the design history
+      if ((s = state_copy(e, B.ck[(size_t)q], false)) != XFD_OK) return s;
+      rd.base = base;
+      rd.shift = 0;
+      k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
+      rd.shift = 1;
+      set_rec<T>(e, 0, rd);
+      e->n_rec = 1;
+      e->graph_dirty = true;
+      s = xfd_run(e, len);
+      e->n_rec = 0;
+      e->graph_dirty = true;
+      if (s != XFD_OK) return s;
+    }
     for (long long m = len; m >= 1; --m) {
-      const long long gstep = q * K + m;  // lam holds dJ/dE^gstep
-      k_adj_h<T><<<grd, blk, 0, st>>>(a, ov);
-      k_adj_sens<T><<<db, 256, 0, st>>>(rd, L, lam_dev, static_cast<const T*>(hist), (int)m, g0,
-                                        g1);
-      k_adj_e<T><<<grd, blk, 0, st>>>(a, ov);
+      const long long gstep = q * K + m;  // u holds cb dJ/dE^gstep
+      if (has_box) k_march_h_tma<T, kMTJ, 32, MF, false, true><<<gbox, blk_m, msm_free, st>>>(am);
+      k_adj_h<T><<<grd, blk, 0, st>>>(ap, abox);
+      k_adj_sens<T><<<db, 256, 0, st>>>(rd, a, ov, static_cast<const T*>(hist), (int)m, g0, g1);
+      if (e->n_ovr) k_ovr_gather<T><<<blocks_for(e->n_ovr, 256), 256, 0, st>>>(ovd, lam_dev);
+      if (has_box) k_march_e_tma<T, kMTJ, 32, MF, false, true><<<gbox, blk_m, msm_free, st>>>(am);
+      k_adj_e<T><<<grd, blk, 0, st>>>(ap, abox);
+      if (e->n_ovr)
+        k_ovr_apply<T><<<blocks_for(e->n_ovr, 256), 256, 0, st>>>(ovd, lam_dev, nullptr);
       if (gstep - 1 >= 1)
-        k_adj_source<T><<<sb, 256, 0, st>>>(rs, L, lam_dev, srcd + (gstep - 2) * n_obj);
+        k_adj_source<T><<<sb, 256, 0, st>>>(rs, a, ov, srcd + (gstep - 2) * n_obj);
     }
     CUDA_TRY(e, cudaGetLastError());
   }
@@ -381,6 +502,8 @@ xfd_status xfd_adjoint_run(xfd_engine* e, const xfd_adjoint_desc* d, double* val
                 "the adjoint covers CPML, TFSF and lumped sources; not ADE media, NF2FF or movies");
   CUDA_TRY(e, cudaSetDevice(e->device));
   xfd_status s = ensure_ready(e);
+  if (s == XFD_OK && !e->tma_ready)
+    s = e->precision == XFD_FP64 ? build_tma_maps<double>(e) : build_tma_maps<float>(e);
   if (s != XFD_OK) return s;
   return e->precision == XFD_FP64 ? adjoint_run_t<double>(e, d, value, sens)
                                   : adjoint_run_t<float>(e, d, value, sens);

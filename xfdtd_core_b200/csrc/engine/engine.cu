@@ -70,6 +70,7 @@ struct xfd_engine {
   int n_classes = 0;
   void* fe[3] = {};
   void* fh[3] = {};
+  std::vector<double> fe_h[3], fh_h[3];  // host copies (fh padded to n+1)
   bool have_classes = false, have_curl = false;
 
   struct Slab {
@@ -324,9 +325,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 // Tensor maps for the pipelined sweep: one per field component and buffer
 // (3-D: k, j, i over the logical lattice extent so out-of-range boxes read
 // zeros) and one for the class index.
-template <typename T>
-xfd_status build_tma_maps(xfd_engine* e) {
-  using G = TmaGeom<T, kTJ, kTK>;
+xfd_status tensor_map_encoder(xfd_engine* e, EncodeTiledFn* out) {
   static EncodeTiledFn encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -335,6 +334,40 @@ xfd_status build_tma_maps(xfd_engine* e) {
     if (!fn || q != cudaDriverEntryPointSuccess)
       return fail(e, XFD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     encode = reinterpret_cast<EncodeTiledFn>(fn);
+  }
+  *out = encode;
+  return XFD_OK;
+}
+
+// Tensor maps of the marching sweeps over six field arrays of the lattice
+// layout (the engine's buffers, or the adjoint's scaled fields).
+template <typename T>
+xfd_status build_march_maps(xfd_engine* e, void* const f[6], MarchMaps* m) {
+  EncodeTiledFn encode = nullptr;
+  xfd_status st = tensor_map_encoder(e, &encode);
+  if (st != XFD_OK) return st;
+  using MG = MarchGeom<T, kMTJ, 32>;
+  const CUtensorMapDataType dt =
+      sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  for (int c = 0; c < 6; ++c) {
+    CUresult r = encode_lattice(encode, &m->halo[c], dt, sizeof(T), f[c], e->L, MG::W, MG::R);
+    if (r == CUDA_SUCCESS)
+      r = encode_lattice(encode, &m->tile[c], dt, sizeof(T), f[c], e->L, 32, kMTJ);
+    if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march %d): %d", c, (int)r);
+  }
+  CUresult r = encode_lattice(encode, &m->cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, e->cls, e->L, 32,
+                              kMTJ);
+  if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march class): %d", (int)r);
+  return XFD_OK;
+}
+
+template <typename T>
+xfd_status build_tma_maps(xfd_engine* e) {
+  using G = TmaGeom<T, kTJ, kTK>;
+  EncodeTiledFn encode = nullptr;
+  {
+    xfd_status st = tensor_map_encoder(e, &encode);
+    if (st != XFD_OK) return st;
   }
   const Lat& L = e->L;
   const cuuint64_t dims[3] = {(cuuint64_t)L.nz + 1, (cuuint64_t)L.ny + 1, (cuuint64_t)L.nx + 1};
@@ -362,16 +395,8 @@ xfd_status build_tma_maps(xfd_engine* e) {
   // Marching sweeps: halo and tile boxes of every component, class tiles.
   using MG = MarchGeom<T, kMTJ, 32>;
   for (int b = 0; b < 2; ++b) {
-    for (int c = 0; c < 6; ++c) {
-      CUresult r = encode_lattice(encode, &e->mtma[b].halo[c], dt, sizeof(T), e->fbuf[b][c], L,
-                                  MG::W, MG::R);
-      if (r == CUDA_SUCCESS)
-        r = encode_lattice(encode, &e->mtma[b].tile[c], dt, sizeof(T), e->fbuf[b][c], L, 32, kMTJ);
-      if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march %d): %d", c, (int)r);
-    }
-    CUresult r = encode_lattice(encode, &e->mtma[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, e->cls,
-                                L, 32, kMTJ);
-    if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march class): %d", (int)r);
+    xfd_status st = build_march_maps<T>(e, e->fbuf[b], &e->mtma[b]);
+    if (st != XFD_OK) return st;
   }
   // Fused marching sweep: E (TJ+1 rows) and H (TJ rows) boxes of width
   // 32 elements + 16 bytes, class boxes of 40.
@@ -1176,6 +1201,8 @@ xfd_status xfd_set_curl_factors(xfd_engine* e, const double* const fe[3],
     if (s != XFD_OK) return s;
     s = upload_real(e, &e->fh[a], hh.data(), hh.size());
     if (s != XFD_OK) return s;
+    e->fe_h[a] = he;
+    e->fh_h[a] = hh;
   }
   e->have_curl = true;
   e->graph_dirty = true;

@@ -50,6 +50,11 @@ struct MarchMaps {
 // IN = true (CP = false only) is for a box away from every lattice boundary:
 // all nodes of its tiles have every component in range and the full main
 // update, so the form carries no range tests.
+// `shift` moves the tile grid by whole nodes (k by a multiple of 8 nodes, so
+// that every TMA x coordinate -- field values and the uint16 class index --
+// stays a multiple of 16 bytes): tile (x, y, z) starts at node
+// (shift[0] + 32 x, shift[1] + TJ y, shift[2] + ichunk z).  Zero for the time
+// step; the adjoint's reverse sweeps use it to fit their box to the CPML.
 template <typename T>
 struct MarchTmaP {
   MarchP<T> p;
@@ -57,6 +62,7 @@ struct MarchTmaP {
   int* err;
   int org[3];
   int box_lo[3], box_hi[3];
+  int shift[3];
 };
 
 template <typename T, int TJ, int TK>
@@ -152,9 +158,9 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
     return;  // swept by the CPML-free form
   // One thread reads the error word, so that the whole CTA returns or none.
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
-  const int k0 = gx * TK, j0 = gy * TJ;
+  const int k0 = gx * TK + P.shift[0], j0 = gy * TJ + P.shift[1];
   const int k = k0 + tk, j = j0 + tj;
-  const int i_lo = gz * p.ichunk;
+  const int i_lo = gz * p.ichunk + P.shift[2];
   const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
   const int n_planes = i_hi - i_lo;
   const int n_staged = n_planes + (i_hi <= L.nx ? 1 : 0);
@@ -354,9 +360,9 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
     return;  // swept by the CPML-free form
   // One thread reads the error word, so that the whole CTA returns or none.
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
-  const int k0 = gx * TK, j0 = gy * TJ;
+  const int k0 = gx * TK + P.shift[0], j0 = gy * TJ + P.shift[1];
   const int k = k0 + tk, j = j0 + tj;
-  const int i_lo = gz * p.ichunk;
+  const int i_lo = gz * p.ichunk + P.shift[2];
   const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
   const int n_planes = i_hi - i_lo;
   const int q_first = i_lo >= 1 ? -1 : 0;  // first staged plane
