@@ -171,24 +171,32 @@ __device__ __forceinline__ void psi_adj(const MarchP<T>& p, int i, int j, int k,
 
 // H_Q at y (R1 = Q+1, R2 = Q+2) is the d_a operand of E_R1 (differenced
 // along R2) and the d_b operand of E_R2 (differenced along R1) in the forward
-// E update.  Completes the previous reverse step's H adjoint first.
+// E update.  The gather (loads only) is split from the update (stores), so
+// that a node's three components read before any of them is written.
 template <typename T, int Q>
-__device__ __forceinline__ void adj_h_comp(const MarchP<T>& p, const T* row, int i, int j, int k,
-                                           long long id, bool main_rng) {
+__device__ __forceinline__ bool adj_h_gather(const MarchP<T>& p, int i, int j, int k, long long id,
+                                             T& w, T& sum) {
   constexpr int R1 = (Q + 1) % 3, R2 = (Q + 2) % 3;
   const Lat& L = p.L;
   if (pick<R1>(i, j, k) >= pick<R1>(L.nx, L.ny, L.nz) ||
       pick<R2>(i, j, k) >= pick<R2>(L.nx, L.ny, L.nz))
-    return;  // H_Q out of range
-  T* Wq = p.f[3 + Q];
-  const T w = Wq[id];
+    return false;  // H_Q out of range
+  w = p.f[3 + Q][id];
+  sum = x_term<T, R1, true>(p, i, j, k) -
+        x_term<T, R1, true>(p, i + (R2 == 0), j + (R2 == 1), k + (R2 == 2)) +
+        x_term<T, R2, false>(p, i, j, k) -
+        x_term<T, R2, false>(p, i + (R1 == 0), j + (R1 == 1), k + (R1 == 2));
+  return true;
+}
+
+// Completes the previous reverse step's H adjoint (psi) and writes H_Q.
+template <typename T, int Q>
+__device__ __forceinline__ void adj_h_update(const MarchP<T>& p, const T* row, int i, int j, int k,
+                                             long long id, bool main_rng, T w, T sum) {
+  constexpr int R1 = (Q + 1) % 3, R2 = (Q + 2) % 3;
   psi_adj<T, Q, R1, false>(p, i, j, k, w);
   psi_adj<T, Q, R2, false>(p, i, j, k, w);
-  const T sum = x_term<T, R1, true>(p, i, j, k) -
-                x_term<T, R1, true>(p, i + (R2 == 0), j + (R2 == 1), k + (R2 == 2)) +
-                x_term<T, R2, false>(p, i, j, k) -
-                x_term<T, R2, false>(p, i + (R1 == 0), j + (R1 == 1), k + (R1 == 2));
-  Wq[id] = (main_rng ? row[6 + 2 * Q] * w : w) - row[7 + 2 * Q] * sum;
+  p.f[3 + Q][id] = (main_rng ? row[6 + 2 * Q] * w : w) - row[7 + 2 * Q] * sum;
 }
 
 // E_Q at x (R1 = Q+1, R2 = Q+2) is the d_a operand of H_R2 (differenced
@@ -196,23 +204,30 @@ __device__ __forceinline__ void adj_h_comp(const MarchP<T>& p, const T* row, int
 // H update.  Nodes with a coefficient override take the class pair here and
 // the override fix-up afterwards, as in the forward step.
 template <typename T, int Q>
-__device__ __forceinline__ void adj_e_comp(const MarchP<T>& p, const T* row, int i, int j, int k,
-                                           long long id) {
+__device__ __forceinline__ bool adj_e_gather(const MarchP<T>& p, int i, int j, int k, long long id,
+                                             T& u, T& sum) {
   constexpr int R1 = (Q + 1) % 3, R2 = (Q + 2) % 3;
   const Lat& L = p.L;
-  if (pick<Q>(i, j, k) >= pick<Q>(L.nx, L.ny, L.nz)) return;  // E_Q out of range
-  T* Uq = p.f[Q];
-  const T u = Uq[id];
+  if (pick<Q>(i, j, k) >= pick<Q>(L.nx, L.ny, L.nz)) return false;  // E_Q out of range
+  u = p.f[Q][id];
+  sum = y_term<T, R2, true>(p, i - (R1 == 0), j - (R1 == 1), k - (R1 == 2)) -
+        y_term<T, R2, true>(p, i, j, k) +
+        y_term<T, R1, false>(p, i - (R2 == 0), j - (R2 == 1), k - (R2 == 2)) -
+        y_term<T, R1, false>(p, i, j, k);
+  return true;
+}
+
+template <typename T, int Q>
+__device__ __forceinline__ void adj_e_update(const MarchP<T>& p, const T* row, int i, int j, int k,
+                                             long long id, T u, T sum) {
+  constexpr int R1 = (Q + 1) % 3, R2 = (Q + 2) % 3;
+  const Lat& L = p.L;
   psi_adj<T, Q, R1, true>(p, i, j, k, u);
   psi_adj<T, Q, R2, true>(p, i, j, k, u);
   const int x1 = pick<R1>(i, j, k), x2 = pick<R2>(i, j, k);
   const bool main_rng = x1 >= 1 && x1 < pick<R1>(L.nx, L.ny, L.nz) && x2 >= 1 &&
                         x2 < pick<R2>(L.nx, L.ny, L.nz);
-  const T sum = y_term<T, R2, true>(p, i - (R1 == 0), j - (R1 == 1), k - (R1 == 2)) -
-                y_term<T, R2, true>(p, i, j, k) +
-                y_term<T, R1, false>(p, i - (R2 == 0), j - (R2 == 1), k - (R2 == 2)) -
-                y_term<T, R1, false>(p, i, j, k);
-  Uq[id] = (main_rng ? row[2 * Q] * u : u) + row[2 * Q + 1] * sum;
+  p.f[Q][id] = (main_rng ? row[2 * Q] * u : u) + row[2 * Q + 1] * sum;
 }
 
 // Reverse H sweep outside the box (one thread per node).
@@ -228,9 +243,13 @@ __global__ void __launch_bounds__(256) k_adj_h(const __grid_constant__ MarchP<T>
   const long long id = lat_index(L, i, j, k);
   const T* row = p.tab + (size_t)p.cls[id] * 12;
   const bool main_rng = (i < L.nx) && (j < L.ny) && (k < L.nz);
-  adj_h_comp<T, 0>(p, row, i, j, k, id, main_rng);
-  adj_h_comp<T, 1>(p, row, i, j, k, id, main_rng);
-  adj_h_comp<T, 2>(p, row, i, j, k, id, main_rng);
+  T w0, w1, w2, s0, s1, s2;
+  const bool v0 = adj_h_gather<T, 0>(p, i, j, k, id, w0, s0);
+  const bool v1 = adj_h_gather<T, 1>(p, i, j, k, id, w1, s1);
+  const bool v2 = adj_h_gather<T, 2>(p, i, j, k, id, w2, s2);
+  if (v0) adj_h_update<T, 0>(p, row, i, j, k, id, main_rng, w0, s0);
+  if (v1) adj_h_update<T, 1>(p, row, i, j, k, id, main_rng, w1, s1);
+  if (v2) adj_h_update<T, 2>(p, row, i, j, k, id, main_rng, w2, s2);
 }
 
 // Reverse E sweep outside the box (one thread per node).
@@ -245,9 +264,13 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ MarchP<T>
   if (k < 0 || j < 0 || k > L.nz || j > L.ny || i > L.nx || in_adj_box(box, i, j, k)) return;
   const long long id = lat_index(L, i, j, k);
   const T* row = p.tab + (size_t)p.cls[id] * 12;
-  adj_e_comp<T, 0>(p, row, i, j, k, id);
-  adj_e_comp<T, 1>(p, row, i, j, k, id);
-  adj_e_comp<T, 2>(p, row, i, j, k, id);
+  T u0, u1, u2, s0, s1, s2;
+  const bool v0 = adj_e_gather<T, 0>(p, i, j, k, id, u0, s0);
+  const bool v1 = adj_e_gather<T, 1>(p, i, j, k, id, u1, s1);
+  const bool v2 = adj_e_gather<T, 2>(p, i, j, k, id, u2, s2);
+  if (v0) adj_e_update<T, 0>(p, row, i, j, k, id, u0, s0);
+  if (v1) adj_e_update<T, 1>(p, row, i, j, k, id, u1, s1);
+  if (v2) adj_e_update<T, 2>(p, row, i, j, k, id, u2, s2);
 }
 
 // A node box of the lattice and some of its field components, copied into

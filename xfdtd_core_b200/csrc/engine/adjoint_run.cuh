@@ -98,25 +98,37 @@ void ckpt_free(xfd_engine::Ckpt& c) {
   c = xfd_engine::Ckpt{};
 }
 
-// Device buffers of one adjoint run, freed on every exit path.
+// Device buffers of an adjoint run, taken in a fixed order from the
+// engine's kept buffers (reused while the size matches, else reallocated)
+// and zeroed on the run's stream.
 struct AdjBuffers {
-  std::vector<void*> p;
-  std::vector<xfd_engine::Ckpt> ck;
-  ~AdjBuffers() {
-    for (void* q : p) cudaFree(q);
-    for (auto& c : ck) ckpt_free(c);
-  }
+  xfd_engine* e;
+  size_t next = 0;
 };
 
 xfd_status adj_alloc(xfd_engine* e, AdjBuffers& B, void** out, size_t bytes) {
-  cudaError_t r = cudaMalloc(out, std::max<size_t>(bytes, 16));
-  if (r != cudaSuccess) {
-    *out = nullptr;
-    return fail(e, r == cudaErrorMemoryAllocation ? XFD_ERR_OUT_OF_MEMORY : XFD_ERR_CUDA,
-                "adjoint cudaMalloc(%zu): %s", bytes, cudaGetErrorString(r));
+  bytes = std::max<size_t>(bytes, 16);
+  if (B.next < e->adj_bufs.size() && e->adj_sizes[B.next] != bytes) {
+    CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+    cudaFree(e->adj_bufs[B.next]);
+    e->adj_bufs[B.next] = nullptr;
   }
-  B.p.push_back(*out);
-  CUDA_TRY(e, cudaMemsetAsync(*out, 0, std::max<size_t>(bytes, 16), e->stream));
+  if (B.next >= e->adj_bufs.size()) {
+    e->adj_bufs.push_back(nullptr);
+    e->adj_sizes.push_back(0);
+  }
+  if (!e->adj_bufs[B.next]) {
+    cudaError_t r = cudaMalloc(&e->adj_bufs[B.next], bytes);
+    if (r != cudaSuccess) {
+      e->adj_bufs[B.next] = nullptr;
+      *out = nullptr;
+      return fail(e, r == cudaErrorMemoryAllocation ? XFD_ERR_OUT_OF_MEMORY : XFD_ERR_CUDA,
+                  "adjoint cudaMalloc(%zu): %s", bytes, cudaGetErrorString(r));
+    }
+    e->adj_sizes[B.next] = bytes;
+  }
+  *out = e->adj_bufs[B.next++];
+  CUDA_TRY(e, cudaMemsetAsync(*out, 0, bytes, e->stream));
   return XFD_OK;
 }
 
@@ -208,7 +220,7 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   const long long n_obj = box_nodes(d->obj_s, d->obj_e);
   const long long n_des = box_nodes(d->design_s, d->design_e);
   cudaStream_t st = e->stream;
-  AdjBuffers B;
+  AdjBuffers B{e};
   xfd_status s;
   void *rec = nullptr, *hist = nullptr, *src = nullptr, *g = nullptr, *lamp = nullptr;
   if ((s = adj_alloc(e, B, &rec, (size_t)N * n_obj * sizeof(T))) != XFD_OK) return s;
@@ -272,7 +284,8 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
     }
   }
   T* const* lam_dev = static_cast<T* const*>(lamp);
-  B.ck.resize((size_t)S + 1);
+  if (e->adj_ck.size() < (size_t)S + 1) e->adj_ck.resize((size_t)S + 1);
+  std::vector<xfd_engine::Ckpt>& ck = e->adj_ck;
   // Coefficient overrides as dense arrays over their bounding node box.
   OvBoxD<T> ov{};
   if (e->n_ovr) {
@@ -338,7 +351,7 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   const unsigned db = blocks_for(3 * n_des, 256);
   T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
   for (long long q = 0; q < S; ++q) {
-    if ((s = ckpt_save(e, B.ck[(size_t)q])) != XFD_OK) break;
+    if ((s = ckpt_save(e, ck[(size_t)q])) != XFD_OK) break;
     if (q == S - 1) {
       rd.base = t0 + q * K;
       rd.shift = 0;
@@ -353,7 +366,7 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   e->n_rec = 0;
   e->graph_dirty = true;
   if (s != XFD_OK) return s;
-  if ((s = ckpt_save(e, B.ck[(size_t)S])) != XFD_OK) return s;
+  if ((s = ckpt_save(e, ck[(size_t)S])) != XFD_OK) return s;
 
   // Objective on the host.
   std::vector<T> rec_h((size_t)(N * n_obj));
@@ -412,7 +425,7 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   for (long long q = S - 1; q >= 0; --q) {
     const long long base = t0 + q * K, len = std::min(K, N - q * K);
     if (q < S - 1) {  // recompute the segment, recording the design history
-      if ((s = state_copy(e, B.ck[(size_t)q], false)) != XFD_OK) return s;
+      if ((s = state_copy(e, ck[(size_t)q], false)) != XFD_OK) return s;
       rd.base = base;
       rd.shift = 0;
       k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
@@ -440,7 +453,7 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
     }
     CUDA_TRY(e, cudaGetLastError());
   }
-  if ((s = state_copy(e, B.ck[(size_t)S], false)) != XFD_OK) return s;
+  if ((s = state_copy(e, ck[(size_t)S], false)) != XFD_OK) return s;
   CUDA_TRY(e, cudaMemcpyAsync(sens, g, (size_t)6 * n_des * sizeof(double), cudaMemcpyDeviceToHost,
                               st));
   CUDA_TRY(e, cudaStreamSynchronize(st));

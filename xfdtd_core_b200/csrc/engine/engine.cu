@@ -146,6 +146,11 @@ struct xfd_engine {
     int64_t step = -1;
   };
   std::vector<Ckpt> ckpts;
+  // Device buffers and saved states of the last adjoint run, kept for the
+  // next run (reused in allocation order while the sizes match).
+  std::vector<void*> adj_bufs;
+  std::vector<size_t> adj_sizes;
+  std::vector<Ckpt> adj_ck;
   // Per-step node-box records of the adjoint (objective field, design
   // history), launched after the record phase of each step.
   BoxRecD<double> rec64[2]{};
@@ -1064,6 +1069,9 @@ void xfd_destroy(xfd_engine* e) {
   drop_graph(e);
   for (auto& c : e->ckpts)
     if (c.buf) cudaFree(c.buf);
+  for (auto& c : e->adj_ck)
+    if (c.buf) cudaFree(c.buf);
+  for (void* p : e->adj_bufs) cudaFree(p);
   for (void* p : e->allocs) cudaFree(p);
   for (void* p : e->host_allocs) cudaFreeHost(p);
   if (e->copy_ev) cudaEventDestroy(e->copy_ev);
