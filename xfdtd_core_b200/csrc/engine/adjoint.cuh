@@ -16,18 +16,23 @@
 //     psi' = b_e psi + a_e d   (slab along tb: d = d_b, "which" 0, sign -;
 //                               slab along ta: d = d_a, "which" 1, sign +)
 //     E' = [M ? ca : 1] E + cb (M fe[ta] d_a - M fe[tb] d_b) + cb (-psi'_0 + psi'_1)
-// (M: the node is in the main update range.)  The adjoint variables lam
-// (fields, scaled as described below) and lam_psi (CPML) live in arrays of
-// the forward layout.  One reverse step m -> m-1 is two lattice sweeps:
-//   k_adj_h: per H node, lam_psi_h <- b_h (lam_psi_h + s cb lam_H);
-//            lam_H <- [M ? ca : 1] lam_H + (transposed E-update differences of lam_E)
-//   k_adj_e: per E node, lam_psi_e <- b_e (lam_psi_e + s cb lam_E);
-//            lam_E <- [M ? ca : 1] lam_E + (transposed H-update differences of lam_H)
+// (M: the node is in the main update range.)  One reverse step m -> m-1,
+// on adjoint variables lam (fields) and lam_psi (CPML) in arrays of the
+// forward layout, is two lattice sweeps:
+//   H: lam_psi_h <- b_h (lam_psi_h + s cb lam_H)  (the previous step's H part);
+//      lam_H <- [M ? ca : 1] lam_H + (transposed E-update differences of lam_E)
+//   E: lam_psi_e <- b_e (lam_psi_e + s cb lam_E);
+//      lam_E <- [M ? ca : 1] lam_E + (transposed H-update differences of lam_H)
 // where the transposed differences are gathered from the neighbour nodes
-// that read this node in the forward step (no atomics).  k_adj_h fuses the
-// self part of the previous reverse step's H adjoint with this step's
-// gather, so both sweeps read their neighbours' values as the exact
-// transpose requires.
+// that read this node in the forward step (no atomics), each sweep reading
+// its neighbours' values before the other sweep changes them, as the exact
+// transpose requires.  The fields are held scaled, u = cb lam_E and
+// w = -cb lam_H: in those variables the reverse step is node for node the
+// forward step with the same (ca, cb), so on a box with no CPML and one curl
+// factor per axis the forward marching sweeps (march_tma.cuh) run it
+// unchanged, and the gather kernels here (k_adj_h, k_adj_e) do the exact
+// transpose on the shell around that box, without class lookups at
+// neighbour nodes.
 #pragma once
 
 #include "fused.cuh"
