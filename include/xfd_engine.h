@@ -214,6 +214,27 @@ typedef struct {
 xfd_status xfd_nf2ff_far_field(xfd_engine* e, const xfd_far_field_desc* d, double* out,
                                int64_t capacity);
 
+/* Time-domain NF2FF for one observation direction.  Per step and Huygens
+ * point (faces as in xfd_nf2ff_desc; points face by face XN..ZP, k fastest),
+ * the change since the previous step of the surface-centre tangential E and
+ * H, times the point's face-cell area ds, is added to the retarded-time bins
+ * nn, nn + 1 (linear weights) of six potentials, nn + f = delay + 1/2 + t for
+ * E and delay + t for H; delay = (the surface's largest projected distance -
+ * the point's) / (c dt), computed by the caller.  xfd_get_nf2ff_td returns
+ * the raw sums, 6 x n_bins doubles: W_x W_y W_z (from H) then U_x U_y U_z
+ * (from E).
+ * Replaces: NFFFTTimeDomain::update -> TDPlaneData::update
+ * (src/nffft/nfffft_time_domain.cpp:80-96, src/include/nffft/nffft_td_data.h:169-240). */
+typedef struct {
+  int32_t task_s[6][3], task_e[6][3];
+  const double* delay;  /* P values */
+  const double* ds;     /* P values */
+  int64_t n_bins;
+} xfd_nf2ff_td_desc;
+
+xfd_status xfd_set_nf2ff_td(xfd_engine* e, const xfd_nf2ff_td_desc* d);
+xfd_status xfd_get_nf2ff_td(xfd_engine* e, double* out, int64_t capacity, int64_t* count);
+
 /* Movie monitor: every `interval` steps (from step 0) the box [box_s, box_e)
  * of `field` is recorded into a device frame store.
  * Replaces: MovieMonitor::update -> FieldMonitor::output

@@ -540,6 +540,49 @@ class NFFFTFrequencyDomain {
   std::array<std::vector<Real>, 3> _node_e, _node_h, _size_e;  // grid, per axis
 };
 
+/// Time-domain near-to-far-field transform for one observation direction
+/// (include/xfdtd/nffft/nffft_time_domain.h:23-86): the Huygens box `distance`
+/// cells inside the domain, retarded-time potentials accumulated on the GPU
+/// every step (xfd_set_nf2ff_td).
+class NFFFTTimeDomain {
+ public:
+  NFFFTTimeDomain(Index dx, Index dy, Index dz, Real theta, Real phi)
+      : _d{dx, dy, dz}, _theta{theta}, _phi{phi} {}
+  NFFFTTimeDomain(Index dx, Index dy, Index dz, std::string_view output_dir, Real theta,
+                  Real phi)
+      : _d{dx, dy, dz}, _output_dir{output_dir}, _theta{theta}, _phi{phi} {}
+  std::array<Index, 3> distance() const { return _d; }
+  const std::string& outputDir() const { return _output_dir; }
+  void setOutputDir(std::string d) { _output_dir = std::move(d); }
+  Real theta() const { return _theta; }
+  Real phi() const { return _phi; }
+  /// (sin theta cos phi, sin theta sin phi, cos theta)
+  Vector observationDirection() const;
+  /// Potentials over the retarded-time bins, divided by (c dt 4 pi)
+  /// (NFFFTTimeDomain::wx..uz, src/nffft/nfffft_time_domain.cpp:481-509).
+  Array1D<Real> wx() const { return scaled(0); }
+  Array1D<Real> wy() const { return scaled(1); }
+  Array1D<Real> wz() const { return scaled(2); }
+  Array1D<Real> ux() const { return scaled(3); }
+  Array1D<Real> uy() const { return scaled(4); }
+  Array1D<Real> uz() const { return scaled(5); }
+  /// Writes w_theta.npy, w_phi.npy, u_theta.npy, u_phi.npy (float64, one
+  /// value per bin) into outputDir() (NFFFTTimeDomain::processFarField,
+  /// src/nffft/nfffft_time_domain.cpp:98-160).
+  void processFarField() const;
+  /// The four far-field series of processFarField, in that order.
+  std::array<std::vector<Real>, 4> farField() const;
+
+ private:
+  friend class Simulation;
+  Array1D<Real> scaled(int q) const;
+  std::array<Index, 3> _d;
+  std::string _output_dir;
+  Real _theta, _phi;
+  std::vector<Real> _raw;  // 6 x n_bins sums: W_x W_y W_z U_x U_y U_z
+  Real _c_dt = 0;
+};
+
 class ThreadConfig {
  public:
   ThreadConfig(std::size_t x = 1, std::size_t y = 1, std::size_t z = 1) : _n{x, y, z} {}
@@ -565,6 +608,7 @@ class Simulation {
   void addWaveformSource(std::shared_ptr<WaveformSource> source);
   void addMonitor(std::shared_ptr<Monitor> monitor);
   void addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> nffft);
+  void addNF2FF(std::shared_ptr<NFFFTTimeDomain> nffft);
 
   /// Builds the grid and coefficients, runs `time_step` steps on the GPU and
   /// copies fields, movie frames and NF2FF currents back to the host.
@@ -626,6 +670,7 @@ class Simulation {
  private:
   void setupTfsf(xfd_engine* e);
   void setupNf2ff(xfd_engine* e);
+  void setupNf2ffTd(xfd_engine* e);
 
   Real _dl[3];
   Real _cfl;
@@ -637,6 +682,7 @@ class Simulation {
   std::vector<std::shared_ptr<WaveformSource>> _sources;
   std::vector<std::shared_ptr<Monitor>> _monitors;
   std::vector<std::shared_ptr<NFFFTFrequencyDomain>> _nffts;
+  std::vector<std::shared_ptr<NFFFTTimeDomain>> _nffts_td;
   EMF _emf;
   Real _dt = 0;
   Index _n[3] = {0, 0, 0};

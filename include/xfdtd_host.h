@@ -86,6 +86,10 @@ int xfdtd_scene_dft_objective(xfdtd_scene* s, int64_t n_steps, int32_t field,
                               int32_t voxel_object, int32_t checkpoint_interval, double* value,
                               double* grad, int64_t capacity);
 
+/* Time-domain NF2FF of the finished scene: 4 x n_bins doubles, w_theta,
+ * w_phi, u_theta, u_phi (NFFFTTimeDomain::processFarField).  count = 4 n_bins. */
+int xfdtd_scene_nf2ff_td(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count);
+
 int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir);
 
 #ifdef __cplusplus

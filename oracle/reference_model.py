@@ -128,11 +128,17 @@ class _Nf2ff(ctypes.Structure):
                 ("off", ctypes.POINTER(_i64))]
 
 
+class _Nf2ffTd(ctypes.Structure):
+    _fields_ = [("task_s", (_i64 * 3) * 6), ("task_e", (_i64 * 3) * 6), ("delay", _dp),
+                ("ds", _dp), ("prev", _dp), ("pot", _dp), ("P", _i64), ("n_bins", _i64)]
+
+
 class _Sim(ctypes.Structure):
     _fields_ = [("yee", ctypes.POINTER(_Yee)), ("ade", ctypes.POINTER(_Ade)),
                 ("pml", ctypes.POINTER(_Pml)), ("n_pml", _i64),
                 ("tfsf", ctypes.POINTER(_Tfsf)), ("lumped", ctypes.POINTER(_Lumped)),
-                ("n_lumped", _i64), ("nf2ff", ctypes.POINTER(_Nf2ff))]
+                ("n_lumped", _i64), ("nf2ff", ctypes.POINTER(_Nf2ff)),
+                ("nf2ff_td", ctypes.POINTER(_Nf2ffTd))]
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -778,6 +784,94 @@ class RefSimulation:
             self.ceh_b[c][i, j, k] = f_chb(da)
 
     # ---------------------------------------------------------------- NF2FF
+    def _huygens_tasks(self, d):
+        """NFFFT::initGlobal/makeNodeAxisTask (src/nffft/nffft.cpp:88-245), one
+        domain: per face XN..ZP ([s], [e]) or None."""
+        nn = (self.nx, self.ny, self.nz)
+        gs = [d[a] for a in range(3)]
+        ge = [nn[a] - d[a] for a in range(3)]
+        tasks = []
+        for face in range(6):
+            m, positive = face // 2, face % 2
+            s = list(gs)
+            e = list(ge)
+            c = ge[m] if positive else gs[m]
+            if (not positive) and (c <= 0 or c == 1):
+                tasks.append(None)
+                continue
+            if positive and c >= nn[m]:
+                tasks.append(None)
+                continue
+            s[m], e[m] = c, c + 1
+            for a in range(3):  # make_secondary_axis_range
+                if a == m:
+                    continue
+                if s[a] <= 0:
+                    s[a] = 1
+                if e[a] >= nn[a]:
+                    e[a] = nn[a] - 1
+            tasks.append((s, e))
+        return tasks
+
+    def _nf2ff_td(self):
+        """NFFFTTimeDomain::initTimeDependentVariable and distanceRange
+        (src/nffft/nfffft_time_domain.cpp:49-78, 414-479), the per-point delay
+        and face-cell area of TDPlaneData (src/include/nffft/nffft_td_data.h:
+        22-46, 338-362)."""
+        self.nf2ff_td = None
+        spec = getattr(self.scene, "nf2ff_td", None)
+        if spec is None:
+            return
+        tasks = self._huygens_tasks(spec.distance)
+        ru = (math.sin(spec.theta) * math.cos(spec.phi), math.sin(spec.theta) * math.sin(spec.phi),
+              math.cos(spec.theta))
+        proj, ds = [], []
+        for face, task in enumerate(tasks):
+            if task is None:
+                continue
+            s, e = task
+            m = face // 2
+            A, B = (m + 1) % 3, (m + 2) % 3
+            axes = [self.e_node[a] if a == m else self.h_node[a] for a in range(3)]
+            R = np.meshgrid(*[axes[a][s[a]:e[a]] for a in range(3)], indexing="ij")
+            proj.append((R[0] * ru[0] + R[1] * ru[1] + R[2] * ru[2]).ravel())
+            sz = [self.e_size[a][s[a]:e[a]] for a in range(3)]
+            S = np.meshgrid(*sz, indexing="ij")
+            ds.append((S[A] * S[B]).ravel())
+        if not proj:
+            return
+        proj = np.concatenate(proj)
+        ds = np.ascontiguousarray(np.concatenate(ds))
+        lo, hi = float(proj.min()), float(proj.max())
+        dt = self.dt
+        delay = np.ascontiguousarray((hi - proj) / (C_0 * dt))
+        n_bins = int(math.ceil((hi - lo) / (C_0 * dt))) + self.scene.steps + 4
+        P = proj.size
+        self.nf2ff_td = {"tasks": tasks, "delay": delay, "ds": ds, "P": P, "n_bins": n_bins,
+                         "prev": np.zeros(4 * P), "pot": np.zeros(6 * 4 * n_bins),
+                         "theta": spec.theta, "phi": spec.phi}
+
+    def nf2ff_td_far_field(self) -> Dict[str, np.ndarray]:
+        """NFFFTTimeDomain::wx..uz and processFarField
+        (src/nffft/nfffft_time_domain.cpp:98-160, 481-509): w_theta, w_phi,
+        u_theta, u_phi over the retarded-time bins."""
+        td = self.nf2ff_td
+        nb = td["n_bins"]
+        pot = td["pot"].reshape(6, 4, nb)
+        den = C_0 * self.dt * 4 * PI
+        ua, ub, wa, wb = (pot[:, q] / den for q in range(4))
+        XN, XP, YN, YP, ZN, ZP = range(6)
+        wx = wa[ZN] + wa[ZP] + wb[YN] + wb[YP]
+        wy = wa[XN] + wa[XP] + wb[ZN] + wb[ZP]
+        wz = wb[XN] + wb[XP] + wa[YN] + wa[YP]
+        ux = ua[ZN] + ua[ZP] + ub[YN] + ub[YP]
+        uy = ua[XN] + ua[XP] + ub[ZN] + ub[ZP]
+        uz = ub[XN] + ub[XP] + ua[YN] + ua[YP]
+        ct, st = math.cos(td["theta"]), math.sin(td["theta"])
+        cp, sp = math.cos(td["phi"]), math.sin(td["phi"])
+        return {"w_theta": wx * ct * cp + wy * ct * sp - wz * st, "w_phi": -wx * sp + wy * cp,
+                "u_theta": ux * ct * cp + uy * ct * sp - uz * st, "u_phi": -ux * sp + uy * cp}
+
     def _nf2ff(self):
         """NFFFT::initGlobal/makeNodeAxisTask (src/nffft/nffft.cpp:88-245) and
         FDPlaneData::initDFT (src/nffft/nffft_fd_data.cpp:65-76)."""
@@ -964,6 +1058,7 @@ class RefSimulation:
         self._tfsf()
         self._ade()
         self._nf2ff()
+        self._nf2ff_td()
         self._monitors()
         nt = self.scene.steps
         h_time = linspace((0 + 0.5) * self.dt, (0 + nt + 0.5) * self.dt, nt)
@@ -1056,6 +1151,21 @@ class RefSimulation:
             s.off = nf["off"].ctypes.data_as(ctypes.POINTER(_i64))
             k.append(s)
             sim.nf2ff = ctypes.pointer(s)
+        if self.nf2ff_td is not None:
+            td = self.nf2ff_td
+            s = _Nf2ffTd()
+            for face in range(6):
+                task = td["tasks"][face]
+                for d in range(3):
+                    if task is None:
+                        s.task_s[face][d], s.task_e[face][d] = 0, 0
+                    else:
+                        s.task_s[face][d], s.task_e[face][d] = task[0][d], task[1][d]
+            s.delay, s.ds = _ptr(td["delay"]), _ptr(td["ds"])
+            s.prev, s.pot = _ptr(td["prev"]), _ptr(td["pot"])
+            s.P, s.n_bins = td["P"], td["n_bins"]
+            k.append(s)
+            sim.nf2ff_td = ctypes.pointer(s)
         k.append(sim)
         self._sim = sim
 

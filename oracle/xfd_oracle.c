@@ -555,6 +555,65 @@ void orc_nf2ff_update(const orc_yee *y, const orc_nf2ff *nf, idx_t step) {
 }
 
 /* ------------------------------------------------------------------------
+ * Time-domain NF2FF: NFFFTTimeDomain::update (src/nffft/nfffft_time_domain.cpp:80-96)
+ * -> TDPlaneData<D>::update<E> for the six faces, then update<H> for the six
+ * (src/include/nffft/nffft_td_data.h:169-240).  Per face d: pot + (d*4 + q)*n_bins
+ * holds ua, ub (q = 0, 1; from E) and wa, wb (q = 2, 3; from H) over the
+ * retarded-time bins; prev holds, per point, the previous step's surface-centre
+ * E_a, E_b, H_a, H_b (4 x P); delay and ds per point, faces in order, k fastest.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  idx_t task_s[6][3], task_e[6][3];
+  const double *delay, *ds;
+  double *prev, *pot;
+  idx_t P, n_bins;
+} orc_nf2ff_td;
+
+void orc_nf2ff_td_update(const orc_yee *y, const orc_nf2ff_td *td, idx_t step) {
+  for (int attr = 0; attr < 2; ++attr) {
+    const int is_e = attr == 0;
+    const double offset = is_e ? 0.5 : 0.0;
+    idx_t off = 0;
+    for (int d = 0; d < 6; ++d) {
+      const int m = d / 2;
+      const int positive = d % 2;
+      const idx_t *s = td->task_s[d], *e = td->task_e[d];
+      if (e[0] <= s[0] || e[1] <= s[1] || e[2] <= s[2]) continue;
+      const int A = tan_a(m), B = tan_b(m);
+      double ca = is_e ? 1.0 : -1.0, cb = is_e ? -1.0 : 1.0;
+      if (!positive) {
+        ca *= -1.0;
+        cb *= -1.0;
+      }
+      double *pa = td->pot + (d * 4 + (is_e ? 0 : 2)) * td->n_bins;
+      double *pb = td->pot + (d * 4 + (is_e ? 1 : 3)) * td->n_bins;
+      double *prev_a = td->prev + (is_e ? 0 : 2) * td->P;
+      double *prev_b = td->prev + (is_e ? 1 : 3) * td->P;
+      const idx_t n1 = e[1] - s[1], n2 = e[2] - s[2];
+      for (idx_t i = s[0]; i < e[0]; ++i)
+        for (idx_t j = s[1]; j < e[1]; ++j)
+          for (idx_t k = s[2]; k < e[2]; ++k) {
+            const idx_t q = off + ((i - s[0]) * n1 + (j - s[1])) * n2 + (k - s[2]);
+            const double x = td->delay[q] + offset + (double)step;
+            const idx_t nn = (idx_t)floor(x);
+            const double f = x - (double)nn;
+            const double ds = td->ds[q];
+            const double a = interp_surface(y, m, is_e, A, i, j, k);
+            const double b = interp_surface(y, m, is_e, B, i, j, k);
+            const double da = a - prev_a[q], db = b - prev_b[q];
+            pa[nn] += ca * (1 - f) * ds * db;
+            pa[nn + 1] += ca * f * ds * db;
+            pb[nn] += cb * (1 - f) * ds * da;
+            pb[nn + 1] += cb * f * ds * da;
+            prev_a[q] = a;
+            prev_b[q] = b;
+          }
+      off += (e[0] - s[0]) * n1 * n2;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------
  * One whole time step in the order of Domain::run (src/domain/domain.cpp:82-135):
  * updateH -> correctH (objects -> TFSF -> PML slabs in insertion order)
  * -> updateE -> correctE (same corrector order) -> record (NF2FF; monitors are
@@ -569,6 +628,7 @@ typedef struct {
   const orc_lumped *lumped;
   idx_t n_lumped;
   const orc_nf2ff *nf2ff;      /* NULL: none */
+  const orc_nf2ff_td *nf2ff_td;  /* NULL: none */
 } orc_sim;
 
 void orc_step(const orc_sim *s, idx_t step) {
@@ -584,6 +644,7 @@ void orc_step(const orc_sim *s, idx_t step) {
   if (s->tfsf) orc_tfsf_correct(s->yee, s->tfsf, step, 1);
   for (idx_t p = 0; p < s->n_pml; ++p) orc_pml_correct(s->yee, &s->pml[p], 1);
   if (s->nf2ff) orc_nf2ff_update(s->yee, s->nf2ff, step);
+  if (s->nf2ff_td) orc_nf2ff_td_update(s->yee, s->nf2ff_td, step);
 }
 
 void orc_run(const orc_sim *s, idx_t step0, idx_t nsteps) {

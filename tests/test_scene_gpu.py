@@ -161,3 +161,34 @@ def test_fp32_bistatic_rcs_error_budget():
     keep = p64 >= p64.max(axis=1, keepdims=True) * 1e-3
     err_db = np.abs(10 * np.log10(p32[keep] / p64[keep]))
     assert err_db.max() <= 0.1, err_db.max()
+
+
+def _td_scene(steps=160):
+    sc = sphere_small(steps=steps)
+    sc.nf2ff_td = S.NF2FFTDSpec((8, 8, 8), 0.7, 1.1)
+    return sc
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-4)], ids=["fp64", "fp32"])
+def test_nf2ff_time_domain_matches_oracle(precision, tol, tmp_path):
+    """NFFFTTimeDomain: the far-field series w_theta, w_phi, u_theta, u_phi
+    against the oracle's restatement of TDPlaneData::update (FP64 <= 1e-12
+    relative L2; the FP32 form within 1e-4)."""
+    sc = _td_scene()
+    orc = RefSimulation(sc)
+    orc.run()
+    want = orc.nf2ff_td_far_field()
+    run = SceneRun(sc, precision=precision)
+    run.run()
+    got = run.nf2ff_td()
+    for key in ("w_theta", "w_phi", "u_theta", "u_phi"):
+        assert got[key].shape == want[key].shape, key
+        ref = np.linalg.norm(want[key])
+        assert ref > 0, key
+        err = float(np.linalg.norm(got[key] - want[key]) / ref)
+        assert err <= tol, (key, err)
+    if precision == 0:
+        run.write_outputs(str(tmp_path))
+        for key in ("w_theta", "w_phi", "u_theta", "u_phi"):
+            v = np.load(tmp_path / "nf2ff_td" / f"{key}.npy")
+            assert np.array_equal(v, got[key])

@@ -510,7 +510,7 @@ xfd_status xfd_adjoint_run(xfd_engine* e, const xfd_adjoint_desc* d, double* val
   if (d->obj_field < 0 || d->obj_field > 2 || !box_ok(e->L, d->obj_s, d->obj_e) ||
       (!d->forward_only && !box_ok(e->L, d->design_s, d->design_e)))
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad objective field or node box");
-  if (e->ade_kind >= 0 || e->have_nf2ff || !e->movies.empty())
+  if (e->ade_kind >= 0 || e->have_nf2ff || e->have_td || !e->movies.empty())
     return fail(e, XFD_ERR_UNSUPPORTED,
                 "the adjoint covers CPML, TFSF and lumped sources; not ADE media, NF2FF or movies");
   CUDA_TRY(e, cudaSetDevice(e->device));

@@ -104,6 +104,8 @@ struct xfd_engine {
 
   bool have_nf2ff = false;
   Nf2ffD nf2ff{};
+  bool have_td = false;  // time-domain NF2FF
+  Nf2ffTdD td{};
   long long nf_sampled_since_flush = 0;
   long long nf_last_flush_step = 0;
 
@@ -794,6 +796,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     if (t % mv.d.interval == 0)
       k_movie<T><<<blocks_for(mv.n_nodes, 256), 256, 0, s>>>(mv.d, e->L, fields, e->d_step);
   }
+  if (e->have_td)
+    k_nf2ff_td<T><<<blocks_for(e->td.P, 256), 256, 0, s>>>(e->td, e->L, fields, e->d_step,
+                                                          e->d_err);
   for (int r = 0; r < e->n_rec; ++r) {
     BoxRecD<T> rd;
     if constexpr (sizeof(T) == 8) rd = e->rec64[r]; else rd = e->rec32[r];
@@ -1600,6 +1605,67 @@ xfd_status xfd_nf2ff_far_field(xfd_engine* e, const xfd_far_field_desc* d, doubl
   return s2;
 }
 
+xfd_status xfd_set_nf2ff_td(xfd_engine* e, const xfd_nf2ff_td_desc* d) {
+  if (!e || !d || !d->delay || !d->ds || d->n_bins < 2)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad time-domain NF2FF description");
+  if (e->have_td) return fail(e, XFD_ERR_STATE, "time-domain NF2FF already set");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  Nf2ffTdD td{};
+  long long P = 0;
+  const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
+  for (int f = 0; f < 6; ++f) {
+    td.begin[f] = P;
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) {
+      td.s[f][a] = d->task_s[f][a];
+      td.e[f][a] = d->task_e[f][a];
+      if (td.e[f][a] <= td.s[f][a]) empty = true;
+    }
+    if (empty) {
+      for (int a = 0; a < 3; ++a) td.s[f][a] = td.e[f][a] = 0;
+      continue;
+    }
+    // The interpolation reads one node on either side along the tangential axes.
+    for (int a = 0; a < 3; ++a)
+      if (td.s[f][a] < 1 || td.e[f][a] > n[a])
+        return fail(e, XFD_ERR_INVALID_ARGUMENT, "time-domain NF2FF face %d out of range", f);
+    P += (long long)(td.e[f][0] - td.s[f][0]) * (td.e[f][1] - td.s[f][1]) *
+         (td.e[f][2] - td.s[f][2]);
+  }
+  td.begin[6] = P;
+  td.P = P;
+  td.n_bins = d->n_bins;
+  xfd_status st;
+  double *dl = nullptr, *ds = nullptr;
+  if ((st = upload_raw(e, &dl, d->delay, (size_t)P)) != XFD_OK) return st;
+  if ((st = upload_raw(e, &ds, d->ds, (size_t)P)) != XFD_OK) return st;
+  void *prev = nullptr, *pot = nullptr;
+  if ((st = dev_alloc(e, &prev, (size_t)4 * P * sizeof(double))) != XFD_OK) return st;
+  if ((st = dev_alloc(e, &pot, (size_t)6 * td.n_bins * sizeof(double))) != XFD_OK) return st;
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  td.delay = dl;
+  td.ds = ds;
+  td.prev = static_cast<double*>(prev);
+  td.pot = static_cast<double*>(pot);
+  e->td = td;
+  e->have_td = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_get_nf2ff_td(xfd_engine* e, double* out, int64_t capacity, int64_t* count) {
+  if (!e || !count) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null argument");
+  if (!e->have_td) return fail(e, XFD_ERR_STATE, "no time-domain NF2FF");
+  *count = 6 * e->td.n_bins;
+  if (!out) return XFD_OK;
+  if (capacity < *count) return fail(e, XFD_ERR_INVALID_ARGUMENT, "buffer too small");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  CUDA_TRY(e, cudaMemcpyAsync(out, e->td.pot, (size_t)*count * sizeof(double),
+                              cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
 xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* count) {
   if (!e || !e->have_nf2ff) return fail(e, XFD_ERR_STATE, "no NF2FF");
   CUDA_TRY(e, cudaSetDevice(e->device));
@@ -1825,6 +1891,7 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (e->ade_kind >= 0) n += fused ? 1 : 2;
   if (!e->lumped_h.empty()) n += 1;
   if (e->have_nf2ff) n += 1;
+  if (e->have_td) n += 1;
   if (e->n_ovr) n += fused ? 1 : 2;
   return n + e->n_rec;
 }

@@ -712,6 +712,82 @@ __global__ void k_ovr_apply(OverrideD<T> o, T* const* fields, T* const* fields_i
   E[id] = o.r[q] * E[id] + o.d[q] * old;
 }
 
+// ---------------------------------------------------------------------------
+// Time-domain NF2FF (NFFFTTimeDomain::update, src/nffft/nfffft_time_domain.cpp:80-96
+// -> TDPlaneData::update, src/include/nffft/nffft_td_data.h:169-240): per
+// Huygens point and step, the surface-centre tangential E and H
+// (interpolateSurfaceCenter, as for the frequency-domain transform) minus
+// their values of the previous step, weighted by the face-cell area, are
+// added to the retarded-time bins nn, nn + 1 of the far-field potentials,
+// nn + f = delay + offset + t (offset 1/2 for E, 0 for H; delay = (the
+// surface's largest projected distance - the point's) / (c dt), FP64 on the
+// host).  Face with normal m, tangential axes A = m+1, B = m+2, sign
+// s = -1 on the negative face: U[A] += s (B change), U[B] -= s (A change) for
+// E; W[A] -= s (B change), W[B] += s (A change) for H.  The bins are shared
+// by many points: FP64 atomics.
+// ---------------------------------------------------------------------------
+struct Nf2ffTdD {
+  int s[6][3], e[6][3];
+  long long begin[7];  // point offsets per face, begin[6] = P
+  long long P;
+  const double* delay;  // P
+  const double* ds;     // P
+  double* prev;         // 4 x P: E_a, E_b, H_a, H_b of the previous step
+  double* pot;          // 6 x n_bins: W_x W_y W_z U_x U_y U_z
+  long long n_bins;
+};
+
+__device__ __forceinline__ void td_add(double* row, long long n_bins, double x, double c,
+                                       double ds, double delta, int* err) {
+  const long long nn = (long long)floor(x);
+  const double f = x - (double)nn;
+  if (nn < 0 || nn + 1 >= n_bins) {
+    atomicOr(err, 1);
+    return;
+  }
+  atomicAdd(row + nn, c * (1 - f) * ds * delta);
+  atomicAdd(row + nn + 1, c * f * ds * delta);
+}
+
+template <typename T>
+__global__ void k_nf2ff_td(Nf2ffTdD td, Lat L, T* const* fields, const long long* step,
+                           int* err) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= td.P) return;
+  int d = 0;
+  while (d < 5 && p >= td.begin[d + 1]) ++d;
+  long long r = p - td.begin[d];
+  const int* s = td.s[d];
+  const int* e = td.e[d];
+  const int e2 = e[2] - s[2], e1 = e[1] - s[1];
+  const int k = s[2] + (int)(r % e2);
+  r /= e2;
+  const int j = s[1] + (int)(r % e1);
+  r /= e1;
+  const int i = s[0] + (int)r;
+  const int m = d / 2;
+  const double sg = (d % 2) ? 1.0 : -1.0;
+  const int A = (m + 1) % 3, B = (m + 2) % 3;
+  const double t = (double)*step;
+  const double ds = td.ds[p];
+  // E: coefficients (1, -1) times the face sign, bins at delay + 1/2 + t
+  const double ea = surf_e(fields, L, m, A, i, j, k), eb = surf_e(fields, L, m, B, i, j, k);
+  const double dea = ea - td.prev[p], deb = eb - td.prev[td.P + p];
+  td.prev[p] = ea;
+  td.prev[td.P + p] = eb;
+  const double xe = (td.delay[p] + 0.5) + t;
+  td_add(td.pot + (3 + A) * td.n_bins, td.n_bins, xe, sg, ds, deb, err);
+  td_add(td.pot + (3 + B) * td.n_bins, td.n_bins, xe, -sg, ds, dea, err);
+  // H: coefficients (-1, 1) times the face sign, bins at delay + t
+  const double ha = surf_h(fields, L, m, A, i, j, k), hb = surf_h(fields, L, m, B, i, j, k);
+  const double dha = ha - td.prev[2 * td.P + p], dhb = hb - td.prev[3 * td.P + p];
+  td.prev[2 * td.P + p] = ha;
+  td.prev[3 * td.P + p] = hb;
+  const double xh = (td.delay[p] + 0.0) + t;
+  td_add(td.pot + A * td.n_bins, td.n_bins, xh, -sg, ds, dhb, err);
+  td_add(td.pot + B * td.n_bins, td.n_bins, xh, sg, ds, dha, err);
+}
+
 __global__ void k_advance(long long* step) { *step += 1; }
 
 // Step counters of many lattices.

@@ -115,6 +115,7 @@ struct xfdtd_scene {
   std::vector<std::shared_ptr<MovieMonitor>> movies;
   std::vector<std::shared_ptr<FieldTimeMonitor>> probes;
   std::shared_ptr<NFFFTFrequencyDomain> nf2ff;
+  std::shared_ptr<NFFFTTimeDomain> nf2ff_td;
   int64_t steps = 0;
   bool finished = false;
 };
@@ -238,6 +239,12 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       for (int q = 0; q < nf; ++q) fr.push_back(num(in));
       sc->nf2ff = std::make_shared<NFFFTFrequencyDomain>(dx, dy, dz, Array1D<Real>(fr));
       sc->sim->addNF2FF(sc->nf2ff);
+    } else if (kw == "nf2ff_td") {
+      const auto dx = static_cast<Index>(num(in)), dy = static_cast<Index>(num(in)),
+                 dz = static_cast<Index>(num(in));
+      const double theta = num(in), phi = num(in);
+      sc->nf2ff_td = std::make_shared<NFFFTTimeDomain>(dx, dy, dz, theta, phi);
+      sc->sim->addNF2FF(sc->nf2ff_td);
     } else {
       throw XFDTDException("unknown scene line: " + l);
     }
@@ -475,6 +482,24 @@ int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir) {
         v.push_back(z.imag());
       }
       writeNpy((root / "nf2ff.npy").string(), v, {acc.size(), 2});
+    }
+    if (s->nf2ff_td) {
+      s->nf2ff_td->setOutputDir((root / "nf2ff_td").string());
+      s->nf2ff_td->processFarField();
+    }
+  })
+}
+
+int xfdtd_scene_nf2ff_td(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count) {
+  HOST_TRY({
+    if (!s || !s->nf2ff_td) throw XFDTDException("scene has no time-domain NF2FF");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    const auto ff = s->nf2ff_td->farField();
+    const std::size_t n = ff[0].size();
+    if (count) *count = (int64_t)(4 * n);
+    if (out) {
+      if ((std::size_t)capacity < 4 * n) throw XFDTDException("buffer too small");
+      for (int q = 0; q < 4; ++q) std::copy(ff[q].begin(), ff[q].end(), out + q * n);
     }
   })
 }

@@ -295,6 +295,7 @@ void Simulation::addWaveformSource(std::shared_ptr<WaveformSource> s) {
   _sources.push_back(std::move(s));
 }
 void Simulation::addMonitor(std::shared_ptr<Monitor> m) { _monitors.push_back(std::move(m)); }
+void Simulation::addNF2FF(std::shared_ptr<NFFFTTimeDomain> n) { _nffts_td.push_back(std::move(n)); }
 void Simulation::addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> n) {
   _nffts.push_back(std::move(n));
 }
@@ -1017,6 +1018,7 @@ void Simulation::init(Index time_step) {
   }
   setupTfsf(E);
   setupNf2ff(E);
+  setupNf2ffTd(E);
   // Movie monitors (FieldMonitor box with the +1 origin shift at index 0,
   // src/monitor/field_monitor.cpp:17-67).
   for (const auto& mon : _monitors) {
@@ -1134,6 +1136,14 @@ void Simulation::finish() {
     for (int64_t f = 0; f < frames && f < (int64_t)d.size(); ++f)
       d[f] = (w == 8) ? reinterpret_cast<double*>(buf.data())[f]
                       : reinterpret_cast<float*>(buf.data())[f];
+  }
+  if (!_nffts_td.empty()) {
+    int64_t cnt = 0;
+    checkStatus(_engine, xfd_get_nf2ff_td(_engine, nullptr, 0, &cnt), "nf2ff_td");
+    auto& td = *_nffts_td[0];
+    td._raw.assign((std::size_t)cnt, 0.0);
+    checkStatus(_engine, xfd_get_nf2ff_td(_engine, td._raw.data(), cnt, &cnt), "nf2ff_td");
+    td._c_dt = C_0 * _dt;
   }
   if (I.nf2ff) {
     int64_t cnt = 0;
@@ -1467,6 +1477,140 @@ void Simulation::setupNf2ff(xfd_engine* E) {
     nf._node_h[a] = _impl->h_node[a];
     nf._size_e[a] = _impl->e_size[a];
   }
+}
+
+}  // namespace xfdtd
+
+namespace xfdtd {
+
+// NFFFT::initGlobal / makeNodeAxisTask (src/nffft/nffft.cpp:88-245), one
+// domain: the six Huygens faces [s, e) of a box `d` cells inside the grid
+// (all zero when a face is not valid).
+static void huygensFaces(const Index n[3], const std::array<Index, 3>& d, int s_out[6][3],
+                         int e_out[6][3]) {
+  for (int face = 0; face < 6; ++face) {
+    const int m = face / 2;
+    const bool positive = face % 2;
+    int s[3], e[3];
+    for (int a = 0; a < 3; ++a) {
+      s[a] = (int)d[a];
+      e[a] = (int)(n[a] - d[a]);
+    }
+    const int c = positive ? e[m] : s[m];
+    bool valid = positive ? (c < (int)n[m]) : (c > 1);
+    s[m] = c;
+    e[m] = c + 1;
+    for (int a = 0; a < 3; ++a) {
+      if (a == m) continue;
+      if (s[a] <= 0) s[a] = 1;
+      if (e[a] >= (int)n[a]) e[a] = (int)n[a] - 1;
+      if (e[a] <= s[a]) valid = false;
+    }
+    for (int a = 0; a < 3; ++a) {
+      s_out[face][a] = valid ? s[a] : 0;
+      e_out[face][a] = valid ? e[a] : 0;
+    }
+  }
+}
+
+// NFFFTTimeDomain::initTimeDependentVariable / distanceRange and the per-point
+// terms of TDPlaneData::update (src/nffft/nfffft_time_domain.cpp:49-78,
+// 414-479; src/include/nffft/nffft_td_data.h:22-46, 169-240, 338-362).
+void Simulation::setupNf2ffTd(xfd_engine* E) {
+  if (_nffts_td.empty()) return;
+  if (_nffts_td.size() > 1) throw XFDTDException("one NFFFTTimeDomain per simulation");
+  const Impl& I = *_impl;
+  auto& td = *_nffts_td[0];
+  xfd_nf2ff_td_desc desc{};
+  huygensFaces(_n, td.distance(), desc.task_s, desc.task_e);
+  const Vector ru = td.observationDirection();
+  // Point positions: e node along the face normal, h nodes across it.
+  std::vector<Real> proj, ds;
+  for (int face = 0; face < 6; ++face) {
+    const int m = face / 2;
+    const int* s = desc.task_s[face];
+    const int* e = desc.task_e[face];
+    for (int i = s[0]; i < e[0]; ++i)
+      for (int j = s[1]; j < e[1]; ++j)
+        for (int k = s[2]; k < e[2]; ++k) {
+          const int x[3] = {i, j, k};
+          Real r[3];
+          for (int a = 0; a < 3; ++a) r[a] = a == m ? I.e_node[a][x[a]] : I.h_node[a][x[a]];
+          proj.push_back(r[0] * ru(0) + r[1] * ru(1) + r[2] * ru(2));
+          const int A = (m + 1) % 3, B = (m + 2) % 3;
+          ds.push_back(I.e_size[A][x[A]] * I.e_size[B][x[B]]);
+        }
+  }
+  if (proj.empty()) return;  // the reference's valid() is false: nothing recorded
+  const Real lo = *std::min_element(proj.begin(), proj.end());
+  const Real hi = *std::max_element(proj.begin(), proj.end());
+  const Real dt = _dt;
+  std::vector<Real> delay(proj.size());
+  for (std::size_t q = 0; q < proj.size(); ++q) delay[q] = (hi - proj[q]) / (C_0 * dt);
+  const Real aux = (hi - lo) / (C_0 * dt);
+  desc.n_bins = (int64_t)((Index)std::ceil(aux) + _steps + 4);
+  desc.delay = delay.data();
+  desc.ds = ds.data();
+  checkStatus(E, xfd_set_nf2ff_td(E, &desc), "xfd_set_nf2ff_td");
+}
+
+Vector NFFFTTimeDomain::observationDirection() const {
+  return Vector{std::sin(_theta) * std::cos(_phi), std::sin(_theta) * std::sin(_phi),
+                std::cos(_theta)};
+}
+
+Array1D<Real> NFFFTTimeDomain::scaled(int q) const {
+  if (_raw.empty()) return Array1D<Real>(std::vector<Real>{});
+  const std::size_t n = _raw.size() / 6;
+  const Real den = _c_dt * 4 * PI;
+  std::vector<Real> v(n);
+  for (std::size_t b = 0; b < n; ++b) v[b] = _raw[q * n + b] / den;
+  return Array1D<Real>(v);
+}
+
+std::array<std::vector<Real>, 4> NFFFTTimeDomain::farField() const {
+  std::array<std::vector<Real>, 4> out;
+  if (_raw.empty()) return out;
+  const auto wx_ = wx(), wy_ = wy(), wz_ = wz(), ux_ = ux(), uy_ = uy(), uz_ = uz();
+  const Real ct = std::cos(_theta), st = std::sin(_theta), cp = std::cos(_phi),
+             sp = std::sin(_phi);
+  const std::size_t n = wx_.size();
+  for (auto& v : out) v.resize(n);
+  for (std::size_t b = 0; b < n; ++b) {
+    out[0][b] = wx_[b] * ct * cp + wy_[b] * ct * sp - wz_[b] * st;
+    out[1][b] = -wx_[b] * sp + wy_[b] * cp;
+    out[2][b] = ux_[b] * ct * cp + uy_[b] * ct * sp - uz_[b] * st;
+    out[3][b] = -ux_[b] * sp + uy_[b] * cp;
+  }
+  return out;
+}
+
+namespace {
+void writeRealNpy(const std::string& path, const std::vector<Real>& v) {
+  std::ostringstream hdr;
+  hdr << "{'descr': '<f8', 'fortran_order': False, 'shape': (" << v.size() << ",), }";
+  std::string h = hdr.str();
+  const std::size_t total = 10 + h.size() + 1;
+  h.append((64 - total % 64) % 64, ' ');
+  h.push_back('\n');
+  std::ofstream f(path, std::ios::binary);
+  if (!f) throw XFDTDException("cannot write " + path);
+  f.write("\x93NUMPY\x01\x00", 8);
+  const uint16_t len = static_cast<uint16_t>(h.size());
+  f.write(reinterpret_cast<const char*>(&len), 2);
+  f.write(h.data(), (std::streamsize)h.size());
+  f.write(reinterpret_cast<const char*>(v.data()), (std::streamsize)(v.size() * sizeof(Real)));
+}
+}  // namespace
+
+void NFFFTTimeDomain::processFarField() const {
+  if (_raw.empty()) return;
+  namespace fs = std::filesystem;
+  const fs::path dir(_output_dir.empty() ? "." : _output_dir);
+  fs::create_directories(dir);
+  const auto ff = farField();
+  static const char* names[4] = {"w_theta.npy", "w_phi.npy", "u_theta.npy", "u_phi.npy"};
+  for (int q = 0; q < 4; ++q) writeRealNpy((dir / names[q]).string(), ff[q]);
 }
 
 }  // namespace xfdtd

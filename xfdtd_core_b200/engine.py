@@ -159,7 +159,8 @@ def exported_symbols() -> List[str]:
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
             "xfd_launches_per_step", "xfd_stencil_bytes_per_step", "xfd_set_e_overrides",
             "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
-            "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_batch_create",
+            "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_set_nf2ff_td", "xfd_get_nf2ff_td",
+            "xfd_batch_create",
             "xfd_batch_destroy", "xfd_batch_last_error", "xfd_batch_run", "xfd_batch_sync",
             "xfd_batch_set_option", "xfd_batch_get_option", "xfd_batch_tuning",
             "xfd_batch_size", "xfd_batch_launches_per_step", "xfd_batch_stream"]

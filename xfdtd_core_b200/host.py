@@ -57,6 +57,7 @@ def load():
         "xfdtd_scene_write_outputs": ([vp, ctypes.c_char_p], ctypes.c_int),
         "xfdtd_scene_dft_objective": ([vp, i64, i32, i32 * 3, i32 * 3, ctypes.c_double, i32, i32,
                                        _dp, _dp, i64], ctypes.c_int),
+        "xfdtd_scene_nf2ff_td": ([vp, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -72,7 +73,7 @@ def exported_symbols() -> List[str]:
             "xfdtd_scene_advance", "xfdtd_scene_tfsf", "xfdtd_scene_finish",
             "xfdtd_scene_coefficients", "xfdtd_scene_field", "xfdtd_scene_movie",
             "xfdtd_scene_nf2ff", "xfdtd_scene_far_field", "xfdtd_scene_field_time",
-            "xfdtd_scene_write_outputs", "xfdtd_scene_dft_objective"]
+            "xfdtd_scene_write_outputs", "xfdtd_scene_dft_objective", "xfdtd_scene_nf2ff_td"]
 
 
 class SceneRun:
@@ -238,6 +239,17 @@ class SceneRun:
             self.h, int(n_steps), field, bs, be, float(freq), voxel_object, checkpoint_interval,
             ctypes.byref(J), g.ctypes.data_as(_dp), g.size))
         return J.value, g
+
+    def nf2ff_td(self) -> dict:
+        """Time-domain NF2FF far-field series (w_theta, w_phi, u_theta, u_phi)."""
+        cnt = ctypes.c_int64()
+        self._check(self.L.xfdtd_scene_nf2ff_td(self.h, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value)
+        self._check(self.L.xfdtd_scene_nf2ff_td(self.h, out.ctypes.data_as(_dp), cnt.value,
+                                                ctypes.byref(cnt)))
+        n = cnt.value // 4
+        return {k: out[q * n:(q + 1) * n] for q, k in
+                enumerate(("w_theta", "w_phi", "u_theta", "u_phi"))}
 
     def write_outputs(self, directory: str):
         self._check(self.L.xfdtd_scene_write_outputs(self.h, directory.encode()))

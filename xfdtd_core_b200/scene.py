@@ -278,6 +278,18 @@ class NF2FFSpec:
 
 
 @dataclass
+class NF2FFTDSpec:
+    """NFFFTTimeDomain(distance_x, distance_y, distance_z, theta, phi)."""
+    distance: Tuple[int, int, int]
+    theta: float
+    phi: float
+
+    def text(self) -> str:
+        d = self.distance
+        return f"nf2ff_td {d[0]} {d[1]} {d[2]} {_f(self.theta)} {_f(self.phi)}"
+
+
+@dataclass
 class Scene:
     """Everything a reference user program passes to ``xfdtd::Simulation``."""
 
@@ -291,6 +303,7 @@ class Scene:
     movies: List[MovieSpec] = field(default_factory=list)
     field_times: List[FieldTimeSpec] = field(default_factory=list)
     nf2ff: Optional[NF2FFSpec] = None
+    nf2ff_td: Optional[NF2FFTDSpec] = None
     name: str = "scene"
 
     def to_text(self) -> str:
@@ -306,6 +319,8 @@ class Scene:
         lines += [m.text() for m in self.field_times]
         if self.nf2ff is not None:
             lines.append(self.nf2ff.text())
+        if self.nf2ff_td is not None:
+            lines.append(self.nf2ff_td.text())
         return "\n".join(lines) + "\n"
 
     def write(self, path: str) -> str:
