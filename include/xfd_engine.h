@@ -142,6 +142,17 @@ xfd_status xfd_add_current_source(xfd_engine* e, int32_t comp, const int32_t box
                                   const int32_t box_e[3], const double* coff,
                                   const double* waveform);
 
+/* Lumped inductor on a box of E_comp nodes [box_s, box_e): after the E update
+ * and the current sources, E += cecjc[node] * J[node], then
+ * J[node] += cjcec[node] * E[node]; J (FP64) starts at zero and is part of the
+ * saved state.  cecjc and cjcec are box-shaped (k fastest).  Added before the
+ * first step.  The voltage source (the current-source form above), resistor
+ * and capacitor are coefficient changes and source terms only.
+ * Replaces: Inductor::generateCorrector (src/object/lumped_element/inductor.cpp:111-135)
+ * and InductorCorrector::correctE (src/object/lumped_element/lumped_element_corrrector.cpp:42-99). */
+xfd_status xfd_add_inductor(xfd_engine* e, int32_t comp, const int32_t box_s[3],
+                            const int32_t box_e[3], const double* cecjc, const double* cjcec);
+
 /* Dispersive (ADE) E nodes on a compacted list.  kind 0 = modified Lorentz
  * (J, J_prev, E_prev), 1 = Drude, 2 = Debye.  mat_coeff holds, per material,
  * 2 + 7*n_poles doubles: c_e_j_sum, c_e_e_prev, then per pole
@@ -234,6 +245,17 @@ typedef struct {
 
 xfd_status xfd_set_nf2ff_td(xfd_engine* e, const xfd_nf2ff_td_desc* d);
 xfd_status xfd_get_nf2ff_td(xfd_engine* e, double* out, int64_t capacity, int64_t* count);
+
+/* Weighted probe: every step t, value = sum_q weight[q] F_comp[q](node q)
+ * (comp 0..5 = Ex..Hz; node = (i, j, k), 3 per entry), reduced in FP64 into
+ * row t of the probe's series.  xfd_get_probe copies the n_steps values.
+ * Replaces: VoltageMonitor::update and CurrentMonitor::update
+ * (src/monitor/voltage_monitor.cpp:198-235, src/monitor/current_monitor.cpp:253-379),
+ * whose index ranges and weights the host computes. */
+xfd_status xfd_add_probe(xfd_engine* e, int64_t n, const int32_t* comp, const int32_t* node,
+                         const double* weight, int32_t* id);
+xfd_status xfd_get_probe(xfd_engine* e, int32_t id, double* out, int64_t capacity,
+                         int64_t* count);
 
 /* Movie monitor: every `interval` steps (from step 0) the box [box_s, box_e)
  * of `field` is recorded into a device frame store.

@@ -494,6 +494,58 @@ class FieldTimeMonitor : public Monitor {
   std::vector<Real> _time, _data;
 };
 
+/// Voltage along `direction` across the cube's node box, every step
+/// (src/monitor/voltage_monitor.cpp:17-235): the E component along the
+/// direction, weighted by -h_c / (na nb) over the box (a, b extended by one
+/// node and kept off the domain edges), sign flipped for a negative
+/// direction.  time() = E times; output() writes <outputDir>/<name>.npy, a
+/// (2, n_steps) array [time; data] (TimeMonitor::output, time_monitor.cpp:9-18).
+class VoltageMonitor : public Monitor {
+ public:
+  VoltageMonitor(std::string name, std::unique_ptr<Cube> cube, Axis::Direction direction,
+                 std::string output_dir = "")
+      : Monitor{std::move(name), std::move(output_dir)},
+        _cube{std::move(cube)},
+        _direction{direction} {}
+  const std::unique_ptr<Cube>& cube() const { return _cube; }
+  Axis::Direction direction() const { return _direction; }
+  const std::vector<Real>& time() const { return _time; }
+  const std::vector<Real>& data() const { return _data; }
+  void output() const;
+
+ private:
+  friend class Simulation;
+  std::unique_ptr<Cube> _cube;
+  Axis::Direction _direction;
+  std::vector<Real> _time, _data;
+  int _probe = -1;
+};
+
+/// Current through the cube's face normal to `direction`, every step: the
+/// loop integral of H around it on the last node plane along the direction
+/// (src/monitor/current_monitor.cpp:17-379).  time() = H times; output() as
+/// for VoltageMonitor.
+class CurrentMonitor : public Monitor {
+ public:
+  CurrentMonitor(std::string name, std::unique_ptr<Cube> cube, Axis::Direction direction,
+                 std::string output_dir = "")
+      : Monitor{std::move(name), std::move(output_dir)},
+        _cube{std::move(cube)},
+        _direction{direction} {}
+  const std::unique_ptr<Cube>& cube() const { return _cube; }
+  Axis::Direction direction() const { return _direction; }
+  const std::vector<Real>& time() const { return _time; }
+  const std::vector<Real>& data() const { return _data; }
+  void output() const;
+
+ private:
+  friend class Simulation;
+  std::unique_ptr<Cube> _cube;
+  Axis::Direction _direction;
+  std::vector<Real> _time, _data;
+  int _probe = -1;
+};
+
 // ------------------------------------------------------------------ NF2FF
 /// Frequency-domain NF2FF on a Huygens box `distance` cells inside the grid
 /// faces (src/nffft/nffft_frequency_domain.cpp).  After run() the surface
@@ -671,6 +723,10 @@ class Simulation {
   void setupTfsf(xfd_engine* e);
   void setupNf2ff(xfd_engine* e);
   void setupNf2ffTd(xfd_engine* e);
+  void voltageProbe(const VoltageMonitor& m, std::vector<int32_t>& comp, std::vector<int32_t>& node,
+                    std::vector<double>& w) const;
+  void currentProbe(const CurrentMonitor& m, std::vector<int32_t>& comp, std::vector<int32_t>& node,
+                    std::vector<double>& w) const;
 
   Real _dl[3];
   Real _cfl;

@@ -86,6 +86,11 @@ int xfdtd_scene_dft_objective(xfdtd_scene* s, int64_t n_steps, int32_t field,
                               int32_t voxel_object, int32_t checkpoint_interval, double* value,
                               double* grad, int64_t capacity);
 
+/* Voltage (kind 0) or current (kind 1) monitor number `index` of the
+ * finished scene: [time; data], 2 x n_steps doubles, count = 2 n_steps. */
+int xfdtd_scene_line_monitor(xfdtd_scene* s, int32_t kind, int32_t index, double* out,
+                             int64_t capacity, int64_t* count);
+
 /* Time-domain NF2FF of the finished scene: 4 x n_bins doubles, w_theta,
  * w_phi, u_theta, u_phi (NFFFTTimeDomain::processFarField).  count = 4 n_bins. */
 int xfdtd_scene_nf2ff_td(xfdtd_scene* s, double* out, int64_t capacity, int64_t* count);

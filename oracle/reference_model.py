@@ -237,6 +237,8 @@ class RefSimulation:
         self.lumped = list(lumped)
         self.ade = ade
         self.nf2ff = nf2ff
+        self.nf2ff_td = None
+        self.line_monitors = []
         self._bind()
         self.t = 0
         return self
@@ -1039,6 +1041,82 @@ class RefSimulation:
             t_arr = (linspace((0 + 1) * self.dt, (0 + nt) * self.dt, nt) if ft.field[0] == "E"
                      else linspace((0 + 0.5) * self.dt, (0 + nt + 0.5) * self.dt, nt))
             self.field_time_data[ft.name] = np.stack([t_arr, np.zeros(nt)])
+        self._line_monitors()
+
+    def _line_monitors(self):
+        """VoltageMonitor::init/update (src/monitor/voltage_monitor.cpp:17-235)
+        and CurrentMonitor::init/update (src/monitor/current_monitor.cpp:17-379)
+        for one domain (node task = global task, lower corner 0, upper corner
+        n), as lists of (field name, node, weight) summed every step."""
+        self.line_monitors = []
+        self.line_monitor_data: Dict[str, np.ndarray] = {}
+        nt = self.scene.steps
+        n = (self.nx, self.ny, self.nz)
+        for spec in getattr(self.scene, "line_monitors", []):
+            c = "XYZ".index(spec.direction[0])
+            neg = spec.direction[1] == "N"
+            a, b = (c + 1) % 3, (c + 2) % 3
+            o, e = self.grid_box(spec.shape)
+            entries = []
+            if spec.kind == "voltage":
+                r = [None, None, None]
+                for ax in (a, b):
+                    s0, s1 = o[ax], e[ax] + 1
+                    if s0 <= 0:
+                        s0 = 1
+                    if n[ax] <= s1:
+                        s1 = n[ax] - 1
+                    r[ax] = (s0, s1)
+                r[c] = (o[c], e[c])
+                if any(r[q][1] <= r[q][0] for q in range(3)):
+                    raise ValueError(f"{spec.name} globalTask is not valid")
+                nab = (r[a][1] - r[a][0]) * (r[b][1] - r[b][0])
+                for i in range(*r[0]):
+                    for j in range(*r[1]):
+                        for k in range(*r[2]):
+                            x = (i, j, k)
+                            coff = -self.h_size[c][x[c]] / float(nab)
+                            if neg:
+                                coff *= -1.0
+                            entries.append(("E" + "XYZ"[c], x, coff))
+                t_arr = linspace((0 + 1) * self.dt, (0 + nt) * self.dt, nt)
+            else:
+                if e[c] == 0 or o[a] == 0 or e[a] == n[a] or o[b] == 0 or e[b] == n[b]:
+                    raise ValueError(f"{spec.name}: invalid current monitor box")
+                lo, hi = list(o), list(e)
+                lo[c] = e[c] - 1
+
+                def ranges(b_start, b_end, n_b, n_a, start, end):
+                    if start <= 0:
+                        start = 1
+                    end = end + 1
+                    if n_a <= end:
+                        end = n_a - 1
+                    rn = (start, end) if b_start not in (0, n_b - 1, n_b) else (0, 0)
+                    rp = (start, end) if b_end not in (n_b, n_b - 1, 0) else (0, 0)
+                    return rn, rp
+
+                ha_bn, ha_bp = ranges(lo[b], hi[b], n[b], n[a], lo[a], hi[a])
+                hb_an, hb_ap = ranges(lo[a], hi[a], n[a], n[b], lo[b], hi[b])
+                sgn = -1.0 if neg else 1.0
+                plane = hi[c] - 1
+
+                def node(av, bv):
+                    x = [0, 0, 0]
+                    x[a], x[b], x[c] = av, bv, plane
+                    return tuple(x)
+
+                for v in range(*ha_bn):
+                    entries.append(("H" + "XYZ"[a], node(v, lo[b] - 1), sgn * self.e_size[a][v]))
+                for v in range(*ha_bp):
+                    entries.append(("H" + "XYZ"[a], node(v, hi[b]), -sgn * self.e_size[a][v]))
+                for v in range(*hb_an):
+                    entries.append(("H" + "XYZ"[b], node(lo[a] - 1, v), -sgn * self.e_size[b][v]))
+                for v in range(*hb_ap):
+                    entries.append(("H" + "XYZ"[b], node(hi[a], v), sgn * self.e_size[b][v]))
+                t_arr = linspace((0 + 0.5) * self.dt, (0 + nt + 0.5) * self.dt, nt)
+            self.line_monitors.append({"name": spec.name, "entries": entries})
+            self.line_monitor_data[spec.name] = np.stack([t_arr, np.zeros(nt)])
 
     # ----------------------------------------------------------------- init
     def _init(self):
@@ -1171,6 +1249,12 @@ class RefSimulation:
 
     # ------------------------------------------------------------------ run
     def _record_monitors(self):
+        for lm in self.line_monitors:
+            v = 0.0
+            for fname, x, w in lm["entries"]:
+                arr = (self.e if fname[0] == "E" else self.h)["XYZ".index(fname[1])]
+                v += w * arr[x]
+            self.line_monitor_data[lm["name"]][1, self.t] = v
         for ft in self.field_times:
             if ft["node"] is not None:
                 f = ft["field"]
@@ -1190,7 +1274,8 @@ class RefSimulation:
         if self.threads:
             L.orc_set_num_threads(self.threads)
         n = self.scene.steps - self.t if nsteps is None else nsteps
-        if not self.movies and not getattr(self, "field_times", None):
+        if not self.movies and not getattr(self, "field_times", None) and \
+                not getattr(self, "line_monitors", None):
             L.orc_run(ctypes.byref(self._sim), self.t, n)
             self.t += n
             return

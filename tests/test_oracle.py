@@ -162,3 +162,15 @@ def test_far_field_restatement_matches_loop_and_origin_shift():
     rhat = np.stack([np.sin(theta) * math.cos(phi), np.sin(theta) * math.sin(phi), np.cos(theta)])
     shift = np.exp(-1j * k0[:, None] * (d @ rhat)[None, :])
     assert np.linalg.norm(moved - ff * shift[:, None, :]) <= 1e-11 * np.linalg.norm(ff)
+
+
+def test_kernel_case_oracle_steps():
+    """The kernel-level oracle (explicit arrays, no scene init) steps and
+    changes the fields."""
+    from tests.cases import KernelCase
+    kc = KernelCase(seed=1)
+    orc = kc.oracle()
+    before = [f.copy() for f in orc.e]
+    orc.run(2)
+    assert orc.t == 2
+    assert any(not np.array_equal(a, b) for a, b in zip(before, orc.e))

@@ -192,3 +192,39 @@ def test_nf2ff_time_domain_matches_oracle(precision, tol, tmp_path):
         for key in ("w_theta", "w_phi", "u_theta", "u_phi"):
             v = np.load(tmp_path / "nf2ff_td" / f"{key}.npy")
             assert np.array_equal(v, got[key])
+
+
+def test_voltage_and_current_monitors_match_oracle(tmp_path):
+    """VoltageMonitor and CurrentMonitor series (weighted per-step probes on
+    the GPU) against the oracle's restatement of their index rules; FP64
+    <= 1e-12 relative L2, and the [time; data] npy files."""
+    from tests.scenes import boxes_small
+    sc = boxes_small(steps=150)
+    dl = sc.dl[0]
+    # a z-directed dipole sits at the centre: a voltage across it, the current
+    # through a loop around it, one of each direction more off-centre
+    sc.line_monitors = [
+        S.LineMonitorSpec("voltage", "v_dipole", S.cube((0.0, 0.0, -2 * dl), (0.0, 0.0, 4 * dl)),
+                          "ZP"),
+        S.LineMonitorSpec("voltage", "v_x", S.cube((-3 * dl, dl, 0.0), (6 * dl, dl, 0.0)), "XN"),
+        S.LineMonitorSpec("current", "i_dipole",
+                          S.cube((-dl, -dl, -dl), (2 * dl, 2 * dl, 2 * dl)), "ZP"),
+        S.LineMonitorSpec("current", "i_y", S.cube((-2 * dl, -dl, -2 * dl), (4 * dl, 3 * dl, 3 * dl)),
+                          "YN"),
+    ]
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc)
+    run.run()
+    for q, kind, name in ((0, "voltage", "v_dipole"), (1, "voltage", "v_x"),
+                          (0, "current", "i_dipole"), (1, "current", "i_y")):
+        got = run.line_monitor(kind, q)
+        want = orc.line_monitor_data[name]
+        assert got.shape == want.shape
+        assert np.array_equal(got[0], want[0]), name
+        ref = np.linalg.norm(want[1])
+        assert ref > 0, name
+        assert np.linalg.norm(got[1] - want[1]) / ref <= 1e-12, name
+    run.write_outputs(str(tmp_path))
+    v = np.load(tmp_path / "monitors" / "v_dipole.npy")
+    assert v.shape == (2, 150) and np.array_equal(v, run.line_monitor("voltage", 0))

@@ -90,6 +90,16 @@ struct xfd_engine {
   LumpedD lumped{};
   bool lumped_dirty = false;
 
+  // lumped inductors: host lists, device list with its FP64 current state
+  struct InductorH {
+    int comp;
+    std::vector<long long> node;
+    std::vector<double> cecjc, cjcec;
+  };
+  std::vector<InductorH> ind_h;
+  InductorD ind{};
+  bool ind_dirty = false;
+
   // per-node E coefficient overrides (device list + host copy for the adjoint)
   long long n_ovr = 0;
   OverrideD<double> ovr64{};
@@ -106,6 +116,13 @@ struct xfd_engine {
   Nf2ffD nf2ff{};
   bool have_td = false;  // time-domain NF2FF
   Nf2ffTdD td{};
+  // weighted probes: host lists, device copy rebuilt when one is added
+  std::vector<long long> pr_begin{0};
+  std::vector<long long> pr_node;
+  std::vector<uint8_t> pr_comp;
+  std::vector<double> pr_w;
+  ProbeD probes{};
+  bool probes_dirty = false;
   long long nf_sampled_since_flush = 0;
   long long nf_last_flush_step = 0;
 
@@ -783,6 +800,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   if (e->ade_kind == 2) k_ade_update<T, 2><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
   if (e->lumped.n > 0)
     k_lumped<T><<<blocks_for(e->lumped.n, 256), 256, 0, s>>>(e->lumped, fields, e->d_step);
+  if (e->ind.n > 0) k_inductor<T><<<blocks_for(e->ind.n, 256), 256, 0, s>>>(e->ind, fields);
   if (e->have_tfsf) {
     for (int g = 2; g < 4; ++g) {
       const auto& G = e->tfsf_groups[g];
@@ -796,6 +814,8 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     if (t % mv.d.interval == 0)
       k_movie<T><<<blocks_for(mv.n_nodes, 256), 256, 0, s>>>(mv.d, e->L, fields, e->d_step);
   }
+  if (e->probes.n_probes)
+    k_probes<T><<<e->probes.n_probes, 256, 0, s>>>(e->probes, fields, e->d_step);
   if (e->have_td)
     k_nf2ff_td<T><<<blocks_for(e->td.P, 256), 256, 0, s>>>(e->td, e->L, fields, e->d_step,
                                                           e->d_err);
@@ -863,6 +883,36 @@ xfd_status ensure_ready(xfd_engine* e) {
     e->xlayer_slabs = e->slabs.size();
     e->graph_dirty = true;
   }
+  if (e->probes_dirty) {
+    // Upload the probe lists (all probes in one launch per step).
+    ProbeD pd{};
+    pd.n_probes = (int)e->pr_begin.size() - 1;
+    pd.n_steps = e->n_steps;
+    long long *db = nullptr, *dn = nullptr;
+    uint8_t* dc = nullptr;
+    double* dw = nullptr;
+    xfd_status st;
+    if ((st = upload_raw(e, &db, e->pr_begin.data(), e->pr_begin.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dn, e->pr_node.data(), e->pr_node.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dc, e->pr_comp.data(), e->pr_comp.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dw, e->pr_w.data(), e->pr_w.size())) != XFD_OK) return st;
+    void* ser = nullptr;
+    if ((st = dev_alloc(e, &ser, (size_t)pd.n_probes * e->n_steps * sizeof(double))) != XFD_OK)
+      return st;
+    // keep the series recorded so far
+    if (e->probes.series && e->probes.n_probes)
+      CUDA_TRY(e, cudaMemcpyAsync(ser, e->probes.series,
+                                  (size_t)e->probes.n_probes * e->n_steps * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, e->stream));
+    pd.begin = db;
+    pd.node = dn;
+    pd.comp = dc;
+    pd.w = dw;
+    pd.series = static_cast<double*>(ser);
+    e->probes = pd;
+    e->probes_dirty = false;
+    e->graph_dirty = true;
+  }
   if (e->lumped_dirty) {
     // Concatenate the current sources into one device list.
     std::vector<long long> node;
@@ -897,6 +947,37 @@ xfd_status ensure_ready(xfd_engine* e) {
     d.wave = dw;
     e->lumped = d;
     e->lumped_dirty = false;
+  }
+  if (e->ind_dirty) {
+    // Concatenate the inductors; their current state starts at zero.
+    std::vector<long long> node;
+    std::vector<int> comp;
+    std::vector<double> cecjc, cjcec;
+    for (const auto& l : e->ind_h) {
+      node.insert(node.end(), l.node.begin(), l.node.end());
+      comp.insert(comp.end(), l.node.size(), l.comp);
+      cecjc.insert(cecjc.end(), l.cecjc.begin(), l.cecjc.end());
+      cjcec.insert(cjcec.end(), l.cjcec.begin(), l.cjcec.end());
+    }
+    InductorD d{};
+    d.n = (long long)node.size();
+    long long* dn = nullptr;
+    int* dc = nullptr;
+    double *da = nullptr, *db = nullptr, *dj = nullptr;
+    const std::vector<double> zero(node.size(), 0.0);
+    xfd_status st;
+    if ((st = upload_raw(e, &dn, node.data(), node.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dc, comp.data(), comp.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &da, cecjc.data(), cecjc.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &db, cjcec.data(), cjcec.size())) != XFD_OK) return st;
+    if ((st = upload_raw(e, &dj, zero.data(), zero.size())) != XFD_OK) return st;
+    d.node = dn;
+    d.comp = dc;
+    d.cecjc = da;
+    d.cjcec = db;
+    d.j = dj;
+    e->ind = d;
+    e->ind_dirty = false;
   }
   return XFD_OK;
 }
@@ -1400,6 +1481,32 @@ xfd_status xfd_add_current_source(xfd_engine* e, int32_t comp, const int32_t box
   return XFD_OK;
 }
 
+xfd_status xfd_add_inductor(xfd_engine* e, int32_t comp, const int32_t box_s[3],
+                            const int32_t box_e[3], const double* cecjc, const double* cjcec) {
+  if (!e || !box_s || !box_e || !cecjc || !cjcec || comp < 0 || comp > 2)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad inductor arguments");
+  if (e->ind.n > 0) return fail(e, XFD_ERR_STATE, "inductors are added before the first step");
+  int shp[3];
+  comp_shape(e->L, comp, shp);
+  for (int a = 0; a < 3; ++a)
+    if (box_s[a] < 0 || box_e[a] > shp[a] || box_e[a] <= box_s[a])
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "inductor box out of range on axis %d", a);
+  xfd_engine::InductorH l;
+  l.comp = comp;
+  long long q = 0;
+  for (int i = box_s[0]; i < box_e[0]; ++i)
+    for (int j = box_s[1]; j < box_e[1]; ++j)
+      for (int k = box_s[2]; k < box_e[2]; ++k, ++q) {
+        l.node.push_back(lat_index(e->L, i, j, k));
+        l.cecjc.push_back(cecjc[q]);
+        l.cjcec.push_back(cjcec[q]);
+      }
+  e->ind_h.push_back(std::move(l));
+  e->ind_dirty = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
 xfd_status xfd_set_ade(xfd_engine* e, const xfd_ade_desc* a) {
   if (!e || !a) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null ADE");
   if (a->kind < 0 || a->kind > 2 || a->n_poles <= 0 || a->n_materials <= 0 ||
@@ -1666,6 +1773,47 @@ xfd_status xfd_get_nf2ff_td(xfd_engine* e, double* out, int64_t capacity, int64_
   return XFD_OK;
 }
 
+xfd_status xfd_add_probe(xfd_engine* e, int64_t n, const int32_t* comp, const int32_t* node,
+                         const double* weight, int32_t* id) {
+  if (!e || n < 0 || (n > 0 && (!comp || !node || !weight)) || !id)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad probe arguments");
+  const int nn[3] = {e->L.nx, e->L.ny, e->L.nz};
+  for (int64_t q = 0; q < n; ++q) {
+    const int c = comp[q];
+    bool ok = c >= 0 && c <= 5;
+    for (int a = 0; a < 3 && ok; ++a) ok = node[3 * q + a] >= 0 && node[3 * q + a] <= nn[a];
+    if (!ok) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad probe entry %lld", (long long)q);
+  }
+  for (int64_t q = 0; q < n; ++q) {
+    e->pr_node.push_back(lat_index(e->L, node[3 * q], node[3 * q + 1], node[3 * q + 2]));
+    e->pr_comp.push_back((uint8_t)comp[q]);
+    e->pr_w.push_back(weight[q]);
+  }
+  e->pr_begin.push_back((long long)e->pr_node.size());
+  *id = (int32_t)e->pr_begin.size() - 2;
+  e->probes_dirty = true;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_get_probe(xfd_engine* e, int32_t id, double* out, int64_t capacity,
+                         int64_t* count) {
+  if (!e || !count || id < 0 || id >= (int32_t)e->pr_begin.size() - 1)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad probe id");
+  *count = e->n_steps;
+  if (!out) return XFD_OK;
+  if (capacity < *count) return fail(e, XFD_ERR_INVALID_ARGUMENT, "buffer too small");
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  if (!e->probes.series || id >= e->probes.n_probes) {
+    std::fill(out, out + *count, 0.0);
+    return XFD_OK;
+  }
+  CUDA_TRY(e, cudaMemcpyAsync(out, e->probes.series + (size_t)id * e->n_steps,
+                              (size_t)*count * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  return XFD_OK;
+}
+
 xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* count) {
   if (!e || !e->have_nf2ff) return fail(e, XFD_ERR_STATE, "no NF2FF");
   CUDA_TRY(e, cudaSetDevice(e->device));
@@ -1890,8 +2038,10 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (e->have_tfsf) n += fused ? 2 : 4;
   if (e->ade_kind >= 0) n += fused ? 1 : 2;
   if (!e->lumped_h.empty()) n += 1;
+  if (!e->ind_h.empty()) n += 1;
   if (e->have_nf2ff) n += 1;
   if (e->have_td) n += 1;
+  if (e->probes.n_probes) n += 1;
   if (e->n_ovr) n += fused ? 1 : 2;
   return n + e->n_rec;
 }

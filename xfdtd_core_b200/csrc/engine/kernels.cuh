@@ -423,6 +423,33 @@ __global__ void k_lumped(LumpedD lp, T* const* fields, const long long* step) {
 }
 
 // ---------------------------------------------------------------------------
+// Lumped inductors on their compacted node list (InductorCorrector::correctE,
+// src/object/lumped_element/lumped_element_corrrector.cpp:42-99): after the E
+// update, E += cecjc * J, then J += cjcec * E with the corrected E.  J is an
+// FP64 state in both precisions; in FP32 it advances with the stored E.
+// ---------------------------------------------------------------------------
+struct InductorD {
+  long long n;
+  const long long* node;
+  const int* comp;
+  const double* cecjc;
+  const double* cjcec;
+  double* j;
+};
+
+template <typename T>
+__global__ void k_inductor(InductorD d, T* const* fields) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= d.n) return;
+  T* E = fields[d.comp[q]];
+  const long long id = d.node[q];
+  const double jq = d.j[q];
+  const T en = (T)((double)E[id] + d.cecjc[q] * jq);
+  E[id] = en;
+  d.j[q] = jq + d.cjcec[q] * (double)en;
+}
+
+// ---------------------------------------------------------------------------
 // ADE on the compacted dispersive node list.  The E sweep has already
 // written the plain Yee value with the ADE-overwritten (ca, cb) of the node;
 // k_ade_update adds the polarisation terms and advances J
@@ -786,6 +813,40 @@ __global__ void k_nf2ff_td(Nf2ffTdD td, Lat L, T* const* fields, const long long
   const double xh = (td.delay[p] + 0.0) + t;
   td_add(td.pot + A * td.n_bins, td.n_bins, xh, -sg, ds, dhb, err);
   td_add(td.pot + B * td.n_bins, td.n_bins, xh, sg, ds, dha, err);
+}
+
+// ---------------------------------------------------------------------------
+// Weighted probes: per probe and step, value = sum_q w[q] F_{comp[q]}(node q),
+// one CTA per probe (FP64 block reduction), written to series[probe][t]
+// (VoltageMonitor::update, src/monitor/voltage_monitor.cpp:198-235;
+// CurrentMonitor::update, src/monitor/current_monitor.cpp:253-379).
+// ---------------------------------------------------------------------------
+struct ProbeD {
+  int n_probes;
+  const long long* begin;  // n_probes + 1 entry offsets
+  const long long* node;   // lattice index
+  const uint8_t* comp;     // 0..5
+  const double* w;
+  double* series;          // n_probes x n_steps
+  long long n_steps;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_probes(ProbeD pr, T* const* fields, const long long* step) {
+  const int q = blockIdx.x;
+  double acc = 0.0;
+  for (long long e = pr.begin[q] + threadIdx.x; e < pr.begin[q + 1]; e += blockDim.x)
+    acc += pr.w[e] * (double)fields[pr.comp[e]][pr.node[e]];
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) v += red[wi];
+    const long long t = *step;
+    if (t >= 0 && t < pr.n_steps) pr.series[(long long)q * pr.n_steps + t] = v;
+  }
 }
 
 __global__ void k_advance(long long* step) { *step += 1; }

@@ -114,6 +114,8 @@ struct xfdtd_scene {
   std::unique_ptr<Simulation> sim;
   std::vector<std::shared_ptr<MovieMonitor>> movies;
   std::vector<std::shared_ptr<FieldTimeMonitor>> probes;
+  std::vector<std::shared_ptr<VoltageMonitor>> voltages;
+  std::vector<std::shared_ptr<CurrentMonitor>> currents;
   std::shared_ptr<NFFFTFrequencyDomain> nf2ff;
   std::shared_ptr<NFFFTTimeDomain> nf2ff_td;
   int64_t steps = 0;
@@ -187,6 +189,22 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       sc->sim->addObject(std::make_shared<VoxelObject>(
           name, std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), dims,
           std::move(eps), mu_r, sigma_e));
+    } else if (kw == "voltage_monitor" || kw == "current_monitor") {
+      in >> name;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      std::string dir;
+      in >> dir;
+      auto cube = std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz});
+      if (kw == "voltage_monitor") {
+        auto m = std::make_shared<VoltageMonitor>(name, std::move(cube), parseDir(dir));
+        sc->voltages.push_back(m);
+        sc->sim->addMonitor(m);
+      } else {
+        auto m = std::make_shared<CurrentMonitor>(name, std::move(cube), parseDir(dir));
+        sc->currents.push_back(m);
+        sc->sim->addMonitor(m);
+      }
     } else if (kw == "current_source") {
       in >> name;
       const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
@@ -486,6 +504,39 @@ int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir) {
     if (s->nf2ff_td) {
       s->nf2ff_td->setOutputDir((root / "nf2ff_td").string());
       s->nf2ff_td->processFarField();
+    }
+    for (const auto& m : s->voltages) {
+      m->setOutputDir((root / "monitors").string());
+      m->output();
+    }
+    for (const auto& m : s->currents) {
+      m->setOutputDir((root / "monitors").string());
+      m->output();
+    }
+  })
+}
+
+int xfdtd_scene_line_monitor(xfdtd_scene* s, int32_t kind, int32_t index, double* out,
+                             int64_t capacity, int64_t* count) {
+  HOST_TRY({
+    if (!s || !count) throw XFDTDException("null argument");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    const std::vector<Real>* t = nullptr;
+    const std::vector<Real>* d = nullptr;
+    if (kind == 0 && index >= 0 && index < (int32_t)s->voltages.size()) {
+      t = &s->voltages[(std::size_t)index]->time();
+      d = &s->voltages[(std::size_t)index]->data();
+    } else if (kind == 1 && index >= 0 && index < (int32_t)s->currents.size()) {
+      t = &s->currents[(std::size_t)index]->time();
+      d = &s->currents[(std::size_t)index]->data();
+    } else {
+      throw XFDTDException("no such voltage/current monitor");
+    }
+    *count = (int64_t)(t->size() + d->size());
+    if (out) {
+      if (capacity < *count) throw XFDTDException("buffer too small");
+      std::copy(t->begin(), t->end(), out);
+      std::copy(d->begin(), d->end(), out + t->size());
     }
   })
 }

@@ -1045,6 +1045,28 @@ void Simulation::init(Index time_step) {
                        (std::size_t)(h.e[2] - h.s[2])});
     I.movies.push_back(h);
   }
+  // Voltage and current monitors as weighted probes.
+  for (const auto& mon : _monitors) {
+    if (auto vm = std::dynamic_pointer_cast<VoltageMonitor>(mon)) {
+      std::vector<int32_t> comp, node;
+      std::vector<double> w;
+      voltageProbe(*vm, comp, node, w);
+      checkStatus(E, xfd_add_probe(E, (int64_t)comp.size(), comp.data(), node.data(), w.data(),
+                                   &vm->_probe),
+                  "xfd_add_probe");
+      vm->_time = linspace((0 + 1) * dt, (0 + _steps) * dt, _steps);
+      vm->_data.assign(_steps, 0.0);
+    } else if (auto cm = std::dynamic_pointer_cast<CurrentMonitor>(mon)) {
+      std::vector<int32_t> comp, node;
+      std::vector<double> w;
+      currentProbe(*cm, comp, node, w);
+      checkStatus(E, xfd_add_probe(E, (int64_t)comp.size(), comp.data(), node.data(), w.data(),
+                                   &cm->_probe),
+                  "xfd_add_probe");
+      cm->_time = linspace((0 + 0.5) * dt, (0 + _steps + 0.5) * dt, _steps);
+      cm->_data.assign(_steps, 0.0);
+    }
+  }
   // Field time monitors: the last node of the shifted box, every step.
   for (const auto& mon : _monitors) {
     auto ft = std::dynamic_pointer_cast<FieldTimeMonitor>(mon);
@@ -1136,6 +1158,22 @@ void Simulation::finish() {
     for (int64_t f = 0; f < frames && f < (int64_t)d.size(); ++f)
       d[f] = (w == 8) ? reinterpret_cast<double*>(buf.data())[f]
                       : reinterpret_cast<float*>(buf.data())[f];
+  }
+  for (const auto& mon : _monitors) {
+    std::vector<Real>* d = nullptr;
+    int id = -1;
+    if (auto vm = std::dynamic_pointer_cast<VoltageMonitor>(mon)) {
+      d = &vm->_data;
+      id = vm->_probe;
+    } else if (auto cm = std::dynamic_pointer_cast<CurrentMonitor>(mon)) {
+      d = &cm->_data;
+      id = cm->_probe;
+    }
+    if (!d || id < 0) continue;
+    int64_t cnt = 0;
+    checkStatus(_engine, xfd_get_probe(_engine, id, nullptr, 0, &cnt), "probe");
+    d->assign((std::size_t)cnt, 0.0);
+    checkStatus(_engine, xfd_get_probe(_engine, id, d->data(), cnt, &cnt), "probe");
   }
   if (!_nffts_td.empty()) {
     int64_t cnt = 0;
@@ -1511,6 +1549,151 @@ static void huygensFaces(const Index n[3], const std::array<Index, 3>& d, int s_
       e_out[face][a] = valid ? e[a] : 0;
     }
   }
+}
+
+// ---------------------------------------------------------------- probes
+namespace {
+struct IRange {
+  long long s, e;
+  bool valid() const { return s < e; }
+};
+}  // namespace
+
+// VoltageMonitor::init (src/monitor/voltage_monitor.cpp:17-180), one domain
+// (node task = global task, lower corner 0, upper corner n): the a and b
+// ranges of the cube's grid box extended by one node and kept off the domain
+// edges, the c range as is; weight -h_c / (na nb) per node, negated for a
+// negative direction (coff, :150-180).
+void Simulation::voltageProbe(const VoltageMonitor& m, std::vector<int32_t>& comp,
+                              std::vector<int32_t>& node, std::vector<double>& w) const {
+  const Impl& I = *_impl;
+  const int c = Axis::axisOf(m.direction()), a = (c + 1) % 3, b = (c + 2) % 3;
+  long long o[3], e[3];
+  for (int q = 0; q < 3; ++q) {
+    o[q] = (long long)nearestNode(I.e_node[q], m.cube()->origin()(q));
+    e[q] = (long long)nearestNode(I.e_node[q], m.cube()->end()(q));
+  }
+  auto clamp = [&](int ax, IRange r) {
+    if (r.s <= 0) r.s = 1;
+    if ((long long)_n[ax] <= r.e) r.e = (long long)_n[ax] - 1;
+    return r;
+  };
+  IRange r[3];
+  r[a] = clamp(a, IRange{o[a], e[a] + 1});
+  r[b] = clamp(b, IRange{o[b], e[b] + 1});
+  r[c] = IRange{o[c], e[c]};
+  if (!r[0].valid() || !r[1].valid() || !r[2].valid())
+    throw XFDTDException(m.name() + " globalTask is not valid");
+  const long long nab = (r[a].e - r[a].s) * (r[b].e - r[b].s);
+  for (long long i = r[0].s; i < r[0].e; ++i)
+    for (long long j = r[1].s; j < r[1].e; ++j)
+      for (long long k = r[2].s; k < r[2].e; ++k) {
+        const long long x[3] = {i, j, k};
+        double coff = -I.h_size[c][(std::size_t)x[c]] / (double)(std::size_t)nab;
+        if (Axis::negative(m.direction())) coff *= -1.0;
+        comp.push_back(c);
+        node.push_back((int32_t)i);
+        node.push_back((int32_t)j);
+        node.push_back((int32_t)k);
+        w.push_back(coff);
+      }
+}
+
+// CurrentMonitor::init / update (src/monitor/current_monitor.cpp:17-379), one
+// domain: the loop of H around the cube's face on its last node plane along
+// the direction c, sides kept off the domain edges (make_ranges, :128-150).
+void Simulation::currentProbe(const CurrentMonitor& m, std::vector<int32_t>& comp,
+                              std::vector<int32_t>& node, std::vector<double>& w) const {
+  const Impl& I = *_impl;
+  const int c = Axis::axisOf(m.direction()), a = (c + 1) % 3, b = (c + 2) % 3;
+  long long o[3], e[3];
+  for (int q = 0; q < 3; ++q) {
+    o[q] = (long long)nearestNode(I.e_node[q], m.cube()->origin()(q));
+    e[q] = (long long)nearestNode(I.e_node[q], m.cube()->end()(q));
+  }
+  const long long n[3] = {(long long)_n[0], (long long)_n[1], (long long)_n[2]};
+  if (e[c] == 0) throw XFDTDException("CurrentMonitor::init(): global_c_e is 0");
+  if (o[a] == 0 || e[a] == n[a] || o[b] == 0 || e[b] == n[b])
+    throw XFDTDException("CurrentMonitor::init(): global range is invalid");
+  long long lo[3], hi[3];  // node task
+  lo[a] = o[a];
+  hi[a] = e[a];
+  lo[b] = o[b];
+  hi[b] = e[b];
+  lo[c] = e[c] - 1;
+  hi[c] = e[c];
+  auto make_ranges = [](long long b_start, long long b_end, long long n_b, long long n_a,
+                        long long start, long long end) {
+    if (start <= 0) start = 1;
+    end = end + 1;
+    if (n_a <= end) end = n_a - 1;
+    IRange rn{0, 0}, rp{0, 0};
+    if (b_start != 0 && b_start != n_b - 1 && b_start != n_b) rn = IRange{start, end};
+    if (b_end != n_b && b_end != n_b - 1 && b_end != 0) rp = IRange{start, end};
+    return std::pair<IRange, IRange>{rn, rp};
+  };
+  const auto [ha_bn, ha_bp] = make_ranges(lo[b], hi[b], n[b], n[a], lo[a], hi[a]);
+  const auto [hb_an, hb_ap] = make_ranges(lo[a], hi[a], n[a], n[b], lo[b], hi[b]);
+  const double positive = Axis::negative(m.direction()) ? -1.0 : 1.0;
+  // H_a along a at b = lo_b - 1 (+) and b = hi_b (-); H_b along b at
+  // a = lo_a - 1 (-) and a = hi_a (+); all on the plane c = hi_c - 1.
+  auto add = [&](int comp_axis, long long x[3], double weight) {
+    comp.push_back(3 + comp_axis);
+    for (int q = 0; q < 3; ++q) node.push_back((int32_t)x[q]);
+    w.push_back(positive * weight);
+  };
+  long long x[3];
+  x[c] = hi[c] - 1;
+  for (long long v = ha_bn.s; ha_bn.valid() && v < ha_bn.e; ++v) {
+    x[a] = v;
+    x[b] = lo[b] - 1;
+    add(a, x, I.e_size[a][(std::size_t)v]);
+  }
+  for (long long v = ha_bp.s; ha_bp.valid() && v < ha_bp.e; ++v) {
+    x[a] = v;
+    x[b] = hi[b];
+    add(a, x, -I.e_size[a][(std::size_t)v]);
+  }
+  for (long long v = hb_an.s; hb_an.valid() && v < hb_an.e; ++v) {
+    x[b] = v;
+    x[a] = lo[a] - 1;
+    add(b, x, -I.e_size[b][(std::size_t)v]);
+  }
+  for (long long v = hb_ap.s; hb_ap.valid() && v < hb_ap.e; ++v) {
+    x[b] = v;
+    x[a] = hi[a];
+    add(b, x, I.e_size[b][(std::size_t)v]);
+  }
+}
+
+namespace {
+void writeTimeNpy(const std::string& dir, const std::string& name, const std::vector<Real>& t,
+                  const std::vector<Real>& d) {
+  namespace fs = std::filesystem;
+  const fs::path root(dir.empty() ? "." : dir);
+  fs::create_directories(root);
+  std::ostringstream hdr;
+  hdr << "{'descr': '<f8', 'fortran_order': False, 'shape': (2, " << t.size() << "), }";
+  std::string h = hdr.str();
+  const std::size_t total = 10 + h.size() + 1;
+  h.append((64 - total % 64) % 64, ' ');
+  h.push_back('\n');
+  std::ofstream f((root / (name + ".npy")).string(), std::ios::binary);
+  if (!f) throw XFDTDException("cannot write " + name + ".npy");
+  f.write("\x93NUMPY\x01\x00", 8);
+  const uint16_t len = static_cast<uint16_t>(h.size());
+  f.write(reinterpret_cast<const char*>(&len), 2);
+  f.write(h.data(), (std::streamsize)h.size());
+  f.write(reinterpret_cast<const char*>(t.data()), (std::streamsize)(t.size() * sizeof(Real)));
+  f.write(reinterpret_cast<const char*>(d.data()), (std::streamsize)(d.size() * sizeof(Real)));
+}
+}  // namespace
+
+void VoltageMonitor::output() const {
+  if (_probe >= 0) writeTimeNpy(outputDir(), name(), _time, _data);
+}
+void CurrentMonitor::output() const {
+  if (_probe >= 0) writeTimeNpy(outputDir(), name(), _time, _data);
 }
 
 // NFFFTTimeDomain::initTimeDependentVariable / distanceRange and the per-point

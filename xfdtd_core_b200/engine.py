@@ -102,6 +102,7 @@ def load(build_if_missing: bool = True):
         "xfd_add_cpml": ([vp, ctypes.POINTER(CpmlSlab)], ctypes.c_int),
         "xfd_set_tfsf": ([vp, ctypes.POINTER(TfsfDesc)], ctypes.c_int),
         "xfd_add_current_source": ([vp, _i32, _i32 * 3, _i32 * 3, _dp, _dp], ctypes.c_int),
+        "xfd_add_inductor": ([vp, _i32, _i32 * 3, _i32 * 3, _dp, _dp], ctypes.c_int),
         "xfd_set_ade": ([vp, ctypes.POINTER(AdeDesc)], ctypes.c_int),
         "xfd_set_nf2ff": ([vp, ctypes.POINTER(Nf2ffDesc)], ctypes.c_int),
         "xfd_get_nf2ff": ([vp, _dp, _i64, ctypes.POINTER(_i64)], ctypes.c_int),
@@ -153,6 +154,7 @@ def exported_symbols() -> List[str]:
     """Names declared in include/xfd_engine.h that the library must export."""
     return ["xfd_create", "xfd_destroy", "xfd_last_error", "xfd_set_material_classes",
             "xfd_set_curl_factors", "xfd_add_cpml", "xfd_set_tfsf", "xfd_add_current_source",
+            "xfd_add_inductor",
             "xfd_set_ade", "xfd_set_nf2ff", "xfd_get_nf2ff", "xfd_add_movie",
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
@@ -160,6 +162,7 @@ def exported_symbols() -> List[str]:
             "xfd_launches_per_step", "xfd_stencil_bytes_per_step", "xfd_set_e_overrides",
             "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
             "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_set_nf2ff_td", "xfd_get_nf2ff_td",
+            "xfd_add_probe", "xfd_get_probe",
             "xfd_batch_create",
             "xfd_batch_destroy", "xfd_batch_last_error", "xfd_batch_run", "xfd_batch_sync",
             "xfd_batch_set_option", "xfd_batch_get_option", "xfd_batch_tuning",
@@ -258,6 +261,12 @@ class Engine:
         self._check(self.L.xfd_add_current_source(
             self.h, comp, (_i32 * 3)(*box_s), (_i32 * 3)(*box_e), _p(coff), _p(waveform)),
             "add_current_source")
+
+    def add_inductor(self, comp: int, box_s, box_e, cecjc, cjcec):
+        cecjc, cjcec = _f64(cecjc), _f64(cjcec)
+        self._check(self.L.xfd_add_inductor(
+            self.h, comp, (_i32 * 3)(*box_s), (_i32 * 3)(*box_e), _p(cecjc), _p(cjcec)),
+            "add_inductor")
 
     def set_ade(self, kind: int, n_poles: int, mat_coeff: np.ndarray, comp: np.ndarray,
                 node: np.ndarray, material: np.ndarray):

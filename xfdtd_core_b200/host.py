@@ -58,6 +58,7 @@ def load():
         "xfdtd_scene_dft_objective": ([vp, i64, i32, i32 * 3, i32 * 3, ctypes.c_double, i32, i32,
                                        _dp, _dp, i64], ctypes.c_int),
         "xfdtd_scene_nf2ff_td": ([vp, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "xfdtd_scene_line_monitor": ([vp, i32, i32, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -73,7 +74,8 @@ def exported_symbols() -> List[str]:
             "xfdtd_scene_advance", "xfdtd_scene_tfsf", "xfdtd_scene_finish",
             "xfdtd_scene_coefficients", "xfdtd_scene_field", "xfdtd_scene_movie",
             "xfdtd_scene_nf2ff", "xfdtd_scene_far_field", "xfdtd_scene_field_time",
-            "xfdtd_scene_write_outputs", "xfdtd_scene_dft_objective", "xfdtd_scene_nf2ff_td"]
+            "xfdtd_scene_write_outputs", "xfdtd_scene_dft_objective", "xfdtd_scene_nf2ff_td",
+            "xfdtd_scene_line_monitor"]
 
 
 class SceneRun:
@@ -239,6 +241,17 @@ class SceneRun:
             self.h, int(n_steps), field, bs, be, float(freq), voxel_object, checkpoint_interval,
             ctypes.byref(J), g.ctypes.data_as(_dp), g.size))
         return J.value, g
+
+    def line_monitor(self, kind: str, index: int = 0) -> np.ndarray:
+        """[time; data] (2 x n_steps) of voltage (kind "voltage") or current
+        monitor number `index`."""
+        k = {"voltage": 0, "current": 1}[kind]
+        cnt = ctypes.c_int64()
+        self._check(self.L.xfdtd_scene_line_monitor(self.h, k, index, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value)
+        self._check(self.L.xfdtd_scene_line_monitor(self.h, k, index, out.ctypes.data_as(_dp),
+                                                    cnt.value, ctypes.byref(cnt)))
+        return out.reshape(2, -1)
 
     def nf2ff_td(self) -> dict:
         """Time-domain NF2FF far-field series (w_theta, w_phi, u_theta, u_phi)."""

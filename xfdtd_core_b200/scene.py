@@ -278,6 +278,21 @@ class NF2FFSpec:
 
 
 @dataclass
+class LineMonitorSpec:
+    """VoltageMonitor / CurrentMonitor(name, cube, direction): `kind` is
+    "voltage" or "current"."""
+    kind: str
+    name: str
+    shape: Shape  # Cube
+    direction: str
+
+    def text(self) -> str:
+        o, s = self.shape.origin, self.shape.size
+        return (f"{self.kind}_monitor {self.name} " + " ".join(_f(v) for v in (*o, *s)) +
+                f" {self.direction}")
+
+
+@dataclass
 class NF2FFTDSpec:
     """NFFFTTimeDomain(distance_x, distance_y, distance_z, theta, phi)."""
     distance: Tuple[int, int, int]
@@ -302,6 +317,7 @@ class Scene:
     tfsf: Optional[TFSFSpec] = None
     movies: List[MovieSpec] = field(default_factory=list)
     field_times: List[FieldTimeSpec] = field(default_factory=list)
+    line_monitors: List[LineMonitorSpec] = field(default_factory=list)
     nf2ff: Optional[NF2FFSpec] = None
     nf2ff_td: Optional[NF2FFTDSpec] = None
     name: str = "scene"
@@ -317,6 +333,7 @@ class Scene:
             lines.append(self.tfsf.text())
         lines += [m.text() for m in self.movies]
         lines += [m.text() for m in self.field_times]
+        lines += [m.text() for m in self.line_monitors]
         if self.nf2ff is not None:
             lines.append(self.nf2ff.text())
         if self.nf2ff_td is not None:
