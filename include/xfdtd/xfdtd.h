@@ -321,15 +321,32 @@ class VoxelObject : public Object {
   Real _mu_r, _sigma_e;
 };
 
+/// Lumped element on a Cube of E nodes along one axis
+/// (include/xfdtd/object/lumped_element/lumped_element.h:19-104): the E_xyz
+/// nodes of the Cube's grid box, its end included on the two other axes.
+/// Elements change their nodes' E coefficients in the order they were added
+/// (the last one on a node wins, each computed from the node's material).
+class LumpedElement : public Object {
+ public:
+  LumpedElement(std::string name, std::unique_ptr<Cube> cube, Axis::XYZ xyz,
+                std::unique_ptr<Material> material = Material::createAir())
+      : Object{std::move(name), std::move(cube), std::move(material)}, _xyz{xyz} {}
+  Axis::XYZ xyz() const { return _xyz; }
+
+ private:
+  Axis::XYZ _xyz;
+};
+
 /// Lumped current source on a Cube of E nodes along its direction
 /// (src/object/lumped_element/current_source.cpp).  Resistance 0 becomes 1e-20;
 /// an infinite resistance leaves the E coefficients unchanged (beta = 0).
-class CurrentSource : public Object {
+class CurrentSource : public LumpedElement {
  public:
   CurrentSource(std::string name, std::unique_ptr<Cube> cube, Axis::Direction direction,
                 Real resistance, std::unique_ptr<Waveform> waveform,
                 std::unique_ptr<Material> material = Material::createAir())
-      : Object{std::move(name), std::move(cube), std::move(material)},
+      : LumpedElement{std::move(name), std::move(cube),
+                      static_cast<Axis::XYZ>(Axis::axisOf(direction)), std::move(material)},
         _direction{direction},
         _resistance{resistance == 0 ? 1e-20 : resistance},
         _waveform{std::move(waveform)} {}
@@ -341,6 +358,73 @@ class CurrentSource : public Object {
   Axis::Direction _direction;
   Real _resistance;
   std::unique_ptr<Waveform> _waveform;
+};
+
+/// Lumped voltage source with an internal resistance
+/// (src/object/lumped_element/voltage_source.cpp:15-177): the amplitude is
+/// split over the nodes along the axis, the resistance over the node count.
+/// Resistance 0 becomes 1e-20.
+class VoltageSource : public LumpedElement {
+ public:
+  VoltageSource(std::string name, std::unique_ptr<Cube> cube, Axis::Direction direction,
+                Real resistance, std::unique_ptr<Waveform> waveform,
+                std::unique_ptr<Material> material = Material::createAir())
+      : LumpedElement{std::move(name), std::move(cube),
+                      static_cast<Axis::XYZ>(Axis::axisOf(direction)), std::move(material)},
+        _direction{direction},
+        _resistance{resistance == 0 ? 1e-20 : resistance},
+        _waveform{std::move(waveform)} {}
+  Axis::Direction direction() const { return _direction; }
+  Real resistance() const { return _resistance; }
+  const std::unique_ptr<Waveform>& waveform() const { return _waveform; }
+
+ private:
+  Axis::Direction _direction;
+  Real _resistance;
+  std::unique_ptr<Waveform> _waveform;
+};
+
+/// Lumped resistor (src/object/lumped_element/resistor.cpp:12-131): E
+/// coefficients only.  Resistance 0 becomes 1e-10.
+class Resistor : public LumpedElement {
+ public:
+  Resistor(std::string name, std::unique_ptr<Cube> cube, Axis::XYZ xyz, Real resistance,
+           std::unique_ptr<Material> material = Material::createAir())
+      : LumpedElement{std::move(name), std::move(cube), xyz, std::move(material)},
+        _resistance{resistance == 0 ? 1e-10 : resistance} {}
+  Real resistance() const { return _resistance; }
+
+ private:
+  Real _resistance;
+};
+
+/// Lumped capacitor (src/object/lumped_element/capacitor.cpp:8-116): E
+/// coefficients only.
+class Capacitor : public LumpedElement {
+ public:
+  Capacitor(std::string name, std::unique_ptr<Cube> cube, Axis::XYZ xyz, Real capacitance,
+            std::unique_ptr<Material> material = Material::createAir())
+      : LumpedElement{std::move(name), std::move(cube), xyz, std::move(material)},
+        _capacitance{capacitance} {}
+  Real capacitance() const { return _capacitance; }
+
+ private:
+  Real _capacitance;
+};
+
+/// Lumped inductor (src/object/lumped_element/inductor.cpp:12-137): a
+/// current state per node, advanced after every E update.  Inductance 0
+/// becomes 1e-10.
+class Inductor : public LumpedElement {
+ public:
+  Inductor(std::string name, std::unique_ptr<Cube> cube, Axis::XYZ xyz, Real inductance,
+           std::unique_ptr<Material> material = Material::createAir())
+      : LumpedElement{std::move(name), std::move(cube), xyz, std::move(material)},
+        _inductance{inductance == 0 ? 1e-10 : inductance} {}
+  Real inductance() const { return _inductance; }
+
+ private:
+  Real _inductance;
 };
 
 // --------------------------------------------------------------- boundary

@@ -119,7 +119,7 @@ class _Tfsf(ctypes.Structure):
 
 class _Lumped(ctypes.Structure):
     _fields_ = [("comp", ctypes.c_int), ("s", _i64 * 3), ("e", _i64 * 3), ("coff", _dp),
-                ("wave", _dp)]
+                ("wave", _dp), ("cecjc", _dp), ("j", _dp)]
 
 
 class _Nf2ff(ctypes.Structure):
@@ -247,7 +247,8 @@ class RefSimulation:
     def _grid(self):
         sc = self.scene
         dx, dy, dz = sc.dl
-        shapes = [o.shape for o in sc.objects] + [c.shape for c in sc.current_sources]
+        shapes = [o.shape for o in sc.objects] + [c.shape for c in sc.current_sources] + \
+            [c.shape for c in getattr(sc, "lumped_elements", [])]
         lo = np.full(3, np.finfo(np.float64).max)
         hi = np.full(3, np.finfo(np.float64).min)
         for s in shapes:  # Shape::makeWrappedCube (src/shape/shape.cpp:8-38)
@@ -324,8 +325,9 @@ class RefSimulation:
         painters = [(o.shape, o.material) for o in self.scene.objects]
         voxels = [o if hasattr(o, "voxel_index") else None for o in self.scene.objects]
         from_air = __import__("xfdtd_core_b200.scene", fromlist=["air"]).air
-        painters += [(c.shape, from_air()) for c in self.scene.current_sources]
-        voxels += [None] * len(self.scene.current_sources)
+        lumped = list(self.scene.current_sources) + list(getattr(self.scene, "lumped_elements", []))
+        painters += [(c.shape, from_air()) for c in lumped]
+        voxels += [None] * len(lumped)
         # Simulation::correctMaterialSpace (src/simulation/simulation.cpp:608-636)
         # -> Object::defaultCorrectMaterialSpace (src/object/object.cpp:114-198)
         for index, (shape, mat) in enumerate(painters):
@@ -440,40 +442,78 @@ class RefSimulation:
 
     # ------------------------------------------------------- current sources
     def _current_sources(self):
-        """CurrentSource::init/correctUpdateCoefficient/initTimeDependentVariable
-        (src/object/lumped_element/current_source.cpp:43-165)."""
+        """Lumped elements in object order (current and voltage sources, then
+        resistors, capacitors, inductors): ::init and ::correctUpdateCoefficient
+        of src/object/lumped_element/current_source.cpp:40-165,
+        voltage_source.cpp:47-163, resistor.cpp:27-127, capacitor.cpp:16-112,
+        inductor.cpp:23-105, computed from the eps / sigma arrays."""
         self.lumped = []
         dt = self.dt
-        for cs in self.scene.current_sources:
-            axis, neg = DIR[cs.direction]
-            o, e = self.grid_box(cs.shape)
+        elements = list(self.scene.current_sources) + \
+            list(getattr(self.scene, "lumped_elements", []))
+        for el in elements:
+            kind = getattr(el, "kind", "current")
+            if kind in ("current", "voltage"):
+                axis, neg = DIR[el.direction]
+            else:
+                axis, neg = "XYZ".index(el.axis), False
+            o, e = self.grid_box(el.shape)
             # LumpedElement::rangeX/Y/Z (include/xfdtd/object/lumped_element/lumped_element.h:79-104)
             s = list(o)
             en = [e[a] if a == axis else e[a] + 1 for a in range(3)]
             size = [e[a] - o[a] for a in range(3)]
             A, B = tan_a(axis), tan_b(axis)
-            r = cs.resistance if cs.resistance != 0 else 1e-20
             na, nb, nc = size[A] + 1, size[B] + 1, size[axis]
-            res_factor = r * na * nb / nc
-            amp = cs.waveform.amplitude / (na * nb)
-            if neg:
-                amp *= -1
             sizes = [self.h_size[0], self.h_size[1], self.h_size[2]]
             sizes[axis] = self.e_size[axis]
             sl = [slice(s[a], en[a]) for a in range(3)]
             g = np.meshgrid(sizes[0][sl[0]], sizes[1][sl[1]], sizes[2][sl[2]], indexing="ij")
             d_a, d_b, d_c = g[A], g[B], g[axis]
-            beta = (dt * d_c) / (res_factor * d_a * d_b)
             eps = self.eps_arr[axis][sl[0], sl[1], sl[2]]
             sig = self.sig_e_arr[axis][sl[0], sl[1], sl[2]]
-            self.ce[axis][sl[0], sl[1], sl[2]] = (2 * eps - dt * sig - beta) / (
+            if kind == "inductor":
+                ind = el.value if el.value != 0 else 1e-10
+                ind_factor = ind * na * nb / nc
+                self.lumped.append({
+                    "comp": axis, "s": s, "e": en,
+                    "coff": np.ascontiguousarray(dt * d_c / (ind_factor * d_a * d_b)),
+                    "cecjc": np.ascontiguousarray(-(2 * dt) / (2 * eps + dt * sig)),
+                    "j": np.zeros(d_c.shape)})
+                continue
+            sign = 1.0
+            if kind == "capacitor":
+                cap_factor = el.value * nc / (nc * nb)
+                beta = 2 * cap_factor * d_c / (d_a * d_b)
+                sign = -1.0
+            else:
+                r = el.resistance if kind in ("current", "voltage") else el.value
+                if r == 0:
+                    r = 1e-10 if kind == "resistor" else 1e-20
+                res_factor = r * na * nb / nc
+                if kind == "voltage":
+                    alpha = d_a * d_b * res_factor
+                    beta = dt * d_c / alpha
+                else:
+                    beta = (dt * d_c) / (res_factor * d_a * d_b)
+            self.ce[axis][sl[0], sl[1], sl[2]] = (2 * eps - dt * sig - sign * beta) / (
                 2 * eps + dt * sig + beta)
             self.ceh_a[axis][sl[0], sl[1], sl[2]] = -2 * dt / ((2 * eps + dt * sig + beta) * d_b)
             self.ceh_b[axis][sl[0], sl[1], sl[2]] = 2 * dt / ((2 * eps + dt * sig + beta) * d_a)
-            coff = -2 * dt / ((2 * eps + dt * sig + beta) * (d_b * d_a)) * amp
+            if kind == "current":
+                amp = el.waveform.amplitude / (na * nb)
+                if neg:
+                    amp *= -1
+                coff = -2 * dt / ((2 * eps + dt * sig + beta) * (d_b * d_a)) * amp
+            elif kind == "voltage":
+                amp = el.waveform.amplitude / nc
+                if neg:
+                    amp *= -1
+                coff = -2 * dt / ((2 * eps + dt * sig + beta) * alpha) * amp
+            else:
+                continue
             self.lumped.append({"comp": axis, "s": s, "e": en,
                                 "coff": np.ascontiguousarray(coff, dtype=np.float64),
-                                "waveform": cs.waveform})
+                                "waveform": el.waveform})
 
     # ---------------------------------------------------------------- CPML
     def _pml(self):
@@ -1140,8 +1180,9 @@ class RefSimulation:
         self._monitors()
         nt = self.scene.steps
         h_time = linspace((0 + 0.5) * self.dt, (0 + nt + 0.5) * self.dt, nt)
-        for l in self.lumped:  # CurrentSource::initTimeDependentVariable
-            l["wave"] = np.ascontiguousarray(l["waveform"](h_time))
+        for l in self.lumped:  # CurrentSource / VoltageSource ::initTimeDependentVariable
+            if "waveform" in l:
+                l["wave"] = np.ascontiguousarray(l["waveform"](h_time))
         self._bind()
         self.t = 0
 
@@ -1209,7 +1250,11 @@ class RefSimulation:
             s.comp = l["comp"]
             for d in range(3):
                 s.s[d], s.e[d] = l["s"][d], l["e"][d]
-            s.coff, s.wave = _ptr(l["coff"]), _ptr(l["wave"])
+            s.coff = _ptr(l["coff"])
+            if "j" in l:
+                s.cecjc, s.j = _ptr(l["cecjc"]), _ptr(l["j"])
+            else:
+                s.wave = _ptr(l["wave"])
         k.append(lums)
         sim.lumped = ctypes.cast(lums, ctypes.POINTER(_Lumped))
         sim.n_lumped = len(self.lumped)

@@ -423,26 +423,37 @@ void orc_tfsf_correct(const orc_yee *y, const orc_tfsf *t, idx_t step, int is_e)
 }
 
 /* ------------------------------------------------------------------------
- * Lumped current source: CurrentSourceCorrector::correctE
- * (src/object/lumped_element/lumped_element_corrrector.cpp:24-37):
- *   E_box += coff_i * waveform[t]
+ * Lumped current / voltage source: CurrentSourceCorrector::correctE and
+ * VoltageSourceCorrector::correctE
+ * (src/object/lumped_element/lumped_element_corrrector.cpp:8-37):
+ *   E_box += coff * waveform[t]
+ * Lumped inductor (j != NULL): InductorCorrector::correctE (same file,
+ * 42-99), per node in i, j, k order:
+ *   E += cecjc * J;  J += cjcec * E        (cjcec in coff)
  * ---------------------------------------------------------------------- */
 typedef struct {
   int comp;
   idx_t s[3], e[3];
-  const double *coff;   /* box-shaped */
-  const double *wave;   /* length nt */
+  const double *coff;   /* box-shaped; the inductor's cjcec */
+  const double *wave;   /* length nt; NULL for an inductor */
+  const double *cecjc;  /* inductor: box-shaped */
+  double *j;            /* inductor: box-shaped current state */
 } orc_lumped;
 
 void orc_current_source(const orc_yee *y, const orc_lumped *l, idx_t step) {
   orc_arr F = y->e[l->comp];
   const idx_t n1 = l->e[1] - l->s[1], n2 = l->e[2] - l->s[2];
-  const double w = l->wave[step];
+  const double w = l->j ? 0.0 : l->wave[step];
   for (idx_t i = l->s[0]; i < l->e[0]; ++i)
     for (idx_t j = l->s[1]; j < l->e[1]; ++j)
       for (idx_t k = l->s[2]; k < l->e[2]; ++k) {
         const idx_t q = ((i - l->s[0]) * n1 + (j - l->s[1])) * n2 + (k - l->s[2]);
-        AT(F, i, j, k) += l->coff[q] * w;
+        if (l->j) {
+          AT(F, i, j, k) += l->cecjc[q] * l->j[q];
+          l->j[q] += l->coff[q] * AT(F, i, j, k);
+        } else {
+          AT(F, i, j, k) += l->coff[q] * w;
+        }
       }
 }
 

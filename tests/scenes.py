@@ -38,5 +38,42 @@ def voxels_objective(**kw):
     return S.adjoint_slab(**base)[1]
 
 
+def lumped_small(steps=120, n=32, pml=6, dl=1e-3):
+    """Every lumped element in a CPML-bounded air box: a 50-ohm z-directed
+    voltage source (two cells) at the centre with a 100-ohm resistor sharing
+    its upper node (the later element's coefficients win there), a resistor,
+    an x-directed capacitor, a z-directed inductor, a y-directed current
+    source with R = 200 ohm, and voltage / current monitors on them."""
+    import math
+    interior = n - 2 * pml
+    half = interior * dl / 2
+    sc = S.Scene(dl=(dl, dl, dl), cfl=0.99, steps=steps, name="lumped")
+    sc.objects.append(S.ObjectSpec("domain", S.cube((-half,) * 3, (2 * half,) * 3), S.air()))
+    tau = math.sqrt(2 * math.log(2)) / (math.pi * 15e9)
+    wave = S.Waveform("cosgauss", tau, 4.5 * tau, 30e9)
+    sc.current_sources += [
+        S.VoltageSourceSpec("vs", S.cube((0.0, 0.0, -dl), (0.0, 0.0, 2 * dl)), "ZP", 50.0, wave),
+        S.CurrentSourceSpec("is", S.cube((-3 * dl, -2 * dl, 2 * dl), (0.0, 2 * dl, 0.0)), "YN",
+                            200.0, wave),
+    ]
+    sc.lumped_elements += [
+        S.LumpedSpec("resistor", "r_top", S.cube((0.0, 0.0, 0.0), (0.0, 0.0, dl)), "Z", 100.0),
+        S.LumpedSpec("resistor", "r1", S.cube((4 * dl, 0.0, -dl), (0.0, 0.0, 2 * dl)), "Z", 100.0),
+        S.LumpedSpec("capacitor", "c1", S.cube((-5 * dl, 2 * dl, 0.0), (2 * dl, 0.0, 0.0)), "X",
+                     1e-12),
+        S.LumpedSpec("inductor", "l1", S.cube((0.0, -4 * dl, -dl), (dl, 0.0, 2 * dl)), "Z", 2e-9),
+    ]
+    sc.pmls = S.pml_all(pml)
+    sc.line_monitors = [
+        S.LineMonitorSpec("voltage", "v_vs", S.cube((0.0, 0.0, -dl), (0.0, 0.0, 2 * dl)), "ZP"),
+        S.LineMonitorSpec("voltage", "v_l1", S.cube((0.0, -4 * dl, -dl), (dl, 0.0, 2 * dl)), "ZP"),
+        S.LineMonitorSpec("current", "i_vs", S.cube((-dl, -dl, -dl), (2 * dl, 2 * dl, 2 * dl)),
+                          "ZP"),
+        S.LineMonitorSpec("current", "i_r1",
+                          S.cube((3 * dl, -dl, -dl), (2 * dl, 2 * dl, 2 * dl)), "ZP"),
+    ]
+    return sc
+
+
 ALL = {"sphere": sphere_small, "boxes": boxes_small, "dispersive": dispersive_small,
-       "voxels": voxels_small}
+       "voxels": voxels_small, "lumped": lumped_small}

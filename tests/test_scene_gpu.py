@@ -57,6 +57,13 @@ def test_scene_fp64_matches_oracle(name, opts):
         want = acc[0::2] + 1j * acc[1::2]
         assert got.shape == want.shape
         assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
+    counts = {"voltage": 0, "current": 0}
+    for lm in sc.line_monitors:
+        got = run.line_monitor(lm.kind, counts[lm.kind])
+        counts[lm.kind] += 1
+        want = orc.line_monitor_data[lm.name]
+        assert np.array_equal(got[0], want[0])
+        assert rel_l2(got[1], want[1]) <= TOL64, lm.name
 
 
 def test_dielectric_sphere_full_size_fp64():
@@ -89,7 +96,8 @@ def test_dielectric_sphere_full_size_fp64():
 # twice the largest error any sweep showed (dispersive: ~1.0e-4, from the
 # ADE recursions accumulating FP32 rounding).
 @pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
-                                         ("dispersive", 2e-4), ("voxels", 2e-4)])
+                                         ("dispersive", 2e-4), ("voxels", 2e-4),
+                                         ("lumped", 1e-4)])
 def test_scene_fp32_error_budget(name, budget, opts):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)

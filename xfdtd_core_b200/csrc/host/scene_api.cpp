@@ -205,7 +205,7 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
         sc->currents.push_back(m);
         sc->sim->addMonitor(m);
       }
-    } else if (kw == "current_source") {
+    } else if (kw == "current_source" || kw == "voltage_source") {
       in >> name;
       const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
                    sz = num(in);
@@ -213,9 +213,29 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       in >> dir;
       const double r = num(in);
       auto w = parseWaveform(in);
-      sc->sim->addObject(std::make_shared<CurrentSource>(
-          name, std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), parseDir(dir), r,
-          std::move(w)));
+      auto cube = std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz});
+      if (kw == "current_source")
+        sc->sim->addObject(
+            std::make_shared<CurrentSource>(name, std::move(cube), parseDir(dir), r, std::move(w)));
+      else
+        sc->sim->addObject(
+            std::make_shared<VoltageSource>(name, std::move(cube), parseDir(dir), r, std::move(w)));
+    } else if (kw == "resistor" || kw == "capacitor" || kw == "inductor") {
+      in >> name;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      std::string axis;
+      in >> axis;
+      if (axis != "X" && axis != "Y" && axis != "Z") throw XFDTDException("bad axis " + axis);
+      const auto xyz = static_cast<Axis::XYZ>(axis[0] - 'X');
+      const double v = num(in);
+      auto cube = std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz});
+      if (kw == "resistor")
+        sc->sim->addObject(std::make_shared<Resistor>(name, std::move(cube), xyz, v));
+      else if (kw == "capacitor")
+        sc->sim->addObject(std::make_shared<Capacitor>(name, std::move(cube), xyz, v));
+      else
+        sc->sim->addObject(std::make_shared<Inductor>(name, std::move(cube), xyz, v));
     } else if (kw == "pml") {
       const int t = static_cast<int>(num(in));
       std::string dir;

@@ -9,7 +9,8 @@
 //                          last object wins)
 //   edge/face averaging    src/calculation_param/calculation_param.cpp:43-168
 //   Yee coefficients       calculation_param.cpp:170-264
-//   lumped current source  src/object/lumped_element/current_source.cpp:43-165
+//   lumped elements        src/object/lumped_element/{current_source,voltage_source,
+//                          resistor,capacitor,inductor}.cpp (init, coefficients)
 //   CPML grading / kappa   src/boundary/pml.cpp:98-244, 286-633
 //   TFSF incident grid     src/waveform_source/tfsf.cpp:36-302
 //   ADE coefficients       src/material/ade_method/{m_lor,drude,debye}_ade_method.cpp
@@ -551,64 +552,128 @@ void Simulation::init(Index time_step) {
   };
   auto lat = [&](Index i, Index j, Index k) { return (i * NY + j) * NZ + k; };
 
-  // --------------------------------------------------- lumped current sources
+  // ------------------------------------------- lumped elements, object order
+  // CurrentSource / VoltageSource / Resistor / Capacitor / Inductor ::init and
+  // ::correctUpdateCoefficient (src/object/lumped_element/current_source.cpp:40-165,
+  // voltage_source.cpp:47-163, resistor.cpp:27-127, capacitor.cpp:16-112,
+  // inductor.cpp:23-105).  Per node: the cell sizes across (da, db) and along
+  // (dc) the axis give beta; (2 eps + dt sigma) and (2 eps - dt sigma) come
+  // from the (ca, cb) of the node's material class, so that a later element on
+  // the same node replaces an earlier one, as the reference recomputes from
+  // eps and sigma.
   struct CsH {
     int comp;
     int s[3], e[3];
     std::vector<double> coff, wave;
   };
+  struct IndH {
+    int comp;
+    int s[3], e[3];
+    std::vector<double> cecjc, cjcec;
+  };
+  struct LumpBox {
+    int comp;
+    int s[3], e[3];
+  };
   std::vector<CsH> current_sources;
+  std::vector<IndH> inductors;
+  std::vector<LumpBox> lumped_boxes;
+  std::map<Index, uint16_t> material_class;
   int override_tag = 0;
   for (const auto& o : _objects) {
+    auto le = std::dynamic_pointer_cast<LumpedElement>(o);
+    if (!le) continue;
     auto cs = std::dynamic_pointer_cast<CurrentSource>(o);
-    if (!cs) continue;
-    const Cube* cube = dynamic_cast<const Cube*>(cs->shape().get());
-    if (!cube) throw XFDTDException("CurrentSource needs a Cube");
-    const int ax = Axis::axisOf(cs->direction());
+    auto vs = std::dynamic_pointer_cast<VoltageSource>(o);
+    auto res = std::dynamic_pointer_cast<Resistor>(o);
+    auto cap = std::dynamic_pointer_cast<Capacitor>(o);
+    auto ind = std::dynamic_pointer_cast<Inductor>(o);
+    const Cube* cube = dynamic_cast<const Cube*>(le->shape().get());
+    if (!cube) throw XFDTDException("a lumped element needs a Cube");
+    const int ax = static_cast<int>(le->xyz());
     const int A = (ax + 1) % 3, B = (ax + 2) % 3;
     Index gs[3], ge[3];
     for (int a = 0; a < 3; ++a) {
       gs[a] = nearestNode(I.e_node[a], cube->origin()(a));
       ge[a] = nearestNode(I.e_node[a], cube->end()(a));
     }
-    CsH h;
-    h.comp = ax;
+    LumpBox box;
+    box.comp = ax;
     for (int a = 0; a < 3; ++a) {  // LumpedElement::rangeX/Y/Z
-      h.s[a] = (int)gs[a];
-      h.e[a] = (int)(a == ax ? ge[a] : ge[a] + 1);
+      box.s[a] = (int)gs[a];
+      box.e[a] = (int)(a == ax ? ge[a] : ge[a] + 1);
     }
-    const Real r = cs->resistance();
+    lumped_boxes.push_back(box);
     const Index na = ge[A] - gs[A] + 1, nb = ge[B] - gs[B] + 1, nc = ge[ax] - gs[ax];
-    const Real res_factor = r * na * nb / nc;
-    Real amp = cs->waveform()->amplitude() / (na * nb);
-    if (Axis::negative(cs->direction())) amp *= -1;
-    for (int i = h.s[0]; i < h.e[0]; ++i)
-      for (int j = h.s[1]; j < h.e[1]; ++j)
-        for (int k = h.s[2]; k < h.e[2]; ++k) {
+    // rf / cf / inf lambdas of the element's init, in the reference's order
+    Real factor = 0, amp = 0;
+    if (cs) {
+      factor = cs->resistance() * na * nb / nc;
+      amp = cs->waveform()->amplitude() / (na * nb);
+      if (Axis::negative(cs->direction())) amp *= -1;
+    } else if (vs) {
+      factor = vs->resistance() * na * nb / nc;
+      amp = vs->waveform()->amplitude() / nc;
+      if (Axis::negative(vs->direction())) amp *= -1;
+    } else if (res) {
+      factor = res->resistance() * na * nb / nc;
+    } else if (cap) {
+      factor = cap->capacitance() * nc / (nc * nb);
+    } else if (ind) {
+      factor = ind->inductance() * na * nb / nc;
+    } else {
+      throw XFDTDException("unknown lumped element " + o->name());
+    }
+    CsH h;
+    IndH hi;
+    h.comp = hi.comp = ax;
+    std::copy(box.s, box.s + 3, h.s);
+    std::copy(box.e, box.e + 3, h.e);
+    std::copy(box.s, box.s + 3, hi.s);
+    std::copy(box.e, box.e + 3, hi.e);
+    for (int i = box.s[0]; i < box.e[0]; ++i)
+      for (int j = box.s[1]; j < box.e[1]; ++j)
+        for (int k = box.s[2]; k < box.e[2]; ++k) {
           const int x[3] = {i, j, k};
           auto dsize = [&](int a) { return a == ax ? I.e_size[a][x[a]] : I.h_size[a][x[a]]; };
           const Real da = dsize(A), db = dsize(B), dc = dsize(ax);
-          const Real beta = (dt * dc) / (res_factor * da * db);
-          // Averaged eps / sigma of this E node: the class row's source values.
           const Index node = lat(i, j, k);
-          const double* row = &I.table[12 * I.lattice_class[node]];
-          // Recover (2 eps + dt sigma) and (2 eps - dt sigma) from (ca, cb):
+          const uint16_t mat = material_class.emplace(node, I.lattice_class[node]).first->second;
+          const double* row = &I.table[12 * mat];
           // cb = 2 dt / (2 eps + sigma dt), ca = (2 eps - dt sigma) / (2 eps + dt sigma).
           const Real denom = 2 * dt / row[2 * ax + 1];
           const Real numer = row[2 * ax] * denom;
+          if (ind) {
+            hi.cecjc.push_back(-(2 * dt) / denom);
+            hi.cjcec.push_back(dt * dc / (factor * da * db));
+            continue;
+          }
+          Real beta, ca;
+          if (vs) {
+            beta = dt * dc / (da * db * factor);
+          } else if (cap) {
+            beta = 2 * factor * dc / (da * db);
+          } else {
+            beta = (dt * dc) / (factor * da * db);
+          }
           const Real den_b = denom + beta;
-          const Real ca = (numer - beta) / den_b;
+          ca = cap ? (numer + beta) / den_b : (numer - beta) / den_b;
           const Real cb = 2 * dt / den_b;
-          h.coff.push_back(-2 * dt / (den_b * (db * da)) * amp);
+          if (cs) h.coff.push_back(-2 * dt / (den_b * (db * da)) * amp);
+          if (vs) h.coff.push_back(-2 * dt / (den_b * (da * db * factor)) * amp);
           overrideClass(node, override_tag++, [&](double* rw) {
             rw[2 * ax] = ca;
             rw[2 * ax + 1] = cb;
           });
         }
-    std::vector<Real> h_time = linspace((0 + 0.5) * dt, (0 + _steps + 0.5) * dt, _steps);
-    cs->waveform()->init(h_time);
-    h.wave.assign(cs->waveform()->value().begin(), cs->waveform()->value().end());
-    current_sources.push_back(std::move(h));
+    if (cs || vs) {
+      std::vector<Real> h_time = linspace((0 + 0.5) * dt, (0 + _steps + 0.5) * dt, _steps);
+      const auto& w = cs ? cs->waveform() : vs->waveform();
+      w->init(h_time);
+      h.wave.assign(w->value().begin(), w->value().end());
+      current_sources.push_back(std::move(h));
+    }
+    if (ind) inductors.push_back(std::move(hi));
   }
 
   // --------------------------------------------------------------- CPML
@@ -936,11 +1001,11 @@ void Simulation::init(Index time_step) {
                       within = within && (long long)x[a] >= tf_lo[a] && (long long)x[a] <= tf_hi[a];
                   if (within) throw XFDTDException("a VoxelObject touches a TFSF face");
                 }
-                for (const auto& h : current_sources)
+                for (const auto& h : lumped_boxes)
                   if (h.comp == c && i >= (Index)h.s[0] && i < (Index)h.e[0] &&
                       j >= (Index)h.s[1] && j < (Index)h.e[1] && k >= (Index)h.s[2] &&
                       k < (Index)h.e[2])
-                    throw XFDTDException("a VoxelObject touches a current source");
+                    throw XFDTDException("a VoxelObject touches a lumped element");
                 for (int q = 0; q < 4; ++q) {
                   const uint16_t pm = I.cell[(cells[q][0] * ny + cells[q][1]) * nz + cells[q][2]];
                   if (I.painters[pm]->dispersion())
@@ -1010,6 +1075,9 @@ void Simulation::init(Index time_step) {
   for (const auto& h : current_sources)
     checkStatus(E, xfd_add_current_source(E, h.comp, h.s, h.e, h.coff.data(), h.wave.data()),
                 "xfd_add_current_source");
+  for (const auto& h : inductors)
+    checkStatus(E, xfd_add_inductor(E, h.comp, h.s, h.e, h.cecjc.data(), h.cjcec.data()),
+                "xfd_add_inductor");
   if (ade_kind >= 0) {
     xfd_ade_desc a{ade_kind, num_pole, (int32_t)(ade_coef.size() / (2 + 7 * num_pole)),
                    ade_coef.data(), (int64_t)ade_comp.size(), ade_comp.data(), ade_node.data(),

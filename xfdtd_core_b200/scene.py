@@ -11,6 +11,9 @@ reference's user-facing API one to one:
                                                        include/xfdtd/boundary/pml.h:19-21
 * ``TFSF3D(x, y, z, theta, phi, psi, waveform)``      include/xfdtd/waveform_source/tfsf_3d.h:10-11
 * ``CurrentSource(name, cube, dir, R, waveform)``     include/xfdtd/object/lumped_element/current_source.h:11-14
+* ``VoltageSource(name, cube, dir, R, waveform)``     include/xfdtd/object/lumped_element/voltage_source.h:15-18
+* ``Resistor / Capacitor / Inductor(name, cube, xyz, value)``
+                                                       include/xfdtd/object/lumped_element/{resistor,capacitor,inductor}.h:9-12
 * ``MovieMonitor(FieldMonitor(cube, field), k)``      include/xfdtd/monitor/movie_monitor.h:13-15
 * ``NFFFTFrequencyDomain(dx, dy, dz, freqs)``         include/xfdtd/nffft/nffft_frequency_domain.h:19-45
 * ``Waveform::gaussian / cosineModulatedGaussian``    src/waveform/waveform.cpp:80-96
@@ -200,12 +203,34 @@ class CurrentSourceSpec:
     direction: str
     resistance: float
     waveform: Waveform
+    kind: str = "current"  # "current" | "voltage"
 
     def text(self) -> str:
         o, s = self.shape.origin, self.shape.size
-        return (f"current_source {self.name} " +
+        return (f"{self.kind}_source {self.name} " +
                 " ".join(_f(v) for v in (*o, *s)) +
                 f" {self.direction} {_f(self.resistance)} {self.waveform.text()}")
+
+
+@dataclass
+class VoltageSourceSpec(CurrentSourceSpec):
+    kind: str = "voltage"
+
+
+@dataclass
+class LumpedSpec:
+    """Resistor, Capacitor or Inductor (kind "resistor" | "capacitor" |
+    "inductor") on a Cube of E nodes along `axis` ("X" | "Y" | "Z")."""
+    kind: str
+    name: str
+    shape: Shape  # a Cube
+    axis: str
+    value: float
+
+    def text(self) -> str:
+        o, s = self.shape.origin, self.shape.size
+        return (f"{self.kind} {self.name} " + " ".join(_f(v) for v in (*o, *s)) +
+                f" {self.axis} {_f(self.value)}")
 
 
 @dataclass
@@ -313,6 +338,7 @@ class Scene:
     steps: int
     objects: List[ObjectSpec] = field(default_factory=list)
     current_sources: List[CurrentSourceSpec] = field(default_factory=list)
+    lumped_elements: List[LumpedSpec] = field(default_factory=list)
     pmls: List[PMLSpec] = field(default_factory=list)
     tfsf: Optional[TFSFSpec] = None
     movies: List[MovieSpec] = field(default_factory=list)
@@ -328,6 +354,7 @@ class Scene:
                  f"steps {self.steps}"]
         lines += [o.text() for o in self.objects]
         lines += [c.text() for c in self.current_sources]
+        lines += [c.text() for c in self.lumped_elements]
         lines += [p.text() for p in self.pmls]
         if self.tfsf is not None:
             lines.append(self.tfsf.text())
