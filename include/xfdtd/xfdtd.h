@@ -19,6 +19,7 @@
 #include <array>
 #include <cmath>
 #include <complex>
+#include <map>
 #include <cstdint>
 #include <functional>
 #include <initializer_list>
@@ -172,6 +173,8 @@ class ElectroMagneticProperty {
  public:
   ElectroMagneticProperty(Real eps_r = 1, Real mu_r = 1, Real sigma_e = 0, Real sigma_m = 0);
   static ElectroMagneticProperty air() { return {1, 1, 0, 0}; }
+  /// ElectroMagneticProperty::pec (src/material/material.cpp:32-34).
+  static ElectroMagneticProperty pec() { return {1, 1, 1e10, 0}; }
   Real epsilonR() const { return _eps_r; }
   Real muR() const { return _mu_r; }
   Real sigmaE() const { return _sigma_e; }
@@ -190,6 +193,9 @@ class Material {
   virtual ~Material() = default;
   static std::unique_ptr<Material> createAir() {
     return std::make_unique<Material>("air", ElectroMagneticProperty::air());
+  }
+  static std::unique_ptr<Material> createPec() {
+    return std::make_unique<Material>("pec", ElectroMagneticProperty::pec());
   }
   const std::string& name() const { return _name; }
   const ElectroMagneticProperty& emProperty() const { return _emp; }
@@ -319,6 +325,15 @@ class VoxelObject : public Object {
   std::array<Index, 3> _dims;
   std::vector<Real> _eps_r;
   Real _mu_r, _sigma_e;
+};
+
+/// Zero-thickness PEC sheet (src/object/lumped_element/pec_plane.cpp:9-66):
+/// paints no cells; after the edge averaging its two tangential E components
+/// on the plane take the PEC sigma_e.  The Cube must be flat on one axis.
+class PecPlane : public Object {
+ public:
+  PecPlane(std::string name, std::unique_ptr<Cube> cube)
+      : Object{std::move(name), std::move(cube), Material::createPec()} {}
 };
 
 /// Lumped element on a Cube of E nodes along one axis
@@ -630,6 +645,78 @@ class CurrentMonitor : public Monitor {
   int _probe = -1;
 };
 
+// ---------------------------------------------------------------- network
+/// One port of a Network (include/xfdtd/network/port.h:15-70,
+/// src/network/port.cpp:10-130): a current and a voltage monitor and a
+/// reference impedance z.  calculateSParameters takes the DFTs
+/// I(f) = dt sum_n i_n exp(-j 2 pi f ((n+1) dt - 1.5 dt)) and
+/// V(f) = dt sum_n v_n exp(-j 2 pi f (n+1) dt) of the two series and forms the
+/// power waves a = (V + z I) / (2 sqrt(Re z)), b = (V - conj(z) I) / (2 sqrt(Re z)).
+class Port {
+ public:
+  Port(std::size_t index, bool is_source, std::complex<Real> impedance,
+       std::shared_ptr<CurrentMonitor> current_monitor,
+       std::shared_ptr<VoltageMonitor> voltage_monitor)
+      : _index{index},
+        _is_source{is_source},
+        _impedance{impedance},
+        _current_monitor{std::move(current_monitor)},
+        _voltage_monitor{std::move(voltage_monitor)} {}
+  std::size_t index() const { return _index; }
+  bool isSource() const { return _is_source; }
+  std::complex<Real> impedance() const { return _impedance; }
+  const std::shared_ptr<CurrentMonitor>& currentMonitor() const { return _current_monitor; }
+  const std::shared_ptr<VoltageMonitor>& voltageMonitor() const { return _voltage_monitor; }
+  const std::vector<std::complex<Real>>& a() const { return _a; }
+  const std::vector<std::complex<Real>>& b() const { return _b; }
+  void init(Real dt) { _dt = dt; }
+  void calculateSParameters(const Array1D<Real>& frequencies);
+
+ private:
+  std::size_t _index;
+  bool _is_source;
+  std::complex<Real> _impedance;
+  std::shared_ptr<CurrentMonitor> _current_monitor;
+  std::shared_ptr<VoltageMonitor> _voltage_monitor;
+  Real _dt = 0;
+  std::vector<std::complex<Real>> _a, _b;
+};
+
+/// S-parameters of a set of ports (include/xfdtd/network/network.h:21-70,
+/// src/network/network.cpp:12-84).  output() computes every port's waves and
+/// S[10 j + i] = b_j / a_i for each source port i, and writes
+/// <output_dir>/s<10 j + i>.npy (complex128) and frequencies.npy.
+class Network {
+ public:
+  Network() = default;
+  explicit Network(std::string output_dir) : _output_dir{std::move(output_dir)} {}
+  Network(std::vector<std::shared_ptr<Port>> ports, Array1D<Real> frequencies,
+          std::string output_dir)
+      : _ports{std::move(ports)},
+        _frequencies{std::move(frequencies)},
+        _output_dir{std::move(output_dir)} {}
+  void addPort(std::shared_ptr<Port> port) { _ports.emplace_back(std::move(port)); }
+  void setFrequencies(Array1D<Real> frequencies) { _frequencies = std::move(frequencies); }
+  void setOutputDir(std::string output_dir) { _output_dir = std::move(output_dir); }
+  /// Port::init for every port; port indices must be unique.
+  void init(Real dt);
+  /// The waves of every port and the S-parameters, without writing files.
+  void compute();
+  /// compute(), then the .npy files.
+  void output();
+  const std::vector<std::shared_ptr<Port>>& ports() const { return _ports; }
+  const Array1D<Real>& frequencies() const { return _frequencies; }
+  const std::map<int, std::vector<std::complex<Real>>>& sParameters() const {
+    return _s_parameters;
+  }
+
+ private:
+  std::vector<std::shared_ptr<Port>> _ports;
+  Array1D<Real> _frequencies;
+  std::string _output_dir;
+  std::map<int, std::vector<std::complex<Real>>> _s_parameters;
+};
+
 // ------------------------------------------------------------------ NF2FF
 /// Frequency-domain NF2FF on a Huygens box `distance` cells inside the grid
 /// faces (src/nffft/nffft_frequency_domain.cpp).  After run() the surface
@@ -745,6 +832,7 @@ class Simulation {
   void addMonitor(std::shared_ptr<Monitor> monitor);
   void addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> nffft);
   void addNF2FF(std::shared_ptr<NFFFTTimeDomain> nffft);
+  void addNetwork(std::shared_ptr<Network> network);
 
   /// Builds the grid and coefficients, runs `time_step` steps on the GPU and
   /// copies fields, movie frames and NF2FF currents back to the host.
@@ -823,6 +911,7 @@ class Simulation {
   std::vector<std::shared_ptr<Monitor>> _monitors;
   std::vector<std::shared_ptr<NFFFTFrequencyDomain>> _nffts;
   std::vector<std::shared_ptr<NFFFTTimeDomain>> _nffts_td;
+  std::vector<std::shared_ptr<Network>> _networks;
   EMF _emf;
   Real _dt = 0;
   Index _n[3] = {0, 0, 0};

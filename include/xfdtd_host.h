@@ -86,6 +86,14 @@ int xfdtd_scene_dft_objective(xfdtd_scene* s, int64_t n_steps, int32_t field,
                               int32_t voxel_object, int32_t checkpoint_interval, double* value,
                               double* grad, int64_t capacity);
 
+/* S-parameter S[key] (key = 10 j + i: port j's outgoing wave over source
+ * port i's incident wave) of the finished scene's network, one complex value
+ * per network frequency as (re, im) pairs; count = 2 n_freqs.
+ * Replaces: Network::output (src/network/network.cpp:47-84) without the
+ * files; xfdtd_scene_write_outputs writes them under network/. */
+int xfdtd_scene_s_parameter(xfdtd_scene* s, int32_t key, double* out, int64_t capacity,
+                            int64_t* count);
+
 /* Voltage (kind 0) or current (kind 1) monitor number `index` of the
  * finished scene: [time; data], 2 x n_steps doubles, count = 2 n_steps. */
 int xfdtd_scene_line_monitor(xfdtd_scene* s, int32_t kind, int32_t index, double* out,

@@ -248,7 +248,8 @@ class RefSimulation:
         sc = self.scene
         dx, dy, dz = sc.dl
         shapes = [o.shape for o in sc.objects] + [c.shape for c in sc.current_sources] + \
-            [c.shape for c in getattr(sc, "lumped_elements", [])]
+            [c.shape for c in getattr(sc, "lumped_elements", [])] + \
+            [c.shape for c in getattr(sc, "pec_planes", [])]
         lo = np.full(3, np.finfo(np.float64).max)
         hi = np.full(3, np.finfo(np.float64).min)
         for s in shapes:  # Shape::makeWrappedCube (src/shape/shape.cpp:8-38)
@@ -404,6 +405,23 @@ class RefSimulation:
             qy[0:nx, 1:ny, 0:nz] + qy[0:nx, 0:ny - 1, 0:nz])
         qz[:, :, 1:nz] = 2 * qz[0:nx, 0:ny, 1:nz] * qz[0:nx, 0:ny, 0:nz - 1] / (
             qz[0:nx, 0:ny, 1:nz] + qz[0:nx, 0:ny, 0:nz - 1])
+        # PecPlane::correctMaterialSpace (src/object/lumped_element/pec_plane.cpp:12-66)
+        # after the averaging (src/simulation/simulation.cpp:628-635): the PEC
+        # sigma_e (ElectroMagneticProperty::pec, src/material/material.cpp:32-34)
+        # on the plane's two tangential E components.
+        for pp in getattr(self.scene, "pec_planes", []):
+            (i0, j0, k0), (i1, j1, k1) = self.grid_box(pp.shape)
+            if i0 == i1:
+                sig_e[1][i0, j0:j1, k0:k1 + 1] = 1e10
+                sig_e[2][i0, j0:j1 + 1, k0:k1] = 1e10
+            elif j0 == j1:
+                sig_e[2][i0:i1 + 1, j0, k0:k1] = 1e10
+                sig_e[0][i0:i1, j0, k0:k1 + 1] = 1e10
+            elif k0 == k1:
+                sig_e[0][i0:i1, j0:j1 + 1, k0] = 1e10
+                sig_e[1][i0:i1 + 1, j0:j1, k0] = 1e10
+            else:
+                raise ValueError(f"{pp.name} PecPlane is not a plane!")
         self.eps_arr, self.sig_e_arr, self.mu_arr, self.sig_m_arr = eps, sig_e, mu, sig_m
 
     # ----------------------------------------------------------- coefficients
@@ -1333,3 +1351,32 @@ class RefSimulation:
     def fields(self) -> Dict[str, np.ndarray]:
         return {"EX": self.e[0], "EY": self.e[1], "EZ": self.e[2], "HX": self.h[0],
                 "HY": self.h[1], "HZ": self.h[2]}
+
+
+def network_s_parameters(sim: "RefSimulation", network) -> Dict[int, np.ndarray]:
+    """Network::output's S-parameters (src/network/network.cpp:47-65) from the
+    ports' waves (Port::calculateSParameters, src/network/port.cpp:104-130)
+    and the reference's DFT (include/xfdtd/util/dft.h:9-26):
+    X(f) = dt sum_n x_n exp(-j 2 pi f ((n + 1) dt + shift)), shift -1.5 dt for
+    the current.  Keys are 10 j + i for source port i."""
+    dt = sim.dt
+    f = np.asarray(network.frequencies, dtype=np.float64)
+
+    def dft(x, shift):
+        t = (np.arange(len(x)) + 1) * dt + shift
+        return dt * (x[None, :] * np.exp(-2j * np.pi * f[:, None] * t[None, :])).sum(axis=1)
+
+    waves = {}
+    for p in network.ports:
+        i = dft(sim.line_monitor_data[p.current][1], -1.5 * dt)
+        v = dft(sim.line_monitor_data[p.voltage][1], 0.0)
+        z = complex(p.impedance)
+        k = np.sqrt(z.real)
+        waves[p.index] = (0.5 * (v + z * i) / k, 0.5 * (v - np.conj(z) * i) / k)
+    out = {}
+    for pi in network.ports:
+        if not pi.is_source:
+            continue
+        for pj in network.ports:
+            out[pj.index * 10 + pi.index] = waves[pj.index][1] / waves[pi.index][0]
+    return out

@@ -75,5 +75,13 @@ def lumped_small(steps=120, n=32, pml=6, dl=1e-3):
     return sc
 
 
+def microstrip_small(steps=150, **kw):
+    """The microstrip-line example (PEC planes, voltage source, port, network)
+    at half the cell count."""
+    base = dict(steps=steps, n_freqs=40, scale=2)
+    base.update(kw)
+    return S.microstrip_line(**base)
+
+
 ALL = {"sphere": sphere_small, "boxes": boxes_small, "dispersive": dispersive_small,
-       "voxels": voxels_small, "lumped": lumped_small}
+       "voxels": voxels_small, "lumped": lumped_small, "microstrip": microstrip_small}

@@ -6,7 +6,7 @@ against the FP64 oracle is stated per test."""
 import numpy as np
 import pytest
 
-from oracle.reference_model import RefSimulation
+from oracle.reference_model import RefSimulation, network_s_parameters
 from tests.cases import rel_l2
 from tests.scenes import ALL, sphere_small, dispersive_small
 from xfdtd_core_b200 import scene as S
@@ -64,6 +64,12 @@ def test_scene_fp64_matches_oracle(name, opts):
         want = orc.line_monitor_data[lm.name]
         assert np.array_equal(got[0], want[0])
         assert rel_l2(got[1], want[1]) <= TOL64, lm.name
+    if sc.network is not None:
+        want = network_s_parameters(orc, sc.network)
+        for key, w in want.items():
+            got = run.s_parameter(key)
+            assert got.shape == w.shape
+            assert np.linalg.norm(got - w) / np.linalg.norm(w) <= TOL64, key
 
 
 def test_dielectric_sphere_full_size_fp64():
@@ -91,13 +97,36 @@ def test_dielectric_sphere_full_size_fp64():
     assert max(late) <= TOL64, late
 
 
+def test_microstrip_line_full_size_fp64(tmp_path):
+    """The reference's microstrip-line example at its own size (60 x 74 x 26
+    cells, 1000 steps): the port's voltage and current series and S11 at 500
+    frequencies within 1e-12 of the oracle, and the network's npy files."""
+    sc = S.microstrip_line()
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc)
+    run.run()
+    assert max(_fields_rel(run, orc)) <= TOL64
+    for q, kind, name in ((0, "voltage", "v1"), (0, "current", "c1")):
+        assert rel_l2(run.line_monitor(kind, q)[1], orc.line_monitor_data[name][1]) <= TOL64
+    want = network_s_parameters(orc, sc.network)[11]
+    got = run.s_parameter(11)
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
+    assert np.abs(got).max() < 0.1  # a matched 50-ohm line reflects little
+    run.write_outputs(str(tmp_path))
+    s11 = np.load(tmp_path / "network" / "s11.npy")
+    fr = np.load(tmp_path / "network" / "frequencies.npy")
+    assert s11.dtype == np.complex128 and np.array_equal(s11, got)
+    assert fr.shape == (500,) and fr[0] == 2e7 and fr[-1] == 10e9
+
+
 @pytest.mark.parametrize("opts", [s for s in SWEEPS if s.id != "fused"])
 # FP32 budgets: relative L2 against the FP64 oracle after 150 steps, about
 # twice the largest error any sweep showed (dispersive: ~1.0e-4, from the
 # ADE recursions accumulating FP32 rounding).
 @pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
                                          ("dispersive", 2e-4), ("voxels", 2e-4),
-                                         ("lumped", 1e-4)])
+                                         ("lumped", 1e-4), ("microstrip", 1e-4)])
 def test_scene_fp32_error_budget(name, budget, opts):
     sc = ALL[name](steps=150)
     orc = RefSimulation(sc)

@@ -118,6 +118,7 @@ struct xfdtd_scene {
   std::vector<std::shared_ptr<CurrentMonitor>> currents;
   std::shared_ptr<NFFFTFrequencyDomain> nf2ff;
   std::shared_ptr<NFFFTTimeDomain> nf2ff_td;
+  std::shared_ptr<Network> network;
   int64_t steps = 0;
   bool finished = false;
 };
@@ -220,6 +221,35 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       else
         sc->sim->addObject(
             std::make_shared<VoltageSource>(name, std::move(cube), parseDir(dir), r, std::move(w)));
+    } else if (kw == "network") {
+      if (sc->network) throw XFDTDException("one network per scene");
+      const auto nf = static_cast<std::size_t>(num(in));
+      std::vector<Real> fr(nf);
+      for (auto& v : fr) v = num(in);
+      sc->network = std::make_shared<Network>(std::vector<std::shared_ptr<Port>>{},
+                                              Array1D<Real>(std::move(fr)), "");
+      sc->sim->addNetwork(sc->network);
+    } else if (kw == "port") {
+      if (!sc->network) throw XFDTDException("port before network");
+      const auto index = static_cast<std::size_t>(num(in));
+      const bool src = num(in) != 0;
+      const double zr = num(in), zi = num(in);
+      std::string cname, vname;
+      in >> cname >> vname;
+      std::shared_ptr<CurrentMonitor> cm;
+      std::shared_ptr<VoltageMonitor> vm;
+      for (const auto& c : sc->currents)
+        if (c->name() == cname) cm = c;
+      for (const auto& v : sc->voltages)
+        if (v->name() == vname) vm = v;
+      if (!cm || !vm) throw XFDTDException("port monitors " + cname + " / " + vname + " not found");
+      sc->network->addPort(std::make_shared<Port>(index, src, std::complex<Real>(zr, zi), cm, vm));
+    } else if (kw == "pec_plane") {
+      in >> name;
+      const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
+                   sz = num(in);
+      sc->sim->addObject(std::make_shared<PecPlane>(
+          name, std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz})));
     } else if (kw == "resistor" || kw == "capacitor" || kw == "inductor") {
       in >> name;
       const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),
@@ -532,6 +562,31 @@ int xfdtd_scene_write_outputs(xfdtd_scene* s, const char* dir) {
     for (const auto& m : s->currents) {
       m->setOutputDir((root / "monitors").string());
       m->output();
+    }
+    if (s->network) {
+      s->network->setOutputDir((root / "network").string());
+      s->network->output();
+    }
+  })
+}
+
+int xfdtd_scene_s_parameter(xfdtd_scene* s, int32_t key, double* out, int64_t capacity,
+                            int64_t* count) {
+  HOST_TRY({
+    if (!s || !count) throw XFDTDException("null argument");
+    if (!s->network) throw XFDTDException("scene has no network");
+    if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
+    s->network->compute();
+    const auto& m = s->network->sParameters();
+    auto it = m.find(key);
+    if (it == m.end()) throw XFDTDException("no S-parameter " + std::to_string(key));
+    *count = (int64_t)(2 * it->second.size());
+    if (out) {
+      if (capacity < *count) throw XFDTDException("buffer too small");
+      for (std::size_t q = 0; q < it->second.size(); ++q) {
+        out[2 * q] = it->second[q].real();
+        out[2 * q + 1] = it->second[q].imag();
+      }
     }
   })
 }

@@ -30,6 +30,7 @@
 #include <limits>
 #include <map>
 #include <numeric>
+#include <set>
 #include <sstream>
 #include <unordered_map>
 
@@ -297,6 +298,7 @@ void Simulation::addWaveformSource(std::shared_ptr<WaveformSource> s) {
 }
 void Simulation::addMonitor(std::shared_ptr<Monitor> m) { _monitors.push_back(std::move(m)); }
 void Simulation::addNF2FF(std::shared_ptr<NFFFTTimeDomain> n) { _nffts_td.push_back(std::move(n)); }
+void Simulation::addNetwork(std::shared_ptr<Network> n) { _networks.push_back(std::move(n)); }
 void Simulation::addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> n) {
   _nffts.push_back(std::move(n));
 }
@@ -385,6 +387,7 @@ void Simulation::init(Index time_step) {
     } else {
       I.mat.push_back({mp.epsilon(), mp.mu(), mp.sigmaE(), mp.sigmaM()});
     }
+    if (std::dynamic_pointer_cast<PecPlane>(o)) continue;  // paints no cells
     // Only cells whose centre lies within the wrapped cube (+ tolerance) can
     // test inside; the reference tests every cell with the same predicate.
     auto wc = o->shape()->wrappedCube();
@@ -406,7 +409,11 @@ void Simulation::init(Index time_step) {
 
   // ------------------------------------------------------ material classes
   const MatP def{EPSILON_0, MU_0, constant::SIGMA_E_ZERO_APPROX, constant::SIGMA_M_ZERO_APPROX};
-  auto classRow = [&](const ClassKey& key, double* row) {
+  // Beside each class row: the averaged (eps, sigma_e) of Ex, Ey, Ez, from
+  // which later coefficient changes (PEC planes, lumped elements) start, as
+  // the reference's start from its eps / sigma arrays.
+  std::vector<double> class_es;
+  auto classRow = [&](const ClassKey& key, double* row, double* es) {
     auto P = [&](int a, int b, int c) -> const MatP& {
       const uint16_t m = key.m[a * 4 + b * 2 + c];
       return m == kNoCell ? def : I.mat[m];
@@ -416,6 +423,8 @@ void Simulation::init(Index time_step) {
     auto eCoef = [&](Real eps, Real sig, double* out) {
       out[0] = (2 * eps - dt * sig) / (2 * eps + dt * sig);
       out[1] = (2 * dt) / (2 * eps + sig * dt);
+      es[out - row] = eps;
+      es[out - row + 1] = sig;
     };
     auto hCoef = [&](Real mu, Real sig, double* out) {
       out[0] = (2 * mu - dt * sig) / (2 * mu + dt * sig);
@@ -424,6 +433,7 @@ void Simulation::init(Index time_step) {
     auto avg4 = [](Real a, Real b, Real c, Real d) { return 0.25 * (((a + b) + c) + d); };
     auto harm = [](Real a, Real b) { return 2 * a * b / (a + b); };
     std::fill(row, row + 12, 0.0);
+    std::fill(es, es + 6, 0.0);
     // Ex(i, j, k): cells (i, j-1..j, k-1..k)
     if (il) {
       if (jg && jl && kg && kl) {
@@ -521,7 +531,8 @@ void Simulation::init(Index time_step) {
               id = static_cast<uint16_t>(ids.size());
               ids.emplace(key, id);
               I.table.resize(I.table.size() + 12);
-              classRow(key, I.table.data() + 12 * id);
+              class_es.resize(class_es.size() + 6);
+              classRow(key, I.table.data() + 12 * id, class_es.data() + 6 * id);
             } else {
               id = it->second;
             }
@@ -534,7 +545,8 @@ void Simulation::init(Index time_step) {
   }
   // Overrides create new classes: (base class, override tag) -> class.
   std::map<std::pair<uint16_t, int>, uint16_t> override_ids;
-  auto overrideClass = [&](Index node, int tag, const std::function<void(double*)>& edit) {
+  auto overrideClass = [&](Index node, int tag,
+                           const std::function<void(double*, double*)>& edit) {
     const uint16_t base = I.lattice_class[node];
     auto key = std::make_pair(base, tag);
     auto it = override_ids.find(key);
@@ -545,8 +557,10 @@ void Simulation::init(Index time_step) {
     const std::size_t n_cls = I.table.size() / 12;
     if (n_cls >= 65535) throw XFDTDException("more than 65535 material classes");
     std::vector<double> row(I.table.begin() + 12 * base, I.table.begin() + 12 * base + 12);
-    edit(row.data());
+    std::vector<double> es(class_es.begin() + 6 * base, class_es.begin() + 6 * base + 6);
+    edit(row.data(), es.data());
     I.table.insert(I.table.end(), row.begin(), row.end());
+    class_es.insert(class_es.end(), es.begin(), es.end());
     override_ids.emplace(key, static_cast<uint16_t>(n_cls));
     I.lattice_class[node] = static_cast<uint16_t>(n_cls);
   };
@@ -580,6 +594,41 @@ void Simulation::init(Index time_step) {
   std::vector<LumpBox> lumped_boxes;
   std::map<Index, uint16_t> material_class;
   int override_tag = 0;
+  // PecPlane::correctMaterialSpace (src/object/lumped_element/pec_plane.cpp:12-66),
+  // applied after the averaging (src/simulation/simulation.cpp:628-635): the
+  // PEC sigma_e on the plane's two tangential E components; eps unchanged.
+  for (const auto& o : _objects) {
+    auto pp = std::dynamic_pointer_cast<PecPlane>(o);
+    if (!pp) continue;
+    const Cube* cube = dynamic_cast<const Cube*>(pp->shape().get());
+    if (!cube) throw XFDTDException("a PecPlane needs a Cube");
+    Index gs[3], ge[3];
+    for (int a = 0; a < 3; ++a) {
+      gs[a] = nearestNode(I.e_node[a], cube->origin()(a));
+      ge[a] = nearestNode(I.e_node[a], cube->end()(a));
+    }
+    int p = -1;
+    for (int a = 0; a < 3 && p < 0; ++a)
+      if (gs[a] == ge[a]) p = a;
+    if (p < 0) throw XFDTDException(o->name() + " PecPlane is not a plane!");
+    const Real sig_pec = pp->material()->emProperty().sigmaE();
+    for (int c : {(p + 1) % 3, (p + 2) % 3}) {
+      Index s[3], e[3];
+      for (int a = 0; a < 3; ++a) {
+        s[a] = gs[a];
+        e[a] = a == p ? gs[a] + 1 : (a == c ? ge[a] : ge[a] + 1);
+      }
+      for (Index i = s[0]; i < e[0]; ++i)
+        for (Index j = s[1]; j < e[1]; ++j)
+          for (Index k = s[2]; k < e[2]; ++k)
+            overrideClass(lat(i, j, k), -1 - c, [&](double* rw, double* es) {
+              const Real eps = es[2 * c];
+              rw[2 * c] = (2 * eps - dt * sig_pec) / (2 * eps + dt * sig_pec);
+              rw[2 * c + 1] = (2 * dt) / (2 * eps + sig_pec * dt);
+              es[2 * c + 1] = sig_pec;
+            });
+    }
+  }
   for (const auto& o : _objects) {
     auto le = std::dynamic_pointer_cast<LumpedElement>(o);
     if (!le) continue;
@@ -639,12 +688,9 @@ void Simulation::init(Index time_step) {
           const Real da = dsize(A), db = dsize(B), dc = dsize(ax);
           const Index node = lat(i, j, k);
           const uint16_t mat = material_class.emplace(node, I.lattice_class[node]).first->second;
-          const double* row = &I.table[12 * mat];
-          // cb = 2 dt / (2 eps + sigma dt), ca = (2 eps - dt sigma) / (2 eps + dt sigma).
-          const Real denom = 2 * dt / row[2 * ax + 1];
-          const Real numer = row[2 * ax] * denom;
+          const Real eps = class_es[6 * mat + 2 * ax], sig = class_es[6 * mat + 2 * ax + 1];
           if (ind) {
-            hi.cecjc.push_back(-(2 * dt) / denom);
+            hi.cecjc.push_back(-(2 * dt) / (2 * eps + dt * sig));
             hi.cjcec.push_back(dt * dc / (factor * da * db));
             continue;
           }
@@ -656,12 +702,12 @@ void Simulation::init(Index time_step) {
           } else {
             beta = (dt * dc) / (factor * da * db);
           }
-          const Real den_b = denom + beta;
-          ca = cap ? (numer + beta) / den_b : (numer - beta) / den_b;
+          const Real den_b = 2 * eps + dt * sig + beta;
+          ca = cap ? (2 * eps - dt * sig + beta) / den_b : (2 * eps - dt * sig - beta) / den_b;
           const Real cb = 2 * dt / den_b;
           if (cs) h.coff.push_back(-2 * dt / (den_b * (db * da)) * amp);
           if (vs) h.coff.push_back(-2 * dt / (den_b * (da * db * factor)) * amp);
-          overrideClass(node, override_tag++, [&](double* rw) {
+          overrideClass(node, override_tag++, [&](double* rw, double*) {
             rw[2 * ax] = ca;
             rw[2 * ax + 1] = cb;
           });
@@ -873,7 +919,7 @@ void Simulation::init(Index time_step) {
                 "the absorbing layers");
           const auto& ec = e_coef[slot[pm]];
           // Object::handleDispersion -> correctCoeff overwrites Ex, Ey, Ez at (i,j,k).
-          overrideClass(lat(i, j, k), 1000000 + slot[pm], [&](double* rw) {
+          overrideClass(lat(i, j, k), 1000000 + slot[pm], [&](double* rw, double*) {
             for (int c = 0; c < 3; ++c) {
               rw[2 * c] = ec[0];
               rw[2 * c + 1] = ec[1];
@@ -1135,6 +1181,8 @@ void Simulation::init(Index time_step) {
       cm->_data.assign(_steps, 0.0);
     }
   }
+  // Network::init (src/network/network.cpp:32-45).
+  for (const auto& n : _networks) n->init(dt);
   // Field time monitors: the last node of the shifted box, every step.
   for (const auto& mon : _monitors) {
     auto ft = std::dynamic_pointer_cast<FieldTimeMonitor>(mon);
@@ -1949,6 +1997,75 @@ void NFFFTFrequencyDomain::processFarField(Real theta, const Array1D<Real>& phi,
                                            const std::string& sub_dir,
                                            const Vector& origin) const {
   processFarField(Array1D<Real>{theta}, phi, sub_dir, origin);
+}
+
+// ---------------------------------------------------------------- network
+namespace {
+// dft (include/xfdtd/util/dft.h:9-26):
+// X(f) = dt sum_n x_n exp(-j 2 pi f t_n), t_n = (n + 1) dt + shift.
+std::vector<std::complex<Real>> timeDft(const std::vector<Real>& x, Real dt,
+                                        const Array1D<Real>& freqs, Real shift) {
+  std::vector<std::complex<Real>> out(freqs.size());
+#pragma omp parallel for schedule(static)
+  for (std::size_t q = 0; q < freqs.size(); ++q) {
+    std::complex<Real> sum{0.0, 0.0};
+    for (std::size_t n = 0; n < x.size(); ++n) {
+      const Real t = (n + 1) * dt + shift;
+      const Real ph = -2 * constant::PI * freqs[q] * t;
+      sum += x[n] * std::complex<Real>(std::cos(ph), std::sin(ph));
+    }
+    out[q] = sum * dt;
+  }
+  return out;
+}
+}  // namespace
+
+void Port::calculateSParameters(const Array1D<Real>& frequencies) {
+  if (!_current_monitor || !_voltage_monitor || _current_monitor->data().empty() ||
+      _voltage_monitor->data().empty())
+    throw XFDTDException(
+        "Port: Monitor is not valid. Please make sure you had add monitor to the simulation.");
+  const Real dt = _dt;
+  const std::complex<Real> z = _impedance;
+  const Real k = std::sqrt(std::real(z));
+  const auto i = timeDft(_current_monitor->data(), dt, frequencies, -1.5 * dt);
+  const auto v = timeDft(_voltage_monitor->data(), dt, frequencies, 0.0);
+  _a.resize(frequencies.size());
+  _b.resize(frequencies.size());
+  for (std::size_t q = 0; q < frequencies.size(); ++q) {
+    _a[q] = Real{0.5} * (v[q] + z * i[q]) / k;
+    _b[q] = Real{0.5} * (v[q] - std::conj(z) * i[q]) / k;
+  }
+}
+
+void Network::init(Real dt) {
+  std::set<std::size_t> seen;
+  for (const auto& p : _ports) {
+    p->init(dt);
+    if (!seen.insert(p->index()).second) throw XFDTDException("Port index must be unique");
+  }
+}
+
+void Network::compute() {
+  for (auto& p : _ports) p->calculateSParameters(_frequencies);
+  for (const auto& pi : _ports) {
+    if (!pi->isSource()) continue;
+    for (const auto& pj : _ports) {
+      std::vector<std::complex<Real>> s(_frequencies.size());
+      for (std::size_t q = 0; q < s.size(); ++q) s[q] = pj->b()[q] / pi->a()[q];
+      _s_parameters[(int)(pj->index() * 10 + pi->index())] = std::move(s);
+    }
+  }
+}
+
+void Network::output() {
+  compute();
+  const std::filesystem::path out(_output_dir);
+  std::filesystem::create_directories(out);
+  for (const auto& [key, s] : _s_parameters)
+    writeComplexNpy((out / ("s" + std::to_string(key) + ".npy")).string(), s.data(), s.size());
+  writeRealNpy((out / "frequencies.npy").string(),
+               std::vector<Real>(_frequencies.begin(), _frequencies.end()));
 }
 
 }  // namespace xfdtd

@@ -59,6 +59,7 @@ def load():
                                        _dp, _dp, i64], ctypes.c_int),
         "xfdtd_scene_nf2ff_td": ([vp, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
         "xfdtd_scene_line_monitor": ([vp, i32, i32, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
+        "xfdtd_scene_s_parameter": ([vp, i32, _dp, i64, ctypes.POINTER(i64)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -75,7 +76,7 @@ def exported_symbols() -> List[str]:
             "xfdtd_scene_coefficients", "xfdtd_scene_field", "xfdtd_scene_movie",
             "xfdtd_scene_nf2ff", "xfdtd_scene_far_field", "xfdtd_scene_field_time",
             "xfdtd_scene_write_outputs", "xfdtd_scene_dft_objective", "xfdtd_scene_nf2ff_td",
-            "xfdtd_scene_line_monitor"]
+            "xfdtd_scene_line_monitor", "xfdtd_scene_s_parameter"]
 
 
 class SceneRun:
@@ -252,6 +253,15 @@ class SceneRun:
         self._check(self.L.xfdtd_scene_line_monitor(self.h, k, index, out.ctypes.data_as(_dp),
                                                     cnt.value, ctypes.byref(cnt)))
         return out.reshape(2, -1)
+
+    def s_parameter(self, key: int) -> np.ndarray:
+        """S[key] (key = 10 j + i) of the scene's network, per frequency."""
+        cnt = ctypes.c_int64()
+        self._check(self.L.xfdtd_scene_s_parameter(self.h, key, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value)
+        self._check(self.L.xfdtd_scene_s_parameter(self.h, key, out.ctypes.data_as(_dp),
+                                                   cnt.value, ctypes.byref(cnt)))
+        return out[0::2] + 1j * out[1::2]
 
     def nf2ff_td(self) -> dict:
         """Time-domain NF2FF far-field series (w_theta, w_phi, u_theta, u_phi)."""

@@ -12,6 +12,8 @@ reference's user-facing API one to one:
 * ``TFSF3D(x, y, z, theta, phi, psi, waveform)``      include/xfdtd/waveform_source/tfsf_3d.h:10-11
 * ``CurrentSource(name, cube, dir, R, waveform)``     include/xfdtd/object/lumped_element/current_source.h:11-14
 * ``VoltageSource(name, cube, dir, R, waveform)``     include/xfdtd/object/lumped_element/voltage_source.h:15-18
+* ``Network(ports, freqs) / Port(i, src, z, c, v)``   include/xfdtd/network/{network,port}.h
+* ``PecPlane(name, cube)``                            include/xfdtd/object/lumped_element/pec_plane.h:10-12
 * ``Resistor / Capacitor / Inductor(name, cube, xyz, value)``
                                                        include/xfdtd/object/lumped_element/{resistor,capacitor,inductor}.h:9-12
 * ``MovieMonitor(FieldMonitor(cube, field), k)``      include/xfdtd/monitor/movie_monitor.h:13-15
@@ -218,6 +220,45 @@ class VoltageSourceSpec(CurrentSourceSpec):
 
 
 @dataclass
+class PortSpec:
+    """``Port(index, is_source, impedance, current_monitor, voltage_monitor)``
+    with the monitors named."""
+    index: int
+    is_source: bool
+    impedance: complex
+    current: str
+    voltage: str
+
+    def text(self) -> str:
+        z = complex(self.impedance)
+        return (f"port {self.index} {int(bool(self.is_source))} {_f(z.real)} {_f(z.imag)} "
+                f"{self.current} {self.voltage}")
+
+
+@dataclass
+class NetworkSpec:
+    """``Network(ports, frequencies, output_dir)``."""
+    frequencies: List[float]
+    ports: List[PortSpec] = field(default_factory=list)
+
+    def text(self) -> str:
+        return "\n".join([f"network {len(self.frequencies)} " +
+                          " ".join(_f(float(f)) for f in self.frequencies)] +
+                         [p.text() for p in self.ports])
+
+
+@dataclass
+class PecPlaneSpec:
+    """``PecPlane(name, cube)``: a Cube flat on one axis."""
+    name: str
+    shape: Shape
+
+    def text(self) -> str:
+        o, s = self.shape.origin, self.shape.size
+        return f"pec_plane {self.name} " + " ".join(_f(v) for v in (*o, *s))
+
+
+@dataclass
 class LumpedSpec:
     """Resistor, Capacitor or Inductor (kind "resistor" | "capacitor" |
     "inductor") on a Cube of E nodes along `axis` ("X" | "Y" | "Z")."""
@@ -339,6 +380,7 @@ class Scene:
     objects: List[ObjectSpec] = field(default_factory=list)
     current_sources: List[CurrentSourceSpec] = field(default_factory=list)
     lumped_elements: List[LumpedSpec] = field(default_factory=list)
+    pec_planes: List[PecPlaneSpec] = field(default_factory=list)
     pmls: List[PMLSpec] = field(default_factory=list)
     tfsf: Optional[TFSFSpec] = None
     movies: List[MovieSpec] = field(default_factory=list)
@@ -346,6 +388,7 @@ class Scene:
     line_monitors: List[LineMonitorSpec] = field(default_factory=list)
     nf2ff: Optional[NF2FFSpec] = None
     nf2ff_td: Optional[NF2FFTDSpec] = None
+    network: Optional[NetworkSpec] = None
     name: str = "scene"
 
     def to_text(self) -> str:
@@ -355,6 +398,7 @@ class Scene:
         lines += [o.text() for o in self.objects]
         lines += [c.text() for c in self.current_sources]
         lines += [c.text() for c in self.lumped_elements]
+        lines += [c.text() for c in self.pec_planes]
         lines += [p.text() for p in self.pmls]
         if self.tfsf is not None:
             lines.append(self.tfsf.text())
@@ -365,6 +409,8 @@ class Scene:
             lines.append(self.nf2ff.text())
         if self.nf2ff_td is not None:
             lines.append(self.nf2ff_td.text())
+        if self.network is not None:
+            lines.append(self.network.text())
         return "\n".join(lines) + "\n"
 
     def write(self, path: str) -> str:
@@ -586,3 +632,44 @@ def batched_spheres(count: int = 96, seed: int = 1, steps: int = 3000, n_lo: int
     sizes (batched_sphere_params), each lit by its own plane wave."""
     return [batched_sphere(steps=steps, **p, **kw)
             for p in batched_sphere_params(count, seed, n_lo, n_hi)]
+
+
+def microstrip_line(steps: int = 1000, n_freqs: int = 500, scale: int = 1) -> Scene:
+    """The reference's microstrip-line example (test/src/examples/microstrip_line.cpp):
+    cells 0.203 x 0.203 x 0.1325 mm; a 60 x 64 x 16-cell air domain on a
+    6-cell eps_r = 2.2 substrate with a PEC ground plane and a 12-cell-wide
+    PEC strip; a 50-ohm z-directed VoltageSource under the strip at y = 0
+    driven by gaussian(tau, 4.5 tau), tau = 30 dz / 6e8; port 1 (source,
+    50 ohm) from a voltage monitor under the strip and a current monitor on
+    it 40 cells along; S11 at `n_freqs` frequencies in [20 MHz, 10 GHz];
+    10-cell CPML on all faces but ZN (inside the domain on XN, XP, YP),
+    CFL 0.9.  `scale` divides the cell counts for small parity cases."""
+    dx = dy = 0.203e-3 * scale
+    dz = 0.1325e-3 * scale
+    q = lambda v: v // scale  # noqa: E731
+    s = Scene(dl=(dx, dy, dz), cfl=0.9, steps=steps, name="microstrip_line")
+    s.objects.append(ObjectSpec("domain", cube((0.0, -q(4) * dy, 0.0),
+                                               (q(60) * dx, q(64) * dy, q(16) * dz)), air()))
+    s.objects.append(ObjectSpec("substrate", cube((0.0, 0.0, 0.0),
+                                                  (q(60) * dx, q(60) * dy, q(6) * dz)),
+                                Material("simple", 2.2, 1.0, 0.0, 0.0)))
+    s.pec_planes += [
+        PecPlaneSpec("microstrip_0", cube((q(24) * dx, 0.0, q(6) * dz), (q(12) * dx, q(60) * dy, 0.0))),
+        PecPlaneSpec("ground_0", cube((0.0, 0.0, 0.0), (q(60) * dx, q(60) * dy, 0.0))),
+    ]
+    tau = q(30) * dz / 6e8
+    s.current_sources.append(VoltageSourceSpec(
+        "v_s", cube((q(24) * dx, 0.0, 0.0), (q(12) * dx, 0.0, q(6) * dz)), "ZP", 50.0,
+        Waveform("gaussian", tau, 4.5 * tau)))
+    s.line_monitors += [
+        LineMonitorSpec("voltage", "v1", cube((q(24) * dx, q(40) * dy, 0.0),
+                                              (q(12) * dx, 0.0, q(6) * dz)), "ZP"),
+        LineMonitorSpec("current", "c1", cube((q(24) * dx, q(40) * dy, q(6) * dz),
+                                              (q(12) * dx, 0.0, 0.0)), "YP"),
+    ]
+    s.network = NetworkSpec(list(np.linspace(2e7, 10e9, n_freqs)),
+                            [PortSpec(1, True, 50.0, "c1", "v1")])
+    t = q(10)
+    s.pmls = [PMLSpec(-t, "XN"), PMLSpec(-t, "XP"), PMLSpec(t, "YN"), PMLSpec(-t, "YP"),
+              PMLSpec(t, "ZP")]
+    return s
