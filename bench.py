@@ -655,6 +655,11 @@ def main():
     ap.add_argument("--ichunk", type=int, default=None, help="planes per CTA, fused sweeps")
     ap.add_argument("--march-ichunk", type=int, default=None,
                     help="planes per CTA, split marching sweeps")
+    ap.add_argument("--march-wide", type=int, default=None,
+                    help="1: two-rows-per-thread form on the CPML-free interior (default), "
+                         "0: one-row form")
+    ap.add_argument("--march-concurrent", type=int, default=None,
+                    help="1: CPML-free box and face kernels beside the CPML form (default)")
     args = ap.parse_args()
     global KIND
     KIND = args.workload
@@ -711,7 +716,9 @@ def main():
     # FP32 form (headline)
     sc = workload_scene(steps=warmup + steps, n=args.grid)
     opts = {} if args.kernel is None else {"kernel": args.kernel}
-    for key, val in (("ichunk", args.ichunk), ("march_ichunk", args.march_ichunk)):
+    for key, val in (("ichunk", args.ichunk), ("march_ichunk", args.march_ichunk),
+                     ("march_wide", args.march_wide),
+                     ("march_concurrent", args.march_concurrent)):
         if val is not None:
             opts[key] = val
     run32 = SceneRun(sc, precision=1, options=opts)

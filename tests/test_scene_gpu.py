@@ -265,3 +265,24 @@ def test_voltage_and_current_monitors_match_oracle(tmp_path):
     run.write_outputs(str(tmp_path))
     v = np.load(tmp_path / "monitors" / "v_dipole.npy")
     assert v.shape == (2, 150) and np.array_equal(v, run.line_monitor("voltage", 0))
+
+
+@pytest.mark.parametrize("precision,tol", [(0, TOL64), (1, 1e-4)], ids=["fp64", "fp32"])
+def test_wide_interior_form_matches_oracle(precision, tol):
+    """128^3 dielectric boxes with an 8-cell CPML: large enough that the
+    default sweep has a CPML-free interior box, swept by the two-rows-per-
+    thread form (march_wide 1) or the one-row form (march_wide 0); both
+    against the oracle, and against each other."""
+    sc = S.dielectric_boxes(n=128, pml=8, n_boxes=24, edge_lo=4, edge_hi=20, steps=60)
+    orc = RefSimulation(sc)
+    orc.run()
+    got = {}
+    for wide in (1, 0):
+        run = SceneRun(sc, precision=precision, options={"kernel": 4, "march_wide": wide})
+        run.run()
+        errs = _fields_rel(run, orc)
+        assert max(errs) <= tol, (wide, errs)
+        got[wide] = run.fields()
+        run.close()
+    for a, b in zip(got[1], got[0]):
+        assert rel_l2(a, b) <= (1e-14 if precision == 0 else 1e-6)

@@ -21,6 +21,7 @@
 #include "fused_tma.cuh"
 #include "march.cuh"
 #include "march_tma.cuh"
+#include "march_wide.cuh"
 #include "fmarch.cuh"
 #include "fvec.cuh"
 #include "farfield.cuh"
@@ -135,6 +136,12 @@ struct xfd_engine {
   // monitor copy-out: D2H of finished frames on a side stream
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t copy_ev = nullptr;
+  // Side streams of the TMA marching sweeps: the CPML-free box and the
+  // lattice-face kernel run beside the CPML form (disjoint nodes), forked
+  // from and joined back into `stream` (also inside graph capture).
+  cudaStream_t side[2]{};
+  cudaEvent_t fork_ev = nullptr, join_ev[2]{};
+  bool march_concurrent = true;
   std::vector<void*> host_allocs;
 
   // graph
@@ -149,6 +156,8 @@ struct xfd_engine {
   bool tma_ready = false;
   TmaMaps tma[2]{};       // tensor maps over buffer 0 / 1 (and the class index)
   MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
+  MarchMaps mtma_w[2]{};  // and of their two-rows-per-thread interior form
+  bool march_wide = false;  // sweep the interior box with k_march_*_wide
   int2* d_xlayer = nullptr;  // per x plane: CPML layer code of the H / E layers
   size_t xlayer_slabs = (size_t)-1;  // slab count the table was built for
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
@@ -314,6 +323,10 @@ constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchS
 // fewer stages keep their shared memory from capping that.
 template <typename T>
 constexpr int march_free_stages() { return sizeof(T) == 8 ? 3 : 4; }
+// Stages of the two-rows-per-thread interior form (3 CTAs per SM in FP32,
+// 2 in FP64).
+template <typename T>
+constexpr int march_wide_stages() { return sizeof(T) == 8 ? 4 : 5; }
 constexpr int kFmStages = 4;
 constexpr int kFmTJ = 8;
 template <typename T>
@@ -365,22 +378,23 @@ xfd_status tensor_map_encoder(xfd_engine* e, EncodeTiledFn* out) {
 
 // Tensor maps of the marching sweeps over six field arrays of the lattice
 // layout (the engine's buffers, or the adjoint's scaled fields).
+// `tj` rows per tile (halo boxes tj + 1 rows).
 template <typename T>
-xfd_status build_march_maps(xfd_engine* e, void* const f[6], MarchMaps* m) {
+xfd_status build_march_maps(xfd_engine* e, void* const f[6], MarchMaps* m, int tj = kMTJ) {
   EncodeTiledFn encode = nullptr;
   xfd_status st = tensor_map_encoder(e, &encode);
   if (st != XFD_OK) return st;
-  using MG = MarchGeom<T, kMTJ, 32>;
+  const int W = 32 + 16 / (int)sizeof(T);
   const CUtensorMapDataType dt =
       sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   for (int c = 0; c < 6; ++c) {
-    CUresult r = encode_lattice(encode, &m->halo[c], dt, sizeof(T), f[c], e->L, MG::W, MG::R);
+    CUresult r = encode_lattice(encode, &m->halo[c], dt, sizeof(T), f[c], e->L, W, tj + 1);
     if (r == CUDA_SUCCESS)
-      r = encode_lattice(encode, &m->tile[c], dt, sizeof(T), f[c], e->L, 32, kMTJ);
+      r = encode_lattice(encode, &m->tile[c], dt, sizeof(T), f[c], e->L, 32, tj);
     if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march %d): %d", c, (int)r);
   }
   CUresult r = encode_lattice(encode, &m->cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, e->cls, e->L, 32,
-                              kMTJ);
+                              tj);
   if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (march class): %d", (int)r);
   return XFD_OK;
 }
@@ -420,6 +434,7 @@ xfd_status build_tma_maps(xfd_engine* e) {
   using MG = MarchGeom<T, kMTJ, 32>;
   for (int b = 0; b < 2; ++b) {
     xfd_status st = build_march_maps<T>(e, e->fbuf[b], &e->mtma[b]);
+    if (st == XFD_OK) st = build_march_maps<T>(e, e->fbuf[b], &e->mtma_w[b], kWideTJ);
     if (st != XFD_OK) return st;
   }
   // Fused marching sweep: E (TJ+1 rows) and H (TJ rows) boxes of width
@@ -480,6 +495,13 @@ xfd_status build_tma_maps(xfd_engine* e) {
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
   CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, kMTJ, 32, MF, false, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
+  constexpr int MW = march_wide_stages<T>();
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_wide<T, MW>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   WideGeom<T, MW>::smem()));
+  CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_wide<T, MW>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   WideGeom<T, MW>::smem()));
   e->tma_ready = true;
   return XFD_OK;
 }
@@ -744,24 +766,64 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     const bool m_in = mbox && mlo[0] >= 1 && 32 * mhi[0] <= e->L.nz && mlo[1] >= 1 &&
                       kMTJ * mhi[1] <= e->L.ny && mlo[2] >= 1 &&
                       mhi[2] * e->march_ichunk <= e->L.nx;
-    auto launch_march = [&](auto kfree, auto kfree_in, auto kcp) {
-      if (mbox) {
+    // The two-rows-per-thread form takes the interior box's whole pairs of
+    // 8-row tiles (16-row tiles wy_lo .. wy_hi-1); the CPML form sweeps the
+    // rest, an unpaired tile row included.
+    const int wy_lo = (mlo[1] + 1) / 2, wy_hi = mhi[1] / 2;
+    const bool wide = march_tma && m_in && e->march_wide && wy_hi > wy_lo;
+    if (wide) {
+      mtp.box_lo[1] = 2 * wy_lo;
+      mtp.box_hi[1] = 2 * wy_hi;
+    }
+    constexpr int MW = march_wide_stages<T>();
+    // With march_concurrent, the box form runs on side[0] and the face kernel
+    // on side[1], beside the CPML form on the main stream.
+    const bool conc = march_tma && e->march_concurrent;
+    auto fork = [&]() -> cudaError_t {
+      if (!conc) return cudaSuccess;
+      cudaError_t c = cudaEventRecord(e->fork_ev, s);
+      for (int q = 0; q < 2 && c == cudaSuccess; ++q) c = cudaStreamWaitEvent(e->side[q], e->fork_ev, 0);
+      return c;
+    };
+    auto join = [&]() -> cudaError_t {
+      if (!conc) return cudaSuccess;
+      cudaError_t c = cudaSuccess;
+      for (int q = 0; q < 2 && c == cudaSuccess; ++q) {
+        c = cudaEventRecord(e->join_ev[q], e->side[q]);
+        if (c == cudaSuccess) c = cudaStreamWaitEvent(s, e->join_ev[q], 0);
+      }
+      return c;
+    };
+    cudaStream_t s_box = conc ? e->side[0] : s, s_edge = conc ? e->side[1] : s;
+    auto launch_march = [&](auto kfree, auto kfree_in, auto kwide, auto kcp) {
+      if (wide) {
+        MarchTmaP<T> q = mtp;
+        q.m = e->mtma_w[e->cur];
+        q.org[0] = mlo[0];
+        q.org[1] = wy_lo;
+        q.org[2] = mlo[2];
+        const dim3 g(mhi[0] - mlo[0], wy_hi - wy_lo, mhi[2] - mlo[2]);
+        kwide<<<g, dim3(32, kWideCW + 1, 1), WideGeom<T, MW>::smem(), s_box>>>(q);
+      } else if (mbox) {
         MarchTmaP<T> q = mtp;
         for (int a = 0; a < 3; ++a) q.org[a] = mlo[a];
         const dim3 g(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]);
         if (m_in)
-          kfree_in<<<g, blk_m, msm_free, s>>>(q);
+          kfree_in<<<g, blk_m, msm_free, s_box>>>(q);
         else
-          kfree<<<g, blk_m, msm_free, s>>>(q);
+          kfree<<<g, blk_m, msm_free, s_box>>>(q);
       }
       kcp<<<grd_m, blk_m, msm, s>>>(mtp);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma) {
+      cudaError_t c = fork();
+      if (c != cudaSuccess) return c;
       launch_march(k_march_h_tma<T, kMTJ, 32, MF, false, false>,
-                   k_march_h_tma<T, kMTJ, 32, MF, false, true>,
+                   k_march_h_tma<T, kMTJ, 32, MF, false, true>, k_march_h_wide<T, MW>,
                    k_march_h_tma<T, kMTJ, 32, MS, true, false>);
-      k_edge_h<T><<<edge_blocks, 256, 0, s>>>(yp);
+      k_edge_h<T><<<edge_blocks, 256, 0, s_edge>>>(yp);
+      if ((c = join()) != cudaSuccess) return c;
     }
     else if (march)
       k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
@@ -779,10 +841,13 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     if (e->ade_kind >= 0) k_ade_gather<T><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields);
     if (e->n_ovr) k_ovr_gather<T><<<blocks_for(e->n_ovr, 256), 256, 0, s>>>(ovr_of<T>(e), fields);
     if (march_tma) {
+      cudaError_t c = fork();
+      if (c != cudaSuccess) return c;
       launch_march(k_march_e_tma<T, kMTJ, 32, MF, false, false>,
-                   k_march_e_tma<T, kMTJ, 32, MF, false, true>,
+                   k_march_e_tma<T, kMTJ, 32, MF, false, true>, k_march_e_wide<T, MW>,
                    k_march_e_tma<T, kMTJ, 32, MS, true, false>);
-      k_edge_e<T><<<edge_blocks, 256, 0, s>>>(yp);
+      k_edge_e<T><<<edge_blocks, 256, 0, s_edge>>>(yp);
+      if ((c = join()) != cudaSuccess) return c;
     }
     else if (march)
       k_march_e<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
@@ -1089,9 +1154,20 @@ xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
   if (c != cudaSuccess) return fail(nullptr, XFD_ERR_CUDA, "stream: %s", cudaGetErrorString(c));
   c = cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking);
   if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->copy_ev, cudaEventDisableTiming);
+  for (int q = 0; q < 2 && c == cudaSuccess; ++q) {
+    c = cudaStreamCreateWithFlags(&e->side[q], cudaStreamNonBlocking);
+    if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->join_ev[q], cudaEventDisableTiming);
+  }
+  if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
   if (c != cudaSuccess) {
+    for (int q = 0; q < 2; ++q) {
+      if (e->side[q]) cudaStreamDestroy(e->side[q]);
+      if (e->join_ev[q]) cudaEventDestroy(e->join_ev[q]);
+    }
+    if (e->copy_ev) cudaEventDestroy(e->copy_ev);
+    if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
     cudaStreamDestroy(e->stream);
-    return fail(nullptr, XFD_ERR_CUDA, "copy stream: %s", cudaGetErrorString(c));
+    return fail(nullptr, XFD_ERR_CUDA, "copy / side streams: %s", cudaGetErrorString(c));
   }
   e->precision = g->precision;
   e->wsize = g->precision == XFD_FP64 ? 8 : 4;
@@ -1162,6 +1238,11 @@ void xfd_destroy(xfd_engine* e) {
   for (void* p : e->host_allocs) cudaFreeHost(p);
   if (e->copy_ev) cudaEventDestroy(e->copy_ev);
   if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
+  for (int q = 0; q < 2; ++q) {
+    if (e->join_ev[q]) cudaEventDestroy(e->join_ev[q]);
+    if (e->side[q]) cudaStreamDestroy(e->side[q]);
+  }
+  if (e->fork_ev) cudaEventDestroy(e->fork_ev);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -1987,6 +2068,8 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "kernel")) *value = e->kernel_mode;
   else if (!strcmp(name, "ichunk")) *value = e->ichunk;
   else if (!strcmp(name, "march_ichunk")) *value = e->march_ichunk;
+  else if (!strcmp(name, "march_wide")) *value = e->march_wide ? 1 : 0;
+  else if (!strcmp(name, "march_concurrent")) *value = e->march_concurrent ? 1 : 0;
   else return fail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -2009,7 +2092,10 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096)
       return fail(e, XFD_ERR_INVALID_ARGUMENT, "march_ichunk range");
     e->march_ichunk = (int)value;
-
+  } else if (!strcmp(name, "march_wide")) {
+    e->march_wide = value != 0;
+  } else if (!strcmp(name, "march_concurrent")) {
+    e->march_concurrent = value != 0;
   } else {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
