@@ -660,6 +660,11 @@ def main():
                          "0: one-row form")
     ap.add_argument("--march-concurrent", type=int, default=None,
                     help="1: CPML-free box and face kernels beside the CPML form (default)")
+    ap.add_argument("--march-shift", type=int, default=None,
+                    help="1: tile grid shifted to fit the CPML layers, 0: unshifted (default)")
+    ap.add_argument("--march-split-axes", type=int, default=None,
+                    help="1: CPML tiles in x-only, y-only, z-only and several-axis lists "
+                         "(default), 0: one list")
     args = ap.parse_args()
     global KIND
     KIND = args.workload
@@ -718,7 +723,9 @@ def main():
     opts = {} if args.kernel is None else {"kernel": args.kernel}
     for key, val in (("ichunk", args.ichunk), ("march_ichunk", args.march_ichunk),
                      ("march_wide", args.march_wide),
-                     ("march_concurrent", args.march_concurrent)):
+                     ("march_concurrent", args.march_concurrent),
+                     ("march_split_axes", args.march_split_axes),
+                     ("march_shift", args.march_shift)):
         if val is not None:
             opts[key] = val
     run32 = SceneRun(sc, precision=1, options=opts)

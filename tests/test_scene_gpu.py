@@ -271,18 +271,24 @@ def test_voltage_and_current_monitors_match_oracle(tmp_path):
 def test_wide_interior_form_matches_oracle(precision, tol):
     """128^3 dielectric boxes with an 8-cell CPML: large enough that the
     default sweep has a CPML-free interior box, swept by the two-rows-per-
-    thread form (march_wide 1) or the one-row form (march_wide 0); both
-    against the oracle, and against each other."""
+    thread form (march_wide 1) or the one-row form (march_wide 0), and CPML
+    tiles in x-only, y-only, z-only and several-axis lists on a tile grid
+    shifted to the CPML layers (or one list on the unshifted grid, run
+    without the side streams); all against the oracle, and against each
+    other."""
     sc = S.dielectric_boxes(n=128, pml=8, n_boxes=24, edge_lo=4, edge_hi=20, steps=60)
     orc = RefSimulation(sc)
     orc.run()
     got = {}
-    for wide in (1, 0):
-        run = SceneRun(sc, precision=precision, options={"kernel": 4, "march_wide": wide})
+    for key, opts in (("wide", {"march_wide": 1}), ("one-row", {"march_wide": 0}),
+                      ("one-list", {"march_split_axes": 0, "march_concurrent": 0,
+                                    "march_shift": 0})):
+        run = SceneRun(sc, precision=precision, options={"kernel": 4, **opts})
         run.run()
         errs = _fields_rel(run, orc)
-        assert max(errs) <= tol, (wide, errs)
-        got[wide] = run.fields()
+        assert max(errs) <= tol, (key, errs)
+        got[key] = run.fields()
         run.close()
-    for a, b in zip(got[1], got[0]):
-        assert rel_l2(a, b) <= (1e-14 if precision == 0 else 1e-6)
+    for key in ("one-row", "one-list"):
+        for a, b in zip(got["wide"], got[key]):
+            assert rel_l2(a, b) <= (1e-14 if precision == 0 else 1e-6), key

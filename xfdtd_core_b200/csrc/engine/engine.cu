@@ -51,6 +51,8 @@ struct LumpedH {
 
 }  // namespace
 
+constexpr int kSides = 4;  // side streams of the TMA marching sweeps
+
 struct xfd_engine {
   int device = 0;
   int precision = XFD_FP64;
@@ -139,8 +141,8 @@ struct xfd_engine {
   // Side streams of the TMA marching sweeps: the CPML-free box and the
   // lattice-face kernel run beside the CPML form (disjoint nodes), forked
   // from and joined back into `stream` (also inside graph capture).
-  cudaStream_t side[2]{};
-  cudaEvent_t fork_ev = nullptr, join_ev[2]{};
+  cudaStream_t side[kSides]{};
+  cudaEvent_t fork_ev = nullptr, join_ev[kSides]{};
   bool march_concurrent = true;
   std::vector<void*> host_allocs;
 
@@ -158,6 +160,18 @@ struct xfd_engine {
   MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
   MarchMaps mtma_w[2]{};  // and of their two-rows-per-thread interior form
   bool march_wide = false;  // sweep the interior box with k_march_*_wide
+  // Tile lists of the CPML form, by the CPML axes their tiles meet: x only,
+  // y only, z only, several (lists 0..3 at mt_off[q] .. mt_off[q+1]).
+  bool march_split_axes = true;
+  // Shift the tile grid to fit the CPML layers.  Off by default: a k shift
+  // that is not a multiple of 32 values leaves every tile row off the 128-byte
+  // lines (TMA boxes and the warps' stores), which costs more than the larger
+  // CPML-free box gains.
+  bool march_shift = false;
+  int4* d_mtiles = nullptr;
+  size_t mtiles_cap = 0;
+  int mt_off[5] = {0, 0, 0, 0, 0};
+  long long mtiles_key = -1;
   int2* d_xlayer = nullptr;  // per x plane: CPML layer code of the H / E layers
   size_t xlayer_slabs = (size_t)-1;  // slab count the table was built for
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
@@ -495,6 +509,20 @@ xfd_status build_tma_maps(xfd_engine* e) {
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
   CUDA_TRY(e, cudaFuncSetAttribute(k_march_e_tma<T, kMTJ, 32, MF, false, true>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MF)));
+  {
+    auto attr = [&](const void* f) {
+      return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, MG::smem(MS));
+    };
+    const void* fs[8] = {(const void*)k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 1>,
+                         (const void*)k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 2>,
+                         (const void*)k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 4>,
+                         (const void*)k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 7>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 1>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 2>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 4>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 7>};
+    for (const void* f : fs) CUDA_TRY(e, attr(f));
+  }
   constexpr int MW = march_wide_stages<T>();
   CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_wide<T, MW>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -591,35 +619,171 @@ void fmarch_split(const xfd_engine* e, int nt[3], int lo[3], int hi[3]) {
 
 // The box of (k tile of 32, j tile of 8, chunk of march_ichunk planes) of
 // the split marching sweeps whose nodes lie in no CPML layer of either phase.
-void march_split(const xfd_engine* e, int lo[3], int hi[3]) {
+// Along grid dimension g (0: k tiles of 32, 1: j tiles of kMTJ, 2: chunks of
+// march_ichunk x planes) with the grid shifted by sh nodes (-size < sh <= 0),
+// tile b covers nodes [sh + b size, sh + (b+1) size) within the lattice.  The
+// longest run [lo, hi) of tiles that meet no CPML layer of either phase;
+// returns the nodes it covers.
+int march_free_run(const xfd_engine* e, int g, int sh, int& lo, int& hi) {
   const Lat& L = e->L;
-  const int nt[3] = {(L.nz + 31) / 32, (L.ny + kMTJ - 1) / kMTJ,
-                     (L.nx + 1 + e->march_ichunk - 1) / e->march_ichunk};
   const int size[3] = {32, kMTJ, e->march_ichunk};
   const int n_nodes[3] = {L.nz, L.ny, L.nx + 1};
   const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
-  for (int g = 0; g < 3; ++g) {
-    const int m = axis_of[g];
-    auto is_free = [&](int b) {
-      const int a0 = b * size[g], a1 = std::min((b + 1) * size[g], n_nodes[g]) - 1;
-      for (const auto& S : e->slabs) {
-        if (S.m != m) continue;
-        if (a0 < S.e_lo + S.n && S.e_lo <= a1) return false;
-        if (a0 < S.h_lo + S.n && S.h_lo <= a1) return false;
-      }
-      return true;
-    };
-    int best_lo = 0, best_len = 0;
-    for (int b = 0; b < nt[g];) {
-      if (!is_free(b)) { ++b; continue; }
-      int c = b;
-      while (c < nt[g] && is_free(c)) ++c;
-      if (c - b > best_len) { best_lo = b; best_len = c - b; }
-      b = c;
+  const int m = axis_of[g], z = size[g], n = n_nodes[g];
+  const int nt = (n - sh + z - 1) / z;
+  auto is_free = [&](int b) {
+    const int a0 = std::max(sh + b * z, 0), a1 = std::min(sh + (b + 1) * z, n) - 1;
+    for (const auto& S : e->slabs) {
+      if (S.m != m) continue;
+      if (a0 < S.e_lo + S.n && S.e_lo <= a1) return false;
+      if (a0 < S.h_lo + S.n && S.h_lo <= a1) return false;
     }
-    lo[g] = best_lo;
-    hi[g] = best_lo + best_len;
+    return true;
+  };
+  lo = hi = 0;
+  int best = 0;
+  for (int b = 0; b < nt;) {
+    if (!is_free(b)) {
+      ++b;
+      continue;
+    }
+    int c = b;
+    while (c < nt && is_free(c)) ++c;
+    const int nodes = std::min(sh + c * z, n) - std::max(sh + b * z, 0);
+    if (nodes > best) {
+      best = nodes;
+      lo = b;
+      hi = c;
+    }
+    b = c;
   }
+  return best;
+}
+
+// The CPML-free box of the unshifted tile grid (the batched sweeps' split).
+void march_split(const xfd_engine* e, int lo[3], int hi[3]) {
+  for (int g = 0; g < 3; ++g) march_free_run(e, g, 0, lo[g], hi[g]);
+}
+
+// Work split of the TMA marching sweeps for the current options: the
+// CPML-free box (in 8-row tiles), whether it is away from every lattice
+// boundary, the 16-row tiles of the two-rows-per-thread form, and the box of
+// tiles that the CPML form skips.
+struct MarchLayout {
+  int nt[3];                 // tiles along k, j and chunks along i
+  int shift[3];              // grid shift (nodes) along k, j, i
+  int lo[3], hi[3];          // CPML-free box
+  bool box, in, wide;
+  int wy_lo, wy_hi;          // 16-row tiles of the wide form
+  int skip_lo[3], skip_hi[3];  // tiles swept by the box or wide form
+};
+
+MarchLayout march_layout(const xfd_engine* e) {
+  MarchLayout m{};
+  const Lat& L = e->L;
+  const int size[3] = {32, kMTJ, e->march_ichunk};
+  const int n_nodes[3] = {L.nz, L.ny, L.nx + 1};
+  // Per axis the shift whose CPML-free run covers the most nodes (k in steps
+  // of 8 nodes, so that every TMA x coordinate stays a multiple of 16 bytes
+  // for the field and the uint16 class maps alike).
+  const int step[3] = {8, 1, 1};
+  for (int g = 0; g < 3; ++g) {
+    int best = -1;
+    for (int sh = 0; sh > -size[g]; sh -= step[g]) {
+      if (!e->march_shift && sh != 0) break;
+      int lo = 0, hi = 0;
+      const int nodes = march_free_run(e, g, sh, lo, hi);
+      if (nodes > best) {
+        best = nodes;
+        m.shift[g] = sh;
+        m.lo[g] = lo;
+        m.hi[g] = hi;
+      }
+    }
+    m.nt[g] = (n_nodes[g] - m.shift[g] + size[g] - 1) / size[g];
+  }
+  m.box = m.hi[0] > m.lo[0] && m.hi[1] > m.lo[1] && m.hi[2] > m.lo[2];
+  // The box is away from every lattice boundary when no tile holds k = 0,
+  // j = 0 or a node past nz-1 / ny-1 and no chunk holds plane 0 or nx.
+  m.in = m.box && 32 * m.lo[0] + m.shift[0] >= 1 && 32 * m.hi[0] + m.shift[0] <= L.nz &&
+         kMTJ * m.lo[1] + m.shift[1] >= 1 && kMTJ * m.hi[1] + m.shift[1] <= L.ny &&
+         e->march_ichunk * m.lo[2] + m.shift[2] >= 1 &&
+         e->march_ichunk * m.hi[2] + m.shift[2] <= L.nx;
+  // The two-rows-per-thread form takes the interior box's whole pairs of
+  // 8-row tiles; the CPML form sweeps the rest, an unpaired tile row included.
+  m.wy_lo = (m.lo[1] + 1) / 2;
+  m.wy_hi = m.hi[1] / 2;
+  m.wide = m.in && e->march_wide && m.wy_hi > m.wy_lo;
+  for (int a = 0; a < 3; ++a) {
+    m.skip_lo[a] = m.box ? m.lo[a] : 0;
+    m.skip_hi[a] = m.box ? m.hi[a] : 0;
+  }
+  if (m.wide) {
+    m.skip_lo[1] = 2 * m.wy_lo;
+    m.skip_hi[1] = 2 * m.wy_hi;
+  }
+  return m;
+}
+
+// The CPML form's tiles outside the skip box, sorted by the CPML axes whose
+// layers (of either phase) their node ranges meet: lists of x-only, y-only,
+// z-only and several-axis (or none) tiles, as (0, k tile, j tile, chunk).
+void march_tile_lists(const xfd_engine* e, std::vector<int4> lists[4]) {
+  const MarchLayout m = march_layout(e);
+  const Lat& L = e->L;
+  auto meets = [&](int axis, int a0, int a1) {  // node range [a0, a1)
+    for (const auto& S : e->slabs) {
+      if (S.m != axis) continue;
+      if (a0 < S.e_lo + S.n && S.e_lo < a1) return true;
+      if (a0 < S.h_lo + S.n && S.h_lo < a1) return true;
+    }
+    return false;
+  };
+  for (int gz = 0; gz < m.nt[2]; ++gz)
+    for (int gy = 0; gy < m.nt[1]; ++gy)
+      for (int gx = 0; gx < m.nt[0]; ++gx) {
+        if (gx >= m.skip_lo[0] && gx < m.skip_hi[0] && gy >= m.skip_lo[1] &&
+            gy < m.skip_hi[1] && gz >= m.skip_lo[2] && gz < m.skip_hi[2])
+          continue;
+        const int ich = e->march_ichunk, sx = m.shift[2], sy = m.shift[1], sz = m.shift[0];
+        const int mask =
+            (meets(0, std::max(gz * ich + sx, 0), std::min((gz + 1) * ich + sx, L.nx + 1)) ? 1
+                                                                                           : 0) |
+            (meets(1, std::max(gy * kMTJ + sy, 0), std::min((gy + 1) * kMTJ + sy, L.ny)) ? 2
+                                                                                          : 0) |
+            (meets(2, std::max(gx * 32 + sz, 0), std::min((gx + 1) * 32 + sz, L.nz)) ? 4 : 0);
+        int q = 3;
+        if (e->march_split_axes) q = mask == 1 ? 0 : mask == 2 ? 1 : mask == 4 ? 2 : 3;
+        lists[q].push_back(make_int4(0, gx, gy, gz));
+      }
+}
+
+xfd_status build_march_tiles(xfd_engine* e) {
+  const long long key = (long long)e->slabs.size() * 1000003LL + e->march_ichunk * 8 +
+                        (e->march_shift ? 4 : 0) + (e->march_wide ? 2 : 0) +
+                        (e->march_split_axes ? 1 : 0);
+  if (key == e->mtiles_key) return XFD_OK;
+  std::vector<int4> lists[4];
+  march_tile_lists(e, lists);
+  std::vector<int4> all;
+  e->mt_off[0] = 0;
+  for (int q = 0; q < 4; ++q) {
+    all.insert(all.end(), lists[q].begin(), lists[q].end());
+    e->mt_off[q + 1] = (int)all.size();
+  }
+  if (all.size() > e->mtiles_cap) {
+    void* p = nullptr;
+    xfd_status st = dev_alloc(e, &p, all.size() * sizeof(int4));
+    if (st != XFD_OK) return st;
+    e->d_mtiles = static_cast<int4*>(p);
+    e->mtiles_cap = all.size();
+  }
+  if (!all.empty())
+    CUDA_TRY(e, cudaMemcpy(e->d_mtiles, all.data(), all.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice));
+  e->mtiles_key = key;
+  e->graph_dirty = true;
+  return XFD_OK;
 }
 
 template <typename T>
@@ -742,78 +906,74 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
                    (unsigned)(e->L.nx + 1));
     // The TMA marching sweeps tile k < nz, j < ny (the faces k = nz, j = ny
     // go to k_edge_h / k_edge_e); the plain marching sweeps tile all nodes.
-    const dim3 grd_m(march_tma ? (unsigned)((e->L.nz + 31) / 32) : grd.x,
-                     march_tma ? (unsigned)((e->L.ny + kMTJ - 1) / kMTJ) : grd.y,
+    const dim3 grd_m(grd.x, grd.y,
                      (unsigned)((e->L.nx + 1 + mp.ichunk - 1) / std::max(1, mp.ichunk)));
     const unsigned edge_blocks = (unsigned)((edge_nodes(e->L) + 255) / 256);
-    // The CPML-free box of (k tile, j tile, chunk) for the TMA marching sweeps.
-    int mlo[3] = {0, 0, 0}, mhi[3] = {0, 0, 0};
-    bool mbox = false;
+    MarchLayout ml{};
     if (march_tma) {
-      march_split(e, mlo, mhi);
-      mbox = mhi[0] > mlo[0] && mhi[1] > mlo[1] && mhi[2] > mlo[2];
+      ml = march_layout(e);
       for (int a = 0; a < 3; ++a) {
-        mtp.box_lo[a] = mbox ? mlo[a] : 0;
-        mtp.box_hi[a] = mbox ? mhi[a] : 0;
+        mtp.box_lo[a] = ml.skip_lo[a];
+        mtp.box_hi[a] = ml.skip_hi[a];
+        mtp.shift[a] = ml.shift[a];
       }
     }
     const dim3 blk_m(32, kMTJ, 1);
     const size_t msm = MarchGeom<T, kMTJ, 32>::smem(MS);
     constexpr int MF = march_free_stages<T>();
     const size_t msm_free = MarchGeom<T, kMTJ, 32>::smem(MF);
-    // The box is away from every lattice boundary when no tile holds k = 0,
-    // j = 0 or a node past nz-1 / ny-1 and no chunk holds plane 0 or nx.
-    const bool m_in = mbox && mlo[0] >= 1 && 32 * mhi[0] <= e->L.nz && mlo[1] >= 1 &&
-                      kMTJ * mhi[1] <= e->L.ny && mlo[2] >= 1 &&
-                      mhi[2] * e->march_ichunk <= e->L.nx;
-    // The two-rows-per-thread form takes the interior box's whole pairs of
-    // 8-row tiles (16-row tiles wy_lo .. wy_hi-1); the CPML form sweeps the
-    // rest, an unpaired tile row included.
-    const int wy_lo = (mlo[1] + 1) / 2, wy_hi = mhi[1] / 2;
-    const bool wide = march_tma && m_in && e->march_wide && wy_hi > wy_lo;
-    if (wide) {
-      mtp.box_lo[1] = 2 * wy_lo;
-      mtp.box_hi[1] = 2 * wy_hi;
-    }
     constexpr int MW = march_wide_stages<T>();
-    // With march_concurrent, the box form runs on side[0] and the face kernel
-    // on side[1], beside the CPML form on the main stream.
+    // With march_concurrent, the box form runs on side[0], the face kernel on
+    // side[1], and the CPML form's tile lists spread over the main stream and
+    // side[1..3] (x-only after the faces, y-only, z-only, several on main).
     const bool conc = march_tma && e->march_concurrent;
     auto fork = [&]() -> cudaError_t {
       if (!conc) return cudaSuccess;
       cudaError_t c = cudaEventRecord(e->fork_ev, s);
-      for (int q = 0; q < 2 && c == cudaSuccess; ++q) c = cudaStreamWaitEvent(e->side[q], e->fork_ev, 0);
+      for (int q = 0; q < kSides && c == cudaSuccess; ++q)
+        c = cudaStreamWaitEvent(e->side[q], e->fork_ev, 0);
       return c;
     };
     auto join = [&]() -> cudaError_t {
       if (!conc) return cudaSuccess;
       cudaError_t c = cudaSuccess;
-      for (int q = 0; q < 2 && c == cudaSuccess; ++q) {
+      for (int q = 0; q < kSides && c == cudaSuccess; ++q) {
         c = cudaEventRecord(e->join_ev[q], e->side[q]);
         if (c == cudaSuccess) c = cudaStreamWaitEvent(s, e->join_ev[q], 0);
       }
       return c;
     };
     cudaStream_t s_box = conc ? e->side[0] : s, s_edge = conc ? e->side[1] : s;
-    auto launch_march = [&](auto kfree, auto kfree_in, auto kwide, auto kcp) {
-      if (wide) {
+    // kcp: the CPML form's tile-list kernels for x-only, y-only, z-only and
+    // several-axis tiles.
+    auto launch_march = [&](auto kfree, auto kfree_in, auto kwide, auto kx, auto ky, auto kz,
+                            auto kcp) {
+      if (ml.wide) {
         MarchTmaP<T> q = mtp;
         q.m = e->mtma_w[e->cur];
-        q.org[0] = mlo[0];
-        q.org[1] = wy_lo;
-        q.org[2] = mlo[2];
-        const dim3 g(mhi[0] - mlo[0], wy_hi - wy_lo, mhi[2] - mlo[2]);
+        q.org[0] = ml.lo[0];
+        q.org[1] = ml.wy_lo;
+        q.org[2] = ml.lo[2];
+        const dim3 g(ml.hi[0] - ml.lo[0], ml.wy_hi - ml.wy_lo, ml.hi[2] - ml.lo[2]);
         kwide<<<g, dim3(32, kWideCW + 1, 1), WideGeom<T, MW>::smem(), s_box>>>(q);
-      } else if (mbox) {
+      } else if (ml.box) {
         MarchTmaP<T> q = mtp;
-        for (int a = 0; a < 3; ++a) q.org[a] = mlo[a];
-        const dim3 g(mhi[0] - mlo[0], mhi[1] - mlo[1], mhi[2] - mlo[2]);
-        if (m_in)
+        for (int a = 0; a < 3; ++a) q.org[a] = ml.lo[a];
+        const dim3 g(ml.hi[0] - ml.lo[0], ml.hi[1] - ml.lo[1], ml.hi[2] - ml.lo[2]);
+        if (ml.in)
           kfree_in<<<g, blk_m, msm_free, s_box>>>(q);
         else
           kfree<<<g, blk_m, msm_free, s_box>>>(q);
       }
-      kcp<<<grd_m, blk_m, msm, s>>>(mtp);
+      auto list = [&](auto k, int q) {
+        const int n = e->mt_off[q + 1] - e->mt_off[q];
+        cudaStream_t sq = !conc || q == 3 ? s : e->side[q + 1];
+        if (n > 0) k<<<n, blk_m, msm, sq>>>(mtp, e->d_mtiles + e->mt_off[q]);
+      };
+      list(kx, 0);
+      list(ky, 1);
+      list(kz, 2);
+      list(kcp, 3);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma) {
@@ -821,7 +981,10 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       if (c != cudaSuccess) return c;
       launch_march(k_march_h_tma<T, kMTJ, 32, MF, false, false>,
                    k_march_h_tma<T, kMTJ, 32, MF, false, true>, k_march_h_wide<T, MW>,
-                   k_march_h_tma<T, kMTJ, 32, MS, true, false>);
+                   k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 1>,
+                   k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 2>,
+                   k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 4>,
+                   k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 7>);
       k_edge_h<T><<<edge_blocks, 256, 0, s_edge>>>(yp);
       if ((c = join()) != cudaSuccess) return c;
     }
@@ -845,7 +1008,10 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       if (c != cudaSuccess) return c;
       launch_march(k_march_e_tma<T, kMTJ, 32, MF, false, false>,
                    k_march_e_tma<T, kMTJ, 32, MF, false, true>, k_march_e_wide<T, MW>,
-                   k_march_e_tma<T, kMTJ, 32, MS, true, false>);
+                   k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 1>,
+                   k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 2>,
+                   k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 4>,
+                   k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 7>);
       k_edge_e<T><<<edge_blocks, 256, 0, s_edge>>>(yp);
       if ((c = join()) != cudaSuccess) return c;
     }
@@ -947,6 +1113,10 @@ xfd_status ensure_ready(xfd_engine* e) {
                            cudaMemcpyHostToDevice));
     e->xlayer_slabs = e->slabs.size();
     e->graph_dirty = true;
+  }
+  if (e->kernel_mode == 4) {
+    xfd_status st = build_march_tiles(e);
+    if (st != XFD_OK) return st;
   }
   if (e->probes_dirty) {
     // Upload the probe lists (all probes in one launch per step).
@@ -1154,13 +1324,13 @@ xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
   if (c != cudaSuccess) return fail(nullptr, XFD_ERR_CUDA, "stream: %s", cudaGetErrorString(c));
   c = cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking);
   if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->copy_ev, cudaEventDisableTiming);
-  for (int q = 0; q < 2 && c == cudaSuccess; ++q) {
+  for (int q = 0; q < kSides && c == cudaSuccess; ++q) {
     c = cudaStreamCreateWithFlags(&e->side[q], cudaStreamNonBlocking);
     if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->join_ev[q], cudaEventDisableTiming);
   }
   if (c == cudaSuccess) c = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
   if (c != cudaSuccess) {
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kSides; ++q) {
       if (e->side[q]) cudaStreamDestroy(e->side[q]);
       if (e->join_ev[q]) cudaEventDestroy(e->join_ev[q]);
     }
@@ -1238,7 +1408,7 @@ void xfd_destroy(xfd_engine* e) {
   for (void* p : e->host_allocs) cudaFreeHost(p);
   if (e->copy_ev) cudaEventDestroy(e->copy_ev);
   if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < kSides; ++q) {
     if (e->join_ev[q]) cudaEventDestroy(e->join_ev[q]);
     if (e->side[q]) cudaStreamDestroy(e->side[q]);
   }
@@ -2070,6 +2240,8 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "march_ichunk")) *value = e->march_ichunk;
   else if (!strcmp(name, "march_wide")) *value = e->march_wide ? 1 : 0;
   else if (!strcmp(name, "march_concurrent")) *value = e->march_concurrent ? 1 : 0;
+  else if (!strcmp(name, "march_split_axes")) *value = e->march_split_axes ? 1 : 0;
+  else if (!strcmp(name, "march_shift")) *value = e->march_shift ? 1 : 0;
   else return fail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -2096,6 +2268,10 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     e->march_wide = value != 0;
   } else if (!strcmp(name, "march_concurrent")) {
     e->march_concurrent = value != 0;
+  } else if (!strcmp(name, "march_split_axes")) {
+    e->march_split_axes = value != 0;
+  } else if (!strcmp(name, "march_shift")) {
+    e->march_shift = value != 0;
   } else {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
@@ -2116,10 +2292,15 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
     if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 1;  // CPML-free part
   }
   if (e->kernel_mode == 4) {
-    n += 2;  // lattice-face sweeps k_edge_h / k_edge_e
-    int lo[3], hi[3];
-    march_split(e, lo, hi);
-    if (hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2]) n += 2;  // CPML-free H and E
+    // The two sweeps counted above become, per sweep: the lattice-face kernel
+    // (k_edge_h / k_edge_e), the CPML-free box form and the CPML form's
+    // nonempty tile lists.  The face kernels make up for the two.
+    const MarchLayout ml = march_layout(e);
+    if (ml.box) n += 2;
+    std::vector<int4> lists[4];
+    march_tile_lists(e, lists);
+    for (int q = 0; q < 4; ++q)
+      if (!lists[q].empty()) n += 2;
   }
   if (e->have_tfsf) n += fused ? 2 : 4;
   if (e->ade_kind >= 0) n += fused ? 1 : 2;

@@ -53,8 +53,11 @@ struct MarchMaps {
 // `shift` moves the tile grid by whole nodes (k by a multiple of 8 nodes, so
 // that every TMA x coordinate -- field values and the uint16 class index --
 // stays a multiple of 16 bytes): tile (x, y, z) starts at node
-// (shift[0] + 32 x, shift[1] + TJ y, shift[2] + ichunk z).  Zero for the time
-// step; the adjoint's reverse sweeps use it to fit their box to the CPML.
+// (shift[0] + 32 x, shift[1] + TJ y, shift[2] + ichunk z).  The time step
+// shifts by -size < shift <= 0 so that tile and chunk edges fall near the CPML
+// layers' edges (the first tile and chunk then start below node 0: nodes
+// k < 0, j < 0 are inactive, planes i < 0 are not swept); the adjoint's
+// reverse sweeps shift forward to fit their box to the CPML.
 template <typename T>
 struct MarchTmaP {
   MarchP<T> p;
@@ -145,7 +148,7 @@ struct StageRing {
 // H sweep.  Planes q = 0 .. n_planes of the chunk are staged (plane n_planes
 // is i_hi, E only, when i_hi <= nx); plane q lives in stage q % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7>
 __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx, const int gy,
                                             const int gz) {
   using G = MarchGeom<T, TJ, TK>;
@@ -160,8 +163,10 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
   const int k0 = gx * TK + P.shift[0], j0 = gy * TJ + P.shift[1];
   const int k = k0 + tk, j = j0 + tj;
-  const int i_lo = gz * p.ichunk + P.shift[2];
-  const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
+  // A negative shift moves the first chunk (and tile) partly below node 0.
+  const int i0 = gz * p.ichunk + P.shift[2];
+  const int i_lo = max(i0, 0);
+  const int i_hi = min(i0 + p.ichunk, L.nx + 1);
   const int n_planes = i_hi - i_lo;
   const int n_staged = n_planes + (i_hi <= L.nx ? 1 : 0);
 
@@ -204,7 +209,7 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
 
   // Per-thread constants (as k_march_h).  The faces k = nz and j = ny are
   // left to k_edge_h (kernels.cuh).
-  const bool act = IN || (k < L.nz && j < L.ny);
+  const bool act = IN || (k >= 0 && j >= 0 && k < L.nz && j < L.ny);
   const long long PS = (long long)L.NY * L.KP;
   const int KP = L.KP;
   const long long row = (long long)j * KP + k;
@@ -212,8 +217,8 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
   const T fhj = (act && jv) ? p.fh[1][j] : T(0);
   const T fhk = (act && kv) ? p.fh[2][k] : T(0);
   int qy = 0, qz = 0;
-  const int ly = (CP && act) ? layer_of(p.slab[1], j, false, qy) : -1;
-  const int lz = (CP && act) ? layer_of(p.slab[2], k, false, qz) : -1;
+  const int ly = (CP && (AX & 2) && act) ? layer_of(p.slab[1], j, false, qy) : -1;
+  const int lz = (CP && (AX & 4) && act) ? layer_of(p.slab[2], k, false, qz) : -1;
   T ay = 0, by = 0, az = 0, bz = 0;
   T* psy[2] = {nullptr, nullptr};
   T* psz[2] = {nullptr, nullptr};
@@ -248,7 +253,7 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
     pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
     pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
     int qx = 0;
-    const int cx = p.xl[i].x;
+    const int cx = (AX & 1) ? p.xl[i].x : -1;
     const int lx = (act && cx >= 0) ? (cx >> 1) : -1;
     qx = cx & 1;
     const long long ox = (long long)lx * PS + row;
@@ -300,7 +305,7 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
       const T dEx_j = ex_j - ex, dEy_i = ey_n - ey;  // Hz
       const long long o = i * PS;
       int qx = 0;
-      const int cx = CP ? p.xl[i].x : -1;
+      const int cx = (CP && (AX & 1)) ? p.xl[i].x : -1;
       const int lx = cx >= 0 ? (cx >> 1) : -1;
       qx = cx & 1;
       if (jv && kv) {
@@ -347,7 +352,7 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
 // E sweep.  Staged planes q = -1 .. n_planes-1 (plane -1 = i_lo-1, H only,
 // when i_lo >= 1); plane q lives in stage (q+1) % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7>
 __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx, const int gy,
                                             const int gz) {
   using G = MarchGeom<T, TJ, TK>;
@@ -362,8 +367,10 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
   const int k0 = gx * TK + P.shift[0], j0 = gy * TJ + P.shift[1];
   const int k = k0 + tk, j = j0 + tj;
-  const int i_lo = gz * p.ichunk + P.shift[2];
-  const int i_hi = min(i_lo + p.ichunk, L.nx + 1);
+  // A negative shift moves the first chunk (and tile) partly below node 0.
+  const int i0 = gz * p.ichunk + P.shift[2];
+  const int i_lo = max(i0, 0);
+  const int i_hi = min(i0 + p.ichunk, L.nx + 1);
   const int n_planes = i_hi - i_lo;
   const int q_first = i_lo >= 1 ? -1 : 0;  // first staged plane
 
@@ -407,7 +414,8 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
   for (int q = q_first; q < q_first + S && q < q_end; ++q) ring.pending |= 1u << slot(q);
   stage_half_table<T, G::NC, TJ * TK>(sT, p.tab, p.n_classes, 0, tid);
 
-  const bool act = IN || (k < L.nz && j < L.ny);  // faces k = nz, j = ny: k_edge_e
+  // faces k = nz, j = ny: k_edge_e
+  const bool act = IN || (k >= 0 && j >= 0 && k < L.nz && j < L.ny);
   const long long PS = (long long)L.NY * L.KP;
   const int KP = L.KP;
   const long long row = (long long)j * KP + k;
@@ -416,8 +424,8 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
   const T fej = act ? p.fe[1][j] : T(0);
   const T fek = act ? p.fe[2][k] : T(0);
   int qy = 0, qz = 0;
-  const int ly = (CP && act) ? layer_of(p.slab[1], j, true, qy) : -1;
-  const int lz = (CP && act) ? layer_of(p.slab[2], k, true, qz) : -1;
+  const int ly = (CP && (AX & 2) && act) ? layer_of(p.slab[1], j, true, qy) : -1;
+  const int lz = (CP && (AX & 4) && act) ? layer_of(p.slab[2], k, true, qz) : -1;
   T ay = 0, by = 0, az = 0, bz = 0;
   T* psy[2] = {nullptr, nullptr};
   T* psz[2] = {nullptr, nullptr};
@@ -451,7 +459,7 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
     pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
     pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
     int qx = 0;
-    const int cx = p.xl[i].y;
+    const int cx = (AX & 1) ? p.xl[i].y : -1;
     const int lx = (act && cx >= 0) ? (cx >> 1) : -1;
     qx = cx & 1;
     const long long ox = (long long)lx * PS + row;
@@ -506,7 +514,7 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
       const T dHy_i = hy - hy_p, dHx_j = hx - hx_j;  // Ez
       const long long o = i * PS;
       int qx = 0;
-      const int cx = CP ? p.xl[i].y : -1;
+      const int cx = (CP && (AX & 1)) ? p.xl[i].y : -1;
       const int lx = cx >= 0 ? (cx >> 1) : -1;
       qx = cx & 1;
       if (iv) {
@@ -560,6 +568,23 @@ template <typename T, int TJ, int TK, int S, bool CP, bool IN>
 __global__ void __launch_bounds__(TJ* TK) k_march_e_tma(const __grid_constant__ MarchTmaP<T> P) {
   march_e_cta<T, TJ, TK, S, CP, IN>(P, blockIdx.x + P.org[0], blockIdx.y + P.org[1],
                                     blockIdx.z + P.org[2]);
+}
+
+// One lattice, a tile list: CTA b sweeps tile tiles[b] = (-, k tile, j tile,
+// chunk).  AX names the CPML axes (bits x, y, z) whose layers the listed
+// tiles can meet, so that the other axes' layer code is left out.
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX>
+__global__ void __launch_bounds__(TJ* TK)
+    k_march_h_tma_list(const __grid_constant__ MarchTmaP<T> P, const int4* __restrict__ tiles) {
+  const int4 w = tiles[blockIdx.x];
+  march_h_cta<T, TJ, TK, S, CP, IN, AX>(P, w.y, w.z, w.w);
+}
+
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX>
+__global__ void __launch_bounds__(TJ* TK)
+    k_march_e_tma_list(const __grid_constant__ MarchTmaP<T> P, const int4* __restrict__ tiles) {
+  const int4 w = tiles[blockIdx.x];
+  march_e_cta<T, TJ, TK, S, CP, IN, AX>(P, w.y, w.z, w.w);
 }
 
 // Many lattices in one launch: CTA b sweeps the tile list entry

@@ -110,8 +110,9 @@ __global__ void __launch_bounds__(WideGeom<T, S>::kThreads)
   const int lane = threadIdx.x, warp = threadIdx.y, tid = warp * 32 + lane;
   // One thread reads the error word, so that the whole CTA returns or none.
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
-  const int k0 = (blockIdx.x + P.org[0]) * 32, j0 = (blockIdx.y + P.org[1]) * kWideTJ;
-  const int i_lo = (blockIdx.z + P.org[2]) * p.ichunk;
+  const int k0 = (blockIdx.x + P.org[0]) * 32 + P.shift[0];
+  const int j0 = (blockIdx.y + P.org[1]) * kWideTJ + P.shift[1];
+  const int i_lo = (blockIdx.z + P.org[2]) * p.ichunk + P.shift[2];
   const int n_planes = min(p.ichunk, L.nx - i_lo);  // the box ends at or before nx
   const int n_staged = n_planes + 1;
   T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);
@@ -231,8 +232,9 @@ __global__ void __launch_bounds__(WideGeom<T, S>::kThreads)
   const Lat L = p.L;
   const int lane = threadIdx.x, warp = threadIdx.y, tid = warp * 32 + lane;
   if (__syncthreads_or(tid == 0 && (*(volatile int*)P.err & 2))) return;
-  const int k0 = (blockIdx.x + P.org[0]) * 32, j0 = (blockIdx.y + P.org[1]) * kWideTJ;
-  const int i_lo = (blockIdx.z + P.org[2]) * p.ichunk;  // >= 1 inside the box
+  const int k0 = (blockIdx.x + P.org[0]) * 32 + P.shift[0];
+  const int j0 = (blockIdx.y + P.org[1]) * kWideTJ + P.shift[1];
+  const int i_lo = (blockIdx.z + P.org[2]) * p.ichunk + P.shift[2];  // >= 1 inside the box
   const int n_planes = min(p.ichunk, L.nx - i_lo);
   const int n_staged = n_planes + 1;
   T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);
