@@ -662,6 +662,9 @@ def main():
                     help="1: CPML-free box and face kernels beside the CPML form (default)")
     ap.add_argument("--march-shift", type=int, default=None,
                     help="1: tile grid shifted to fit the CPML layers, 0: unshifted (default)")
+    ap.add_argument("--march-cp-stages", type=int, default=None,
+                    help="stages of the single-axis CPML lists: 1 as the CPML-free forms "
+                         "(default), 0 as the general CPML form")
     ap.add_argument("--march-split-axes", type=int, default=None,
                     help="1: CPML tiles in x-only, y-only, z-only and several-axis lists "
                          "(default), 0: one list")
@@ -725,7 +728,8 @@ def main():
                      ("march_wide", args.march_wide),
                      ("march_concurrent", args.march_concurrent),
                      ("march_split_axes", args.march_split_axes),
-                     ("march_shift", args.march_shift)):
+                     ("march_shift", args.march_shift),
+                     ("march_cp_stages", args.march_cp_stages)):
         if val is not None:
             opts[key] = val
     run32 = SceneRun(sc, precision=1, options=opts)

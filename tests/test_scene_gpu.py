@@ -280,7 +280,8 @@ def test_wide_interior_form_matches_oracle(precision, tol):
     orc = RefSimulation(sc)
     orc.run()
     got = {}
-    for key, opts in (("wide", {"march_wide": 1}), ("one-row", {"march_wide": 0}),
+    for key, opts in (("wide", {"march_wide": 1}),
+                      ("one-row", {"march_wide": 0, "march_cp_stages": 0}),
                       ("one-list", {"march_split_axes": 0, "march_concurrent": 0,
                                     "march_shift": 0})):
         run = SceneRun(sc, precision=precision, options={"kernel": 4, **opts})

@@ -163,6 +163,9 @@ struct xfd_engine {
   // Tile lists of the CPML form, by the CPML axes their tiles meet: x only,
   // y only, z only, several (lists 0..3 at mt_off[q] .. mt_off[q+1]).
   bool march_split_axes = true;
+  // Stages of the single-axis CPML lists: 0 as the general CPML form, 1 as
+  // the CPML-free forms (less shared memory, more CTAs per SM).
+  int march_cp_stages = 1;
   // Shift the tile grid to fit the CPML layers.  Off by default: a k shift
   // that is not a multiple of 32 values leaves every tile row off the 128-byte
   // lines (TMA boxes and the warps' stores), which costs more than the larger
@@ -522,6 +525,16 @@ xfd_status build_tma_maps(xfd_engine* e) {
                          (const void*)k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 4>,
                          (const void*)k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 7>};
     for (const void* f : fs) CUDA_TRY(e, attr(f));
+    constexpr int MF4 = march_free_stages<T>();
+    const void* f4[6] = {(const void*)k_march_h_tma_list<T, kMTJ, 32, MF4, true, false, 1>,
+                         (const void*)k_march_h_tma_list<T, kMTJ, 32, MF4, true, false, 2>,
+                         (const void*)k_march_h_tma_list<T, kMTJ, 32, MF4, true, false, 4>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MF4, true, false, 1>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MF4, true, false, 2>,
+                         (const void*)k_march_e_tma_list<T, kMTJ, 32, MF4, true, false, 4>};
+    for (const void* f : f4)
+      CUDA_TRY(e, cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       MG::smem(MF4)));
   }
   constexpr int MW = march_wide_stages<T>();
   CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_wide<T, MW>,
@@ -947,7 +960,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     // kcp: the CPML form's tile-list kernels for x-only, y-only, z-only and
     // several-axis tiles.
     auto launch_march = [&](auto kfree, auto kfree_in, auto kwide, auto kx, auto ky, auto kz,
-                            auto kcp) {
+                            auto kx4, auto ky4, auto kz4, auto kcp) {
       if (ml.wide) {
         MarchTmaP<T> q = mtp;
         q.m = e->mtma_w[e->cur];
@@ -965,15 +978,21 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
         else
           kfree<<<g, blk_m, msm_free, s_box>>>(q);
       }
-      auto list = [&](auto k, int q) {
+      auto list = [&](auto k, int q, size_t sm) {
         const int n = e->mt_off[q + 1] - e->mt_off[q];
         cudaStream_t sq = !conc || q == 3 ? s : e->side[q + 1];
-        if (n > 0) k<<<n, blk_m, msm, sq>>>(mtp, e->d_mtiles + e->mt_off[q]);
+        if (n > 0) k<<<n, blk_m, sm, sq>>>(mtp, e->d_mtiles + e->mt_off[q]);
       };
-      list(kx, 0);
-      list(ky, 1);
-      list(kz, 2);
-      list(kcp, 3);
+      if (e->march_cp_stages == 1) {
+        list(kx4, 0, msm_free);
+        list(ky4, 1, msm_free);
+        list(kz4, 2, msm_free);
+      } else {
+        list(kx, 0, msm);
+        list(ky, 1, msm);
+        list(kz, 2, msm);
+      }
+      list(kcp, 3, msm);
     };
     // H phase: updateH + CPML (fused) -> TFSF H faces.
     if (march_tma) {
@@ -984,6 +1003,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
                    k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 1>,
                    k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 2>,
                    k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 4>,
+                   k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 1>,
+                   k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 2>,
+                   k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 4>,
                    k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 7>);
       k_edge_h<T><<<edge_blocks, 256, 0, s_edge>>>(yp);
       if ((c = join()) != cudaSuccess) return c;
@@ -1011,6 +1033,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
                    k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 1>,
                    k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 2>,
                    k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 4>,
+                   k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 1>,
+                   k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 2>,
+                   k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 4>,
                    k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 7>);
       k_edge_e<T><<<edge_blocks, 256, 0, s_edge>>>(yp);
       if ((c = join()) != cudaSuccess) return c;
@@ -2242,6 +2267,7 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "march_concurrent")) *value = e->march_concurrent ? 1 : 0;
   else if (!strcmp(name, "march_split_axes")) *value = e->march_split_axes ? 1 : 0;
   else if (!strcmp(name, "march_shift")) *value = e->march_shift ? 1 : 0;
+  else if (!strcmp(name, "march_cp_stages")) *value = e->march_cp_stages;
   else return fail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -2272,6 +2298,9 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     e->march_split_axes = value != 0;
   } else if (!strcmp(name, "march_shift")) {
     e->march_shift = value != 0;
+  } else if (!strcmp(name, "march_cp_stages")) {
+    if (value != 0 && value != 1) return fail(e, XFD_ERR_INVALID_ARGUMENT, "march_cp_stages 0 or 1");
+    e->march_cp_stages = (int)value;
   } else {
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
