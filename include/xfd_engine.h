@@ -291,12 +291,18 @@ int64_t xfd_current_step(const xfd_engine* e);
 /* Engine options: "graph" (0/1, default 1), "graph_chunk" (steps per graph,
  * default 32), "kernel" (the Yee sweep: 0 = split H/E sweeps, 1 = fused
  * H-then-E sweep, 2 = fused sweep with its per-plane inputs staged by TMA,
- * 3 = split sweeps marching along x, 4 = the same with TMA-staged planes
- * (default), 5 = fused marching sweep with overlapped tiles and TMA-staged
- * planes, 6 = 5 with a two-nodes-per-thread form in the CPML-free interior),
+ * 3 = split sweeps marching along x, 4 = the same with TMA-staged planes,
+ * 5 = fused marching sweep with overlapped tiles and TMA-staged planes,
+ * 6 = 5 with a two-nodes-per-thread form in the CPML-free interior; default
+ * 4, or 0 on lattices whose marching tiles number fewer than two per SM),
  * "ichunk" (planes per CTA of the fused sweeps, default 32), "march_ichunk"
- * (planes per CTA of the split marching sweeps, default 16).  Every sweep
- * computes the same update; they differ in speed only. */
+ * (planes per CTA of the split marching sweeps, default 16), and the forms
+ * of sweep 4: "march_concurrent" (launches of a phase on four streams,
+ * default 1), "march_split_axes" (CPML tiles in lists by slab axis, default
+ * 1), "march_cp_stages" (single-axis lists with fewer stages, default 1),
+ * "march_wide" (two-rows-per-thread interior form, default 0),
+ * "march_shift" (tile grid moved to the CPML layers, default 0).  Every
+ * sweep computes the same update; they differ in speed only. */
 xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value);
 /* Current value of an option of xfd_set_option. */
 xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value);

@@ -45,7 +45,8 @@ def _alone(scenes, precision, opts=None):
 def test_batch_equals_alone_runs(precision, depth):
     steps = 70
     scenes = _scenes(steps)
-    want = _alone(scenes, precision, {"march_ichunk": depth})
+    # the marching sweep alone (small lattices default to the split sweep)
+    want = _alone(scenes, precision, {"march_ichunk": depth, "kernel": 4})
     runs = [SceneRun(sc, precision=precision) for sc in scenes]
     b = Batch([r.engine_handle() for r in runs], {"march_ichunk": depth, "graph_chunk": 16})
     assert b.size() == len(scenes)

@@ -1374,6 +1374,17 @@ xfd_status xfd_create(const xfd_grid_desc* g, xfd_engine** out) {
   e->L.NY = g->ny + 1;
   e->L.KP = ((g->nz + 1) + 31) / 32 * 32;
   e->n_lat = (long long)(g->nx + 1) * e->L.NY * e->L.KP;
+  // Small lattices: the marching sweeps' CTAs (a 32 x 8 tile through 16
+  // planes each) would not fill the GPU twice over, so the one-thread-per-
+  // node split sweep (more, shorter CTAs) is the default there.  The
+  // "kernel" option overrides the choice.
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+    const long long tiles = (long long)((g->nz + 31) / 32) * ((g->ny + 7) / 8) *
+                            ((g->nx + 1 + 15) / 16);
+    if (tiles < 2LL * sms) e->kernel_mode = 0;
+  }
   if (e->n_lat > (1LL << 40))
     return fail(nullptr, XFD_ERR_INVALID_ARGUMENT, "grid too large");
   xfd_engine* ep = e.get();
