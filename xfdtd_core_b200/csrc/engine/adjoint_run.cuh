@@ -196,6 +196,17 @@ void adjoint_split(const xfd_engine* e, int ich, int lo[3], int hi[3], int shift
   }
 }
 
+// Fork side stream 0 from `st` / join it back (the adjoint's reverse step).
+cudaError_t side_fork(xfd_engine* e, cudaStream_t st) {
+  cudaError_t c = cudaEventRecord(e->fork_ev, st);
+  return c == cudaSuccess ? cudaStreamWaitEvent(e->side[0], e->fork_ev, 0) : c;
+}
+
+cudaError_t side_join(xfd_engine* e, cudaStream_t st) {
+  cudaError_t c = cudaEventRecord(e->join_ev[0], e->side[0]);
+  return c == cudaSuccess ? cudaStreamWaitEvent(st, e->join_ev[0], 0) : c;
+}
+
 bool box_ok(const Lat& L, const int32_t s[3], const int32_t t[3]) {
   const int n[3] = {L.nx, L.ny, L.nz};
   for (int a = 0; a < 3; ++a)
@@ -441,12 +452,22 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
     }
     for (long long m = len; m >= 1; --m) {
       const long long gstep = q * K + m;  // u holds cb dJ/dE^gstep
-      if (has_box) k_march_h_tma<T, kMTJ, 32, MF, false, true><<<gbox, blk_m, msm_free, st>>>(am);
+      // The box sweep (on a side stream) and the shell gather write disjoint
+      // nodes and read only the other field: they run side by side.
+      if (has_box) {
+        CUDA_TRY(e, side_fork(e, st));
+        k_march_h_tma<T, kMTJ, 32, MF, false, true><<<gbox, blk_m, msm_free, e->side[0]>>>(am);
+      }
       k_adj_h<T><<<grd, blk, 0, st>>>(ap, abox);
+      if (has_box) CUDA_TRY(e, side_join(e, st));
       k_adj_sens<T><<<db, 256, 0, st>>>(rd, a, ov, static_cast<const T*>(hist), (int)m, g0, g1);
       if (e->n_ovr) k_ovr_gather<T><<<blocks_for(e->n_ovr, 256), 256, 0, st>>>(ovd, lam_dev);
-      if (has_box) k_march_e_tma<T, kMTJ, 32, MF, false, true><<<gbox, blk_m, msm_free, st>>>(am);
+      if (has_box) {
+        CUDA_TRY(e, side_fork(e, st));
+        k_march_e_tma<T, kMTJ, 32, MF, false, true><<<gbox, blk_m, msm_free, e->side[0]>>>(am);
+      }
       k_adj_e<T><<<grd, blk, 0, st>>>(ap, abox);
+      if (has_box) CUDA_TRY(e, side_join(e, st));
       if (e->n_ovr)
         k_ovr_apply<T><<<blocks_for(e->n_ovr, 256), 256, 0, st>>>(ovd, lam_dev, nullptr);
       if (gstep - 1 >= 1)
