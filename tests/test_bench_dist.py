@@ -66,3 +66,17 @@ def test_reference_arm_under_torchrun_rank0_only():
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     assert json.loads(lines[0])["impl"] == "reference"
+
+
+def test_reference_arm_sphere_workload_counts_its_own_cells():
+    """The reference's dielectric-sphere example (63^3): the line names the
+    workload and counts the example's cells, not the --grid default."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--workload", "sphere", "--steps", "5", "--warmup", "3"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["config"]["workload"].startswith("dielectric_sphere_63^3")
+    assert line["config"]["cells"] == 63 ** 3
+    assert "63x63x63" in line["cpu_baseline"]["sample"]
+    assert line["value"] > 0

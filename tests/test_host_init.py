@@ -84,3 +84,37 @@ def test_random_angle_tfsf_tables_match_oracle():
     for a in range(3):
         assert np.array_equal(p_int[a], t["p_int"][a])
         assert np.array_equal(p_half[a], t["p_half"][a])
+
+
+def test_scene_text_lines_for_lumped_network_and_pec_planes():
+    """The scene lines of the lumped elements, PEC planes and the network
+    round-trip through the host parser (host set-up only)."""
+    from tests.scenes import lumped_small, microstrip_small
+    for sc in (lumped_small(steps=4), microstrip_small(steps=4)):
+        text = sc.to_text()
+        for kw in ("voltage_source", "current_monitor", "voltage_monitor"):
+            assert kw in text
+        host = SceneRun(sc, engine=False)
+        assert host.n[0] > 0
+        host.close()
+    text = microstrip_small(steps=4).to_text()
+    assert "pec_plane microstrip_0" in text and "pec_plane ground_0" in text
+    assert "network 40 " in text and "port 1 1 " in text
+    text = lumped_small(steps=4).to_text()
+    for kw in ("resistor r1", "capacitor c1", "inductor l1"):
+        assert kw in text
+
+
+def test_pec_plane_coefficients_are_pec_on_the_plane():
+    """On the microstrip's ground plane (z = 0) the tangential E components
+    take the PEC sigma_e: ca ~ -1, cb ~ 0; Ez there is untouched."""
+    from tests.scenes import microstrip_small
+    host = SceneRun(microstrip_small(steps=4), engine=False)
+    co = host.coefficients()
+    orc = RefSimulation(microstrip_small(steps=4))
+    k0 = orc.grid_box(microstrip_small(steps=4).pec_planes[1].shape)[0][2]
+    cexe, ceye = co[0], co[3]
+    i0, j0, _ = orc.grid_box(microstrip_small(steps=4).pec_planes[1].shape)[0]
+    assert cexe[i0 + 1, j0 + 1, k0] < -0.99 and ceye[i0 + 1, j0 + 1, k0] < -0.99
+    assert cexe[i0 + 1, j0 + 1, k0 + 1] > 0.9
+    host.close()
