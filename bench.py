@@ -818,8 +818,9 @@ def main():
                          "traffic": (profiled_traffic(args.grid, kmode.value)
                                      if KIND == "boxes" else None),
                          "peak_source": peak_kind,
-                         "kernel": "the step's sweep launches (k_march_h_tma + k_march_e_tma, "
-                                   "CPML-free and CPML forms; 99% of a step's device time)",
+                         "kernel": "the step's sweep launches (k_march_h_tma / k_march_e_tma on "
+                                   "the CPML-free box, k_march_*_tma_list on the CPML tiles, "
+                                   "k_edge_h/e; 98% of a step's device time)",
                          "note": "achieved = algorithmic stencil bytes per step "
                                  f"({bytes32} B: 12 field values + uint16 class per cell, "
                                  "8 CPML psi per slab cell) / step time by CUDA events on "
