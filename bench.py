@@ -374,7 +374,10 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
     L = E.load()
     handles = [r.engine_handle() for r in runs]
     bytes_step = sum(int(L.xfd_stencil_bytes_per_step(ctypes_handle(h))) for h in handles)
-    batch = E.Batch(handles, {"autotune": tune})
+    bopts = {"autotune": tune}
+    if args.march_split_axes is not None:
+        bopts["march_split_axes"] = args.march_split_axes
+    batch = E.Batch(handles, bopts)
     batch.run(warm)
     batch.sync()
     tuning = batch.tuning()

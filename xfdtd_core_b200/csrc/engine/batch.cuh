@@ -51,7 +51,10 @@ struct xfd_batch {
   void* d_tfsf = nullptr;   // TfsfSceneD<T>[n]
   long long** d_steps = nullptr;
   int4* d_tiles = nullptr;
-  long long tile_off[4] = {0, 0, 0, 0};  // lists: CPML-free interior, CPML-free, CPML
+  // lists: CPML-free interior, CPML-free, CPML tiles meeting x layers only,
+  // y only, z only, several axes
+  long long tile_off[7] = {0, 0, 0, 0, 0, 0, 0};
+  bool split_axes = true;
   int2* d_edge = nullptr;
   long long n_edge = 0;
   int2* d_tfb = nullptr;
@@ -129,6 +132,12 @@ xfd_status batch_set_smem() {
   set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, false, true>, msm_free);
   set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, false, false>, msm_free);
   set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MS, true, false>, msm);
+  set((const void*)k_march_h_tma_batch<T, kMTJ, 32, MF, true, false, 1>, msm_free);
+  set((const void*)k_march_h_tma_batch<T, kMTJ, 32, MF, true, false, 2>, msm_free);
+  set((const void*)k_march_h_tma_batch<T, kMTJ, 32, MF, true, false, 4>, msm_free);
+  set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 1>, msm_free);
+  set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 2>, msm_free);
+  set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 4>, msm_free);
   if (c != cudaSuccess) {
     g_create_error = cudaGetErrorString(c);
     return XFD_ERR_CUDA;
@@ -150,7 +159,7 @@ xfd_status batch_prepare(xfd_batch* b) {
   std::vector<YeeP<T>> yp((size_t)n);
   std::vector<TfsfSceneD<T>> ts((size_t)n);
   std::vector<long long*> steps((size_t)n);
-  std::vector<int4> tiles[3];
+  std::vector<int4> tiles[6];
   std::vector<int2> edge;
   std::vector<int2> tfb[4];
   for (int s = 0; s < n; ++s) {
@@ -182,7 +191,14 @@ xfd_status batch_prepare(xfd_batch* b) {
         for (int x = 0; x < nt[0]; ++x) {
           const bool inbox = box && x >= lo[0] && x < hi[0] && y >= lo[1] && y < hi[1] &&
                              z >= lo[2] && z < hi[2];
-          tiles[inbox ? (in ? 0 : 1) : 2].push_back(make_int4(s, x, y, z));
+          int f = inbox ? (in ? 0 : 1) : 5;
+          if (!inbox && b->split_axes) {
+            const int ich = e->march_ichunk;
+            f = 2 + cpml_tile_list(e, 32 * x, std::min(32 * x + 32, L.nz), kMTJ * y,
+                                   std::min(kMTJ * y + kMTJ, L.ny), ich * z,
+                                   std::min(ich * z + ich, L.nx + 1));
+          }
+          tiles[f].push_back(make_int4(s, x, y, z));
         }
     mp[(size_t)s] = q;
     yp[(size_t)s] = yee_params<T>(e);
@@ -213,11 +229,11 @@ xfd_status batch_prepare(xfd_batch* b) {
   if ((st = batch_upload(b, &dt, ts.data(), ts.size())) != XFD_OK) return st;
   if ((st = batch_upload(b, &b->d_steps, steps.data(), steps.size())) != XFD_OK) return st;
   std::vector<int4> all;
-  for (int f = 0; f < 3; ++f) {
+  for (int f = 0; f < 6; ++f) {
     b->tile_off[f] = (long long)all.size();
     all.insert(all.end(), tiles[f].begin(), tiles[f].end());
   }
-  b->tile_off[3] = (long long)all.size();
+  b->tile_off[6] = (long long)all.size();
   if ((st = batch_upload(b, &b->d_tiles, all.data(), all.size())) != XFD_OK) return st;
   if ((st = batch_upload(b, &b->d_edge, edge.data(), edge.size())) != XFD_OK) return st;
   b->n_edge = (long long)edge.size();
@@ -249,10 +265,13 @@ cudaError_t batch_enqueue_t(xfd_batch* b) {
   const auto* dt = static_cast<const TfsfSceneD<T>*>(b->d_tfsf);
   auto n_of = [&](int f) { return (unsigned)(b->tile_off[f + 1] - b->tile_off[f]); };
   auto list = [&](int f) { return b->d_tiles + b->tile_off[f]; };
-  auto sweeps = [&](auto k_in, auto k_free, auto k_cp) {
+  auto sweeps = [&](auto k_in, auto k_free, auto kx, auto ky, auto kz, auto k_cp) {
     if (n_of(0)) k_in<<<n_of(0), blk, msm_free, s>>>(dm, list(0));
     if (n_of(1)) k_free<<<n_of(1), blk, msm_free, s>>>(dm, list(1));
-    if (n_of(2)) k_cp<<<n_of(2), blk, msm, s>>>(dm, list(2));
+    if (n_of(2)) kx<<<n_of(2), blk, msm_free, s>>>(dm, list(2));
+    if (n_of(3)) ky<<<n_of(3), blk, msm_free, s>>>(dm, list(3));
+    if (n_of(4)) kz<<<n_of(4), blk, msm_free, s>>>(dm, list(4));
+    if (n_of(5)) k_cp<<<n_of(5), blk, msm, s>>>(dm, list(5));
   };
   auto tfsf = [&](int g) {
     const long long nb = b->tfsf_off[g + 1] - b->tfsf_off[g];
@@ -260,12 +279,18 @@ cudaError_t batch_enqueue_t(xfd_batch* b) {
   };
   sweeps(k_march_h_tma_batch<T, kMTJ, 32, MF, false, true>,
          k_march_h_tma_batch<T, kMTJ, 32, MF, false, false>,
+         k_march_h_tma_batch<T, kMTJ, 32, MF, true, false, 1>,
+         k_march_h_tma_batch<T, kMTJ, 32, MF, true, false, 2>,
+         k_march_h_tma_batch<T, kMTJ, 32, MF, true, false, 4>,
          k_march_h_tma_batch<T, kMTJ, 32, MS, true, false>);
   if (b->n_edge) k_edge_batch<T, false><<<(unsigned)b->n_edge, 256, 0, s>>>(dy, b->d_edge);
   tfsf(0);
   tfsf(1);
   sweeps(k_march_e_tma_batch<T, kMTJ, 32, MF, false, true>,
          k_march_e_tma_batch<T, kMTJ, 32, MF, false, false>,
+         k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 1>,
+         k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 2>,
+         k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 4>,
          k_march_e_tma_batch<T, kMTJ, 32, MS, true, false>);
   if (b->n_edge) k_edge_batch<T, true><<<(unsigned)b->n_edge, 256, 0, s>>>(dy, b->d_edge);
   tfsf(2);
@@ -487,6 +512,7 @@ xfd_status xfd_batch_get_option(const xfd_batch* b, const char* name, int64_t* v
   else if (!strcmp(name, "graph_chunk")) *value = b->graph_chunk;
   else if (!strcmp(name, "march_ichunk")) *value = b->march_ichunk;
   else if (!strcmp(name, "autotune")) *value = b->autotune;
+  else if (!strcmp(name, "march_split_axes")) *value = b->split_axes ? 1 : 0;
   else return bfail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -507,6 +533,10 @@ xfd_status xfd_batch_set_option(xfd_batch* b, const char* name, int64_t value) {
   } else if (!strcmp(name, "autotune")) {
     if (value < 0 || value > 4096) return bfail(b, XFD_ERR_INVALID_ARGUMENT, "autotune range");
     b->autotune = (int)value;
+  } else if (!strcmp(name, "march_split_axes")) {
+    b->split_axes = value != 0;
+    b->ready = false;
+    batch_drop_graph(b);
   } else {
     return bfail(b, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
@@ -527,7 +557,7 @@ xfd_status xfd_batch_tuning(const xfd_batch* b, int32_t* depth, double* ms_per_s
 int32_t xfd_batch_launches_per_step(const xfd_batch* b) {
   if (!b || !b->ready) return 0;
   int n = 1;  // step counters
-  for (int f = 0; f < 3; ++f) n += b->tile_off[f + 1] > b->tile_off[f] ? 2 : 0;
+  for (int f = 0; f < 6; ++f) n += b->tile_off[f + 1] > b->tile_off[f] ? 2 : 0;
   if (b->n_edge) n += 2;
   for (int g = 0; g < 4; ++g) n += b->tfsf_off[g + 1] > b->tfsf_off[g] ? 1 : 0;
   return n;

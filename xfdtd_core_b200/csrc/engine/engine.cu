@@ -741,17 +741,28 @@ MarchLayout march_layout(const xfd_engine* e) {
 // The CPML form's tiles outside the skip box, sorted by the CPML axes whose
 // layers (of either phase) their node ranges meet: lists of x-only, y-only,
 // z-only and several-axis (or none) tiles, as (0, k tile, j tile, chunk).
+// Whether the node range [a0, a1) along lattice axis `axis` meets a CPML
+// layer of either phase.
+bool meets_cpml(const xfd_engine* e, int axis, int a0, int a1) {
+  for (const auto& S : e->slabs) {
+    if (S.m != axis) continue;
+    if (a0 < S.e_lo + S.n && S.e_lo < a1) return true;
+    if (a0 < S.h_lo + S.n && S.h_lo < a1) return true;
+  }
+  return false;
+}
+
+// List of a CPML-form tile by the axes whose layers it meets: 0 x only,
+// 1 y only, 2 z only, 3 several (or none).  Node ranges along k, j, i.
+int cpml_tile_list(const xfd_engine* e, int k0, int k1, int j0, int j1, int i0, int i1) {
+  const int mask = (meets_cpml(e, 0, i0, i1) ? 1 : 0) | (meets_cpml(e, 1, j0, j1) ? 2 : 0) |
+                   (meets_cpml(e, 2, k0, k1) ? 4 : 0);
+  return mask == 1 ? 0 : mask == 2 ? 1 : mask == 4 ? 2 : 3;
+}
+
 void march_tile_lists(const xfd_engine* e, std::vector<int4> lists[4]) {
   const MarchLayout m = march_layout(e);
   const Lat& L = e->L;
-  auto meets = [&](int axis, int a0, int a1) {  // node range [a0, a1)
-    for (const auto& S : e->slabs) {
-      if (S.m != axis) continue;
-      if (a0 < S.e_lo + S.n && S.e_lo < a1) return true;
-      if (a0 < S.h_lo + S.n && S.h_lo < a1) return true;
-    }
-    return false;
-  };
   for (int gz = 0; gz < m.nt[2]; ++gz)
     for (int gy = 0; gy < m.nt[1]; ++gy)
       for (int gx = 0; gx < m.nt[0]; ++gx) {
@@ -759,14 +770,11 @@ void march_tile_lists(const xfd_engine* e, std::vector<int4> lists[4]) {
             gy < m.skip_hi[1] && gz >= m.skip_lo[2] && gz < m.skip_hi[2])
           continue;
         const int ich = e->march_ichunk, sx = m.shift[2], sy = m.shift[1], sz = m.shift[0];
-        const int mask =
-            (meets(0, std::max(gz * ich + sx, 0), std::min((gz + 1) * ich + sx, L.nx + 1)) ? 1
-                                                                                           : 0) |
-            (meets(1, std::max(gy * kMTJ + sy, 0), std::min((gy + 1) * kMTJ + sy, L.ny)) ? 2
-                                                                                          : 0) |
-            (meets(2, std::max(gx * 32 + sz, 0), std::min((gx + 1) * 32 + sz, L.nz)) ? 4 : 0);
         int q = 3;
-        if (e->march_split_axes) q = mask == 1 ? 0 : mask == 2 ? 1 : mask == 4 ? 2 : 3;
+        if (e->march_split_axes)
+          q = cpml_tile_list(e, std::max(gx * 32 + sz, 0), std::min((gx + 1) * 32 + sz, L.nz),
+                             std::max(gy * kMTJ + sy, 0), std::min((gy + 1) * kMTJ + sy, L.ny),
+                             std::max(gz * ich + sx, 0), std::min((gz + 1) * ich + sx, L.nx + 1));
         lists[q].push_back(make_int4(0, gx, gy, gz));
       }
 }

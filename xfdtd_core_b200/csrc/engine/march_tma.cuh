@@ -604,20 +604,20 @@ __device__ __forceinline__ void acquire_march_maps(const MarchMaps& m) {
   }
 }
 
-template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7>
 __global__ void __launch_bounds__(TJ* TK)
     k_march_h_tma_batch(const MarchTmaP<T>* __restrict__ scenes, const int4* __restrict__ tiles) {
   const int4 w = tiles[blockIdx.x];
   acquire_march_maps(scenes[w.x].m);
-  march_h_cta<T, TJ, TK, S, CP, IN>(scenes[w.x], w.y, w.z, w.w);
+  march_h_cta<T, TJ, TK, S, CP, IN, AX>(scenes[w.x], w.y, w.z, w.w);
 }
 
-template <typename T, int TJ, int TK, int S, bool CP, bool IN>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7>
 __global__ void __launch_bounds__(TJ* TK)
     k_march_e_tma_batch(const MarchTmaP<T>* __restrict__ scenes, const int4* __restrict__ tiles) {
   const int4 w = tiles[blockIdx.x];
   acquire_march_maps(scenes[w.x].m);
-  march_e_cta<T, TJ, TK, S, CP, IN>(scenes[w.x], w.y, w.z, w.w);
+  march_e_cta<T, TJ, TK, S, CP, IN, AX>(scenes[w.x], w.y, w.z, w.w);
 }
 
 }  // namespace xfd
