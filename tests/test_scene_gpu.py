@@ -1,7 +1,7 @@
 """End-to-end parity through the drop-in host: the C++ xfdtd::Simulation built
 from a scene runs on the GPU; fields, movie frames and NF2FF surface currents
 are compared with the oracle on the same scene.  FP64 tolerance: relative L2
-<= 1e-12 (north_star's bar for the plain form).  FP32 form: the error budget
+<= 1e-12 (the plain form's parity bar).  FP32 form: the error budget
 against the FP64 oracle is stated per test."""
 import numpy as np
 import pytest
