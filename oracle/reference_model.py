@@ -2,9 +2,10 @@
 
 numpy restatement of EMinsight/XFDTD_CORE's initialisation (grid generation,
 object painting, edge/face averaging, the 18 Yee coefficients, CPML grading,
-TFSF incident grid, lumped current source, ADE coefficients, NF2FF phasors,
-movie monitors) driving the C per-step routines in ``xfd_oracle.c``.  It is
-the checker for the CUDA engine and the timed CPU baseline; the product never
+TFSF incident grid, lumped elements, PEC planes, ADE coefficients, NF2FF
+phasors, movie, voltage and current monitors, network S-parameters) driving
+the C per-step routines in ``xfd_oracle.c``.  The CUDA engine's parity tests
+compare against it, and it is the timed CPU baseline; the product never
 imports it.
 
 The reference publishes no golden vectors and cannot be compiled here (its

@@ -2,9 +2,9 @@
  * ORACLE -- TEST INFRASTRUCTURE ONLY.  PARITY UNPINNED.
  *
  * CPU restatement, in plain C (FP64, no FMA contraction), of the per-time-step
- * arithmetic of EMinsight/XFDTD_CORE's 3-D FDTD hot path.  It is the checker
- * the CUDA engine is compared against and the timed CPU baseline; nothing in
- * the product links it.  The reference ships no golden vectors and cannot be
+ * arithmetic of EMinsight/XFDTD_CORE's 3-D FDTD hot path.  The CUDA
+ * engine's parity tests compare against it, and it is the timed CPU baseline;
+ * nothing in the product links it.  The reference ships no golden vectors and cannot be
  * compiled here (it needs xtensor/xtl, which are absent), so this restatement
  * is not pinned to outputs of the reference itself: every routine instead
  * cites the reference lines it follows.
