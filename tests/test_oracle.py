@@ -174,3 +174,38 @@ def test_kernel_case_oracle_steps():
     orc.run(2)
     assert orc.t == 2
     assert any(not np.array_equal(a, b) for a, b in zip(before, orc.e))
+
+
+def _lumped_oracle():
+    from tests.scenes import lumped_small
+    sc = lumped_small(steps=4)
+    orc = RefSimulation(sc)
+    return sc, orc, {m["name"]: m["entries"] for m in orc.line_monitors}
+
+
+def test_voltage_monitor_is_the_line_integral():
+    """A uniform Ez = 3 V/m across the two-cell z-directed monitor reads
+    V = -integral E.dl = -3 x 2 dl (the monitor's sign convention, ZP)."""
+    sc, orc, entries = _lumped_oracle()
+    v = sum(w * 3.0 for f, x, w in entries["v_vs"] if f == "EZ")
+    assert abs(v - (-3.0 * 2 * sc.dl[0])) <= 1e-15
+
+
+def test_current_monitor_closes_the_ampere_loop():
+    """For Hx = -g y, Hy = g x (curl_z H = 2g everywhere) the current
+    monitor's weighted H entries sum to 2 g times the area between its H rows
+    and columns: the restated index ranges close the loop."""
+    sc, orc, entries = _lumped_oracle()
+    g = 2.5
+    hn = orc.h_node
+    total, xs, ys = 0.0, set(), set()
+    for f, (i, j, k), w in entries["i_vs"]:
+        if f == "HX":  # Hx(i, j, k) sits at y = h_node[1][j]
+            total += w * (-g * hn[1][j])
+            ys.add(float(hn[1][j]))
+        elif f == "HY":  # Hy(i, j, k) sits at x = h_node[0][i]
+            total += w * (g * hn[0][i])
+            xs.add(float(hn[0][i]))
+    area = (max(xs) - min(xs)) * (max(ys) - min(ys))
+    assert area > 0
+    assert abs(total - 2 * g * area) <= 1e-12 * 2 * g * area
