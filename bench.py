@@ -1,12 +1,16 @@
 """Benchmark: Gcell-updates/s of the XFDTD 3-D time step on B200.
 
-Workload (one "step" = one FDTD time step of this scene): the dielectric-boxes
-scene -- 256^3 cells including a 12-cell CPML (order 3, kappa_max 5,
-alpha_max 0.05), 64 random dielectric boxes (numpy default_rng(0)), a
-z-directed one-cell current source with a 30 GHz cosine-modulated Gaussian,
-CFL 0.99.  The headline `value` is the FP32 form; the FP64 plain form is
-timed in the same run and reported under "forms".  Inputs (fields: 6 x 257^3
-values) are larger than the 126 MB L2, so no flush is needed between steps.
+Workload (one "step" = one FDTD time step of this scene): the dispersive
+scene -- 384^3 cells including a 10-cell CPML, three spheres of radius 40
+cells (Drude, Lorentz, Debye media on the ADE path), a TFSF plane wave at
+theta = 45 deg, phi = 30 deg, and a 32-frequency NF2FF running DFT on a
+Huygens box 5 cells inside the CPML, CFL 0.9.  The headline `value` is the
+FP32 form (FP64 for the NF2FF sums and the incident grid); the FP64 plain
+form is timed in the same run and reported under "forms".  Inputs (fields:
+6 x 385^3 values) are larger than the 126 MB L2, so no flush is needed
+between steps.  `--workload boxes` is the 256^3 dielectric-boxes scene
+(64 random boxes, a z-directed current source, 12-cell CPML with order 3,
+kappa_max 5, alpha_max 0.05, CFL 0.99).
 
 Lines (one JSON line on rank 0):
   ours:       python bench.py [--gpus N --steps K --warmup W]
@@ -46,7 +50,16 @@ if ROOT not in sys.path:
 METRIC = "Gcell-updates/s"
 UNIT = "Gcell/s"
 WORKLOAD = "dielectric_boxes_256^3_cpml12_64boxes_dipole"
-KIND = "boxes"  # --workload: boxes (the default) or dispersive
+KIND = "dispersive"  # --workload: dispersive (the default), boxes, sphere, batched, adjoint
+DEFAULT_GRID = {"dispersive": 384, "boxes": 256}
+
+# DRAM bytes per FP32 time step of the default sweep, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum summed over every kernel of
+# consecutive steps, one pass, --clock-control none) and scaled to the full
+# lattice by cell count where the capture ran a smaller one.  Keyed by
+# (workload, cells per axis, sweep); a configuration without an entry
+# reports null.
+MEASURED_TRAFFIC = {}
 
 
 def workload_name(n: int) -> str:
@@ -89,19 +102,9 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(grid: int, kmode: int):
-    """DRAM bytes per FP32 step of the default sweep from the committed ncu
-    summary (profiles/traffic_march_tma_boxes.md), for the 256^3 workload."""
-    if grid != 256 or kmode != 4:
-        return None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic_march_tma_boxes.md")) as fh:
-            for line in fh:
-                if line.startswith("traffic_bytes_per_step_fp32_256"):
-                    return int(line.split("=")[1])
-    except OSError:
-        pass
-    return None
+def measured_traffic(grid: int, kmode: int):
+    """DRAM bytes per FP32 step of this workload's sweep, or None."""
+    return MEASURED_TRAFFIC.get((KIND, grid, kmode))
 
 
 # ----------------------------------------------------------------- clocks
@@ -277,15 +280,6 @@ def run_e2e(scene, steps: int, warmup: int, pg, device: int, options=None):
     return max_over_ranks(pg, elapsed), field_bytes, field_bytes + steps * frame_bytes
 
 
-def scene_dims(scene):
-    """Cells per axis of a scene, from the host library's grid generation."""
-    from xfdtd_core_b200.host import SceneRun
-    run = SceneRun(scene, engine=False)
-    n = run.n
-    run.close()
-    return n
-
-
 def scene_cells(scene) -> int:
     n = scene_n(scene)
     return n ** 3
@@ -304,24 +298,31 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
-def time_oracle(scene, budget_s: float, max_steps: int):
+def time_oracle(scene, budget_s: float, max_steps: int, warmup: int = 1,
+                warmup_budget_s: float = 30.0):
     """The oracle (CPU restatement of the reference's FP64 std::thread path,
-    OpenMP over all host threads) on the same scene: one warm-up step, then
-    as many steps as fit in `budget_s` (at most max_steps)."""
+    OpenMP over all host threads) on the same scene: `warmup` untimed steps
+    (the first of them also sizes the sample; the others only while they fit
+    in warmup_budget_s), then as many steps as fit in `budget_s` (at most
+    max_steps).  Returns (Gcell/s, steps, threads, seconds, cells, (nx, ny,
+    nz), warm-up steps run) -- the dimensions from the oracle's own grid
+    generation."""
     from oracle.reference_model import RefSimulation, lib
     threads = cpu_threads()
     r = RefSimulation(scene, threads=threads)
     lib().orc_set_num_threads(threads)
-    r.run(1)
     t0 = time.perf_counter()
     r.run(1)
     one = time.perf_counter() - t0
+    extra = int(min(max(warmup - 1, 0), warmup_budget_s // max(one, 1e-6)))
+    if extra > 0:
+        r.run(extra)
     k = int(max(1, min(max_steps, budget_s / max(one, 1e-6))))
     t0 = time.perf_counter()
     r.run(k)
     el = time.perf_counter() - t0
     cells = r.nx * r.ny * r.nz
-    return cells * k / el / 1e9, k, threads, el, cells
+    return cells * k / el / 1e9, k, threads, el, cells, (r.nx, r.ny, r.nz), 1 + extra
 
 
 def cpu_model() -> str:
@@ -449,8 +450,8 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         mid = sorted(params, key=lambda p: p["n"])[len(params) // 2]
         try:
-            cv, k, threads, el, _ = time_oracle(S.batched_sphere(steps=400, **mid),
-                                             budget_s=args.cpu_budget, max_steps=300)
+            cv, k, threads, el, _, _, _ = time_oracle(S.batched_sphere(steps=400, **mid),
+                                                      budget_s=args.cpu_budget, max_steps=300)
             cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{k} FDTD steps of the median scene ({mid['n']}^3) in {el:.1f} s, "
                              f"FP64, OpenMP on {threads} threads, {cpu_model()}"}
@@ -649,11 +650,12 @@ def main():
                     help="timed steps (default 4000; 3000 for --workload batched)")
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--grid", type=int, default=256, help="cells per axis incl. CPML")
-    ap.add_argument("--workload", default="boxes",
+    ap.add_argument("--grid", type=int, default=None,
+                    help="cells per axis incl. CPML (default 384 for dispersive, 256 for boxes)")
+    ap.add_argument("--workload", default="dispersive",
                     choices=["boxes", "dispersive", "batched", "adjoint", "sphere"],
-                    help="boxes: the headline dielectric-boxes scene; dispersive: ADE + TFSF + "
-                         "NF2FF spheres (use --grid 384 for its full size); batched: 96 sphere "
+                    help="dispersive: the headline ADE + TFSF + NF2FF spheres scene at 384^3; "
+                         "boxes: the 256^3 dielectric-boxes scene; batched: 96 sphere "
                          "scenes of uneven sizes advanced together; sphere: the reference's "
                          "dielectric-sphere example (63^3, 2000 steps)")
     ap.add_argument("--scenes", type=int, default=96, help="scenes of --workload batched")
@@ -689,20 +691,25 @@ def main():
     args = ap.parse_args()
     global KIND
     KIND = args.workload
+    if args.grid is None:
+        args.grid = DEFAULT_GRID.get(KIND, 256)
     warmup = max(3, args.warmup)
     steps = args.steps if args.steps is not None else {"batched": 3000, "adjoint": 5000,
-                                                       "sphere": 2000}.get(KIND, 4000)
+                                                       "sphere": 2000,
+                                                       "dispersive": 6000}.get(KIND, 4000)
 
     world, rank, local, pg = dist_setup(args.gpus)
 
     if args.impl == "reference":
         if rank != 0:
             return
+        # The oracle alone: no library of this package is loaded on this arm.
         scene = workload_scene(steps=warmup + steps + 2, n=args.grid)
-        value, k, threads, el, ocells = time_oracle(scene, budget_s=60.0, max_steps=steps)
-        size = "x".join(str(v) for v in scene_dims(scene))
+        value, k, threads, el, ocells, dims, warm_run = time_oracle(
+            scene, budget_s=45.0, max_steps=steps, warmup=warmup)
+        size = "x".join(str(v) for v in dims)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-                "steps": k, "warmup": 1, "ms_per_step": el / k * 1e3,
+                "steps": k, "warmup": warm_run, "ms_per_step": el / k * 1e3,
                 "higher_is_better": True,
                 "scaling": "strong" if KIND == "batched" else "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic",
@@ -716,8 +723,14 @@ def main():
                                            + (f"full {size} scene" if KIND != "batched"
                                               else f"median batched scene ({scene_cells(scene)} "
                                                    "cells)")
-                                           + f" (requested {steps}; bounded to ~60 s), "
-                                           f"{cpu_model()}"},
+                                           + f" (requested {steps}; bounded to ~45 s), "
+                                           f"{warm_run} warm-up step(s) (requested {warmup}; "
+                                           "bounded to ~30 s), " + cpu_model()
+                                           + ("; the reference's frequency-domain NF2FF "
+                                              "update is single-threaded and O(nF^2 x surface) "
+                                              "per step (its per-plane loop runs once per "
+                                              "frequency), which dominates this scene on the CPU"
+                                              if KIND == "dispersive" else "")},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -764,9 +777,12 @@ def main():
              3: "split H and E sweeps marching along x",
              4: "split H and E sweeps marching along x, TMA-staged planes",
              5: "fused H-then-E sweep marching along x, overlapped tiles, TMA-staged planes",
-             6: "fused marching sweep, two nodes per thread in the CPML-free interior"
+             6: "fused marching sweep, two nodes per thread in the CPML-free interior",
+             7: "fused H-then-E sweep of the CPML-free interior box (TMA-staged planes, "
+                "ping-pong buffers) beside the split marching sweeps of the CPML tiles"
              }[kmode.value]
-    bytes32 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h32)))
+    bytes32 = int(L.xfd_algorithmic_bytes_per_step(ctypes_handle(h32)))
+    stencil32 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h32)))
     sampler = ClockSampler(local)
     ms32, clocks = time_engine_steps(h32, steps, warmup, pg, local, sampler)
     run32.close()
@@ -777,7 +793,7 @@ def main():
     # FP64 plain form
     run64 = SceneRun(workload_scene(steps=warmup + steps, n=args.grid), precision=0, options=opts)
     h64 = run64.engine_handle()
-    bytes64 = int(L.xfd_stencil_bytes_per_step(ctypes_handle(h64)))
+    bytes64 = int(L.xfd_algorithmic_bytes_per_step(ctypes_handle(h64)))
     ms64, _ = time_engine_steps(h64, steps, warmup, pg, local, None)
     run64.close()
     value64 = cells * steps * world / (ms64 / 1e3) / 1e9
@@ -793,9 +809,9 @@ def main():
         try:
             full = KIND == "sphere"  # the whole 2000-step example fits the budget
             csc = workload_scene(steps=steps + 2 if full else 400, n=args.grid)
-            cv, k, threads, el, _ = time_oracle(csc, budget_s=args.cpu_budget,
-                                                max_steps=steps if full else 300)
-            size = "x".join(str(v) for v in scene_dims(csc))
+            cv, k, threads, el, _, dims, _ = time_oracle(csc, budget_s=args.cpu_budget,
+                                                         max_steps=steps if full else 300)
+            size = "x".join(str(v) for v in dims)
             cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{k} FDTD steps of the full {size} scene in {el:.1f} s, "
                              f"FP64, OpenMP on {threads} threads, {cpu_model()}"}
@@ -818,17 +834,22 @@ def main():
                        "parallelism": f"replicas x{world}", "sweep": sweep},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm,
-                         "traffic": (profiled_traffic(args.grid, kmode.value)
-                                     if KIND == "boxes" else None),
+                         "traffic": measured_traffic(args.grid, kmode.value),
                          "peak_source": peak_kind,
-                         "kernel": "the step's sweep launches (k_march_h_tma / k_march_e_tma on "
-                                   "the CPML-free box, k_march_*_tma_list on the CPML tiles, "
-                                   "k_edge_h/e; 98% of a step's device time)",
-                         "note": "achieved = algorithmic stencil bytes per step "
+                         "kernel": ("the step's sweep launches (k_hyb on the CPML-free box, "
+                                    "k_march_*_tma_list on the CPML tiles, k_edge_pp)"
+                                    if kmode.value == 7 else
+                                    "the step's sweep launches (k_march_h_tma / k_march_e_tma "
+                                    "on the CPML-free box, k_march_*_tma_list on the CPML tiles, "
+                                    "k_edge_h/e)"),
+                         "note": "achieved = algorithmic bytes per step "
                                  f"({bytes32} B: 12 field values + uint16 class per cell, "
-                                 "8 CPML psi per slab cell) / step time by CUDA events on "
-                                 "the engine stream; traffic = DRAM bytes per step from "
-                                 "profiles/traffic_march_tma_boxes.md"},
+                                 "8 CPML psi per slab cell = "
+                                 f"{stencil32} B; plus ADE currents, TFSF face passes and "
+                                 "NF2FF samples and accumulators) / step time by CUDA events "
+                                 "on the engine stream; traffic = ncu DRAM bytes per step "
+                                 "(read + write over all kernels of a step), null when not "
+                                 "measured for this configuration"},
             "forms": {"fp64_plain": {"value": value64, "unit": UNIT,
                                      "ms_per_step": ms64 / steps,
                                      "roofline_achieved_gbs": achieved64,

@@ -318,6 +318,14 @@ int32_t xfd_launches_per_step(const xfd_engine* e);
  * written once, class index, CPML auxiliaries) -- the roofline numerator. */
 int64_t xfd_stencil_bytes_per_step(const xfd_engine* e);
 
+/* Algorithmic DRAM bytes per time step of the whole step: the stencil bytes
+ * above plus the ADE currents (J, and for the modified-Lorentz form J_prev and
+ * E_prev, read and written once per dispersive entry), the TFSF face passes
+ * (each corrected node read and written once) and the NF2FF (four FP64
+ * samples written per surface point, and the complex FP64 accumulators read
+ * and written once per DFT batch).  No credit for reuse across steps. */
+int64_t xfd_algorithmic_bytes_per_step(const xfd_engine* e);
+
 /* ---- Allocation-free NF2FF step -------------------------------------------
  * No counterpart in the reference: an addition of this library for callers
  * that cannot allocate device memory -- an FDTD loop embedded in a larger GPU
@@ -332,7 +340,8 @@ int64_t xfd_stencil_bytes_per_step(const xfd_engine* e);
  * library, which every GPU that loads the library holds until exit.
  *   - The first call on a device looks up that array's device address
  *     (cudaGetSymbolAddress) with the device current; make that first call
- *     before any stream capture.
+ *     before any stream capture.  The address is kept per CUDA context, so
+ *     the first call after a cudaDeviceReset looks it up again.
  *   - All calls on a device share the one scratch array: calls whose kernels
  *     overlap on the GPU (different streams or host threads) race and corrupt
  *     each other's samples -- serialise them.
@@ -362,6 +371,10 @@ typedef struct {
   double scale;
   double* acc;            /* device, n_freq x 4 x P complex, accumulated in place
                              (P = points of the six faces, face by face) */
+  double* acc_comp;       /* optional device array shaped like acc (zeroed before
+                             the first step) for compensated accumulation: each
+                             step's rounding error goes there, and the surface
+                             current is acc + acc_comp.  NULL: plain sums. */
 } xfd_nf2ff_step_desc;
 
 /* Queues the step on `stream` (a cudaStream_t; NULL = legacy default). */
@@ -371,7 +384,10 @@ xfd_status xfd_nf2ff_step_static(const xfd_nf2ff_step_desc* d, void* stream);
  * No counterpart in the reference (whose TimeParam has a start step but no
  * saved field state).  A slot holds a device copy of what the next step
  * reads: the six fields, the CPML auxiliaries, the ADE currents and the step
- * counter.  Movie frames and NF2FF sums are outputs and are not rewound.
+ * counter.  Movie frames are outputs and are not rewound.  An engine with a
+ * frequency- or time-domain NF2FF surface refuses xfd_checkpoint_load
+ * (XFD_ERR_UNSUPPORTED): its running DFT sums and per-step sample ring cover
+ * the steps already taken and cannot be rewound.
  * Slots are engine-owned device memory (0 <= slot < 4096); saving over a
  * slot reuses it.  Loading a slot saved under another configuration (CPML
  * slabs, ADE) is rejected (XFD_ERR_STATE). */

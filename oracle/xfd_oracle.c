@@ -541,6 +541,9 @@ static void nf2ff_plane_update(const orc_yee *y, const orc_nf2ff *nf, idx_t f, i
       }
       double *acc1 = nf->acc + 2 * nf->off[((f * 6 + d) * 4) + (is_m ? 2 : 0)];
       double *acc2 = nf->acc + 2 * nf->off[((f * 6 + d) * 4) + (is_m ? 3 : 1)];
+      /* Points are independent: each keeps the reference's order of additions,
+       * so the threads change nothing but the time. */
+#pragma omp parallel for collapse(2) schedule(static)
       for (idx_t i = s[0]; i < e[0]; ++i)
         for (idx_t j = s[1]; j < e[1]; ++j)
           for (idx_t k = s[2]; k < e[2]; ++k) {

@@ -117,9 +117,12 @@ class KernelCase:
 
     # -------------------------------------------------------------- engine
     def engine(self, precision=0, n_steps=8, kernel=1, ichunk=None):
+        """The case as an engine; kernel=None keeps the engine's own choice of
+        sweep for the lattice."""
         from xfdtd_core_b200.engine import Engine
         eng = Engine(*self.n, precision=precision, n_steps=n_steps, dt=1.0)
-        eng.set_option("kernel", kernel)
+        if kernel is not None:
+            eng.set_option("kernel", kernel)
         if ichunk is not None:
             eng.set_option("ichunk", ichunk)
             eng.set_option("march_ichunk", ichunk)

@@ -162,6 +162,36 @@ def test_checkpoint_save_load_roundtrip(precision):
     r.close()
 
 
+def test_checkpoint_load_refused_with_nf2ff():
+    """An engine with an NF2FF surface saves states but refuses to load them
+    (its running DFT sums cover the steps already taken), and the refused
+    load leaves the run untouched: the NF2FF currents after 64 + 40 steps
+    (one batch boundary crossed after the save) equal those of a run that
+    never tried to load."""
+    from xfdtd_core_b200 import engine as E
+    import ctypes
+    from tests.scenes import dispersive_small
+    runs = []
+    for try_load in (False, True):
+        r = SceneRun(dispersive_small(steps=120), precision=0)
+        L = E.load()
+        h = ctypes.c_void_p(r.engine_handle())
+        r.advance(40)
+        assert L.xfd_checkpoint_save(h, 0) == 0
+        r.advance(64)
+        if try_load:
+            st = L.xfd_checkpoint_load(h, 0)
+            assert st == 3  # XFD_ERR_UNSUPPORTED
+            assert b"NF2FF" in L.xfd_last_error(h)
+            assert L.xfd_current_step(h) == 104
+        r.finish()
+        runs.append((r.fields(), r.nf2ff()))
+        r.close()
+    for x, y in zip(runs[0][0], runs[1][0]):
+        assert np.array_equal(x, y)
+    assert np.array_equal(runs[0][1], runs[1][1])
+
+
 class DftPower:
     """torch.autograd.Function over the adjoint (test harness only): J(eps_r)
     forward, dJ/deps_r from the discrete adjoint on backward."""

@@ -45,7 +45,8 @@ def test_max_over_ranks_gloo(tmp_path):
 
 def test_reference_arm_line():
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--grid", "40", "--steps", "4", "--warmup", "3"], capture_output=True,
+                          "--workload", "boxes", "--grid", "40", "--steps", "4", "--warmup", "3"],
+                         capture_output=True,
                          text=True, timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr
     line = json.loads(out.stdout.strip().splitlines()[-1])
@@ -60,8 +61,9 @@ def test_reference_arm_under_torchrun_rank0_only():
     out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
                           "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
                           "--master-port", str(port), os.path.join(ROOT, "bench.py"),
-                          "--impl", "reference", "--gpus", "2", "--grid", "40", "--steps", "3",
-                          "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+                          "--impl", "reference", "--gpus", "2", "--workload", "boxes", "--grid",
+                          "40", "--steps", "3", "--warmup", "3"], capture_output=True, text=True,
+                         timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1

@@ -21,7 +21,8 @@ KERNELS = [pytest.param((0, None), id="split"), pytest.param((1, None), id="fuse
            pytest.param((4, 3), id="march-tma-ichunk3"), pytest.param((4, 1), id="march-tma-ichunk1"),
            pytest.param((5, None), id="fmarch"), pytest.param((5, 3), id="fmarch-ichunk3"),
            pytest.param((5, 1), id="fmarch-ichunk1"), pytest.param((6, None), id="fvec"),
-           pytest.param((6, 3), id="fvec-ichunk3")]
+           pytest.param((6, 3), id="fvec-ichunk3"), pytest.param((7, None), id="hyb"),
+           pytest.param((7, 3), id="hyb-ichunk3"), pytest.param((7, 1), id="hyb-ichunk1")]
 
 
 def _compare(case, steps, precision=0, tol=FP64_TOL, graph=True, kernel=(1, None)):
@@ -64,13 +65,14 @@ def test_yee_large_tile_crossing_fp32(kernel):
     assert max(errs) <= 1e-5, errs
 
 
-@pytest.mark.parametrize("kernel", [4, 5, 6])
+@pytest.mark.parametrize("kernel", [4, 5, 6, 7])
 @pytest.mark.parametrize("ichunk", [3, 4])
 @pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, 1e-5)], ids=["fp64", "fp32"])
 def test_interior_forms(kernel, ichunk, precision, tol):
     """A grid long enough along z that the CPML-free interior holds whole
     tiles (pairs of tiles for kernel 6), so the CPML-free forms of the
-    marching sweeps run next to their CPML forms."""
+    marching sweeps (the fused box kernel for kernel 7) run next to their
+    CPML forms."""
     _compare(KernelCase(n=(24, 20, 140), seed=16), steps=3, precision=precision, tol=tol,
              kernel=(kernel, ichunk))
 
@@ -86,7 +88,7 @@ def test_yee_cpml_fp32(kernel):
     _compare(KernelCase(n=(9, 10, 11), seed=4), steps=3, precision=1, tol=1e-5, kernel=kernel)
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_graph_matches_eager(kernel):
     c = KernelCase(n=(10, 9, 8), seed=5)
     a = c.engine(n_steps=64, kernel=kernel)

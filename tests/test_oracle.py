@@ -25,7 +25,7 @@ def test_constants_match_reference():
     assert abs(C_0 - 299792458.0) / 299792458.0 < 1e-9
 
 
-def test_grid_matches_survey_sizes():
+def test_grid_of_the_dielectric_sphere_example():
     r = RefSimulation(S.dielectric_sphere(steps=2))
     assert (r.nx, r.ny, r.nz) == (63, 63, 63)
     assert r.movies[0]["s"] == [8, 31, 8] and r.movies[0]["e"] == [55, 32, 55]

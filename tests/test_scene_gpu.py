@@ -27,7 +27,41 @@ SWEEPS = [pytest.param({"kernel": 0}, id="split"), pytest.param({"kernel": 1}, i
           pytest.param({"kernel": 2}, id="fused-tma"), pytest.param({"kernel": 3}, id="march"),
           pytest.param({"kernel": 4}, id="march-tma"), pytest.param({"kernel": 5}, id="fmarch"),
           pytest.param({"kernel": 5, "ichunk": 4}, id="fmarch-ichunk4"),
-          pytest.param({"kernel": 6, "ichunk": 4}, id="fvec-ichunk4")]
+          pytest.param({"kernel": 6, "ichunk": 4}, id="fvec-ichunk4"),
+          pytest.param({"kernel": 7}, id="hyb")]
+
+
+def _box_scenes():
+    """Scenes at 96^3 with a 6-cell CPML: large enough that the fused
+    interior box of sweep 7 exists (k tiles 32-63, j 8-87, i 16-79), with the
+    TFSF faces (start 9) crossing its boundary, the dispersive spheres inside
+    it, and the NF2FF surface beside it."""
+    return {
+        "dispersive96": lambda steps: S.dispersive_spheres(
+            n=96, pml=6, radius_cells=8, offsets_cells=((-14, 0), (8, 13), (8, -13)),
+            steps=steps, tfsf_start=9, nf2ff_distance=8, n_freqs=4, movie_interval=0),
+        "boxes96": lambda steps: S.dielectric_boxes(n=96, pml=6, n_boxes=12, edge_lo=4,
+                                                    edge_hi=20, steps=steps, seed=3,
+                                                    movie_interval=0),
+    }
+
+
+@pytest.mark.parametrize("name", ["dispersive96", "boxes96"])
+def test_fused_box_scene_fp64(name):
+    """Sweep 7 on lattices where its fused box runs beside the CPML tiles:
+    fields and NF2FF currents within 1e-12 of the oracle after 120 steps."""
+    sc = _box_scenes()[name](120)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc, options={"kernel": 7})
+    run.run()
+    errs = _fields_rel(run, orc)
+    assert max(errs) <= TOL64, errs
+    if sc.nf2ff is not None:
+        got = run.nf2ff()
+        acc = orc.nf2ff["acc"]
+        want = acc[0::2] + 1j * acc[1::2]
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
 
 
 @pytest.mark.parametrize("opts", SWEEPS)

@@ -3,8 +3,9 @@
 //
 // A saved state (xfd_checkpoint_save / _load) is a device copy of what the
 // next step reads: the six field arrays of the current buffer, the CPML psi
-// arrays, the ADE currents and the step counter.  Movie frames and NF2FF
-// sums are outputs and are not rewound.
+// arrays, the ADE currents and the step counter.  Movie frames are outputs
+// and are not rewound; engines with NF2FF surfaces save states but refuse to
+// load them, because their running DFT sums cannot be rewound.
 //
 // xfd_adjoint_run: forward n steps from the current state, saving the state
 // every K steps and recording the objective component over its node box
@@ -37,7 +38,7 @@ std::vector<StateRegion> state_regions(xfd_engine* e) {
     const size_t b = slab_cells(e, S) * e->wsize;
     for (int w = 0; w < 2; ++w) {
       r.push_back({S.psi_e[w], b});
-      r.push_back({S.psi_h[e->cur][w], b});
+      r.push_back({S.psi_h[psi_h_buf(e)][w], b});
     }
   }
   if (e->ade_kind >= 0) {
@@ -361,13 +362,14 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
   rd.rows = K + 1;
   rd.dst = static_cast<T*>(hist);
   const unsigned db = blocks_for(3 * n_des, 256);
-  T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
   for (long long q = 0; q < S; ++q) {
     if ((s = ckpt_save(e, ck[(size_t)q])) != XFD_OK) break;
     if (q == S - 1) {
       rd.base = t0 + q * K;
       rd.shift = 0;
-      k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
+      // E at the segment start (the buffer holding it: ping-pong sweeps alternate)
+      T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
+      k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);
       rd.shift = 1;
       set_rec<T>(e, 1, rd);
       e->n_rec = 2;
@@ -440,6 +442,7 @@ xfd_status adjoint_run_t(xfd_engine* e, const xfd_adjoint_desc* d, double* value
       if ((s = state_copy(e, ck[(size_t)q], false)) != XFD_OK) return s;
       rd.base = base;
       rd.shift = 0;
+      T* const* fields = reinterpret_cast<T* const*>(e->d_fields[e->cur]);
       k_box_record<T><<<db, 256, 0, st>>>(rd, L, fields, e->d_step);  // E at the segment start
       rd.shift = 1;
       set_rec<T>(e, 0, rd);
@@ -500,6 +503,13 @@ xfd_status xfd_checkpoint_save(xfd_engine* e, int32_t slot) {
 xfd_status xfd_checkpoint_load(xfd_engine* e, int32_t slot) {
   if (!e || slot < 0 || (size_t)slot >= e->ckpts.size() || !e->ckpts[(size_t)slot].buf)
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "no saved state in slot %d", slot);
+  // The NF2FF accumulators and the per-step sample ring are running sums over
+  // the steps already taken; a state rewound under them would fold samples of
+  // steps after the saved one with the phasors of earlier steps.
+  if (e->have_nf2ff || e->have_td)
+    return fail(e, XFD_ERR_UNSUPPORTED,
+                "loading a saved state is not supported on an engine with an NF2FF surface "
+                "(its running DFT sums cannot be rewound)");
   CUDA_TRY(e, cudaSetDevice(e->device));
   if (e->ckpts[(size_t)slot].bytes != state_bytes(e))
     return fail(e, XFD_ERR_STATE, "slot %d was saved with another configuration", slot);

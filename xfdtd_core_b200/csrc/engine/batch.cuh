@@ -46,6 +46,9 @@ struct xfd_batch {
   int graph_chunk = 32;
   int autotune = 0;  // steps timed per candidate depth on the next run (0: off)
   bool ready = false;
+  // Field buffer of each engine (in `eng` order) when the tables were built:
+  // the tables hold that buffer's pointers and tensor maps.
+  std::vector<int> cur_at_prepare;
   void* d_march = nullptr;  // MarchTmaP<T>[n]
   void* d_yee = nullptr;    // YeeP<T>[n]
   void* d_tfsf = nullptr;   // TfsfSceneD<T>[n]
@@ -248,6 +251,8 @@ xfd_status batch_prepare(xfd_batch* b) {
   b->d_march = dm;
   b->d_yee = dy;
   b->d_tfsf = dt;
+  b->cur_at_prepare.clear();
+  for (const xfd_engine* e : b->eng) b->cur_at_prepare.push_back(e->cur);
   b->ready = true;
   return XFD_OK;
 }
@@ -463,6 +468,16 @@ xfd_status xfd_batch_run(xfd_batch* b, int64_t n) {
     if (e->host_step + n > e->n_steps)
       return bfail(b, XFD_ERR_INVALID_ARGUMENT, "lattice %zu: run past n_steps (%lld + %lld > %lld)",
                    s, (long long)e->host_step, (long long)n, (long long)e->n_steps);
+  }
+  // A member engine run alone in a fused (ping-pong) sweep since the tables
+  // were built may hold its fields in the other buffer: rebuild them.
+  if (b->ready) {
+    for (size_t s = 0; s < b->eng.size(); ++s) {
+      if (s >= b->cur_at_prepare.size() || b->eng[s]->cur != b->cur_at_prepare[s]) {
+        b->ready = false;
+        break;
+      }
+    }
   }
   BATCH_TRY(b, cudaSetDevice(b->device));
   // Order after each engine's own queued work (uploads, earlier runs).

@@ -24,6 +24,7 @@
 #include "march_wide.cuh"
 #include "fmarch.cuh"
 #include "fvec.cuh"
+#include "hyb.cuh"
 #include "farfield.cuh"
 #include "kernels.cuh"
 #include "adjoint.cuh"
@@ -151,8 +152,10 @@ struct xfd_engine {
   int graph_chunk = 32;
   // 0 split, 1 fused, 2 fused + TMA, 3 split marching, 4 split marching + TMA,
   // 5 fused marching (overlapped tiles) + TMA, 6 = 5 with a two-nodes-per-
-  // thread form on the CPML-free interior
-  int kernel_mode = 4;
+  // thread form on the CPML-free interior, 7 fused H-then-E TMA sweep of the
+  // CPML-free interior box with the split marching forms on the CPML tiles
+  // (ping-pong buffers)
+  int kernel_mode = 7;
   int ichunk = 32;
   int march_ichunk = 16;  // planes per CTA of the marching split sweeps
   bool tma_ready = false;
@@ -177,6 +180,7 @@ struct xfd_engine {
   long long mtiles_key = -1;
   int2* d_xlayer = nullptr;  // per x plane: CPML layer code of the H / E layers
   size_t xlayer_slabs = (size_t)-1;  // slab count the table was built for
+  HybMaps hmaps[2]{};     // tensor maps of the fused interior sweep (sweep 7), by input buffer
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
   FvecMaps fvmaps[2]{};   // tensor maps of its two-nodes-per-thread interior form
   cudaGraphExec_t graph_exec = nullptr;
@@ -296,6 +300,21 @@ cudaMemcpy3DParms copy_parms(const xfd_engine* e, int c, void* dev, void* host, 
   return p;
 }
 
+inline bool is_fused(const xfd_engine* e) {
+  return e->kernel_mode == 1 || e->kernel_mode == 2 || e->kernel_mode == 5 ||
+         e->kernel_mode == 6;
+}
+// Sweeps whose step reads one field buffer and writes the other.
+inline bool is_pingpong(const xfd_engine* e) { return is_fused(e) || e->kernel_mode == 7; }
+inline bool uses_tma(const xfd_engine* e) {
+  return e->kernel_mode == 2 || e->kernel_mode == 4 || e->kernel_mode == 5 ||
+         e->kernel_mode == 6 || e->kernel_mode == 7;
+}
+// The CPML H psi buffer the next step reads: the fused sweeps ping-pong it
+// with the fields; sweep 7 updates it in place (the split CPML forms) and
+// keeps it in buffer 0; the in-place sweeps use the field buffer's.
+inline int psi_h_buf(const xfd_engine* e) { return e->kernel_mode == 7 ? 0 : e->cur; }
+
 template <typename T>
 YeeP<T> yee_params(xfd_engine* e) {
   YeeP<T> p{};
@@ -321,7 +340,7 @@ YeeP<T> yee_params(xfd_engine* e) {
     D.b_h = static_cast<const T*>(S.b_h);
     for (int w = 0; w < 2; ++w) {
       D.psi_e[w] = static_cast<T*>(S.psi_e[w]);
-      D.psi_h[w] = static_cast<T*>(S.psi_h[e->cur][w]);
+      D.psi_h[w] = static_cast<T*>(S.psi_h[psi_h_buf(e)][w]);
     }
   }
   return p;
@@ -348,15 +367,12 @@ constexpr int kFmStages = 4;
 constexpr int kFmTJ = 8;
 template <typename T>
 constexpr int kFvStages() { return sizeof(T) == 8 ? 3 : 4; }
+// Stages of the fused interior sweep (sweep 7): 4 CTAs per SM in FP32 and 3
+// in FP64 with the shared memory these take.
+template <typename T>
+constexpr int hyb_stages() { return sizeof(T) == 8 ? 3 : 4; }
 
-inline bool is_fused(const xfd_engine* e) {
-  return e->kernel_mode == 1 || e->kernel_mode == 2 || e->kernel_mode == 5 ||
-         e->kernel_mode == 6;
-}
-inline bool uses_tma(const xfd_engine* e) {
-  return e->kernel_mode == 2 || e->kernel_mode == 4 || e->kernel_mode == 5 ||
-         e->kernel_mode == 6;
-}
+
 
 // Encodes one 3-D tiled map over the (nz+1, ny+1, nx+1) lattice of `base`.
 template <typename EncFn>
@@ -536,6 +552,29 @@ xfd_status build_tma_maps(xfd_engine* e) {
       CUDA_TRY(e, cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        MG::smem(MF4)));
   }
+  // Fused interior sweep (sweep 7): per input buffer, E boxes (32 + 2 XA) x
+  // (kMTJ + 2), H boxes (32 + XA) x (kMTJ + 1), class boxes 40 x (kMTJ + 1).
+  {
+    using HG = HybGeom<T, kMTJ>;
+    for (int b = 0; b < 2; ++b) {
+      for (int c = 0; c < 3; ++c) {
+        CUresult r = encode_lattice(encode, &e->hmaps[b].e[c], dt, sizeof(T), e->fbuf[b][c], L,
+                                    HG::WE, HG::RE);
+        if (r == CUDA_SUCCESS)
+          r = encode_lattice(encode, &e->hmaps[b].h[c], dt, sizeof(T), e->fbuf[b][3 + c], L,
+                             HG::WH, HG::RH);
+        if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (hyb %d): %d", c, (int)r);
+      }
+      CUresult r = encode_lattice(encode, &e->hmaps[b].cls, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2,
+                                  e->cls, L, HG::WC, HG::RC);
+      if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (hyb class): %d", (int)r);
+    }
+    constexpr int HS = hyb_stages<T>();
+    CUDA_TRY(e, cudaFuncSetAttribute(k_hyb<T, kMTJ, HS, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, HG::smem(HS)));
+    CUDA_TRY(e, cudaFuncSetAttribute(k_hyb<T, kMTJ, HS, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, HG::smem(HS)));
+  }
   constexpr int MW = march_wide_stages<T>();
   CUDA_TRY(e, cudaFuncSetAttribute(k_march_h_wide<T, MW>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -700,10 +739,11 @@ MarchLayout march_layout(const xfd_engine* e) {
   // of 8 nodes, so that every TMA x coordinate stays a multiple of 16 bytes
   // for the field and the uint16 class maps alike).
   const int step[3] = {8, 1, 1};
+  const bool hyb = e->kernel_mode == 7;
   for (int g = 0; g < 3; ++g) {
     int best = -1;
     for (int sh = 0; sh > -size[g]; sh -= step[g]) {
-      if (!e->march_shift && sh != 0) break;
+      if ((!e->march_shift || hyb) && sh != 0) break;
       int lo = 0, hi = 0;
       const int nodes = march_free_run(e, g, sh, lo, hi);
       if (nodes > best) {
@@ -714,6 +754,26 @@ MarchLayout march_layout(const xfd_engine* e) {
       }
     }
     m.nt[g] = (n_nodes[g] - m.shift[g] + size[g] - 1) / size[g];
+  }
+  if (hyb) {
+    // The fused interior sweep has no range tests and no CPML terms: its box
+    // keeps one node away from the lattice's low faces (k, j, i >= 1) and
+    // below nz, ny, nx, and the nodes it recomputes below the box (row
+    // j0-1, column k0-1, plane i_lo-1) lie in no H layer of that axis.
+    const int upper[3] = {L.nz, L.ny, L.nx};
+    const int axis_of[3] = {2, 1, 0};
+    for (int g = 0; g < 3; ++g) {
+      if (m.lo[g] * size[g] < 1) m.lo[g] = 1;
+      m.hi[g] = std::min(m.hi[g], upper[g] / size[g]);
+      while (m.hi[g] > m.lo[g]) {
+        const int below = m.lo[g] * size[g] - 1;
+        bool in_layer = false;
+        for (const auto& S : e->slabs)
+          if (S.m == axis_of[g] && below >= S.h_lo && below < S.h_lo + S.n) in_layer = true;
+        if (!in_layer) break;
+        ++m.lo[g];
+      }
+    }
   }
   m.box = m.hi[0] > m.lo[0] && m.hi[1] > m.lo[1] && m.hi[2] > m.lo[2];
   // The box is away from every lattice boundary when no tile holds k = 0,
@@ -726,7 +786,8 @@ MarchLayout march_layout(const xfd_engine* e) {
   // 8-row tiles; the CPML form sweeps the rest, an unpaired tile row included.
   m.wy_lo = (m.lo[1] + 1) / 2;
   m.wy_hi = m.hi[1] / 2;
-  m.wide = m.in && e->march_wide && m.wy_hi > m.wy_lo;
+  m.wide = m.in && e->march_wide && m.wy_hi > m.wy_lo && !hyb;
+  if (hyb && !m.in) m.box = false;  // every tile goes to the CPML forms
   for (int a = 0; a < 3; ++a) {
     m.skip_lo[a] = m.box ? m.lo[a] : 0;
     m.skip_hi[a] = m.box ? m.hi[a] : 0;
@@ -780,9 +841,9 @@ void march_tile_lists(const xfd_engine* e, std::vector<int4> lists[4]) {
 }
 
 xfd_status build_march_tiles(xfd_engine* e) {
-  const long long key = (long long)e->slabs.size() * 1000003LL + e->march_ichunk * 8 +
-                        (e->march_shift ? 4 : 0) + (e->march_wide ? 2 : 0) +
-                        (e->march_split_axes ? 1 : 0);
+  const long long key = (long long)e->slabs.size() * 1000003LL + e->march_ichunk * 16 +
+                        (e->kernel_mode == 7 ? 8 : 0) + (e->march_shift ? 4 : 0) +
+                        (e->march_wide ? 2 : 0) + (e->march_split_axes ? 1 : 0);
   if (key == e->mtiles_key) return XFD_OK;
   std::vector<int4> lists[4];
   march_tile_lists(e, lists);
@@ -809,10 +870,11 @@ xfd_status build_march_tiles(xfd_engine* e) {
 
 template <typename T>
 MarchP<T> march_params(xfd_engine* e) {
-  const FusedP<T> f = fused_params<T>(e, e->cur, e->cur);
+  const int pb = psi_h_buf(e);
+  const FusedP<T> f = fused_params<T>(e, pb, pb);
   MarchP<T> p{};
   p.L = f.L;
-  for (int c = 0; c < 6; ++c) p.f[c] = f.out[c];
+  for (int c = 0; c < 6; ++c) p.f[c] = static_cast<T*>(e->fbuf[e->cur][c]);
   p.cls = f.cls;
   p.tab = f.tab;
   p.n_classes = e->n_classes;
@@ -834,18 +896,142 @@ OverrideD<T> ovr_of(const xfd_engine* e) {
 }
 
 // Launches one time step (host step index t decides the periodic kernels).
+// Sweep 7, one step from buffer `in` to `out`: the fused box kernel (side
+// stream 0) beside the CPML form's H tile lists and the H lattice faces (main
+// stream, side streams 1-3); then the TFSF H passes outside the box; then,
+// once the box kernel is done, the CPML form's E tile lists and the E faces.
+// The CPML forms read the old fields of `in` and the new H of `out` through
+// their tensor maps and write `out`; their psi stay in place (buffer 0).
+template <typename T>
+cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
+  cudaStream_t s = e->stream;
+  const MarchLayout ml = march_layout(e);
+  constexpr int MS = march_stages<T>();
+  constexpr int MF = march_free_stages<T>();
+  constexpr int HS = hyb_stages<T>();
+  const size_t msm = MarchGeom<T, kMTJ, 32>::smem(MS);
+  const size_t msm_free = MarchGeom<T, kMTJ, 32>::smem(MF);
+  const dim3 blk_m(32, kMTJ, 1);
+  T* const* fields_in = reinterpret_cast<T* const*>(e->d_fields[in]);
+  MarchTmaP<T> mh{};
+  mh.p = march_params<T>(e);
+  for (int c = 0; c < 6; ++c) mh.p.f[c] = static_cast<T*>(e->fbuf[out][c]);
+  mh.m = e->mtma[in];  // old E halo boxes, old H tiles
+  mh.err = e->d_err;
+  for (int a = 0; a < 3; ++a) {
+    mh.box_lo[a] = ml.skip_lo[a];
+    mh.box_hi[a] = ml.skip_hi[a];
+    mh.shift[a] = 0;
+  }
+  MarchTmaP<T> me = mh;
+  for (int c = 0; c < 3; ++c) {
+    me.m.halo[3 + c] = e->mtma[out].halo[3 + c];  // new H halo boxes
+    me.m.tile[c] = e->mtma[in].tile[c];           // old E tiles
+  }
+  YeeP<T> yp = yee_params<T>(e);
+  for (int c = 0; c < 6; ++c) yp.f[c] = static_cast<T*>(e->fbuf[out][c]);
+  const unsigned edge_blocks = (unsigned)((edge_nodes(e->L) + 255) / 256);
+  cudaError_t c = cudaSuccess;
+  auto fork = [&](int first) {
+    if (c == cudaSuccess) c = cudaEventRecord(e->fork_ev, s);
+    for (int q = first; q < kSides && c == cudaSuccess; ++q)
+      c = cudaStreamWaitEvent(e->side[q], e->fork_ev, 0);
+  };
+  auto join = [&](int first, int last) {
+    for (int q = first; q <= last && c == cudaSuccess; ++q) {
+      c = cudaEventRecord(e->join_ev[q], e->side[q]);
+      if (c == cudaSuccess) c = cudaStreamWaitEvent(s, e->join_ev[q], 0);
+    }
+  };
+  auto lists = [&](const MarchTmaP<T>& P, auto kx4, auto ky4, auto kz4, auto kcp) {
+    auto list = [&](auto k, int q, size_t sm) {
+      const int n = e->mt_off[q + 1] - e->mt_off[q];
+      cudaStream_t sq = q == 3 ? s : e->side[q + 1];
+      if (n > 0 && c == cudaSuccess) k<<<n, blk_m, sm, sq>>>(P, e->d_mtiles + e->mt_off[q]);
+    };
+    list(kx4, 0, msm_free);
+    list(ky4, 1, msm_free);
+    list(kz4, 2, msm_free);
+    list(kcp, 3, msm);
+  };
+  fork(0);
+  if (ml.box && c == cudaSuccess) {
+    HybP<T> hp{};
+    hp.L = e->L;
+    for (int q = 0; q < 6; ++q) hp.out[q] = static_cast<T*>(e->fbuf[out][q]);
+    hp.tab = static_cast<const T*>(e->tab);
+    hp.n_classes = e->n_classes;
+    for (int a = 0; a < 3; ++a) {
+      hp.fe[a] = static_cast<const T*>(e->fe[a]);
+      hp.fh[a] = static_cast<const T*>(e->fh[a]);
+      hp.org[a] = ml.lo[a];
+    }
+    hp.tf = e->tfsf;
+    hp.tfh = e->tfsf_h;
+    hp.tfh.enabled = e->have_tfsf ? 1 : 0;
+    hp.step = e->d_step;
+    hp.err = e->d_err;
+    hp.m = e->hmaps[in];
+    hp.ichunk = e->march_ichunk;
+    const dim3 g(ml.hi[0] - ml.lo[0], ml.hi[1] - ml.lo[1], ml.hi[2] - ml.lo[2]);
+    const size_t hsm = HybGeom<T, kMTJ>::smem(HS);
+    if (e->have_tfsf)
+      k_hyb<T, kMTJ, HS, true><<<g, blk_m, hsm, e->side[0]>>>(hp);
+    else
+      k_hyb<T, kMTJ, HS, false><<<g, blk_m, hsm, e->side[0]>>>(hp);
+  }
+  lists(mh, k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 1>,
+        k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 2>,
+        k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 4>,
+        k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 7>);
+  if (c == cudaSuccess) k_edge_pp<T, false><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in);
+  join(1, kSides - 1);
+  if (e->have_tfsf && c == cudaSuccess) {
+    Box3 skip{};
+    if (ml.box) {
+      const int size[3] = {32, kMTJ, e->march_ichunk};
+      for (int g = 0; g < 3; ++g) {
+        const int a = 2 - g;  // tile dimension g -> lattice axis
+        skip.lo[a] = ml.lo[g] * size[g];
+        skip.hi[a] = ml.hi[g] * size[g];
+      }
+    }
+    T* const* fo = reinterpret_cast<T* const*>(e->d_fields[out]);
+    for (int g = 0; g < 2; ++g) {
+      const auto& G = e->tfsf_groups[g];
+      if (G.total > 0)
+        k_tfsf_outside<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fo,
+                                                                   e->d_step, e->d_err, skip);
+    }
+  }
+  join(0, 0);  // the box kernel's new H
+  fork(1);
+  lists(me, k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 1>,
+        k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 2>,
+        k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 4>,
+        k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 7>);
+  if (c == cudaSuccess) k_edge_pp<T, true><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in);
+  join(1, kSides - 1);
+  if (c != cudaSuccess) return c;
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   cudaStream_t s = e->stream;
   const bool fused = is_fused(e);
-  const int in = e->cur, out = fused ? 1 - e->cur : e->cur;
+  const bool pp = is_pingpong(e);
+  const int in = e->cur, out = pp ? 1 - e->cur : e->cur;
   T* const* fields = reinterpret_cast<T* const*>(e->d_fields[out]);
   T* const* fields_in = reinterpret_cast<T* const*>(e->d_fields[in]);
   AdeD<T> ad{};
   if (e->ade_kind >= 0) {
     if constexpr (sizeof(T) == 8) ad = e->ade64; else ad = e->ade32;
   }
-  if (fused) {
+  if (e->kernel_mode == 7) {
+    cudaError_t c = enqueue_hyb_t<T>(e, in, out);
+    if (c != cudaSuccess) return c;
+  } else if (fused) {
     // H + TFSF-H + CPML-H, then E + CPML-E, in one sweep: in -> out.
     const dim3 blk(kTK, kTJ, 1);
     const dim3 grd((unsigned)((e->L.nz + 1 + kTK - 1) / kTK),
@@ -1056,9 +1242,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   // Coefficient overrides complete the E update of their nodes.
   if (e->n_ovr)
     k_ovr_apply<T><<<blocks_for(e->n_ovr, 256), 256, 0, s>>>(ovr_of<T>(e), fields,
-                                                             fused ? fields_in : nullptr);
+                                                             pp ? fields_in : nullptr);
   // ADE -> lumped -> TFSF E faces (the reference's updateE then correctE order).
-  T* const* ecur = fused ? fields_in : nullptr;
+  T* const* ecur = pp ? fields_in : nullptr;
   if (e->ade_kind == 0) k_ade_update<T, 0><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
   if (e->ade_kind == 1) k_ade_update<T, 1><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
   if (e->ade_kind == 2) k_ade_update<T, 2><<<blocks_for(ad.n, 256), 256, 0, s>>>(ad, fields, ecur);
@@ -1112,7 +1298,7 @@ long long pattern_period(const xfd_engine* e) {
   long long per = 1;
   for (const auto& mv : e->movies) per = per / gcd_ll(per, mv.d.interval) * mv.d.interval;
   if (e->have_nf2ff) per = per / gcd_ll(per, e->nf2ff.batch) * e->nf2ff.batch;
-  if (is_fused(e) && per % 2) per *= 2;  // buffers alternate every step
+  if (is_pingpong(e) && per % 2) per *= 2;  // buffers alternate every step
   return per;
 }
 
@@ -1147,7 +1333,7 @@ xfd_status ensure_ready(xfd_engine* e) {
     e->xlayer_slabs = e->slabs.size();
     e->graph_dirty = true;
   }
-  if (e->kernel_mode == 4) {
+  if (e->kernel_mode == 4 || e->kernel_mode == 7) {
     xfd_status st = build_march_tiles(e);
     if (st != XFD_OK) return st;
   }
@@ -1892,6 +2078,8 @@ xfd_status xfd_set_nf2ff(xfd_engine* e, const xfd_nf2ff_desc* d) {
   nf.sample = static_cast<double*>(p);
   if ((s = dev_alloc(e, &p, (size_t)nf.nf * 4 * total * sizeof(double2))) != XFD_OK) return s;
   nf.acc = static_cast<double2*>(p);
+  if ((s = dev_alloc(e, &p, (size_t)nf.nf * 4 * total * sizeof(double2))) != XFD_OK) return s;
+  nf.comp = static_cast<double2*>(p);
   double* q = nullptr;
   if ((s = upload_raw(e, &q, d->te, (size_t)nf.nf * e->n_steps * 2)) != XFD_OK) return s;
   nf.te = reinterpret_cast<const double2*>(q);
@@ -1971,6 +2159,7 @@ xfd_status xfd_nf2ff_far_field(xfd_engine* e, const xfd_far_field_desc* d, doubl
       fd.e[f][a] = nf.e[f][a];
     }
   fd.acc = nf.acc;
+  fd.comp = nf.comp;
   for (int a = 0; a < 3; ++a) fd.origin[a] = d->origin[a];
   xfd_status s2 = XFD_OK;
   double2* dout = nullptr;
@@ -2119,10 +2308,16 @@ xfd_status xfd_get_nf2ff(xfd_engine* e, double* out, int64_t capacity, int64_t* 
   if (count) *count = total;
   if (!out) return XFD_OK;
   if (capacity < total) return fail(e, XFD_ERR_INVALID_ARGUMENT, "NF2FF buffer too small");
-  std::vector<double2> h((size_t)total);
+  std::vector<double2> h((size_t)total), hc((size_t)total);
   CUDA_TRY(e, cudaMemcpyAsync(h.data(), nf.acc, total * sizeof(double2), cudaMemcpyDeviceToHost,
                               e->stream));
+  CUDA_TRY(e, cudaMemcpyAsync(hc.data(), nf.comp, total * sizeof(double2),
+                              cudaMemcpyDeviceToHost, e->stream));
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  for (long long x = 0; x < total; ++x) {  // running sums + their compensation
+    h[(size_t)x].x += hc[(size_t)x].x;
+    h[(size_t)x].y += hc[(size_t)x].y;
+  }
   // device [f][q][p] (p over all faces) -> [f][face][q][face nodes]
   long long o = 0;
   for (int f = 0; f < nf.nf; ++f)
@@ -2246,7 +2441,7 @@ xfd_status xfd_run(xfd_engine* e, int64_t n) {
       if (left >= e->graph_len) {
         CUDA_TRY(e, cudaGraphLaunch(e->graph_exec, e->stream));
         e->host_step += e->graph_len;
-        if (e->graph_len % 2 && is_fused(e)) e->cur = 1 - e->cur;
+        if (e->graph_len % 2 && is_pingpong(e)) e->cur = 1 - e->cur;
         left -= e->graph_len;
         if ((s = queue_frame_copies(e)) != XFD_OK) return s;
         continue;
@@ -2299,9 +2494,23 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "graph_chunk range");
     e->graph_chunk = (int)value;
   } else if (!strcmp(name, "kernel")) {
-    if (value < 0 || value > 6)
+    if (value < 0 || value > 7)
       return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
+    const int before = psi_h_buf(e);
     e->kernel_mode = (int)value;
+    const int after = psi_h_buf(e);
+    if (before != after) {  // the next step reads the H psi from another buffer
+      CUDA_TRY(e, cudaSetDevice(e->device));
+      for (const auto& S : e->slabs) {
+        const size_t b = (S.m == 0   ? (size_t)S.n * e->L.NY * e->L.KP
+                          : S.m == 1 ? (size_t)(e->L.nx + 1) * S.n * e->L.KP
+                                     : (size_t)(e->L.nx + 1) * e->L.NY * S.n) *
+                         e->wsize;
+        for (int w = 0; w < 2; ++w)
+          CUDA_TRY(e, cudaMemcpyAsync(S.psi_h[after][w], S.psi_h[before][w], b,
+                                      cudaMemcpyDeviceToDevice, e->stream));
+      }
+    }
   } else if (!strcmp(name, "ichunk")) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "ichunk range");
     e->ichunk = (int)value;
@@ -2332,6 +2541,25 @@ void* xfd_stream(xfd_engine* e) { return e ? (void*)e->stream : nullptr; }
 int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (!e) return 0;
   const bool fused = is_fused(e);
+  if (e->kernel_mode == 7) {
+    // box kernel, the nonempty CPML tile lists and the lattice faces of both
+    // phases, the TFSF H passes outside the box, then the common tail
+    const MarchLayout ml = march_layout(e);
+    std::vector<int4> lists[4];
+    march_tile_lists(e, lists);
+    int n = 1 + (ml.box ? 1 : 0) + 2;  // step counter, box, faces
+    for (int q = 0; q < 4; ++q)
+      if (!lists[q].empty()) n += 2;
+    if (e->have_tfsf) n += 4;
+    if (e->ade_kind >= 0) n += 1;
+    if (!e->lumped_h.empty()) n += 1;
+    if (!e->ind_h.empty()) n += 1;
+    if (e->have_nf2ff) n += 1;
+    if (e->have_td) n += 1;
+    if (e->probes.n_probes) n += 1;
+    if (e->n_ovr) n += 1;
+    return n + e->n_rec;
+  }
   int n = fused ? 2 : 3;  // sweep(s) + step counter
   if (e->kernel_mode == 5 || e->kernel_mode == 6) {
     int nt[3], lo[3], hi[3];
@@ -2371,6 +2599,25 @@ int64_t xfd_stencil_bytes_per_step(const xfd_engine* e) {
     for (int a = 0; a < 3; ++a)
       if (a != s.m) slab_cells *= n[a];
     b += slab_cells * 8LL * (long long)e->wsize;
+  }
+  return b;
+}
+
+int64_t xfd_algorithmic_bytes_per_step(const xfd_engine* e) {
+  if (!e) return 0;
+  const long long w = (long long)e->wsize;
+  long long b = xfd_stencil_bytes_per_step(e);
+  if (e->ade_kind >= 0) {
+    const long long n = e->precision == XFD_FP64 ? e->ade64.n : e->ade32.n;
+    const long long np = e->precision == XFD_FP64 ? e->ade64.np : e->ade32.np;
+    b += n * (2 * np * w + (e->ade_kind == 0 ? 2 * np * w + 2 * w : 0));
+  }
+  if (e->have_tfsf)
+    for (int g = 0; g < 4; ++g) b += e->tfsf_groups[g].total * 2 * w;
+  if (e->have_nf2ff) {
+    const Nf2ffD& nf = e->nf2ff;
+    b += nf.P * 4 * 8;                                    // FP64 samples
+    b += nf.P * 4LL * nf.nf * 16 * 2 / (long long)nf.batch;  // accumulators per batch
   }
   return b;
 }

@@ -25,6 +25,7 @@ struct FarFieldD {
   long long begin[7];        // first point of each face; begin[6] = P
   int s[6][3], e[6][3];      // face boxes [s, e)
   const double2* acc;        // (nf * 4) x P: J_a, J_b, M_a, M_b per frequency
+  const double2* comp;       // same shape: compensation terms, value = acc + comp
   const double* k0;          // nf: wave numbers 2 pi f / c
   const double* ang;         // n_ang x 8: T_theta[x,y,z], T_phi[x,y,z], st*cp, st*sp
   const double* cos_t;       // n_ang
@@ -48,6 +49,11 @@ __global__ void __launch_bounds__(256) k_far_field(const __grid_constant__ FarFi
 #pragma unroll
   for (int r = 0; r < 4; ++r) acc[r] = make_double2(0.0, 0.0);
   const double2* J = d.acc + (long long)f * 4 * d.P;
+  const double2* Jc = d.comp + (long long)f * 4 * d.P;
+  auto cur = [&](long long o) {
+    const double2 a = J[o], c = Jc[o];
+    return make_double2(a.x + c.x, a.y + c.y);
+  };
   for (long long p = threadIdx.x; p < d.P; p += blockDim.x) {
     int face = 0;
     while (face < 5 && p >= d.begin[face + 1]) ++face;
@@ -67,7 +73,7 @@ __global__ void __launch_bounds__(256) k_far_field(const __grid_constant__ FarFi
     double sn, cs;
     sincos(k0 * arg, &sn, &cs);
     const double2 ph = make_double2(cs, sn);
-    const double2 ja = J[p], jb = J[d.P + p], ma = J[2 * d.P + p], mb = J[3 * d.P + p];
+    const double2 ja = cur(p), jb = cur(d.P + p), ma = cur(2 * d.P + p), mb = cur(3 * d.P + p);
     const double tta = T[A], ttb = T[B], tpa = T[3 + A], tpb = T[3 + B];
     // rows: a_theta (J, theta), f_phi (M, phi), a_phi (J, phi), f_theta (M, theta)
     const double2 src[4] = {

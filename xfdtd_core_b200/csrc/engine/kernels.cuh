@@ -82,8 +82,12 @@ __device__ __forceinline__ long long sel3(int m, long long a, long long b, long 
   return m == 0 ? a : (m == 1 ? b : c);
 }
 
+// `rd` (ping-pong sweeps): the buffer holding the old fields, read for the
+// node's own value and its E neighbours; the result goes to p.f.  Null: in
+// place.
 template <typename T>
-__device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, int k) {
+__device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, int k,
+                                              T* const* rd = nullptr) {
   const Lat L = p.L;
   const long long id = lat_index(L, i, j, k);
   const int x[3] = {i, j, k};
@@ -101,10 +105,10 @@ __device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, in
     T* H = p.f[3 + c];
     const T ca = row[6 + 2 * c];
     const T cb = row[7 + 2 * c];
-    T h = H[id];
+    T h = rd ? rd[3 + c][id] : H[id];
     if (main_rng) {
-      const T* Ea = p.f[ta];
-      const T* Eb = p.f[tb];
+      const T* Ea = rd ? rd[ta] : p.f[ta];
+      const T* Eb = rd ? rd[tb] : p.f[tb];
       const T d_a = Ea[id + st[tb]] - Ea[id];
       const T d_b = Eb[id + st[ta]] - Eb[id];
       h = ca * h + cb * (p.fh[tb][x[tb]] * d_a - p.fh[ta][x[ta]] * d_b);
@@ -116,7 +120,8 @@ __device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, in
       if (l < 0 || l >= sl.n) continue;
       const int which = (c == (sl.m + 1) % 3) ? 0 : 1;
       // H_A differences E_B, H_B differences E_A, forward along m.
-      const T* D = p.f[which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3];
+      const int dc = which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3;
+      const T* D = rd ? rd[dc] : p.f[dc];
       const T diff = D[id + sel3(sl.m, st[0], st[1], st[2])] - D[id];
       T* ps = sl.psi_h[which] + psi_index(sl, L, i, j, k, l);
       const T psi = sl.b_h[l] * *ps + sl.a_h[l] * diff;
@@ -133,8 +138,11 @@ __device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, in
 // CPML (PMLCorrector<xyz>::correctE, pml_corrector.h:178-288): layers
 // [e_lo, e_lo + n) along m, whole transverse extent.
 // ---------------------------------------------------------------------------
+// `rd` (ping-pong sweeps): the buffer holding the old E, read for the node's
+// own value; the new H neighbours and the result are in p.f.  Null: in place.
 template <typename T>
-__device__ __forceinline__ void update_e_node(const YeeP<T>& p, int i, int j, int k) {
+__device__ __forceinline__ void update_e_node(const YeeP<T>& p, int i, int j, int k,
+                                              T* const* rd = nullptr) {
   const Lat L = p.L;
   const long long id = lat_index(L, i, j, k);
   const int x[3] = {i, j, k};
@@ -159,7 +167,7 @@ __device__ __forceinline__ void update_e_node(const YeeP<T>& p, int i, int j, in
     T* E = p.f[c];
     const T ca = row[2 * c];
     const T cb = row[2 * c + 1];
-    T e = E[id];
+    T e = rd ? rd[c][id] : E[id];
     if (main_rng) {
       const T* Ha = p.f[3 + ta];
       const T* Hb = p.f[3 + tb];
@@ -259,6 +267,22 @@ __global__ void __launch_bounds__(256) k_edge_e(const __grid_constant__ YeeP<T> 
   edge_update<T, true>(p, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// Ping-pong forms (sweep 7): every face node is written to p.f from the old
+// fields in `rd` -- its CPML-corrected value, or the old value carried over
+// when it lies in no layer -- so that the output buffer is complete.
+template <typename T, bool E>
+__global__ void __launch_bounds__(256) k_edge_pp(const __grid_constant__ YeeP<T> p,
+                                                 T* const* rd) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= edge_nodes(p.L)) return;
+  int i, j, k;
+  edge_node(p.L, t, i, j, k);
+  if (E)
+    update_e_node(p, i, j, k, rd);
+  else
+    update_h_node(p, i, j, k, rd);
+}
+
 // Many lattices in one launch: block b covers the 256 face nodes starting at
 // blocks[b].y * 256 of lattice blocks[b].x.
 template <typename T, bool E>
@@ -330,10 +354,15 @@ __device__ __forceinline__ double tfsf_incident(const TfsfD& tf, bool inc_e, int
   return tr * ((1 - w) * row[idx] + w * row[idx + 1]);
 }
 
+// A node box [lo, hi) (empty when lo = hi).
+struct Box3 {
+  int lo[3], hi[3];
+};
+
 template <typename T>
 __device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, const Lat& L,
                                           T* const* fields, const long long* step, int* err,
-                                          long long tid) {
+                                          long long tid, const Box3& skip = Box3{}) {
   if (tid >= g.total) return;
   int q = 0;
   while (q + 1 < g.n && tid >= g.pass[q + 1].begin) ++q;
@@ -357,6 +386,9 @@ __device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, 
     inc_e = true;   // H face corrects the node half a cell outside
     if (P.neg) xf[m] -= 1;
   }
+  if (xf[0] >= skip.lo[0] && xf[0] < skip.hi[0] && xf[1] >= skip.lo[1] && xf[1] < skip.hi[1] &&
+      xf[2] >= skip.lo[2] && xf[2] < skip.hi[2])
+    return;  // corrected inside the fused sweep
   const int dual = (P.field == (m + 1) % 3) ? (m + 2) % 3 : (m + 1) % 3;
   int e_flag = 0;
   const double v = tfsf_incident(tf, inc_e, dual, t, xi, &e_flag);
@@ -370,6 +402,15 @@ template <typename T>
 __global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const long long* step,
                        int* err) {
   tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The passes of one group on the nodes outside `skip` (sweep 7: the fused
+// box kernel applies the H passes of its own nodes inline).
+template <typename T>
+__global__ void k_tfsf_outside(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields,
+                               const long long* step, int* err, Box3 skip) {
+  tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+               skip);
 }
 
 // Per-lattice TFSF state for the batched launch: the incident tables, the
@@ -529,13 +570,29 @@ __global__ void k_ade_update(AdeD<T> a, T* const* fields, T* const* fields_in) {
 // k_nf2ff_dft folds a full batch into the complex FP64 accumulators with the
 // per-step phasors (FDPlaneData::initDFT, src/nffft/nffft_fd_data.cpp:65-76).
 // ---------------------------------------------------------------------------
+// Compensated accumulation across batches (a run of thousands of steps adds
+// one batch partial per window to each running sum): s + x is rounded into s
+// and its exact rounding error (Knuth's TwoSum, six additions, no branch) is
+// added to c, so the error of the final s + c does not grow with the number
+// of windows.  The _rn intrinsics keep the compiler from contracting or
+// reassociating the additions.
+__device__ __forceinline__ void two_sum_acc(double& s, double& c, double x) {
+  const double t = __dadd_rn(s, x);
+  const double bp = __dsub_rn(t, s);
+  const double err = __dadd_rn(__dsub_rn(s, __dsub_rn(t, bp)), __dsub_rn(x, bp));
+  c = __dadd_rn(c, err);
+  s = t;
+}
+
 struct Nf2ffD {
   int nf, batch;
   int s[6][3], e[6][3];
   long long begin[7];  // node offsets per face, begin[6] = total
   long long P;
   double* sample;      // batch x 4 x P
-  double2* acc;        // (nf*4) x P
+  double2* acc;        // (nf*4) x P: running sums
+  double2* comp;       // (nf*4) x P: their compensation terms (TwoSum errors);
+                       // the accumulated value is acc + comp
   const double2* te;   // nf x n_steps
   const double2* th;
   int n_steps;
@@ -650,11 +707,12 @@ __global__ void __launch_bounds__(256) k_nf2ff_dft(Nf2ffD nf, const long long* s
 #pragma unroll
     for (int u = 0; u < FCH; ++u) {
       if (f0 + u < nf.nf) {
-        double2* a = nf.acc + ((long long)(f0 + u) * 4 + q) * nf.P + p;
-        double2 z = *a;
-        z.x += nf.scale * re[u];
-        z.y += nf.scale * im[u];
-        *a = z;
+        const long long o = ((long long)(f0 + u) * 4 + q) * nf.P + p;
+        double2 z = nf.acc[o], c = nf.comp[o];
+        two_sum_acc(z.x, c.x, __dmul_rn(nf.scale, re[u]));
+        two_sum_acc(z.y, c.y, __dmul_rn(nf.scale, im[u]));
+        nf.acc[o] = z;
+        nf.comp[o] = c;
       }
     }
   }

@@ -43,7 +43,39 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_nf2ff_scratch[4 * kMaxPoints];
 
 std::mutex g_mu;
-double* g_scratch_addr[kMaxDevices] = {};  // device address, per device
+// Device address of the scratch array per device, with the CUDA context it
+// was looked up in: a cudaDeviceReset ends that context, and the next call
+// (in a new context) looks the address up again.
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;
+  double* addr = nullptr;
+};
+ScratchAddr g_scratch_addr[kMaxDevices];
+
+// Unique id of the calling thread's current context (cuCtxGetId, through the
+// runtime's driver entry point: this library links only the runtime).
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+bool current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    looked_up = true;
+  }
+  void* ctx = nullptr;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx) return false;
+  return get_id(ctx, id) == 0;
+}
 
 struct FieldView {
   const void* f[6];
@@ -120,11 +152,20 @@ __global__ void k_nf2ff_sample_static(FieldView v, Faces fc, double* scratch) {
   out[3 * P] = -cj2 * surf_e<T>(v, m, A, i, j, k);
 }
 
+// s + x rounded into s, its exact rounding error (Knuth's TwoSum) added to c.
+__device__ __forceinline__ void two_sum_acc(double& s, double& c, double x) {
+  const double t = __dadd_rn(s, x);
+  const double bp = __dsub_rn(t, s);
+  c = __dadd_rn(c, __dadd_rn(__dsub_rn(s, __dsub_rn(t, bp)), __dsub_rn(x, bp)));
+  s = t;
+}
+
 // One thread per (q, p): acc[f][q][p] += scale * sample[q][p] * phasor_q[f][t]
-// (J currents q = 0, 1 take the H-time phasors th, M currents q = 2, 3 te).
+// (J currents q = 0, 1 take the H-time phasors th, M currents q = 2, 3 te);
+// with `comp` the addition is compensated (acc + comp is the sum).
 __global__ void k_nf2ff_dft_static(const double* scratch, long long P, int nf,
                                    const double2* te, const double2* th, long long n_steps,
-                                   long long t, double scale, double2* acc) {
+                                   long long t, double scale, double2* acc, double2* comp) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= 4 * P) return;
   const int q = (int)(tid / P);
@@ -133,11 +174,18 @@ __global__ void k_nf2ff_dft_static(const double* scratch, long long P, int nf,
   const double2* ph = q < 2 ? th : te;
   for (int f = 0; f < nf; ++f) {
     const double2 z = ph[(long long)f * n_steps + t];
-    double2* a = acc + ((long long)f * 4 + q) * P + p;
-    double2 w = *a;
-    w.x += scale * (v * z.x);
-    w.y += scale * (v * z.y);
-    *a = w;
+    const long long o = ((long long)f * 4 + q) * P + p;
+    double2 w = acc[o];
+    if (comp) {
+      double2 c = comp[o];
+      two_sum_acc(w.x, c.x, __dmul_rn(scale, __dmul_rn(v, z.x)));
+      two_sum_acc(w.y, c.y, __dmul_rn(scale, __dmul_rn(v, z.y)));
+      comp[o] = c;
+    } else {
+      w.x += scale * (v * z.x);
+      w.y += scale * (v * z.y);
+    }
+    acc[o] = w;
   }
 }
 
@@ -153,21 +201,30 @@ xfd_status fail(xfd_status s, const char* fmt, ...) {
 
 // The device address of the scratch array on the current device.  The
 // array's name in host code is only a host-side handle, so the address is
-// looked up once per device (with that device current) and kept.
+// looked up once per device and context (with that device current) and kept.
 xfd_status scratch_on_current_device(double** out) {
   int dev = 0;
   cudaError_t c = cudaGetDevice(&dev);
   if (c != cudaSuccess) return fail(XFD_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(c));
   if (dev < 0 || dev >= kMaxDevices) return fail(XFD_ERR_UNSUPPORTED, "device %d", dev);
+  // Make the device's primary context current (since CUDA 12 cudaSetDevice
+  // initialises it), so that the context id below is the one the launches
+  // will use.
+  c = cudaSetDevice(dev);
+  if (c != cudaSuccess) return fail(XFD_ERR_CUDA, "CUDA context: %s", cudaGetErrorString(c));
+  unsigned long long ctx = 0;
+  const bool have_ctx = current_context_id(&ctx);
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev]) {
+  ScratchAddr& a = g_scratch_addr[dev];
+  if (!a.addr || !have_ctx || a.ctx_id != ctx) {
     void* p = nullptr;
     c = cudaGetSymbolAddress(&p, g_nf2ff_scratch);
     if (c != cudaSuccess || !p)
       return fail(XFD_ERR_CUDA, "cudaGetSymbolAddress(NF2FF scratch): %s", cudaGetErrorString(c));
-    g_scratch_addr[dev] = static_cast<double*>(p);
+    a.addr = static_cast<double*>(p);
+    a.ctx_id = have_ctx ? ctx : 0;
   }
-  *out = g_scratch_addr[dev];
+  *out = a.addr;
   return XFD_OK;
 }
 
@@ -237,7 +294,8 @@ extern "C" xfd_status xfd_nf2ff_step_static(const xfd_nf2ff_step_desc* d, void* 
   k_nf2ff_dft_static<<<g2, 256, 0, s>>>(scratch, total, d->n_freq,
                                          reinterpret_cast<const double2*>(d->te),
                                          reinterpret_cast<const double2*>(d->th), d->n_steps,
-                                         d->step, d->scale, reinterpret_cast<double2*>(d->acc));
+                                         d->step, d->scale, reinterpret_cast<double2*>(d->acc),
+                                         reinterpret_cast<double2*>(d->acc_comp));
   cudaError_t c = cudaGetLastError();
   if (c != cudaSuccess) return fail(XFD_ERR_CUDA, "NF2FF step launch: %s", cudaGetErrorString(c));
   return XFD_OK;

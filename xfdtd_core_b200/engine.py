@@ -59,7 +59,8 @@ class Nf2ffStepDesc(ctypes.Structure):
                 ("fields", ctypes.c_void_p * 6), ("n_freq", _i32),
                 ("task_s", (_i32 * 3) * 6), ("task_e", (_i32 * 3) * 6),
                 ("te", ctypes.c_void_p), ("th", ctypes.c_void_p), ("n_steps", _i64),
-                ("step", _i64), ("scale", ctypes.c_double), ("acc", ctypes.c_void_p)]
+                ("step", _i64), ("scale", ctypes.c_double), ("acc", ctypes.c_void_p),
+                ("acc_comp", ctypes.c_void_p)]
 
 
 class FarFieldDesc(ctypes.Structure):
@@ -122,6 +123,7 @@ def load(build_if_missing: bool = True):
         "xfd_stream": ([vp], vp),
         "xfd_launches_per_step": ([vp], _i32),
         "xfd_stencil_bytes_per_step": ([vp], _i64),
+        "xfd_algorithmic_bytes_per_step": ([vp], _i64),
         "xfd_set_e_overrides": ([vp, _i64, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _dp, _dp],
                                 ctypes.c_int),
         "xfd_checkpoint_save": ([vp, _i32], ctypes.c_int),
@@ -159,7 +161,8 @@ def exported_symbols() -> List[str]:
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
-            "xfd_launches_per_step", "xfd_stencil_bytes_per_step", "xfd_set_e_overrides",
+            "xfd_launches_per_step", "xfd_stencil_bytes_per_step",
+            "xfd_algorithmic_bytes_per_step", "xfd_set_e_overrides",
             "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
             "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_set_nf2ff_td", "xfd_get_nf2ff_td",
             "xfd_add_probe", "xfd_get_probe",
@@ -384,12 +387,15 @@ class Engine:
 
 
 def nf2ff_step_static(n, precision: int, fields, tasks, te_dev: int, th_dev: int, n_freq: int,
-                      n_steps: int, step: int, scale: float, acc_dev: int, stream: int = 0):
+                      n_steps: int, step: int, scale: float, acc_dev: int, stream: int = 0,
+                      acc_comp_dev: int = 0):
     """Folds one time step of the Huygens-surface fields into `acc_dev` through
     xfd_nf2ff_step_static, the entry point that allocates no device memory
     (for callers whose device memory belongs to another allocator).  `fields`
     are six device addresses of the component arrays in the reference shapes;
-    te_dev/th_dev/acc_dev are device addresses of complex128 arrays."""
+    te_dev/th_dev/acc_dev are device addresses of complex128 arrays;
+    `acc_comp_dev` (optional, shaped like acc, zeroed before the first step)
+    turns on compensated accumulation (the sum is acc + acc_comp)."""
     L = load()
     d = Nf2ffStepDesc()
     d.nx, d.ny, d.nz = (int(x) for x in n)
@@ -403,6 +409,7 @@ def nf2ff_step_static(n, precision: int, fields, tasks, te_dev: int, th_dev: int
             d.task_s[f][a] = 0 if t is None else int(t[0][a])
             d.task_e[f][a] = 0 if t is None else int(t[1][a])
     d.te, d.th, d.acc = int(te_dev), int(th_dev), int(acc_dev)
+    d.acc_comp = int(acc_comp_dev) if acc_comp_dev else None
     d.n_steps, d.step, d.scale = int(n_steps), int(step), float(scale)
     st = L.xfd_nf2ff_step_static(ctypes.byref(d), ctypes.c_void_p(int(stream)))
     if st != 0:
