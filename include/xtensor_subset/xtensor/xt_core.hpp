@@ -42,8 +42,85 @@
 
 namespace xt {
 
-using shape_type = std::vector<std::size_t>;
-using strides_type = std::vector<std::ptrdiff_t>;
+// Shapes and strides: a vector-like sequence with inline storage (ranks up to
+// 8), so that small arrays and per-element temporaries allocate no heap blocks
+// for them.
+template <class T>
+class svector {
+ public:
+  static constexpr std::size_t cap = 8;
+  using value_type = T;
+  using size_type = std::size_t;
+  using iterator = T*;
+  using const_iterator = const T*;
+  svector() = default;
+  explicit svector(std::size_t n, const T& v = T()) { resize(n, v); }
+  svector(std::initializer_list<T> l) { assign(l.begin(), l.end()); }
+  template <class It, class = decltype(*std::declval<It>())>
+  svector(It a, It b) {
+    assign(a, b);
+  }
+  template <class U, std::size_t N>
+  svector(const std::array<U, N>& a) {
+    assign(a.begin(), a.end());
+  }
+  template <class U>
+  svector(const std::vector<U>& v) {
+    assign(v.begin(), v.end());
+  }
+  template <class It>
+  void assign(It a, It b) {
+    n_ = 0;
+    for (; a != b; ++a) push_back((T)*a);
+  }
+  std::size_t size() const { return n_; }
+  bool empty() const { return n_ == 0; }
+  T* data() { return v_; }
+  const T* data() const { return v_; }
+  T* begin() { return v_; }
+  T* end() { return v_ + n_; }
+  const T* begin() const { return v_; }
+  const T* end() const { return v_ + n_; }
+  T& operator[](std::size_t i) { return v_[i]; }
+  const T& operator[](std::size_t i) const { return v_[i]; }
+  T& front() { return v_[0]; }
+  const T& front() const { return v_[0]; }
+  T& back() { return v_[n_ - 1]; }
+  const T& back() const { return v_[n_ - 1]; }
+  void push_back(const T& x) {
+    if (n_ == cap) throw std::length_error("xt: rank above 8");
+    v_[n_++] = x;
+  }
+  void resize(std::size_t n, const T& x = T()) {
+    if (n > cap) throw std::length_error("xt: rank above 8");
+    for (std::size_t i = n_; i < n; ++i) v_[i] = x;
+    n_ = n;
+  }
+  T* insert(T* pos, const T& x) {
+    const std::size_t at = (std::size_t)(pos - v_);
+    push_back(x);
+    for (std::size_t i = n_ - 1; i > at; --i) v_[i] = v_[i - 1];
+    v_[at] = x;
+    return v_ + at;
+  }
+  T* erase(T* pos) {
+    for (T* p = pos; p + 1 < v_ + n_; ++p) *p = p[1];
+    --n_;
+    return pos;
+  }
+  operator std::vector<T>() const { return std::vector<T>(begin(), end()); }
+  friend bool operator==(const svector& a, const svector& b) {
+    return a.n_ == b.n_ && std::equal(a.begin(), a.end(), b.begin());
+  }
+  friend bool operator!=(const svector& a, const svector& b) { return !(a == b); }
+
+ private:
+  T v_[cap] = {};
+  std::size_t n_ = 0;
+};
+
+using shape_type = svector<std::size_t>;
+using strides_type = svector<std::ptrdiff_t>;
 
 template <class T>
 class xarray;
@@ -106,7 +183,7 @@ void for_each_offset(const shape_type& shape, const strides_type& st, std::ptrdi
     f(base);
     return;
   }
-  std::vector<std::size_t> idx(r, 0);
+  std::size_t idx[svector<std::size_t>::cap] = {};
   std::ptrdiff_t off = base;
   const std::size_t inner = shape[r - 1];
   const std::ptrdiff_t ist = st[r - 1];
@@ -146,24 +223,56 @@ inline strides_type broadcast_strides(const shape_type& s, const strides_type& s
   return out;
 }
 
+// Element storage: up to 4 numeric elements inline (small vectors such as a
+// 3-component coordinate), otherwise one heap block.
 template <class T>
 struct buffer {
-  std::unique_ptr<T[]> p;
+  static constexpr std::size_t inline_cap =
+      (std::is_arithmetic_v<T> || is_complex<T>::value) ? 4 : 0;
+  std::unique_ptr<T[]> heap;
+  T small[inline_cap > 0 ? inline_cap : 1] = {};
+  T* p = nullptr;
   std::size_t n = 0;
   buffer() = default;
-  explicit buffer(std::size_t m) : p(m ? new T[m]() : nullptr), n(m) {}
-  buffer(const buffer& o) : p(o.n ? new T[o.n] : nullptr), n(o.n) {
-    std::copy(o.p.get(), o.p.get() + n, p.get());
+  explicit buffer(std::size_t m) : n(m) {
+    if (m == 0) return;
+    if (m <= inline_cap) {
+      for (std::size_t i = 0; i < m; ++i) small[i] = T();
+      p = small;
+    } else {
+      heap.reset(new T[m]());
+      p = heap.get();
+    }
   }
-  buffer(buffer&&) noexcept = default;
+  buffer(const buffer& o) : buffer(o.n) { std::copy(o.p, o.p + o.n, p); }
+  buffer(buffer&& o) noexcept { steal(std::move(o)); }
   buffer& operator=(const buffer& o) {
     if (this != &o) {
       buffer t(o);
-      *this = std::move(t);
+      steal(std::move(t));
     }
     return *this;
   }
-  buffer& operator=(buffer&&) noexcept = default;
+  buffer& operator=(buffer&& o) noexcept {
+    if (this != &o) steal(std::move(o));
+    return *this;
+  }
+  T* get() const { return p; }
+
+ private:
+  void steal(buffer&& o) {
+    n = o.n;
+    if (o.p == o.small) {
+      heap.reset();
+      for (std::size_t i = 0; i < n; ++i) small[i] = std::move(o.small[i]);
+      p = n ? small : nullptr;
+    } else {
+      heap = std::move(o.heap);
+      p = heap.get();
+    }
+    o.p = nullptr;
+    o.n = 0;
+  }
 };
 
 }  // namespace detail
@@ -223,8 +332,8 @@ class xdense {
   const strides_type& strides() const { return strides_; }
   std::size_t dimension() const { return shape_.size(); }
   std::size_t size() const { return buf_.n; }
-  T* data() { return buf_.p.get(); }
-  const T* data() const { return buf_.p.get(); }
+  T* data() { return buf_.get(); }
+  const T* data() const { return buf_.get(); }
   std::ptrdiff_t data_offset() const { return 0; }
   T* begin() { return data(); }
   T* end() { return data() + size(); }

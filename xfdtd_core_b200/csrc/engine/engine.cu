@@ -181,6 +181,12 @@ struct xfd_engine {
   int2* d_xlayer = nullptr;  // per x plane: CPML layer code of the H / E layers
   size_t xlayer_slabs = (size_t)-1;  // slab count the table was built for
   HybMaps hmaps[2]{};     // tensor maps of the fused interior sweep (sweep 7), by input buffer
+  // Its box tiles as two lists: tiles no TFSF H pass reaches (swept by the
+  // form without TFSF code) and tiles one does (hyb_off[0..2]).
+  int4* d_hyb_tiles = nullptr;
+  size_t hyb_tiles_cap = 0;
+  int hyb_off[3] = {0, 0, 0};
+  long long hyb_key = -1;
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
   FvecMaps fvmaps[2]{};   // tensor maps of its two-nodes-per-thread interior form
   cudaGraphExec_t graph_exec = nullptr;
@@ -840,6 +846,56 @@ void march_tile_lists(const xfd_engine* e, std::vector<int4> lists[4]) {
       }
 }
 
+// The box tiles of sweep 7 split by whether a TFSF H pass reaches a node
+// that the tile's CTA computes: its own nodes over planes i_lo-1 .. i_hi-1,
+// the recomputed row j0-1 and column k0-1.  Without TFSF every tile is in the
+// first list.
+xfd_status build_hyb_tiles(xfd_engine* e) {
+  const MarchLayout ml = march_layout(e);
+  const long long key = (long long)e->slabs.size() * 1000003LL + e->march_ichunk * 4 +
+                        (e->have_tfsf ? 2 : 0) + (ml.box ? 1 : 0);
+  if (key == e->hyb_key) return XFD_OK;
+  std::vector<int4> clean, tf;
+  if (ml.box) {
+    const int ich = e->march_ichunk;
+    for (int gz = ml.lo[2]; gz < ml.hi[2]; ++gz)
+      for (int gy = ml.lo[1]; gy < ml.hi[1]; ++gy)
+        for (int gx = ml.lo[0]; gx < ml.hi[0]; ++gx) {
+          bool meets = false;
+          if (e->have_tfsf) {
+            const int lo[3] = {gz * ich - 1, gy * kMTJ - 1, gx * 32 - 1};
+            const int hi[3] = {gz * ich + ich, gy * kMTJ + kMTJ, gx * 32 + 32};
+            for (int c = 0; c < 3 && !meets; ++c)
+              for (int q = 0; q < e->tfsf_h.n[c] && !meets; ++q) {
+                const TfsfHPass& P = e->tfsf_h.pass[c][q];
+                bool ov = true;
+                for (int a = 0; a < 3; ++a) ov = ov && P.lo[a] < hi[a] && lo[a] < P.hi[a];
+                meets = ov;
+              }
+          }
+          (meets ? tf : clean).push_back(make_int4(0, gx, gy, gz));
+        }
+  }
+  std::vector<int4> all(clean);
+  all.insert(all.end(), tf.begin(), tf.end());
+  e->hyb_off[0] = 0;
+  e->hyb_off[1] = (int)clean.size();
+  e->hyb_off[2] = (int)all.size();
+  if (all.size() > e->hyb_tiles_cap) {
+    void* p = nullptr;
+    xfd_status st = dev_alloc(e, &p, all.size() * sizeof(int4));
+    if (st != XFD_OK) return st;
+    e->d_hyb_tiles = static_cast<int4*>(p);
+    e->hyb_tiles_cap = all.size();
+  }
+  if (!all.empty())
+    CUDA_TRY(e, cudaMemcpy(e->d_hyb_tiles, all.data(), all.size() * sizeof(int4),
+                           cudaMemcpyHostToDevice));
+  e->hyb_key = key;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
 xfd_status build_march_tiles(xfd_engine* e) {
   const long long key = (long long)e->slabs.size() * 1000003LL + e->march_ichunk * 16 +
                         (e->kernel_mode == 7 ? 8 : 0) + (e->march_shift ? 4 : 0) +
@@ -973,12 +1029,15 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
     hp.err = e->d_err;
     hp.m = e->hmaps[in];
     hp.ichunk = e->march_ichunk;
-    const dim3 g(ml.hi[0] - ml.lo[0], ml.hi[1] - ml.lo[1], ml.hi[2] - ml.lo[2]);
     const size_t hsm = HybGeom<T, kMTJ>::smem(HS);
-    if (e->have_tfsf)
-      k_hyb<T, kMTJ, HS, true><<<g, blk_m, hsm, e->side[0]>>>(hp);
-    else
-      k_hyb<T, kMTJ, HS, false><<<g, blk_m, hsm, e->side[0]>>>(hp);
+    const dim3 blk_h(32, kMTJ + 1, 1);  // kMTJ compute warps + the helper warp
+    // Tiles no TFSF H pass reaches, then (without TFSF none) those one does.
+    const int n_clean = e->hyb_off[1] - e->hyb_off[0];
+    const int n_tf = e->hyb_off[2] - e->hyb_off[1];
+    hp.tiles = e->d_hyb_tiles;
+    if (n_clean > 0) k_hyb<T, kMTJ, HS, false><<<n_clean, blk_h, hsm, e->side[0]>>>(hp);
+    hp.tiles = e->d_hyb_tiles + e->hyb_off[1];
+    if (n_tf > 0) k_hyb<T, kMTJ, HS, true><<<n_tf, blk_h, hsm, e->side[0]>>>(hp);
   }
   lists(mh, k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 1>,
         k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 2>,
@@ -1335,6 +1394,7 @@ xfd_status ensure_ready(xfd_engine* e) {
   }
   if (e->kernel_mode == 4 || e->kernel_mode == 7) {
     xfd_status st = build_march_tiles(e);
+    if (st == XFD_OK && e->kernel_mode == 7) st = build_hyb_tiles(e);
     if (st != XFD_OK) return st;
   }
   if (e->probes_dirty) {
@@ -2547,7 +2607,8 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
     const MarchLayout ml = march_layout(e);
     std::vector<int4> lists[4];
     march_tile_lists(e, lists);
-    int n = 1 + (ml.box ? 1 : 0) + 2;  // step counter, box, faces
+    int n = 1 + 2;  // step counter, faces
+    if (ml.box) n += (e->hyb_off[1] > e->hyb_off[0] ? 1 : 0) + (e->hyb_off[2] > e->hyb_off[1] ? 1 : 0);
     for (int q = 0; q < 4; ++q)
       if (!lists[q].empty()) n += 2;
     if (e->have_tfsf) n += 4;

@@ -7,7 +7,8 @@
 // has already advanced.  DRAM traffic per node is the compulsory one: six field
 // values read, six written, one uint16 class index read (50 B in FP32).
 //
-// A CTA of 32 x TJ threads owns a 32-node (k) x TJ-row (j) tile and marches
+// A CTA of 32 x TJ compute threads (plus a helper warp) owns a 32-node (k) x
+// TJ-row (j) tile and marches
 // along i over a chunk of planes; tiles are 128-byte aligned along k.  Per
 // plane i it stages, by TMA into a ring of S shared-memory stages:
 //   E of plane i over rows j0-1 .. j0+TJ and nodes k0-XA .. k0+31+XA,
@@ -19,9 +20,9 @@
 // src/include/updator/update_scheme.h:57-62, over BasicUpdator::updateH's
 // ranges, src/updator/basic_updator.cpp:23-36), with the TFSF H-face
 // corrections of TFSF3DCorrector::correctH (src/waveform_source/tfsf_corrector.cpp:205-232)
-// applied inline; warp 0 also recomputes H_x, H_z of row j0-1 and lane 0 of
-// each warp H_x, H_y of column k0-1 (nodes of the neighbouring tiles that the
-// E update reads).  After one CTA barrier it computes the three E components
+// applied inline; a helper warp issues the loads and recomputes H_x, H_z of row
+// j0-1 and H_x, H_y of column k0-1 (nodes of the neighbouring tiles that the E
+// update reads).  After one CTA barrier each thread computes the three E components
 // (eNext, update_scheme.h:26-31, over BasicUpdator3D::updateE's ranges,
 // src/updator/basic_updator_3d.cpp:38-69): the k-1 neighbours of H come by
 // warp shuffle, the j-1 neighbours from shared memory, the i-1 neighbours are
@@ -39,6 +40,8 @@
 // Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
 // the engine's error word, drains its loads in flight and returns.
 #pragma once
+
+#include <climits>
 
 #include "march_tma.cuh"
 
@@ -65,6 +68,9 @@ struct HybP {
   HybMaps m;
   int org[3];   // first (k tile, j tile, chunk) of the box
   int ichunk;
+  // Tile list: CTA b sweeps tile (tiles[b].y, tiles[b].z, tiles[b].w) (k tile,
+  // j tile, chunk); null: CTA (x, y, z) sweeps tile org + (x, y, z).
+  const int4* tiles;
 };
 
 template <typename T, int TJ>
@@ -92,22 +98,42 @@ struct HybGeom {
   __host__ __device__ static constexpr int smem(int S) { return S * STAGE + TB + HN + 8 * S; }
 };
 
-// Bit 4 c + s: TFSF H pass s of component c covers rows j and nodes k (its
-// i range is checked per plane).
-template <typename T>
-__device__ __forceinline__ uint32_t hyb_tfsf_mask(const HybP<T>& p, int j, int k) {
+// TFSF H passes that can touch node (j, k), and the planes where they do:
+// bit 4 c + s of m is pass s of component c; the x-normal passes touch one
+// plane each (px0, px1), the y- and z-normal ones the planes [ylo, yhi).
+struct TfsfSel {
   uint32_t m = 0;
+  int px0 = -1, px1 = -1, ylo = 0, yhi = 0;
+  __device__ __forceinline__ bool hits(int i) const {
+    return m != 0 && (i == px0 || i == px1 || (i >= ylo && i < yhi));
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ TfsfSel hyb_tfsf_sel(const HybP<T>& p, int j, int k) {
+  TfsfSel r;
+  r.ylo = INT_MAX;
+  r.yhi = INT_MIN;
   for (int c = 0; c < 3; ++c)
     for (int s = 0; s < p.tfh.n[c]; ++s) {
       const TfsfHPass& Q = p.tfh.pass[c][s];
-      if (j >= Q.lo[1] && j < Q.hi[1] && k >= Q.lo[2] && k < Q.hi[2]) m |= 1u << (4 * c + s);
+      if (j < Q.lo[1] || j >= Q.hi[1] || k < Q.lo[2] || k >= Q.hi[2]) continue;
+      r.m |= 1u << (4 * c + s);
+      if (Q.m == 0 && Q.hi[0] == Q.lo[0] + 1) {
+        if (r.px0 < 0 || r.px0 == Q.lo[0]) r.px0 = Q.lo[0];
+        else r.px1 = Q.lo[0];
+      } else {
+        r.ylo = min(r.ylo, Q.lo[0]);
+        r.yhi = max(r.yhi, Q.hi[0]);
+      }
     }
-  return m;
+  return r;
 }
 
 // TFSF H-face corrections of component c at node (i, j, k), in the
 // reference's pass order (correctTFSF, src/include/waveform_source/tfsf_corrector.h:89-229),
-// over the passes of `mask`.
+// over the passes of `mask`.  Called only inside a warp-uniform branch taken
+// by warps with a node on a TFSF face at this plane.
 template <typename T>
 __device__ __forceinline__ T hyb_tfsf_h(const HybP<T>& p, uint32_t mask, int c, int i, int j,
                                         int k, T h, long long t) {
@@ -127,22 +153,68 @@ __device__ __forceinline__ T hyb_tfsf_h(const HybP<T>& p, uint32_t mask, int c, 
   return h;
 }
 
+// The 12 (ca, cb) values of a class as vector loads: FP32 3 x float4, FP64
+// 6 x double2 (rows are 48 / 96 bytes, so 16-byte aligned), from shared memory
+// for the first NC classes, else from the table in global memory.
+template <typename T>
+struct ClassRow {
+  T v[12];
+  __device__ __forceinline__ void load(const T* r) {
+    if constexpr (sizeof(T) == 4) {
+      const float4* q = reinterpret_cast<const float4*>(r);
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        const float4 a = q[u];
+        v[4 * u] = a.x;
+        v[4 * u + 1] = a.y;
+        v[4 * u + 2] = a.z;
+        v[4 * u + 3] = a.w;
+      }
+    } else {
+      const double2* q = reinterpret_cast<const double2*>(r);
+#pragma unroll
+      for (int u = 0; u < 6; ++u) {
+        const double2 a = q[u];
+        v[2 * u] = a.x;
+        v[2 * u + 1] = a.y;
+      }
+    }
+  }
+};
+
+// CTA: TJ compute warps (warp w owns row j0 + w of the tile, lane = k - k0)
+// and one helper warp (threadIdx.y == TJ) that issues the TMA loads and
+// recomputes the H values of the neighbouring tiles that the E update reads:
+// H_x, H_z of row j0-1 (lane = k - k0) and H_x, H_y of column k0-1 (lanes
+// 0 .. TJ-1 = j - j0).  Compute warps carry no halo work, so no warp diverges.
 template <typename T, int TJ, int S, bool TF>
-__global__ void __launch_bounds__(32 * TJ) k_hyb(const __grid_constant__ HybP<T> p) {
+__global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
+    k_hyb(const __grid_constant__ HybP<T> p) {
   using G = HybGeom<T, TJ>;
   constexpr int TK = G::TK;
   extern __shared__ __align__(128) unsigned char smem[];
   const Lat L = p.L;
-  const int tk = threadIdx.x, tj = threadIdx.y, tid = tj * TK + tk;
+  const int tk = threadIdx.x, wj = threadIdx.y, tid = wj * TK + tk;
+  const bool helper = wj == TJ;
   if (__syncthreads_or(tid == 0 && (*(volatile int*)p.err & 2))) return;
-  const int k0 = (blockIdx.x + p.org[0]) * TK, j0 = (blockIdx.y + p.org[1]) * TJ;
-  const int i_lo = (blockIdx.z + p.org[2]) * p.ichunk;
+  int gx, gy, gz;
+  if (p.tiles) {
+    const int4 w = p.tiles[blockIdx.x];
+    gx = w.y;
+    gy = w.z;
+    gz = w.w;
+  } else {
+    gx = blockIdx.x + p.org[0];
+    gy = blockIdx.y + p.org[1];
+    gz = blockIdx.z + p.org[2];
+  }
+  const int k0 = gx * TK, j0 = gy * TJ;
+  const int i_lo = gz * p.ichunk;
   const int i_hi = min(i_lo + p.ichunk, L.nx);
   const int n = i_hi - i_lo;  // planes updated; staged: i_lo-1 .. i_hi (n + 2)
-  const int k = k0 + tk, j = j0 + tj;
 
-  T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);                  // [NC][12]
-  T* sN = reinterpret_cast<T*>(smem + S * G::STAGE + G::TB);          // new H
+  T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);          // [NC][12]
+  T* sN = reinterpret_cast<T*>(smem + S * G::STAGE + G::TB);  // new H
   StageRing ring;
   ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::TB + G::HN);
   auto sE = [&](int s, int c) {
@@ -158,6 +230,7 @@ __global__ void __launch_bounds__(32 * TJ) k_hyb(const __grid_constant__ HybP<T>
   auto nrow = [&](int b, int w) { return sN + (b * 2 + w) * (G::RH * TK); };
   auto ncol = [&](int b, int w) { return sN + 4 * (G::RH * TK) + (b * 2 + w) * TJ; };
   const int n_staged = n + 2;
+  const bool issuer = helper && tk == 0;
   auto issue = [&](int u) {  // plane i_lo - 1 + u into stage u % S
     const int s = u % S, i = i_lo - 1 + u;
     uint64_t* bar = &ring.bars[s];
@@ -172,66 +245,74 @@ __global__ void __launch_bounds__(32 * TJ) k_hyb(const __grid_constant__ HybP<T>
       tma_load_3d(base + G::C_OFF, &p.m.cls, k0 - 8, j0 - 1, i, bar);
     }
   };
-  if (tid == 0) {
+  if (issuer) {
     for (int s = 0; s < S; ++s) mbar_init(&ring.bars[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0)
+  if (issuer)
     for (int u = 0; u < S && u < n_staged; ++u) issue(u);
   for (int u = 0; u < S && u < n_staged; ++u) ring.pending |= 1u << (u % S);
-  for (int x = tid; x < min(p.n_classes, G::NC) * 12; x += 32 * TJ) sT[x] = p.tab[x];
+  for (int x = tid; x < min(p.n_classes, G::NC) * 12; x += 32 * (TJ + 1)) sT[x] = p.tab[x];
 
   const long long t = TF ? *p.step : 0;
   const long long PS = (long long)L.NY * L.KP;
+  // Node of this thread: compute warps own (j0 + wj, k0 + tk); the helper
+  // warp's lane tk handles row-halo node (j0-1, k0+tk) and, for tk < TJ,
+  // column-halo node (j0+tk, k0-1).
+  const int j = helper ? j0 - 1 : j0 + wj, k = k0 + tk;
   const long long row = (long long)j * L.KP + k;
   const T fhj = p.fh[1][j], fhk = p.fh[2][k];
-  const T fej = p.fe[1][j], fek = p.fe[2][k];
-  // Halo duties: warp 0 recomputes row j0-1 (node k), lane 0 of warp tj
-  // column k0-1 (node j).
-  const bool row_halo = tj == 0;
-  const bool col_halo = tk == 0;
-  const T fhj_r = row_halo ? p.fh[1][j0 - 1] : T(0);
-  const T fhk_c = col_halo ? p.fh[2][k0 - 1] : T(0);
-  // Offsets of this thread's node in the staged boxes.
-  const int eq = (tj + 1) * G::WE + tk + G::XA;
-  const int hq = (tj + 1) * G::WH + tk + G::XA;
-  const int cq = (tj + 1) * G::WC + tk + 8;
-  // Row halo node (j0-1, k): row 0 of the boxes; column halo (j, k0-1).
-  const int eq_r = tk + G::XA, hq_r = tk + G::XA, cq_r = tk + 8;
-  const int eq_c = (tj + 1) * G::WE + G::XA - 1, hq_c = (tj + 1) * G::WH + G::XA - 1,
-            cq_c = (tj + 1) * G::WC + 7;
-  // TFSF H passes that can meet this thread's node, row halo and column halo.
-  const uint32_t tm = TF ? hyb_tfsf_mask(p, j, k) : 0u;
-  const uint32_t tm_r = TF && row_halo ? hyb_tfsf_mask(p, j0 - 1, k) : 0u;
-  const uint32_t tm_c = TF && col_halo ? hyb_tfsf_mask(p, j, k0 - 1) : 0u;
+  const T fej = helper ? T(0) : p.fe[1][j], fek = p.fe[2][k];
+  const bool col = helper && tk < TJ;
+  const int jc = j0 + tk;  // column-halo row (helper lanes tk < TJ)
+  const T fhj_c = col ? p.fh[1][jc] : T(0);
+  const T fhk_c = p.fh[2][k0 - 1];
+  // Offsets in the staged boxes: own / row-halo node, column-halo node.
+  const int wr = helper ? 0 : wj + 1;  // box row of j
+  const int eq = wr * G::WE + tk + G::XA;
+  const int hq = wr * G::WH + tk + G::XA;
+  const int cq = wr * G::WC + tk + 8;
+  const int eq_c = (tk + 1) * G::WE + G::XA - 1, hq_c = (tk + 1) * G::WH + G::XA - 1,
+            cq_c = (tk + 1) * G::WC + 7;
+  T* const o_ex = p.out[0] + row;
+  T* const o_ey = p.out[1] + row;
+  T* const o_ez = p.out[2] + row;
+  T* const o_hx = p.out[3] + row;
+  T* const o_hy = p.out[4] + row;
+  T* const o_hz = p.out[5] + row;
+  TfsfSel ts, ts_c;  // TFSF passes of this lane's node and column-halo node
+  if (TF) ts = hyb_tfsf_sel(p, j, k);
+  if (TF && col) ts_c = hyb_tfsf_sel(p, jc, k0 - 1);
   __syncthreads();  // class rows staged
 
-  auto coef = [&](int cl, int x) -> T {
-    return cl < G::NC ? sT[cl * 12 + x] : p.tab[(size_t)cl * 12 + x];
-  };
+  auto row_of = [&](int cl) { return cl < G::NC ? sT + cl * 12 : p.tab + (size_t)cl * 12; };
 
   bool ok = true;
-  // ---- plane i_lo - 1: H_y, H_z of this node (the E update's i-1 neighbours)
+  // ---- plane i_lo - 1: H_y, H_z of the compute warps' nodes (the E update's
+  // i-1 neighbours)
   T hy_prev = T(0), hz_prev = T(0);
   if (n > 0) {
     ok = ring.wait(0);
     if (ok) ok = ring.wait(1 % S);
-    if (ok) {
+    if (ok && !helper) {
       const int i = i_lo - 1;
       const T fhi = p.fh[0][i];
       const T* E0 = sE(0, 0);
       const T* E1 = sE(0, 1);
       const T* E2 = sE(0, 2);
-      const int cl = sC(0)[cq];
+      ClassRow<T> c;
+      c.load(row_of(sC(0)[cq]));
       const T ex = E0[eq], ey = E1[eq], ez = E2[eq];
-      const T ex_k = E0[eq + 1], ex_j = E0[eq + G::WE];
-      const T ez_n = sE(1 % S, 2)[eq], ey_n = sE(1 % S, 1)[eq];
-      T hy = coef(cl, 8) * sH(0, 1)[hq] + coef(cl, 9) * (fhi * (ez_n - ez) - fhk * (ex_k - ex));
-      T hz = coef(cl, 10) * sH(0, 2)[hq] + coef(cl, 11) * (fhj * (ex_j - ex) - fhi * (ey_n - ey));
-      if (TF) {
-        hy = hyb_tfsf_h(p, tm, 1, i, j, k, hy, t);
-        hz = hyb_tfsf_h(p, tm, 2, i, j, k, hz, t);
+      T hy = c.v[8] * sH(0, 1)[hq] +
+             c.v[9] * (fhi * (sE(1 % S, 2)[eq] - ez) - fhk * (E0[eq + 1] - ex));
+      T hz = c.v[10] * sH(0, 2)[hq] +
+             c.v[11] * (fhj * (E0[eq + G::WE] - ex) - fhi * (sE(1 % S, 1)[eq] - ey));
+      if (TF && __any_sync(0xffffffffu, ts.hits(i))) {
+        if (ts.hits(i)) {
+          hy = hyb_tfsf_h(p, ts.m, 1, i, j, k, hy, t);
+          hz = hyb_tfsf_h(p, ts.m, 2, i, j, k, hz, t);
+        }
       }
       hy_prev = hy;
       hz_prev = hz;
@@ -242,11 +323,9 @@ __global__ void __launch_bounds__(32 * TJ) k_hyb(const __grid_constant__ HybP<T>
     const int i = i_lo + q;
     const int sc = (q + 1) % S, sn = (q + 2) % S;
     if (ok) ok = ring.wait(sn);  // E of plane i+1
-    // ---------------------------------------------------------- H(i)
-    T hx = T(0), hy = T(0), hz = T(0);
-    T ex = T(0), ey = T(0), ez = T(0);
-    int cl = 0;
     const int b = q & 1;
+    T hx = T(0), hy = T(0), hz = T(0), ex = T(0), ey = T(0), ez = T(0);
+    ClassRow<T> c;
     if (ok) {
       const T fhi = p.fh[0][i];
       const T* E0 = sE(sc, 0);
@@ -254,86 +333,78 @@ __global__ void __launch_bounds__(32 * TJ) k_hyb(const __grid_constant__ HybP<T>
       const T* E2 = sE(sc, 2);
       const T* N1 = sE(sn, 1);
       const T* N2 = sE(sn, 2);
-      cl = sC(sc)[cq];
+      // H_x, H_z of this lane's node (own node, or row-halo node for the helper)
+      c.load(row_of(sC(sc)[cq]));
       ex = E0[eq];
       ey = E1[eq];
       ez = E2[eq];
-      const T dEy_k = E1[eq + 1] - ey, dEz_j = E2[eq + G::WE] - ez;
-      const T dEz_i = N2[eq] - ez, dEx_k = E0[eq + 1] - ex;
-      const T dEx_j = E0[eq + G::WE] - ex, dEy_i = N1[eq] - ey;
-      hx = coef(cl, 6) * sH(sc, 0)[hq] + coef(cl, 7) * (fhk * dEy_k - fhj * dEz_j);
-      hy = coef(cl, 8) * sH(sc, 1)[hq] + coef(cl, 9) * (fhi * dEz_i - fhk * dEx_k);
-      hz = coef(cl, 10) * sH(sc, 2)[hq] + coef(cl, 11) * (fhj * dEx_j - fhi * dEy_i);
-      if (TF && tm) {
-        hx = hyb_tfsf_h(p, tm, 0, i, j, k, hx, t);
-        hy = hyb_tfsf_h(p, tm, 1, i, j, k, hy, t);
-        hz = hyb_tfsf_h(p, tm, 2, i, j, k, hz, t);
-      }
-      const long long o = i * PS + row;
-      p.out[3][o] = hx;
-      p.out[4][o] = hy;
-      p.out[5][o] = hz;
-      nrow(b, 0)[(tj + 1) * TK + tk] = hx;
-      nrow(b, 1)[(tj + 1) * TK + tk] = hz;
-      if (row_halo) {  // H_x, H_z at (i, j0-1, k)
-        const int cr = sC(sc)[cq_r];
-        const T ex_r = E0[eq_r], ey_r = E1[eq_r], ez_r = E2[eq_r];
-        T hxr = coef(cr, 6) * sH(sc, 0)[hq_r] +
-                coef(cr, 7) * (fhk * (E1[eq_r + 1] - ey_r) - fhj_r * (E2[eq_r + G::WE] - ez_r));
-        T hzr = coef(cr, 10) * sH(sc, 2)[hq_r] +
-                coef(cr, 11) * (fhj_r * (E0[eq_r + G::WE] - ex_r) - fhi * (N1[eq_r] - ey_r));
-        if (TF && tm_r) {
-          hxr = hyb_tfsf_h(p, tm_r, 0, i, j0 - 1, k, hxr, t);
-          hzr = hyb_tfsf_h(p, tm_r, 2, i, j0 - 1, k, hzr, t);
+      hx = c.v[6] * sH(sc, 0)[hq] +
+           c.v[7] * (fhk * (E1[eq + 1] - ey) - fhj * (E2[eq + G::WE] - ez));
+      hz = c.v[10] * sH(sc, 2)[hq] +
+           c.v[11] * (fhj * (E0[eq + G::WE] - ex) - fhi * (N1[eq] - ey));
+      if (!helper)
+        hy = c.v[8] * sH(sc, 1)[hq] +
+             c.v[9] * (fhi * (N2[eq] - ez) - fhk * (E0[eq + 1] - ex));
+      if (TF && __any_sync(0xffffffffu, ts.hits(i))) {
+        if (ts.hits(i)) {
+          hx = hyb_tfsf_h(p, ts.m, 0, i, j, k, hx, t);
+          hz = hyb_tfsf_h(p, ts.m, 2, i, j, k, hz, t);
+          if (!helper) hy = hyb_tfsf_h(p, ts.m, 1, i, j, k, hy, t);
         }
-        nrow(b, 0)[tk] = hxr;
-        nrow(b, 1)[tk] = hzr;
       }
-      if (col_halo) {  // H_x, H_y at (i, j, k0-1)
-        const int cc = sC(sc)[cq_c];
+      nrow(b, 0)[wr * TK + tk] = hx;
+      nrow(b, 1)[wr * TK + tk] = hz;
+      if (!helper) {
+        const long long o = i * PS;
+        o_hx[o] = hx;
+        o_hy[o] = hy;
+        o_hz[o] = hz;
+      } else if (col) {  // H_x, H_y at (i, j0 + tk, k0-1)
+        ClassRow<T> cc;
+        cc.load(row_of(sC(sc)[cq_c]));
         const T ex_c = E0[eq_c], ey_c = E1[eq_c], ez_c = E2[eq_c];
-        T hxc = coef(cc, 6) * sH(sc, 0)[hq_c] +
-                coef(cc, 7) * (fhk_c * (E1[eq_c + 1] - ey_c) - fhj * (E2[eq_c + G::WE] - ez_c));
-        T hyc = coef(cc, 8) * sH(sc, 1)[hq_c] +
-                coef(cc, 9) * (fhi * (N2[eq_c] - ez_c) - fhk_c * (E0[eq_c + 1] - ex_c));
-        if (TF && tm_c) {
-          hxc = hyb_tfsf_h(p, tm_c, 0, i, j, k0 - 1, hxc, t);
-          hyc = hyb_tfsf_h(p, tm_c, 1, i, j, k0 - 1, hyc, t);
+        T hxc = cc.v[6] * sH(sc, 0)[hq_c] +
+                cc.v[7] * (fhk_c * (E1[eq_c + 1] - ey_c) - fhj_c * (E2[eq_c + G::WE] - ez_c));
+        T hyc = cc.v[8] * sH(sc, 1)[hq_c] +
+                cc.v[9] * (fhi * (N2[eq_c] - ez_c) - fhk_c * (E0[eq_c + 1] - ex_c));
+        if (TF && ts_c.hits(i)) {
+          hxc = hyb_tfsf_h(p, ts_c.m, 0, i, jc, k0 - 1, hxc, t);
+          hyc = hyb_tfsf_h(p, ts_c.m, 1, i, jc, k0 - 1, hyc, t);
         }
-        ncol(b, 0)[tj] = hxc;
-        ncol(b, 1)[tj] = hyc;
+        ncol(b, 0)[tk] = hxc;
+        ncol(b, 1)[tk] = hyc;
       }
     }
     if (__syncthreads_or(!ok)) {
       ok = false;
       break;
     }
-    // Every thread is past plane i-1 (stage q % S): refill it.
-    if (q + S < n_staged) {
-      if (tid == 0) {
-        fence_proxy_async();
-        issue(q + S);
+    // The stage of plane i (u = q + 1) is read only before this barrier (the
+    // E update below works from registers and the new-H buffers), so it is
+    // free now -- and at q = 0 so is that of plane i_lo - 1 (u = 0): refill
+    // them with the planes S further on.
+    for (int u = q == 0 ? 0 : q + 1; u <= q + 1; ++u) {
+      if (u + S < n_staged) {
+        if (issuer) {
+          fence_proxy_async();
+          issue(u + S);
+        }
+        ring.pending |= 1u << (u % S);
       }
-      ring.pending |= 1u << (q % S);
     }
     // ---------------------------------------------------------- E(i)
-    {
+    if (!helper) {
       const T fei = p.fe[0][i];
-      const T hy_k = tk > 0 ? T(0) : ncol(b, 1)[tj];
-      const T hx_k = tk > 0 ? T(0) : ncol(b, 0)[tj];
       const T hy_s = __shfl_up_sync(0xffffffffu, hy, 1);
       const T hx_s = __shfl_up_sync(0xffffffffu, hx, 1);
-      const T hym = tk > 0 ? hy_s : hy_k;
-      const T hxm_k = tk > 0 ? hx_s : hx_k;
-      const T hzm_j = nrow(b, 1)[tj * TK + tk];
-      const T hxm_j = nrow(b, 0)[tj * TK + tk];
-      const T ex_n = coef(cl, 0) * ex + coef(cl, 1) * (fej * (hz - hzm_j) - fek * (hy - hym));
-      const T ey_n = coef(cl, 2) * ey + coef(cl, 3) * (fek * (hx - hxm_k) - fei * (hz - hz_prev));
-      const T ez_n = coef(cl, 4) * ez + coef(cl, 5) * (fei * (hy - hy_prev) - fej * (hx - hxm_j));
-      const long long o = i * PS + row;
-      p.out[0][o] = ex_n;
-      p.out[1][o] = ey_n;
-      p.out[2][o] = ez_n;
+      const T hym = tk > 0 ? hy_s : ncol(b, 1)[wj];
+      const T hxm_k = tk > 0 ? hx_s : ncol(b, 0)[wj];
+      const T hzm_j = nrow(b, 1)[wj * TK + tk];
+      const T hxm_j = nrow(b, 0)[wj * TK + tk];
+      const long long o = i * PS;
+      o_ex[o] = c.v[0] * ex + c.v[1] * (fej * (hz - hzm_j) - fek * (hy - hym));
+      o_ey[o] = c.v[2] * ey + c.v[3] * (fek * (hx - hxm_k) - fei * (hz - hz_prev));
+      o_ez[o] = c.v[4] * ez + c.v[5] * (fei * (hy - hy_prev) - fej * (hx - hxm_j));
       hy_prev = hy;
       hz_prev = hz;
     }

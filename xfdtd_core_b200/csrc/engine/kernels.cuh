@@ -221,16 +221,18 @@ __host__ __device__ __forceinline__ long long edge_nodes(const Lat& L) {
   return (long long)(L.nx + 1) * (L.ny + 1) + (long long)(L.nx + 1) * L.nz;
 }
 
+// Face node t (< 2^31: two lattice faces) as (i, j, k), 32-bit decoding.
 __device__ __forceinline__ void edge_node(const Lat& L, long long t, int& i, int& j, int& k) {
-  const long long fa = (long long)(L.nx + 1) * (L.ny + 1);
-  if (t < fa) {
-    i = (int)(t / (L.ny + 1));
-    j = (int)(t - (long long)i * (L.ny + 1));
+  const unsigned fa = (unsigned)((L.nx + 1) * (L.ny + 1));
+  unsigned u = (unsigned)t;
+  if (u < fa) {
+    i = (int)(u / (unsigned)(L.ny + 1));
+    j = (int)(u - (unsigned)i * (unsigned)(L.ny + 1));
     k = L.nz;
   } else {
-    t -= fa;
-    i = (int)(t / L.nz);
-    k = (int)(t - (long long)i * L.nz);
+    u -= fa;
+    i = (int)(u / (unsigned)L.nz);
+    k = (int)(u - (unsigned)i * (unsigned)L.nz);
     j = L.ny;
   }
 }
@@ -367,8 +369,9 @@ __device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, 
   int q = 0;
   while (q + 1 < g.n && tid >= g.pass[q + 1].begin) ++q;
   const TfsfPassD& P = g.pass[q];
-  long long r = tid - P.begin;
-  const int e2 = P.e[2] - P.s[2], e1 = P.e[1] - P.s[1];
+  // A pass covers one face: far fewer than 2^31 nodes, so 32-bit decoding.
+  unsigned r = (unsigned)(tid - P.begin);
+  const unsigned e2 = (unsigned)(P.e[2] - P.s[2]), e1 = (unsigned)(P.e[1] - P.s[1]);
   const int k = P.s[2] + (int)(r % e2);
   r /= e2;
   const int j = P.s[1] + (int)(r % e1);
@@ -641,10 +644,11 @@ __global__ void k_nf2ff_sample(Nf2ffD nf, Lat L, T* const* fields, const long lo
   if (p >= nf.P) return;
   int d = 0;
   while (d < 5 && p >= nf.begin[d + 1]) ++d;
-  long long r = p - nf.begin[d];
+  // A face holds far fewer than 2^31 points: 32-bit decoding.
+  unsigned r = (unsigned)(p - nf.begin[d]);
   const int* s = nf.s[d];
   const int* e = nf.e[d];
-  const int e2 = e[2] - s[2], e1 = e[1] - s[1];
+  const unsigned e2 = (unsigned)(e[2] - s[2]), e1 = (unsigned)(e[1] - s[1]);
   const int k = s[2] + (int)(r % e2);
   r /= e2;
   const int j = s[1] + (int)(r % e1);
@@ -738,12 +742,22 @@ __global__ void k_movie(MovieD mv, Lat L, T* const* fields, const long long* ste
   if (tid >= n) return;
   const long long frame = *step / mv.interval;
   if (frame >= mv.max_frames) return;
-  long long r = tid;
-  const int k = mv.s[2] + (int)(r % e2);
-  r /= e2;
-  const int j = mv.s[1] + (int)(r % e1);
-  r /= e1;
-  const int i = mv.s[0] + (int)r;
+  int i, j, k;
+  if (n < (1LL << 31)) {  // 32-bit decoding (64-bit division is emulated)
+    unsigned r = (unsigned)tid;
+    k = mv.s[2] + (int)(r % (unsigned)e2);
+    r /= (unsigned)e2;
+    j = mv.s[1] + (int)(r % (unsigned)e1);
+    r /= (unsigned)e1;
+    i = mv.s[0] + (int)r;
+  } else {
+    long long r = tid;
+    k = mv.s[2] + (int)(r % e2);
+    r /= e2;
+    j = mv.s[1] + (int)(r % e1);
+    r /= e1;
+    i = mv.s[0] + (int)r;
+  }
   T* out = static_cast<T*>(mv.store) + frame * n + tid;
   *out = fields[mv.field][lat_index(L, i, j, k)];
 }
@@ -841,10 +855,10 @@ __global__ void k_nf2ff_td(Nf2ffTdD td, Lat L, T* const* fields, const long long
   if (p >= td.P) return;
   int d = 0;
   while (d < 5 && p >= td.begin[d + 1]) ++d;
-  long long r = p - td.begin[d];
+  unsigned r = (unsigned)(p - td.begin[d]);  // one face: 32-bit decoding
   const int* s = td.s[d];
   const int* e = td.e[d];
-  const int e2 = e[2] - s[2], e1 = e[1] - s[1];
+  const unsigned e2 = (unsigned)(e[2] - s[2]), e1 = (unsigned)(e[1] - s[1]);
   const int k = s[2] + (int)(r % e2);
   r /= e2;
   const int j = s[1] + (int)(r % e1);
