@@ -71,8 +71,18 @@ xfd_status state_copy(xfd_engine* e, xfd_engine::Ckpt& c, bool save) {
                                 cudaMemcpyDeviceToDevice, e->stream));
     off += (r.bytes + 255) / 256 * 256;
   }
-  if (save) c.step = e->host_step;
-  else e->host_step = c.step;
+  if (save) {
+    c.step = e->host_step;
+  } else {
+    e->host_step = c.step;
+    // Ping-pong sweeps: the other buffer gets the same fields, so that nodes
+    // no kernel writes hold equal values in both (the sweeps then skip them).
+    if (is_pingpong(e))
+      for (int q = 0; q < 6; ++q)
+        CUDA_TRY(e, cudaMemcpyAsync(e->fbuf[1 - e->cur][q], e->fbuf[e->cur][q],
+                                    (size_t)e->n_lat * e->wsize, cudaMemcpyDeviceToDevice,
+                                    e->stream));
+  }
   return XFD_OK;
 }
 

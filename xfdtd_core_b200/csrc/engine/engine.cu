@@ -1043,7 +1043,23 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
         k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 2>,
         k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 4>,
         k_march_h_tma_list<T, kMTJ, 32, MS, true, false, 7>);
-  if (c == cudaSuccess) k_edge_pp<T, false><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in);
+  // Lumped elements, inductors and overrides add to their nodes after the
+  // sweep: if one sits on a lattice face k = nz or j = ny, those faces are
+  // carried over in full.
+  bool face_targets = false;
+  auto on_face = [&](long long id) {
+    const long long jk = id % ((long long)e->L.NY * e->L.KP);
+    const int j = (int)(jk / e->L.KP), k = (int)(jk % e->L.KP);
+    return j == e->L.ny || k == e->L.nz;
+  };
+  for (const auto& l : e->lumped_h)
+    for (long long id : l.node) face_targets = face_targets || on_face(id);
+  for (const auto& l : e->ind_h)
+    for (long long id : l.node) face_targets = face_targets || on_face(id);
+  for (size_t q = 0; q < e->ovr_node.size(); q += 3)
+    face_targets = face_targets || e->ovr_node[q + 1] == e->L.ny || e->ovr_node[q + 2] == e->L.nz;
+  if (c == cudaSuccess)
+    k_edge_pp<T, false><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in, face_targets);
   join(1, kSides - 1);
   if (e->have_tfsf && c == cudaSuccess) {
     Box3 skip{};
@@ -1069,7 +1085,8 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
         k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 2>,
         k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 4>,
         k_march_e_tma_list<T, kMTJ, 32, MS, true, false, 7>);
-  if (c == cudaSuccess) k_edge_pp<T, true><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in);
+  if (c == cudaSuccess)
+    k_edge_pp<T, true><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in, face_targets);
   join(1, kSides - 1);
   if (c != cudaSuccess) return c;
   return cudaGetLastError();
@@ -2456,6 +2473,14 @@ xfd_status xfd_upload_fields(xfd_engine* e, const void* const fields[6]) {
         copy_parms(e, c, e->fbuf[e->cur][c], const_cast<void*>(fields[c]), true, e->wsize);
     CUDA_TRY(e, cudaMemcpy3DAsync(&p, e->stream));
   }
+  // Ping-pong sweeps: the other buffer gets the same fields, so that nodes no
+  // kernel writes (PEC walls, lattice-face nodes outside the CPML) hold equal
+  // values in both and the sweeps need not carry them over every step.
+  if (is_pingpong(e))
+    for (int c = 0; c < 6; ++c)
+      CUDA_TRY(e, cudaMemcpyAsync(e->fbuf[1 - e->cur][c], e->fbuf[e->cur][c],
+                                  (size_t)e->n_lat * e->wsize, cudaMemcpyDeviceToDevice,
+                                  e->stream));
   CUDA_TRY(e, cudaStreamSynchronize(e->stream));
   return XFD_OK;
 }
@@ -2557,8 +2582,16 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 0 || value > 7)
       return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
     const int before = psi_h_buf(e);
+    const bool was_pp = is_pingpong(e);
     e->kernel_mode = (int)value;
     const int after = psi_h_buf(e);
+    if (!was_pp && is_pingpong(e)) {  // both buffers must agree on untouched nodes
+      CUDA_TRY(e, cudaSetDevice(e->device));
+      for (int c = 0; c < 6; ++c)
+        CUDA_TRY(e, cudaMemcpyAsync(e->fbuf[1 - e->cur][c], e->fbuf[e->cur][c],
+                                    (size_t)e->n_lat * e->wsize, cudaMemcpyDeviceToDevice,
+                                    e->stream));
+    }
     if (before != after) {  // the next step reads the H psi from another buffer
       CUDA_TRY(e, cudaSetDevice(e->device));
       for (const auto& S : e->slabs) {

@@ -269,16 +269,20 @@ __global__ void __launch_bounds__(256) k_edge_e(const __grid_constant__ YeeP<T> 
   edge_update<T, true>(p, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// Ping-pong forms (sweep 7): every face node is written to p.f from the old
-// fields in `rd` -- its CPML-corrected value, or the old value carried over
-// when it lies in no layer -- so that the output buffer is complete.
+// Ping-pong forms (sweep 7): a face node in a CPML layer is written to p.f
+// from the old fields in `rd`.  A node in no layer never changes, and the
+// engine keeps both buffers equal on such nodes (uploads and restored states
+// fill both), so it is skipped as in the in-place form -- unless `copy_all`
+// (a lumped element, inductor or coefficient override adds to some face
+// node after the sweep), when every face node is carried over.
 template <typename T, bool E>
 __global__ void __launch_bounds__(256) k_edge_pp(const __grid_constant__ YeeP<T> p,
-                                                 T* const* rd) {
+                                                 T* const* rd, bool copy_all) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= edge_nodes(p.L)) return;
   int i, j, k;
   edge_node(p.L, t, i, j, k);
+  if (!copy_all && !in_some_layer(p, i, j, k, E)) return;
   if (E)
     update_e_node(p, i, j, k, rd);
   else
@@ -328,22 +332,21 @@ struct TfsfGroupD {
 
 __device__ __forceinline__ double tfsf_incident(const TfsfD& tf, bool inc_e, int comp,
                                                 long long t, const int x[3], int* err) {
-  int r[3] = {x[0] - tf.bs[0], x[1] - tf.bs[1], x[2] - tf.bs[2]};
+  // Per axis d: the offset from the box start, one further along the
+  // component axis (E incident) or along the other two (H incident); the
+  // projection table is the half-step one along the component axis for E and
+  // the integer one for H, and the other way round across.  Written with
+  // selects so that nothing is indexed by a run-time axis (no local memory).
   double parts[3];
-  double proj;
-  if (inc_e) {
-    r[comp] += 1;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) parts[d] = (d == comp) ? tf.p_half[d][r[d]] : tf.p_int[d][r[d]];
-    proj = parts[0] + parts[1] + parts[2];
-  } else {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      if (d != comp) r[d] += 1;
-      parts[d] = (d == comp) ? tf.p_int[d][r[d]] : tf.p_half[d][r[d]];
-    }
-    proj = parts[0] + parts[1] + parts[2] - 0.5;
+  for (int d = 0; d < 3; ++d) {
+    const bool along = d == comp;
+    const int r = x[d] - tf.bs[d] + ((inc_e ? along : !along) ? 1 : 0);
+    const bool half = inc_e ? along : !along;
+    parts[d] = half ? tf.p_half[d][r] : tf.p_int[d][r];
   }
+  const double proj = inc_e ? parts[0] + parts[1] + parts[2]
+                            : parts[0] + parts[1] + parts[2] - 0.5;
   long long idx = (long long)proj;
   const double w = proj - (double)idx;
   const int len = inc_e ? tf.aux : tf.aux - 1;
@@ -402,7 +405,8 @@ __device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, 
 }
 
 template <typename T>
-__global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const long long* step,
+__global__ void k_tfsf(const __grid_constant__ TfsfD tf, const __grid_constant__ TfsfGroupD g,
+                       Lat L, T* const* fields, const long long* step,
                        int* err) {
   tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
@@ -410,7 +414,8 @@ __global__ void k_tfsf(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields, const lo
 // The passes of one group on the nodes outside `skip` (sweep 7: the fused
 // box kernel applies the H passes of its own nodes inline).
 template <typename T>
-__global__ void k_tfsf_outside(TfsfD tf, TfsfGroupD g, Lat L, T* const* fields,
+__global__ void k_tfsf_outside(const __grid_constant__ TfsfD tf,
+                               const __grid_constant__ TfsfGroupD g, Lat L, T* const* fields,
                                const long long* step, int* err, Box3 skip) {
   tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x,
                skip);
@@ -639,7 +644,8 @@ __device__ double surf_h(T* const* f, const Lat& L, int m, int comp, int i, int 
 }
 
 template <typename T>
-__global__ void k_nf2ff_sample(Nf2ffD nf, Lat L, T* const* fields, const long long* step) {
+__global__ void k_nf2ff_sample(const __grid_constant__ Nf2ffD nf, Lat L, T* const* fields,
+                               const long long* step) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nf.P) return;
   int d = 0;
@@ -735,7 +741,8 @@ struct MovieD {
 };
 
 template <typename T>
-__global__ void k_movie(MovieD mv, Lat L, T* const* fields, const long long* step) {
+__global__ void k_movie(const __grid_constant__ MovieD mv, Lat L, T* const* fields,
+                        const long long* step) {
   const int e2 = mv.e[2] - mv.s[2], e1 = mv.e[1] - mv.s[1], e0 = mv.e[0] - mv.s[0];
   const long long n = (long long)e0 * e1 * e2;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -849,7 +856,8 @@ __device__ __forceinline__ void td_add(double* row, long long n_bins, double x, 
 }
 
 template <typename T>
-__global__ void k_nf2ff_td(Nf2ffTdD td, Lat L, T* const* fields, const long long* step,
+__global__ void k_nf2ff_td(const __grid_constant__ Nf2ffTdD td, Lat L, T* const* fields,
+                           const long long* step,
                            int* err) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= td.P) return;
@@ -904,7 +912,8 @@ struct ProbeD {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_probes(ProbeD pr, T* const* fields, const long long* step) {
+__global__ void __launch_bounds__(256) k_probes(const __grid_constant__ ProbeD pr, T* const* fields,
+                                                const long long* step) {
   const int q = blockIdx.x;
   double acc = 0.0;
   for (long long e = pr.begin[q] + threadIdx.x; e < pr.begin[q + 1]; e += blockDim.x)
