@@ -22,6 +22,14 @@ def dispersive_small(steps=120, **kw):
     return S.dispersive_spheres(**base)
 
 
+def dispersive_stable_small(steps=120, **kw):
+    """The dispersive scene with its Drude and Lorentz spheres only: the same
+    modified-Lorentz ADE storage and kernels, without the Debye sphere whose
+    modified-Lorentz form is unstable in the reference's scheme."""
+    kw.setdefault("media", ("drude", "lorentz"))
+    return dispersive_small(steps=steps, **kw)
+
+
 def voxels_small(steps=120, **kw):
     """The adjoint scene's geometry at 40 x 40 x 32: slab, 8 x 8 x 3 design
     voxels, normal-incidence TFSF, Ez patch objective."""
@@ -84,4 +92,5 @@ def microstrip_small(steps=150, **kw):
 
 
 ALL = {"sphere": sphere_small, "boxes": boxes_small, "dispersive": dispersive_small,
-       "voxels": voxels_small, "lumped": lumped_small, "microstrip": microstrip_small}
+       "dispersive_stable": dispersive_stable_small, "voxels": voxels_small,
+       "lumped": lumped_small, "microstrip": microstrip_small}

@@ -1,0 +1,137 @@
+"""Parity and FP32 error budgets at the benchmark sizes.
+
+* C2, the dielectric-boxes scene at its full 256^3 (12-cell graded CPML, 64
+  random boxes, z-directed current source): the FP64 engine against the
+  oracle after 200 steps, every field component within 1e-12 relative L2.
+* C3, the dispersive scene at its full 384^3 (three ADE spheres, oblique TFSF,
+  32-frequency NF2FF on a Huygens box 5 cells inside the 10-cell CPML): the
+  FP64 engine against the oracle from the same random initial fields (so that
+  every kernel -- Yee, CPML, ADE on all three media, TFSF, NF2FF surface DFT
+  at 32 frequencies -- works on non-trivial values from the first step), 12
+  steps; fields and NF2FF surface currents within 1e-12.
+* The FP32 form over the full run length at full size, against the FP64
+  engine on the same GPU (which the two tests above and the scene tests pin
+  to the oracle within 1e-12): C3 with its Drude and Lorentz spheres for 6000
+  steps -- field snapshots every 1000 steps within 1e-4 relative L2 of the
+  run's peak field, the bistatic scattered power within 0.1 dB at every angle
+  and frequency within 30 dB of that frequency's strongest, and the spectrum
+  of an Ez probe over the 10-80 GHz band within 1e-4 relative L2.  (C3 with
+  all three spheres diverges in the reference's own algorithm: the Debye
+  medium's modified-Lorentz form breaks the reference's stability condition,
+  so no error budget is meaningful on it; its FP64 parity is checked above.)
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle.reference_model import RefSimulation
+from tests.cases import rel_l2
+from xfdtd_core_b200 import engine as E
+from xfdtd_core_b200 import scene as S
+from xfdtd_core_b200.host import SceneRun
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-12
+FP32_FIELD = 1e-4
+FP32_RCS_DB = 0.1
+FP32_SPECTRUM = 1e-4
+
+
+def _upload(run, fields):
+    L = E.load()
+    h = ctypes.c_void_p(run.engine_handle())
+    arrs = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]
+    ptrs = (ctypes.c_void_p * 6)(*[a.ctypes.data for a in arrs])
+    assert L.xfd_upload_fields(h, ptrs) == 0, L.xfd_last_error(h)
+
+
+def test_boxes_full_size_fp64_200_steps():
+    sc = S.dielectric_boxes(steps=200)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc)
+    run.run()
+    assert run.n == (256, 256, 256)
+    got = run.fields()
+    for c, (g, w) in enumerate(zip(got, orc.e + orc.h)):
+        assert rel_l2(g, w) <= TOL64, (c, rel_l2(g, w))
+    run.close()
+
+
+def test_dispersive_full_size_fp64_random_fields():
+    steps = 12
+    sc = S.dispersive_spheres(steps=steps + 4)
+    orc = RefSimulation(sc)
+    rng = np.random.default_rng(11)
+    init = [rng.standard_normal(a.shape) for a in orc.e + orc.h]
+    for a, v in zip(orc.e + orc.h, init):
+        a[...] = v
+    orc.run(steps)
+    run = SceneRun(sc)
+    assert run.n == (384, 384, 384)
+    _upload(run, init)
+    run.advance(steps)
+    run.finish()
+    for c, (g, w) in enumerate(zip(run.fields(), orc.e + orc.h)):
+        assert rel_l2(g, w) <= TOL64, (c, rel_l2(g, w))
+    got = run.nf2ff()
+    acc = orc.nf2ff["acc"]
+    want = acc[0::2] + 1j * acc[1::2]
+    assert got.shape == want.shape and orc.nf2ff["nf"] == 32
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
+    run.close()
+
+
+def _scattered_power(ff, eta=376.730313668):
+    a_t, f_p, a_p, f_t = ff[:, 0], ff[:, 1], ff[:, 2], ff[:, 3]
+    return np.abs(eta * a_t + f_p) ** 2 + np.abs(eta * a_p - f_t) ** 2
+
+
+def _c3_stable_run(precision):
+    sc = S.dispersive_spheres(steps=6000, media=("drude", "lorentz"))
+    sc.field_times.append(S.FieldTimeSpec(
+        "probe_ez", "EZ", S.cube((0.0, 0.0, 0.004), (5e-4, 5e-4, 5e-4))))
+    run = SceneRun(sc, precision=precision)
+    snaps = []
+    for _ in range(6):
+        run.advance(1000)
+        run.finish()
+        snaps.append(run.fields())
+    ff = run.far_field(np.linspace(0.0, np.pi, 181), np.pi / 6)
+    probe = run.field_time(0)
+    run.close()
+    return snaps, ff, probe
+
+
+@pytest.fixture(scope="module")
+def c3_stable():
+    return _c3_stable_run(0), _c3_stable_run(1)
+
+
+def test_fp32_full_size_field_error(c3_stable):
+    (s64, _, _), (s32, _, _) = c3_stable
+    peak = max(max(float(np.linalg.norm(x)) for x in s) for s in s64)
+    assert peak > 0 and np.isfinite(peak)
+    for step, (a, b) in enumerate(zip(s32, s64)):
+        err = max(float(np.linalg.norm(x - y)) for x, y in zip(a, b)) / peak
+        assert err <= FP32_FIELD, ((step + 1) * 1000, err)
+
+
+def test_fp32_full_size_bistatic_rcs(c3_stable):
+    (_, ff64, _), (_, ff32, _) = c3_stable
+    p64, p32 = _scattered_power(ff64), _scattered_power(ff32)
+    mask = p64 >= p64.max(axis=1, keepdims=True) * 1e-3
+    db = np.abs(10 * np.log10(p32[mask] / p64[mask]))
+    assert db.max() <= FP32_RCS_DB, float(db.max())
+
+
+def test_fp32_full_size_probe_spectrum(c3_stable):
+    (_, _, pr64), (_, _, pr32) = c3_stable
+    np.testing.assert_array_equal(pr32[0], pr64[0])
+    t = pr64[0]
+    dt = t[1] - t[0]
+    f = np.linspace(10e9, 80e9, 71)
+    kern = np.exp(-2j * np.pi * f[:, None] * t[None, :]) * dt
+    s64, s32 = kern @ pr64[1], kern @ pr32[1]
+    assert np.linalg.norm(s32 - s64) / np.linalg.norm(s64) <= FP32_SPECTRUM

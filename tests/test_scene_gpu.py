@@ -8,7 +8,7 @@ import pytest
 
 from oracle.reference_model import RefSimulation, network_s_parameters
 from tests.cases import rel_l2
-from tests.scenes import ALL, sphere_small, dispersive_small
+from tests.scenes import ALL, dispersive_small, dispersive_stable_small, sphere_small
 from xfdtd_core_b200 import scene as S
 from xfdtd_core_b200.host import SceneRun
 
@@ -155,11 +155,14 @@ def test_microstrip_line_full_size_fp64(tmp_path):
 
 
 @pytest.mark.parametrize("opts", [s for s in SWEEPS if s.id != "fused"])
-# FP32 budgets: relative L2 against the FP64 oracle after 150 steps, about
-# twice the largest error any sweep showed (dispersive: ~1.0e-4, from the
-# ADE recursions accumulating FP32 rounding).
+# FP32 budget: relative L2 against the FP64 oracle after 150 steps, 1e-4 for
+# every scene (measured: 0.6e-6 .. 5e-6).  The three-sphere dispersive scene
+# is left out: the reference's algorithm diverges on it (its Debye medium in
+# modified-Lorentz form breaks the reference's stability condition), so its
+# FP32 difference grows with the instability; the Drude + Lorentz scene runs
+# the same ADE storage and kernels and is stable.
 @pytest.mark.parametrize("name,budget", [("sphere", 1e-4), ("boxes", 1e-4),
-                                         ("dispersive", 2e-4), ("voxels", 2e-4),
+                                         ("dispersive_stable", 1e-4), ("voxels", 1e-4),
                                          ("lumped", 1e-4), ("microstrip", 1e-4)])
 def test_scene_fp32_error_budget(name, budget, opts):
     sc = ALL[name](steps=150)
@@ -219,9 +222,10 @@ def _scattered_power(ff, eta=376.730313668):
 
 def test_fp32_bistatic_rcs_error_budget():
     """FP32 form against the FP64 oracle on the bistatic scattered power of
-    the dispersive scene (TFSF, three ADE spheres, NF2FF): within 0.1 dB at
-    every angle whose power is within 30 dB of the strongest."""
-    sc = dispersive_small(steps=150)
+    the stable dispersive scene (TFSF, Drude and Lorentz ADE spheres, NF2FF):
+    within 0.1 dB at every angle whose power is within 30 dB of the
+    strongest."""
+    sc = dispersive_stable_small(steps=150)
     orc = RefSimulation(sc)
     orc.run()
     run = SceneRun(sc, precision=1)
