@@ -325,6 +325,54 @@ def time_oracle(scene, budget_s: float, max_steps: int, warmup: int = 1,
     return cells * k / el / 1e9, k, threads, el, cells, (r.nx, r.ny, r.nz), 1 + extra
 
 
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "xfd_ref_driver")
+
+
+def reference_step_estimate(cells: int, nf: int, surface: int, threads: int) -> float:
+    """Rough seconds per step of the reference library on this host: the
+    threaded stencil plus its single-threaded frequency-domain NF2FF update,
+    which runs its per-plane loop once per frequency (nF^2 x surface)."""
+    return cells * 60e-9 / max(threads, 1) + nf * nf * surface * 56e-9
+
+
+def time_reference_library(scene, warmup: int, steps: int, budget_s: float = 45.0):
+    """The reference's own library (oracle/_ref/xfd_ref_driver, its unmodified
+    sources built against the xtensor subset) on the scene, std::thread domains
+    ThreadConfig{1, 1, C} over all host cores: one run of W' + K' steps, the
+    per-step times from a SimulationFlagVisitor; the first W' steps are
+    warm-up.  W' <= warmup and K' <= steps are bounded so that the timed steps
+    take about `budget_s`.  Returns (Gcell/s, K', threads, seconds, cells,
+    dims, W') or None when the driver is missing or cannot run the scene."""
+    import tempfile
+    if not os.access(REF_DRIVER, os.X_OK):
+        return None
+    threads = cpu_threads()
+    # Cubic workload scenes: n = round(L / dl) + 2 x PML cells per axis, as the
+    # reference's grid generation gives; the NF2FF surface from its distance.
+    n = scene_n(scene)
+    dims = (n, n, n)
+    cells = n ** 3
+    nf, surface = 0, 0
+    if scene.nf2ff is not None:
+        nf = len(scene.nf2ff.freqs)
+        surface = 6 * (n - 2 * int(scene.nf2ff.distance[0])) ** 2
+    est = reference_step_estimate(cells, nf, surface, threads)
+    k = int(max(1, min(steps, budget_s / est)))
+    w = int(max(1, min(warmup, (budget_s / 2) / est)))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "scene.txt")
+        scene.write(path)
+        r = subprocess.run([REF_DRIVER, path, d, "--steps", str(w + k), "--threads", str(threads),
+                            "--time-only"], capture_output=True, text=True)
+        if r.returncode != 0:
+            return None
+        per_step = [float(x) for x in open(os.path.join(d, "time.txt")).read().split("\n")[1:]
+                    if x.strip()]
+    timed = per_step[w:w + k]
+    el = sum(timed)
+    return cells * len(timed) / el / 1e9, len(timed), threads, el, cells, dims, w
+
+
 def cpu_model() -> str:
     try:
         for ln in open("/proc/cpuinfo"):
@@ -703,10 +751,15 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        # The oracle alone: no library of this package is loaded on this arm.
+        # The reference's own library (oracle/_ref), or where it cannot run the
+        # workload the oracle port; no library of this package is loaded here.
         scene = workload_scene(steps=warmup + steps + 2, n=args.grid)
-        value, k, threads, el, ocells, dims, warm_run = time_oracle(
-            scene, budget_s=45.0, max_steps=steps, warmup=warmup)
+        got = time_reference_library(scene, warmup, steps) if KIND != "adjoint" else None
+        kind = "reference"
+        if got is None:
+            kind = "port"
+            got = time_oracle(scene, budget_s=45.0, max_steps=steps, warmup=warmup)
+        value, k, threads, el, ocells, dims, warm_run = got
         size = "x".join(str(v) for v in dims)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": k, "warmup": warm_run, "ms_per_step": el / k * 1e3,
@@ -718,14 +771,18 @@ def main():
                            {"workload": workload_name(0), "cells": scene_cells(scene),
                             "sample": "the median-size scene of the batch"}),
                 "impl": "reference",
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{k} FDTD steps of the "
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                                 "sample": ("the reference's own library (its unmodified "
+                                            "sources, std::thread domains ThreadConfig{1,1,"
+                                            f"{threads}}}): " if kind == "reference" else
+                                            "the oracle port (FP64, OpenMP): ") +
+                                           f"{k} FDTD steps of the "
                                            + (f"full {size} scene" if KIND != "batched"
                                               else f"median batched scene ({scene_cells(scene)} "
                                                    "cells)")
                                            + f" (requested {steps}; bounded to ~45 s), "
                                            f"{warm_run} warm-up step(s) (requested {warmup}; "
-                                           "bounded to ~30 s), " + cpu_model()
+                                           "time-bounded), " + cpu_model()
                                            + ("; the reference's frequency-domain NF2FF "
                                               "update is single-threaded and O(nF^2 x surface) "
                                               "per step (its per-plane loop runs once per "

@@ -574,7 +574,29 @@ class xtensor : public xdense<T> {
   static xtensor from_shape(std::initializer_list<std::size_t> s) { return xtensor(shape_type(s)); }
   void take_from(xdense<T>&& o) { this->take(std::move(o)); }
 
+  // Element access with the rank known at compile time (one multiply-add per
+  // index, no run-time rank loop), as xtensor's fixed-rank containers do.
+  template <class... I>
+  T& operator()(I... idx) {
+    if constexpr (sizeof...(I) == N) return this->data()[fixed_offset(idx...)];
+    else return base::operator()(idx...);
+  }
+  template <class... I>
+  const T& operator()(I... idx) const {
+    if constexpr (sizeof...(I) == N) return this->data()[fixed_offset(idx...)];
+    else return base::operator()(idx...);
+  }
+
  private:
+  template <class... I>
+  std::ptrdiff_t fixed_offset(I... idx) const {
+    const std::ptrdiff_t v[N > 0 ? N : 1] = {(std::ptrdiff_t)idx...};
+    const std::ptrdiff_t* st = this->full_.data();
+    std::ptrdiff_t o = 0;
+#pragma GCC unroll 8
+    for (std::size_t d = 0; d < N; ++d) o += v[d] * st[d];
+    return o;
+  }
   void rank_check() const {
     if (this->shape_.size() != N) throw std::runtime_error("xt::xtensor: rank mismatch");
   }
