@@ -52,7 +52,8 @@ def test_reference_arm_line():
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference"
     assert line["metric"] == "Gcell-updates/s" and line["unit"] == "Gcell/s"
-    assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+    # the reference's own library where oracle/_ref is built, else the port
+    assert line["value"] > 0 and line["cpu_baseline"]["kind"] in ("reference", "port")
     assert line["e2e"]["h2d_bytes_per_step"] == 0
 
 
