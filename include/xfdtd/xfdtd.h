@@ -10,8 +10,11 @@
 //
 // Deliberate differences, each documented at the member:
 // * ThreadConfig is accepted and ignored (the time loop runs on the GPU).
-// * Array1D is a small owning vector, not xt::xtensor; xt_compat.h gives the
-//   xt::xarray / xt::linspace spellings reference programs use.
+// * The xt:: containers, builders and .npy writer come from the xtensor subset
+//   in include/xtensor_subset (xtensor itself is not needed).
+// * MPI is not used: MpiSupport keeps its calls and runs them as one rank.
+// * Flag visitors are told about the time loop at the boundaries of the
+//   engine's step chunks, not at every step.
 // * Precision is chosen per Simulation (FP64 default, FP32 form optional)
 //   instead of at build time (CMake XFDTD_CORE_SINGLE_PRECISION).
 #pragma once
@@ -30,6 +33,8 @@
 #include <string_view>
 #include <vector>
 
+#include "../xtensor_subset/xtensor/xt_core.hpp"
+
 struct xfd_engine;
 
 namespace xfdtd {
@@ -37,56 +42,21 @@ namespace xfdtd {
 using Real = double;
 using Index = std::size_t;
 
-// ---------------------------------------------------------------- Array1D
+// ----------------------------------------------------------------- arrays
+// The reference's array types (include/xfdtd/common/type_define.h:18-31):
+// xtensor containers, here from the xtensor subset shipped beside this
+// header (include/xtensor_subset; programs add it to their include path to
+// use <xtensor/...> themselves).
 template <typename T>
-class Array1D {
- public:
-  Array1D() = default;
-  Array1D(std::initializer_list<T> v) : _v(v) {}
-  explicit Array1D(std::vector<T> v) : _v(std::move(v)) {}
-  explicit Array1D(std::size_t n, T fill = T{}) : _v(n, fill) {}
-  std::size_t size() const { return _v.size(); }
-  T& operator()(std::size_t i) { return _v[i]; }
-  const T& operator()(std::size_t i) const { return _v[i]; }
-  T& operator[](std::size_t i) { return _v[i]; }
-  const T& operator[](std::size_t i) const { return _v[i]; }
-  T* data() { return _v.data(); }
-  const T* data() const { return _v.data(); }
-  auto begin() { return _v.begin(); }
-  auto end() { return _v.end(); }
-  auto begin() const { return _v.begin(); }
-  auto end() const { return _v.end(); }
-  const T& front() const { return _v.front(); }
-  const T& back() const { return _v.back(); }
-  std::vector<T>& vec() { return _v; }
-  const std::vector<T>& vec() const { return _v; }
-
- private:
-  std::vector<T> _v;
-};
-
-/// Row-major 3-D array (k fastest), the EMF field storage.
+using Array1D = xt::xtensor<T, 1>;
 template <typename T>
-class Array3D {
- public:
-  Array3D() = default;
-  Array3D(std::size_t n0, std::size_t n1, std::size_t n2)
-      : _n{n0, n1, n2}, _v(n0 * n1 * n2, T{}) {}
-  T& operator()(std::size_t i, std::size_t j, std::size_t k) {
-    return _v[(i * _n[1] + j) * _n[2] + k];
-  }
-  const T& operator()(std::size_t i, std::size_t j, std::size_t k) const {
-    return _v[(i * _n[1] + j) * _n[2] + k];
-  }
-  const std::array<std::size_t, 3>& shape() const { return _n; }
-  std::size_t size() const { return _v.size(); }
-  T* data() { return _v.data(); }
-  const T* data() const { return _v.data(); }
-
- private:
-  std::array<std::size_t, 3> _n{0, 0, 0};
-  std::vector<T> _v;
-};
+using Array2D = xt::xtensor<T, 2>;
+template <typename T>
+using Array3D = xt::xtensor<T, 3>;
+template <typename T>
+using Array4D = xt::xtensor<T, 4>;
+template <typename T>
+using Array = xt::xarray<T>;
 
 // ------------------------------------------------------------- constants
 // include/xfdtd/common/constant.h:11-18
@@ -814,6 +784,47 @@ class ThreadConfig {
   std::array<std::size_t, 3> _n;
 };
 
+/// MPI decomposition of the reference (include/xfdtd/parallel/mpi_support.h).
+/// This library runs one simulation on one GPU and does not use MPI: the calls
+/// reference programs make are kept and behave as on a single rank.
+class MpiSupport {
+ public:
+  static void setMpiParallelDim(int /*nx*/, int /*ny*/, int /*nz*/) {}
+  static MpiSupport& instance() {
+    static MpiSupport s;
+    return s;
+  }
+  bool isRoot() const { return true; }
+  int rank() const { return 0; }
+  int size() const { return 1; }
+  void barrier() const {}
+};
+
+// ------------------------------------------------------- flag visitors
+/// include/xfdtd/simulation/simulation_flag.h:8-31.
+enum class SimulationInitFlag { SimulationStart, SimulationEnd, InitStart, InitEnd, UpdateStart, UpdateEnd };
+enum class SimulationIteratorFlag { UpdateHSStart, UpdateHSEnd, UpdateEStart, UpdateEEnd, NextStep };
+
+class SimulationFlagVisitor {
+ public:
+  virtual ~SimulationFlagVisitor() = default;
+  virtual void initStep(SimulationInitFlag flag) = 0;
+  virtual void iteratorStep(SimulationIteratorFlag flag, Index cur, Index start, Index end) = 0;
+};
+
+/// Prints the phases and their elapsed times to stderr, and the progress of
+/// the time loop (the reference's DefaultSimulationFlagVisitor,
+/// src/simulation/simulation.cpp:157-280).
+class DefaultSimulationFlagVisitor : public SimulationFlagVisitor {
+ public:
+  void initStep(SimulationInitFlag flag) override;
+  void iteratorStep(SimulationIteratorFlag flag, Index cur, Index start, Index end) override;
+
+ private:
+  double _t_init = 0, _t_update = 0;
+  Index _last_percent = 101;
+};
+
 enum class Precision { FP64 = 0, FP32 = 1 };
 
 // ------------------------------------------------------------- Simulation
@@ -833,6 +844,19 @@ class Simulation {
   void addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> nffft);
   void addNF2FF(std::shared_ptr<NFFFTTimeDomain> nffft);
   void addNetwork(std::shared_ptr<Network> network);
+  /// Flag visitors (include/xfdtd/simulation/simulation.h:66-68): told
+  /// SimulationStart / InitStart / InitEnd / UpdateStart / UpdateEnd /
+  /// SimulationEnd, and NextStep (with the current, first and last step) at
+  /// the end of every chunk of steps the engine runs as one graph (32 steps
+  /// unless the "graph_chunk" option says otherwise) rather than every step.
+  void addVisitor(std::shared_ptr<SimulationFlagVisitor> visitor);
+  void addDefaultVisitor();
+
+  /// One process, one GPU: always the root, rank 0 of 1.
+  bool isRoot() const { return true; }
+  int myRank() const { return 0; }
+  int numNode() const { return 1; }
+  int numThread() const { return 1; }
 
   /// Builds the grid and coefficients, runs `time_step` steps on the GPU and
   /// copies fields, movie frames and NF2FF currents back to the host.
@@ -912,6 +936,8 @@ class Simulation {
   std::vector<std::shared_ptr<NFFFTFrequencyDomain>> _nffts;
   std::vector<std::shared_ptr<NFFFTTimeDomain>> _nffts_td;
   std::vector<std::shared_ptr<Network>> _networks;
+  std::vector<std::shared_ptr<SimulationFlagVisitor>> _visitors;
+  long long _chunk = 32;  // steps per visitor NextStep (the engine's graph chunk)
   EMF _emf;
   Real _dt = 0;
   Index _n[3] = {0, 0, 0};

@@ -74,16 +74,16 @@ std::shared_ptr<Material> parseMaterial(std::istringstream& in, const std::strin
       y.push_back(num(in));
     }
     if (kind == "drude")
-      return DrudeMedium::makeDrudeMedium(name, eps_inf, Array1D<Real>(x), Array1D<Real>(y));
-    return DebyeMedium::makeDebyeMedium(name, eps_inf, Array1D<Real>(x), Array1D<Real>(y));
+      return DrudeMedium::makeDrudeMedium(name, eps_inf, Array1D<Real>(xt::adapt(x)), Array1D<Real>(xt::adapt(y)));
+    return DebyeMedium::makeDebyeMedium(name, eps_inf, Array1D<Real>(xt::adapt(x)), Array1D<Real>(xt::adapt(y)));
   }
   if (kind == "mlorentz") {
     std::vector<Real> v[5];
     for (int p = 0; p < P; ++p)
       for (int q = 0; q < 5; ++q) v[q].push_back(num(in));
-    return MLorentzMaterial::makeMLorentz(name, eps_inf, Array1D<Real>(v[0]), Array1D<Real>(v[1]),
-                                          Array1D<Real>(v[2]), Array1D<Real>(v[3]),
-                                          Array1D<Real>(v[4]));
+    return MLorentzMaterial::makeMLorentz(name, eps_inf, Array1D<Real>(xt::adapt(v[0])), Array1D<Real>(xt::adapt(v[1])),
+                                          Array1D<Real>(xt::adapt(v[2])), Array1D<Real>(xt::adapt(v[3])),
+                                          Array1D<Real>(xt::adapt(v[4])));
   }
   throw XFDTDException("bad material '" + kind + "'");
 }
@@ -227,7 +227,7 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       std::vector<Real> fr(nf);
       for (auto& v : fr) v = num(in);
       sc->network = std::make_shared<Network>(std::vector<std::shared_ptr<Port>>{},
-                                              Array1D<Real>(std::move(fr)), "");
+                                              Array1D<Real>(xt::adapt(fr)), "");
       sc->sim->addNetwork(sc->network);
     } else if (kw == "port") {
       if (!sc->network) throw XFDTDException("port before network");
@@ -305,7 +305,7 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       const int nf = static_cast<int>(num(in));
       std::vector<Real> fr;
       for (int q = 0; q < nf; ++q) fr.push_back(num(in));
-      sc->nf2ff = std::make_shared<NFFFTFrequencyDomain>(dx, dy, dz, Array1D<Real>(fr));
+      sc->nf2ff = std::make_shared<NFFFTFrequencyDomain>(dx, dy, dz, Array1D<Real>(xt::adapt(fr)));
       sc->sim->addNF2FF(sc->nf2ff);
     } else if (kw == "nf2ff_td") {
       const auto dx = static_cast<Index>(num(in)), dy = static_cast<Index>(num(in)),

@@ -21,6 +21,8 @@
 // materials of the 2x2x2 cells around a lattice node) plus a uint16 class per
 // node, and per-axis curl factors 1/(d*kappa).
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -168,8 +170,8 @@ void Waveform::init(const std::vector<Real>& time) {
   // Waveform::init (src/waveform/waveform.cpp:28-34)
   std::vector<Real> v(time.size());
   for (std::size_t i = 0; i < time.size(); ++i) v[i] = amplitude() * _f(time[i]);
-  _value = Array1D<Real>(std::move(v));
-  _time = Array1D<Real>(time);
+  _value = Array1D<Real>(xt::adapt(v));
+  _time = Array1D<Real>(xt::adapt(time));
 }
 
 // --------------------------------------------------------- helpers
@@ -303,10 +305,76 @@ void Simulation::addNF2FF(std::shared_ptr<NFFFTFrequencyDomain> n) {
   _nffts.push_back(std::move(n));
 }
 
+void Simulation::addVisitor(std::shared_ptr<SimulationFlagVisitor> v) {
+  if (v) _visitors.push_back(std::move(v));
+}
+void Simulation::addDefaultVisitor() {
+  _visitors.push_back(std::make_shared<DefaultSimulationFlagVisitor>());
+}
+
 void Simulation::run(Index time_step) {
+  auto flag = [&](SimulationInitFlag f) {
+    for (auto& v : _visitors) v->initStep(f);
+  };
+  flag(SimulationInitFlag::SimulationStart);
+  flag(SimulationInitFlag::InitStart);
   init(time_step);
-  advance(time_step);
+  flag(SimulationInitFlag::InitEnd);
+  flag(SimulationInitFlag::UpdateStart);
+  if (_visitors.empty()) {
+    advance(time_step);
+  } else {
+    // Chunks of the engine's graph length; a visitor sees NextStep after each
+    // (the engine is synchronised there, so the step it reports is done).
+    const Index start = 0, end = time_step;
+    for (Index t = 0; t < time_step;) {
+      const Index n = std::min<Index>((Index)std::max<long long>(_chunk, 1), time_step - t);
+      advance(n);
+      checkStatus(_engine, xfd_sync(_engine), "xfd_sync");
+      t += n;
+      for (auto& v : _visitors) v->iteratorStep(SimulationIteratorFlag::NextStep, t, start, end);
+    }
+  }
   finish();
+  flag(SimulationInitFlag::UpdateEnd);
+  flag(SimulationInitFlag::SimulationEnd);
+}
+
+void DefaultSimulationFlagVisitor::initStep(SimulationInitFlag flag) {
+  using clk = std::chrono::steady_clock;
+  const double now = std::chrono::duration<double>(clk::now().time_since_epoch()).count();
+  switch (flag) {
+    case SimulationInitFlag::SimulationStart:
+      std::fprintf(stderr, "Simulation start\n");
+      break;
+    case SimulationInitFlag::InitStart:
+      _t_init = now;
+      std::fprintf(stderr, "Simulation init start\n");
+      break;
+    case SimulationInitFlag::InitEnd:
+      std::fprintf(stderr, "Simulation init end\nElapsed time: %.3f s\n", now - _t_init);
+      break;
+    case SimulationInitFlag::UpdateStart:
+      _t_update = now;
+      std::fprintf(stderr, "Simulation update start\n");
+      break;
+    case SimulationInitFlag::UpdateEnd:
+      std::fprintf(stderr, "Simulation update end\nElapsed time: %.3f s\n", now - _t_update);
+      break;
+    case SimulationInitFlag::SimulationEnd:
+      std::fprintf(stderr, "Simulation end\n");
+      break;
+  }
+}
+
+void DefaultSimulationFlagVisitor::iteratorStep(SimulationIteratorFlag flag, Index cur, Index start,
+                                                Index end) {
+  if (flag != SimulationIteratorFlag::NextStep || end <= start) return;
+  const Index percent = (cur - start) * 100 / (end - start);
+  if (percent == _last_percent) return;
+  _last_percent = percent;
+  std::fprintf(stderr, "\rProgress: %zu%% (%zu/%zu)%s", (size_t)percent, (size_t)(cur - start),
+               (size_t)(end - start), cur >= end ? "\n" : "");
 }
 
 void Simulation::init(Index time_step) {
@@ -1217,6 +1285,7 @@ void Simulation::init(Index time_step) {
 void Simulation::setEngineOption(const std::string& name, long long value) {
   if (_engine) checkStatus(_engine, xfd_set_option(_engine, name.c_str(), value), "xfd_set_option");
   _engine_options.emplace_back(name, value);
+  if (name == "graph_chunk") _chunk = value;
 }
 
 void Simulation::advance(Index n) {
@@ -1236,7 +1305,7 @@ void Simulation::finish() {
       const bool along = (d == c % 3);
       s[d] = (c < 3) ? (along ? n[d] : n[d] + 1) : (along ? n[d] + 1 : n[d]);
     }
-    _emf._f[c] = Array3D<Real>(s[0], s[1], s[2]);
+    _emf._f[c] = Array3D<Real>::from_shape({(std::size_t)s[0], (std::size_t)s[1], (std::size_t)s[2]});
     if (_precision == Precision::FP64) {
       checkStatus(_engine, xfd_download_field(_engine, c, _emf._f[c].data()), "download");
     } else {
@@ -1859,12 +1928,12 @@ Vector NFFFTTimeDomain::observationDirection() const {
 }
 
 Array1D<Real> NFFFTTimeDomain::scaled(int q) const {
-  if (_raw.empty()) return Array1D<Real>(std::vector<Real>{});
+  if (_raw.empty()) return Array1D<Real>::from_shape({std::size_t{0}});
   const std::size_t n = _raw.size() / 6;
   const Real den = _c_dt * 4 * PI;
   std::vector<Real> v(n);
   for (std::size_t b = 0; b < n; ++b) v[b] = _raw[q * n + b] / den;
-  return Array1D<Real>(v);
+  return Array1D<Real>(xt::adapt(v));
 }
 
 std::array<std::vector<Real>, 4> NFFFTTimeDomain::farField() const {
