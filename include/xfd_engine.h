@@ -94,6 +94,24 @@ xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t 
 xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, const int32_t* comp,
                                const double* ca, const double* cb);
 
+/* Per-node H curl-term corrections: after the H sweep of every step, the H
+ * component comp[q] at node (node[3q], node[3q+1], node[3q+2]) gets
+ *   delta_a[q] * (E_a[x_b+1] - E_a) + delta_b[q] * (E_b[x_a+1] - E_b)
+ * added (a = comp+1, b = comp+2 mod 3; the E of the same step) -- for
+ * coefficients that scale one curl term of a node but not the other, which
+ * the class table's single cb per component cannot hold.  Nodes in the main H
+ * range (x < n on every axis), one entry per (node, component); call once.
+ * The correction runs between the H and E phases of a split sweep: an engine
+ * on a fused sweep moves to the split one (kernel 4 from 7, else 0), and
+ * the fused kernels (1, 2, 5, 6, 7) are refused afterwards.  Not batched, no
+ * adjoint.
+ * Replaces: ThinWire::correctUpdateCoefficient's scaling of chxey, chyex,
+ * chzex, chzey next to the wire (src/object/thin_wire.cpp:42-133) in the
+ * full-grid coefficient arrays. */
+xfd_status xfd_set_h_term_overrides(xfd_engine* e, int64_t n, const int32_t* node,
+                                    const int32_t* comp, const double* delta_a,
+                                    const double* delta_b);
+
 /* Per-axis curl factors.  fe[a] has n_a+1 entries, 1/(h_size * kappa_e);
  * fh[a] has n_a entries, 1/(e_size * kappa_h) (kappa = 1 outside CPML).
  * Replaces: the grid sizes folded into the coefficients

@@ -24,8 +24,10 @@
 #include <complex>
 #include <map>
 #include <cstdint>
+#include <cstdlib>
 #include <functional>
 #include <initializer_list>
+#include <limits>
 #include <memory>
 #include <numbers>
 #include <stdexcept>
@@ -65,8 +67,12 @@ inline constexpr Real PI{std::numbers::pi_v<Real>};
 inline constexpr Real EPSILON_0{8.854187817e-12};
 inline constexpr Real MU_0{4 * PI * 1e-7};
 inline const Real C_0{1 / std::sqrt(EPSILON_0 * MU_0)};
+inline const Real Z_0{std::sqrt(MU_0 / EPSILON_0)};
 inline constexpr Real SIGMA_E_ZERO_APPROX{1e-20};
 inline constexpr Real SIGMA_M_ZERO_APPROX{1e-20};
+inline constexpr Real INF{std::numeric_limits<Real>::infinity()};
+inline constexpr Real NEG_INF{-std::numeric_limits<Real>::infinity()};
+inline constexpr std::complex<Real> II{0.0, 1.0};
 }  // namespace constant
 
 class XFDTDException : public std::runtime_error {
@@ -85,17 +91,80 @@ class Vector {
   Real operator()(int a) const { return _d[a]; }
   Vector operator+(const Vector& o) const { return {x() + o.x(), y() + o.y(), z() + o.z()}; }
   Vector operator-(const Vector& o) const { return {x() - o.x(), y() - o.y(), z() - o.z()}; }
+  Vector operator*(Real f) const { return {x() * f, y() * f, z() * f}; }
+  Vector operator/(Real f) const { return {x() / f, y() / f, z() / f}; }
+  bool operator==(const Vector& o) const { return _d == o._d; }
+  bool operator!=(const Vector& o) const { return !(*this == o); }
 
  private:
   std::array<Real, 3> _d{0, 0, 0};
 };
 
-struct Axis {
+/// A unit vector along a coordinate axis, and the axis / direction enums
+/// (include/xfdtd/coordinate_system/coordinate_system.h:93-170,
+/// src/coordinate_system/asix.cpp).
+class Axis : public Vector {
+ public:
   enum class XYZ { X = 0, Y = 1, Z = 2 };
   enum class Direction { XN, XP, YN, YP, ZN, ZP };
+  explicit Axis(const Vector& direction) : Vector{direction} {}
+  bool operator==(const Axis& rhs) const { return Vector::operator==(rhs); }
+  bool operator!=(const Axis& rhs) const { return !(*this == rhs); }
+  bool operator==(Direction d) const { return *this == fromDirectionToAxis(d); }
+  bool operator!=(Direction d) const { return !(*this == d); }
+  /// True for both directions along the axis.
+  bool operator==(XYZ c) const {
+    const int a = static_cast<int>(c);
+    return std::abs((*this)(a)) == 1 && (*this)((a + 1) % 3) == 0 && (*this)((a + 2) % 3) == 0;
+  }
+  bool operator!=(XYZ c) const { return !(*this == c); }
+  static const Axis XN, XP, YN, YP, ZN, ZP;
+  static Axis fromDirectionToAxis(Direction d) {
+    const int a = axisOf(d);
+    const Real s = negative(d) ? -1 : 1;
+    return Axis{Vector{a == 0 ? s : 0, a == 1 ? s : 0, a == 2 ? s : 0}};
+  }
+  static XYZ fromDirectionToXYZ(Direction d) { return static_cast<XYZ>(axisOf(d)); }
+  template <Direction d>
+  static constexpr XYZ fromDirectionToXYZ() {
+    return static_cast<XYZ>(static_cast<int>(d) / 2);
+  }
+  static constexpr XYZ tangentialAAxis(XYZ c) {
+    return static_cast<XYZ>((static_cast<int>(c) + 1) % 3);
+  }
+  static constexpr XYZ tangentialBAxis(XYZ c) {
+    return static_cast<XYZ>((static_cast<int>(c) + 2) % 3);
+  }
+  static bool directionNegative(Direction d) { return negative(d); }
+  static bool directionPositive(Direction d) { return !negative(d); }
+  template <Direction d>
+  static constexpr bool directionNegative() { return static_cast<int>(d) % 2 == 0; }
+  template <Direction d>
+  static constexpr bool directionPositive() { return static_cast<int>(d) % 2 == 1; }
+  static std::string toString(Direction d) {
+    static const char* n[6] = {"XN", "XP", "YN", "YP", "ZN", "ZP"};
+    return n[static_cast<int>(d)];
+  }
+  static std::string toString(XYZ c) {
+    static const char* n[3] = {"X", "Y", "Z"};
+    return n[static_cast<int>(c)];
+  }
+  /// The axis (0, 1, 2) of a direction, and whether it points down that axis.
   static int axisOf(Direction d) { return static_cast<int>(d) / 2; }
   static bool negative(Direction d) { return static_cast<int>(d) % 2 == 0; }
+  /// The axis of this unit vector (0, 1, 2), or -1 when it is not along one.
+  int axisIndex() const {
+    for (int a = 0; a < 3; ++a)
+      if (*this == static_cast<XYZ>(a)) return a;
+    return -1;
+  }
 };
+inline const Axis Axis::XN{Vector{-1, 0, 0}};
+inline const Axis Axis::XP{Vector{1, 0, 0}};
+inline const Axis Axis::YN{Vector{0, -1, 0}};
+inline const Axis Axis::YP{Vector{0, 1, 0}};
+inline const Axis Axis::ZN{Vector{0, 0, -1}};
+inline const Axis Axis::ZP{Vector{0, 0, 1}};
 
 class Cube;
 
@@ -117,6 +186,10 @@ class Cube : public Shape {
   const Vector& origin() const { return _origin; }
   const Vector& size() const { return _size; }
   const Vector& end() const { return _end; }
+  Vector center() const { return _origin + _size / 2; }
+  Real centerX() const { return center().x(); }
+  Real centerY() const { return center().y(); }
+  Real centerZ() const { return center().z(); }
 
  private:
   Vector _origin, _size, _end;
@@ -136,6 +209,26 @@ class Sphere : public Shape {
   Real _radius;
 };
 
+/// Cylinder(center, radius, height, axis) (src/shape/cylinder.cpp): the
+/// points of its wrapped cube within `radius` of the axis line through
+/// `center`.
+class Cylinder : public Shape {
+ public:
+  Cylinder(Vector center, Real radius, Real height, Axis axis);
+  bool isInside(Real x, Real y, Real z, Real eps) const override;
+  std::unique_ptr<Cube> wrappedCube() const override;
+  std::unique_ptr<Shape> clone() const override { return std::make_unique<Cylinder>(*this); }
+  Vector center() const { return _center; }
+  Real radius() const { return _radius; }
+  Real height() const { return _height; }
+  Axis axis() const { return _axis; }
+
+ private:
+  Vector _center;
+  Real _radius, _height;
+  Axis _axis;
+};
+
 // -------------------------------------------------------------- materials
 /// ElectroMagneticProperty(eps_r, mu_r, sigma_e, sigma_m); zero conductivities
 /// become 1e-20 (src/material/material.cpp:11-26).
@@ -151,6 +244,11 @@ class ElectroMagneticProperty {
   Real sigmaM() const { return _sigma_m; }
   Real epsilon() const { return _eps_r * constant::EPSILON_0; }
   Real mu() const { return _mu_r * constant::MU_0; }
+  std::string toString() const {
+    return "ElectroMagneticProperty{epsilon_r: " + std::to_string(_eps_r) +
+           ", mu_r: " + std::to_string(_mu_r) + ", sigma_e: " + std::to_string(_sigma_e) +
+           ", sigma_m: " + std::to_string(_sigma_m) + "}";
+  }
 
  private:
   Real _eps_r, _mu_r, _sigma_e, _sigma_m;
@@ -170,6 +268,10 @@ class Material {
   const std::string& name() const { return _name; }
   const ElectroMagneticProperty& emProperty() const { return _emp; }
   bool dispersion() const { return _dispersion; }
+  virtual std::string toString() const {
+    return "Material{name: " + _name + ", em_property: " + _emp.toString() +
+           ", dispersion: " + std::to_string(static_cast<int>(_dispersion)) + "}";
+  }
 
  private:
   std::string _name;
@@ -197,6 +299,14 @@ class LinearDispersiveMaterial : public Material {
   const std::array<Real, 5>& pole(Index p) const { return _poles[p]; }
   /// Drude (omega_p, gamma) or Debye (eps_static, tau) of pole p.
   const std::array<Real, 2>& native(Index p) const { return _native[p]; }
+  /// chi_p(f) = (a1 jw + a0) / (b2 (jw)^2 + b1 jw + b0), w = 2 pi f
+  /// (MLorentzEqDecision::susceptibility,
+  /// src/material/dispersive_material_equation.cpp:35-41).
+  std::complex<Real> susceptibility(Real freq, Index p) const;
+  /// eps_inf + sum_p chi_p(f) per frequency
+  /// (LinearDispersiveMaterial::relativePermittivity,
+  /// src/material/dipersive_material.cpp:31-41).
+  Array1D<std::complex<Real>> relativePermittivity(const Array1D<Real>& freq) const;
 
  private:
   Real _eps_inf;
@@ -241,6 +351,14 @@ class Waveform {
   static std::unique_ptr<Waveform> cosineModulatedGaussian(Real tau, Real t_0, Real frequency,
                                                            Real amplitude = 1.0);
   static std::unique_ptr<Waveform> sine(Real frequency, Real amplitude = 1.0);
+  static std::unique_ptr<Waveform> cosine(Real frequency, Real amplitude = 1.0);
+  static std::unique_ptr<Waveform> square(Real frequency, Real amplitude = 1.0);
+  /// As in the reference, the triangle wave keeps amplitude 1 whatever is
+  /// passed (src/waveform/waveform.cpp:64-70).
+  static std::unique_ptr<Waveform> triangle(Real frequency, Real amplitude = 1.0);
+  static std::unique_ptr<Waveform> sawtooth(Real frequency, Real amplitude = 1.0);
+  /// 1 from t_0 on, 0 before.
+  static std::unique_ptr<Waveform> step(Real t_0, Real amplitude = 1.0);
   Real amplitude() const { return _amplitude; }
   Real operator()(Real t) const { return _f(t); }
   void init(const std::vector<Real>& time);
@@ -304,6 +422,20 @@ class PecPlane : public Object {
  public:
   PecPlane(std::string name, std::unique_ptr<Cube> cube)
       : Object{std::move(name), std::move(cube), Material::createPec()} {}
+};
+
+/// Thin wire along a Cylinder's axis (src/object/thin_wire.cpp:9-152): air,
+/// painted like any object; on a uniform grid with the radius below half the
+/// cell on both transverse axes, the E component along the wire on the
+/// wire's nodes is held at zero, and the H coefficients next to the wire that
+/// the reference scales by k 2 / ln(d / r) (chyex, chzex for an x wire;
+/// chzey, chxey for y; chxey, chyex for z -- the reference's choice) take
+/// that factor.  Coefficient changes apply in object order with the lumped
+/// elements'.
+class ThinWire : public Object {
+ public:
+  ThinWire(const std::string& name, std::unique_ptr<Cylinder> shape)
+      : Object{name, std::move(shape), Material::createAir()} {}
 };
 
 /// Lumped element on a Cube of E nodes along one axis
@@ -722,6 +854,14 @@ class NFFFTFrequencyDomain {
                        const Vector& origin = Vector{0, 0, 0}) const;
   void processFarField(const Array1D<Real>& theta, const Array1D<Real>& phi,
                        const std::string& sub_dir, const Vector& origin) const;
+  /// Radiated power per frequency, 0.5 Re sum over the faces of
+  /// (+-) sum ds (conj(J_a) M_b - conj(J_b) M_a) (FDPlaneData::power and
+  /// calculatePower, src/nffft/nffft_fd_data_process.cpp:38-190).
+  std::vector<Real> radiationPower() const;
+  /// Writes <outputDir>/power.npy: the 2 x n_freq stack of the frequencies and
+  /// radiationPower() (NFFFTFrequencyDomain::outputRadiationPower,
+  /// src/nffft/nffft_frequency_domain.cpp:67-100).
+  void outputRadiationPower() const;
 
  private:
   friend class Simulation;
@@ -776,6 +916,61 @@ class NFFFTTimeDomain {
   Real _c_dt = 0;
 };
 
+/// The time axis of a run (include/xfdtd/calculation_param/time_param.h,
+/// src/calculation_param/time_param.cpp): dt, the number of steps, the
+/// first step, and the E / H sample times of every step.
+class TimeParam {
+ public:
+  /// cfl / (c sqrt(1/dx^2 + 1/dy^2 + 1/dz^2)), and its 2-D and 1-D forms.
+  static Real calculateDt(Real cfl, Real dx, Real dy, Real dz) {
+    return cfl / (constant::C_0 * std::sqrt(1.0 / (dx * dx) + 1.0 / (dy * dy) + 1.0 / (dz * dz)));
+  }
+  static Real calculateDt(Real cfl, Real dx, Real dy) {
+    return cfl / (constant::C_0 * std::sqrt(1.0 / (dx * dx) + 1.0 / (dy * dy)));
+  }
+  static Real calculateDt(Real cfl, Real dz) {
+    return cfl / (constant::C_0 * std::sqrt(1.0 / (dz * dz)));
+  }
+  TimeParam(Real dt, std::size_t size, std::size_t start_time_step = 0)
+      : _dt{dt}, _start{start_time_step}, _size{size}, _current{start_time_step} {}
+  Real dt() const { return _dt; }
+  std::size_t startTimeStep() const { return _start; }
+  std::size_t size() const { return _size; }
+  std::size_t endTimeStep() const { return _start + _size; }
+  std::size_t currentTimeStep() const { return _current; }
+  std::size_t remainingTimeStep() const { return _start + _size - _current; }
+  void nextStep() { ++_current; }
+  void setCurrentTimeStep(std::size_t t) { _current = t; }
+  void setDt(Real dt) { _dt = dt; }
+  /// linspace((start + 1) dt, (start + size) dt, size)
+  Array1D<Real> eTime() const {
+    return xt::linspace<Real>((_start + 1) * _dt, (_start + _size) * _dt, _size);
+  }
+  /// linspace((start + 0.5) dt, (start + size + 0.5) dt, size)
+  Array1D<Real> hTime() const {
+    return xt::linspace<Real>((_start + 0.5) * _dt, (_start + _size + 0.5) * _dt, _size);
+  }
+
+ private:
+  Real _dt;
+  std::size_t _start, _size, _current;
+};
+
+/// The parameters of a run the reference's objects read
+/// (include/xfdtd/calculation_param/calculation_param.h:26-60): here the
+/// time axis.  The update coefficients live on the GPU as a class table
+/// (Simulation::coefficientArrays gives the reference's 18 arrays).
+class CalculationParam {
+ public:
+  explicit CalculationParam(std::unique_ptr<TimeParam> time_param)
+      : _time_param{std::move(time_param)} {}
+  const std::unique_ptr<TimeParam>& timeParam() const { return _time_param; }
+  std::unique_ptr<TimeParam>& timeParam() { return _time_param; }
+
+ private:
+  std::unique_ptr<TimeParam> _time_param;
+};
+
 class ThreadConfig {
  public:
   ThreadConfig(std::size_t x = 1, std::size_t y = 1, std::size_t z = 1) : _n{x, y, z} {}
@@ -789,8 +984,13 @@ class ThreadConfig {
 /// reference programs make are kept and behave as on a single rank.
 class MpiSupport {
  public:
-  static void setMpiParallelDim(int /*nx*/, int /*ny*/, int /*nz*/) {}
-  static MpiSupport& instance() {
+  /// False: this library is not built with MPI (the reference's answer when
+  /// it is compiled without it, mpi_support.h:27-30).
+  static bool init(int /*argc*/ = 0, char** /*argv*/ = nullptr) { return false; }
+  static bool setMpiParallelDim(int /*nx*/, int /*ny*/, int /*nz*/) { return true; }
+  static int globalRank() { return 0; }
+  static int globalSize() { return 1; }
+  static MpiSupport& instance(int /*argc*/ = 0, char** /*argv*/ = nullptr) {
     static MpiSupport s;
     return s;
   }
@@ -798,6 +998,8 @@ class MpiSupport {
   int rank() const { return 0; }
   int size() const { return 1; }
   void barrier() const {}
+  /// Ends the process with the code, as MPI_Abort does for one rank.
+  [[noreturn]] void abort(int error_code) const { std::exit(error_code); }
 };
 
 // ------------------------------------------------------- flag visitors
@@ -882,6 +1084,9 @@ class Simulation {
 
   const EMF& emf() const { return _emf; }
   Real dt() const { return _dt; }
+  /// The run's time axis once init() or run() has set it up (null before):
+  /// dt, the step count and the current step, which advances with the run.
+  const std::shared_ptr<CalculationParam>& calculationParam() const { return _calc; }
   std::array<Index, 3> gridSize() const { return {_n[0], _n[1], _n[2]}; }
   xfd_engine* engine() const { return _engine; }
 
@@ -938,6 +1143,7 @@ class Simulation {
   std::vector<std::shared_ptr<Network>> _networks;
   std::vector<std::shared_ptr<SimulationFlagVisitor>> _visitors;
   long long _chunk = 32;  // steps per visitor NextStep (the engine's graph chunk)
+  std::shared_ptr<CalculationParam> _calc;
   EMF _emf;
   Real _dt = 0;
   Index _n[3] = {0, 0, 0};

@@ -1268,25 +1268,30 @@ xarray<T> linspace(T start, T stop, std::size_t num = 50, bool endpoint = true) 
   return out;
 }
 // arange(start, stop, step): start + i * step while below stop (above, for a
-// negative step).
-template <class T, class A, class B, class C>
-xarray<T> arange(A start, B stop, C step) {
-  std::vector<T> v;
-  const T a = (T)start, b = (T)stop, s = (T)step;
+// negative step).  The value type is the explicit template argument, else the
+// common type of the arguments.
+namespace detail {
+template <class T, class... A>
+using arange_t = std::conditional_t<std::is_void_v<T>, std::common_type_t<A...>, T>;
+}
+template <class T = void, class A, class B, class C>
+xarray<detail::arange_t<T, A, B, C>> arange(A start, B stop, C step) {
+  using R = detail::arange_t<T, A, B, C>;
+  const R a = (R)start, b = (R)stop, s = (R)step;
   const std::size_t n =
-      s > T(0) ? (b > a ? (std::size_t)std::ceil((double)(b - a) / (double)s) : 0)
+      s > R(0) ? (b > a ? (std::size_t)std::ceil((double)(b - a) / (double)s) : 0)
                : (a > b ? (std::size_t)std::ceil((double)(a - b) / (double)(-s)) : 0);
-  xarray<T> out = xarray<T>::from_shape(shape_type{n});
-  for (std::size_t i = 0; i < n; ++i) out.data()[i] = (T)(a + (T)i * s);
+  xarray<R> out = xarray<R>::from_shape(shape_type{n});
+  for (std::size_t i = 0; i < n; ++i) out.data()[i] = (R)(a + (R)i * s);
   return out;
 }
-template <class T, class A, class B>
-xarray<T> arange(A start, B stop) {
-  return arange<T>(start, stop, 1);
+template <class T = void, class A, class B>
+xarray<detail::arange_t<T, A, B>> arange(A start, B stop) {
+  return arange<detail::arange_t<T, A, B>>(start, stop, 1);
 }
-template <class T, class B>
-xarray<T> arange(B stop) {
-  return arange<T>(0, stop, 1);
+template <class T = void, class B>
+xarray<detail::arange_t<T, B>> arange(B stop) {
+  return arange<detail::arange_t<T, B>>(0, stop, 1);
 }
 
 // xtuple: the operands of concatenate / stack.

@@ -5,7 +5,7 @@
 // engine can be pinned against the reference itself.
 //
 //   xfd_ref_driver SCENE_TEXT OUT_DIR [--steps N] [--threads C]
-//                  [--far-field N_THETA PHI] [--time-only]
+//                  [--far-field N_THETA PHI] [--time-only] [--coefficients]
 //
 // The scene text is the line format xfdtd_core_b200/scene.py writes (one
 // object / source / boundary / monitor per line).  Every line is turned into
@@ -17,19 +17,26 @@
 //   <movie>/NNNNN.npy         movie frames, written by the reference's MovieMonitor
 //   <field_time>/<name>.npy   written by the reference's FieldTimeMonitor::output
 //   fd/<sub>/...              NFFFTFrequencyDomain::processFarField (with --far-field)
+//   fd/power.npy              NFFFTFrequencyDomain::outputRadiationPower
+//   line/<name>.npy           VoltageMonitor / CurrentMonitor::output
+//   network/s<ji>.npy         Network::output (with frequencies.npy)
 //   time.txt                  "run_s steps update_s" then one line per step with
 //                             its seconds: Simulation::run's wall time, and the
 //                             time loop alone (UpdateStart .. UpdateEnd) and each
 //                             step (NextStep to NextStep) from a SimulationFlagVisitor
 //                             (with --time-only nothing else is written)
+//   coef/<name>.npy           with --coefficients: the 18 update-coefficient
+//                             arrays (cexe .. chzey) as the run left them
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <filesystem>
 #include <fstream>
 #include <iostream>
 #include <limits>
+#include <map>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -37,6 +44,8 @@
 #include <xtensor/xnpy.hpp>
 
 #include "xfdtd/boundary/pml.h"
+#include "xfdtd/object/thin_wire.h"
+#include "xfdtd/shape/cylinder.h"
 #include "xfdtd/common/constant.h"
 #include "xfdtd/common/type_define.h"
 #include "xfdtd/coordinate_system/coordinate_system.h"
@@ -47,12 +56,20 @@
 #include "xfdtd/monitor/field_time_monitor.h"
 #include "xfdtd/monitor/movie_monitor.h"
 #include "xfdtd/nffft/nffft_frequency_domain.h"
+#include "xfdtd/monitor/current_monitor.h"
+#include "xfdtd/monitor/voltage_monitor.h"
+#include "xfdtd/network/network.h"
+#include "xfdtd/network/port.h"
+#include "xfdtd/object/lumped_element/capacitor.h"
 #include "xfdtd/object/lumped_element/current_source.h"
+#include "xfdtd/object/lumped_element/inductor.h"
+#include "xfdtd/object/lumped_element/resistor.h"
 #include "xfdtd/object/lumped_element/voltage_source.h"
 #include "xfdtd/object/object.h"
 #include "xfdtd/parallel/parallelized_config.h"
 #include "xfdtd/shape/cube.h"
 #include "xfdtd/shape/sphere.h"
+#include "xfdtd/calculation_param/calculation_param.h"
 #include "xfdtd/simulation/simulation.h"
 #include "xfdtd/simulation/simulation_flag.h"
 #include "xfdtd/waveform/waveform.h"
@@ -177,7 +194,7 @@ int main(int argc, char** argv) {
   int threads = 1;
   int n_theta = 0;
   double ff_phi = 0.0;
-  bool time_only = false;
+  bool time_only = false, coefficients = false;
   for (int a = 3; a < argc; ++a) {
     const std::string o = argv[a];
     if (o == "--steps" && a + 1 < argc) steps_override = std::stoll(argv[++a]);
@@ -186,6 +203,7 @@ int main(int argc, char** argv) {
       n_theta = std::stoi(argv[++a]);
       ff_phi = std::stod(argv[++a]);
     } else if (o == "--time-only") time_only = true;
+    else if (o == "--coefficients") coefficients = true;
     else die("unknown option " + o);
   }
   std::filesystem::create_directories(out);
@@ -215,6 +233,17 @@ int main(int argc, char** argv) {
   xfdtd::Simulation s{dl[0], dl[1], dl[2], cfl, xfdtd::ThreadConfig{1, 1, threads}};
   std::shared_ptr<xfdtd::NFFFTFrequencyDomain> nf2ff;
   std::vector<std::shared_ptr<xfdtd::FieldTimeMonitor>> time_monitors;
+  std::map<std::string, std::shared_ptr<xfdtd::VoltageMonitor>> v_monitors;
+  std::map<std::string, std::shared_ptr<xfdtd::CurrentMonitor>> c_monitors;
+  std::vector<std::shared_ptr<xfdtd::Port>> ports;
+  std::vector<double> net_freqs;
+  bool have_network = false;
+  auto xyz = [](const std::string& a) {
+    if (a == "X") return xfdtd::Axis::XYZ::X;
+    if (a == "Y") return xfdtd::Axis::XYZ::Y;
+    if (a != "Z") die("bad axis " + a);
+    return xfdtd::Axis::XYZ::Z;
+  };
   for (const auto& t : lines) {
     const std::string& k = t[0];
     if (k == "xfdtd-scene" || k == "name" || k == "grid" || k == "steps") continue;
@@ -232,6 +261,14 @@ int main(int argc, char** argv) {
         die("bad shape " + t[2]);
       }
       s.addObject(std::make_shared<xfdtd::Object>(t[1], std::move(shape), material_at(t[1], t, mi)));
+    } else if (k == "thin_wire") {
+      if (t.size() != 8 || (t[7] != "X" && t[7] != "Y" && t[7] != "Z"))
+        die("bad thin_wire line");
+      const xfdtd::Axis axis = t[7] == "X" ? xfdtd::Axis::XP
+                               : t[7] == "Y" ? xfdtd::Axis::YP : xfdtd::Axis::ZP;
+      s.addObject(std::make_shared<xfdtd::ThinWire>(
+          t[1], std::make_unique<xfdtd::Cylinder>(
+                    xfdtd::Vector{num(t[2]), num(t[3]), num(t[4])}, num(t[5]), num(t[6]), axis)));
     } else if (k == "current_source" || k == "voltage_source") {
       std::size_t used = 0;
       auto w = waveform_at(t, 10, &used);
@@ -269,9 +306,45 @@ int main(int argc, char** argv) {
           (xfdtd::Index)std::stoul(t[1]), (xfdtd::Index)std::stoul(t[2]),
           (xfdtd::Index)std::stoul(t[3]), arr1(f), (out / "fd").string());
       s.addNF2FF(nf2ff);
+    } else if (k == "resistor" || k == "capacitor" || k == "inductor") {
+      if (t.size() != 10) die("bad " + k + " line");
+      if (k == "resistor")
+        s.addObject(std::make_shared<xfdtd::Resistor>(t[1], cube_at(t, 2), xyz(t[8]), num(t[9])));
+      else if (k == "capacitor")
+        s.addObject(std::make_shared<xfdtd::Capacitor>(t[1], cube_at(t, 2), xyz(t[8]), num(t[9])));
+      else
+        s.addObject(std::make_shared<xfdtd::Inductor>(t[1], cube_at(t, 2), xyz(t[8]), num(t[9])));
+    } else if (k == "voltage_monitor" || k == "current_monitor") {
+      if (t.size() != 9) die("bad " + k + " line");
+      const std::string dir = (out / "line").string();
+      if (k == "voltage_monitor") {
+        auto m = std::make_shared<xfdtd::VoltageMonitor>(t[1], cube_at(t, 2), direction(t[8]), dir);
+        v_monitors[t[1]] = m;
+        s.addMonitor(m);
+      } else {
+        auto m = std::make_shared<xfdtd::CurrentMonitor>(t[1], cube_at(t, 2), direction(t[8]), dir);
+        c_monitors[t[1]] = m;
+        s.addMonitor(m);
+      }
+    } else if (k == "network") {
+      const std::size_t n = (std::size_t)std::stoul(t[1]);
+      if (t.size() != 2 + n) die("bad network line");
+      for (std::size_t q = 0; q < n; ++q) net_freqs.push_back(num(t[2 + q]));
+      have_network = true;
+    } else if (k == "port") {
+      if (t.size() != 7 || !c_monitors.count(t[5]) || !v_monitors.count(t[6]))
+        die("bad port line");
+      ports.push_back(std::make_shared<xfdtd::Port>(
+          (std::size_t)std::stoul(t[1]), t[2] == "1", std::complex<double>{num(t[3]), num(t[4])},
+          c_monitors[t[5]], v_monitors[t[6]]));
     } else {
       die("scene line '" + k + "' is not supported by the reference driver");
     }
+  }
+  std::shared_ptr<xfdtd::Network> network;
+  if (have_network) {
+    network = std::make_shared<xfdtd::Network>(ports, arr1(net_freqs), (out / "network").string());
+    s.addNetwork(network);
   }
 
   auto step_clock = std::make_shared<StepClock>();
@@ -296,6 +369,25 @@ int main(int argc, char** argv) {
   xt::dump_npy((out / "hy.npy").string(), emf->hy());
   xt::dump_npy((out / "hz.npy").string(), emf->hz());
   for (auto& m : time_monitors) m->output();
+  for (auto& [n, m] : v_monitors) m->output();
+  for (auto& [n, m] : c_monitors) m->output();
+  if (network) network->output();
+  if (coefficients) {
+    const auto& c = s.calculationParam()->fdtdCoefficient();
+    const auto d = out / "coef";
+    std::filesystem::create_directories(d);
+    auto put = [&](const char* n, const auto& a) { xt::dump_npy((d / n).string() + ".npy", a); };
+    put("cexe", c->cexe()); put("cexhy", c->cexhy()); put("cexhz", c->cexhz());
+    put("ceye", c->ceye()); put("ceyhz", c->ceyhz()); put("ceyhx", c->ceyhx());
+    put("ceze", c->ceze()); put("cezhx", c->cezhx()); put("cezhy", c->cezhy());
+    put("chxh", c->chxh()); put("chxey", c->chxey()); put("chxez", c->chxez());
+    put("chyh", c->chyh()); put("chyez", c->chyez()); put("chyex", c->chyex());
+    put("chzh", c->chzh()); put("chzex", c->chzex()); put("chzey", c->chzey());
+  }
+  if (nf2ff) {  // NFFFTFrequencyDomain::outputRadiationPower -> fd/power.npy
+    nf2ff->setOutputDir((out / "fd").string());
+    nf2ff->outputRadiationPower();
+  }
   if (nf2ff && n_theta > 0) {
     nf2ff->setOutputDir((out / "fd").string());
     nf2ff->processFarField(

@@ -181,6 +181,12 @@ class _Cube:
 def wrapped_cube(shape) -> _Cube:
     if shape.kind == "cube":
         return _Cube(shape.origin, shape.size)
+    if shape.kind == "cylinder":
+        # Cylinder::wrappedCube (src/shape/cylinder.cpp:72-98)
+        c = np.array(shape.origin, dtype=np.float64)
+        half = np.array([shape.radius] * 3)
+        half[shape.axis] = shape.height / 2
+        return _Cube(c - half, 2 * half)
     c = np.array(shape.origin, dtype=np.float64)
     r = shape.radius
     # Sphere::wrappedCube (src/shape/sphere.cpp:34-37)
@@ -199,6 +205,18 @@ def inside(shape, x, y, z, eps):
         dx, dy, dz = x - c[0], y - c[1], z - c[2]
         d = np.sqrt(dx * dx + dy * dy + dz * dz)
         return float_le(d, shape.radius, eps)
+    if shape.kind == "cylinder":
+        # Cylinder::isInside (src/shape/cylinder.cpp:44-66): inside the wrapped
+        # cube, then within the radius of the axis (floatCompare's 1e-8)
+        cb = wrapped_cube(shape)
+        box = (float_le(cb.origin[0], x, eps) & float_le(x, cb.end[0], eps) &
+               float_le(cb.origin[1], y, eps) & float_le(y, cb.end[1], eps) &
+               float_le(cb.origin[2], z, eps) & float_le(z, cb.end[2], eps))
+        c = shape.origin
+        d = [x - c[0], y - c[1], z - c[2]]
+        u, v = [(1, 2), (0, 2), (0, 1)][shape.axis]
+        dis = np.sqrt(d[u] ** 2 + d[v] ** 2)
+        return box & float_le(dis, shape.radius, 1e-8)
     cb = _Cube(shape.origin, shape.size)
     return (float_le(cb.origin[0], x, eps) & float_le(x, cb.end[0], eps) &
             float_le(cb.origin[1], y, eps) & float_le(y, cb.end[1], eps) &
@@ -248,7 +266,9 @@ class RefSimulation:
     def _grid(self):
         sc = self.scene
         dx, dy, dz = sc.dl
-        shapes = [o.shape for o in sc.objects] + [c.shape for c in sc.current_sources] + \
+        shapes = [o.shape for o in sc.objects] + \
+            [w.shape for w in getattr(sc, "thin_wires", [])] + \
+            [c.shape for c in sc.current_sources] + \
             [c.shape for c in getattr(sc, "lumped_elements", [])] + \
             [c.shape for c in getattr(sc, "pec_planes", [])]
         lo = np.full(3, np.finfo(np.float64).max)
@@ -327,6 +347,9 @@ class RefSimulation:
         painters = [(o.shape, o.material) for o in self.scene.objects]
         voxels = [o if hasattr(o, "voxel_index") else None for o in self.scene.objects]
         from_air = __import__("xfdtd_core_b200.scene", fromlist=["air"]).air
+        wires = list(getattr(self.scene, "thin_wires", []))
+        painters += [(w.shape, from_air()) for w in wires]
+        voxels += [None] * len(wires)
         lumped = list(self.scene.current_sources) + list(getattr(self.scene, "lumped_elements", []))
         painters += [(c.shape, from_air()) for c in lumped]
         voxels += [None] * len(lumped)
@@ -458,6 +481,53 @@ class RefSimulation:
             che_b.append(np.ascontiguousarray(chceb))
         self.ce, self.ceh_a, self.ceh_b = ce, ceh_a, ceh_b
         self.ch, self.che_a, self.che_b = ch, che_a, che_b
+
+    # ------------------------------------------------------------ thin wires
+    def _thin_wires(self):
+        """ThinWire::init / correctUpdateCoefficient (src/object/thin_wire.cpp:12-152):
+        on the wire's nodes the E along the wire gets ce = ceh_a = ceh_b = 0;
+        the H coefficients the reference scales next to the wire take
+        k 2 / ln(d / r): chyex, chzex for an x wire; chzey, chxey for y;
+        chxey, chyex for z."""
+        dx, dy, dz = self.based
+        for w in getattr(self.scene, "thin_wires", []):
+            sh = w.shape
+            ax, r = sh.axis, sh.radius
+            u, v = (ax + 1) % 3, (ax + 2) % 3
+            if not (r < self.based[u] / 2 and r < self.based[v] / 2):
+                raise ValueError("ThinWire::init: wire is not thin enough")
+            (i_s, j_s, k_s), (i_e, j_e, k_e) = self.grid_box(sh)
+            if ax == 0:
+                sl = (slice(i_s, i_e), j_s, k_s)
+            elif ax == 1:
+                sl = (i_s, slice(j_s, j_e), k_s)
+            else:
+                sl = (i_s, j_s, slice(k_s, k_e))
+            for arr in (self.ce, self.ceh_a, self.ceh_b):
+                arr[ax][sl] = 0
+            # che_a / che_b of component c multiply E_{c+1} / E_{c+2}:
+            # chxey = che_a[0], chyex = che_b[1], chzex = che_a[2], chzey = che_b[2]
+            if ax == 0:
+                khy = dz * math.atan(dy / dy) / dy
+                khz = dy * math.atan(dz / dy) / dz
+                v1 = self.che_b[1][i_s:i_e, j_s, k_s - 1:k_s + 1]
+                self.che_b[1][i_s:i_e, j_s, k_s - 1:k_s + 1] = khy * 2 * v1 / math.log(dz / r)
+                v2 = self.che_a[2][i_s:i_e, j_s - 1:j_s + 1, k_s]
+                self.che_a[2][i_s:i_e, j_s - 1:j_s + 1, k_s] = khz * 2 * v2 / math.log(dy / r)
+            elif ax == 1:
+                khz = dx * math.atan(dz / dx) / dz
+                khx = dz * math.atan(dx / dz) / dx
+                v1 = self.che_b[2][i_s - 1:i_s + 1, j_s:j_e, k_s]
+                self.che_b[2][i_s - 1:i_s + 1, j_s:j_e, k_s] = khz * 2 * v1 / math.log(dx / r)
+                v2 = self.che_a[0][i_s, j_s:j_e, k_s - 1:k_s + 1]
+                self.che_a[0][i_s, j_s:j_e, k_s - 1:k_s + 1] = khx * 2 * v2 / math.log(dz / r)
+            else:
+                khx = dy * math.atan(dx / dy) / dx
+                khy = dx * math.atan(dy / dx) / dy
+                v1 = self.che_a[0][i_s, j_s - 1:j_s + 1, k_s:k_e]
+                self.che_a[0][i_s, j_s - 1:j_s + 1, k_s:k_e] = khx * 2 * v1 / math.log(dy / r)
+                v2 = self.che_b[1][i_s - 1:i_s + 1, j_s, k_s:k_e]
+                self.che_b[1][i_s - 1:i_s + 1, j_s, k_s:k_e] = khy * 2 * v2 / math.log(dx / r)
 
     # ------------------------------------------------------- current sources
     def _current_sources(self):
@@ -1048,6 +1118,31 @@ class RefSimulation:
                 out[fi, row] = acc
         return out
 
+    def radiation_power(self) -> np.ndarray:
+        """Radiated power per frequency: FDPlaneData::power / calculatePower
+        (src/nffft/nffft_fd_data_process.cpp:38-190), 0.5 Re of the sum over
+        the faces XN..ZP of (-1 on the negative faces) sum ds (conj(J_a) M_b -
+        conj(J_b) M_a), ds the E-cell sizes across the face."""
+        nf = self.nf2ff
+        out = np.zeros(nf["nf"])
+        for fi in range(nf["nf"]):
+            total = 0j
+            for face in range(6):
+                if nf["tasks"][face] is None:
+                    continue
+                s, e = nf["tasks"][face]
+                m = face // 2
+                A, B = (m + 1) % 3, (m + 2) % 3
+                ja, jb, ma, mb = (self.nf2ff_surface(fi, face, q).ravel() for q in range(4))
+                ii, jj, kk = np.meshgrid(np.arange(s[0], e[0]), np.arange(s[1], e[1]),
+                                         np.arange(s[2], e[2]), indexing="ij")
+                idx = [ii.ravel(), jj.ravel(), kk.ravel()]
+                ds = self.e_size[A][idx[A]] * self.e_size[B][idx[B]]
+                acc = np.sum(ds * (np.conj(ja) * mb - np.conj(jb) * ma))
+                total += (-1.0 if face % 2 == 0 else 1.0) * acc
+            out[fi] = 0.5 * total.real
+        return out
+
     def nf2ff_surface(self, f: int, face: int, q: int) -> Optional[np.ndarray]:
         """Complex accumulator (ja, jb, ma, mb) of frequency f on face d, shaped
         like the face task."""
@@ -1189,7 +1284,9 @@ class RefSimulation:
         self._materials()
         self._coefficients()
         # Simulation::correctUpdateCoefficient (simulation.cpp:638-652):
-        # objects (lumped) -> boundaries (PML) -> sources -> dispersive space.
+        # objects (thin wires, lumped) -> boundaries (PML) -> sources ->
+        # dispersive space.
+        self._thin_wires()
         self._current_sources()
         self._pml()
         self._tfsf()

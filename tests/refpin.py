@@ -18,9 +18,18 @@ def available() -> bool:
     return os.access(DRIVER, os.X_OK)
 
 
+COEFFICIENTS = ("cexe", "cexhy", "cexhz", "ceye", "ceyhz", "ceyhx", "ceze", "cezhx", "cezhy",
+                "chxh", "chxey", "chxez", "chyh", "chyez", "chyex", "chzh", "chzex", "chzey")
+
+
 def run(scene, out_dir: str, steps: int | None = None, threads: int = 1,
-        far_field: tuple | None = None, timeout: float = 1800) -> dict:
-    """far_field = (n_theta, phi): processFarField over linspace(-pi, pi, n_theta)."""
+        far_field: tuple | None = None, timeout: float = 1800,
+        coefficients: bool = False) -> dict:
+    """far_field = (n_theta, phi): processFarField over linspace(-pi, pi, n_theta).
+    coefficients: also the 18 update-coefficient arrays as the run left them
+    (out["coefficients"], in the order of COEFFICIENTS).  Voltage / current
+    monitor series land in out["lines"], the network's S-parameters in
+    out["s"] (keyed 10 j + i) and the radiated power in out["power"]."""
     os.makedirs(out_dir, exist_ok=True)
     path = os.path.join(out_dir, "scene.txt")
     scene.write(path)
@@ -29,6 +38,8 @@ def run(scene, out_dir: str, steps: int | None = None, threads: int = 1,
         cmd += ["--steps", str(steps)]
     if far_field is not None:
         cmd += ["--far-field", str(int(far_field[0])), repr(float(far_field[1]))]
+    if coefficients:
+        cmd += ["--coefficients"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"reference driver failed: {r.stderr[-2000:]}")
@@ -40,6 +51,16 @@ def run(scene, out_dir: str, steps: int | None = None, threads: int = 1,
     for ft in scene.field_times:
         out.setdefault("field_times", {})[ft.name] = np.load(
             os.path.join(out_dir, "field_time", f"{ft.name}.npy"))
+    if coefficients:
+        out["coefficients"] = [np.load(os.path.join(out_dir, "coef", f"{n}.npy"))
+                               for n in COEFFICIENTS]
+    for f in glob.glob(os.path.join(out_dir, "line", "*.npy")):
+        out.setdefault("lines", {})[os.path.basename(f)[:-4]] = np.load(f)
+    for f in glob.glob(os.path.join(out_dir, "network", "s*.npy")):
+        out.setdefault("s", {})[int(os.path.basename(f)[1:-4])] = np.load(f)
+    power = os.path.join(out_dir, "fd", "power.npy")
+    if scene.nf2ff is not None and os.path.exists(power):
+        out["power"] = np.load(power)
     if far_field is not None and scene.nf2ff is not None:
         ff = []
         for f in scene.nf2ff.freqs:

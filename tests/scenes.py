@@ -94,3 +94,28 @@ def microstrip_small(steps=150, **kw):
 ALL = {"sphere": sphere_small, "boxes": boxes_small, "dispersive": dispersive_small,
        "dispersive_stable": dispersive_stable_small, "voxels": voxels_small,
        "lumped": lumped_small, "microstrip": microstrip_small}
+
+
+def wires_small(steps=120, n=30, pml=6, dl=1e-3):
+    """Thin wires along all three axes in a CPML-bounded air box: a z dipole
+    fed by a 50-ohm voltage source in its gap, an x wire and a y wire off to
+    the sides (each with the radius below half a cell), a Gaussian voltage,
+    and an NF2FF surface at two frequencies."""
+    import math
+    interior = n - 2 * pml
+    half = interior * dl / 2
+    sc = S.Scene(dl=(dl, dl, dl), cfl=0.9, steps=steps, name="wires")
+    sc.objects.append(S.ObjectSpec("domain", S.cube((-half,) * 3, (2 * half,) * 3), S.air()))
+    sc.thin_wires += [
+        S.ThinWireSpec("z_up", S.cylinder((0.0, 0.0, 3.5 * dl), 1e-4, 5 * dl, 2)),
+        S.ThinWireSpec("z_dn", S.cylinder((0.0, 0.0, -3.5 * dl), 1e-4, 5 * dl, 2)),
+        S.ThinWireSpec("x_w", S.cylinder((0.0, 5 * dl, -2 * dl), 2e-4, 6 * dl, 0)),
+        S.ThinWireSpec("y_w", S.cylinder((-5 * dl, 0.0, 2 * dl), 5e-5, 6 * dl, 1)),
+    ]
+    tau = 20 * dl / 6e8
+    sc.current_sources.append(S.VoltageSourceSpec(
+        "v_s", S.cube((0.0, 0.0, -dl), (0.0, 0.0, 2 * dl)), "ZP", 50.0,
+        S.Waveform("gaussian", tau, 4.5 * tau)))
+    sc.pmls = S.pml_all(pml)
+    sc.nf2ff = S.NF2FFSpec((3, 3, 3), [2e10, 5e10])
+    return sc

@@ -331,3 +331,47 @@ def test_wide_interior_form_matches_oracle(precision, tol):
     for key in ("one-row", "one-list"):
         for a, b in zip(got["wide"], got[key]):
             assert rel_l2(a, b) <= (1e-14 if precision == 0 else 1e-6), key
+
+
+@pytest.mark.parametrize("opts", [pytest.param({}, id="default"),
+                                  pytest.param({"kernel": 0}, id="split"),
+                                  pytest.param({"kernel": 3}, id="march"),
+                                  pytest.param({"kernel": 4}, id="march-tma")])
+def test_thin_wires_match_oracle(opts):
+    """ThinWire along x, y and z beside a voltage-fed gap: the E along each
+    wire held at zero by its class, the scaled H curl terms by the engine's
+    H-term pass between the H and E sweeps (xfd_set_h_term_overrides).
+    Fields and NF2FF surface currents within 1e-12 after 150 steps, on every
+    split sweep."""
+    from tests.scenes import wires_small
+    sc = wires_small(steps=150)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc, options=opts)
+    run.run()
+    errs = _fields_rel(run, orc)
+    assert max(errs) <= TOL64, errs
+    got = run.nf2ff()
+    acc = orc.nf2ff["acc"]
+    want = acc[0::2] + 1j * acc[1::2]
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= TOL64
+    run.close()
+
+
+def test_thin_wires_fp32_and_fused_sweeps_refused():
+    """The FP32 form of the thin-wire scene within 1e-4 of the FP64 oracle
+    (relative to the largest field); the fused sweeps, which cannot run the
+    H-term pass between H and E, are refused once the wires are set."""
+    from tests.scenes import wires_small
+    from xfdtd_core_b200.host import HostError
+    sc = wires_small(steps=150)
+    orc = RefSimulation(sc)
+    orc.run()
+    run = SceneRun(sc, precision=1)
+    run.run()
+    assert max(_fields_rel(run, orc)) <= 1e-4
+    assert run.get_engine_option("kernel") in (0, 3, 4)
+    for mode in (1, 2, 5, 6, 7):
+        with pytest.raises(HostError):
+            run.set_engine_option("kernel", mode)
+    run.close()

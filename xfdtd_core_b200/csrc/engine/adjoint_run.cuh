@@ -552,10 +552,11 @@ xfd_status xfd_adjoint_run(xfd_engine* e, const xfd_adjoint_desc* d, double* val
   if (d->obj_field < 0 || d->obj_field > 2 || !box_ok(e->L, d->obj_s, d->obj_e) ||
       (!d->forward_only && !box_ok(e->L, d->design_s, d->design_e)))
     return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad objective field or node box");
-  if (e->ade_kind >= 0 || e->have_nf2ff || e->have_td || !e->movies.empty() || !e->ind_h.empty())
+  if (e->ade_kind >= 0 || e->have_nf2ff || e->have_td || !e->movies.empty() ||
+      !e->ind_h.empty() || e->n_hterm)
     return fail(e, XFD_ERR_UNSUPPORTED,
                 "the adjoint covers CPML, TFSF and lumped sources; not ADE media, inductors, "
-                "NF2FF or movies");
+                "thin wires, NF2FF or movies");
   CUDA_TRY(e, cudaSetDevice(e->device));
   xfd_status s = ensure_ready(e);
   if (s == XFD_OK && !e->tma_ready)

@@ -412,7 +412,7 @@ xfd_status xfd_batch_create(xfd_engine* const* engines, int32_t n, xfd_batch** o
       return bfail(nullptr, XFD_ERR_INVALID_ARGUMENT,
                    "engine %d: all batched engines need one device and one precision", s);
     if (e->ade_kind >= 0 || !e->lumped_h.empty() || !e->movies.empty() || e->have_nf2ff ||
-        e->have_td || e->n_ovr || e->pr_begin.size() > 1 || !e->ind_h.empty())
+        e->have_td || e->n_ovr || e->n_hterm || e->pr_begin.size() > 1 || !e->ind_h.empty())
       return bfail(nullptr, XFD_ERR_UNSUPPORTED,
                    "engine %d: ADE media, lumped sources and inductors, movies, NF2FF, probes "
                    "and coefficient overrides are not batched", s);

@@ -9,11 +9,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -111,6 +113,9 @@ struct xfd_engine {
   std::vector<int32_t> ovr_node;  // 3 per entry
   std::vector<uint8_t> ovr_comp;
   std::vector<double> ovr_ca, ovr_cb;
+  long long n_hterm = 0;  // H curl-term corrections (xfd_set_h_term_overrides)
+  HTermD<double> hterm64{};
+  HTermD<float> hterm32{};
 
   int ade_kind = -1;
   AdeD<double> ade64{};
@@ -951,6 +956,11 @@ OverrideD<T> ovr_of(const xfd_engine* e) {
   if constexpr (sizeof(T) == 8) return e->ovr64; else return e->ovr32;
 }
 
+template <typename T>
+HTermD<T> hterm_of(const xfd_engine* e) {
+  if constexpr (sizeof(T) == 8) return e->hterm64; else return e->hterm32;
+}
+
 // Launches one time step (host step index t decides the periodic kernels).
 // Sweep 7, one step from buffer `in` to `out`: the fused box kernel (side
 // stream 0) beside the CPML form's H tile lists and the H lattice faces (main
@@ -1284,6 +1294,8 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
     else
       k_update_h<T><<<grd, blk, 0, s>>>(yp);
+    if (e->n_hterm)
+      k_hterm<T><<<blocks_for(e->n_hterm, 256), 256, 0, s>>>(hterm_of<T>(e), e->L, fields);
     if (e->have_tfsf) {
       for (int g = 0; g < 2; ++g) {
         const auto& G = e->tfsf_groups[g];
@@ -1835,6 +1847,60 @@ xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, co
   e->ovr_ca.assign(ca, ca + n);
   e->ovr_cb.assign(cb, cb + n);
   e->n_ovr = n;
+  e->graph_dirty = true;
+  return XFD_OK;
+}
+
+xfd_status xfd_set_h_term_overrides(xfd_engine* e, int64_t n, const int32_t* node,
+                                    const int32_t* comp, const double* delta_a,
+                                    const double* delta_b) {
+  if (!e || n < 0 || (n > 0 && (!node || !comp || !delta_a || !delta_b)))
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad H term arguments");
+  if (e->n_hterm) return fail(e, XFD_ERR_STATE, "H term corrections already set");
+  if (n == 0) return XFD_OK;
+  const int nn[3] = {e->L.nx, e->L.ny, e->L.nz};
+  std::vector<long long> id((size_t)n);
+  std::vector<uint8_t> cm((size_t)n);
+  std::set<std::pair<long long, int>> seen;
+  for (int64_t q = 0; q < n; ++q) {
+    const int c = comp[q];
+    const int* x = node + 3 * q;
+    bool ok = c >= 0 && c <= 2 && std::isfinite(delta_a[q]) && std::isfinite(delta_b[q]);
+    for (int d = 0; d < 3 && ok; ++d) ok = x[d] >= 0 && x[d] < nn[d];  // main H range
+    if (!ok) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad H term entry %lld", (long long)q);
+    id[(size_t)q] = lat_index(e->L, x[0], x[1], x[2]);
+    cm[(size_t)q] = (uint8_t)c;
+    if (!seen.emplace(id[(size_t)q], c).second)
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "H term entry %lld repeats a node", (long long)q);
+  }
+  // The correction runs between a split sweep's H and E phases.
+  if (e->kernel_mode == 7) {
+    xfd_status st = xfd_set_option(e, "kernel", 4);
+    if (st != XFD_OK) return st;
+  } else if (is_pingpong(e)) {
+    xfd_status st = xfd_set_option(e, "kernel", 0);
+    if (st != XFD_OK) return st;
+  }
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  xfd_status s;
+  long long* dn = nullptr;
+  uint8_t* dc = nullptr;
+  if ((s = upload_raw(e, &dn, id.data(), id.size())) != XFD_OK) return s;
+  if ((s = upload_raw(e, &dc, cm.data(), cm.size())) != XFD_OK) return s;
+  if (e->precision == XFD_FP64) {
+    double *da = nullptr, *db = nullptr;
+    if ((s = upload_raw(e, &da, delta_a, (size_t)n)) != XFD_OK) return s;
+    if ((s = upload_raw(e, &db, delta_b, (size_t)n)) != XFD_OK) return s;
+    e->hterm64 = HTermD<double>{n, dn, dc, da, db};
+  } else {
+    std::vector<float> fa(delta_a, delta_a + n), fb(delta_b, delta_b + n);
+    float *da = nullptr, *db = nullptr;
+    if ((s = upload_raw(e, &da, fa.data(), fa.size())) != XFD_OK) return s;
+    if ((s = upload_raw(e, &db, fb.data(), fb.size())) != XFD_OK) return s;
+    e->hterm32 = HTermD<float>{n, dn, dc, da, db};
+  }
+  CUDA_TRY(e, cudaStreamSynchronize(e->stream));
+  e->n_hterm = n;
   e->graph_dirty = true;
   return XFD_OK;
 }
@@ -2581,6 +2647,10 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
   } else if (!strcmp(name, "kernel")) {
     if (value < 0 || value > 7)
       return fail(e, XFD_ERR_UNSUPPORTED, "kernel mode %lld", (long long)value);
+    if (e->n_hterm && (value == 1 || value == 2 || value >= 5))
+      return fail(e, XFD_ERR_UNSUPPORTED,
+                  "kernel mode %lld: H curl-term corrections need a split H/E sweep (0, 3, 4)",
+                  (long long)value);
     const int before = psi_h_buf(e);
     const bool was_pp = is_pingpong(e);
     e->kernel_mode = (int)value;
@@ -2680,6 +2750,7 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (e->have_td) n += 1;
   if (e->probes.n_probes) n += 1;
   if (e->n_ovr) n += fused ? 1 : 2;
+  if (e->n_hterm) n += 1;
   return n + e->n_rec;
 }
 

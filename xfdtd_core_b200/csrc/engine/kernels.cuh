@@ -819,6 +819,38 @@ __global__ void k_ovr_apply(OverrideD<T> o, T* const* fields, T* const* fields_i
 }
 
 // ---------------------------------------------------------------------------
+// Per-node H curl-term corrections, for coefficients that scale one curl term
+// of an H node but not the other (ThinWire::correctUpdateCoefficient,
+// src/object/thin_wire.cpp:42-133, multiplies chxey / chyex / chzex / chzey
+// next to the wire).  The class table holds one cb per component, so the
+// sweep applies the unscaled pair and this pass adds the difference:
+//   H_c += da (E_a[x_b+1] - E_a) + db (E_b[x_a+1] - E_b)
+// with the E of the same step (the E sweep has not run yet); a = c+1,
+// b = c+2.  One entry per (node, component): no two threads write one value.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct HTermD {
+  long long n;
+  const long long* node;  // lattice index
+  const uint8_t* comp;    // 0..2: Hx Hy Hz
+  const T* da;
+  const T* db;
+};
+
+template <typename T>
+__global__ void k_hterm(const __grid_constant__ HTermD<T> h, Lat L, T* const* fields) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= h.n) return;
+  const int c = h.comp[q], a = (c + 1) % 3, b = (c + 2) % 3;
+  const long long st[3] = {(long long)L.NY * L.KP, (long long)L.KP, 1};
+  const long long id = h.node[q];
+  const T* Ea = fields[a];
+  const T* Eb = fields[b];
+  T* H = fields[3 + c];
+  H[id] += h.da[q] * (Ea[id + st[b]] - Ea[id]) + h.db[q] * (Eb[id + st[a]] - Eb[id]);
+}
+
+// ---------------------------------------------------------------------------
 // Time-domain NF2FF (NFFFTTimeDomain::update, src/nffft/nfffft_time_domain.cpp:80-96
 // -> TDPlaneData::update, src/include/nffft/nffft_td_data.h:169-240): per
 // Huygens point and step, the surface-centre tangential E and H

@@ -174,6 +174,15 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       }
       auto mat = parseMaterial(in, name);
       sc->sim->addObject(std::make_shared<Object>(name, std::move(sh), mat));
+    } else if (kw == "thin_wire") {
+      in >> name;
+      const double cx = num(in), cy = num(in), cz = num(in), r = num(in), h = num(in);
+      std::string ax;
+      in >> ax;
+      const Axis axis = ax == "X" ? Axis::XP : ax == "Y" ? Axis::YP : ax == "Z" ? Axis::ZP
+                        : throw XFDTDException("bad thin-wire axis '" + ax + "'");
+      sc->sim->addObject(std::make_shared<ThinWire>(
+          name, std::make_unique<Cylinder>(Vector{cx, cy, cz}, r, h, axis)));
     } else if (kw == "voxels") {
       in >> name;
       const double ox = num(in), oy = num(in), oz = num(in), sx = num(in), sy = num(in),

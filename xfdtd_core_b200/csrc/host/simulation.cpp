@@ -71,6 +71,42 @@ std::unique_ptr<Cube> Sphere::wrappedCube() const {
                                 Vector{_radius * 2, _radius * 2, _radius * 2});
 }
 
+Cylinder::Cylinder(Vector center, Real radius, Real height, Axis axis)
+    : _center{center}, _radius{radius}, _height{height}, _axis{axis} {
+  // Cylinder::Cylinder (src/shape/cylinder.cpp:13-26)
+  if (_radius < 0) throw XFDTDException("Cylinder radius must be positive");
+  if (_height < 0) throw XFDTDException("Cylinder height must be positive");
+}
+
+std::unique_ptr<Cube> Cylinder::wrappedCube() const {
+  // Cylinder::wrappedCube (src/shape/cylinder.cpp:72-98): height along the
+  // axis, 2 r across, centred on `center`.
+  const int w = _axis.axisIndex();
+  if (w < 0) throw XFDTDException("Cylinder axis is not supported");
+  Real o[3], sz[3];
+  for (int a = 0; a < 3; ++a) {
+    const Real half = a == w ? _height / 2 : _radius;
+    o[a] = _center(a) - half;
+    sz[a] = 2 * half;
+  }
+  return std::make_unique<Cube>(Vector{o[0], o[1], o[2]}, Vector{sz[0], sz[1], sz[2]});
+}
+
+bool Cylinder::isInside(Real x, Real y, Real z, Real eps) const {
+  // Cylinder::isInside (src/shape/cylinder.cpp:44-66): inside the wrapped
+  // cube and within the radius of the axis line (floatCompare's default
+  // tolerance, 1e-8, on the distance).
+  if (!wrappedCube()->isInside(x, y, z, eps)) return false;
+  const int w = _axis.axisIndex();
+  const Real p[3] = {x, y, z};
+  const int u = (w + 1) % 3, v = (w + 2) % 3;
+  const Real du = p[u] - _center(u), dv = p[v] - _center(v);
+  // the reference orders the two transverse axes (y, z), (x, z), (x, y)
+  const Real dis = w == 1 ? std::sqrt(std::pow(dv, 2) + std::pow(du, 2))
+                          : std::sqrt(std::pow(du, 2) + std::pow(dv, 2));
+  return floatLE(dis, _radius, 1e-8);
+}
+
 ElectroMagneticProperty::ElectroMagneticProperty(Real eps_r, Real mu_r, Real sigma_e,
                                                  Real sigma_m)
     : _eps_r{eps_r},
@@ -145,6 +181,23 @@ std::unique_ptr<MLorentzMaterial> MLorentzMaterial::makeMLorentz(
   return std::make_unique<MLorentzMaterial>(name, eps_inf, Kind::MLorentz, poles, native);
 }
 
+std::complex<Real> LinearDispersiveMaterial::susceptibility(Real freq, Index p) const {
+  const auto& c = _poles.at(p);  // a0 a1 b0 b1 b2
+  const std::complex<Real> jw = constant::II * (static_cast<Real>(2.0) * constant::PI * freq);
+  return (c[1] * jw + c[0]) / (c[4] * jw * jw + c[3] * jw + c[2]);
+}
+
+Array1D<std::complex<Real>> LinearDispersiveMaterial::relativePermittivity(
+    const Array1D<Real>& freq) const {
+  auto out = Array1D<std::complex<Real>>::from_shape({freq.size()});
+  for (std::size_t q = 0; q < freq.size(); ++q) {
+    std::complex<Real> sum{0, 0};
+    for (Index p = 0; p < numPoles(); ++p) sum += susceptibility(freq(q), p);
+    out(q) = _eps_inf + sum;
+  }
+  return out;
+}
+
 // ---------------------------------------------------------- waveform
 std::unique_ptr<Waveform> Waveform::gaussian(Real tau, Real t_0, Real amplitude) {
   return std::make_unique<Waveform>(
@@ -164,6 +217,34 @@ std::unique_ptr<Waveform> Waveform::cosineModulatedGaussian(Real tau, Real t_0, 
 std::unique_ptr<Waveform> Waveform::sine(Real frequency, Real amplitude) {
   return std::make_unique<Waveform>(
       [frequency](Real t) { return std::sin(2 * constant::PI * frequency * t); }, amplitude);
+}
+
+// src/waveform/waveform.cpp:47-101
+std::unique_ptr<Waveform> Waveform::cosine(Real frequency, Real amplitude) {
+  return std::make_unique<Waveform>(
+      [frequency](Real t) { return std::cos(2 * constant::PI * frequency * t); }, amplitude);
+}
+
+std::unique_ptr<Waveform> Waveform::square(Real frequency, Real amplitude) {
+  return std::make_unique<Waveform>(
+      [frequency](Real t) { return std::copysign(1.0, std::sin(2 * constant::PI * frequency * t)); },
+      amplitude);
+}
+
+std::unique_ptr<Waveform> Waveform::triangle(Real frequency, Real /*amplitude*/) {
+  return std::make_unique<Waveform>([frequency](Real t) {
+    return std::asin(std::sin(2 * constant::PI * frequency * t)) * 2 / constant::PI;
+  });
+}
+
+std::unique_ptr<Waveform> Waveform::sawtooth(Real frequency, Real amplitude) {
+  return std::make_unique<Waveform>(
+      [frequency](Real t) { return 2 * std::fmod(frequency * t, 1.0) - 1; }, amplitude);
+}
+
+std::unique_ptr<Waveform> Waveform::step(Real t_0, Real amplitude) {
+  return std::make_unique<Waveform>([t_0](Real t) { return static_cast<Real>(t >= t_0); },
+                                    amplitude);
 }
 
 void Waveform::init(const std::vector<Real>& time) {
@@ -278,6 +359,9 @@ struct Simulation::Impl {
     double w;
   };
   std::vector<OvrE> ovr;
+  // ThinWire H coefficient factors: (lattice node, H component) -> the
+  // factors on its two curl-term coefficients (che_a, che_b).
+  std::map<std::pair<Index, int>, std::array<double, 2>> hterm;
   // TFSF set-up kept for inspection (Simulation::tfsfTables)
   std::vector<double> tf_e_inc, tf_h_inc, tf_p_int[3], tf_p_half[3];
   int tf_aux = 0;
@@ -440,6 +524,7 @@ void Simulation::init(Index time_step) {
                                 1.0 / (I.min_d[1] * I.min_d[1]) +
                                 1.0 / (I.min_d[2] * I.min_d[2])));
   const Real dt = _dt;
+  _calc = std::make_shared<CalculationParam>(std::make_unique<TimeParam>(dt, time_step, 0));
   const Real eps_tol = std::min({I.min_d[0], I.min_d[1], I.min_d[2]}) / 1000;
   if (_objects.size() >= kNoCell) throw XFDTDException("too many objects");
 
@@ -697,7 +782,74 @@ void Simulation::init(Index time_step) {
             });
     }
   }
+  // ThinWire::init and ::correctUpdateCoefficient (src/object/thin_wire.cpp:12-133)
+  auto thinWire = [&](const ThinWire& tw) {
+    const auto* cyl = dynamic_cast<const Cylinder*>(tw.shape().get());
+    if (!cyl) throw XFDTDException("ThinWire::init: shape is not Cylinder");
+    const int w = cyl->axis().axisIndex();
+    if (w < 0) throw XFDTDException("ThinWire::init: invalid axis");
+    const Real r = cyl->radius();
+    const Real dx = _dl[0], dy = _dl[1], dz = _dl[2];
+    const int u = (w + 1) % 3, v = (w + 2) % 3;
+    if (!(r < _dl[u] / 2 && r < _dl[v] / 2))
+      throw XFDTDException("ThinWire::init: wire is not thin enough");
+    auto wc = cyl->wrappedCube();
+    Index gs[3], ge[3];
+    for (int a = 0; a < 3; ++a) {
+      gs[a] = nearestNode(I.e_node[a], wc->origin()(a));
+      ge[a] = nearestNode(I.e_node[a], wc->end()(a));
+    }
+    // E along the wire on its nodes: ce = ceh_a = ceh_b = 0.
+    const int tag = override_tag++;
+    for (Index t = gs[w]; t < ge[w]; ++t) {
+      Index x[3];
+      x[w] = t;
+      x[u] = gs[u];
+      x[v] = gs[v];
+      overrideClass(lat(x[0], x[1], x[2]), tag, [&](double* rw, double*) {
+        rw[2 * w] = 0;
+        rw[2 * w + 1] = 0;
+      });
+    }
+    // H coefficients next to the wire: (component, term a/b, node box, factor).
+    auto scale = [&](int c, int term, Index i0, Index i1, Index j0, Index j1, Index k0, Index k1,
+                     Real f) {
+      for (Index i = i0; i < i1; ++i)
+        for (Index j = j0; j < j1; ++j)
+          for (Index k = k0; k < k1; ++k) {
+            if (i >= _n[0] || j >= _n[1] || k >= _n[2])
+              throw XFDTDException("ThinWire " + tw.name() + " reaches the domain's far faces");
+            auto it = I.hterm.emplace(std::make_pair(lat(i, j, k), c),
+                                      std::array<double, 2>{1.0, 1.0}).first;
+            it->second[term] *= f;
+          }
+    };
+    const Index is = gs[0], ie = ge[0], js = gs[1], je = ge[1], ks = gs[2], ke = ge[2];
+    if (w == 0) {
+      const Real khy = dz * std::atan(dy / dy) / dy;
+      const Real khz = dy * std::atan(dz / dy) / dz;
+      if (ks < 1 || js < 1) throw XFDTDException("ThinWire on the domain's faces");
+      scale(1, 1, is, ie, js, js + 1, ks - 1, ks + 1, khy * 2 / std::log(dz / r));  // chyex
+      scale(2, 0, is, ie, js - 1, js + 1, ks, ks + 1, khz * 2 / std::log(dy / r));  // chzex
+    } else if (w == 1) {
+      const Real khz = dx * std::atan(dz / dx) / dz;
+      const Real khx = dz * std::atan(dx / dz) / dx;
+      if (is < 1 || ks < 1) throw XFDTDException("ThinWire on the domain's faces");
+      scale(2, 1, is - 1, is + 1, js, je, ks, ks + 1, khz * 2 / std::log(dx / r));  // chzey
+      scale(0, 0, is, is + 1, js, je, ks - 1, ks + 1, khx * 2 / std::log(dz / r));  // chxey
+    } else {
+      const Real khx = dy * std::atan(dx / dy) / dx;
+      const Real khy = dx * std::atan(dy / dx) / dy;
+      if (is < 1 || js < 1) throw XFDTDException("ThinWire on the domain's faces");
+      scale(0, 0, is, is + 1, js - 1, js + 1, ks, ke, khx * 2 / std::log(dy / r));  // chxey
+      scale(1, 1, is - 1, is + 1, js, js + 1, ks, ke, khy * 2 / std::log(dx / r));  // chyex
+    }
+  };
   for (const auto& o : _objects) {
+    if (auto tw = std::dynamic_pointer_cast<ThinWire>(o)) {
+      thinWire(*tw);
+      continue;
+    }
     auto le = std::dynamic_pointer_cast<LumpedElement>(o);
     if (!le) continue;
     auto cs = std::dynamic_pointer_cast<CurrentSource>(o);
@@ -1178,6 +1330,25 @@ void Simulation::init(Index time_step) {
                                        ob.data()),
                 "xfd_set_e_overrides");
   }
+  if (!I.hterm.empty()) {
+    // The scaled coefficient minus the one the class table applies.
+    std::vector<int32_t> hn, hc;
+    std::vector<double> ha, hb;
+    for (const auto& [key, f] : I.hterm) {
+      const Index node = key.first;
+      const int c = key.second, ta = (c + 1) % 3, tb = (c + 2) % 3;
+      const Index x[3] = {node / (NY * NZ), (node / NZ) % NY, node % NZ};
+      const double cb = I.table[12 * I.lattice_class[node] + 6 + 2 * c + 1];
+      const double che_a = cb * I.fh[tb][x[tb]], che_b = -cb * I.fh[ta][x[ta]];
+      for (int a = 0; a < 3; ++a) hn.push_back((int32_t)x[a]);
+      hc.push_back(c);
+      ha.push_back(f[0] * che_a - che_a);
+      hb.push_back(f[1] * che_b - che_b);
+    }
+    checkStatus(E, xfd_set_h_term_overrides(E, (int64_t)hc.size(), hn.data(), hc.data(),
+                                            ha.data(), hb.data()),
+                "xfd_set_h_term_overrides");
+  }
   const double* fe[3] = {I.fe[0].data(), I.fe[1].data(), I.fe[2].data()};
   const double* fh[3] = {I.fh[0].data(), I.fh[1].data(), I.fh[2].data()};
   checkStatus(E, xfd_set_curl_factors(E, fe, fh), "xfd_set_curl_factors");
@@ -1291,6 +1462,7 @@ void Simulation::setEngineOption(const std::string& name, long long value) {
 void Simulation::advance(Index n) {
   if (!_impl->initialised || !_engine) throw XFDTDException("Simulation not initialised");
   checkStatus(_engine, xfd_run(_engine, (int64_t)n), "xfd_run");
+  if (_calc) _calc->timeParam()->setCurrentTimeStep((std::size_t)xfd_current_step(_engine));
 }
 
 void Simulation::finish() {
@@ -1410,6 +1582,15 @@ std::vector<std::vector<Real>> Simulation::coefficientArrays() const {
               cb[q] = -b * I.fh[ta][x[ta]];
             }
           }
+      if (h == 1)
+        for (const auto& [key, f] : I.hterm) {
+          if (key.second != c) continue;
+          const Index node = key.first;
+          const Index x[3] = {node / (NY * NZ), (node / NZ) % NY, node % NZ};
+          const Index q = (x[0] * s[1] + x[1]) * s[2] + x[2];
+          ca[q] *= f[0];
+          cb[q] *= f[1];
+        }
       if (h == 0)
         for (const auto& o : I.ovr) {
           if (o.comp != c) continue;
@@ -2066,6 +2247,55 @@ void NFFFTFrequencyDomain::processFarField(Real theta, const Array1D<Real>& phi,
                                            const std::string& sub_dir,
                                            const Vector& origin) const {
   processFarField(Array1D<Real>{theta}, phi, sub_dir, origin);
+}
+
+std::vector<Real> NFFFTFrequencyDomain::radiationPower() const {
+  const std::size_t nf = _freqs.size();
+  std::size_t per_freq = 0, count[6];
+  for (int f = 0; f < 6; ++f) {
+    count[f] = 1;
+    for (int a = 0; a < 3; ++a) count[f] *= (std::size_t)std::max(0, faces[f][3 + a] - faces[f][a]);
+    per_freq += 4 * count[f];
+  }
+  if (nf == 0 || _acc.size() != nf * per_freq)
+    throw XFDTDException("radiation power: no surface currents (run the simulation first)");
+  std::vector<Real> out(nf);
+  for (std::size_t q = 0; q < nf; ++q) {
+    const std::complex<Real>* base = _acc.data() + q * per_freq;
+    std::complex<Real> total{0.0};
+    for (int f = 0; f < 6; ++f) {
+      const int m = f / 2, A = (m + 1) % 3, B = (m + 2) % 3;
+      const std::size_t n = count[f];
+      const std::complex<Real>*ja = base, *jb = base + n, *ma = base + 2 * n, *mb = base + 3 * n;
+      base += 4 * n;
+      if (n == 0) continue;
+      std::complex<Real> face{0.0};
+      std::size_t p = 0;
+      for (int i = faces[f][0]; i < faces[f][3]; ++i)
+        for (int j = faces[f][1]; j < faces[f][4]; ++j)
+          for (int k = faces[f][2]; k < faces[f][5]; ++k, ++p) {
+            const int x[3] = {i, j, k};
+            // ds: the E-cell sizes across the face (y z, z x, x y)
+            const Real ds = _size_e[A][x[A]] * _size_e[B][x[B]];
+            face += ds * (std::conj(ja[p]) * mb[p] - std::conj(jb[p]) * ma[p]);
+          }
+      total += (f % 2 == 0 ? -1.0 : 1.0) * face;
+    }
+    out[q] = 0.5 * std::real(total);
+  }
+  return out;
+}
+
+void NFFFTFrequencyDomain::outputRadiationPower() const {
+  const auto power = radiationPower();
+  const std::size_t n = power.size();
+  auto data = Array2D<Real>::from_shape({2, n});
+  for (std::size_t q = 0; q < n; ++q) {
+    data(0, q) = _freqs[q];
+    data(1, q) = power[q];
+  }
+  std::filesystem::create_directories(_output_dir.empty() ? "." : _output_dir);
+  xt::dump_npy((std::filesystem::path(_output_dir) / "power.npy").string(), data);
 }
 
 // ---------------------------------------------------------------- network

@@ -126,6 +126,8 @@ def load(build_if_missing: bool = True):
         "xfd_algorithmic_bytes_per_step": ([vp], _i64),
         "xfd_set_e_overrides": ([vp, _i64, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _dp, _dp],
                                 ctypes.c_int),
+        "xfd_set_h_term_overrides": ([vp, _i64, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _dp,
+                                      _dp], ctypes.c_int),
         "xfd_checkpoint_save": ([vp, _i32], ctypes.c_int),
         "xfd_checkpoint_load": ([vp, _i32], ctypes.c_int),
         "xfd_checkpoint_drop": ([vp, _i32], ctypes.c_int),
@@ -162,7 +164,7 @@ def exported_symbols() -> List[str]:
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
             "xfd_launches_per_step", "xfd_stencil_bytes_per_step",
-            "xfd_algorithmic_bytes_per_step", "xfd_set_e_overrides",
+            "xfd_algorithmic_bytes_per_step", "xfd_set_e_overrides", "xfd_set_h_term_overrides",
             "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
             "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_set_nf2ff_td", "xfd_get_nf2ff_td",
             "xfd_add_probe", "xfd_get_probe",

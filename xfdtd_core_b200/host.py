@@ -110,6 +110,17 @@ class SceneRun:
         """Engine option (graph, graph_chunk, kernel, ichunk)."""
         self._check(self.L.xfdtd_scene_set_engine_option(self.h, name.encode(), int(value)))
 
+    def get_engine_option(self, name: str) -> int:
+        """The engine's current value of an option (xfd_get_option)."""
+        import ctypes
+        from xfdtd_core_b200 import engine as E
+        v = ctypes.c_int64()
+        L = E.load()
+        if L.xfd_get_option(ctypes.c_void_p(self.engine_handle()), name.encode(),
+                            ctypes.byref(v)) != 0:
+            raise HostError(L.xfd_last_error(ctypes.c_void_p(self.engine_handle())).decode())
+        return int(v.value)
+
     def _check(self, st):
         if st != 0:
             raise HostError(self.L.xfdtd_host_last_error().decode())

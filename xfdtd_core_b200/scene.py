@@ -14,6 +14,7 @@ reference's user-facing API one to one:
 * ``VoltageSource(name, cube, dir, R, waveform)``     include/xfdtd/object/lumped_element/voltage_source.h:15-18
 * ``Network(ports, freqs) / Port(i, src, z, c, v)``   include/xfdtd/network/{network,port}.h
 * ``PecPlane(name, cube)``                            include/xfdtd/object/lumped_element/pec_plane.h:10-12
+* ``ThinWire(name, Cylinder(center, r, h, axis))``   include/xfdtd/object/thin_wire.h:14-16
 * ``Resistor / Capacitor / Inductor(name, cube, xyz, value)``
                                                        include/xfdtd/object/lumped_element/{resistor,capacitor,inductor}.h:9-12
 * ``MovieMonitor(FieldMonitor(cube, field), k)``      include/xfdtd/monitor/movie_monitor.h:13-15
@@ -134,14 +135,19 @@ def mlorentz(eps_inf: float, a0, a1, b0, b1, b2) -> Material:
 
 @dataclass
 class Shape:
-    kind: str  # "cube" | "sphere"
-    origin: Vec3  # cube origin or sphere centre
+    kind: str  # "cube" | "sphere" | "cylinder"
+    origin: Vec3  # cube origin, sphere or cylinder centre
     size: Vec3 = (0.0, 0.0, 0.0)  # cube size
     radius: float = 0.0
+    height: float = 0.0  # cylinder length along its axis
+    axis: int = 2  # cylinder axis: 0, 1, 2 for x, y, z
 
     def text(self) -> str:
         if self.kind == "cube":
             return "cube " + " ".join(_f(v) for v in (*self.origin, *self.size))
+        if self.kind == "cylinder":
+            return ("cylinder " + " ".join(_f(v) for v in (*self.origin, self.radius, self.height))
+                    + " " + "XYZ"[self.axis])
         return "sphere " + " ".join(_f(v) for v in (*self.origin, self.radius))
 
 
@@ -151,6 +157,12 @@ def cube(origin: Vec3, size: Vec3) -> Shape:
 
 def sphere(center: Vec3, radius: float) -> Shape:
     return Shape("sphere", tuple(map(float, center)), radius=float(radius))
+
+
+def cylinder(center: Vec3, radius: float, height: float, axis: int) -> Shape:
+    """``Cylinder(center, radius, height, Axis)`` (src/shape/cylinder.cpp:13-26)."""
+    return Shape("cylinder", tuple(map(float, center)), radius=float(radius),
+                 height=float(height), axis=int(axis))
 
 
 @dataclass
@@ -256,6 +268,21 @@ class PecPlaneSpec:
     def text(self) -> str:
         o, s = self.shape.origin, self.shape.size
         return f"pec_plane {self.name} " + " ".join(_f(v) for v in (*o, *s))
+
+
+@dataclass
+class ThinWireSpec:
+    """``ThinWire(name, Cylinder)`` (src/object/thin_wire.cpp): an air object
+    whose E along the wire is held at zero and whose neighbouring H
+    coefficients take the thin-wire factor."""
+    name: str
+    shape: Shape  # a cylinder
+
+    def text(self) -> str:
+        sh = self.shape
+        return (f"thin_wire {self.name} " + " ".join(_f(v) for v in (*sh.origin, sh.radius,
+                                                                      sh.height))
+                + " " + "XYZ"[sh.axis])
 
 
 @dataclass
@@ -378,6 +405,7 @@ class Scene:
     cfl: float
     steps: int
     objects: List[ObjectSpec] = field(default_factory=list)
+    thin_wires: List[ThinWireSpec] = field(default_factory=list)
     current_sources: List[CurrentSourceSpec] = field(default_factory=list)
     lumped_elements: List[LumpedSpec] = field(default_factory=list)
     pec_planes: List[PecPlaneSpec] = field(default_factory=list)
@@ -396,6 +424,7 @@ class Scene:
                  "grid " + " ".join(_f(v) for v in self.dl) + f" {_f(self.cfl)}",
                  f"steps {self.steps}"]
         lines += [o.text() for o in self.objects]
+        lines += [w.text() for w in self.thin_wires]
         lines += [c.text() for c in self.current_sources]
         lines += [c.text() for c in self.lumped_elements]
         lines += [c.text() for c in self.pec_planes]
@@ -452,6 +481,41 @@ def dielectric_sphere(steps: int = 2000, dl: float = 7.5e-3, half: float = 0.175
         # the example's scattered-field probe (dielectric_sphere_scatter.cpp:85-90)
         s.field_times.append(FieldTimeSpec("ex_point", "EX",
                                            cube((0.0, -half + 3 * dl, 0.0), (dl, dl, dl))))
+    if nf2ff_freqs:
+        s.nf2ff = NF2FFSpec((nf2ff_distance,) * 3, list(nf2ff_freqs))
+    return s
+
+
+def half_wave_dipole(steps: int = 4000, dl: float = 2.5e-4, arm_cells: int = 39,
+                     pad_cells: int = 10, pml: int = 8, nf2ff_distance: int = 13,
+                     nf2ff_freqs: Sequence[float] = (7e9,), network: bool = True) -> Scene:
+    """The reference's half-wave dipole (test/src/examples/half_wave_dipole.cpp:
+    20-99): two z-directed ThinWire arms of radius 5e-5 and length arm_cells dl
+    either side of a two-cell 50-ohm voltage source gap (Gaussian, tau =
+    30 dl / 6e8), an air domain pad_cells beyond the arms on every side, an
+    8-cell PML, a voltage / current monitor port on the gap with a one-port
+    network over 20 MHz .. 20 GHz, and a frequency-domain NF2FF surface 13
+    cells in."""
+    reach = (arm_cells + 1) * dl  # the arms end at z = +-(arm_cells + 1) dl
+    s = Scene(dl=(dl, dl, dl), cfl=0.9, steps=steps, name="half_wave_dipole")
+    s.objects.append(ObjectSpec("domain", cube((-pad_cells * dl, -pad_cells * dl,
+                                                -reach - pad_cells * dl),
+                                               (2 * pad_cells * dl, 2 * pad_cells * dl,
+                                                2 * reach + 2 * pad_cells * dl)), air()))
+    zc = dl + arm_cells * dl / 2
+    s.thin_wires += [ThinWireSpec("arm_0", cylinder((0.0, 0.0, zc), 5e-5, arm_cells * dl, 2)),
+                     ThinWireSpec("arm_1", cylinder((0.0, 0.0, -zc), 5e-5, arm_cells * dl, 2))]
+    tau = dl * 30 / 6e8
+    gap = cube((0.0, 0.0, -dl), (0.0, 0.0, 2 * dl))
+    s.current_sources.append(VoltageSourceSpec("v_s", gap, "ZP", 50.0,
+                                               Waveform("gaussian", tau, 4.5 * tau)))
+    s.pmls = pml_all(pml)
+    if network:
+        s.line_monitors += [LineMonitorSpec("voltage", "v1", gap, "ZP"),
+                            LineMonitorSpec("current", "c1", cube((0.0, 0.0, 0.0),
+                                                                  (0.0, 0.0, 0.0)), "ZP")]
+        s.network = NetworkSpec(list(np.arange(2e7, 2e10, 2e7)),
+                                [PortSpec(1, True, 50.0, "c1", "v1")])
     if nf2ff_freqs:
         s.nf2ff = NF2FFSpec((nf2ff_distance,) * 3, list(nf2ff_freqs))
     return s
