@@ -64,7 +64,8 @@ class svector {
   svector(const std::array<U, N>& a) {
     assign(a.begin(), a.end());
   }
-  template <class U>
+  // Integer sequences only: a vector of values is not a shape.
+  template <class U, std::enable_if_t<std::is_integral_v<U>, int> = 0>
   svector(const std::vector<U>& v) {
     assign(v.begin(), v.end());
   }

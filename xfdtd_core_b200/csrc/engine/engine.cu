@@ -186,11 +186,10 @@ struct xfd_engine {
   int2* d_xlayer = nullptr;  // per x plane: CPML layer code of the H / E layers
   size_t xlayer_slabs = (size_t)-1;  // slab count the table was built for
   HybMaps hmaps[2]{};     // tensor maps of the fused interior sweep (sweep 7), by input buffer
-  // Its box tiles as two lists: tiles no TFSF H pass reaches (swept by the
-  // form without TFSF code) and tiles one does (hyb_off[0..2]).
+  // Its box tiles, one CTA each.
   int4* d_hyb_tiles = nullptr;
   size_t hyb_tiles_cap = 0;
-  int hyb_off[3] = {0, 0, 0};
+  int n_hyb_tiles = 0;
   long long hyb_key = -1;
   FmarchMaps fmaps[2]{};  // tensor maps of the fused marching sweep
   FvecMaps fvmaps[2]{};   // tensor maps of its two-nodes-per-thread interior form
@@ -581,9 +580,7 @@ xfd_status build_tma_maps(xfd_engine* e) {
       if (r != CUDA_SUCCESS) return fail(e, XFD_ERR_CUDA, "tensor map (hyb class): %d", (int)r);
     }
     constexpr int HS = hyb_stages<T>();
-    CUDA_TRY(e, cudaFuncSetAttribute(k_hyb<T, kMTJ, HS, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, HG::smem(HS)));
-    CUDA_TRY(e, cudaFuncSetAttribute(k_hyb<T, kMTJ, HS, true>,
+    CUDA_TRY(e, cudaFuncSetAttribute(k_hyb<T, kMTJ, HS>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, HG::smem(HS)));
   }
   constexpr int MW = march_wide_stages<T>();
@@ -748,13 +745,15 @@ MarchLayout march_layout(const xfd_engine* e) {
   const int n_nodes[3] = {L.nz, L.ny, L.nx + 1};
   // Per axis the shift whose CPML-free run covers the most nodes (k in steps
   // of 8 nodes, so that every TMA x coordinate stays a multiple of 16 bytes
-  // for the field and the uint16 class maps alike).
+  // for the field and the uint16 class maps alike).  Sweep 7 always shifts
+  // along j and i (rows and planes carry no alignment), along k only with the
+  // march_shift option.
   const int step[3] = {8, 1, 1};
   const bool hyb = e->kernel_mode == 7;
   for (int g = 0; g < 3; ++g) {
     int best = -1;
     for (int sh = 0; sh > -size[g]; sh -= step[g]) {
-      if ((!e->march_shift || hyb) && sh != 0) break;
+      if (sh != 0 && !e->march_shift && !(hyb && g > 0)) break;
       int lo = 0, hi = 0;
       const int nodes = march_free_run(e, g, sh, lo, hi);
       if (nodes > best) {
@@ -774,10 +773,11 @@ MarchLayout march_layout(const xfd_engine* e) {
     const int upper[3] = {L.nz, L.ny, L.nx};
     const int axis_of[3] = {2, 1, 0};
     for (int g = 0; g < 3; ++g) {
-      if (m.lo[g] * size[g] < 1) m.lo[g] = 1;
-      m.hi[g] = std::min(m.hi[g], upper[g] / size[g]);
+      const int sh = m.shift[g];
+      while (m.lo[g] * size[g] + sh < 1) ++m.lo[g];
+      m.hi[g] = std::min(m.hi[g], (upper[g] - sh) / size[g]);
       while (m.hi[g] > m.lo[g]) {
-        const int below = m.lo[g] * size[g] - 1;
+        const int below = m.lo[g] * size[g] + sh - 1;
         bool in_layer = false;
         for (const auto& S : e->slabs)
           if (S.m == axis_of[g] && below >= S.h_lo && below < S.h_lo + S.n) in_layer = true;
@@ -858,34 +858,16 @@ void march_tile_lists(const xfd_engine* e, std::vector<int4> lists[4]) {
 xfd_status build_hyb_tiles(xfd_engine* e) {
   const MarchLayout ml = march_layout(e);
   const long long key = (long long)e->slabs.size() * 1000003LL + e->march_ichunk * 4 +
-                        (e->have_tfsf ? 2 : 0) + (ml.box ? 1 : 0);
+                        (e->march_shift ? 2 : 0) + (ml.box ? 1 : 0);
   if (key == e->hyb_key) return XFD_OK;
-  std::vector<int4> clean, tf;
-  if (ml.box) {
-    const int ich = e->march_ichunk;
+  // j tiles fastest, then k tiles, then chunks: CTAs resident together share
+  // the E / H rows of their j halos through L2.
+  std::vector<int4> all;
+  if (ml.box)
     for (int gz = ml.lo[2]; gz < ml.hi[2]; ++gz)
-      for (int gy = ml.lo[1]; gy < ml.hi[1]; ++gy)
-        for (int gx = ml.lo[0]; gx < ml.hi[0]; ++gx) {
-          bool meets = false;
-          if (e->have_tfsf) {
-            const int lo[3] = {gz * ich - 1, gy * kMTJ - 1, gx * 32 - 1};
-            const int hi[3] = {gz * ich + ich, gy * kMTJ + kMTJ, gx * 32 + 32};
-            for (int c = 0; c < 3 && !meets; ++c)
-              for (int q = 0; q < e->tfsf_h.n[c] && !meets; ++q) {
-                const TfsfHPass& P = e->tfsf_h.pass[c][q];
-                bool ov = true;
-                for (int a = 0; a < 3; ++a) ov = ov && P.lo[a] < hi[a] && lo[a] < P.hi[a];
-                meets = ov;
-              }
-          }
-          (meets ? tf : clean).push_back(make_int4(0, gx, gy, gz));
-        }
-  }
-  std::vector<int4> all(clean);
-  all.insert(all.end(), tf.begin(), tf.end());
-  e->hyb_off[0] = 0;
-  e->hyb_off[1] = (int)clean.size();
-  e->hyb_off[2] = (int)all.size();
+      for (int gx = ml.lo[0]; gx < ml.hi[0]; ++gx)
+        for (int gy = ml.lo[1]; gy < ml.hi[1]; ++gy) all.push_back(make_int4(0, gx, gy, gz));
+  e->n_hyb_tiles = (int)all.size();
   if (all.size() > e->hyb_tiles_cap) {
     void* p = nullptr;
     xfd_status st = dev_alloc(e, &p, all.size() * sizeof(int4));
@@ -987,7 +969,7 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
   for (int a = 0; a < 3; ++a) {
     mh.box_lo[a] = ml.skip_lo[a];
     mh.box_hi[a] = ml.skip_hi[a];
-    mh.shift[a] = 0;
+    mh.shift[a] = ml.shift[a];
   }
   MarchTmaP<T> me = mh;
   for (int c = 0; c < 3; ++c) {
@@ -1020,6 +1002,16 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
     list(kz4, 2, msm_free);
     list(kcp, 3, msm);
   };
+  // TFSF H-face corrections into the H every sweep kernel reads (k_tfsf_pre).
+  if (e->have_tfsf) {
+    T* const* fi = reinterpret_cast<T* const*>(e->d_fields[in]);
+    for (int g = 0; g < 2 && c == cudaSuccess; ++g) {
+      const auto& G = e->tfsf_groups[g];
+      if (G.total > 0)
+        k_tfsf_pre<T><<<blocks_for(G.total, 256), 256, 0, s>>>(
+            e->tfsf, G, e->L, fi, e->cls, static_cast<const T*>(e->tab), e->d_step, e->d_err);
+    }
+  }
   fork(0);
   if (ml.box && c == cudaSuccess) {
     HybP<T> hp{};
@@ -1031,23 +1023,16 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
       hp.fe[a] = static_cast<const T*>(e->fe[a]);
       hp.fh[a] = static_cast<const T*>(e->fh[a]);
       hp.org[a] = ml.lo[a];
+      hp.shift[a] = ml.shift[a];
     }
-    hp.tf = e->tfsf;
-    hp.tfh = e->tfsf_h;
-    hp.tfh.enabled = e->have_tfsf ? 1 : 0;
-    hp.step = e->d_step;
     hp.err = e->d_err;
     hp.m = e->hmaps[in];
     hp.ichunk = e->march_ichunk;
     const size_t hsm = HybGeom<T, kMTJ>::smem(HS);
     const dim3 blk_h(32, kMTJ + 1, 1);  // kMTJ compute warps + the helper warp
-    // Tiles no TFSF H pass reaches, then (without TFSF none) those one does.
-    const int n_clean = e->hyb_off[1] - e->hyb_off[0];
-    const int n_tf = e->hyb_off[2] - e->hyb_off[1];
     hp.tiles = e->d_hyb_tiles;
-    if (n_clean > 0) k_hyb<T, kMTJ, HS, false><<<n_clean, blk_h, hsm, e->side[0]>>>(hp);
-    hp.tiles = e->d_hyb_tiles + e->hyb_off[1];
-    if (n_tf > 0) k_hyb<T, kMTJ, HS, true><<<n_tf, blk_h, hsm, e->side[0]>>>(hp);
+    if (e->n_hyb_tiles > 0)
+      k_hyb<T, kMTJ, HS><<<e->n_hyb_tiles, blk_h, hsm, e->side[0]>>>(hp);
   }
   lists(mh, k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 1>,
         k_march_h_tma_list<T, kMTJ, 32, MF, true, false, 2>,
@@ -1071,24 +1056,6 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
   if (c == cudaSuccess)
     k_edge_pp<T, false><<<edge_blocks, 256, 0, e->side[1]>>>(yp, fields_in, face_targets);
   join(1, kSides - 1);
-  if (e->have_tfsf && c == cudaSuccess) {
-    Box3 skip{};
-    if (ml.box) {
-      const int size[3] = {32, kMTJ, e->march_ichunk};
-      for (int g = 0; g < 3; ++g) {
-        const int a = 2 - g;  // tile dimension g -> lattice axis
-        skip.lo[a] = ml.lo[g] * size[g];
-        skip.hi[a] = ml.hi[g] * size[g];
-      }
-    }
-    T* const* fo = reinterpret_cast<T* const*>(e->d_fields[out]);
-    for (int g = 0; g < 2; ++g) {
-      const auto& G = e->tfsf_groups[g];
-      if (G.total > 0)
-        k_tfsf_outside<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fo,
-                                                                   e->d_step, e->d_err, skip);
-    }
-  }
   join(0, 0);  // the box kernel's new H
   fork(1);
   lists(me, k_march_e_tma_list<T, kMTJ, 32, MF, true, false, 1>,
@@ -2711,7 +2678,7 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
     std::vector<int4> lists[4];
     march_tile_lists(e, lists);
     int n = 1 + 2;  // step counter, faces
-    if (ml.box) n += (e->hyb_off[1] > e->hyb_off[0] ? 1 : 0) + (e->hyb_off[2] > e->hyb_off[1] ? 1 : 0);
+    if (ml.box) n += 1;
     for (int q = 0; q < 4; ++q)
       if (!lists[q].empty()) n += 2;
     if (e->have_tfsf) n += 4;

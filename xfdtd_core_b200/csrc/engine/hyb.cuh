@@ -9,7 +9,8 @@
 //
 // A CTA of 32 x TJ compute threads (plus a helper warp) owns a 32-node (k) x
 // TJ-row (j) tile and marches
-// along i over a chunk of planes; tiles are 128-byte aligned along k.  Per
+// along i over a chunk of planes; tiles are 128-byte aligned along k (unless
+// the march_shift option moves them by a multiple of 8 nodes).  Per
 // plane i it stages, by TMA into a ring of S shared-memory stages:
 //   E of plane i over rows j0-1 .. j0+TJ and nodes k0-XA .. k0+31+XA,
 //   H of plane i over rows j0-1 .. j0+TJ-1 and nodes k0-XA .. k0+31,
@@ -18,11 +19,10 @@
 // multiple of 16 bytes).  E of plane i+1 is the next stage.  Each thread then
 // computes the three H components of its node (the reference's hNext,
 // src/include/updator/update_scheme.h:57-62, over BasicUpdator::updateH's
-// ranges, src/updator/basic_updator.cpp:23-36), with the TFSF H-face
-// corrections of TFSF3DCorrector::correctH (src/waveform_source/tfsf_corrector.cpp:205-232)
-// applied inline; a helper warp issues the loads and recomputes H_x, H_z of row
-// j0-1 and H_x, H_y of column k0-1 (nodes of the neighbouring tiles that the E
-// update reads).  After one CTA barrier each thread computes the three E components
+// ranges, src/updator/basic_updator.cpp:23-36); the TFSF H-face corrections
+// are already in the H it reads (k_tfsf_pre, kernels.cuh).  A helper warp
+// issues the loads and recomputes H_x, H_z of row j0-1 and H_x, H_y of column
+// k0-1 (nodes of the neighbouring tiles that the E update reads).  After one CTA barrier each thread computes the three E components
 // (eNext, update_scheme.h:26-31, over BasicUpdator3D::updateE's ranges,
 // src/updator/basic_updator_3d.cpp:38-69): the k-1 neighbours of H come by
 // warp shuffle, the j-1 neighbours from shared memory, the i-1 neighbours are
@@ -40,8 +40,6 @@
 // Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
 // the engine's error word, drains its loads in flight and returns.
 #pragma once
-
-#include <climits>
 
 #include "march_tma.cuh"
 
@@ -61,12 +59,10 @@ struct HybP {
   int n_classes;
   const T* fe[3];
   const T* fh[3];
-  TfsfD tf;
-  TfsfHD tfh;
-  const long long* step;
   int* err;
   HybMaps m;
   int org[3];   // first (k tile, j tile, chunk) of the box
+  int shift[3];  // node of tile (0, 0, 0): k0 = 32 x + shift[0], j0, i_lo likewise
   int ichunk;
   // Tile list: CTA b sweeps tile (tiles[b].y, tiles[b].z, tiles[b].w) (k tile,
   // j tile, chunk); null: CTA (x, y, z) sweeps tile org + (x, y, z).
@@ -97,61 +93,6 @@ struct HybGeom {
   static constexpr int HN = 2 * 2 * (RH * TK + TJ) * (int)sizeof(T);
   __host__ __device__ static constexpr int smem(int S) { return S * STAGE + TB + HN + 8 * S; }
 };
-
-// TFSF H passes that can touch node (j, k), and the planes where they do:
-// bit 4 c + s of m is pass s of component c; the x-normal passes touch one
-// plane each (px0, px1), the y- and z-normal ones the planes [ylo, yhi).
-struct TfsfSel {
-  uint32_t m = 0;
-  int px0 = -1, px1 = -1, ylo = 0, yhi = 0;
-  __device__ __forceinline__ bool hits(int i) const {
-    return m != 0 && (i == px0 || i == px1 || (i >= ylo && i < yhi));
-  }
-};
-
-template <typename T>
-__device__ __forceinline__ TfsfSel hyb_tfsf_sel(const HybP<T>& p, int j, int k) {
-  TfsfSel r;
-  r.ylo = INT_MAX;
-  r.yhi = INT_MIN;
-  for (int c = 0; c < 3; ++c)
-    for (int s = 0; s < p.tfh.n[c]; ++s) {
-      const TfsfHPass& Q = p.tfh.pass[c][s];
-      if (j < Q.lo[1] || j >= Q.hi[1] || k < Q.lo[2] || k >= Q.hi[2]) continue;
-      r.m |= 1u << (4 * c + s);
-      if (Q.m == 0 && Q.hi[0] == Q.lo[0] + 1) {
-        if (r.px0 < 0 || r.px0 == Q.lo[0]) r.px0 = Q.lo[0];
-        else r.px1 = Q.lo[0];
-      } else {
-        r.ylo = min(r.ylo, Q.lo[0]);
-        r.yhi = max(r.yhi, Q.hi[0]);
-      }
-    }
-  return r;
-}
-
-// TFSF H-face corrections of component c at node (i, j, k), in the
-// reference's pass order (correctTFSF, src/include/waveform_source/tfsf_corrector.h:89-229),
-// over the passes of `mask`.  Called only inside a warp-uniform branch taken
-// by warps with a node on a TFSF face at this plane.
-template <typename T>
-__device__ __forceinline__ T hyb_tfsf_h(const HybP<T>& p, uint32_t mask, int c, int i, int j,
-                                        int k, T h, long long t) {
-  uint32_t m = (mask >> (4 * c)) & 15u;
-  while (m) {
-    const int s = __ffs(m) - 1;
-    m &= m - 1;
-    const TfsfHPass& Q = p.tfh.pass[c][s];
-    if (i < Q.lo[0] || i >= Q.hi[0]) continue;
-    const int xi[3] = {i + (Q.neg && Q.m == 0 ? 1 : 0), j + (Q.neg && Q.m == 1 ? 1 : 0),
-                       k + (Q.neg && Q.m == 2 ? 1 : 0)};
-    int e_flag = 0;
-    const double v = tfsf_incident(p.tf, true, Q.dual, t, xi, &e_flag);
-    if (e_flag) atomicOr(p.err, 1);
-    h = (T)((double)h + v * Q.coeff);
-  }
-  return h;
-}
 
 // The 12 (ca, cb) values of a class as vector loads: FP32 3 x float4, FP64
 // 6 x double2 (rows are 48 / 96 bytes, so 16-byte aligned), from shared memory
@@ -187,7 +128,7 @@ struct ClassRow {
 // recomputes the H values of the neighbouring tiles that the E update reads:
 // H_x, H_z of row j0-1 (lane = k - k0) and H_x, H_y of column k0-1 (lanes
 // 0 .. TJ-1 = j - j0).  Compute warps carry no halo work, so no warp diverges.
-template <typename T, int TJ, int S, bool TF>
+template <typename T, int TJ, int S>
 __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
     k_hyb(const __grid_constant__ HybP<T> p) {
   using G = HybGeom<T, TJ>;
@@ -208,8 +149,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
     gy = blockIdx.y + p.org[1];
     gz = blockIdx.z + p.org[2];
   }
-  const int k0 = gx * TK, j0 = gy * TJ;
-  const int i_lo = gz * p.ichunk;
+  const int k0 = gx * TK + p.shift[0], j0 = gy * TJ + p.shift[1];
+  const int i_lo = gz * p.ichunk + p.shift[2];
   const int i_hi = min(i_lo + p.ichunk, L.nx);
   const int n = i_hi - i_lo;  // planes updated; staged: i_lo-1 .. i_hi (n + 2)
 
@@ -255,7 +196,6 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
   for (int u = 0; u < S && u < n_staged; ++u) ring.pending |= 1u << (u % S);
   for (int x = tid; x < min(p.n_classes, G::NC) * 12; x += 32 * (TJ + 1)) sT[x] = p.tab[x];
 
-  const long long t = TF ? *p.step : 0;
   const long long PS = (long long)L.NY * L.KP;
   // Node of this thread: compute warps own (j0 + wj, k0 + tk); the helper
   // warp's lane tk handles row-halo node (j0-1, k0+tk) and, for tk < TJ,
@@ -281,9 +221,6 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
   T* const o_hx = p.out[3] + row;
   T* const o_hy = p.out[4] + row;
   T* const o_hz = p.out[5] + row;
-  TfsfSel ts, ts_c;  // TFSF passes of this lane's node and column-halo node
-  if (TF) ts = hyb_tfsf_sel(p, j, k);
-  if (TF && col) ts_c = hyb_tfsf_sel(p, jc, k0 - 1);
   __syncthreads();  // class rows staged
 
   auto row_of = [&](int cl) { return cl < G::NC ? sT + cl * 12 : p.tab + (size_t)cl * 12; };
@@ -308,12 +245,6 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
              c.v[9] * (fhi * (sE(1 % S, 2)[eq] - ez) - fhk * (E0[eq + 1] - ex));
       T hz = c.v[10] * sH(0, 2)[hq] +
              c.v[11] * (fhj * (E0[eq + G::WE] - ex) - fhi * (sE(1 % S, 1)[eq] - ey));
-      if (TF && __any_sync(0xffffffffu, ts.hits(i))) {
-        if (ts.hits(i)) {
-          hy = hyb_tfsf_h(p, ts.m, 1, i, j, k, hy, t);
-          hz = hyb_tfsf_h(p, ts.m, 2, i, j, k, hz, t);
-        }
-      }
       hy_prev = hy;
       hz_prev = hz;
     }
@@ -345,13 +276,6 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
       if (!helper)
         hy = c.v[8] * sH(sc, 1)[hq] +
              c.v[9] * (fhi * (N2[eq] - ez) - fhk * (E0[eq + 1] - ex));
-      if (TF && __any_sync(0xffffffffu, ts.hits(i))) {
-        if (ts.hits(i)) {
-          hx = hyb_tfsf_h(p, ts.m, 0, i, j, k, hx, t);
-          hz = hyb_tfsf_h(p, ts.m, 2, i, j, k, hz, t);
-          if (!helper) hy = hyb_tfsf_h(p, ts.m, 1, i, j, k, hy, t);
-        }
-      }
       nrow(b, 0)[wr * TK + tk] = hx;
       nrow(b, 1)[wr * TK + tk] = hz;
       if (!helper) {
@@ -363,14 +287,10 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
         ClassRow<T> cc;
         cc.load(row_of(sC(sc)[cq_c]));
         const T ex_c = E0[eq_c], ey_c = E1[eq_c], ez_c = E2[eq_c];
-        T hxc = cc.v[6] * sH(sc, 0)[hq_c] +
+        const T hxc = cc.v[6] * sH(sc, 0)[hq_c] +
                 cc.v[7] * (fhk_c * (E1[eq_c + 1] - ey_c) - fhj_c * (E2[eq_c + G::WE] - ez_c));
-        T hyc = cc.v[8] * sH(sc, 1)[hq_c] +
+        const T hyc = cc.v[8] * sH(sc, 1)[hq_c] +
                 cc.v[9] * (fhi * (N2[eq_c] - ez_c) - fhk_c * (E0[eq_c + 1] - ex_c));
-        if (TF && ts_c.hits(i)) {
-          hxc = hyb_tfsf_h(p, ts_c.m, 0, i, jc, k0 - 1, hxc, t);
-          hyc = hyb_tfsf_h(p, ts_c.m, 1, i, jc, k0 - 1, hyc, t);
-        }
         ncol(b, 0)[tk] = hxc;
         ncol(b, 1)[tk] = hyc;
       }

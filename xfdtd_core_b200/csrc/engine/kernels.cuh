@@ -359,15 +359,13 @@ __device__ __forceinline__ double tfsf_incident(const TfsfD& tf, bool inc_e, int
   return tr * ((1 - w) * row[idx] + w * row[idx + 1]);
 }
 
-// A node box [lo, hi) (empty when lo = hi).
-struct Box3 {
-  int lo[3], hi[3];
-};
-
+// `cls` / `tab` (H passes only): add the correction divided by the node's ca
+// (sweep 7's pre-pass on the H it is about to read, see k_tfsf_pre).
 template <typename T>
 __device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, const Lat& L,
                                           T* const* fields, const long long* step, int* err,
-                                          long long tid, const Box3& skip = Box3{}) {
+                                          long long tid, const uint16_t* cls = nullptr,
+                                          const T* tab = nullptr) {
   if (tid >= g.total) return;
   int q = 0;
   while (q + 1 < g.n && tid >= g.pass[q + 1].begin) ++q;
@@ -392,16 +390,18 @@ __device__ __forceinline__ void tfsf_node(const TfsfD& tf, const TfsfGroupD& g, 
     inc_e = true;   // H face corrects the node half a cell outside
     if (P.neg) xf[m] -= 1;
   }
-  if (xf[0] >= skip.lo[0] && xf[0] < skip.hi[0] && xf[1] >= skip.lo[1] && xf[1] < skip.hi[1] &&
-      xf[2] >= skip.lo[2] && xf[2] < skip.hi[2])
-    return;  // corrected inside the fused sweep
   const int dual = (P.field == (m + 1) % 3) ? (m + 2) % 3 : (m + 1) % 3;
   int e_flag = 0;
   const double v = tfsf_incident(tf, inc_e, dual, t, xi, &e_flag);
   if (e_flag) atomicOr(err, 1);
   T* F = fields[(P.is_e ? 0 : 3) + P.field];
   const long long id = lat_index(L, xf[0], xf[1], xf[2]);
-  F[id] = (T)((double)F[id] + v * P.coeff);
+  if (cls) {
+    const double ca = (double)tab[(size_t)cls[id] * 12 + 6 + 2 * P.field];
+    F[id] = (T)((double)F[id] + v * P.coeff / ca);
+  } else {
+    F[id] = (T)((double)F[id] + v * P.coeff);
+  }
 }
 
 template <typename T>
@@ -411,14 +411,21 @@ __global__ void k_tfsf(const __grid_constant__ TfsfD tf, const __grid_constant__
   tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// The passes of one group on the nodes outside `skip` (sweep 7: the fused
-// box kernel applies the H passes of its own nodes inline).
+// TFSF H-face corrections before sweep 7 (TFSF3DCorrector::correctH,
+// src/waveform_source/tfsf_corrector.cpp:205-232, in its pass order): the
+// reference adds coeff v to H after updateH, H' = ca H + cb curl E + coeff v.
+// Sweep 7 reads H from the input buffer in several kernels (the fused box,
+// its halo recomputes, the CPML tiles), so the correction goes into that H
+// first, divided by the node's ca: ca (H + coeff v / ca) + cb curl E is the
+// same sum (the two differ by one rounding).  Every reader of the old H then
+// sees the corrected value, and no sweep kernel carries TFSF code.  The input
+// buffer's H is overwritten by the next step's sweep.
 template <typename T>
-__global__ void k_tfsf_outside(const __grid_constant__ TfsfD tf,
-                               const __grid_constant__ TfsfGroupD g, Lat L, T* const* fields,
-                               const long long* step, int* err, Box3 skip) {
-  tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x,
-               skip);
+__global__ void k_tfsf_pre(const __grid_constant__ TfsfD tf, const __grid_constant__ TfsfGroupD g,
+                           Lat L, T* const* fields_in, const uint16_t* cls, const T* tab,
+                           const long long* step, int* err) {
+  tfsf_node<T>(tf, g, L, fields_in, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+               cls, tab);
 }
 
 // Per-lattice TFSF state for the batched launch: the incident tables, the

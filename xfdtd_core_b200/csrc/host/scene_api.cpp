@@ -481,8 +481,8 @@ int xfdtd_scene_far_field(xfdtd_scene* s, int32_t n_theta, const double* theta, 
     if (!s || !s->nf2ff) throw XFDTDException("scene has no NF2FF");
     if (!s->finished) throw XFDTDException("call xfdtd_scene_finish first");
     if (!theta || !phi || n_theta < 1 || n_phi < 1) throw XFDTDException("bad angles");
-    Array1D<Real> th(std::vector<Real>(theta, theta + n_theta));
-    Array1D<Real> ph(std::vector<Real>(phi, phi + n_phi));
+    Array1D<Real> th(xt::adapt(std::vector<Real>(theta, theta + n_theta)));
+    Array1D<Real> ph(xt::adapt(std::vector<Real>(phi, phi + n_phi)));
     const Vector o = origin ? Vector{origin[0], origin[1], origin[2]} : Vector{0, 0, 0};
     const auto data = s->nf2ff->farField(th, ph, o);
     if (count) *count = (int64_t)data.size();
