@@ -54,12 +54,12 @@ KIND = "dispersive"  # --workload: dispersive (the default), boxes, sphere, batc
 DEFAULT_GRID = {"dispersive": 384, "boxes": 256}
 
 # DRAM bytes per FP32 time step of the default sweep, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum summed over every kernel of
-# consecutive steps, one pass, --clock-control none) and scaled to the full
-# lattice by cell count where the capture ran a smaller one.  Keyed by
-# (workload, cells per axis, sweep); a configuration without an entry
-# reports null.
-MEASURED_TRAFFIC = {}
+# (dram__bytes_read.sum + dram__bytes_write.sum summed over every launch of
+# one step of `python bench.py --steps 12 --warmup 3 --no-cpu-baseline`, one
+# pass, --clock-control none --cache-control none so that write-backs of
+# dirty L2 lines land in the step that caused them).  Keyed by (workload,
+# cells per axis, sweep); a configuration without an entry reports null.
+MEASURED_TRAFFIC = {("dispersive", 384, 7): 4796.7e6}
 
 
 def workload_name(n: int) -> str:

@@ -311,16 +311,28 @@ int64_t xfd_current_step(const xfd_engine* e);
  * H-then-E sweep, 2 = fused sweep with its per-plane inputs staged by TMA,
  * 3 = split sweeps marching along x, 4 = the same with TMA-staged planes,
  * 5 = fused marching sweep with overlapped tiles and TMA-staged planes,
- * 6 = 5 with a two-nodes-per-thread form in the CPML-free interior; default
- * 4, or 0 on lattices whose marching tiles number fewer than two per SM),
+ * 6 = 5 with a two-nodes-per-thread form in the CPML-free interior,
+ * 7 = the fused H-then-E sweep of the CPML-free interior box with ping-pong
+ * buffers beside the split marching sweeps of the CPML tiles; default 7, or 0
+ * on lattices whose marching tiles number fewer than two per SM),
  * "ichunk" (planes per CTA of the fused sweeps, default 32), "march_ichunk"
  * (planes per CTA of the split marching sweeps, default 16), and the forms
  * of sweep 4: "march_concurrent" (launches of a phase on four streams,
  * default 1), "march_split_axes" (CPML tiles in lists by slab axis, default
  * 1), "march_cp_stages" (single-axis lists with fewer stages, default 1),
  * "march_wide" (two-rows-per-thread interior form, default 0),
- * "march_shift" (tile grid moved to the CPML layers, default 0).  Every
- * sweep computes the same update; they differ in speed only. */
+ * "march_shift" (tile grid moved to the CPML layers along k, default 0;
+ * sweep 7 always moves it along j and i).  Every sweep computes the same
+ * update; they differ in speed only.
+ * Failure detection: "stage_wait_cycles" (cycles a TMA-staged sweep (3..7)
+ * waits for one staged plane before the CTA gives up, drains its loads in
+ * flight and returns; the next xfd_sync reports XFD_ERR_TIMEOUT; 0 = the
+ * default, about 2 s; batched engines take the value they had at
+ * xfd_batch_create) and "watchdog_interval" (K > 0: every K steps a scan of
+ * the six fields for NaN / Inf; the next xfd_sync reports XFD_ERR_NUMERIC;
+ * default 0 = off; not run by xfd_batch_run).  An engine whose sweep gave up
+ * stays stopped (every later sweep CTA returns at once); the CUDA context
+ * stays usable, so a new engine can take over. */
 xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value);
 /* Current value of an option of xfd_set_option. */
 xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value);

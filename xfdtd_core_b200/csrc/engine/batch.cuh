@@ -177,6 +177,7 @@ xfd_status batch_prepare(xfd_batch* b) {
     q.p = march_params<T>(e);
     q.m = e->mtma[e->cur];
     q.err = e->d_err;
+    q.wait_budget = e->stage_wait;
     int lo[3], hi[3];
     march_split(e, lo, hi);
     const bool box = hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];

@@ -163,6 +163,12 @@ struct xfd_engine {
   int kernel_mode = 7;
   int ichunk = 32;
   int march_ichunk = 16;  // planes per CTA of the marching split sweeps
+  // Cycles a TMA-staged sweep's stage wait may take before the CTA gives up
+  // (error bit 2, XFD_ERR_TIMEOUT at the next sync); 0: about 2 s.
+  long long stage_wait = 0;
+  // NaN / Inf watchdog: every `watchdog` steps a scan of the six fields sets
+  // error bit 4 (XFD_ERR_NUMERIC at the next sync) on a non-finite value; 0: off.
+  long long watchdog = 0;
   bool tma_ready = false;
   TmaMaps tma[2]{};       // tensor maps over buffer 0 / 1 (and the class index)
   MarchMaps mtma[2]{};    // tensor maps of the TMA marching sweeps
@@ -966,6 +972,7 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
   for (int c = 0; c < 6; ++c) mh.p.f[c] = static_cast<T*>(e->fbuf[out][c]);
   mh.m = e->mtma[in];  // old E halo boxes, old H tiles
   mh.err = e->d_err;
+  mh.wait_budget = e->stage_wait;
   for (int a = 0; a < 3; ++a) {
     mh.box_lo[a] = ml.skip_lo[a];
     mh.box_hi[a] = ml.skip_hi[a];
@@ -1026,6 +1033,7 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
       hp.shift[a] = ml.shift[a];
     }
     hp.err = e->d_err;
+    hp.wait_budget = e->stage_wait;
     hp.m = e->hmaps[in];
     hp.ichunk = e->march_ichunk;
     const size_t hsm = HybGeom<T, kMTJ>::smem(HS);
@@ -1160,6 +1168,7 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       mtp.p = mp;
       mtp.m = e->mtma[e->cur];
       mtp.err = e->d_err;
+      mtp.wait_budget = e->stage_wait;
     }
     const dim3 blk(32, 8, 1);
     const dim3 grd((unsigned)((e->L.nz + 1 + 31) / 32), (unsigned)((e->L.ny + 1 + 7) / 8),
@@ -1338,6 +1347,8 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
                                                                         0);
     }
   }
+  if (e->watchdog > 0 && (t + 1) % e->watchdog == 0)
+    k_watchdog<T><<<4 * 148, 256, 0, s>>>(fields, e->n_lat, e->d_err);
   k_advance<<<1, 1, 0, s>>>(e->d_step);
   e->cur = out;
   return cudaGetLastError();
@@ -1353,6 +1364,7 @@ long long pattern_period(const xfd_engine* e) {
   long long per = 1;
   for (const auto& mv : e->movies) per = per / gcd_ll(per, mv.d.interval) * mv.d.interval;
   if (e->have_nf2ff) per = per / gcd_ll(per, e->nf2ff.batch) * e->nf2ff.batch;
+  if (e->watchdog > 0) per = per / gcd_ll(per, e->watchdog) * e->watchdog;
   if (is_pingpong(e) && per % 2) per *= 2;  // buffers alternate every step
   return per;
 }
@@ -2581,6 +2593,7 @@ xfd_status xfd_sync(xfd_engine* e) {
   int err = 0;
   CUDA_TRY(e, cudaMemcpy(&err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err & 2) return fail(e, XFD_ERR_TIMEOUT, "a sweep stage wait ran out of time");
+  if (err & 4) return fail(e, XFD_ERR_NUMERIC, "the watchdog found a non-finite field value");
   if (err) return fail(e, XFD_ERR_NUMERIC, "TFSF projection left the incident grid");
   return XFD_OK;
 }
@@ -2595,6 +2608,8 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "kernel")) *value = e->kernel_mode;
   else if (!strcmp(name, "ichunk")) *value = e->ichunk;
   else if (!strcmp(name, "march_ichunk")) *value = e->march_ichunk;
+  else if (!strcmp(name, "stage_wait_cycles")) *value = e->stage_wait;
+  else if (!strcmp(name, "watchdog_interval")) *value = e->watchdog;
   else if (!strcmp(name, "march_wide")) *value = e->march_wide ? 1 : 0;
   else if (!strcmp(name, "march_concurrent")) *value = e->march_concurrent ? 1 : 0;
   else if (!strcmp(name, "march_split_axes")) *value = e->march_split_axes ? 1 : 0;
@@ -2644,6 +2659,13 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
   } else if (!strcmp(name, "ichunk")) {
     if (value < 1 || value > 4096) return fail(e, XFD_ERR_INVALID_ARGUMENT, "ichunk range");
     e->ichunk = (int)value;
+  } else if (!strcmp(name, "stage_wait_cycles")) {
+    if (value < 0) return fail(e, XFD_ERR_INVALID_ARGUMENT, "stage_wait_cycles >= 0");
+    e->stage_wait = value;
+  } else if (!strcmp(name, "watchdog_interval")) {
+    if (value < 0 || value > (1LL << 30))
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "watchdog_interval range");
+    e->watchdog = value;
   } else if (!strcmp(name, "march_ichunk")) {
     if (value < 1 || value > 4096)
       return fail(e, XFD_ERR_INVALID_ARGUMENT, "march_ichunk range");
@@ -2688,6 +2710,7 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
     if (e->have_nf2ff) n += 1;
     if (e->have_td) n += 1;
     if (e->probes.n_probes) n += 1;
+    if (e->watchdog == 1) n += 1;
     if (e->n_ovr) n += 1;
     return n + e->n_rec;
   }
@@ -2716,6 +2739,7 @@ int32_t xfd_launches_per_step(const xfd_engine* e) {
   if (e->have_nf2ff) n += 1;
   if (e->have_td) n += 1;
   if (e->probes.n_probes) n += 1;
+  if (e->watchdog == 1) n += 1;  // one scan per step (every K-th step otherwise)
   if (e->n_ovr) n += fused ? 1 : 2;
   if (e->n_hterm) n += 1;
   return n + e->n_rec;

@@ -37,8 +37,9 @@
 // ping-pong mode (march_tma.cuh), the lattice faces k = nz, j = ny by
 // k_edge_pp (kernels.cuh).
 //
-// Stage waits are bounded (a cycle budget); on expiry the CTA sets bit 2 of
-// the engine's error word, drains its loads in flight and returns.
+// Stage waits are bounded (a cycle budget, the engine's "stage_wait_cycles"
+// option); on expiry the CTA sets bit 2 of the engine's error word, drains
+// its loads in flight (with the default budget) and returns.
 #pragma once
 
 #include "march_tma.cuh"
@@ -60,6 +61,7 @@ struct HybP {
   const T* fe[3];
   const T* fh[3];
   int* err;
+  long long wait_budget;  // stage-wait cycles (0: the default)
   HybMaps m;
   int org[3];   // first (k tile, j tile, chunk) of the box
   int shift[3];  // node of tile (0, 0, 0): k0 = 32 x + shift[0], j0, i_lo likewise
@@ -157,6 +159,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 8 ? 3 : 4)
   T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);          // [NC][12]
   T* sN = reinterpret_cast<T*>(smem + S * G::STAGE + G::TB);  // new H
   StageRing ring;
+  ring.set_budget(p.wait_budget);
   ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::TB + G::HN);
   auto sE = [&](int s, int c) {
     return reinterpret_cast<const T*>(smem + s * G::STAGE + G::E_OFF + c * G::pad(G::E_B));

@@ -826,6 +826,26 @@ __global__ void k_ovr_apply(OverrideD<T> o, T* const* fields, T* const* fields_i
 }
 
 // ---------------------------------------------------------------------------
+// NaN / Inf watchdog: a grid-stride scan of the six field buffers (padding
+// included: it stays zero) that sets bit 4 of the error word on the first
+// non-finite value; the host reads it at the next sync (XFD_ERR_NUMERIC).
+// Nothing traps and the sweep runs on.  No counterpart in the reference,
+// whose only numeric check is MLorentzEqDecision::stabilityCondition
+// (src/material/dispersive_material_equation.cpp:56-98).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_watchdog(T* const* fields, long long n_lat, int* err) {
+  bool bad = false;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (int c = 0; c < 6; ++c) {
+    const T* f = fields[c];
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n_lat; q += stride)
+      bad = bad || !isfinite(f[q]);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(err, 4);
+}
+
+// ---------------------------------------------------------------------------
 // Per-node H curl-term corrections, for coefficients that scale one curl term
 // of an H node but not the other (ThinWire::correctUpdateCoefficient,
 // src/object/thin_wire.cpp:42-133, multiplies chxey / chyex / chzex / chzey

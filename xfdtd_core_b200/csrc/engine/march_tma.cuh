@@ -66,6 +66,7 @@ struct MarchTmaP {
   int org[3];
   int box_lo[3], box_hi[3];
   int shift[3];
+  long long wait_budget;  // stage-wait cycles (0: the default)
 };
 
 template <typename T, int TJ, int TK>
@@ -111,10 +112,20 @@ __device__ __forceinline__ T psi_upd(T* ps, T old, T b, T a, T diff) {
 
 // Ring bookkeeping shared by the TMA sweeps: bounded stage waits and the
 // drain on failure.  All threads keep identical copies of parity/pending.
+// Stage waits give up after `budget` cycles (the engine's "stage_wait_cycles"
+// option where the kernel takes it; about 2 s by default); drain() waits for
+// the loads still in flight with the default budget whatever `budget` is, so
+// that no CTA exits while a bulk copy is still writing its shared memory.
+constexpr long long kStageWaitDefault = 4000000000LL;  // about 2 s
+
 struct StageRing {
   uint64_t* bars;
   uint32_t parity = 0;   // bit s: phase to wait for on stage s
   uint32_t pending = 0;  // bit s: a load into stage s is in flight
+  long long budget = kStageWaitDefault;
+  __device__ __forceinline__ void set_budget(long long b) {
+    budget = b > 0 ? b : kStageWaitDefault;
+  }
 
   __device__ __forceinline__ bool try_once(uint32_t a, uint32_t ph) {
     uint32_t done;
@@ -126,19 +137,39 @@ struct StageRing {
         : "memory");
     return done != 0;
   }
+  __device__ __forceinline__ bool test_once(uint32_t a, uint32_t ph) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(ph)
+        : "memory");
+    return done != 0;
+  }
   __device__ bool wait(int s) {
     const uint32_t a = smem_u32(&bars[s]);
     const uint32_t ph = (parity >> s) & 1u;
-    if (!try_once(a, ph)) {
+    if (budget == kStageWaitDefault) {
+      // try_wait may suspend the thread until the phase completes (up to a
+      // system-dependent limit): no issue slots spent on polling.
+      if (!try_once(a, ph)) {
+        const long long t0 = clock64();
+        while (!try_once(a, ph))
+          if (clock64() - t0 > budget) return false;
+      }
+    } else {
+      // A caller-set budget is kept to the cycle: non-blocking probes.
       const long long t0 = clock64();
-      while (!try_once(a, ph))
-        if (clock64() - t0 > 4000000000LL) return false;  // about 2 s
+      while (!test_once(a, ph))
+        if (clock64() - t0 >= budget) return false;
     }
     parity ^= 1u << s;
     pending &= ~(1u << s);
     return true;
   }
   __device__ void drain(int S) {
+    budget = kStageWaitDefault;
     for (int s = 0; s < S; ++s)
       if ((pending >> s) & 1u) wait(s);
   }
@@ -171,6 +202,7 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
   const int n_staged = n_planes + (i_hi <= L.nx ? 1 : 0);
 
   StageRing ring;
+  ring.set_budget(P.wait_budget);
   T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);  // [NC][6] (ca, cb) half-rows
   ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::TB);
   auto halo = [&](int s, int c) {
@@ -375,6 +407,7 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
   const int q_first = i_lo >= 1 ? -1 : 0;  // first staged plane
 
   StageRing ring;
+  ring.set_budget(P.wait_budget);
   T* sT = reinterpret_cast<T*>(smem + S * G::STAGE);  // [NC][6] (ca, cb) half-rows
   ring.bars = reinterpret_cast<uint64_t*>(smem + S * G::STAGE + G::TB);
   auto slot = [](int q) { return (q + 1) % S; };
