@@ -94,6 +94,23 @@ xfd_status xfd_set_material_classes(xfd_engine* e, const double* table, int32_t 
 xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, const int32_t* comp,
                                const double* ca, const double* cb);
 
+/* Halo copy between two engines of one slab decomposition (along x):
+ * copies plane `src_plane` of the components comps[0 .. n_comp) (0..5: Ex Ey
+ * Ez Hx Hy Hz) of `src`'s current fields into plane `dst_plane` of `dst`'s
+ * current fields.  The engines must share the y-z lattice (ny, nz) and the
+ * precision; they may sit on different devices (a peer copy, through NVLink
+ * where the devices are peers).  Ordering is on the streams: the copy waits
+ * for every step queued on `src`, and `src`'s next queued work waits for the
+ * copy; `dst`'s next step comes after it on `dst`'s stream.  Asynchronous;
+ * xfd_sync(dst) waits for it.
+ * Replaces: the reference's per-step MPI halo exchange
+ * (MpiSupport::sendRecvHyXHead/Tail etc., src/parallel/mpi_support.cpp:98-229,
+ * called from Domain::exchangeH, src/domain/domain.cpp:237-279); this
+ * library's slabs exchange the tangential E of one plane instead (the dual
+ * scheme, see xfdtd_core_b200/slab.py). */
+xfd_status xfd_halo_copy(xfd_engine* dst, int32_t dst_plane, xfd_engine* src, int32_t src_plane,
+                         int32_t n_comp, const int32_t* comps);
+
 /* Per-node H curl-term corrections: after the H sweep of every step, the H
  * component comp[q] at node (node[3q], node[3q+1], node[3q+2]) gets
  *   delta_a[q] * (E_a[x_b+1] - E_a) + delta_b[q] * (E_b[x_a+1] - E_b)

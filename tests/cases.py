@@ -48,6 +48,22 @@ class KernelCase:
         self.ade = None
         self.nf2ff = None
 
+    @classmethod
+    def from_setup(cls, setup):
+        """A case over explicit engine inputs (xfdtd_core_b200.slab.LocalSetup:
+        one slab of a decomposed lattice), for its oracle and engine."""
+        self = cls.__new__(cls)
+        self.rng = np.random.default_rng(0)
+        self.n = tuple(setup.n)
+        self.table = setup.table
+        self.lattice_class = setup.lattice_class
+        self.fe, self.fh = list(setup.fe), list(setup.fh)
+        self.fields = [np.array(f) for f in setup.fields]
+        self.slabs = [dict(s) for s in setup.slabs]
+        self.lumped = [dict(l) for l in setup.lumped]
+        self.tfsf = self.ade = self.nf2ff = None
+        return self
+
     # ------------------------------------------------------------- oracle
     def _cls_coeff(self, comp6: int):
         shp = comp_shape(self.n, comp6)

@@ -1,0 +1,94 @@
+"""The x-slab decomposition (xfdtd_core_b200/slab.py) on CPU: two and three
+gloo ranks each run the oracle on their slab of a seeded lattice (random
+material classes and curl factors, CPML on all six faces, a lumped current
+source) and exchange the ghost planes' E_y, E_z after every step; the owned
+values gathered on rank 0 equal the one-domain oracle run bit for bit.  Plus
+the planning rules: cuts keep clear of the x-normal CPML layers."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+N = (30, 9, 11)
+SLABS = ((0, True, 3), (0, False, 2), (1, True, 2), (1, False, 3), (2, True, 2), (2, False, 2))
+STEPS = 7
+
+
+def _case():
+    from tests.cases import KernelCase
+    c = KernelCase(n=N, seed=21, slabs=SLABS)
+    c.add_lumped(comp=2, s=(8, 4, 4), e=(10, 6, 6), n_steps=STEPS)   # across a ghost region
+    c.add_lumped(comp=0, s=(14, 3, 3), e=(17, 5, 5), n_steps=STEPS)  # E_x cells
+    return c
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    from tests.cases import KernelCase
+    from xfdtd_core_b200 import slab
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    case = _case()
+    parts = slab.plan(N[0], world, x_cpml=(3, 2))
+    local = slab.split(case, parts)[rank]
+    orc = KernelCase.from_setup(local).oracle()
+    plan = slab.exchanges(parts)
+    for _ in range(STEPS):
+        orc.run(1)
+        reqs, bufs = [], []
+        for dst, dst_plane, src, src_plane in plan:
+            for c in slab.GHOST_COMPONENTS:
+                if src == rank:
+                    reqs.append(dist.isend(torch.from_numpy(orc.e[c][src_plane].copy()), dst))
+                if dst == rank:
+                    b = torch.empty(orc.e[c][dst_plane].shape, dtype=torch.float64)
+                    reqs.append(dist.irecv(b, src))
+                    bufs.append((c, dst_plane, b))
+        for r in reqs:
+            r.wait()
+        for c, plane, b in bufs:
+            orc.e[c][plane] = b.numpy()
+    got = [None] * world
+    dist.all_gather_object(got, [a.copy() for a in orc.e + orc.h])
+    if rank == 0:
+        fields = slab.gather(parts, got, N)
+        np.savez(os.path.join(out, "slab.npz"), *fields)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_ranks_equal_one_domain(tmp_path, world):
+    import torch.multiprocessing as mp
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn")
+    z = np.load(tmp_path / "slab.npz")
+    got = [z[f"arr_{c}"] for c in range(6)]
+    orc = _case().oracle()
+    orc.run(STEPS)
+    for c, (g, w) in enumerate(zip(got, orc.e + orc.h)):
+        assert g.shape == w.shape and np.array_equal(g, w), c
+
+
+def test_plan_keeps_cuts_clear_of_x_cpml():
+    from xfdtd_core_b200 import slab
+    parts = slab.plan(100, 4, x_cpml=(10, 10))
+    assert [p.own_lo for p in parts] == [0, 25, 50, 75] and parts[-1].own_hi == 100
+    assert [(p.lo, p.hi) for p in parts] == [(0, 26), (24, 51), (49, 76), (74, 100)]
+    with pytest.raises(ValueError):
+        slab.plan(24, 2, x_cpml=(11, 10))  # ghost plane 11 of the cut at 12 is a CPML layer
+    ex = slab.exchanges(parts)
+    assert (1, 0, 0, 24) in ex and (0, 26, 1, 2) in ex and len(ex) == 6

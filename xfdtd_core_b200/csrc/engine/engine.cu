@@ -149,6 +149,7 @@ struct xfd_engine {
   // from and joined back into `stream` (also inside graph capture).
   cudaStream_t side[kSides]{};
   cudaEvent_t fork_ev = nullptr, join_ev[kSides]{};
+  cudaEvent_t halo_ev = nullptr;  // xfd_halo_copy: this engine's queued work
   bool march_concurrent = true;
   std::vector<void*> host_allocs;
 
@@ -1711,6 +1712,7 @@ void xfd_destroy(xfd_engine* e) {
     if (e->side[q]) cudaStreamDestroy(e->side[q]);
   }
   if (e->fork_ev) cudaEventDestroy(e->fork_ev);
+  if (e->halo_ev) cudaEventDestroy(e->halo_ev);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -1827,6 +1829,59 @@ xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, co
   e->ovr_cb.assign(cb, cb + n);
   e->n_ovr = n;
   e->graph_dirty = true;
+  return XFD_OK;
+}
+
+namespace {
+xfd_status halo_event(xfd_engine* e) {
+  if (e->halo_ev) return XFD_OK;
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  CUDA_TRY(e, cudaEventCreateWithFlags(&e->halo_ev, cudaEventDisableTiming));
+  return XFD_OK;
+}
+}  // namespace
+
+xfd_status xfd_halo_copy(xfd_engine* dst, int32_t dst_plane, xfd_engine* src, int32_t src_plane,
+                         int32_t n_comp, const int32_t* comps) {
+  if (!dst || !src || dst == src || n_comp < 1 || n_comp > 6 || !comps)
+    return fail(dst, XFD_ERR_INVALID_ARGUMENT, "bad halo copy arguments");
+  if (dst->precision != src->precision || dst->L.ny != src->L.ny || dst->L.nz != src->L.nz ||
+      dst->L.KP != src->L.KP)
+    return fail(dst, XFD_ERR_INVALID_ARGUMENT, "halo copy between lattices of other y-z extent");
+  for (int q = 0; q < n_comp; ++q) {
+    const int c = comps[q];
+    // planes along x: nx + 1 of E_y, E_z, H_x; nx of E_x, H_y, H_z
+    const int extra = (c == 1 || c == 2 || c == 3) ? 1 : 0;
+    if (c < 0 || c > 5 || dst_plane < 0 || dst_plane >= dst->L.nx + extra || src_plane < 0 ||
+        src_plane >= src->L.nx + extra)
+      return fail(dst, XFD_ERR_INVALID_ARGUMENT, "halo copy component %d / plane out of range", c);
+  }
+  xfd_status st;
+  if ((st = halo_event(src)) != XFD_OK) return st;
+  if ((st = halo_event(dst)) != XFD_OK) return st;
+  // dst waits for the source's queued steps, copies, and the source's next
+  // step waits for the copy (its in-place sweeps would overwrite the plane).
+  CUDA_TRY(src, cudaSetDevice(src->device));
+  CUDA_TRY(src, cudaEventRecord(src->halo_ev, src->stream));
+  CUDA_TRY(dst, cudaSetDevice(dst->device));
+  CUDA_TRY(dst, cudaStreamWaitEvent(dst->stream, src->halo_ev, 0));
+  const size_t plane = (size_t)dst->L.NY * dst->L.KP;
+  for (int q = 0; q < n_comp; ++q) {
+    const int c = comps[q];
+    unsigned char* d = static_cast<unsigned char*>(dst->fbuf[dst->cur][c]) +
+                       (size_t)dst_plane * plane * dst->wsize;
+    const unsigned char* sp = static_cast<const unsigned char*>(src->fbuf[src->cur][c]) +
+                              (size_t)src_plane * plane * src->wsize;
+    if (dst->device == src->device)
+      CUDA_TRY(dst, cudaMemcpyAsync(d, sp, plane * dst->wsize, cudaMemcpyDeviceToDevice,
+                                    dst->stream));
+    else
+      CUDA_TRY(dst, cudaMemcpyPeerAsync(d, dst->device, sp, src->device, plane * dst->wsize,
+                                        dst->stream));
+  }
+  CUDA_TRY(dst, cudaEventRecord(dst->halo_ev, dst->stream));
+  CUDA_TRY(src, cudaSetDevice(src->device));
+  CUDA_TRY(src, cudaStreamWaitEvent(src->stream, dst->halo_ev, 0));
   return XFD_OK;
 }
 

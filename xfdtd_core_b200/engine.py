@@ -128,6 +128,7 @@ def load(build_if_missing: bool = True):
                                 ctypes.c_int),
         "xfd_set_h_term_overrides": ([vp, _i64, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _dp,
                                       _dp], ctypes.c_int),
+        "xfd_halo_copy": ([vp, _i32, vp, _i32, _i32, ctypes.POINTER(_i32)], ctypes.c_int),
         "xfd_checkpoint_save": ([vp, _i32], ctypes.c_int),
         "xfd_checkpoint_load": ([vp, _i32], ctypes.c_int),
         "xfd_checkpoint_drop": ([vp, _i32], ctypes.c_int),
@@ -164,7 +165,7 @@ def exported_symbols() -> List[str]:
             "xfd_download_field", "xfd_run", "xfd_sync", "xfd_current_step", "xfd_set_option",
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
             "xfd_launches_per_step", "xfd_stencil_bytes_per_step",
-            "xfd_algorithmic_bytes_per_step", "xfd_set_e_overrides", "xfd_set_h_term_overrides",
+            "xfd_algorithmic_bytes_per_step", "xfd_set_e_overrides", "xfd_set_h_term_overrides", "xfd_halo_copy",
             "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
             "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_set_nf2ff_td", "xfd_get_nf2ff_td",
             "xfd_add_probe", "xfd_get_probe",
@@ -345,6 +346,13 @@ class Engine:
     @property
     def step(self) -> int:
         return int(self.L.xfd_current_step(self.h))
+
+    def halo_copy_from(self, dst_plane: int, src: "Engine", src_plane: int,
+                       comps: Sequence[int]):
+        """xfd_halo_copy: planes of `src`'s current fields into this engine's."""
+        arr = (_i32 * len(comps))(*comps)
+        self._check(self.L.xfd_halo_copy(self.h, int(dst_plane), src.h, int(src_plane),
+                                         len(comps), arr), "halo_copy")
 
     def stream(self) -> int:
         return int(self.L.xfd_stream(self.h) or 0)

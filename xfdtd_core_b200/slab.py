@@ -1,0 +1,235 @@
+"""Slab decomposition of one lattice along x over several engines (GPUs).
+
+The reference decomposes its grid over MPI ranks in slabs with an overlap
+and exchanges a halo after every step (src/simulation/simulation.cpp:530-591,
+src/domain/domain.cpp:237-279, src/parallel/mpi_support.cpp:98-229).  Here
+rank r owns the cells [c_r, c_{r+1}) of the global x range and runs an
+ordinary engine on the local lattice of cells [a_r, b_r) = [c_r - 1, c_{r+1}
++ 1) (no extra cell at the global faces): one ghost cell on each interior
+side.  One time step of the local engine then leaves every value of its
+lattice exact except E_y and E_z on the two ghost planes a_r and b_r, which
+the engine treats as lattice boundaries and does not update:
+
+* H_y, H_z of a cell need E on the two planes around it, H_x of a plane
+  needs E in that plane: all local, exact when the ghost planes held the
+  exact E at the start of the step;
+* E_x of a cell needs H of that cell only; E_y, E_z of the interior planes
+  a_r + 1 .. b_r - 1 need H_y, H_z of the cells either side: all local.
+  (H_x on the high ghost plane is not updated either; only the ghost planes'
+  own E reads it.)
+
+So after every step each rank receives E_y, E_z of its ghost plane a_r from
+rank r - 1, where that plane is interior, and of b_r from rank r + 1: two
+tangential components of one plane per neighbour and step, the dual of the
+reference's H halo.  Values in the ghost cells (E_x, H_y, H_z, ADE and CPML
+state there) are computed by both neighbours from the same inputs and agree
+bit for bit.  The x-normal CPML slabs stay whole on the first and last rank:
+cuts keep the ghost cells and planes clear of their layers.  y- and
+z-normal slabs, materials, curl factors, fields and lumped sources are cut
+by intersection with each local lattice (sources in a ghost region run on
+both ranks, which keeps the ghost values exact).  TFSF, ADE and NF2FF are
+not split here: lattices with them run on one engine.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+# Field component -> axis of its x index: E_x, H_y, H_z live on cells (nx
+# values), E_y, E_z, H_x on node planes (nx + 1 values).
+ON_CELLS = (True, False, False, False, True, True)
+GHOST_COMPONENTS = (1, 2)  # E_y, E_z
+
+
+@dataclass
+class SlabPart:
+    rank: int
+    own_lo: int  # first owned cell (and node plane)
+    own_hi: int  # one past the last owned cell; the last rank also owns plane nx
+    lo: int      # first cell of the local lattice (own_lo - 1 except on rank 0)
+    hi: int      # one past its last cell (own_hi + 1 except on the last rank)
+
+    @property
+    def n(self) -> int:
+        return self.hi - self.lo
+
+
+def plan(nx: int, ranks: int, x_cpml: Tuple[int, int] = (0, 0)) -> List[SlabPart]:
+    """Cuts of nx cells into `ranks` slabs of nearly equal size.  x_cpml:
+    thicknesses of the x-normal CPML slabs at the low and high face; every
+    cut c keeps its ghost planes c - 1 .. c + 1 clear of their layers
+    (E layers 1 .. lo, H layers 0 .. lo-1 at the low face; from nx - hi up
+    at the high face), else ValueError."""
+    if ranks < 1:
+        raise ValueError("ranks must be >= 1")
+    cuts = [round(r * nx / ranks) for r in range(ranks + 1)]
+    lo_t, hi_t = x_cpml
+    for c in cuts[1:-1]:
+        if c - 1 <= lo_t or c + 1 >= nx - hi_t:
+            raise ValueError(f"cut at cell {c} meets an x-normal CPML slab "
+                             f"(thickness {lo_t} / {hi_t} of {nx} cells)")
+    if any(b - a < 2 for a, b in zip(cuts, cuts[1:])):
+        raise ValueError("slabs of fewer than two cells")
+    parts = []
+    for r in range(ranks):
+        a = cuts[r] - (1 if r > 0 else 0)
+        b = cuts[r + 1] + (1 if r < ranks - 1 else 0)
+        parts.append(SlabPart(r, cuts[r], cuts[r + 1], a, b))
+    return parts
+
+
+def _x_range(part: SlabPart, comp6: int) -> slice:
+    """Local x index range of a component in global indices."""
+    return slice(part.lo, part.hi if ON_CELLS[comp6] else part.hi + 1)
+
+
+@dataclass
+class LocalSetup:
+    """Engine inputs of one slab: the arrays of xfd_set_material_classes,
+    xfd_set_curl_factors, xfd_add_cpml, xfd_add_current_source and
+    xfd_upload_fields over the local lattice."""
+    n: Tuple[int, int, int]
+    table: np.ndarray
+    lattice_class: np.ndarray
+    fe: List[np.ndarray]
+    fh: List[np.ndarray]
+    slabs: List[Dict]
+    lumped: List[Dict]
+    fields: List[np.ndarray]
+
+
+def split(setup, parts: Sequence[SlabPart]) -> List[LocalSetup]:
+    """Cuts a lattice set-up (attributes n, table, lattice_class, fe, fh,
+    slabs, lumped, fields; optional tfsf / ade / nf2ff must be None) into the
+    local set-ups of `parts`."""
+    for name in ("tfsf", "ade", "nf2ff"):
+        if getattr(setup, name, None):
+            raise ValueError(f"{name} is not split across slabs")
+    nx, ny, nz = setup.n
+    out = []
+    for p in parts:
+        a, b = p.lo, p.hi
+        slabs = []
+        for s in setup.slabs:
+            if s["m"] != 0:
+                slabs.append(dict(s))
+                continue
+            # whole x slab on the rank that holds its layers, shifted to local planes
+            first = min(s["e_start"], s["h_start"])
+            last = max(s["e_start"], s["h_start"]) + s["n"]
+            if first >= a and last <= b + 1:
+                q = dict(s)
+                q["e_start"] = s["e_start"] - a
+                q["h_start"] = s["h_start"] - a
+                slabs.append(q)
+            elif first < b + 1 and last > a:
+                raise ValueError("an x-normal CPML slab crosses a slab cut")
+        lumped = []
+        for l in setup.lumped:
+            c = l["comp"]
+            hi_x = b if ON_CELLS[c] else b + 1
+            s0, e0 = max(l["s"][0], a), min(l["e"][0], hi_x)
+            if s0 >= e0:
+                continue
+            q = dict(l)
+            q["s"] = [s0 - a, l["s"][1], l["s"][2]]
+            q["e"] = [e0 - a, l["e"][1], l["e"][2]]
+            q["coff"] = np.ascontiguousarray(l["coff"][s0 - l["s"][0]:e0 - l["s"][0]])
+            lumped.append(q)
+        fields = [np.ascontiguousarray(f[_x_range(p, c)]) for c, f in enumerate(setup.fields)]
+        out.append(LocalSetup(
+            n=(b - a, ny, nz), table=setup.table,
+            lattice_class=np.ascontiguousarray(setup.lattice_class[a:b + 1]),
+            fe=[np.ascontiguousarray(setup.fe[0][a:b + 1])] + [setup.fe[1], setup.fe[2]],
+            fh=[np.ascontiguousarray(setup.fh[0][a:b])] + [setup.fh[1], setup.fh[2]],
+            slabs=slabs, lumped=lumped, fields=fields))
+    return out
+
+
+def exchanges(parts: Sequence[SlabPart]) -> List[Tuple[int, int, int, int]]:
+    """The ghost-plane copies after every step: (destination rank, its local
+    plane, source rank, its local plane), for E_y and E_z alike."""
+    out = []
+    for r, p in enumerate(parts):
+        if r > 0:
+            q = parts[r - 1]
+            out.append((r, 0, r - 1, p.lo - q.lo))
+        if r < len(parts) - 1:
+            q = parts[r + 1]
+            out.append((r, p.n, r + 1, p.hi - q.lo))
+    return out
+
+
+def owned(part: SlabPart, comp6: int, nx: int) -> Tuple[slice, slice]:
+    """(global, local) x index ranges of the values a rank owns: its cells,
+    or its node planes [own_lo, own_hi) -- the last rank also plane nx."""
+    hi = part.own_hi
+    if not ON_CELLS[comp6] and part.own_hi == nx:
+        hi = nx + 1
+    return slice(part.own_lo, hi), slice(part.own_lo - part.lo, hi - part.lo)
+
+
+def gather(parts: Sequence[SlabPart], local_fields: Sequence[Sequence[np.ndarray]],
+           n: Tuple[int, int, int]) -> List[np.ndarray]:
+    """The global fields from every rank's owned values."""
+    from xfdtd_core_b200.engine import comp_shape
+    out = [np.empty(comp_shape(n, c), dtype=local_fields[0][c].dtype) for c in range(6)]
+    for p, f in zip(parts, local_fields):
+        for c in range(6):
+            g, l = owned(p, c, n[0])
+            out[c][g] = f[c][l]
+    return out
+
+
+# ------------------------------------------------------------ engine runner
+class SlabEngines:
+    """One engine per slab in this process (each on its own device, or all on
+    one), stepped together: every step runs each engine one step, then copies
+    the ghost planes' E_y, E_z with xfd_halo_copy (device to device, a peer
+    copy between devices; ordered on the engines' streams, so no engine
+    starts its next step before its ghost planes hold the neighbours' values
+    or overwrites a plane a neighbour is still copying)."""
+
+    def __init__(self, setups: Sequence[LocalSetup], parts: Sequence[SlabPart],
+                 devices: Optional[Sequence[int]] = None, precision: int = 0,
+                 n_steps: int = 1, options: Optional[Dict[str, int]] = None):
+        from xfdtd_core_b200.engine import Engine
+        self.parts = list(parts)
+        self.devices = list(devices) if devices is not None else [0] * len(parts)
+        self.engines = []
+        for s, dev in zip(setups, self.devices):
+            e = Engine(*s.n, precision=precision, n_steps=n_steps, dt=1.0, device=dev)
+            for k, v in (options or {}).items():
+                e.set_option(k, v)
+            e.set_material_classes(s.table, s.lattice_class)
+            e.set_curl_factors(s.fe, s.fh)
+            for sl in s.slabs:
+                e.add_cpml(sl["m"], sl["neg"], sl["n"], sl["e_start"], sl["h_start"], sl["a_e"],
+                           sl["b_e"], sl["a_h"], sl["b_h"])
+            for l in s.lumped:
+                e.add_current_source(l["comp"], l["s"], l["e"], l["coff"], l["wave"])
+            e.upload_fields([f.astype(e.dtype) for f in s.fields])
+            self.engines.append(e)
+        self.plan = exchanges(self.parts)
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            for e in self.engines:
+                e.run(1)
+            for dst, dst_plane, src, src_plane in self.plan:
+                self.engines[dst].halo_copy_from(dst_plane, self.engines[src], src_plane,
+                                                 GHOST_COMPONENTS)
+
+    def sync(self):
+        for e in self.engines:
+            e.sync()
+
+    def fields(self) -> List[np.ndarray]:
+        n = (self.parts[-1].own_hi,) + tuple(self.engines[0].n[1:])
+        return gather(self.parts, [e.download_fields() for e in self.engines], n)
+
+    def close(self):
+        for e in self.engines:
+            e.close()
