@@ -869,12 +869,15 @@ __global__ void k_hterm(const __grid_constant__ HTermD<T> h, Lat L, T* const* fi
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= h.n) return;
   const int c = h.comp[q], a = (c + 1) % 3, b = (c + 2) % 3;
-  const long long st[3] = {(long long)L.NY * L.KP, (long long)L.KP, 1};
+  // lattice strides by selects (no run-time-indexed local array)
+  auto stride = [&](int d) {
+    return d == 0 ? (long long)L.NY * L.KP : (d == 1 ? (long long)L.KP : 1LL);
+  };
   const long long id = h.node[q];
   const T* Ea = fields[a];
   const T* Eb = fields[b];
   T* H = fields[3 + c];
-  H[id] += h.da[q] * (Ea[id + st[b]] - Ea[id]) + h.db[q] * (Eb[id + st[a]] - Eb[id]);
+  H[id] += h.da[q] * (Ea[id + stride(b)] - Ea[id]) + h.db[q] * (Eb[id + stride(a)] - Eb[id]);
 }
 
 // ---------------------------------------------------------------------------
