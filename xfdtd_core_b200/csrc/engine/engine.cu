@@ -327,11 +327,10 @@ inline bool uses_tma(const xfd_engine* e) {
   return e->kernel_mode == 2 || e->kernel_mode == 4 || e->kernel_mode == 5 ||
          e->kernel_mode == 6 || e->kernel_mode == 7;
 }
-// The CPML H psi buffer the next step reads: the ping-pong sweeps (1, 2, 5,
-// 6, 7) alternate it with the fields (a step reads psi_h[cur], writes
-// psi_h[1 - cur]: the fused box kernel's halo recomputes read psi values the
-// owning tile is updating); the in-place sweeps keep it where the fields are.
-inline int psi_h_buf(const xfd_engine* e) { return e->cur; }
+// The CPML H psi buffer the next step reads: the fused sweeps ping-pong it
+// with the fields; sweep 7 updates it in place (the split CPML forms) and
+// keeps it in buffer 0; the in-place sweeps use the field buffer's.
+inline int psi_h_buf(const xfd_engine* e) { return e->kernel_mode == 7 ? 0 : e->cur; }
 
 template <typename T>
 YeeP<T> yee_params(xfd_engine* e) {
@@ -919,12 +918,10 @@ xfd_status build_march_tiles(xfd_engine* e) {
   return XFD_OK;
 }
 
-// pp_psi: H psi read from psi_h[cur] and written to psi_h[1 - cur] (sweep 7);
-// else updated in place.
 template <typename T>
-MarchP<T> march_params(xfd_engine* e, bool pp_psi = false) {
+MarchP<T> march_params(xfd_engine* e) {
   const int pb = psi_h_buf(e);
-  const FusedP<T> f = fused_params<T>(e, pb, pp_psi ? 1 - pb : pb);
+  const FusedP<T> f = fused_params<T>(e, pb, pb);
   MarchP<T> p{};
   p.L = f.L;
   for (int c = 0; c < 6; ++c) p.f[c] = static_cast<T*>(e->fbuf[e->cur][c]);
@@ -972,7 +969,7 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
   const dim3 blk_m(32, kMTJ, 1);
   T* const* fields_in = reinterpret_cast<T* const*>(e->d_fields[in]);
   MarchTmaP<T> mh{};
-  mh.p = march_params<T>(e, true);
+  mh.p = march_params<T>(e);
   for (int c = 0; c < 6; ++c) mh.p.f[c] = static_cast<T*>(e->fbuf[out][c]);
   mh.m = e->mtma[in];  // old E halo boxes, old H tiles
   mh.err = e->d_err;
@@ -989,11 +986,6 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
   }
   YeeP<T> yp = yee_params<T>(e);
   for (int c = 0; c < 6; ++c) yp.f[c] = static_cast<T*>(e->fbuf[out][c]);
-  for (size_t q = 0; q < e->slabs.size(); ++q)
-    for (int w = 0; w < 2; ++w) {  // H psi: read the input buffer's, write the output's
-      yp.slab[q].psi_h_rd[w] = static_cast<const T*>(e->slabs[q].psi_h[in][w]);
-      yp.slab[q].psi_h[w] = static_cast<T*>(e->slabs[q].psi_h[out][w]);
-    }
   const unsigned edge_blocks = (unsigned)((edge_nodes(e->L) + 255) / 256);
   cudaError_t c = cudaSuccess;
   auto fork = [&](int first) {

@@ -45,7 +45,6 @@ struct SlabD {
   const T* b_h;
   T* psi_e[2];
   T* psi_h[2];
-  const T* psi_h_rd[2];  // the old H psi when it is not read from psi_h (ping-pong)
 };
 
 template <typename T>
@@ -124,10 +123,8 @@ __device__ __forceinline__ void update_h_node(const YeeP<T>& p, int i, int j, in
       const int dc = which == 0 ? (sl.m + 2) % 3 : (sl.m + 1) % 3;
       const T* D = rd ? rd[dc] : p.f[dc];
       const T diff = D[id + sel3(sl.m, st[0], st[1], st[2])] - D[id];
-      const long long pq = psi_index(sl, L, i, j, k, l);
-      T* ps = sl.psi_h[which] + pq;
-      const T old = sl.psi_h_rd[which] ? sl.psi_h_rd[which][pq] : *ps;
-      const T psi = sl.b_h[l] * old + sl.a_h[l] * diff;
+      T* ps = sl.psi_h[which] + psi_index(sl, L, i, j, k, l);
+      const T psi = sl.b_h[l] * *ps + sl.a_h[l] * diff;
       *ps = psi;
       h += (which == 0 ? cb : -cb) * psi;
     }

@@ -252,35 +252,22 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
   const int ly = (CP && (AX & 2) && act) ? layer_of(p.slab[1], j, false, qy) : -1;
   const int lz = (CP && (AX & 4) && act) ? layer_of(p.slab[2], k, false, qz) : -1;
   T ay = 0, by = 0, az = 0, bz = 0;
-  // psi pointers: old values read through *_in (the other buffer in the
-  // ping-pong sweep 7, the same one in place), new values stored through the
-  // plain ones.
   T* psy[2] = {nullptr, nullptr};
   T* psz[2] = {nullptr, nullptr};
-  const T* psy_in[2] = {nullptr, nullptr};
-  const T* psz_in[2] = {nullptr, nullptr};
   long long psy_st = 0, psz_st = 0;
   if (ly >= 0) {
     const SlabAxisD<T>& A = p.slab[1];
     ay = A.a_h[qy][ly];
     by = A.b_h[qy][ly];
     psy_st = (long long)A.n[qy] * KP;
-    const long long o = (long long)ly * KP + k;
-    for (int w = 0; w < 2; ++w) {
-      psy[w] = A.psi_h_out[qy][w] + o;
-      psy_in[w] = A.psi_h_in[qy][w] + o;
-    }
+    for (int w = 0; w < 2; ++w) psy[w] = A.psi_h_out[qy][w] + (long long)ly * KP + k;
   }
   if (lz >= 0) {
     const SlabAxisD<T>& A = p.slab[2];
     az = A.a_h[qz][lz];
     bz = A.b_h[qz][lz];
     psz_st = (long long)L.NY * A.n[qz];
-    const long long o = (long long)j * A.n[qz] + lz;
-    for (int w = 0; w < 2; ++w) {
-      psz[w] = A.psi_h_out[qz][w] + o;
-      psz_in[w] = A.psi_h_in[qz][w] + o;
-    }
+    for (int w = 0; w < 2; ++w) psz[w] = A.psi_h_out[qz][w] + (long long)j * A.n[qz] + lz;
   }
   T* Hx = p.f[3] + row;
   T* Hy = p.f[4] + row;
@@ -293,17 +280,17 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
   // ahead, so their DRAM latency overlaps the compute of the plane before.
   T pv[6] = {};
   auto load_psi = [&](int i) {
-    pv[0] = ly >= 0 ? psy_in[1][i * psy_st] : T(0);
-    pv[5] = ly >= 0 ? psy_in[0][i * psy_st] : T(0);
-    pv[1] = lz >= 0 ? psz_in[0][i * psz_st] : T(0);
-    pv[3] = lz >= 0 ? psz_in[1][i * psz_st] : T(0);
+    pv[0] = ly >= 0 ? psy[1][i * psy_st] : T(0);
+    pv[5] = ly >= 0 ? psy[0][i * psy_st] : T(0);
+    pv[1] = lz >= 0 ? psz[0][i * psz_st] : T(0);
+    pv[3] = lz >= 0 ? psz[1][i * psz_st] : T(0);
     int qx = 0;
     const int cx = (AX & 1) ? p.xl[i].x : -1;
     const int lx = (act && cx >= 0) ? (cx >> 1) : -1;
     qx = cx & 1;
     const long long ox = (long long)lx * PS + row;
-    pv[2] = lx >= 0 ? p.slab[0].psi_h_in[qx][0][ox] : T(0);
-    pv[4] = lx >= 0 ? p.slab[0].psi_h_in[qx][1][ox] : T(0);
+    pv[2] = lx >= 0 ? p.slab[0].psi_h_out[qx][0][ox] : T(0);
+    pv[4] = lx >= 0 ? p.slab[0].psi_h_out[qx][1][ox] : T(0);
   };
   if constexpr (CP) load_psi(i_lo);
 
