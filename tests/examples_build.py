@@ -47,7 +47,8 @@ EXAMPLES = {
     "lorentz_sphere_scatter": "dispersive_sphere_scatter/lorentz_sphere_scatter.cpp",
 }
 # The ones the GPU tests run (linked executables); the rest are compiled only.
-LINKED = ("dielectric_sphere_scatter", "half_wave_dipole")
+LINKED = ("dielectric_sphere_scatter", "half_wave_dipole", "dielectric_cube_scatter",
+          "drude_sphere_scatter", "microstrip_line")
 
 
 def example_dir(ref: str = DEFAULT_REFERENCE) -> str:

@@ -295,7 +295,9 @@ static xfdtd_scene* buildScene(const char* path, int32_t precision) {
       const auto interval = static_cast<std::size_t>(num(in));
       auto fm = std::make_unique<FieldMonitor>(
           std::make_unique<Cube>(Vector{ox, oy, oz}, Vector{sx, sy, sz}), parseField(field));
-      auto mv = std::make_shared<MovieMonitor>(std::move(fm), interval, name, name);
+      // no output directory: the scene's frames are written by
+      // xfdtd_scene_write_outputs under the directory it is given
+      auto mv = std::make_shared<MovieMonitor>(std::move(fm), interval, name, "");
       sc->movies.push_back(mv);
       sc->sim->addMonitor(mv);
     } else if (kw == "field_time") {

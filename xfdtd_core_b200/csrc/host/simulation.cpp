@@ -1501,6 +1501,22 @@ void Simulation::finish() {
       for (std::size_t q = 0; q < per; ++q)
         out[f][q] = (w == 8) ? reinterpret_cast<double*>(buf.data())[f * per + q]
                              : reinterpret_cast<float*>(buf.data())[f * per + q];
+    // The frames on disk, as the reference's MovieMonitor::update writes them
+    // during its run (src/monitor/movie_monitor.cpp:26-34, 58-63): one
+    // <outputDir>/<step, 5 digits>.npy per frame, the monitor box in (i, j, k).
+    if (!h.mon->outputDir().empty()) {
+      const std::filesystem::path dir{h.mon->outputDir()};
+      std::filesystem::create_directories(dir);
+      const std::size_t sx = (std::size_t)(h.e[0] - h.s[0]), sy = (std::size_t)(h.e[1] - h.s[1]),
+                        sz = (std::size_t)(h.e[2] - h.s[2]);
+      for (std::size_t f = 0; f < out.size(); ++f) {
+        auto a = Array3D<Real>::from_shape({sx, sy, sz});
+        std::copy(out[f].begin(), out[f].end(), a.data());
+        std::ostringstream nm;
+        nm << std::setw(5) << std::setfill('0') << f * h.mon->frameInterval();
+        xt::dump_npy((dir / (nm.str() + ".npy")).string(), a);
+      }
+    }
   }
   for (auto& p : I.probes) {
     if (p.id < 0) continue;
