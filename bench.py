@@ -17,15 +17,17 @@ Lines (one JSON line on rank 0):
   reference:  python bench.py --impl reference ...  (the CPU restatement of
               the reference's std::thread FP64 path, all host threads)
 
-Under torchrun each rank runs its own replica of the scene (the path's
-multi-GPU form in this round is replicas: no data-path collective), the
+Under torchrun each rank runs its own replica of the scene (the bench's
+multi-GPU form is replicas: no data-path collective), the
 timed region is bracketed by barriers, and the time is the max over ranks.
 
 --workload batched: 96 independent sphere scenes of uneven sizes (64^3 to
 224^3 cells, numpy default_rng(1)), each with its own TFSF plane wave at a
 random angle, FP32, advanced together through the batch entry points
-(xfd_batch_*: every phase of a step one launch over all scenes' tiles, the
-tile depth chosen by the autotuner during warm-up).  A step advances every
+(xfd_batch_*: the autotuner picks, during warm-up, between one launch of the
+persistent work-queue kernel per step (tile rows 8 or 16) and a launch per
+phase and sweep form, and the tile depth; `--batch-queue 1` / `0` pins the
+form).  A step advances every
 scene by one time step; `value` counts the cells of all scenes.  The same
 scenes run one at a time (FP32, and the FP64 plain form) are reported under
 "forms".  Under torchrun the scenes are dealt round-robin to the ranks.
@@ -413,9 +415,13 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
     mine = params[rank::world]
     all_cells = sum(p["n"] ** 3 for p in params)
     seq = max(1, args.seq_steps)
-    # Warm-up holds the autotuning: 4 depths x (1 warm + K timed) steps.
-    tune = max(1, warmup // 4 - 1)
-    warm = max(warmup, 4 * (1 + tune))
+    # Warm-up holds the autotuning: 12 candidates x (1 warm + K timed) steps
+    # (the queue form at tile rows 8, 16 and the launch per phase at 8, each
+    # at depths 8, 16, 32, 64).  --batch-queue 0 / 1 without --autotune pins
+    # the form instead.
+    n_cand = 12
+    tune = max(1, warmup // n_cand - 1) if args.batch_queue < 0 else 0
+    warm = max(warmup, n_cand * (1 + tune)) if tune else warmup
     n_total = warm + 2 * steps + seq + 36
     t0 = time.perf_counter()
     runs = [SceneRun(S.batched_sphere(steps=n_total, **p), precision=1) for p in mine]
@@ -423,14 +429,16 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
     L = E.load()
     handles = [r.engine_handle() for r in runs]
     bytes_step = sum(int(L.xfd_stencil_bytes_per_step(ctypes_handle(h))) for h in handles)
-    bopts = {"autotune": tune}
+    bopts = {"autotune": tune} if tune else {"queue": args.batch_queue}
     if args.march_split_axes is not None:
         bopts["march_split_axes"] = args.march_split_axes
     batch = E.Batch(handles, bopts)
     batch.run(warm)
     batch.sync()
-    tuning = batch.tuning()
+    tuning = batch.tuning_shapes()
     depth = batch.get_option("march_ichunk")
+    rows = batch.get_option("tile_rows")
+    form = batch.get_option("queue")
     launches = batch.launches_per_step()
     stream = torch.cuda.ExternalStream(batch.stream(), device=local)
 
@@ -516,14 +524,20 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
                        "cpml": 8, "precision": "fp32",
                        "l2": f"inputs larger than L2 (fields {12 * all_cells * 4 / 1e9:.1f} GB)",
                        "parallelism": f"scenes round-robin over {world} GPU(s)",
-                       "sweep": "batched split H and E sweeps marching along x, TMA-staged "
-                                "planes, one launch per form over every scene's tiles",
-                       "tile_depth": depth, "autotune_ms_per_step": tuning,
+                       "sweep": ("batched split H and E sweeps marching along x, TMA-staged "
+                                 "planes; " + ("one persistent launch per step over a device "
+                                               "work queue of every scene's tiles, face and "
+                                               "TFSF blocks" if form else
+                                               "one launch per phase and form over every "
+                                               "scene's tiles")),
+                       "queue_form": form, "tile_rows": rows, "tile_depth": depth,
+                       "autotune_queue_rows_depth_ms_per_step": tuning,
                        "host_setup_s": setup_s},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
-                         "kernel": "the batch step's sweep launches (k_march_h_tma_batch + "
-                                   "k_march_e_tma_batch over all scenes)",
+                         "kernel": ("k_batch_queue (the whole batch step)" if form
+                                    else "the batch step's launches (k_march_h_tma_batch + "
+                                         "k_march_e_tma_batch over all scenes, faces, TFSF)"),
                          "note": "achieved = algorithmic stencil bytes per batch step "
                                  f"({bytes_step} B summed over this rank's scenes) / batch step "
                                  "time by CUDA events on the batch stream"},
@@ -736,6 +750,10 @@ def main():
     ap.add_argument("--march-split-axes", type=int, default=None,
                     help="1: CPML tiles in x-only, y-only, z-only and several-axis lists "
                          "(default), 0: one list")
+    ap.add_argument("--batch-queue", type=int, default=-1,
+                    help="--workload batched: -1 the autotuner picks the form, tile rows "
+                         "and depth during warm-up (default); 1 one persistent work-queue "
+                         "launch per step, 0 a launch per phase and sweep form (depth 16)")
     args = ap.parse_args()
     global KIND
     KIND = args.workload

@@ -493,8 +493,11 @@ xfd_status xfd_adjoint_run(xfd_engine* e, const xfd_adjoint_desc* d, double* val
  * many independent simulations of uneven grid sizes -- design variants,
  * incidence angles -- advanced together on one GPU.  Each is an engine set
  * up as usual (xfd_create, classes, curl factors, CPML, TFSF, fields); the
- * batch advances them with every phase of a time step one kernel launch over
- * all their tiles (a tile work list per sweep form), captured as CUDA graphs.
+ * batch advances them with a time step of all of them one launch of a
+ * persistent kernel over a device work queue (every tile, lattice-face block
+ * and TFSF block of the step, with bounded per-engine dependency waits; the
+ * option "queue" = 0 gives a launch per phase and sweep form instead),
+ * captured as CUDA graphs.
  * Per engine the arithmetic and order are those of xfd_run with the default
  * sweep.  Engines with ADE media, lumped sources, movies or an NF2FF surface
  * are rejected (XFD_ERR_UNSUPPORTED); all engines share one device and one
@@ -515,16 +518,28 @@ xfd_status xfd_batch_run(xfd_batch* b, int64_t n_steps);
 xfd_status xfd_batch_sync(xfd_batch* b);
 
 /* Options: "graph" (0/1, default 1), "graph_chunk" (steps per graph, default
- * 32), "march_ichunk" (x planes per CTA, the tile depth, default 16) and
- * "autotune" (K > 0: the next xfd_batch_run of at least 4 (1 + K) steps times
- * K steps of each candidate tile depth 8, 16, 32, 64 inside the run and keeps
- * the fastest; tiling does not change the results). */
+ * 32), "march_ichunk" (x planes per CTA, the tile depth, default 16),
+ * "queue" (0/1, default 1: the persistent work-queue launch), "tile_rows"
+ * (rows per tile, 8 or 16; 16 needs the queue form), "queue_wait_cycles"
+ * (cycles a queue item waits for the items it depends on before the batch
+ * reports XFD_ERR_TIMEOUT; 0: the stage-wait default, about 2 s),
+ * "queue_stall_test" (1: one item waits for a count that is never reached,
+ * to test that timeout) and "autotune" (K > 0: the next xfd_batch_run of at
+ * least 12 (1 + K) steps times K steps of each of 12 candidates inside the
+ * run and keeps the fastest, setting "queue", "tile_rows" and "march_ichunk"
+ * -- the queue form at tile rows 8 and 16 and the launch per phase at 8, each
+ * at tile depths 8, 16, 32, 64; neither form nor tiling changes the
+ * results). */
 xfd_status xfd_batch_set_option(xfd_batch* b, const char* name, int64_t value);
 xfd_status xfd_batch_get_option(const xfd_batch* b, const char* name, int64_t* value);
 
 /* The last autotuning: candidate tile depths and their ms per batch step. */
 xfd_status xfd_batch_tuning(const xfd_batch* b, int32_t* depth, double* ms_per_step,
                             int32_t capacity, int32_t* count);
+/* The same with each candidate's form (1: queue) and tile rows. */
+xfd_status xfd_batch_tuning_shapes(const xfd_batch* b, int32_t* queue, int32_t* rows,
+                                   int32_t* depth, double* ms_per_step, int32_t capacity,
+                                   int32_t* count);
 
 int32_t xfd_batch_size(const xfd_batch* b);
 /* Kernel launches per batch step (after the first xfd_batch_run). */

@@ -1,8 +1,9 @@
 """Batched simulations (xfd_batch_*): several independent scenes of uneven
 sizes advanced together must give, per scene, the fields of the same scene run
-alone through xfd_run -- bit for bit at the same tile depth, since every node
-goes through the same CTA body with the same tiling -- and the alone run
-matches the oracle (FP64 relative L2 <= 1e-12).  Random incidence angles
+alone through xfd_run -- bit for bit, in the persistent work-queue form (8-
+and 16-row tiles) and the launch-per-phase form, since every node goes through
+the same arithmetic in the same order -- and the alone run matches the oracle
+(FP64 relative L2 <= 1e-12).  Random incidence angles
 (theta, phi, psi) exercise the TFSF projection on every face."""
 import numpy as np
 import pytest
@@ -40,22 +41,32 @@ def _alone(scenes, precision, opts=None):
     return got
 
 
+# (queue, tile rows): the persistent work-queue launch with 8- and 16-row
+# tiles, and the launch per phase and form
+FORMS = [(1, 8), (1, 16), (0, 8)]
+
+
 @pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
 @pytest.mark.parametrize("depth", [4, 16])
-def test_batch_equals_alone_runs(precision, depth):
+@pytest.mark.parametrize("queue,rows", FORMS, ids=["queue8", "queue16", "launches"])
+def test_batch_equals_alone_runs(precision, depth, queue, rows):
     steps = 70
     scenes = _scenes(steps)
     # the marching sweep alone (small lattices default to the split sweep)
     want = _alone(scenes, precision, {"march_ichunk": depth, "kernel": 4})
     runs = [SceneRun(sc, precision=precision) for sc in scenes]
-    b = Batch([r.engine_handle() for r in runs], {"march_ichunk": depth, "graph_chunk": 16})
+    b = Batch([r.engine_handle() for r in runs],
+              {"queue": queue, "tile_rows": rows, "march_ichunk": depth, "graph_chunk": 16})
     assert b.size() == len(scenes)
     b.run(33)  # two graph chunks and one single step
     b.run(steps - 33)
     b.sync()
-    # per phase <= 6 tile lists (box forms, CPML tiles by slab axis) + faces
-    # + 2 TFSF groups, and the step counters
-    assert b.launches_per_step() <= 19
+    if queue:
+        assert b.launches_per_step() == 1
+    else:
+        # per phase <= 6 tile lists (box forms, CPML tiles by slab axis) +
+        # faces + 2 TFSF groups, and the step counters
+        assert b.launches_per_step() <= 19
     for r, w in zip(runs, want):
         r.finish()
         for c, (g, ww) in enumerate(zip(r.fields(), w)):
@@ -91,12 +102,16 @@ def test_batch_autotune_keeps_results(precision):
     want = _alone(scenes, precision)
     runs = [SceneRun(sc, precision=precision) for sc in scenes]
     b = Batch([r.engine_handle() for r in runs], {"autotune": 3})
-    b.run(steps)  # 4 x (1 + 3) tuning steps inside
+    b.run(steps)  # 12 x (1 + 3) tuning steps inside
     b.sync()
-    tune = b.tuning()
-    assert [d for d, _ in tune] == [8, 16, 32, 64]
-    assert all(ms > 0 for _, ms in tune)
-    assert b.get_option("march_ichunk") == min(tune, key=lambda t: t[1])[0]
+    tune = b.tuning_shapes()
+    assert [t[:3] for t in tune] == ([(1, r, d) for r in (8, 16) for d in (8, 16, 32, 64)] +
+                                     [(0, 8, d) for d in (8, 16, 32, 64)])
+    assert all(t[3] > 0 for t in tune)
+    best = min(tune, key=lambda t: t[3])
+    assert (b.get_option("queue"), b.get_option("tile_rows"),
+            b.get_option("march_ichunk")) == best[:3]
+    assert [d for d, _ in b.tuning()] == [t[2] for t in tune]
     assert b.get_option("autotune") == 0
     tol = 1e-12 if precision == 0 else 1e-6
     for r, w in zip(runs, want):
@@ -128,6 +143,11 @@ def test_batch_rejects_unbatched_features_and_mixed_precision():
         b.run(11)
     with pytest.raises(EngineError, match="unknown option"):
         b.set_option("tile", 3)
+    with pytest.raises(EngineError, match="tile_rows"):
+        b.set_option("tile_rows", 12)
+    b.set_option("queue", 0)
+    with pytest.raises(EngineError, match="UNSUPPORTED"):
+        b.set_option("tile_rows", 16)
     b.close()
     for x in (a, c, d, m):
         x.close()

@@ -7,6 +7,10 @@
   xfd_sync (and xfd_batch_sync for batched engines) then reports
   XFD_ERR_TIMEOUT, and a new engine on the same CUDA context runs clean and
   matches the oracle.
+* Bounded queue waits of the persistent batched kernel: with the test hook
+  "queue_stall_test" one work item waits for a count that nothing reaches; after
+  "queue_wait_cycles" it gives up, xfd_batch_sync reports XFD_ERR_TIMEOUT, and
+  a new batch on the same context is bit-equal to the scenes run alone.
 * The NaN / Inf watchdog ("watchdog_interval"): a field value set to NaN is
   reported by the next sync as XFD_ERR_NUMERIC; on clean fields the watchdog
   changes nothing (bit-equal fields) and the sync succeeds.
@@ -58,6 +62,42 @@ def test_batch_sync_reports_stage_timeout():
     b.run(4)
     with pytest.raises(EngineError, match="TIMEOUT"):
         b.sync()
+    b.close()
+    for r in runs:
+        r.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_batch_queue_wait_reports_timeout_then_clean_batch_runs(precision):
+    from xfdtd_core_b200 import scene as S
+    scenes = [S.batched_sphere(n=n, radius_cells=0.2 * n, eps_r=4.0, theta=0.3, phi=0.5,
+                               psi=0.1, pml=6, tfsf_start=9, steps=20) for n in (40, 33)]
+    runs = [SceneRun(sc, precision=precision) for sc in scenes]
+    b = Batch([r.engine_handle() for r in runs],
+              {"queue": 1, "queue_stall_test": 1, "queue_wait_cycles": 2_000_000,
+               "graph": 0})
+    assert b.get_option("queue_wait_cycles") == 2_000_000
+    b.run(2)
+    with pytest.raises(EngineError, match="TIMEOUT"):
+        b.sync()
+    b.close()
+    for r in runs:
+        r.close()
+    # the context is intact: a clean batch equals the scenes run alone
+    want = []
+    for sc in scenes:
+        r = SceneRun(sc, precision=precision, options={"kernel": 4})
+        r.run()
+        want.append(r.fields())
+        r.close()
+    runs = [SceneRun(sc, precision=precision) for sc in scenes]
+    b = Batch([r.engine_handle() for r in runs], {"queue": 1, "graph_chunk": 8})
+    b.run(20)
+    b.sync()
+    for r, w in zip(runs, want):
+        r.finish()
+        for g, x in zip(r.fields(), w):
+            assert np.array_equal(g, x)
     b.close()
     for r in runs:
         r.close()

@@ -24,13 +24,24 @@
 // lumped sources, movies, an NF2FF surface or coefficient overrides are not
 // batched (their per-step extras stay with xfd_run).
 //
-// The x chunk length (planes per CTA) is the tile depth the autotuner
-// chooses: with the `autotune` option set to K, the next xfd_batch_run
-// spends 1 + K of its steps on each candidate depth 8, 16, 32, 64 (a warm-up
-// step, then K steps in one graph timed by CUDA events) and keeps the
-// fastest.  Tiling
-// does not change any node's arithmetic, so the tuned run advances the same
-// simulation.
+// By default (option `queue` = 1) the whole step is instead ONE launch of
+// the persistent kernel k_batch_queue (batch_queue.cuh): the same CTA bodies
+// over one device work queue that holds every tile, face block and TFSF
+// block of the step of every lattice, with bounded per-lattice dependency
+// waits in place of the launch boundaries; `queue` = 0 keeps the launch per
+// phase and form described above.
+//
+// The form (`queue`), the tile shape (rows per tile, `tile_rows`: 8 or 16,
+// the queue form only) and the x chunk length (planes per CTA,
+// `march_ichunk`) are what the autotuner chooses: with the `autotune` option
+// set to K, the next xfd_batch_run spends 1 + K of its steps on each of 12
+// candidates (the queue form at rows 8 and 16, the launch per phase at rows
+// 8, each at depths 8, 16, 32, 64; a warm-up step, then K steps in one graph
+// timed by CUDA events) and keeps the fastest.  Tiling does not change any node's arithmetic, so the
+// tuned run advances the same simulation.  Temporal blocking is not
+// implemented: every launch advances one time step.
+
+#include "batch_queue.cuh"
 
 struct xfd_batch {
   int device = 0;
@@ -64,7 +75,21 @@ struct xfd_batch {
   long long tfsf_off[5] = {0, 0, 0, 0, 0};  // pass groups H1, H2, E1, E2
   cudaGraphExec_t graph_exec = nullptr;
   long long graph_len = 0;
-  std::vector<std::pair<int, double>> tune_ms;  // (depth, ms per step) of the last tuning
+  struct Tune {
+    int queue, rows, depth;
+    double ms;
+  };
+  std::vector<Tune> tune_ms;  // candidates of the last tuning, ms per step
+  // Persistent queue form (batch_queue.cuh).
+  bool queue = true;
+  int tile_rows = 8;             // rows per tile: kMTJ or kWideTJ
+  long long queue_wait = 0;      // cycles per dependency wait (0: the stage-wait default)
+  bool queue_stall_test = false; // test hook: one item waits for a count never reached
+  int4* d_items = nullptr;
+  int* d_need = nullptr;
+  int* d_qcnt = nullptr;  // head, exits, done[n]
+  int n_items = 0;
+  int queue_grid = 0;
 };
 
 namespace {
@@ -101,6 +126,10 @@ void batch_free_tables(xfd_batch* b) {
   b->d_tiles = nullptr;
   b->d_edge = nullptr;
   b->d_tfb = nullptr;
+  b->d_items = nullptr;
+  b->d_need = nullptr;
+  b->d_qcnt = nullptr;
+  b->n_items = 0;
   b->ready = false;
 }
 
@@ -141,6 +170,8 @@ xfd_status batch_set_smem() {
   set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 1>, msm_free);
   set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 2>, msm_free);
   set((const void*)k_march_e_tma_batch<T, kMTJ, 32, MF, true, false, 4>, msm_free);
+  set((const void*)k_batch_queue<T, kMTJ>, MarchGeom<T, kMTJ, 32>::smem(MS));
+  set((const void*)k_batch_queue<T, kWideTJ>, MarchGeom<T, kWideTJ, 32>::smem(MS));
   if (c != cudaSuccess) {
     g_create_error = cudaGetErrorString(c);
     return XFD_ERR_CUDA;
@@ -165,6 +196,11 @@ xfd_status batch_prepare(xfd_batch* b) {
   std::vector<int4> tiles[6];
   std::vector<int2> edge;
   std::vector<int2> tfb[4];
+  // The queue form sweeps tiles of tile_rows rows; its face and TFSF items
+  // are blocks of one CTA's threads.
+  const int tj = b->queue ? b->tile_rows : kMTJ;
+  const int qnt = 32 * tj;
+  std::vector<std::array<int, 8>> qcount((size_t)n);  // items per lattice and level
   for (int s = 0; s < n; ++s) {
     xfd_engine* e = b->eng[(size_t)s];
     e->march_ichunk = b->march_ichunk;
@@ -175,11 +211,11 @@ xfd_status batch_prepare(xfd_batch* b) {
     BATCH_TRY(b, cudaStreamSynchronize(e->stream));
     MarchTmaP<T> q{};
     q.p = march_params<T>(e);
-    q.m = e->mtma[e->cur];
+    q.m = tj == kMTJ ? e->mtma[e->cur] : e->mtma_w[e->cur];
     q.err = e->d_err;
     q.wait_budget = e->stage_wait;
     int lo[3], hi[3];
-    march_split(e, lo, hi);
+    march_split(e, lo, hi, tj);
     const bool box = hi[0] > lo[0] && hi[1] > lo[1] && hi[2] > lo[2];
     for (int a = 0; a < 3; ++a) {
       q.box_lo[a] = box ? lo[a] : 0;
@@ -187,9 +223,11 @@ xfd_status batch_prepare(xfd_batch* b) {
     }
     const Lat& L = e->L;
     const bool in = box && lo[0] >= 1 && 32 * hi[0] <= L.nz && lo[1] >= 1 &&
-                    kMTJ * hi[1] <= L.ny && lo[2] >= 1 && hi[2] * e->march_ichunk <= L.nx;
-    const int nt[3] = {(L.nz + 31) / 32, (L.ny + kMTJ - 1) / kMTJ,
+                    tj * hi[1] <= L.ny && lo[2] >= 1 && hi[2] * e->march_ichunk <= L.nx;
+    const int nt[3] = {(L.nz + 31) / 32, (L.ny + tj - 1) / tj,
                        (L.nx + 1 + e->march_ichunk - 1) / e->march_ichunk};
+    std::array<int, 8>& qc = qcount[(size_t)s];
+    qc.fill(0);
     for (int z = 0; z < nt[2]; ++z)
       for (int y = 0; y < nt[1]; ++y)
         for (int x = 0; x < nt[0]; ++x) {
@@ -198,23 +236,29 @@ xfd_status batch_prepare(xfd_batch* b) {
           int f = inbox ? (in ? 0 : 1) : 5;
           if (!inbox && b->split_axes) {
             const int ich = e->march_ichunk;
-            f = 2 + cpml_tile_list(e, 32 * x, std::min(32 * x + 32, L.nz), kMTJ * y,
-                                   std::min(kMTJ * y + kMTJ, L.ny), ich * z,
+            f = 2 + cpml_tile_list(e, 32 * x, std::min(32 * x + 32, L.nz), tj * y,
+                                   std::min(tj * y + tj, L.ny), ich * z,
                                    std::min(ich * z + ich, L.nx + 1));
           }
           tiles[f].push_back(make_int4(s, x, y, z));
+          qc[0] += 1;
+          qc[4] += 1;
         }
     mp[(size_t)s] = q;
     yp[(size_t)s] = yee_params<T>(e);
-    const long long nb = (edge_nodes(L) + 255) / 256;
+    const int bn = b->queue ? qnt * kQueueNodeIters : 256;  // nodes per face / TFSF block
+    const long long nb = (edge_nodes(L) + bn - 1) / bn;
     for (long long k = 0; k < nb; ++k) edge.push_back(make_int2(s, (int)k));
+    qc[1] = qc[5] = (int)nb;
     TfsfSceneD<T> t{};
     if (e->have_tfsf) {
       t.tf = e->tfsf;
+      static const int level_of_group[4] = {2, 3, 6, 7};
       for (int g = 0; g < 4; ++g) {
         t.g[g] = e->tfsf_groups[g];
-        const long long gb = (t.g[g].total + 255) / 256;
+        const long long gb = (t.g[g].total + bn - 1) / bn;
         for (long long k = 0; k < gb; ++k) tfb[g].push_back(make_int2(s, (int)k));
+        qc[level_of_group[g]] = (int)gb;
       }
     }
     t.L = L;
@@ -248,6 +292,70 @@ xfd_status batch_prepare(xfd_batch* b) {
   }
   b->tfsf_off[4] = (long long)tall.size();
   if ((st = batch_upload(b, &b->d_tfb, tall.data(), tall.size())) != XFD_OK) return st;
+  if (b->queue) {
+    int per_sm = 0, sms = 0;
+    const void* kq = tj == kMTJ ? (const void*)k_batch_queue<T, kMTJ>
+                                : (const void*)k_batch_queue<T, kWideTJ>;
+    const size_t qsm = tj == kMTJ ? MarchGeom<T, kMTJ, 32>::smem(march_stages<T>())
+                                  : MarchGeom<T, kWideTJ, 32>::smem(march_stages<T>());
+    BATCH_TRY(b, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kq, qnt, qsm));
+    BATCH_TRY(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    if (per_sm < 1) return bfail(b, XFD_ERR_CUDA, "queue kernel does not fit on an SM");
+    const int resident = per_sm * sms;
+    // Items level by level (H tiles, H faces, TFSF H 1, 2, E tiles, E faces,
+    // TFSF E 1, 2); tiles of a level by form, costliest first (CPML tiles
+    // meeting several axes, single-axis CPML tiles, CPML-free, the interior),
+    // lattices largest first within a form.  (Pipelining the queue over
+    // groups of lattices, the H levels of one group between the H and E
+    // levels of the one before, measured slower: 8.2 against 7.6 ms per step
+    // on 96 lattices of 64^3-224^3.)
+    std::vector<int4> items;
+    std::vector<int> need;
+    auto need_of = [&](int s, int level) {
+      int c = 0;
+      for (int l = 0; l < level; ++l) c += qcount[(size_t)s][(size_t)l];
+      return c;
+    };
+    static const int form_order[6] = {5, 2, 3, 4, 1, 0};
+    auto push_tiles = [&](int level, int kind0) {
+      for (int f : form_order)
+        for (const int4& w : tiles[f]) {
+          items.push_back(make_int4(((kind0 + f) << 16) | w.x, w.y, w.z, w.w));
+          need.push_back(need_of(w.x, level));
+        }
+    };
+    auto push_blocks = [&](int level, int kind, const std::vector<int2>& blocks) {
+      for (const int2& v : blocks) {
+        items.push_back(make_int4((kind << 16) | v.x, v.y, 0, 0));
+        need.push_back(need_of(v.x, level));
+      }
+    };
+    push_tiles(0, kQ_H_IN);
+    push_blocks(1, kQ_EDGE_H, edge);
+    push_blocks(2, kQ_TFSF_H1, tfb[0]);
+    push_blocks(3, kQ_TFSF_H2, tfb[1]);
+    push_tiles(4, kQ_E_IN);
+    push_blocks(5, kQ_EDGE_E, edge);
+    push_blocks(6, kQ_TFSF_E1, tfb[2]);
+    push_blocks(7, kQ_TFSF_E2, tfb[3]);
+    if (b->queue_stall_test) {
+      // The first item of lattice 0 that waits at all waits for more items
+      // than the lattice has: a count nothing reaches, so the wait runs out.
+      int total = 0;
+      for (int l = 0; l < 8; ++l) total += qcount[0][(size_t)l];
+      for (size_t t = 0; t < items.size(); ++t)
+        if ((items[t].x & 0xffff) == 0 && need[t] > 0) {
+          need[t] = total + 1;
+          break;
+        }
+    }
+    if ((st = batch_upload(b, &b->d_items, items.data(), items.size())) != XFD_OK) return st;
+    if ((st = batch_upload(b, &b->d_need, need.data(), need.size())) != XFD_OK) return st;
+    std::vector<int> zero((size_t)n + 2, 0);
+    if ((st = batch_upload(b, &b->d_qcnt, zero.data(), zero.size())) != XFD_OK) return st;
+    b->n_items = (int)items.size();
+    b->queue_grid = std::max(1, std::min(b->n_items, resident));
+  }
   BATCH_TRY(b, cudaStreamSynchronize(b->stream));
   b->d_march = dm;
   b->d_yee = dy;
@@ -259,7 +367,33 @@ xfd_status batch_prepare(xfd_batch* b) {
 }
 
 template <typename T>
+cudaError_t batch_enqueue_queue(xfd_batch* b) {
+  BatchQueueD<T> q{};
+  q.march = static_cast<const MarchTmaP<T>*>(b->d_march);
+  q.yee = static_cast<const YeeP<T>*>(b->d_yee);
+  q.tfsf = static_cast<const TfsfSceneD<T>*>(b->d_tfsf);
+  q.items = b->d_items;
+  q.need = b->d_need;
+  q.n_items = b->n_items;
+  q.n_lattices = (int)b->eng.size();
+  q.head = b->d_qcnt;
+  q.exits = b->d_qcnt + 1;
+  q.done = b->d_qcnt + 2;
+  q.steps = b->d_steps;
+  q.wait_budget = b->queue_wait > 0 ? b->queue_wait : kStageWaitDefault;
+  constexpr int MS = march_stages<T>();
+  if (b->tile_rows == kWideTJ)
+    k_batch_queue<T, kWideTJ><<<b->queue_grid, dim3(32, kWideTJ, 1),
+                                MarchGeom<T, kWideTJ, 32>::smem(MS), b->stream>>>(q);
+  else
+    k_batch_queue<T, kMTJ><<<b->queue_grid, dim3(32, kMTJ, 1), MarchGeom<T, kMTJ, 32>::smem(MS),
+                             b->stream>>>(q);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t batch_enqueue_t(xfd_batch* b) {
+  if (b->queue) return batch_enqueue_queue<T>(b);
   cudaStream_t s = b->stream;
   constexpr int MS = march_stages<T>();
   constexpr int MF = march_free_stages<T>();
@@ -357,19 +491,32 @@ xfd_status batch_steps(xfd_batch* b, long long n) {
   return XFD_OK;
 }
 
-// Depths tried by the autotuner.
+// Candidates of the autotuner: the queue form with tile rows 8 and 16, then
+// the launch per phase and form (8 rows), each at the depths below.
 constexpr int kTuneDepths[] = {8, 16, 32, 64};
+constexpr int kTuneCandidates = 12;
 
-// Times each candidate x chunk length on 1 + K steps of the run (K in one
-// graph, by CUDA events) and keeps the fastest.  Returns the steps consumed.
+void tune_candidate(int c, int* queue, int* rows, int* depth) {
+  *queue = c < 8 ? 1 : 0;
+  *rows = c < 4 ? kMTJ : c < 8 ? kWideTJ : kMTJ;
+  *depth = kTuneDepths[c % 4];
+}
+
+// Times each candidate (form, tile rows, x chunk length) on 1 + K steps of
+// the run (K in one graph, by CUDA events) and keeps the fastest.  Returns
+// the steps consumed.
 xfd_status batch_autotune(xfd_batch* b, long long* used) {
   *used = 0;
   const int K = b->autotune;
   b->tune_ms.clear();
-  int best = b->march_ichunk;
+  int best = b->march_ichunk, best_rows = b->tile_rows, best_queue = b->queue ? 1 : 0;
   double best_ms = 0;
-  for (int d : kTuneDepths) {
+  for (int c_i = 0; c_i < kTuneCandidates; ++c_i) {
+    int queue, rows, d;
+    tune_candidate(c_i, &queue, &rows, &d);
+    b->queue = queue != 0;
     b->march_ichunk = d;
+    b->tile_rows = rows;
     xfd_status s = batch_prepare_any(b);
     if (s != XFD_OK) return s;
     cudaError_t c = batch_enqueue(b);  // warm-up step
@@ -382,16 +529,20 @@ xfd_status batch_autotune(xfd_batch* b, long long* used) {
     float ms = 0;
     BATCH_TRY(b, cudaEventElapsedTime(&ms, b->t0, b->t1));
     const double per = (double)ms / K;
-    b->tune_ms.emplace_back(d, per);
+    b->tune_ms.push_back({queue, rows, d, per});
     if (b->tune_ms.size() == 1 || per < best_ms) {
       best = d;
+      best_rows = rows;
+      best_queue = queue;
       best_ms = per;
     }
     *used += 1 + K;
   }
   b->autotune = 0;
-  if (best != b->march_ichunk) {
+  if (best != b->march_ichunk || best_rows != b->tile_rows || (best_queue != 0) != b->queue) {
     b->march_ichunk = best;
+    b->tile_rows = best_rows;
+    b->queue = best_queue != 0;
     xfd_status s = batch_prepare_any(b);
     if (s != XFD_OK) return s;
   }
@@ -405,6 +556,8 @@ extern "C" {
 
 xfd_status xfd_batch_create(xfd_engine* const* engines, int32_t n, xfd_batch** out) {
   if (!engines || !out || n < 1) return bfail(nullptr, XFD_ERR_INVALID_ARGUMENT, "bad batch");
+  if (n > 0xffff)  // queue items carry the lattice in 16 bits
+    return bfail(nullptr, XFD_ERR_INVALID_ARGUMENT, "more than 65535 engines in one batch");
   *out = nullptr;
   for (int32_t s = 0; s < n; ++s) {
     const xfd_engine* e = engines[s];
@@ -489,8 +642,7 @@ xfd_status xfd_batch_run(xfd_batch* b, int64_t n) {
   xfd_status st;
   if (!b->ready && (st = batch_prepare_any(b)) != XFD_OK) return st;
   long long left = n;
-  const long long tune_steps = (long long)(sizeof kTuneDepths / sizeof kTuneDepths[0]) *
-                               (1 + (long long)b->autotune);
+  const long long tune_steps = (long long)kTuneCandidates * (1 + (long long)b->autotune);
   if (b->autotune > 0 && left >= tune_steps) {
     long long used = 0;
     if ((st = batch_autotune(b, &used)) != XFD_OK) return st;
@@ -514,7 +666,8 @@ xfd_status xfd_batch_sync(xfd_batch* b) {
     int err = 0;
     BATCH_TRY(b, cudaMemcpy(&err, b->eng[s]->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err & 2)
-      return bfail(b, XFD_ERR_TIMEOUT, "lattice %zu: a sweep stage wait ran out of time", s);
+      return bfail(b, XFD_ERR_TIMEOUT, "lattice %zu: a sweep stage or queue wait ran out of time",
+                   s);
     if (err)
       return bfail(b, XFD_ERR_NUMERIC, "lattice %zu: TFSF projection left the incident grid", s);
   }
@@ -529,6 +682,10 @@ xfd_status xfd_batch_get_option(const xfd_batch* b, const char* name, int64_t* v
   else if (!strcmp(name, "march_ichunk")) *value = b->march_ichunk;
   else if (!strcmp(name, "autotune")) *value = b->autotune;
   else if (!strcmp(name, "march_split_axes")) *value = b->split_axes ? 1 : 0;
+  else if (!strcmp(name, "queue")) *value = b->queue ? 1 : 0;
+  else if (!strcmp(name, "tile_rows")) *value = b->tile_rows;
+  else if (!strcmp(name, "queue_wait_cycles")) *value = b->queue_wait;
+  else if (!strcmp(name, "queue_stall_test")) *value = b->queue_stall_test ? 1 : 0;
   else return bfail(m, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   return XFD_OK;
 }
@@ -553,6 +710,26 @@ xfd_status xfd_batch_set_option(xfd_batch* b, const char* name, int64_t value) {
     b->split_axes = value != 0;
     b->ready = false;
     batch_drop_graph(b);
+  } else if (!strcmp(name, "queue")) {
+    b->queue = value != 0;
+    b->ready = false;
+    batch_drop_graph(b);
+  } else if (!strcmp(name, "tile_rows")) {
+    if (value != kMTJ && value != kWideTJ)
+      return bfail(b, XFD_ERR_INVALID_ARGUMENT, "tile_rows must be %d or %d", kMTJ, kWideTJ);
+    if (value != kMTJ && !b->queue)
+      return bfail(b, XFD_ERR_UNSUPPORTED, "tile_rows %d needs the queue form", (int)value);
+    b->tile_rows = (int)value;
+    b->ready = false;
+    batch_drop_graph(b);
+  } else if (!strcmp(name, "queue_wait_cycles")) {
+    if (value < 0) return bfail(b, XFD_ERR_INVALID_ARGUMENT, "queue_wait_cycles < 0");
+    b->queue_wait = value;
+    batch_drop_graph(b);
+  } else if (!strcmp(name, "queue_stall_test")) {
+    b->queue_stall_test = value != 0;
+    b->ready = false;
+    batch_drop_graph(b);
   } else {
     return bfail(b, XFD_ERR_INVALID_ARGUMENT, "unknown option '%s'", name);
   }
@@ -561,17 +738,26 @@ xfd_status xfd_batch_set_option(xfd_batch* b, const char* name, int64_t value) {
 
 xfd_status xfd_batch_tuning(const xfd_batch* b, int32_t* depth, double* ms_per_step,
                             int32_t capacity, int32_t* count) {
+  return xfd_batch_tuning_shapes(b, nullptr, nullptr, depth, ms_per_step, capacity, count);
+}
+
+xfd_status xfd_batch_tuning_shapes(const xfd_batch* b, int32_t* queue, int32_t* rows,
+                                   int32_t* depth, double* ms_per_step, int32_t capacity,
+                                   int32_t* count) {
   if (!b || !count) return bfail(const_cast<xfd_batch*>(b), XFD_ERR_INVALID_ARGUMENT, "null");
   *count = (int32_t)b->tune_ms.size();
   for (int32_t q = 0; q < *count && q < capacity; ++q) {
-    if (depth) depth[q] = b->tune_ms[(size_t)q].first;
-    if (ms_per_step) ms_per_step[q] = b->tune_ms[(size_t)q].second;
+    if (queue) queue[q] = b->tune_ms[(size_t)q].queue;
+    if (rows) rows[q] = b->tune_ms[(size_t)q].rows;
+    if (depth) depth[q] = b->tune_ms[(size_t)q].depth;
+    if (ms_per_step) ms_per_step[q] = b->tune_ms[(size_t)q].ms;
   }
   return XFD_OK;
 }
 
 int32_t xfd_batch_launches_per_step(const xfd_batch* b) {
   if (!b || !b->ready) return 0;
+  if (b->queue) return 1;
   int n = 1;  // step counters
   for (int f = 0; f < 6; ++f) n += b->tile_off[f + 1] > b->tile_off[f] ? 2 : 0;
   if (b->n_edge) n += 2;

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -371,11 +372,13 @@ constexpr int kStagesF32 = 4, kStagesF64 = 3;
 constexpr int kMarchStagesF32 = 6, kMarchStagesF64 = 4;
 constexpr int kMTJ = 8;  // rows (warps) per CTA of the TMA marching sweeps
 template <typename T>
-constexpr int march_stages() { return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32; }
+__host__ __device__ constexpr int march_stages() {
+  return sizeof(T) == 8 ? kMarchStagesF64 : kMarchStagesF32;
+}
 // The CPML-free forms need fewer registers, so they run more CTAs per SM;
 // fewer stages keep their shared memory from capping that.
 template <typename T>
-constexpr int march_free_stages() { return sizeof(T) == 8 ? 3 : 4; }
+__host__ __device__ constexpr int march_free_stages() { return sizeof(T) == 8 ? 3 : 4; }
 // Stages of the two-rows-per-thread interior form (3 CTAs per SM in FP32,
 // 2 in FP64).
 template <typename T>
@@ -686,14 +689,14 @@ void fmarch_split(const xfd_engine* e, int nt[3], int lo[3], int hi[3]) {
 
 // The box of (k tile of 32, j tile of 8, chunk of march_ichunk planes) of
 // the split marching sweeps whose nodes lie in no CPML layer of either phase.
-// Along grid dimension g (0: k tiles of 32, 1: j tiles of kMTJ, 2: chunks of
+// Along grid dimension g (0: k tiles of 32, 1: j tiles of tj rows, 2: chunks of
 // march_ichunk x planes) with the grid shifted by sh nodes (-size < sh <= 0),
 // tile b covers nodes [sh + b size, sh + (b+1) size) within the lattice.  The
 // longest run [lo, hi) of tiles that meet no CPML layer of either phase;
 // returns the nodes it covers.
-int march_free_run(const xfd_engine* e, int g, int sh, int& lo, int& hi) {
+int march_free_run(const xfd_engine* e, int g, int sh, int& lo, int& hi, int tj = kMTJ) {
   const Lat& L = e->L;
-  const int size[3] = {32, kMTJ, e->march_ichunk};
+  const int size[3] = {32, tj, e->march_ichunk};
   const int n_nodes[3] = {L.nz, L.ny, L.nx + 1};
   const int axis_of[3] = {2, 1, 0};  // grid dimension -> lattice axis
   const int m = axis_of[g], z = size[g], n = n_nodes[g];
@@ -727,9 +730,10 @@ int march_free_run(const xfd_engine* e, int g, int sh, int& lo, int& hi) {
   return best;
 }
 
-// The CPML-free box of the unshifted tile grid (the batched sweeps' split).
-void march_split(const xfd_engine* e, int lo[3], int hi[3]) {
-  for (int g = 0; g < 3; ++g) march_free_run(e, g, 0, lo[g], hi[g]);
+// The CPML-free box of the unshifted tile grid of tj-row tiles (the batched
+// sweeps' split).
+void march_split(const xfd_engine* e, int lo[3], int hi[3], int tj = kMTJ) {
+  for (int g = 0; g < 3; ++g) march_free_run(e, g, 0, lo[g], hi[g], tj);
 }
 
 // Work split of the TMA marching sweeps for the current options: the

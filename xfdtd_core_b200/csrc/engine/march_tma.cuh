@@ -173,13 +173,24 @@ struct StageRing {
     for (int s = 0; s < S; ++s)
       if ((pending >> s) & 1u) wait(s);
   }
+  // For a CTA that sweeps another tile next (the persistent batched kernel):
+  // once no load is in flight (none is on the normal path, where every staged
+  // plane was waited for) and every thread is done with the stages,
+  // invalidate the barriers, so that their words can be initialised again or
+  // become stage memory.
+  __device__ void release(int S, int tid) {
+    drain(S);
+    __syncthreads();
+    if (tid == 0)
+      for (int s = 0; s < S; ++s) mbar_inval(&bars[s]);
+  }
 };
 
 // ---------------------------------------------------------------------------
 // H sweep.  Planes q = 0 .. n_planes of the chunk are staged (plane n_planes
 // is i_hi, E only, when i_hi <= nx); plane q lives in stage q % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7, bool REUSE = false>
 __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx, const int gy,
                                             const int gz) {
   using G = MarchGeom<T, TJ, TK>;
@@ -378,13 +389,14 @@ __device__ __forceinline__ void march_h_cta(const MarchTmaP<T>& P, const int gx,
     if (tid == 0) atomicOr(P.err, 2);
     ring.drain(S);
   }
+  if constexpr (REUSE) ring.release(S, tid);
 }
 
 // ---------------------------------------------------------------------------
 // E sweep.  Staged planes q = -1 .. n_planes-1 (plane -1 = i_lo-1, H only,
 // when i_lo >= 1); plane q lives in stage (q+1) % S.
 // ---------------------------------------------------------------------------
-template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7>
+template <typename T, int TJ, int TK, int S, bool CP, bool IN, int AX = 7, bool REUSE = false>
 __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx, const int gy,
                                             const int gz) {
   using G = MarchGeom<T, TJ, TK>;
@@ -588,6 +600,7 @@ __device__ __forceinline__ void march_e_cta(const MarchTmaP<T>& P, const int gx,
     if (tid == 0) atomicOr(P.err, 2);
     ring.drain(S);
   }
+  if constexpr (REUSE) ring.release(S, tid);
 }
 
 // One lattice: CTA (x, y, z) sweeps tile (x, y) and chunk z, offset by org.

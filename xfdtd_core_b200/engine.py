@@ -143,6 +143,9 @@ def load(build_if_missing: bool = True):
         "xfd_batch_get_option": ([vp, ctypes.c_char_p, ctypes.POINTER(_i64)], ctypes.c_int),
         "xfd_batch_tuning": ([vp, ctypes.POINTER(_i32), _dp, _i32, ctypes.POINTER(_i32)],
                              ctypes.c_int),
+        "xfd_batch_tuning_shapes": ([vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
+                                     ctypes.POINTER(_i32), _dp, _i32, ctypes.POINTER(_i32)],
+                                    ctypes.c_int),
         "xfd_batch_size": ([vp], _i32),
         "xfd_batch_launches_per_step": ([vp], _i32),
         "xfd_batch_stream": ([vp], vp),
@@ -172,6 +175,7 @@ def exported_symbols() -> List[str]:
             "xfd_batch_create",
             "xfd_batch_destroy", "xfd_batch_last_error", "xfd_batch_run", "xfd_batch_sync",
             "xfd_batch_set_option", "xfd_batch_get_option", "xfd_batch_tuning",
+            "xfd_batch_tuning_shapes",
             "xfd_batch_size", "xfd_batch_launches_per_step", "xfd_batch_stream"]
 
 
@@ -487,6 +491,19 @@ class Batch:
         self._check(self.L.xfd_batch_tuning(self.h, d, _p(ms), cnt.value, ctypes.byref(cnt)),
                     "batch_tuning")
         return [(int(d[q]), float(ms[q])) for q in range(cnt.value)]
+
+    def tuning_shapes(self) -> List[tuple]:
+        """(queue form, tile rows, tile depth, ms per batch step) of the last
+        autotuning."""
+        cnt = _i32()
+        self._check(self.L.xfd_batch_tuning_shapes(self.h, None, None, None, None, 0,
+                                                   ctypes.byref(cnt)), "batch_tuning_shapes")
+        n = max(cnt.value, 1)
+        qf, r, d = (_i32 * n)(), (_i32 * n)(), (_i32 * n)()
+        ms = np.zeros(n)
+        self._check(self.L.xfd_batch_tuning_shapes(self.h, qf, r, d, _p(ms), cnt.value,
+                                                   ctypes.byref(cnt)), "batch_tuning_shapes")
+        return [(int(qf[q]), int(r[q]), int(d[q]), float(ms[q])) for q in range(cnt.value)]
 
     def size(self) -> int:
         return int(self.L.xfd_batch_size(self.h))
