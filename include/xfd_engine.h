@@ -167,6 +167,15 @@ typedef struct {
   double te[3], th[3];
 } xfd_tfsf_desc;
 xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* tfsf);
+/* The same source on one x-slab of a lattice decomposed along x (the slab
+ * decomposition driven by xfdtd_core_b200/slab.py, one engine per slab with a
+ * ghost cell on each interior side): `tfsf` describes it on the global lattice
+ * (box x coordinates global, projections and incident grid unchanged), and
+ * plane 0 of this engine is global plane x_offset.  Every face pass is cut to
+ * the nodes of this engine's lattice that it corrects, ghost cells included.
+ * Replaces: the reference's cut of TFSF3D by the domain a process runs on
+ * (TFSF3D::generateCorrector, src/waveform_source/tfsf_3d.cpp:21-33). */
+xfd_status xfd_set_tfsf_slab(xfd_engine* e, const xfd_tfsf_desc* tfsf, int32_t x_offset);
 
 /* Lumped current source on a box of E_comp nodes [box_s, box_e): per step
  * E += coff[node] * waveform[t].  coff is box-shaped (k fastest); waveform has

@@ -115,7 +115,7 @@ class _Tfsf(ctypes.Structure):
                 ("ke", _i64), ("nt", _i64), ("aux", _i64), ("e_inc", _dp), ("h_inc", _dp),
                 ("p_int", _dp * 3), ("p_half", _dp * 3), ("ca", ctypes.c_double * 3),
                 ("cb", ctypes.c_double * 3), ("te", ctypes.c_double * 3),
-                ("th", ctypes.c_double * 3)]
+                ("th", ctypes.c_double * 3), ("xo", _i64), ("nxl", _i64)]
 
 
 class _Lumped(ctypes.Structure):
@@ -1352,6 +1352,9 @@ class RefSimulation:
             s.is_, s.js, s.ks = t["box_s"]
             s.ie, s.je, s.ke = t["box_e"]
             s.nt, s.aux = t["nt"], t["aux"]
+            # an x-slab of a decomposed lattice: box indices global, the slab
+            # from global plane x_offset (tfsf_3d.cpp:21-33 cuts by domain)
+            s.xo, s.nxl = int(t.get("x_offset", 0)), self.nx
             s.e_inc, s.h_inc = _ptr(t["e_inc"]), _ptr(t["h_inc"])
             for a in range(3):
                 s.p_int[a] = _ptr(t["p_int"][a])

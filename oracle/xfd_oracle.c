@@ -331,6 +331,12 @@ typedef struct {
   const double *p_int[3], *p_half[3];
   double ca[3], cb[3];            /* dt/(eps0 d), dt/(mu0 d) per axis */
   double te[3], th[3];            /* transform_e / transform_h */
+  /* The lattice this oracle runs is the x-slab of the global one whose plane
+   * 0 is global plane xo, nxl cells along x (xo = 0, nxl = nx: the whole
+   * lattice).  Passes correct only the nodes of the slab, as the reference
+   * cuts TFSF3D by the domain a process runs on (TFSF3D::generateCorrector,
+   * src/waveform_source/tfsf_3d.cpp:21-33). */
+  idx_t xo, nxl;
 } orc_tfsf;
 
 /* exInc..hzInc.  The axis whose index is shifted by +1 uses the half-cell
@@ -364,7 +370,9 @@ static double tfsf_inc(const orc_tfsf *t, int is_e, int comp, idx_t step, idx_t 
   return t->th[comp] * ((1 - w) * row[index] + w * row[index + 1]);
 }
 
-/* One correctTFSF<direction, attribute, field_xyz> pass, single domain. */
+/* One correctTFSF<direction, attribute, field_xyz> pass.  Indices are
+ * global; the node corrected is written at local x = global x - xo when the
+ * slab holds it (E_x, H_y, H_z: x < nxl; the others x <= nxl). */
 static void tfsf_pass(const orc_yee *y, const orc_tfsf *t, idx_t step, int dir_axis,
                       int negative, int is_e, int field) {
   const int m = dir_axis, A = tan_a(m), B = tan_b(m);
@@ -385,7 +393,12 @@ static void tfsf_pass(const orc_yee *y, const orc_tfsf *t, idx_t step, int dir_a
   const double flag = (double)(equation_flag * different_flag * direction_flag);
   const double coeff = (is_e ? t->ca[m] : t->cb[m]) * flag;
   orc_arr F = is_e ? y->e[field] : y->h[field];
+  const int on_cells = is_e ? field == 0 : field != 0;
+  const idx_t x_end = on_cells ? t->nxl : t->nxl + 1;  /* local x range [0, x_end) */
   for (idx_t i = s[0]; i < e[0]; ++i) {
+    /* x of the node this i corrects (a negative H face along x: one below) */
+    const idx_t xc = i - ((negative && !is_e && m == 0) ? 1 : 0) - t->xo;
+    if (xc < 0 || xc >= x_end) continue;
     for (idx_t j = s[1]; j < e[1]; ++j) {
       for (idx_t k = s[2]; k < e[2]; ++k) {
         idx_t x[3] = {i, j, k};
@@ -394,14 +407,14 @@ static void tfsf_pass(const orc_yee *y, const orc_tfsf *t, idx_t step, int dir_a
           q[m] -= 1;
           if (is_e) {
             const double v = tfsf_inc(t, 0, dual_field, step, q[0], q[1], q[2]);
-            AT(F, i, j, k) += v * coeff;
+            AT(F, i - t->xo, j, k) += v * coeff;
           } else {
             const double v = tfsf_inc(t, 1, dual_field, step, i, j, k);
-            AT(F, q[0], q[1], q[2]) += v * coeff;
+            AT(F, q[0] - t->xo, q[1], q[2]) += v * coeff;
           }
         } else {
           const double v = tfsf_inc(t, is_e ? 0 : 1, dual_field, step, x[0], x[1], x[2]);
-          AT(F, i, j, k) += v * coeff;
+          AT(F, i - t->xo, j, k) += v * coeff;
         }
       }
     }

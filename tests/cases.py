@@ -61,7 +61,9 @@ class KernelCase:
         self.fields = [np.array(f) for f in setup.fields]
         self.slabs = [dict(s) for s in setup.slabs]
         self.lumped = [dict(l) for l in setup.lumped]
-        self.tfsf = self.ade = self.nf2ff = None
+        self.tfsf = getattr(setup, "tfsf", None)
+        self.ade = getattr(setup, "ade", None)
+        self.nf2ff = None
         return self
 
     # ------------------------------------------------------------- oracle
@@ -150,7 +152,8 @@ class KernelCase:
         if self.tfsf is not None:
             t = self.tfsf
             eng.set_tfsf(t["box_s"], t["box_e"], t["e_inc"], t["h_inc"], t["p_int"],
-                         t["p_half"], t["ca"], t["cb"], t["te"], t["th"])
+                         t["p_half"], t["ca"], t["cb"], t["te"], t["th"],
+                         x_offset=t.get("x_offset"))
         for l in self.lumped:
             eng.add_current_source(l["comp"], l["s"], l["e"], l["coff"], l["wave"])
         if self.ade is not None:
@@ -170,13 +173,17 @@ class KernelCase:
                             "coff": rng.standard_normal(shp),
                             "wave": rng.standard_normal(n_steps)})
 
-    def add_ade(self, kind=0, n_poles=2, n_mat=2, frac=0.3):
-        """Random dispersive nodes: a random set of cells, their three E
-        components within the E update ranges, random per-material
-        coefficients."""
+    def add_ade(self, kind=0, n_poles=2, n_mat=2, frac=0.3, margin=0):
+        """Random dispersive nodes: a random set of cells (none within
+        `margin` cells of a lattice face), their three E components within
+        the E update ranges, random per-material coefficients."""
         rng = self.rng
         nx, ny, nz = self.n
         cells = rng.random((nx, ny, nz)) < frac
+        if margin:
+            inner = np.zeros_like(cells)
+            inner[margin:nx - margin, margin:ny - margin, margin:nz - margin] = True
+            cells &= inner
         mat_of_cell = rng.integers(0, n_mat, (nx, ny, nz))
         coef = rng.uniform(-0.2, 0.2, (n_mat, 2 + 7 * n_poles))
         comp, node, material = [], [], []
@@ -255,6 +262,29 @@ class KernelCase:
         out["acc"] = np.zeros(2 * total)
         out["off"] = np.array(offs, dtype=np.int64)
         return out
+
+
+def tfsf_source(n, start, steps, theta=0.7, phi=0.4, psi=0.3, shift=12):
+    """The oracle's TFSF source (box `start` cells in on every axis, an
+    oblique plane wave) for an empty lattice of n cells of 7.5 mm, as the
+    dict KernelCase.tfsf takes; the incident grid is started `shift` steps
+    late so that the pulse reaches the box within a few steps."""
+    from oracle.reference_model import RefSimulation
+    from xfdtd_core_b200 import scene as S
+    dl = 7.5e-3
+    sc = S.Scene(dl=(dl, dl, dl), cfl=0.9, steps=steps + shift, name="tfsf_source")
+    sc.objects.append(S.ObjectSpec("domain", S.cube((0.0, 0.0, 0.0),
+                                                    tuple(c * dl for c in n)), S.air()))
+    tau = dl * 20 / 6e8
+    sc.tfsf = S.TFSFSpec(start[0], start[1], start[2], theta, phi, psi,
+                         S.Waveform("gaussian", tau, 4.5 * tau))
+    r = RefSimulation(sc)
+    assert (r.nx, r.ny, r.nz) == tuple(n)
+    t = dict(r.tfsf)
+    t["e_inc"] = np.ascontiguousarray(t["e_inc"][shift:])
+    t["h_inc"] = np.ascontiguousarray(t["h_inc"][shift:])
+    t["nt"] = steps
+    return t
 
 
 def rel_l2(a, b) -> float:

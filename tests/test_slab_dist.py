@@ -1,9 +1,11 @@
 """The x-slab decomposition (xfdtd_core_b200/slab.py) on CPU: two and three
 gloo ranks each run the oracle on their slab of a seeded lattice (random
-material classes and curl factors, CPML on all six faces, a lumped current
-source) and exchange the ghost planes' E_y, E_z after every step; the owned
-values gathered on rank 0 equal the one-domain oracle run bit for bit.  Plus
-the planning rules: cuts keep clear of the x-normal CPML layers."""
+material classes and curl factors, CPML on all six faces, lumped current
+sources; and a lattice with an oblique TFSF plane wave and ADE media cut by
+slab as well) and exchange the ghost planes' E_y, E_z after every step; the
+owned values gathered on rank 0 equal the one-domain oracle run bit for bit.
+Plus the planning rules: cuts keep clear of the x-normal CPML layers, and the
+cut of the ADE node lists."""
 import os
 import socket
 import sys
@@ -17,11 +19,14 @@ SLABS = ((0, True, 3), (0, False, 2), (1, True, 2), (1, False, 3), (2, True, 2),
 STEPS = 7
 
 
-def _case():
-    from tests.cases import KernelCase
-    c = KernelCase(n=N, seed=21, slabs=SLABS)
+def _case(media=False):
+    from tests.cases import KernelCase, tfsf_source
+    c = KernelCase(n=N, seed=21, slabs=SLABS, field_scale=1e-3 if media else 1.0)
     c.add_lumped(comp=2, s=(8, 4, 4), e=(10, 6, 6), n_steps=STEPS)   # across a ghost region
     c.add_lumped(comp=0, s=(14, 3, 3), e=(17, 5, 5), n_steps=STEPS)  # E_x cells
+    if media:
+        c.tfsf = tfsf_source(N, (6, 3, 3), STEPS)   # x faces 6 and 24: on different ranks
+        c.add_ade(kind=0, n_poles=2, n_mat=2, frac=0.3)
     return c
 
 
@@ -33,7 +38,7 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, out):
+def _worker(rank, world, port, out, media):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
     import torch
@@ -41,7 +46,7 @@ def _worker(rank, world, port, out):
     from tests.cases import KernelCase
     from xfdtd_core_b200 import slab
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    case = _case()
+    case = _case(media)
     parts = slab.plan(N[0], world, x_cpml=(3, 2))
     local = slab.split(case, parts)[rank]
     orc = KernelCase.from_setup(local).oracle()
@@ -70,14 +75,15 @@ def _worker(rank, world, port, out):
     dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("media", [False, True], ids=["plain", "tfsf_ade"])
 @pytest.mark.parametrize("world", [2, 3])
-def test_slab_ranks_equal_one_domain(tmp_path, world):
+def test_slab_ranks_equal_one_domain(tmp_path, world, media):
     import torch.multiprocessing as mp
-    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path), media), nprocs=world,
                        start_method="spawn")
     z = np.load(tmp_path / "slab.npz")
     got = [z[f"arr_{c}"] for c in range(6)]
-    orc = _case().oracle()
+    orc = _case(media).oracle()
     orc.run(STEPS)
     for c, (g, w) in enumerate(zip(got, orc.e + orc.h)):
         assert g.shape == w.shape and np.array_equal(g, w), c
@@ -92,3 +98,25 @@ def test_plan_keeps_cuts_clear_of_x_cpml():
         slab.plan(24, 2, x_cpml=(11, 10))  # ghost plane 11 of the cut at 12 is a CPML layer
     ex = slab.exchanges(parts)
     assert (1, 0, 0, 24) in ex and (0, 26, 1, 2) in ex and len(ex) == 6
+
+
+def test_split_cuts_ade_nodes_and_passes_the_tfsf_offset():
+    from xfdtd_core_b200 import slab
+    case = _case(media=True)
+    parts = slab.plan(N[0], 3, x_cpml=(3, 2))
+    local = slab.split(case, parts)
+    node, comp = case.ade["node"], case.ade["comp"]
+    for p, l in zip(parts, local):
+        assert l.tfsf["x_offset"] == p.lo and l.tfsf["box_s"] == case.tfsf["box_s"]
+        x = node[:, 0]
+        want = np.where(comp == 0, (x >= p.lo) & (x < p.hi), (x > p.lo) & (x < p.hi))
+        assert len(l.ade["comp"]) == int(want.sum())
+        assert np.array_equal(l.ade["node"][:, 0] + p.lo, x[want])
+        assert l.ade["cells"].shape == (p.n,) + N[1:]
+    # every owned dispersive node sits in the list of the rank that owns it
+    for (i, j, k), c in zip(node, comp):
+        owners = [r for r, p in enumerate(parts) if p.own_lo <= i < p.own_hi]
+        assert len(owners) == 1
+        p, l = parts[owners[0]], local[owners[0]]
+        hit = (l.ade["node"] == (i - p.lo, j, k)).all(axis=1) & (l.ade["comp"] == c)
+        assert hit.sum() == 1

@@ -2014,19 +2014,27 @@ xfd_status xfd_add_cpml(xfd_engine* e, const xfd_cpml_slab* sl) {
   return XFD_OK;
 }
 
-xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* t) {
+// xfd_set_tfsf / xfd_set_tfsf_slab.  slab: `t` is the source on a global
+// lattice of which this engine holds the x-slab whose plane 0 is global plane
+// x_offset; the box's x coordinates are global, and every pass is cut to the
+// nodes of this lattice that it corrects.
+static xfd_status set_tfsf_impl(xfd_engine* e, const xfd_tfsf_desc* t, bool slab,
+                                int x_offset) {
   if (!e || !t) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null TFSF");
   const int n[3] = {e->L.nx, e->L.ny, e->L.nz};
   for (int a = 0; a < 3; ++a) {
-    if (t->box_s[a] < 1 || t->box_e[a] > n[a] - 1 || t->box_e[a] <= t->box_s[a])
-      return fail(e, XFD_ERR_INVALID_ARGUMENT, "TFSF box out of the grid on axis %d", a);
+    const bool bad = (slab && a == 0)
+                         ? (t->box_s[a] < 1 || t->box_e[a] <= t->box_s[a])
+                         : (t->box_s[a] < 1 || t->box_e[a] > n[a] - 1 ||
+                            t->box_e[a] <= t->box_s[a]);
+    if (bad) return fail(e, XFD_ERR_INVALID_ARGUMENT, "TFSF box out of the grid on axis %d", a);
     if (!t->p_int[a] || !t->p_half[a]) return fail(e, XFD_ERR_INVALID_ARGUMENT, "null projection");
   }
   if (t->aux < 3 || !t->e_inc || !t->h_inc) return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad TFSF grid");
   CUDA_TRY(e, cudaSetDevice(e->device));
   TfsfD d{};
   for (int a = 0; a < 3; ++a) {
-    d.bs[a] = t->box_s[a];
+    d.bs[a] = t->box_s[a] - (a == 0 ? x_offset : 0);  // projections index from the box start
     d.te[a] = t->te[a];
     d.th[a] = t->th[a];
   }
@@ -2067,15 +2075,28 @@ xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* t) {
       P.is_e = is_e;
       const int m = ps.axis, A = (m + 1) % 3, B = (m + 2) % 3;
       for (int a = 0; a < 3; ++a) {
-        P.s[a] = t->box_s[a];
-        P.e[a] = t->box_e[a];
+        P.s[a] = t->box_s[a] - (a == 0 ? x_offset : 0);
+        P.e[a] = t->box_e[a] - (a == 0 ? x_offset : 0);
       }
       // offset_a / offset_b (src/include/waveform_source/tfsf_corrector.h:122-140)
       const bool off_a = (is_e && ps.field == B) || (!is_e && ps.field == A);
       if (off_a) P.e[A] += 1; else P.e[B] += 1;
-      const int cs = ps.neg ? t->box_s[m] : t->box_e[m];
+      const int cs = ps.neg ? P.s[m] : P.e[m];  // the box start / end along m
       P.s[m] = cs;
       P.e[m] = cs + 1;
+      if (slab) {
+        // Cut along x to the nodes of this lattice the pass corrects: x of
+        // the corrected node is i - 1 on a negative H face along x, else i;
+        // E_x, H_y and H_z have nx values along x, the others nx + 1.  (As
+        // the reference cuts its TFSF by the domain it runs on,
+        // src/waveform_source/tfsf_3d.cpp:21-33.)
+        const int sh = (!is_e && ps.neg && m == 0) ? 1 : 0;
+        const bool cells = is_e ? ps.field == 0 : ps.field != 0;
+        const int hi = (cells ? n[0] : n[0] + 1) + sh;
+        const int s0 = std::max(P.s[0], sh), e0 = std::max(std::min(P.e[0], hi), s0);
+        P.s[0] = s0;
+        P.e[0] = e0;
+      }
       const int equation_flag = is_e ? 1 : -1;
       const int different_flag = (ps.field == A) ? -1 : 1;
       const int direction_flag = ps.neg ? -1 : 1;
@@ -2114,6 +2135,14 @@ xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* t) {
   e->have_tfsf = true;
   e->graph_dirty = true;
   return XFD_OK;
+}
+
+xfd_status xfd_set_tfsf(xfd_engine* e, const xfd_tfsf_desc* t) {
+  return set_tfsf_impl(e, t, false, 0);
+}
+
+xfd_status xfd_set_tfsf_slab(xfd_engine* e, const xfd_tfsf_desc* t, int32_t x_offset) {
+  return set_tfsf_impl(e, t, true, x_offset);
 }
 
 xfd_status xfd_add_current_source(xfd_engine* e, int32_t comp, const int32_t box_s[3],

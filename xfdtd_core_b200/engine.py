@@ -102,6 +102,7 @@ def load(build_if_missing: bool = True):
         "xfd_set_curl_factors": ([vp, _dp * 3, _dp * 3], ctypes.c_int),
         "xfd_add_cpml": ([vp, ctypes.POINTER(CpmlSlab)], ctypes.c_int),
         "xfd_set_tfsf": ([vp, ctypes.POINTER(TfsfDesc)], ctypes.c_int),
+        "xfd_set_tfsf_slab": ([vp, ctypes.POINTER(TfsfDesc), _i32], ctypes.c_int),
         "xfd_add_current_source": ([vp, _i32, _i32 * 3, _i32 * 3, _dp, _dp], ctypes.c_int),
         "xfd_add_inductor": ([vp, _i32, _i32 * 3, _i32 * 3, _dp, _dp], ctypes.c_int),
         "xfd_set_ade": ([vp, ctypes.POINTER(AdeDesc)], ctypes.c_int),
@@ -161,7 +162,8 @@ def load(build_if_missing: bool = True):
 def exported_symbols() -> List[str]:
     """Names declared in include/xfd_engine.h that the library must export."""
     return ["xfd_create", "xfd_destroy", "xfd_last_error", "xfd_set_material_classes",
-            "xfd_set_curl_factors", "xfd_add_cpml", "xfd_set_tfsf", "xfd_add_current_source",
+            "xfd_set_curl_factors", "xfd_add_cpml", "xfd_set_tfsf", "xfd_set_tfsf_slab",
+            "xfd_add_current_source",
             "xfd_add_inductor",
             "xfd_set_ade", "xfd_set_nf2ff", "xfd_get_nf2ff", "xfd_add_movie",
             "xfd_get_movie_frames", "xfd_upload_fields", "xfd_download_fields",
@@ -253,7 +255,10 @@ class Engine:
         s = CpmlSlab(axis, int(negative), thickness, e_start, h_start, *[_p(a) for a in arrs])
         self._check(self.L.xfd_add_cpml(self.h, ctypes.byref(s)), "add_cpml")
 
-    def set_tfsf(self, box_s, box_e, e_inc, h_inc, p_int, p_half, ca, cb, te, th):
+    def set_tfsf(self, box_s, box_e, e_inc, h_inc, p_int, p_half, ca, cb, te, th,
+                 x_offset=None):
+        """TFSF3D (xfd_set_tfsf); with x_offset, the source of a global lattice
+        on the x-slab whose plane 0 is global plane x_offset (xfd_set_tfsf_slab)."""
         e_inc, h_inc = _f64(e_inc), _f64(h_inc)
         p_int = [_f64(a) for a in p_int]
         p_half = [_f64(a) for a in p_half]
@@ -264,7 +269,11 @@ class Engine:
             d.ca[a], d.cb[a], d.te[a], d.th[a] = ca[a], cb[a], te[a], th[a]
         d.aux = e_inc.shape[1]
         d.e_inc, d.h_inc = _p(e_inc), _p(h_inc)
-        self._check(self.L.xfd_set_tfsf(self.h, ctypes.byref(d)), "set_tfsf")
+        if x_offset is None:
+            self._check(self.L.xfd_set_tfsf(self.h, ctypes.byref(d)), "set_tfsf")
+        else:
+            self._check(self.L.xfd_set_tfsf_slab(self.h, ctypes.byref(d), int(x_offset)),
+                        "set_tfsf_slab")
 
     def add_current_source(self, comp: int, box_s, box_e, coff, waveform):
         coff, waveform = _f64(coff), _f64(waveform)

@@ -27,8 +27,15 @@ bit for bit.  The x-normal CPML slabs stay whole on the first and last rank:
 cuts keep the ghost cells and planes clear of their layers.  y- and
 z-normal slabs, materials, curl factors, fields and lumped sources are cut
 by intersection with each local lattice (sources in a ghost region run on
-both ranks, which keeps the ghost values exact).  TFSF, ADE and NF2FF are
-not split here: lattices with them run on one engine.
+both ranks, which keeps the ghost values exact).  A TFSF source is cut the
+same way: each engine takes the global source and its x offset
+(xfd_set_tfsf_slab), which keeps only the face passes' nodes of its local
+lattice (the reference cuts TFSF3D by its domain, src/waveform_source/
+tfsf_3d.cpp:21-33).  ADE media are cut by node: every dispersive E node of
+the local lattice, ghost cells included, except E_y, E_z on a ghost or
+boundary plane (values the exchange overwrites, and that no update of an
+owned value reads).  NF2FF surfaces are not split here: lattices with one run
+on one engine.
 """
 from __future__ import annotations
 
@@ -98,15 +105,19 @@ class LocalSetup:
     slabs: List[Dict]
     lumped: List[Dict]
     fields: List[np.ndarray]
+    tfsf: Optional[Dict] = None  # the global source plus "x_offset"
+    ade: Optional[Dict] = None   # the local dispersive nodes
 
 
 def split(setup, parts: Sequence[SlabPart]) -> List[LocalSetup]:
     """Cuts a lattice set-up (attributes n, table, lattice_class, fe, fh,
-    slabs, lumped, fields; optional tfsf / ade / nf2ff must be None) into the
-    local set-ups of `parts`."""
-    for name in ("tfsf", "ade", "nf2ff"):
-        if getattr(setup, name, None):
-            raise ValueError(f"{name} is not split across slabs")
+    slabs, lumped, fields; optional tfsf and ade -- the dicts of
+    tests.cases.KernelCase -- and nf2ff, which must be None) into the local
+    set-ups of `parts`."""
+    if getattr(setup, "nf2ff", None):
+        raise ValueError("nf2ff is not split across slabs")
+    tfsf = getattr(setup, "tfsf", None)
+    ade = getattr(setup, "ade", None)
     nx, ny, nz = setup.n
     out = []
     for p in parts:
@@ -139,12 +150,33 @@ def split(setup, parts: Sequence[SlabPart]) -> List[LocalSetup]:
             q["coff"] = np.ascontiguousarray(l["coff"][s0 - l["s"][0]:e0 - l["s"][0]])
             lumped.append(q)
         fields = [np.ascontiguousarray(f[_x_range(p, c)]) for c, f in enumerate(setup.fields)]
+        ltfsf = None
+        if tfsf:
+            ltfsf = dict(tfsf)
+            ltfsf["x_offset"] = a
+        lade = None
+        if ade:
+            node = np.asarray(ade["node"]).reshape(-1, 3)
+            comp = np.asarray(ade["comp"])
+            x = node[:, 0]
+            # E_x on cells [a, b); E_y, E_z on the planes strictly inside (a, b)
+            keep = np.where(comp == 0, (x >= a) & (x < b), (x > a) & (x < b))
+            local = node[keep].copy()
+            local[:, 0] -= a
+            lade = {k: v for k, v in ade.items()
+                    if k not in ("node", "comp", "material", "cells", "mat_of_cell")}
+            lade.update(node=np.ascontiguousarray(local, dtype=np.int32),
+                        comp=np.ascontiguousarray(comp[keep]),
+                        material=np.ascontiguousarray(np.asarray(ade["material"])[keep]))
+            for key in ("cells", "mat_of_cell"):  # per-cell form, where given
+                if key in ade:
+                    lade[key] = np.ascontiguousarray(ade[key][a:b])
         out.append(LocalSetup(
             n=(b - a, ny, nz), table=setup.table,
             lattice_class=np.ascontiguousarray(setup.lattice_class[a:b + 1]),
             fe=[np.ascontiguousarray(setup.fe[0][a:b + 1])] + [setup.fe[1], setup.fe[2]],
             fh=[np.ascontiguousarray(setup.fh[0][a:b])] + [setup.fh[1], setup.fh[2]],
-            slabs=slabs, lumped=lumped, fields=fields))
+            slabs=slabs, lumped=lumped, fields=fields, tfsf=ltfsf, ade=lade))
     return out
 
 
@@ -210,6 +242,14 @@ class SlabEngines:
                            sl["b_e"], sl["a_h"], sl["b_h"])
             for l in s.lumped:
                 e.add_current_source(l["comp"], l["s"], l["e"], l["coff"], l["wave"])
+            if s.tfsf is not None:
+                t = s.tfsf
+                e.set_tfsf(t["box_s"], t["box_e"], t["e_inc"], t["h_inc"], t["p_int"],
+                           t["p_half"], t["ca"], t["cb"], t["te"], t["th"],
+                           x_offset=t["x_offset"])
+            if s.ade is not None and len(s.ade["comp"]):
+                a = s.ade
+                e.set_ade(a["kind"], a["np"], a["mat_coeff"], a["comp"], a["node"], a["material"])
             e.upload_fields([f.astype(e.dtype) for f in s.fields])
             self.engines.append(e)
         self.plan = exchanges(self.parts)
