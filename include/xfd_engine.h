@@ -348,8 +348,9 @@ int64_t xfd_current_step(const xfd_engine* e);
  * 1), "march_cp_stages" (single-axis lists with fewer stages, default 1),
  * "march_wide" (two-rows-per-thread interior form, default 0),
  * "march_shift" (tile grid moved to the CPML layers along k, default 0;
- * sweep 7 always moves it along j and i).  Every sweep computes the same
- * update; they differ in speed only.
+ * sweep 7 always moves it along j and i), and of sweep 0: "pdl"
+ * (programmatic dependent launch of the step's kernels, default 1).  Every
+ * sweep computes the same update; they differ in speed only.
  * Failure detection: "stage_wait_cycles" (cycles a TMA-staged sweep (3..7)
  * waits for one staged plane before the CTA gives up, drains its loads in
  * flight and returns; the next xfd_sync reports XFD_ERR_TIMEOUT; 0 = the

@@ -157,3 +157,24 @@ def test_nf2ff_fp64():
     want = acc[0::2] + 1j * acc[1::2]
     assert got.shape == want.shape
     assert np.linalg.norm(got - want) / np.linalg.norm(want) <= FP64_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_programmatic_dependent_launch_leaves_results_bit_equal(precision):
+    """Sweep 0 with programmatic dependent launch (the default on small
+    lattices: each kernel of the step may launch while the one before it
+    finishes, and waits for it at entry) gives the fields, the movie frames
+    and the field-time probe of the plain launches bit for bit."""
+    from xfdtd_core_b200.host import SceneRun
+    from tests.scenes import sphere_small
+    got = []
+    for pdl in (0, 1):
+        r = SceneRun(sphere_small(steps=60), precision=precision, options={"kernel": 0, "pdl": pdl})
+        assert r.get_engine_option("pdl") == pdl
+        r.run(37)
+        r.run(23)
+        r.finish()
+        got.append(r.fields() + [r.movie(0), r.field_time(0)])
+        r.close()
+    for a, b in zip(*got):
+        assert np.array_equal(a, b)

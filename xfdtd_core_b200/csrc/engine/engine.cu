@@ -165,6 +165,7 @@ struct xfd_engine {
   int kernel_mode = 7;
   int ichunk = 32;
   int march_ichunk = 16;  // planes per CTA of the marching split sweeps
+  bool pdl = true;        // sweep 0: programmatic dependent launch
   // Cycles a TMA-staged sweep's stage wait may take before the CTA gives up
   // (error bit 2, XFD_ERR_TIMEOUT at the next sync); 0: about 2 s.
   long long stage_wait = 0;
@@ -1082,6 +1083,27 @@ cudaError_t enqueue_hyb_t(xfd_engine* e, int in, int out) {
   return cudaGetLastError();
 }
 
+// A launch of kernel k, with programmatic stream serialization when `pdl`
+// (the kernel calls pdl_enter first: kernels.cuh).
+template <typename... KP, typename... A>
+cudaError_t launch_k(bool pdl, void (*k)(KP...), dim3 g, dim3 b, cudaStream_t s, A&&... a) {
+  if (!pdl) {
+    k<<<g, b, 0, s>>>(std::forward<A>(a)...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(a)...);
+}
+
 template <typename T>
 cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   cudaStream_t s = e->stream;
@@ -1094,6 +1116,9 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   if (e->ade_kind >= 0) {
     if constexpr (sizeof(T) == 8) ad = e->ade64; else ad = e->ade32;
   }
+  // Sweep 0 (small lattices): its H / E updates, TFSF passes and step
+  // counter go out with programmatic dependent launch (option "pdl").
+  const bool pdl = e->pdl && e->kernel_mode == 0;
   if (e->kernel_mode == 7) {
     cudaError_t c = enqueue_hyb_t<T>(e, in, out);
     if (c != cudaSuccess) return c;
@@ -1273,16 +1298,19 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
     else if (march)
       k_march_h<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
-    else
-      k_update_h<T><<<grd, blk, 0, s>>>(yp);
+    else if (cudaError_t c = launch_k(pdl, k_update_h<T>, grd, blk, s, yp); c != cudaSuccess)
+      return c;
     if (e->n_hterm)
       k_hterm<T><<<blocks_for(e->n_hterm, 256), 256, 0, s>>>(hterm_of<T>(e), e->L, fields);
     if (e->have_tfsf) {
       for (int g = 0; g < 2; ++g) {
         const auto& G = e->tfsf_groups[g];
         if (G.total > 0)
-          k_tfsf<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fields,
-                                                             e->d_step, e->d_err);
+          if (cudaError_t c = launch_k(pdl, k_tfsf<T>, dim3(blocks_for(G.total, 256)), dim3(256), s,
+                                       e->tfsf, G, e->L, fields, (const long long*)e->d_step,
+                                       e->d_err);
+              c != cudaSuccess)
+            return c;
       }
     }
     // E phase: ADE e_cur gather -> updateE + CPML.
@@ -1305,8 +1333,8 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     }
     else if (march)
       k_march_e<T, 8, 32><<<grd_m, blk, 0, s>>>(mp);
-    else
-      k_update_e<T><<<grd, blk, 0, s>>>(yp);
+    else if (cudaError_t c = launch_k(pdl, k_update_e<T>, grd, blk, s, yp); c != cudaSuccess)
+      return c;
   }
   // Coefficient overrides complete the E update of their nodes.
   if (e->n_ovr)
@@ -1324,8 +1352,11 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
     for (int g = 2; g < 4; ++g) {
       const auto& G = e->tfsf_groups[g];
       if (G.total > 0)
-        k_tfsf<T><<<blocks_for(G.total, 256), 256, 0, s>>>(e->tfsf, G, e->L, fields, e->d_step,
-                                                           e->d_err);
+        if (cudaError_t c = launch_k(pdl, k_tfsf<T>, dim3(blocks_for(G.total, 256)), dim3(256), s,
+                                     e->tfsf, G, e->L, fields, (const long long*)e->d_step,
+                                     e->d_err);
+            c != cudaSuccess)
+          return c;
     }
   }
   // record: monitors, then NF2FF (Domain::record, src/domain/domain.cpp:176-184).
@@ -1334,7 +1365,10 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
       k_movie<T><<<blocks_for(mv.n_nodes, 256), 256, 0, s>>>(mv.d, e->L, fields, e->d_step);
   }
   if (e->probes.n_probes)
-    k_probes<T><<<e->probes.n_probes, 256, 0, s>>>(e->probes, fields, e->d_step);
+    if (cudaError_t c = launch_k(pdl, k_probes<T>, dim3(e->probes.n_probes), dim3(256), s,
+                                 e->probes, fields, (const long long*)e->d_step);
+        c != cudaSuccess)
+      return c;
   if (e->have_td)
     k_nf2ff_td<T><<<blocks_for(e->td.P, 256), 256, 0, s>>>(e->td, e->L, fields, e->d_step,
                                                           e->d_err);
@@ -1354,7 +1388,8 @@ cudaError_t enqueue_step_t(xfd_engine* e, long long t) {
   }
   if (e->watchdog > 0 && (t + 1) % e->watchdog == 0)
     k_watchdog<T><<<4 * 148, 256, 0, s>>>(fields, e->n_lat, e->d_err);
-  k_advance<<<1, 1, 0, s>>>(e->d_step);
+  if (cudaError_t c = launch_k(pdl, k_advance, dim3(1), dim3(1), s, e->d_step); c != cudaSuccess)
+    return c;
   e->cur = out;
   return cudaGetLastError();
 }
@@ -2698,6 +2733,7 @@ xfd_status xfd_get_option(const xfd_engine* e, const char* name, int64_t* value)
   else if (!strcmp(name, "march_ichunk")) *value = e->march_ichunk;
   else if (!strcmp(name, "stage_wait_cycles")) *value = e->stage_wait;
   else if (!strcmp(name, "watchdog_interval")) *value = e->watchdog;
+  else if (!strcmp(name, "pdl")) *value = e->pdl ? 1 : 0;
   else if (!strcmp(name, "march_wide")) *value = e->march_wide ? 1 : 0;
   else if (!strcmp(name, "march_concurrent")) *value = e->march_concurrent ? 1 : 0;
   else if (!strcmp(name, "march_split_axes")) *value = e->march_split_axes ? 1 : 0;
@@ -2754,6 +2790,9 @@ xfd_status xfd_set_option(xfd_engine* e, const char* name, int64_t value) {
     if (value < 0 || value > (1LL << 30))
       return fail(e, XFD_ERR_INVALID_ARGUMENT, "watchdog_interval range");
     e->watchdog = value;
+  } else if (!strcmp(name, "pdl")) {
+    e->pdl = value != 0;
+    e->graph_dirty = true;
   } else if (!strcmp(name, "march_ichunk")) {
     if (value < 1 || value > 4096)
       return fail(e, XFD_ERR_INVALID_ARGUMENT, "march_ichunk range");

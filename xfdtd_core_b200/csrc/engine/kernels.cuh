@@ -22,6 +22,18 @@
 
 namespace xfd {
 
+// Programmatic dependent launch (small lattices, option "pdl"): a kernel
+// launched with programmatic stream serialization may start while the kernel
+// before it still runs; griddepcontrol.wait blocks until that kernel has
+// finished and its writes are visible, and launch_dependents lets the next
+// kernel start launching in turn.  In a kernel launched without the
+// attribute both are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+
 struct Lat {
   int nx, ny, nz;
   int NY;  // ny + 1
@@ -195,6 +207,7 @@ __device__ __forceinline__ void update_e_node(const YeeP<T>& p, int i, int j, in
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeP<T> p) {
+  pdl_enter();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -204,6 +217,7 @@ __global__ void __launch_bounds__(256) k_update_h(const __grid_constant__ YeeP<T
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_e(const __grid_constant__ YeeP<T> p) {
+  pdl_enter();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -408,6 +422,7 @@ template <typename T>
 __global__ void k_tfsf(const __grid_constant__ TfsfD tf, const __grid_constant__ TfsfGroupD g,
                        Lat L, T* const* fields, const long long* step,
                        int* err) {
+  pdl_enter();
   tfsf_node<T>(tf, g, L, fields, step, err, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -976,6 +991,7 @@ struct ProbeD {
 template <typename T>
 __global__ void __launch_bounds__(256) k_probes(const __grid_constant__ ProbeD pr, T* const* fields,
                                                 const long long* step) {
+  pdl_enter();
   const int q = blockIdx.x;
   double acc = 0.0;
   for (long long e = pr.begin[q] + threadIdx.x; e < pr.begin[q + 1]; e += blockDim.x)
@@ -992,7 +1008,10 @@ __global__ void __launch_bounds__(256) k_probes(const __grid_constant__ ProbeD p
   }
 }
 
-__global__ void k_advance(long long* step) { *step += 1; }
+__global__ void k_advance(long long* step) {
+  pdl_enter();
+  *step += 1;
+}
 
 // Step counters of many lattices.
 __global__ void k_advance_batch(long long* const* steps, int n) {
