@@ -487,8 +487,11 @@ def run_batched(args, world, rank, local, pg, warmup, steps):
     e2e_value = all_cells * steps / e2e_s / 1e9
     batch.close()
 
-    # the same scenes one at a time: FP32 at the tuned depth, then FP64 plain
-    # (warm-up of one 32-step graph chunk: the timed steps run as graphs)
+    # the same scenes one at a time, FP32 then FP64 plain, each engine at its
+    # own default tile depth (the batch set its engines to the batch's tuned
+    # depth; warm-up of one 32-step graph chunk: the timed steps run as graphs)
+    for r in runs:
+        r.set_engine_option("march_ichunk", 16)
     ms_alone32 = sum(time_alone(r, seq, 32, local) for r in runs)
     for r in runs:
         r.close()

@@ -529,7 +529,9 @@ xfd_status xfd_batch_sync(xfd_batch* b);
 
 /* Options: "graph" (0/1, default 1), "graph_chunk" (steps per graph, default
  * 32), "march_ichunk" (x planes per CTA, the tile depth, default 16),
- * "queue" (0/1, default 1: the persistent work-queue launch), "tile_rows"
+ * "queue" (0/1, default 1: the persistent work-queue launch), "concurrent"
+ * (0/1, default 1: the launch-per-phase form runs its single-axis CPML tile
+ * lists on three side streams beside the other forms), "tile_rows"
  * (rows per tile, 8 or 16; 16 needs the queue form), "queue_wait_cycles"
  * (cycles a queue item waits for the items it depends on before the batch
  * reports XFD_ERR_TIMEOUT; 0: the stage-wait default, about 2 s),

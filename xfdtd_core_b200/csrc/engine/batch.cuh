@@ -50,6 +50,12 @@ struct xfd_batch {
   std::string err;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev = nullptr;
+  // Launch-per-phase form, option "concurrent" (default 1): the sweep-form
+  // launches of a phase on `stream` and three side streams (they sweep
+  // disjoint tiles), forked from and joined back into `stream`.
+  bool concurrent = true;
+  cudaStream_t side[3]{};
+  cudaEvent_t fork_ev = nullptr, join_ev[3]{};
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   std::vector<void*> allocs;  // device tables of the current preparation
   int march_ichunk = 16;
@@ -405,13 +411,29 @@ cudaError_t batch_enqueue_t(xfd_batch* b) {
   const auto* dt = static_cast<const TfsfSceneD<T>*>(b->d_tfsf);
   auto n_of = [&](int f) { return (unsigned)(b->tile_off[f + 1] - b->tile_off[f]); };
   auto list = [&](int f) { return b->d_tiles + b->tile_off[f]; };
+  cudaError_t cerr = cudaSuccess;
+  const bool conc = b->concurrent && b->side[0];
   auto sweeps = [&](auto k_in, auto k_free, auto kx, auto ky, auto kz, auto k_cp) {
-    if (n_of(0)) k_in<<<n_of(0), blk, msm_free, s>>>(dm, list(0));
-    if (n_of(1)) k_free<<<n_of(1), blk, msm_free, s>>>(dm, list(1));
-    if (n_of(2)) kx<<<n_of(2), blk, msm_free, s>>>(dm, list(2));
-    if (n_of(3)) ky<<<n_of(3), blk, msm_free, s>>>(dm, list(3));
-    if (n_of(4)) kz<<<n_of(4), blk, msm_free, s>>>(dm, list(4));
+    // x-, y-, z-only CPML lists on the side streams, the rest on `stream`
+    cudaStream_t sx = conc ? b->side[0] : s, sy = conc ? b->side[1] : s,
+                 sz = conc ? b->side[2] : s;
+    if (conc) {
+      if (cerr == cudaSuccess) cerr = cudaEventRecord(b->fork_ev, s);
+      for (int q = 0; q < 3 && cerr == cudaSuccess; ++q)
+        cerr = cudaStreamWaitEvent(b->side[q], b->fork_ev, 0);
+    }
     if (n_of(5)) k_cp<<<n_of(5), blk, msm, s>>>(dm, list(5));
+    if (n_of(2)) kx<<<n_of(2), blk, msm_free, sx>>>(dm, list(2));
+    if (n_of(3)) ky<<<n_of(3), blk, msm_free, sy>>>(dm, list(3));
+    if (n_of(4)) kz<<<n_of(4), blk, msm_free, sz>>>(dm, list(4));
+    if (n_of(1)) k_free<<<n_of(1), blk, msm_free, s>>>(dm, list(1));
+    if (n_of(0)) k_in<<<n_of(0), blk, msm_free, s>>>(dm, list(0));
+    if (conc) {
+      for (int q = 0; q < 3 && cerr == cudaSuccess; ++q) {
+        cerr = cudaEventRecord(b->join_ev[q], b->side[q]);
+        if (cerr == cudaSuccess) cerr = cudaStreamWaitEvent(s, b->join_ev[q], 0);
+      }
+    }
   };
   auto tfsf = [&](int g) {
     const long long nb = b->tfsf_off[g + 1] - b->tfsf_off[g];
@@ -437,6 +459,7 @@ cudaError_t batch_enqueue_t(xfd_batch* b) {
   tfsf(3);
   const int n = (int)b->eng.size();
   k_advance_batch<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(b->d_steps, n);
+  if (cerr != cudaSuccess) return cerr;
   return cudaGetLastError();
 }
 
@@ -587,7 +610,18 @@ xfd_status xfd_batch_create(xfd_engine* const* engines, int32_t n, xfd_batch** o
   if (c == cudaSuccess) c = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
   if (c == cudaSuccess) c = cudaEventCreate(&b->t0);
   if (c == cudaSuccess) c = cudaEventCreate(&b->t1);
+  if (c == cudaSuccess) c = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+  for (int q = 0; q < 3 && c == cudaSuccess; ++q) {
+    c = cudaStreamCreateWithFlags(&b->side[q], cudaStreamNonBlocking);
+    if (c == cudaSuccess) c = cudaEventCreateWithFlags(&b->join_ev[q], cudaEventDisableTiming);
+  }
   if (c != cudaSuccess) {
+    for (int q = 0; q < 3; ++q) {
+      if (b->join_ev[q]) cudaEventDestroy(b->join_ev[q]);
+      if (b->side[q]) cudaStreamDestroy(b->side[q]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    if (b->t1) cudaEventDestroy(b->t1);
     if (b->t0) cudaEventDestroy(b->t0);
     if (b->ev) cudaEventDestroy(b->ev);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -603,6 +637,12 @@ void xfd_batch_destroy(xfd_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop_graph(b);
   batch_free_tables(b);
+  for (int q = 0; q < 3; ++q) {
+    if (b->side[q]) cudaStreamSynchronize(b->side[q]);
+    if (b->join_ev[q]) cudaEventDestroy(b->join_ev[q]);
+    if (b->side[q]) cudaStreamDestroy(b->side[q]);
+  }
+  if (b->fork_ev) cudaEventDestroy(b->fork_ev);
   if (b->t1) cudaEventDestroy(b->t1);
   if (b->t0) cudaEventDestroy(b->t0);
   if (b->ev) cudaEventDestroy(b->ev);
@@ -683,6 +723,7 @@ xfd_status xfd_batch_get_option(const xfd_batch* b, const char* name, int64_t* v
   else if (!strcmp(name, "autotune")) *value = b->autotune;
   else if (!strcmp(name, "march_split_axes")) *value = b->split_axes ? 1 : 0;
   else if (!strcmp(name, "queue")) *value = b->queue ? 1 : 0;
+  else if (!strcmp(name, "concurrent")) *value = b->concurrent ? 1 : 0;
   else if (!strcmp(name, "tile_rows")) *value = b->tile_rows;
   else if (!strcmp(name, "queue_wait_cycles")) *value = b->queue_wait;
   else if (!strcmp(name, "queue_stall_test")) *value = b->queue_stall_test ? 1 : 0;
@@ -713,6 +754,9 @@ xfd_status xfd_batch_set_option(xfd_batch* b, const char* name, int64_t value) {
   } else if (!strcmp(name, "queue")) {
     b->queue = value != 0;
     b->ready = false;
+    batch_drop_graph(b);
+  } else if (!strcmp(name, "concurrent")) {
+    b->concurrent = value != 0;
     batch_drop_graph(b);
   } else if (!strcmp(name, "tile_rows")) {
     if (value != kMTJ && value != kWideTJ)
