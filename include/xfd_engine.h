@@ -111,6 +111,23 @@ xfd_status xfd_set_e_overrides(xfd_engine* e, int64_t n, const int32_t* node, co
 xfd_status xfd_halo_copy(xfd_engine* dst, int32_t dst_plane, xfd_engine* src, int32_t src_plane,
                          int32_t n_comp, const int32_t* comps);
 
+/* The same planes between an engine and a buffer, for slabs run by one
+ * process per GPU (xfdtd_core_b200/slab.py: SlabRank, which moves the buffers
+ * between the processes with torch.distributed -- NCCL on device buffers, or
+ * gloo on host buffers).  Plane `plane` of each of the n_comp components
+ * `comps` (0..5 = Ex Ey Ez Hx Hy Hz) of the engine's current fields, NY x KP
+ * values each in the engine's padded layout (xfd_plane_values), from the
+ * engine into `buf` (into_engine = 0) or from `buf` into the engine (1),
+ * component after component.  `buf` may be device memory of any device or
+ * host memory (pinned for speed).  Asynchronous, ordered on the engine's
+ * stream after its queued steps; xfd_sync(e) waits for it.
+ * Replaces: the buffer side of the reference's halo exchange
+ * (MpiSupport::sendRecvHyXHead/Tail, src/parallel/mpi_support.cpp:98-229). */
+xfd_status xfd_plane_copy(xfd_engine* e, int32_t plane, int32_t n_comp, const int32_t* comps,
+                          void* buf, int32_t into_engine);
+/* Values of one padded x-plane of one component: NY x KP. */
+int64_t xfd_plane_values(const xfd_engine* e);
+
 /* Per-node H curl-term corrections: after the H sweep of every step, the H
  * component comp[q] at node (node[3q], node[3q+1], node[3q+2]) gets
  *   delta_a[q] * (E_a[x_b+1] - E_a) + delta_b[q] * (E_b[x_a+1] - E_b)

@@ -1924,6 +1924,34 @@ xfd_status xfd_halo_copy(xfd_engine* dst, int32_t dst_plane, xfd_engine* src, in
   return XFD_OK;
 }
 
+xfd_status xfd_plane_copy(xfd_engine* e, int32_t plane, int32_t n_comp, const int32_t* comps,
+                          void* buf, int32_t into_engine) {
+  if (!e || n_comp < 1 || n_comp > 6 || !comps || !buf)
+    return fail(e, XFD_ERR_INVALID_ARGUMENT, "bad plane copy arguments");
+  for (int q = 0; q < n_comp; ++q) {
+    const int c = comps[q];
+    const int extra = (c == 1 || c == 2 || c == 3) ? 1 : 0;  // E_y, E_z, H_x: nx + 1 planes
+    if (c < 0 || c > 5 || plane < 0 || plane >= e->L.nx + extra)
+      return fail(e, XFD_ERR_INVALID_ARGUMENT, "plane copy component %d / plane out of range", c);
+  }
+  CUDA_TRY(e, cudaSetDevice(e->device));
+  const size_t bytes = (size_t)e->L.NY * e->L.KP * e->wsize;
+  for (int q = 0; q < n_comp; ++q) {
+    unsigned char* f =
+        static_cast<unsigned char*>(e->fbuf[e->cur][comps[q]]) + (size_t)plane * bytes;
+    unsigned char* b = static_cast<unsigned char*>(buf) + (size_t)q * bytes;
+    // cudaMemcpyDefault: `buf` may be device memory (of any device) or host
+    // memory; stream-ordered with the engine's steps either way.
+    CUDA_TRY(e, cudaMemcpyAsync(into_engine ? f : b, into_engine ? b : f, bytes, cudaMemcpyDefault,
+                                e->stream));
+  }
+  return XFD_OK;
+}
+
+int64_t xfd_plane_values(const xfd_engine* e) {
+  return e ? (int64_t)e->L.NY * e->L.KP : 0;
+}
+
 xfd_status xfd_set_h_term_overrides(xfd_engine* e, int64_t n, const int32_t* node,
                                     const int32_t* comp, const double* delta_a,
                                     const double* delta_b) {

@@ -130,6 +130,8 @@ def load(build_if_missing: bool = True):
         "xfd_set_h_term_overrides": ([vp, _i64, ctypes.POINTER(_i32), ctypes.POINTER(_i32), _dp,
                                       _dp], ctypes.c_int),
         "xfd_halo_copy": ([vp, _i32, vp, _i32, _i32, ctypes.POINTER(_i32)], ctypes.c_int),
+        "xfd_plane_copy": ([vp, _i32, _i32, ctypes.POINTER(_i32), vp, _i32], ctypes.c_int),
+        "xfd_plane_values": ([vp], _i64),
         "xfd_checkpoint_save": ([vp, _i32], ctypes.c_int),
         "xfd_checkpoint_load": ([vp, _i32], ctypes.c_int),
         "xfd_checkpoint_drop": ([vp, _i32], ctypes.c_int),
@@ -171,6 +173,7 @@ def exported_symbols() -> List[str]:
             "xfd_get_option", "xfd_nf2ff_step_static", "xfd_nf2ff_far_field", "xfd_stream",
             "xfd_launches_per_step", "xfd_stencil_bytes_per_step",
             "xfd_algorithmic_bytes_per_step", "xfd_set_e_overrides", "xfd_set_h_term_overrides", "xfd_halo_copy",
+            "xfd_plane_copy", "xfd_plane_values",
             "xfd_checkpoint_save", "xfd_checkpoint_load", "xfd_checkpoint_drop",
             "xfd_checkpoint_step", "xfd_adjoint_run", "xfd_set_nf2ff_td", "xfd_get_nf2ff_td",
             "xfd_add_probe", "xfd_get_probe",
@@ -366,6 +369,19 @@ class Engine:
         arr = (_i32 * len(comps))(*comps)
         self._check(self.L.xfd_halo_copy(self.h, int(dst_plane), src.h, int(src_plane),
                                          len(comps), arr), "halo_copy")
+
+    def plane_values(self) -> int:
+        """xfd_plane_values: values of one padded x-plane (NY x KP)."""
+        return int(self.L.xfd_plane_values(self.h))
+
+    def plane_copy(self, plane: int, comps: Sequence[int], buf_ptr: int, into_engine: bool):
+        """xfd_plane_copy: x-plane `plane` of components `comps` between this
+        engine's current fields and the buffer at `buf_ptr` (device or host,
+        len(comps) x plane_values() values of the engine's precision)."""
+        arr = (_i32 * len(comps))(*comps)
+        self._check(self.L.xfd_plane_copy(self.h, int(plane), len(comps), arr,
+                                          ctypes.c_void_p(int(buf_ptr)), 1 if into_engine else 0),
+                    "plane_copy")
 
     def stream(self) -> int:
         return int(self.L.xfd_stream(self.h) or 0)

@@ -215,7 +215,32 @@ def gather(parts: Sequence[SlabPart], local_fields: Sequence[Sequence[np.ndarray
     return out
 
 
-# ------------------------------------------------------------ engine runner
+# ------------------------------------------------------------ engine runners
+def make_engine(s: LocalSetup, device: int = 0, precision: int = 0, n_steps: int = 1,
+                options: Optional[Dict[str, int]] = None):
+    """An engine over one slab's local set-up."""
+    from xfdtd_core_b200.engine import Engine
+    e = Engine(*s.n, precision=precision, n_steps=n_steps, dt=1.0, device=device)
+    for k, v in (options or {}).items():
+        e.set_option(k, v)
+    e.set_material_classes(s.table, s.lattice_class)
+    e.set_curl_factors(s.fe, s.fh)
+    for sl in s.slabs:
+        e.add_cpml(sl["m"], sl["neg"], sl["n"], sl["e_start"], sl["h_start"], sl["a_e"],
+                   sl["b_e"], sl["a_h"], sl["b_h"])
+    for l in s.lumped:
+        e.add_current_source(l["comp"], l["s"], l["e"], l["coff"], l["wave"])
+    if s.tfsf is not None:
+        t = s.tfsf
+        e.set_tfsf(t["box_s"], t["box_e"], t["e_inc"], t["h_inc"], t["p_int"], t["p_half"],
+                   t["ca"], t["cb"], t["te"], t["th"], x_offset=t["x_offset"])
+    if s.ade is not None and len(s.ade["comp"]):
+        a = s.ade
+        e.set_ade(a["kind"], a["np"], a["mat_coeff"], a["comp"], a["node"], a["material"])
+    e.upload_fields([f.astype(e.dtype) for f in s.fields])
+    return e
+
+
 class SlabEngines:
     """One engine per slab in this process (each on its own device, or all on
     one), stepped together: every step runs each engine one step, then copies
@@ -227,31 +252,10 @@ class SlabEngines:
     def __init__(self, setups: Sequence[LocalSetup], parts: Sequence[SlabPart],
                  devices: Optional[Sequence[int]] = None, precision: int = 0,
                  n_steps: int = 1, options: Optional[Dict[str, int]] = None):
-        from xfdtd_core_b200.engine import Engine
         self.parts = list(parts)
         self.devices = list(devices) if devices is not None else [0] * len(parts)
-        self.engines = []
-        for s, dev in zip(setups, self.devices):
-            e = Engine(*s.n, precision=precision, n_steps=n_steps, dt=1.0, device=dev)
-            for k, v in (options or {}).items():
-                e.set_option(k, v)
-            e.set_material_classes(s.table, s.lattice_class)
-            e.set_curl_factors(s.fe, s.fh)
-            for sl in s.slabs:
-                e.add_cpml(sl["m"], sl["neg"], sl["n"], sl["e_start"], sl["h_start"], sl["a_e"],
-                           sl["b_e"], sl["a_h"], sl["b_h"])
-            for l in s.lumped:
-                e.add_current_source(l["comp"], l["s"], l["e"], l["coff"], l["wave"])
-            if s.tfsf is not None:
-                t = s.tfsf
-                e.set_tfsf(t["box_s"], t["box_e"], t["e_inc"], t["h_inc"], t["p_int"],
-                           t["p_half"], t["ca"], t["cb"], t["te"], t["th"],
-                           x_offset=t["x_offset"])
-            if s.ade is not None and len(s.ade["comp"]):
-                a = s.ade
-                e.set_ade(a["kind"], a["np"], a["mat_coeff"], a["comp"], a["node"], a["material"])
-            e.upload_fields([f.astype(e.dtype) for f in s.fields])
-            self.engines.append(e)
+        self.engines = [make_engine(s, dev, precision, n_steps, options)
+                        for s, dev in zip(setups, self.devices)]
         self.plan = exchanges(self.parts)
 
     def step(self, n: int = 1):
@@ -273,3 +277,80 @@ class SlabEngines:
     def close(self):
         for e in self.engines:
             e.close()
+
+
+class SlabRank:
+    """One rank of a slab decomposition run by one process per GPU under
+    torch.distributed (the form for several GPUs of one node: the reference
+    runs one MPI process per domain).  The rank holds the engine of its slab;
+    after every step the ghost planes' E_y, E_z move to the neighbours with
+    torch.distributed point-to-point calls, grouped in one batch_isend_irecv
+    so that every rank posts the same calls in the same order.  On an NCCL
+    process group the buffers are tensors on this rank's GPU, and the planes
+    go GPU to GPU (through NVLink between peers; no library kernel ever reads
+    another GPU's memory); on gloo they are pinned host tensors.  The engine's
+    stream and the transfer meet on the host: the planes are copied out and
+    the stream synchronised before the sends, and copied in after the
+    receives completed."""
+
+    def __init__(self, setup: LocalSetup, parts: Sequence[SlabPart], rank: int, device: int = 0,
+                 group=None, precision: int = 0, n_steps: int = 1,
+                 options: Optional[Dict[str, int]] = None):
+        import torch
+        import torch.distributed as dist
+        self.parts, self.rank, self.group = list(parts), rank, group
+        self.device = device
+        self.engine = make_engine(setup, device, precision, n_steps, options)
+        self.plan = exchanges(self.parts)
+        self.on_device = dist.get_backend(group) == "nccl"
+        dtype = torch.float64 if precision == 0 else torch.float32
+        size = len(GHOST_COMPONENTS) * self.engine.plane_values()
+
+        def buf():
+            if self.on_device:
+                return torch.empty(size, dtype=dtype, device=torch.device("cuda", device))
+            return torch.empty(size, dtype=dtype).pin_memory()
+
+        self.send = {(d, sp): buf() for d, dp, s, sp in self.plan if s == rank}
+        self.recv = {(s, dp): buf() for d, dp, s, sp in self.plan if d == rank}
+
+    def step(self, n: int = 1):
+        import torch
+        import torch.distributed as dist
+        for _ in range(n):
+            self.engine.run(1)
+            for d, dp, s, sp in self.plan:
+                if s == self.rank:
+                    self.engine.plane_copy(sp, GHOST_COMPONENTS, self.send[(d, sp)].data_ptr(),
+                                           into_engine=False)
+            self.engine.sync()
+            ops = []
+            for d, dp, s, sp in self.plan:  # the same list, in the same order, on every rank
+                if s == self.rank:
+                    ops.append(dist.P2POp(dist.isend, self.send[(d, sp)], d, self.group))
+                if d == self.rank:
+                    ops.append(dist.P2POp(dist.irecv, self.recv[(s, dp)], s, self.group))
+            if ops:
+                for r in dist.batch_isend_irecv(ops):
+                    r.wait()
+            if self.on_device:
+                torch.cuda.synchronize(self.device)
+            for d, dp, s, sp in self.plan:
+                if d == self.rank:
+                    self.engine.plane_copy(dp, GHOST_COMPONENTS, self.recv[(s, dp)].data_ptr(),
+                                           into_engine=True)
+
+    def sync(self):
+        self.engine.sync()
+
+    def fields(self) -> List[np.ndarray]:
+        """The global fields, on every rank (the owned values of all ranks)."""
+        import torch.distributed as dist
+        local = self.engine.download_fields()
+        got = [None] * len(self.parts)
+        dist.all_gather_object(got, local, group=self.group)
+        n = (self.parts[-1].own_hi,) + tuple(self.engine.n[1:])
+        return gather(self.parts, got, n)
+
+    def close(self):
+        self.engine.close()
