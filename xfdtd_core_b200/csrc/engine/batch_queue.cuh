@@ -28,8 +28,9 @@
 // Writes of one level are read by TMA loads (the async proxy) of a later level
 // in the same launch, so each thread fences the generic and async proxies
 // after each item, and the thread that issues the loads fences again after
-// its wait (the first item of a CTA has no earlier accesses to order).  The last CTA to leave the queue resets the head and the done
-// counters for the next launch and advances the lattices' step counters.
+// its wait (the first item of a CTA has no earlier accesses to order).  The
+// last CTA to leave the queue resets the head and the done counters for the
+// next launch and advances the lattices' step counters.
 #pragma once
 
 namespace {
