@@ -3,9 +3,11 @@ gloo ranks each run the oracle on their slab of a seeded lattice (random
 material classes and curl factors, CPML on all six faces, lumped current
 sources; and a lattice with an oblique TFSF plane wave and ADE media cut by
 slab as well) and exchange the ghost planes' E_y, E_z after every step; the
-owned values gathered on rank 0 equal the one-domain oracle run bit for bit.
-Plus the planning rules: cuts keep clear of the x-normal CPML layers, and the
-cut of the ADE node lists."""
+owned values gathered on rank 0 equal the one-domain oracle run bit for bit.  The
+same with SlabRank (the one-process-per-GPU runner) driving the exchange,
+the oracle standing in for each rank's engine.  Plus the planning rules:
+cuts keep clear of the x-normal CPML layers, and the cut of the ADE node
+lists."""
 import os
 import socket
 import sys
@@ -120,3 +122,76 @@ def test_split_cuts_ade_nodes_and_passes_the_tfsf_offset():
         p, l = parts[owners[0]], local[owners[0]]
         hit = (l.ade["node"] == (i - p.lo, j, k)).all(axis=1) & (l.ade["comp"] == c)
         assert hit.sum() == 1
+
+
+class _OracleEngine:
+    """Stand-in for a slab's engine in SlabRank on CPU: the oracle of the
+    slab steps, and plane_copy moves the ghost components of one x-plane
+    between the oracle's arrays and the exchange buffer (a (ny+1) x (nz+1)
+    segment per component in this stand-in's layout)."""
+
+    def __init__(self, setup):
+        from tests.cases import KernelCase
+        self.orc = KernelCase.from_setup(setup).oracle()
+        self.n = tuple(setup.n)
+
+    def plane_values(self):
+        return (self.n[1] + 1) * (self.n[2] + 1)
+
+    def run(self, k):
+        self.orc.run(k)
+
+    def plane_copy(self, plane, comps, ptr, into_engine):
+        import ctypes
+        pv = self.plane_values()
+        buf = np.ctypeslib.as_array((ctypes.c_double * (pv * len(comps))).from_address(ptr))
+        for q, c in enumerate(comps):
+            shape = self.orc.e[c][plane].shape  # a component's plane fits in (ny+1) x (nz+1)
+            part = buf[q * pv:q * pv + shape[0] * shape[1]]
+            if into_engine:
+                self.orc.e[c][plane] = part.reshape(shape)
+            else:
+                part[:] = self.orc.e[c][plane].ravel()
+
+    def sync(self):
+        pass
+
+    def download_fields(self):
+        return [a.copy() for a in self.orc.e + self.orc.h]
+
+    def close(self):
+        pass
+
+
+def _rank_worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    from xfdtd_core_b200 import slab
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    slab.make_engine = lambda s, *a, **k: _OracleEngine(s)
+    case = _case(media=True)
+    parts = slab.plan(N[0], world, x_cpml=(3, 2))
+    run = slab.SlabRank(slab.split(case, parts)[rank], parts, rank, device=0, n_steps=STEPS)
+    run.step(STEPS)
+    fields = run.fields()
+    if rank == 0:
+        np.savez(os.path.join(out, "rank.npz"), *fields)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_rank_exchange_equals_one_domain(tmp_path, world):
+    """SlabRank's exchange (plane_copy into gloo buffers, one
+    batch_isend_irecv per step, plane_copy back) with the oracle standing in
+    for each rank's engine: the gathered fields equal the one-domain oracle
+    bit for bit (oblique TFSF wave and ADE media cut per slab)."""
+    import torch.multiprocessing as mp
+    mp.start_processes(_rank_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn")
+    z = np.load(tmp_path / "rank.npz")
+    orc = _case(media=True).oracle()
+    orc.run(STEPS)
+    for c, w in enumerate(orc.e + orc.h):
+        assert np.array_equal(z[f"arr_{c}"], w), c

@@ -309,7 +309,8 @@ class SlabRank:
         def buf():
             if self.on_device:
                 return torch.empty(size, dtype=dtype, device=torch.device("cuda", device))
-            return torch.empty(size, dtype=dtype).pin_memory()
+            t = torch.empty(size, dtype=dtype)
+            return t.pin_memory() if torch.cuda.is_available() else t
 
         self.send = {(d, sp): buf() for d, dp, s, sp in self.plan if s == rank}
         self.recv = {(s, dp): buf() for d, dp, s, sp in self.plan if d == rank}
